@@ -1,0 +1,400 @@
+#!/usr/bin/env python
+"""AO Mrays/s and build Mtri/s of minimumlbvh_b200 on B200.
+
+Workload (default ``soup4m_ao64``): a 4,194,304-triangle Gaussian-cluster soup
+(64 clusters, sigma 0.02, lognormal edges), built into an LBVH, then one AO
+frame at 1920 x 1080: one closest-hit primary ray per pixel and 64
+Owen-Sobol cosine AO rays (radius 0.1) per hit. ``heightfield_ao16`` is the
+212,992-triangle heightfield + icospheres scene at 512 x 512 with 16 AO rays
+of radius 0.25.
+
+A step is one AO frame (primary + AO rays) over the resident BVH; the build
+is timed separately (one build per step) and reported in ``build``. ``e2e``
+times the whole path through the C ABI from pinned HOST triangles: upload,
+build, AO frame, download of the packed image.
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl reference] [--workload NAME]
+
+Under torchrun (N > 1) every rank renders its own replica of the frame
+(the path does not shard: see DESIGN.md); times are the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    "soup4m_ao64": dict(scene="soup", n=4_194_304, w=1920, h=1080, ns=64, radius=0.1),
+    "heightfield_ao16": dict(scene="heightfield", n=212_992, w=512, h=512, ns=16, radius=0.25),
+}
+METRIC = "AO Mrays/s (primary + AO rays, stack-free LBVH traversal)"
+BUILD_BYTES_PER_TRI = 291  # algorithmic bytes per triangle of the build chain
+
+
+def make_scene(wl):
+    from minimumlbvh_b200 import scenes
+    if wl["scene"] == "soup":
+        tris = scenes.gaussian_soup(wl["n"])
+        cam = scenes.camera_soup()
+    else:
+        tris = scenes.heightfield_icospheres()
+        cam = scenes.camera_heightfield()
+    return tris, cam
+
+
+class ClockSampler:
+    """Samples SM clocks and throttle reasons with nvidia-smi while running."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.proc = None
+        self.lines = []
+        self.device = device_index
+        self.error = None
+
+    def __enter__(self):
+        try:
+            import torch
+            uuid = str(torch.cuda.get_device_properties(self.device).uuid)
+            ident = ["--id=GPU-" + uuid if not uuid.startswith("GPU-") else "--id=" + uuid]
+        except Exception:
+            ident = ["-i", str(self.device)]
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", *ident, f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception as e:  # no nvidia-smi
+            self.error = str(e)
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        rows = []
+        for ln in self.lines:
+            p = [x.strip() for x in ln.split(",")]
+            if len(p) < 8:
+                continue
+            try:
+                rows.append((float(p[0]), float(p[1]), p[4:8]))
+            except ValueError:
+                continue
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0,
+                    "note": self.error or "no nvidia-smi samples"}
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for _, _, flags in rows for i, f in enumerate(flags) if f.lower() == "active"})
+        return {"sm_mhz": float(np.median([r[0] for r in rows])), "sm_max_mhz": max(r[1] for r in rows),
+                "reasons": reasons, "samples": len(rows)}
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def committed_traffic(workload):
+    """DRAM bytes per launch of the dominant kernel from the committed ncu
+    summary (profiles/traffic.json), or None."""
+    path = os.path.join(ROOT, "profiles", "traffic.json")
+    if not os.path.exists(path):
+        return None
+    with open(path) as f:
+        return json.load(f).get(workload)
+
+
+def cpu_sample_ao(wl, tris, cam_arr, out, seconds: float):
+    """Reference CPU AO (oracle/_ref: the reference's intersect_stackfree and
+    sampling code, all host threads) on a band of rows around the middle of
+    the frame, grown until about `seconds` of wall time."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import _oracle as O
+    w, h = wl["w"], wl["h"]
+    occ = np.zeros(w * h, np.uint32)
+    nodes = out["nodes"]
+    if O.ref_available():
+        kind, L = "reference", O.ref()
+        threads = L.ref_threads()
+
+        def run(r0, r1):
+            st = np.zeros(1, np.uint64)
+            L.ref_ao_param(O.P(occ), w, h, O.P(cam_arr), out["root"], O.P(nodes), O.P(tris), wl["ns"],
+                           float(wl["radius"]), 12345, r0, r1, O.P(st))
+            return int(st[0])
+    else:
+        kind, L = "port", O.oracle()
+        threads = int(os.environ.get("MLBVH_ORACLE_THREADS", os.cpu_count() or 1))
+
+        def run(r0, r1):
+            _, _, cnt = O.render_ao(cam_arr, out["root"], nodes, tris, w, h, wl["ns"], wl["radius"], 12345, 1,
+                                    trig=0, rows=(r0, r1), counters=True)
+            return int(cnt[2])
+    rows, rays, elapsed = 2, 0, 0.0
+    mid = h // 2
+    while True:
+        r0 = max(0, mid - rows // 2)
+        r1 = min(h, r0 + rows)
+        t0 = time.perf_counter()
+        rays = run(r0, r1)
+        elapsed = time.perf_counter() - t0
+        if elapsed >= seconds or r1 - r0 >= h:
+            break
+        rows = min(h, max(rows * 2, int(rows * seconds / max(elapsed, 1e-3))))
+    return {"value": rays / elapsed / 1e6, "unit": "Mrays/s", "cores": threads, "kind": kind,
+            "sample": f"AO rows {r0}-{r1 - 1} of the {w}x{h} frame ({rays} rays, {elapsed:.1f} s)"}, elapsed
+
+
+def cpu_build_baseline(tris):
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import _oracle as O
+    n = len(tris)
+    nodes = np.zeros((n - 1, 16), np.uint32)
+    deltas = np.zeros(n - 1, np.uint8)
+    root = np.zeros(1, np.uint32)
+    if O.ref_available():
+        t0 = time.perf_counter()
+        O.ref().ref_cpu_builder(O.P(tris), n, 2, O.P(nodes), O.P(deltas), O.P(root))  # BVHCPUBuilder, parallel
+        dt = time.perf_counter() - t0
+        return {"mtri_s": n / dt / 1e6, "ms": dt * 1e3, "kind": "reference",
+                "what": "BVHCPUBuilder::build with BUILD_OPTION_CPU_PARALLEL"}
+    t0 = time.perf_counter()
+    O.build(tris)
+    dt = time.perf_counter() - t0
+    return {"mtri_s": n / dt / 1e6, "ms": dt * 1e3, "kind": "port", "what": "oracle build (serial)"}
+
+
+def run_reference(args, wl, rank):
+    """The reference's own CPU implementation of the path, all host threads."""
+    if rank != 0:
+        return
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import _oracle as O
+    tris, (eye, c, up, fovy) = make_scene(wl)
+    out = O.build(tris)
+    cam_arr = O.lookat(eye, c, up, fovy, wl["w"], wl["h"])
+    values = []
+    sample = None
+    for i in range(args.warmup + args.steps):
+        s, _ = cpu_sample_ao(wl, tris, cam_arr, out, seconds=args.ref_seconds)
+        if i >= args.warmup:
+            values.append(s["value"])
+            sample = s
+    value = float(np.median(values))
+    build = cpu_build_baseline(tris)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
+        "config": {"workload": args.workload, "triangles": wl["n"], "image": [wl["w"], wl["h"]],
+                   "ao_samples": wl["ns"], "ao_radius": wl["radius"], "parallelism": "host threads"},
+        "cpu_baseline": {"value": value, "unit": "Mrays/s", "cores": sample["cores"], "kind": sample["kind"],
+                         "sample": sample["sample"]},
+        "e2e": {"value": value, "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "build": build,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="soup4m_ao64", choices=sorted(WORKLOADS))
+    ap.add_argument("--cpu-seconds", type=float, default=8.0, help="wall time of the CPU-baseline AO sample")
+    ap.add_argument("--ref-seconds", type=float, default=4.0, help="wall time of one reference-arm step")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    wl = WORKLOADS[args.workload]
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local = int(os.environ.get("LOCAL_RANK", 0))
+    if args.impl == "reference":
+        run_reference(args, wl, rank)
+        return
+
+    import torch
+    import minimumlbvh_b200 as mb
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    tris, (eye, c, up, fovy) = make_scene(wl)
+    n, w, h = len(tris), wl["w"], wl["h"]
+    host_tris = torch.from_numpy(tris).pin_memory()
+    d_tris = host_tris.to(dev)
+    builder = mb.BVHGPUBuilder()
+    sorter = mb.OnesweepSort(local)
+    cam = mb.RayGenerator().lookat(eye, c, up, fovy, w, h)
+    pixels = torch.zeros(w * h, dtype=torch.int32, device=dev)
+    host_pixels = torch.empty(w * h, dtype=torch.int32).pin_memory()
+    stats = torch.zeros(5, dtype=torch.int64, device=dev)
+    stream = torch.cuda.current_stream()
+
+    def ao_frame(with_stats=False):
+        mb.render_ao(pixels, (w, h), cam, builder.m_rootNode, builder.m_internals, d_tris, 1, wl["ns"], wl["radius"],
+                     12345, stats=stats if with_stats else None)
+
+    # counting pass: rays, node visits and triangle tests of one frame (the
+    # traversal is deterministic, so every timed frame does the same work)
+    builder.build(d_tris, n, 0, sorter)
+    builder.status()
+    ao_frame(with_stats=True)
+    torch.cuda.synchronize()
+    st = stats.cpu().numpy()
+    rays_per_frame, visits, tests, ao_visits, ao_tests = (int(x) for x in st[:5])
+    primaries = w * h
+    ao_rays = rays_per_frame - primaries
+
+    for _ in range(args.warmup):
+        builder.build(d_tris, n, 0, sorter)
+        ao_frame()
+    torch.cuda.synchronize()
+
+    sampler = ClockSampler(local)
+    with sampler:
+        # ---- AO frames over the resident BVH (inputs > L2: 419 MB working set for the soup)
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+        kev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+        flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev) if wl["scene"] != "soup" else None
+        barrier()
+        torch.cuda.synchronize()
+        for i in range(args.steps):
+            if flush is not None:
+                flush.zero_()  # evict the L2-resident scene between frames
+            ev[i][0].record(stream)
+            mb.profile_events(*kev[i])
+            ao_frame()
+            ev[i][1].record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        ao_ms = [a.elapsed_time(b) for a, b in ev]
+        kernel_ms = [a.elapsed_time(b) for a, b in kev]
+        ao_total_s = max_over_ranks(sum(ao_ms) / 1e3)
+
+        # ---- builds
+        bev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+        barrier()
+        torch.cuda.synchronize()
+        for i in range(args.steps):
+            if flush is not None:
+                flush.zero_()
+            bev[i][0].record(stream)
+            builder.build(d_tris, n, 0, sorter)
+            bev[i][1].record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        build_ms = [a.elapsed_time(b) for a, b in bev]
+        build_total_s = max_over_ranks(sum(build_ms) / 1e3)
+        builder.status()
+
+        # ---- end to end through the C ABI from host buffers
+        eev = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+        barrier()
+        torch.cuda.synchronize()
+        eev[0].record(stream)
+        for i in range(args.steps):
+            d_tris.copy_(host_tris, non_blocking=True)
+            builder.build(d_tris, n, 0, sorter)
+            ao_frame()
+            host_pixels.copy_(pixels, non_blocking=True)
+        eev[1].record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        e2e_s = max_over_ranks(eev[0].elapsed_time(eev[1]) / 1e3)
+    clocks = sampler.summary()
+
+    ms_per_step = ao_total_s * 1e3 / args.steps
+    value = rays_per_frame * args.steps * world / ao_total_s / 1e6
+    kernel_avg_s = float(np.mean(kernel_ms)) / 1e3
+    peak, peak_kind = peaks()
+    line = {
+        "metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scene, no dataset)",
+        "config": {"workload": args.workload, "triangles": n, "image": [w, h], "ao_samples": wl["ns"],
+                   "ao_radius": wl["radius"], "rays_per_frame": rays_per_frame, "primary_rays": primaries,
+                   "ao_rays": ao_rays, "parallelism": "replicas" if world > 1 else "single GPU",
+                   "l2": "inputs larger than L2 (nodes + triangles 419 MB)" if wl["scene"] == "soup"
+                   else "L2 flushed (256 MB write) between timed frames"},
+        "gpu_launches": args.steps * 3 + args.steps * 7 + args.steps * 10,
+        "clocks": clocks,
+    }
+    # roofline of the dominant kernel (k_ao_rays): algorithmic bytes of its rays
+    # (64 B per internal-node visit + 36 B per triangle test, counted by the
+    # deterministic counting pass) over its event-timed duration per launch
+    kernel_bytes = 64 * ao_visits + 36 * ao_tests
+    achieved = kernel_bytes / kernel_avg_s / 1e9
+    traffic = committed_traffic(args.workload)
+    line["roofline"] = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                        "traffic": traffic, "kernel": "k_ao_rays", "kernel_ms": kernel_avg_s * 1e3,
+                        "peak_source": f"{peak_kind} hbm_gbs",
+                        "bytes_model": "64 B per internal-node visit + 36 B per triangle test",
+                        "node_visits_per_ray": visits / rays_per_frame, "tri_tests_per_ray": tests / rays_per_frame, "kernel_bytes": kernel_bytes}
+    build_s = build_total_s / args.steps
+    line["build"] = {"ms": build_s * 1e3, "mtri_s": n * world / build_s / 1e6,
+                     "achieved_gbs": n * BUILD_BYTES_PER_TRI / build_s / 1e9,
+                     "frac": n * BUILD_BYTES_PER_TRI / build_s / 1e9 / peak, "bytes_per_tri": BUILD_BYTES_PER_TRI}
+    line["e2e"] = {"value": rays_per_frame * args.steps * world / e2e_s / 1e6, "unit": "Mrays/s",
+                   "h2d_bytes_per_step": int(host_tris.numel() * 4), "d2h_bytes_per_step": int(w * h * 4),
+                   "ms_per_step": e2e_s * 1e3 / args.steps}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        out = {"nodes": builder.m_internals.cpu().numpy().view(np.uint32)[: n - 1],
+               "root": int(builder.m_rootNode.cpu().numpy().view(np.uint32)[0])}
+        cam_arr = cam.as_array()
+        cb, _ = cpu_sample_ao(wl, tris, cam_arr, out, args.cpu_seconds)
+        cb["build"] = cpu_build_baseline(tris)
+        line["cpu_baseline"] = cb
+    if dist is not None:
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,186 @@
+/*
+ * mlbvh.h — the C-ABI boundary of minimumlbvh_b200, the B200 (sm_100a)
+ * implementation of MinimumLBVH's build and query path.
+ *
+ * Every entry point is `extern "C"`, takes plain pointers and sizes, and is
+ * stream-ordered: device buffers are owned by the caller, nothing is
+ * allocated, and nothing synchronises unless stated. `stream` is a
+ * cudaStream_t passed as void* (NULL = the legacy default stream). Device
+ * pointers must be 16-byte aligned (checked; MLBVH_ERR_INVALID_ARG).
+ *
+ * Data layouts are byte-identical to the reference's minimum_lbvh.h types so
+ * that buffers built here can be handed to code written against it:
+ *   mlbvh_triangle       = minimum_lbvh::Triangle      (minimum_lbvh.h:207-210) 36 B
+ *   mlbvh_aabb           = minimum_lbvh::AABB          (minimum_lbvh.h:217-252) 24 B
+ *   mlbvh_node_index     = minimum_lbvh::NodeIndex     (minimum_lbvh.h:254-265)  4 B
+ *                          bits 0-30 index, bit 31 leaf flag; 0x7FFFFFFF = invalid
+ *   mlbvh_internal_node  = minimum_lbvh::InternalNode  (minimum_lbvh.h:276-282) 64 B
+ *   mlbvh_hit            = minimum_lbvh::Hit           (minimum_lbvh.h:890-896) 32 B
+ *   mlbvh_ray_generator  = RayGenerator                (camera.h:3-32)          36 B
+ *   mlbvh_triangle_attrib= TriangleAttrib              (main_gpu.cu:10-15)      60 B
+ */
+#ifndef MLBVH_H
+#define MLBVH_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MLBVH_VERSION 1
+
+#if defined(__GNUC__)
+#define MLBVH_API __attribute__((visibility("default")))
+#else
+#define MLBVH_API
+#endif
+
+typedef enum mlbvh_status {
+    MLBVH_OK = 0,
+    MLBVH_ERR_INVALID_ARG = 1, /* null/misaligned pointer, bad size, scratch too small */
+    MLBVH_ERR_OOM = 2,         /* reserved for callers' allocation wrappers */
+    MLBVH_ERR_TIMEOUT = 3,     /* a bounded device-side wait gave up (see mlbvh_scratch_status) */
+    MLBVH_ERR_LAUNCH = 4,      /* a kernel launch failed */
+    MLBVH_ERR_CUDA = 5         /* another CUDA runtime error */
+} mlbvh_status;
+
+enum {
+    MLBVH_BUILD_OPTION_USE_NORMAL = 1,  /* BUILD_OPTION_USE_NORMAL, minimum_lbvh.h:44 */
+    MLBVH_BUILD_OPTION_CPU_PARALLEL = 2 /* accepted and ignored: the build always runs on the GPU */
+};
+enum { MLBVH_RAY_QUERY_CLOSEST = 0, MLBVH_RAY_QUERY_ANY = 1 }; /* RAY_QUERY, minimum_lbvh.h:975 */
+enum {
+    MLBVH_TRAVERSAL_STACKFREE = 0,   /* intersect_stackfree,   minimum_lbvh.h:981  */
+    MLBVH_TRAVERSAL_ESCAPE_LINK = 1, /* intersect_escape_link, minimum_lbvh.h:1063 */
+    MLBVH_TRAVERSAL_STACKFULL = 2    /* intersect_stackfull,   minimum_lbvh.h:912  */
+};
+
+typedef struct mlbvh_triangle { float vs[3][3]; } mlbvh_triangle;
+typedef struct mlbvh_aabb { float lower[3]; float upper[3]; } mlbvh_aabb;
+typedef uint32_t mlbvh_node_index;
+typedef struct mlbvh_internal_node {
+    mlbvh_node_index children[2];
+    mlbvh_aabb aabbs[2];
+    mlbvh_node_index parent;
+    uint32_t context; /* upper bound of the leaf range after the build (0xFFFFFFFF at the top) */
+} mlbvh_internal_node;
+typedef struct mlbvh_hit {
+    float t; /* FLT_MAX (3.402823466e+38f) when nothing was hit */
+    uint32_t _pad;
+    float uv[2];
+    float ng[3];
+    uint32_t triangleIndex; /* 0xFFFFFFFF when nothing was hit */
+} mlbvh_hit;
+/* A query ray. The reference's intersect_* take (ro, rd) with the initial
+ * hit.t as the far limit and 0 as the near one; tmin = 0 gives exactly that. */
+typedef struct mlbvh_ray { float ro[3]; float tmin; float rd[3]; float tmax; } mlbvh_ray;
+typedef struct mlbvh_ray_generator { float origin[3]; float right[3]; float up[3]; } mlbvh_ray_generator;
+typedef struct mlbvh_triangle_attrib {
+    float shadingNormals[3][3];
+    float reflectance[3];
+    float emissive[3];
+} mlbvh_triangle_attrib;
+
+/* Library version (MLBVH_VERSION) and the message of the last error raised on
+ * the calling host thread ("" if none). */
+MLBVH_API int mlbvh_version(void);
+MLBVH_API const char* mlbvh_last_error_string(void);
+
+/* ---------------------------------------------------------------- build ---
+ * Replaces BVHGPUBuilder::build (minimum_lbvh.h:783-871) and the
+ * OnesweepSort it drives (tinyhiponesweep.h:592-668). Scene AABB, Morton keys
+ * (minimum_lbvh.cu:38-92), a stable LSD radix sort of (key, triangle index),
+ * deltas (minimum_lbvh.cu:94-102) and the agglomerative build
+ * (minimum_lbvh.h:284-361) run as a chain of kernels on `stream`.
+ *
+ * dInternals receives nTriangles-1 nodes, *dRootNode the root (a leaf when
+ * nTriangles == 1). dSceneAABB may be NULL. dScratch must hold
+ * mlbvh_build_scratch_bytes(nTriangles) bytes; its contents need no
+ * initialisation and must not be shared by builds in flight at the same time.
+ * 1 <= nTriangles < 2^30. */
+MLBVH_API size_t mlbvh_build_scratch_bytes(uint32_t nTriangles);
+MLBVH_API mlbvh_status mlbvh_build(const mlbvh_triangle* dTriangles, uint32_t nTriangles, uint32_t buildOption,
+                         mlbvh_internal_node* dInternals, mlbvh_node_index* dRootNode,
+                         mlbvh_aabb* dSceneAABB, void* dScratch, size_t scratchBytes, void* stream);
+
+/* mlbvh_build plus the intermediate arrays the reference keeps or prints:
+ * the sorted Morton keys and triangle indices (IndexedMorton after
+ * OnesweepSort, minimum_lbvh.h:833) and the split deltas (BVHCPUBuilder::
+ * m_deltas, minimum_lbvh.h:668). Each of the three may be NULL. */
+MLBVH_API mlbvh_status mlbvh_build_ex(const mlbvh_triangle* dTriangles, uint32_t nTriangles, uint32_t buildOption,
+                            mlbvh_internal_node* dInternals, mlbvh_node_index* dRootNode,
+                            mlbvh_aabb* dSceneAABB, uint32_t* dSortedKeys, uint32_t* dSortedIndices,
+                            uint8_t* dDeltas, void* dScratch, size_t scratchBytes, void* stream);
+
+/* Synchronises `stream`, then reports MLBVH_ERR_TIMEOUT if a bounded wait of
+ * the last build that used dScratch gave up (its output is then unusable),
+ * else MLBVH_OK. */
+MLBVH_API mlbvh_status mlbvh_scratch_status(const void* dScratch, void* stream);
+
+/* ---------------------------------------------------------------- query ---
+ * Replaces the per-ray calls of intersect_stackfree / intersect_escape_link /
+ * intersect_stackfull (minimum_lbvh.h:981, 1063, 912) with one launch over
+ * nRays rays. hits[i] follows minimum_lbvh::Hit; for RAY_QUERY_ANY the first
+ * hit found stops the ray. The stackful traversal has no any-hit mode in the
+ * reference and answers closest hits. */
+MLBVH_API mlbvh_status mlbvh_trace(const mlbvh_internal_node* dInternals, const mlbvh_node_index* dRootNode,
+                         const mlbvh_triangle* dTriangles, const mlbvh_ray* dRays, mlbvh_hit* dHits,
+                         uint32_t nRays, int rayQuery, int traversal, void* stream);
+
+/* --------------------------------------------------------------- shading ---
+ * The reference's shading kernels (main_gpu.cu), one launch chain each.
+ * `camera` is a HOST pointer (passed by value to the kernels, as the
+ * reference passes RayGenerator). Pixels are packed RGBA8 as packRGBA writes
+ * them (main_gpu.cu:17-22). */
+
+/* normal (main_gpu.cu:84-109) */
+MLBVH_API mlbvh_status mlbvh_render_normal(uint32_t* dPixels, int width, int height, const mlbvh_ray_generator* camera,
+                                 const mlbvh_node_index* dRootNode, const mlbvh_internal_node* dInternals,
+                                 const mlbvh_triangle* dTriangles, void* stream);
+
+/* ao (main_gpu.cu:111-177) with the sample count, AO ray length and the Sobol
+ * scramble seed as parameters (the reference fixes 16, 1.0f and 12345).
+ * dOccluded (may be NULL) receives per pixel the number of AO rays that hit
+ * something, or 0xFFFFFFFF where the primary ray missed; linear AO is
+ * dOccluded / nSamples. The sample directions use this library's FP32 sincos
+ * instead of CUDA's cosf/sinf, so that the host oracle can reproduce them bit
+ * for bit. dScratch holds mlbvh_render_scratch_bytes(width, height) bytes.
+ * dStats (may be NULL; 5 device uint64) receives {rays traced (primary + AO),
+ * internal-node visits, triangle tests, the AO rays' share of those visits,
+ * the AO rays' share of those tests}; counting runs a slower kernel variant,
+ * so leave it NULL when timing. */
+MLBVH_API size_t mlbvh_render_scratch_bytes(int width, int height);
+MLBVH_API mlbvh_status mlbvh_render_ao(uint32_t* dPixels, uint32_t* dOccluded, int width, int height,
+                             const mlbvh_ray_generator* camera, const mlbvh_node_index* dRootNode,
+                             const mlbvh_internal_node* dInternals, const mlbvh_triangle* dTriangles,
+                             int useSobol, int nSamples, float radius, uint32_t sobolSeed,
+                             unsigned long long* dStats, void* dScratch, size_t scratchBytes, void* stream);
+
+/* One progressive path-tracing pass (pt, main_gpu.cu:179-272): reads and
+ * updates dAccumulators (float4 per pixel, w = samples so far). maxDepth is
+ * the bounce limit (the reference uses 1024). */
+MLBVH_API mlbvh_status mlbvh_render_pt(float* dAccumulators, int width, int height, const mlbvh_ray_generator* camera,
+                             const mlbvh_node_index* dRootNode, const mlbvh_internal_node* dInternals,
+                             const mlbvh_triangle* dTriangles, const mlbvh_triangle_attrib* dAttribs,
+                             int useSobol, int maxSPP, int maxDepth, void* stream);
+
+/* pack (main_gpu.cu:273-286): accumulator / spp, gamma 1/2.2, RGBA8. */
+MLBVH_API mlbvh_status mlbvh_pack(uint32_t* dPixels, const float* dAccumulators, int n, void* stream);
+
+/* Profiling hook (no reference counterpart; the reference times whole calls
+ * with its DeviceStopwatch, minimum_lbvh.h:693-724): the next mlbvh_render_ao
+ * or mlbvh_build on this host thread records the two cudaEvent_t handles
+ * around its dominant kernel (the AO-ray kernel, resp. the agglomerative
+ * build kernel). NULL, NULL cancels. */
+MLBVH_API void mlbvh_profile_events(void* startEvent, void* stopEvent);
+
+/* RayGenerator::lookat (camera.h:10-22), on the host. */
+MLBVH_API mlbvh_status mlbvh_camera_lookat(mlbvh_ray_generator* out, const float eye[3], const float center[3],
+                                 const float up[3], float fovy, int width, int height);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MLBVH_H */

@@ -1,0 +1,309 @@
+"""minimumlbvh_b200 — MinimumLBVH's build, query and shading path on B200.
+
+The work is done by libmlbvh_b200.so (hand-written sm_100a kernels behind the
+C ABI of include/mlbvh.h). This module is the Python host side: it loads that
+library with ctypes and mirrors the reference's host interface
+(minimum_lbvh.h, tinyhiponesweep.h, camera.h, main_gpu.cu launches) over
+torch CUDA tensors, which serve only as device memory and streams.
+
+There is no CPU fallback: every compute call goes to the GPU library, and
+``lib()`` raises if the library is missing.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+__all__ = [
+    "lib", "library_path", "MlbvhError", "BUILD_OPTION_USE_NORMAL", "BUILD_OPTION_CPU_PARALLEL",
+    "RAY_QUERY_CLOSEST", "RAY_QUERY_ANY", "TRAVERSAL_STACKFREE", "TRAVERSAL_ESCAPE_LINK",
+    "TRAVERSAL_STACKFULL", "OnesweepSort", "BVHGPUBuilder", "RayGenerator", "intersect",
+    "render_normal", "render_ao", "render_pt", "pack", "profile_events", "FLT_MAX", "INVALID_NODE",
+]
+
+BUILD_OPTION_USE_NORMAL = 1   # minimum_lbvh.h:44
+BUILD_OPTION_CPU_PARALLEL = 2  # minimum_lbvh.h:45 (accepted, ignored: the build runs on the GPU)
+RAY_QUERY_CLOSEST = 0          # minimum_lbvh.h:977
+RAY_QUERY_ANY = 1              # minimum_lbvh.h:978
+TRAVERSAL_STACKFREE = 0
+TRAVERSAL_ESCAPE_LINK = 1
+TRAVERSAL_STACKFULL = 2
+FLT_MAX = float(np.float32(3.402823466e38))
+INVALID_NODE = 0x7FFFFFFF
+
+_STATUS = {0: "MLBVH_OK", 1: "MLBVH_ERR_INVALID_ARG", 2: "MLBVH_ERR_OOM", 3: "MLBVH_ERR_TIMEOUT",
+           4: "MLBVH_ERR_LAUNCH", 5: "MLBVH_ERR_CUDA"}
+
+library_path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libmlbvh_b200.so")
+
+
+class MlbvhError(RuntimeError):
+    """A non-OK mlbvh_status; ``status`` holds the code."""
+
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{_STATUS.get(status, status)}: {message}")
+        self.status = status
+
+
+_lib = None
+_vp = ctypes.c_void_p
+
+
+def lib() -> ctypes.CDLL:
+    """The loaded libmlbvh_b200.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(library_path):
+            raise ImportError(f"{library_path} is missing: build it with `make -C minimumlbvh_b200` "
+                              "(or __graft_entry__.build()); there is no CPU fallback")
+        L = ctypes.CDLL(library_path)
+        u32, i32, f32, sz = ctypes.c_uint32, ctypes.c_int, ctypes.c_float, ctypes.c_size_t
+        sig = {
+            "mlbvh_version": (i32, []),
+            "mlbvh_last_error_string": (ctypes.c_char_p, []),
+            "mlbvh_build_scratch_bytes": (sz, [u32]),
+            "mlbvh_build": (i32, [_vp, u32, u32, _vp, _vp, _vp, _vp, sz, _vp]),
+            "mlbvh_build_ex": (i32, [_vp, u32, u32, _vp, _vp, _vp, _vp, _vp, _vp, _vp, sz, _vp]),
+            "mlbvh_scratch_status": (i32, [_vp, _vp]),
+            "mlbvh_trace": (i32, [_vp, _vp, _vp, _vp, _vp, u32, i32, i32, _vp]),
+            "mlbvh_render_scratch_bytes": (sz, [i32, i32]),
+            "mlbvh_render_normal": (i32, [_vp, i32, i32, _vp, _vp, _vp, _vp, _vp]),
+            "mlbvh_render_ao": (i32, [_vp, _vp, i32, i32, _vp, _vp, _vp, _vp, i32, i32, f32, u32, _vp, _vp, sz,
+                                      _vp]),
+            "mlbvh_render_pt": (i32, [_vp, i32, i32, _vp, _vp, _vp, _vp, _vp, i32, i32, i32, _vp]),
+            "mlbvh_pack": (i32, [_vp, _vp, i32, _vp]),
+            "mlbvh_profile_events": (None, [_vp, _vp]),
+            "mlbvh_camera_lookat": (i32, [_vp, _vp, _vp, _vp, f32, i32, i32]),
+        }
+        for name, (res, args) in sig.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _check(status: int) -> None:
+    if status != 0:
+        raise MlbvhError(status, lib().mlbvh_last_error_string().decode())
+
+
+def _ptr(t) -> int | None:
+    if t is None:
+        return None
+    return t.data_ptr()
+
+
+def _stream(stream) -> int | None:
+    import torch
+    if stream is None:
+        return torch.cuda.current_stream().cuda_stream
+    if isinstance(stream, int):
+        return stream
+    return stream.cuda_stream
+
+
+def _require_cuda(t, name: str):
+    import torch
+    if not isinstance(t, torch.Tensor) or not t.is_cuda:
+        raise TypeError(f"{name} must be a CUDA tensor")
+    if not t.is_contiguous():
+        raise ValueError(f"{name} must be contiguous")
+
+
+class RayGenerator:
+    """camera.h:3-32. ``lookat`` is computed by the C ABI on the host;
+    ``as_bytes`` is the 36-byte struct the kernels take by value."""
+
+    def __init__(self):
+        self.m_origin = np.zeros(3, np.float32)
+        self.m_right = np.array([1, 0, 0], np.float32)
+        self.m_up = np.array([0, 1, 0], np.float32)
+
+    def lookat(self, eye, center, up, fovy, imageWidth, imageHeight):
+        out = (ctypes.c_float * 9)()
+        e = (ctypes.c_float * 3)(*eye)
+        c = (ctypes.c_float * 3)(*center)
+        u = (ctypes.c_float * 3)(*up)
+        _check(lib().mlbvh_camera_lookat(ctypes.addressof(out), ctypes.addressof(e), ctypes.addressof(c),
+                                         ctypes.addressof(u), float(fovy), int(imageWidth), int(imageHeight)))
+        a = np.frombuffer(bytes(out), dtype=np.float32)
+        self.m_origin, self.m_right, self.m_up = a[0:3].copy(), a[3:6].copy(), a[6:9].copy()
+        return self
+
+    def as_array(self) -> np.ndarray:
+        return np.concatenate([self.m_origin, self.m_right, self.m_up]).astype(np.float32)
+
+    @classmethod
+    def from_array(cls, a) -> "RayGenerator":
+        g = cls()
+        a = np.asarray(a, np.float32)
+        g.m_origin, g.m_right, g.m_up = a[0:3].copy(), a[3:6].copy(), a[6:9].copy()
+        return g
+
+    def _cstruct(self):
+        return (ctypes.c_float * 9)(*self.as_array().tolist())
+
+
+class OnesweepSort:
+    """tinyhiponesweep::OnesweepSort (tinyhiponesweep.h:572-748): owns the
+    persistent scratch of the build (histograms, look-back words, key/value
+    ping-pong buffers), grown on demand."""
+
+    def __init__(self, device=None):
+        import torch
+        self.device = torch.device("cuda", torch.cuda.current_device() if device is None else device)
+        self.scratch = None
+
+    def reserve(self, nbytes: int):
+        import torch
+        if self.scratch is None or self.scratch.numel() < nbytes:
+            self.scratch = torch.empty(max(nbytes, 256), dtype=torch.uint8, device=self.device)
+        return self.scratch
+
+
+class BVHGPUBuilder:
+    """BVHGPUBuilder (minimum_lbvh.h:726-885) over libmlbvh_b200.so.
+
+    ``build`` leaves ``m_internals`` (int32 tensor, nTriangles-1 rows of the
+    16-word InternalNode), ``m_rootNode`` (device int32 tensor of one
+    NodeIndex; kernels dereference it, as in the reference) and
+    ``m_sceneAABB`` (6 floats). Unlike the reference it neither allocates per
+    call nor synchronises nor prints: the build is stream-ordered."""
+
+    def __init__(self, kernelPath=None, includeDir=None):
+        # The reference compiles minimum_lbvh.cu at run time from these paths;
+        # here the kernels are compiled ahead of time, so they are ignored.
+        self.m_internals = None
+        self.m_rootNode = None
+        self.m_sceneAABB = None
+        self.m_nTriangles = 0
+        self.m_sortedKeys = None
+        self.m_sortedIndices = None
+        self.m_deltas = None
+
+    def build(self, triangles, nTriangles: int | None = None, buildOption: int = 0, sorter: OnesweepSort | None = None,
+              stream=None, keep_keys: bool = False):
+        import torch
+        _require_cuda(triangles, "triangles")
+        n = int(nTriangles if nTriangles is not None else triangles.numel() // 9)
+        if n <= 0 or triangles.numel() < 9 * n:
+            raise MlbvhError(1, "nTriangles must be positive and fit the triangle tensor")
+        dev = triangles.device
+        if sorter is None:
+            sorter = OnesweepSort(dev.index)
+        scratch = sorter.reserve(lib().mlbvh_build_scratch_bytes(n))
+        if self.m_internals is None or self.m_internals.shape[0] != max(n - 1, 1) or self.m_internals.device != dev:
+            self.m_internals = torch.empty((max(n - 1, 1), 16), dtype=torch.int32, device=dev)
+        if self.m_rootNode is None or self.m_rootNode.device != dev:
+            self.m_rootNode = torch.empty(4, dtype=torch.int32, device=dev)
+            self.m_sceneAABB = torch.empty(8, dtype=torch.float32, device=dev)
+        if keep_keys:
+            self.m_sortedKeys = torch.empty(n, dtype=torch.int32, device=dev)
+            self.m_sortedIndices = torch.empty(n, dtype=torch.int32, device=dev)
+            self.m_deltas = torch.empty(max(n, 16), dtype=torch.uint8, device=dev)
+            _check(lib().mlbvh_build_ex(_ptr(triangles), n, int(buildOption), _ptr(self.m_internals),
+                                        _ptr(self.m_rootNode), _ptr(self.m_sceneAABB), _ptr(self.m_sortedKeys),
+                                        _ptr(self.m_sortedIndices), _ptr(self.m_deltas), _ptr(scratch),
+                                        scratch.numel(), _stream(stream)))
+        else:
+            _check(lib().mlbvh_build(_ptr(triangles), n, int(buildOption), _ptr(self.m_internals),
+                                     _ptr(self.m_rootNode), _ptr(self.m_sceneAABB), _ptr(scratch), scratch.numel(),
+                                     _stream(stream)))
+        self.m_nTriangles = n
+        self._sorter = sorter
+        return self
+
+    def status(self, stream=None) -> None:
+        """Synchronise and raise MlbvhError(MLBVH_ERR_TIMEOUT) if a bounded wait
+        of the last build gave up."""
+        _check(lib().mlbvh_scratch_status(_ptr(self._sorter.scratch), _stream(stream)))
+
+    def empty(self) -> bool:
+        return self.m_nTriangles == 0
+
+    @property
+    def nodes(self):
+        return self.m_internals[: max(self.m_nTriangles - 1, 0)]
+
+
+def intersect(builder_or_nodes, triangles, rays, rayQuery: int = RAY_QUERY_CLOSEST,
+              traversal: int = TRAVERSAL_STACKFREE, hits=None, root=None, stream=None):
+    """One launch of intersect_stackfree / _escape_link / _stackfull
+    (minimum_lbvh.h:981, 1063, 912) over ``rays`` (float32 (n, 8):
+    ro.xyz, tmin, rd.xyz, tmax). Returns ``hits`` (int32 (n, 8) holding the
+    32-byte Hit records)."""
+    import torch
+    if isinstance(builder_or_nodes, BVHGPUBuilder):
+        nodes, root = builder_or_nodes.m_internals, builder_or_nodes.m_rootNode
+    else:
+        nodes = builder_or_nodes
+    _require_cuda(rays, "rays")
+    n = rays.numel() // 8
+    if hits is None:
+        hits = torch.empty((n, 8), dtype=torch.int32, device=rays.device)
+    _check(lib().mlbvh_trace(_ptr(nodes), _ptr(root), _ptr(triangles), _ptr(rays), _ptr(hits), n, int(rayQuery),
+                             int(traversal), _stream(stream)))
+    return hits
+
+
+def render_normal(pixels, imageSize, rayGenerator: RayGenerator, rootNode, internals, triangles, stream=None):
+    """normal (main_gpu.cu:84-109)."""
+    w, h = imageSize
+    cam = rayGenerator._cstruct()
+    _check(lib().mlbvh_render_normal(_ptr(pixels), int(w), int(h), ctypes.addressof(cam), _ptr(rootNode),
+                                     _ptr(internals), _ptr(triangles), _stream(stream)))
+    return pixels
+
+
+_render_scratch = {}
+
+
+def profile_events(start=None, stop=None):
+    """Make the next render_ao / BVHGPUBuilder.build on this thread record
+    the torch.cuda.Event pair around its dominant kernel."""
+    lib().mlbvh_profile_events(None if start is None else start.cuda_event,
+                               None if stop is None else stop.cuda_event)
+
+
+def render_ao(pixels, imageSize, rayGenerator: RayGenerator, rootNode, internals, triangles, useSobol: int = 1,
+              nSamples: int = 16, radius: float = 1.0, seed: int = 12345, occluded=None, stats=None,
+              scratch=None, stream=None):
+    """ao (main_gpu.cu:111-177) with sample count, radius and Sobol seed as
+    parameters (the reference fixes 16, 1.0, 12345). ``stats`` (int64 CUDA
+    tensor of 3) receives rays traced, node visits and triangle tests."""
+    import torch
+    w, h = imageSize
+    need = lib().mlbvh_render_scratch_bytes(int(w), int(h))
+    if scratch is None:
+        key = (pixels.device.index, need)
+        scratch = _render_scratch.get(key)
+        if scratch is None:
+            scratch = torch.empty(need, dtype=torch.uint8, device=pixels.device)
+            _render_scratch.clear()
+            _render_scratch[key] = scratch
+    cam = rayGenerator._cstruct()
+    _check(lib().mlbvh_render_ao(_ptr(pixels), _ptr(occluded), int(w), int(h), ctypes.addressof(cam),
+                                 _ptr(rootNode), _ptr(internals), _ptr(triangles), int(useSobol), int(nSamples),
+                                 float(radius), int(seed), _ptr(stats), _ptr(scratch), scratch.numel(),
+                                 _stream(stream)))
+    return pixels
+
+
+def render_pt(accumulators, imageSize, rayGenerator: RayGenerator, rootNode, internals, triangles,
+              triangleAttribs, useSobol: int = 1, maxSPP: int = 1 << 30, maxDepth: int = 1024, stream=None):
+    """One progressive pass of pt (main_gpu.cu:179-272)."""
+    w, h = imageSize
+    cam = rayGenerator._cstruct()
+    _check(lib().mlbvh_render_pt(_ptr(accumulators), int(w), int(h), ctypes.addressof(cam), _ptr(rootNode),
+                                 _ptr(internals), _ptr(triangles), _ptr(triangleAttribs), int(useSobol), int(maxSPP),
+                                 int(maxDepth), _stream(stream)))
+    return accumulators
+
+
+def pack(pixels, accumulators, n: int, stream=None):
+    """pack (main_gpu.cu:273-286)."""
+    _check(lib().mlbvh_pack(_ptr(pixels), _ptr(accumulators), int(n), _stream(stream)))
+    return pixels

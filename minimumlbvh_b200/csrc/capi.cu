@@ -1,0 +1,180 @@
+// The extern "C" entry points declared in include/mlbvh.h: argument
+// checks, error strings, and dispatch to the kernels of build.cu, trace.cu
+// and shade.cu. No entry point allocates device memory or synchronises,
+// except mlbvh_scratch_status, which synchronises by design.
+#include <cmath>
+#include <cstring>
+#include <string>
+
+#include "capi_internal.h"
+
+namespace mlbvh {
+
+namespace {
+thread_local std::string g_lastError;
+}
+
+mlbvh_status fail(mlbvh_status status, const char* message)
+{
+    g_lastError = message ? message : "";
+    return status;
+}
+void clear_error() { g_lastError.clear(); }
+
+namespace {
+thread_local ProfileEvents g_profile;
+}
+void set_profile_events(cudaEvent_t start, cudaEvent_t stop)
+{
+    g_profile.start = start;
+    g_profile.stop = stop;
+}
+ProfileEvents take_profile_events()
+{
+    ProfileEvents e = g_profile;
+    g_profile = ProfileEvents{};
+    return e;
+}
+
+int device_sm_count()
+{
+    int dev = 0, sms = 148;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    return sms > 0 ? sms : 148;
+}
+
+}  // namespace mlbvh
+
+using namespace mlbvh;
+
+static inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+
+extern "C" {
+
+int mlbvh_version(void) { return MLBVH_VERSION; }
+
+const char* mlbvh_last_error_string(void) { return g_lastError.c_str(); }
+
+size_t mlbvh_build_scratch_bytes(uint32_t nTriangles) { return build_scratch_bytes(nTriangles); }
+
+mlbvh_status mlbvh_build(const mlbvh_triangle* dTriangles, uint32_t nTriangles, uint32_t buildOption,
+                         mlbvh_internal_node* dInternals, mlbvh_node_index* dRootNode, mlbvh_aabb* dSceneAABB,
+                         void* dScratch, size_t scratchBytes, void* stream)
+{
+    clear_error();
+    return build(dTriangles, nTriangles, buildOption, dInternals, dRootNode, dSceneAABB, nullptr, nullptr, nullptr,
+                 dScratch, scratchBytes, as_stream(stream), 0);
+}
+
+mlbvh_status mlbvh_build_ex(const mlbvh_triangle* dTriangles, uint32_t nTriangles, uint32_t buildOption,
+                            mlbvh_internal_node* dInternals, mlbvh_node_index* dRootNode, mlbvh_aabb* dSceneAABB,
+                            uint32_t* dSortedKeys, uint32_t* dSortedIndices, uint8_t* dDeltas, void* dScratch,
+                            size_t scratchBytes, void* stream)
+{
+    clear_error();
+    return build(dTriangles, nTriangles, buildOption, dInternals, dRootNode, dSceneAABB, dSortedKeys, dSortedIndices,
+                 dDeltas, dScratch, scratchBytes, as_stream(stream), 0);
+}
+
+mlbvh_status mlbvh_scratch_status(const void* dScratch, void* stream)
+{
+    clear_error();
+    return scratch_status(dScratch, as_stream(stream));
+}
+
+mlbvh_status mlbvh_trace(const mlbvh_internal_node* dInternals, const mlbvh_node_index* dRootNode,
+                         const mlbvh_triangle* dTriangles, const mlbvh_ray* dRays, mlbvh_hit* dHits, uint32_t nRays,
+                         int rayQuery, int traversal, void* stream)
+{
+    clear_error();
+    return trace(dInternals, dRootNode, dTriangles, dRays, dHits, nRays, rayQuery, traversal, as_stream(stream));
+}
+
+size_t mlbvh_render_scratch_bytes(int width, int height) { return render_scratch_bytes(width, height); }
+
+mlbvh_status mlbvh_render_normal(uint32_t* dPixels, int width, int height, const mlbvh_ray_generator* camera,
+                                 const mlbvh_node_index* dRootNode, const mlbvh_internal_node* dInternals,
+                                 const mlbvh_triangle* dTriangles, void* stream)
+{
+    clear_error();
+    if (!camera) return fail(MLBVH_ERR_INVALID_ARG, "null camera");
+    return render_normal(dPixels, width, height, *camera, dRootNode, dInternals, dTriangles, as_stream(stream));
+}
+
+mlbvh_status mlbvh_render_ao(uint32_t* dPixels, uint32_t* dOccluded, int width, int height,
+                             const mlbvh_ray_generator* camera, const mlbvh_node_index* dRootNode,
+                             const mlbvh_internal_node* dInternals, const mlbvh_triangle* dTriangles, int useSobol,
+                             int nSamples, float radius, uint32_t sobolSeed, unsigned long long* dStats,
+                             void* dScratch, size_t scratchBytes, void* stream)
+{
+    clear_error();
+    if (!camera) return fail(MLBVH_ERR_INVALID_ARG, "null camera");
+    return render_ao(dPixels, dOccluded, width, height, *camera, dRootNode, dInternals, dTriangles, useSobol, nSamples,
+                     radius, sobolSeed, dStats, dScratch, scratchBytes, as_stream(stream));
+}
+
+mlbvh_status mlbvh_render_pt(float* dAccumulators, int width, int height, const mlbvh_ray_generator* camera,
+                             const mlbvh_node_index* dRootNode, const mlbvh_internal_node* dInternals,
+                             const mlbvh_triangle* dTriangles, const mlbvh_triangle_attrib* dAttribs, int useSobol,
+                             int maxSPP, int maxDepth, void* stream)
+{
+    clear_error();
+    if (!camera) return fail(MLBVH_ERR_INVALID_ARG, "null camera");
+    return render_pt(dAccumulators, width, height, *camera, dRootNode, dInternals, dTriangles, dAttribs, useSobol,
+                     maxSPP, maxDepth, as_stream(stream));
+}
+
+void mlbvh_profile_events(void* startEvent, void* stopEvent)
+{
+    set_profile_events(reinterpret_cast<cudaEvent_t>(startEvent), reinterpret_cast<cudaEvent_t>(stopEvent));
+}
+
+mlbvh_status mlbvh_pack(uint32_t* dPixels, const float* dAccumulators, int n, void* stream)
+{
+    clear_error();
+    return pack(dPixels, dAccumulators, n, as_stream(stream));
+}
+
+// RayGenerator::lookat (camera.h:10-22) on the host; the host compiler runs
+// with -ffp-contract=off, so this rounds as the reference's host build does.
+mlbvh_status mlbvh_camera_lookat(mlbvh_ray_generator* out, const float eye[3], const float center[3],
+                                 const float up[3], float fovy, int width, int height)
+{
+    clear_error();
+    if (!out || !eye || !center || !up || width <= 0 || height <= 0)
+        return fail(MLBVH_ERR_INVALID_ARG, "null pointer or non-positive image size");
+    auto sub = [](const float* a, const float* b, float* r) {
+        r[0] = a[0] - b[0];
+        r[1] = a[1] - b[1];
+        r[2] = a[2] - b[2];
+    };
+    auto cross = [](const float* a, const float* b, float* r) {
+        float x = a[1] * b[2] - a[2] * b[1], y = a[2] * b[0] - a[0] * b[2], z = a[0] * b[1] - a[1] * b[0];
+        r[0] = x;
+        r[1] = y;
+        r[2] = z;
+    };
+    auto normalize = [](float* v) {
+        float d = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
+        float inv = 1.0f / std::sqrt(d);
+        v[0] = v[0] * inv;
+        v[1] = v[1] * inv;
+        v[2] = v[2] * inv;
+    };
+    float f[3], s[3], u[3];
+    sub(center, eye, f);
+    normalize(f);
+    cross(f, up, s);
+    normalize(s);
+    cross(s, f, u);
+    float tanThetaY = std::tan(fovy * 0.5f);
+    float tanThetaX = tanThetaY / (float)height * (float)width;
+    for (int i = 0; i < 3; ++i) {
+        out->origin[i] = eye[i];
+        out->right[i] = s[i] * tanThetaX;
+        out->up[i] = u[i] * tanThetaY;
+    }
+    return MLBVH_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,57 @@
+// Internal declarations shared by the translation units of libmlbvh_b200.so.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "../../include/mlbvh.h"
+
+namespace mlbvh {
+
+// Records the message for mlbvh_last_error_string() on this host thread and
+// returns the status.
+mlbvh_status fail(mlbvh_status status, const char* message);
+void clear_error();
+inline bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
+int device_sm_count();
+
+// CUDA events (cudaEvent_t) that the next render_ao / build call on this host
+// thread records around its dominant kernel; taking them clears them.
+struct ProfileEvents {
+    cudaEvent_t start = nullptr, stop = nullptr;
+};
+void set_profile_events(cudaEvent_t start, cudaEvent_t stop);
+ProfileEvents take_profile_events();
+
+#define MLBVH_CHECK_LAUNCH(name)                                                              \
+    do {                                                                                      \
+        cudaError_t e_ = cudaGetLastError();                                                  \
+        if (e_ != cudaSuccess) return ::mlbvh::fail(MLBVH_ERR_LAUNCH, cudaGetErrorString(e_)); \
+    } while (0)
+
+size_t build_scratch_bytes(uint32_t n);
+mlbvh_status build(const mlbvh_triangle* dTris, uint32_t n, uint32_t option, mlbvh_internal_node* dNodes,
+                   mlbvh_node_index* dRoot, mlbvh_aabb* dScene, uint32_t* dKeysOut, uint32_t* dIdxOut,
+                   uint8_t* dDeltasOut, void* dScratch, size_t scratchBytes, cudaStream_t stream, uint32_t spinLimit);
+mlbvh_status scratch_status(const void* dScratch, cudaStream_t stream);
+
+mlbvh_status trace(const mlbvh_internal_node* dNodes, const mlbvh_node_index* dRoot, const mlbvh_triangle* dTris,
+                   const mlbvh_ray* dRays, mlbvh_hit* dHits, uint32_t nRays, int rayQuery, int traversal,
+                   cudaStream_t stream);
+
+size_t render_scratch_bytes(int w, int h);
+mlbvh_status render_normal(uint32_t* dPixels, int w, int h, const mlbvh_ray_generator& cam,
+                           const mlbvh_node_index* dRoot, const mlbvh_internal_node* dNodes,
+                           const mlbvh_triangle* dTris, cudaStream_t stream);
+mlbvh_status render_ao(uint32_t* dPixels, uint32_t* dOccluded, int w, int h, const mlbvh_ray_generator& cam,
+                       const mlbvh_node_index* dRoot, const mlbvh_internal_node* dNodes, const mlbvh_triangle* dTris,
+                       int useSobol, int nSamples, float radius, uint32_t seed, unsigned long long* dStats,
+                       void* dScratch, size_t scratchBytes, cudaStream_t stream);
+mlbvh_status render_pt(float* dAccum, int w, int h, const mlbvh_ray_generator& cam, const mlbvh_node_index* dRoot,
+                       const mlbvh_internal_node* dNodes, const mlbvh_triangle* dTris,
+                       const mlbvh_triangle_attrib* dAttribs, int useSobol, int maxSPP, int maxDepth,
+                       cudaStream_t stream);
+mlbvh_status pack(uint32_t* dPixels, const float* dAccum, int n, cudaStream_t stream);
+
+}  // namespace mlbvh

@@ -1,0 +1,437 @@
+// Shared device code of minimumlbvh_b200: vector arithmetic with the exact
+// rounding of the reference's host build, Morton coding, the stack-free
+// traversal and the sample streams.
+//
+// Bit-exactness with the reference's CPU path (minimum_lbvh.h compiled for
+// the host) rests on three rules, applied to every kernel in this library:
+//   * the library is compiled with -fmad=false, so each written * and + rounds
+//     on its own, in source order, as the host does under -ffp-contract=off;
+//   * division and sqrtf are IEEE round-to-nearest (no fast-math), and
+//     normalize is v * (1 / sqrtf(dot(v, v))), the host rsqrtf
+//     (helper_math.h:154-157);
+//   * fminf/fmaxf on the host are selects, `a < b ? a : b` (helper_math.h:
+//     134-142); where the operand order can show (AABB merges that may see
+//     +0 and -0) the same selects are used here.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "../../include/mlbvh.h"
+
+namespace mlbvh {
+
+constexpr float kFltMax = 3.402823466e+38F;  // minimum_lbvh.h:37
+constexpr uint32_t kMortonMax = 0x1FFFFF;   // minimum_lbvh.h:38
+constexpr uint32_t kInvalid = 0x7FFFFFFFu;  // NodeIndex::invalid()
+constexpr uint32_t kLeafBit = 0x80000000u;
+// Upper bound on traversal steps per ray. A valid tree of n leaves needs at
+// most 4n steps (each internal node entered from above and from both
+// children, each leaf once); the bound only matters for a corrupt tree, where
+// it turns an endless walk into a wrong answer.
+constexpr uint32_t kMaxTraversalSteps = 1u << 26;
+
+struct f3 {
+    float x, y, z;
+};
+
+__device__ __forceinline__ f3 mk(float x, float y, float z) { return f3{x, y, z}; }
+__device__ __forceinline__ f3 operator+(f3 a, f3 b) { return mk(a.x + b.x, a.y + b.y, a.z + b.z); }
+__device__ __forceinline__ f3 operator-(f3 a, f3 b) { return mk(a.x - b.x, a.y - b.y, a.z - b.z); }
+__device__ __forceinline__ f3 operator*(f3 a, f3 b) { return mk(a.x * b.x, a.y * b.y, a.z * b.z); }
+__device__ __forceinline__ f3 operator*(f3 a, float s) { return mk(a.x * s, a.y * s, a.z * s); }
+__device__ __forceinline__ f3 operator*(float s, f3 a) { return mk(s * a.x, s * a.y, s * a.z); }
+__device__ __forceinline__ f3 operator/(f3 a, float s) { return mk(a.x / s, a.y / s, a.z / s); }
+__device__ __forceinline__ f3 operator/(f3 a, f3 b) { return mk(a.x / b.x, a.y / b.y, a.z / b.z); }
+__device__ __forceinline__ f3 operator-(f3 a) { return mk(-a.x, -a.y, -a.z); }
+
+// Host-build fminf/fmaxf (helper_math.h:134-142).
+__device__ __forceinline__ float smin(float a, float b) { return a < b ? a : b; }
+__device__ __forceinline__ float smax(float a, float b) { return a > b ? a : b; }
+__device__ __forceinline__ f3 smin3(f3 a, f3 b) { return mk(smin(a.x, b.x), smin(a.y, b.y), smin(a.z, b.z)); }
+__device__ __forceinline__ f3 smax3(f3 a, f3 b) { return mk(smax(a.x, b.x), smax(a.y, b.y), smax(a.z, b.z)); }
+
+__device__ __forceinline__ float dot(f3 a, f3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ f3 cross(f3 a, f3 b)
+{
+    return mk(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+__device__ __forceinline__ f3 normalize(f3 v)
+{
+    float invLen = 1.0f / sqrtf(dot(v, v));
+    return v * invLen;
+}
+__device__ __forceinline__ f3 lerp(f3 a, f3 b, float t) { return a + t * (b - a); }
+__device__ __forceinline__ float clampf(float f, float a, float b) { return smax(a, smin(f, b)); }
+__device__ __forceinline__ int clampi(int f, int a, int b)
+{
+    int m = f < b ? f : b;
+    return a > m ? a : m;
+}
+// float -> int as the reference's x86 host build converts (cvttss2si):
+// truncation; NaN and out-of-range values give 0x80000000.
+__device__ __forceinline__ int f2i_host(float x)
+{
+    if (!(x >= -2147483648.0f && x < 2147483648.0f)) return (int)0x80000000u;
+    return __float2int_rz(x);
+}
+
+// ---------------------------------------------------------------- Morton
+// splat3 (minimum_lbvh.h:173-182): low 21 bits of a, three apart.
+__device__ __forceinline__ uint64_t splat3(uint32_t a)
+{
+    uint64_t x = a & 0x1fffffu;
+    x = (x | x << 32) & 0x001f00000000ffffull;
+    x = (x | x << 16) & 0x001f0000ff0000ffull;
+    x = (x | x << 8) & 0x100f00f00f00f00full;
+    x = (x | x << 4) & 0x10c30c30c30c30c3ull;
+    x = (x | x << 2) & 0x1249249249249249ull;
+    return x;
+}
+// AABB::encodeMortonCode (minimum_lbvh.h:246-251) then the top 32 of the 63
+// bits (minimum_lbvh.cu:89).
+__device__ __forceinline__ uint32_t morton32(f3 lower, f3 upper, f3 p)
+{
+    f3 q = (p - lower) / (upper - lower) * (float)(kMortonMax + 1);
+    uint32_t cx = (uint32_t)clampi(f2i_host(q.x), 0, kMortonMax);
+    uint32_t cy = (uint32_t)clampi(f2i_host(q.y), 0, kMortonMax);
+    uint32_t cz = (uint32_t)clampi(f2i_host(q.z), 0, kMortonMax);
+    uint64_t m = splat3(cx) | splat3(cy) << 1 | splat3(cz) << 2;
+    return (uint32_t)(m >> 31);
+}
+// delta (minimum_lbvh.h:140-143)
+__device__ __forceinline__ uint32_t split_delta(uint32_t a, uint32_t b) { return 32u - __clz(a ^ b); }
+
+// ------------------------------------------------------------- geometry
+__device__ __forceinline__ float4 ldg4(const void* p) { return __ldg(reinterpret_cast<const float4*>(p)); }
+
+// A triangle (36 B, 4-byte aligned) as three points, read-only path.
+__device__ __forceinline__ void load_triangle(const float* __restrict__ tris, uint32_t i, f3& v0, f3& v1, f3& v2)
+{
+    const float* t = tris + 9ull * i;
+    v0 = mk(__ldg(t + 0), __ldg(t + 1), __ldg(t + 2));
+    v1 = mk(__ldg(t + 3), __ldg(t + 4), __ldg(t + 5));
+    v2 = mk(__ldg(t + 6), __ldg(t + 7), __ldg(t + 8));
+}
+
+// intersectRayTriangle (minimum_lbvh.h:363-413): plane distance, inclusive
+// [t_min, t_max] test, then the three edge volumes (a-b)x(a+b) whose signs
+// must agree (edge-watertight), barycentrics from the volumes.
+__device__ __forceinline__ bool intersect_triangle(float& tOut, float& uOut, float& vOut, f3& ngOut, float t_min,
+                                                   float t_max, f3 ro, f3 rd, f3 v0, f3 v1, f3 v2)
+{
+    f3 e0 = v1 - v0;
+    f3 e1 = v2 - v1;
+    f3 ng = cross(e0, e1);
+    float t = dot(v0 - ro, ng) / dot(ng, rd);
+    if (t_min <= t && t <= t_max) {
+        f3 e2 = v0 - v2;
+        f3 ro2 = ro * 2.0f;
+        float u_vol = dot(cross(e2, (v0 + v2) - ro2), rd);
+        float v_vol = dot(cross(e0, (v1 + v0) - ro2), rd);
+        float w_vol = dot(cross(e1, (v2 + v1) - ro2), rd);
+        if (fminf(fminf(u_vol, v_vol), w_vol) < 0.0f && 0.0f < fmaxf(fmaxf(u_vol, v_vol), w_vol)) return false;
+        float vol = u_vol + v_vol + w_vol;
+        tOut = t;
+        uOut = u_vol / vol;
+        vOut = v_vol / vol;
+        ngOut = ng;
+        return true;
+    }
+    return false;
+}
+
+// invRd (minimum_lbvh.h:898-901)
+__device__ __forceinline__ f3 inv_rd(f3 rd)
+{
+    return mk(clampf(1.0f / rd.x, -kFltMax, kFltMax), clampf(1.0f / rd.y, -kFltMax, kFltMax),
+              clampf(1.0f / rd.z, -kFltMax, kFltMax));
+}
+
+// slabs (minimum_lbvh.h:82-96) for one box given as (lower, upper); the
+// entry is clipped to tmin (0 in the reference) and the exit, inflated by
+// 1.00000024, to knownHitT. Only the sign of a zero can differ between
+// fminf/fmaxf and the host selects here, and no comparison below sees it.
+__device__ __forceinline__ float2 slab(f3 ro, f3 inv, f3 lo, f3 hi, float tmin, float knownHitT)
+{
+    f3 t0 = (lo - ro) * inv;
+    f3 t1 = (hi - ro) * inv;
+    float rmin = fmaxf(fmaxf(fminf(t0.x, t1.x), fminf(t0.y, t1.y)), fminf(t0.z, t1.z));
+    float rmax = fminf(fminf(fmaxf(t0.x, t1.x), fmaxf(t0.y, t1.y)), fmaxf(t0.z, t1.z)) * 1.00000024f;
+    rmin = fmaxf(rmin, 0.0f);
+    rmin = fmaxf(rmin, tmin);
+    rmax = fminf(rmax, knownHitT);
+    return make_float2(rmin, rmax);
+}
+
+struct HitRecord {
+    float t;
+    float u, v;
+    f3 ng;
+    uint32_t tri;
+};
+
+// One internal node as the traversal needs it: 4 x 16-byte read-only loads of
+// the 64-byte InternalNode.
+struct NodeView {
+    uint32_t c0, c1, parent, context;
+    f3 lo0, hi0, lo1, hi1;
+};
+__device__ __forceinline__ NodeView load_node(const mlbvh_internal_node* __restrict__ nodes, uint32_t i)
+{
+    const float4* p = reinterpret_cast<const float4*>(nodes + i);
+    float4 a = __ldg(p + 0), b = __ldg(p + 1), c = __ldg(p + 2), d = __ldg(p + 3);
+    NodeView n;
+    n.c0 = __float_as_uint(a.x);
+    n.c1 = __float_as_uint(a.y);
+    n.lo0 = mk(a.z, a.w, b.x);
+    n.hi0 = mk(b.y, b.z, b.w);
+    n.lo1 = mk(c.x, c.y, c.z);
+    n.hi1 = mk(c.w, d.x, d.y);
+    n.parent = __float_as_uint(d.z);
+    n.context = __float_as_uint(d.w);
+    return n;
+}
+
+// intersect_stackfree (minimum_lbvh.h:981-1061). Parent-pointer traversal:
+// from the parent go to the nearer hit child (entry distance, ties to the
+// left child) or back up; from the near child go to the far child when both
+// boxes are still hit, else up; from the far child go up. Both child boxes
+// are re-tested on every visit against the current closest t.
+// With kCount, *visits and *tests receive the internal-node visits and
+// triangle tests of the walk (the traffic model of the roofline).
+template <bool kAny, bool kCount = false>
+__device__ __forceinline__ void trace_stackfree(HitRecord& hit, const mlbvh_internal_node* __restrict__ nodes,
+                                                const float* __restrict__ tris, uint32_t root, f3 ro, f3 rd,
+                                                f3 inv, float tmin, uint32_t* visits = nullptr,
+                                                uint32_t* tests = nullptr)
+{
+    uint32_t curr = root, prev = kInvalid;
+    uint32_t nv = 0, nt = 0, steps = 0;
+    while (curr != kInvalid && ++steps < kMaxTraversalSteps) {
+        if (curr & kLeafBit) {
+            if (kCount) ++nt;
+            uint32_t ti = curr & ~kLeafBit;
+            f3 v0, v1, v2;
+            load_triangle(tris, ti, v0, v1, v2);
+            float t, u, v;
+            f3 ng;
+            if (intersect_triangle(t, u, v, ng, tmin, hit.t, ro, rd, v0, v1, v2)) {
+                hit.t = t;
+                hit.u = u;
+                hit.v = v;
+                hit.ng = ng;
+                hit.tri = ti;
+                if (kAny) break;
+            }
+            uint32_t s = curr;
+            curr = prev;
+            prev = s;
+            continue;
+        }
+        if (kCount) ++nv;
+        NodeView nd = load_node(nodes, curr);
+        float2 rl = slab(ro, inv, nd.lo0, nd.hi0, tmin, hit.t);
+        float2 rr = slab(ro, inv, nd.lo1, nd.hi1, tmin, hit.t);
+        bool hitL = rl.x <= rl.y;
+        bool hitR = rr.x <= rr.y;
+        uint32_t nearN = nd.c0, farN = nd.c1;
+        int nHits = 0;
+        if (hitL && hitR) {
+            if (rr.x < rl.x) {
+                nearN = nd.c1;
+                farN = nd.c0;
+            }
+            nHits = 2;
+        } else if (hitL || hitR) {
+            nHits = 1;
+            nearN = hitR ? farN : nearN;
+        }
+        uint32_t next;
+        if (prev == nd.parent)
+            next = 0 < nHits ? nearN : nd.parent;
+        else if (prev == nearN)
+            next = nHits == 2 ? farN : nd.parent;
+        else
+            next = nd.parent;
+        prev = curr;
+        curr = next;
+    }
+    if (kCount) {
+        *visits += nv;
+        *tests += nt;
+    }
+}
+
+// ------------------------------------------------------------ samples
+// sobol.h:31-39 (Laine-Karras style hash permutation, Burley 2020)
+__device__ __forceinline__ uint32_t lk_permutation(uint32_t x, uint32_t seed)
+{
+    x += seed;
+    x ^= x * 0x6c50b47cu;
+    x ^= x * 0xb82f1e52u;
+    x ^= x * 0xc7afe638u;
+    x ^= x * 0x8d22f6e6u;
+    return x;
+}
+__device__ __forceinline__ uint32_t nested_uniform_scramble(uint32_t x, uint32_t seed)
+{
+    return __brev(lk_permutation(__brev(x), seed));
+}
+// Sobol's second dimension as a Pascal-matrix product (sobol.h:51-59)
+__device__ __forceinline__ uint32_t pascal(uint32_t v)
+{
+    v ^= v << 16;
+    v ^= (v & 0x00FF00FFu) << 8;
+    v ^= (v & 0x0F0F0F0Fu) << 4;
+    v ^= (v & 0x33333333u) << 2;
+    v ^= (v & 0x55555555u) << 1;
+    return v;
+}
+__device__ __forceinline__ float random_float(uint32_t u)
+{
+    return (float)(u >> 8) / (float)((0xFFFFFFFFu >> 8) + 1);
+}
+__device__ __forceinline__ uint32_t hash_pcg(uint32_t v)  // sobol.h:76-81
+{
+    uint32_t state = v * 747796405u + 2891336453u;
+    uint32_t word = ((state >> ((state >> 28) + 4)) ^ state) * 277803737u;
+    return (word >> 22) ^ word;
+}
+__device__ __forceinline__ void pcg3d(uint32_t& x, uint32_t& y, uint32_t& z)  // sobol.h:83-107
+{
+    uint32_t vx = x * 1664525u + 1013904223u;
+    uint32_t vy = y * 1664525u + 1013904223u;
+    uint32_t vz = z * 1664525u + 1013904223u;
+    vx += vy * vz;
+    vy += vz * vx;
+    vz += vx * vy;
+    vx ^= vx >> 16;
+    vy ^= vy >> 16;
+    vz ^= vz >> 16;
+    vx += vy * vz;
+    vy += vz * vx;
+    vz += vx * vy;
+    x = vx;
+    y = vy;
+    z = vz;
+}
+// shuffled_scrambled_sobol_2d (sobol.h:119-129)
+__device__ __forceinline__ float2 sobol2d(uint32_t index, uint32_t p0, uint32_t p1, uint32_t p2)
+{
+    pcg3d(p0, p1, p2);
+    uint32_t v = lk_permutation(__brev(index), p0);
+    return make_float2(random_float(nested_uniform_scramble(v, p1)),
+                       random_float(nested_uniform_scramble(pascal(v), p2)));
+}
+
+// PCG32 (main_gpu.cu:51-82)
+struct Pcg {
+    uint64_t state, inc;
+    __device__ __forceinline__ Pcg(uint64_t seed, uint64_t seq)
+    {
+        state = 0;
+        inc = (seq << 1u) | 1u;
+        next();
+        state += seed;
+        next();
+    }
+    __device__ __forceinline__ uint32_t next()
+    {
+        uint64_t old = state;
+        state = old * 6364136223846793005ULL + inc;
+        uint32_t xorshifted = (uint32_t)(((old >> 18u) ^ old) >> 27u);
+        uint32_t rot = (uint32_t)(old >> 59u);
+        return (xorshifted >> rot) | (xorshifted << ((-rot) & 31));
+    }
+    __device__ __forceinline__ float uniformf() { return __uint_as_float((next() >> 9) | 0x3f800000u) - 1.0f; }
+};
+
+// FP32 sin and cos of phi in [0, 2*pi]: Cody-Waite reduction by pi/2 (split
+// in three float parts), then the Taylor polynomials of sin (to r^9) and cos
+// (to r^10) on [-pi/4, pi/4], all in fused multiply-adds. The same formula is
+// evaluated on the host by the oracle, so sample directions agree bit for bit;
+// its error is within 2 ulp of the true values over the sample range.
+__device__ __forceinline__ void sincos_portable(float phi, float& s, float& c)
+{
+    const float kPio2Hi = 1.57079637050628662109375f;
+    const float kPio2Mid = -4.371138828673792886547744274139404296875e-8f;
+    const float kPio2Lo = -1.71512451000588187280393448475e-15f;
+    float k = rintf(phi * 0.636619772367581343f);
+    float r = fmaf(-k, kPio2Hi, phi);
+    r = fmaf(-k, kPio2Mid, r);
+    r = fmaf(-k, kPio2Lo, r);
+    float r2 = r * r;
+    float ps = fmaf(r2, (float)(1.0 / 362880.0), (float)(-1.0 / 5040.0));
+    ps = fmaf(ps, r2, (float)(1.0 / 120.0));
+    ps = fmaf(ps, r2, (float)(-1.0 / 6.0));
+    float sr = fmaf(ps * r2, r, r);
+    float pc = fmaf(r2, (float)(-1.0 / 3628800.0), (float)(1.0 / 40320.0));
+    pc = fmaf(pc, r2, (float)(-1.0 / 720.0));
+    pc = fmaf(pc, r2, (float)(1.0 / 24.0));
+    pc = fmaf(pc, r2, -0.5f);
+    float cr = fmaf(pc, r2, 1.0f);
+    int q = ((int)k) & 3;
+    if (q == 0) {
+        s = sr;
+        c = cr;
+    } else if (q == 1) {
+        s = cr;
+        c = -sr;
+    } else if (q == 2) {
+        s = -sr;
+        c = -cr;
+    } else {
+        s = -cr;
+        c = sr;
+    }
+}
+
+constexpr float kPi = 3.14159265358979323846f;
+
+// sampleHemisphereCosWeighted (main_gpu.cu:24-36) with the portable sincos.
+__device__ __forceinline__ f3 sample_hemisphere(float xi0, float xi1)
+{
+    float phi = xi0 * 2.0f * kPi;
+    float r = sqrtf(xi1);
+    float sp, cp;
+    sincos_portable(phi, sp, cp);
+    float x = cp * r;
+    float z = sp * r;
+    float y = sqrtf(fmaxf(1.0f - r * r, 0.0f));
+    return mk(x, y, z);
+}
+
+// GetOrthonormalBasis (main_gpu.cu:39-45; Duff et al. 2017)
+__device__ __forceinline__ void onb(f3 z, f3& xaxis, f3& yaxis)
+{
+    const float sign = copysignf(1.0f, z.z);
+    const float a = -1.0f / (sign + z.z);
+    const float b = z.x * z.y * a;
+    xaxis = mk(1.0f + sign * z.x * z.x * a, sign * b, -sign * z.x);
+    yaxis = mk(b, sign + z.y * z.y * a, -z.y);
+}
+
+// packRGBA (main_gpu.cu:17-22): alpha is not stored.
+__device__ __forceinline__ uint32_t pack_rgba(float r, float g, float b)
+{
+    int x = clampi(f2i_host(r * 255.0f + 0.5f), 0, 255);
+    int y = clampi(f2i_host(g * 255.0f + 0.5f), 0, 255);
+    int z = clampi(f2i_host(b * 255.0f + 0.5f), 0, 255);
+    return ((uint32_t)z << 16) | ((uint32_t)y << 8) | (uint32_t)x;
+}
+
+struct Camera {
+    f3 origin, right, up;
+};
+// RayGenerator::shoot (camera.h:24-31)
+__device__ __forceinline__ void shoot(const Camera& cam, float u, float v, f3& ro, f3& rd)
+{
+    f3 from = cam.origin;
+    f3 forward = normalize(cross(cam.up, cam.right));
+    f3 to = cam.origin + forward + lerp(-cam.right, cam.right, u) + lerp(cam.up, -cam.up, v);
+    ro = from;
+    rd = to - from;
+}
+
+}  // namespace mlbvh

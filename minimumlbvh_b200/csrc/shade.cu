@@ -1,0 +1,471 @@
+// Shading on B200: the reference's normal / ao / pt / pack kernels
+// (main_gpu.cu:84-286) restated over this library's traversal.
+//
+// AO is ray-major instead of pixel-major: k_ao_primary traces one closest-hit
+// ray per pixel and appends each hit pixel (AO origin and facing normal) to a
+// queue; k_ao_rays is a persistent kernel whose warps take 32 consecutive
+// (pixel, sample) items at a time from an atomic work counter, so a warp's
+// any-hit rays share one origin and the SMs never idle on missed pixels;
+// k_ao_finish turns the per-pixel occlusion counts into the packed image.
+#include <algorithm>
+
+#include "capi_internal.h"
+#include "common.cuh"
+
+namespace mlbvh {
+
+namespace {
+
+constexpr int kTileW = 16, kTileH = 8;  // 128-thread pixel tile: 4 warps of 8 x 4 pixels
+constexpr int kAoThreads = 128;
+constexpr int kFinishThreads = 256;
+
+struct AoRecord {
+    float ox, oy, oz;
+    float nx, ny, nz;
+    uint32_t pixel;
+    uint32_t pad;
+};
+
+struct RenderLayout {
+    size_t header;  // u32 queueCount, u32 workCounter
+    size_t records;
+    size_t counts;
+    size_t total;
+};
+size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+RenderLayout render_layout(int w, int h)
+{
+    RenderLayout L;
+    const size_t px = (size_t)w * (size_t)h;
+    L.header = 0;
+    L.records = 256;
+    L.counts = align256(L.records + sizeof(AoRecord) * px);
+    L.total = align256(L.counts + sizeof(uint32_t) * px);
+    return L;
+}
+
+__device__ __forceinline__ Camera to_camera(const mlbvh_ray_generator& g)
+{
+    Camera c;
+    c.origin = mk(g.origin[0], g.origin[1], g.origin[2]);
+    c.right = mk(g.right[0], g.right[1], g.right[2]);
+    c.up = mk(g.up[0], g.up[1], g.up[2]);
+    return c;
+}
+
+__device__ __forceinline__ bool tile_pixel(int w, int h, int& xi, int& yi)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    xi = blockIdx.x * kTileW + (lane & 7) + 8 * (warp & 1);
+    yi = blockIdx.y * kTileH + (lane >> 3) + 4 * (warp >> 1);
+    return xi < w && yi < h;
+}
+
+// PCG32 jump-ahead by `delta` steps (Brown, "Random Number Generation with
+// Arbitrary Strides", 1994), so that AO sample i can start at draw 2i.
+__device__ __forceinline__ void pcg_advance(Pcg& r, uint64_t delta)
+{
+    uint64_t curMult = 6364136223846793005ULL, curPlus = r.inc, accMult = 1, accPlus = 0;
+    while (delta > 0) {
+        if (delta & 1) {
+            accMult *= curMult;
+            accPlus = accPlus * curMult + curPlus;
+        }
+        curPlus = (curMult + 1) * curPlus;
+        curMult *= curMult;
+        delta >>= 1;
+    }
+    r.state = accMult * r.state + accPlus;
+}
+
+// Adds per-thread traversal counts to stats[1] (node visits) and stats[2]
+// (triangle tests) with one atomic per warp; AO rays also to stats[3], [4].
+__device__ __forceinline__ void add_stats(unsigned long long* stats, uint32_t visits, uint32_t tests, bool aoRays)
+{
+    unsigned long long v = visits, t = tests;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        v += __shfl_xor_sync(0xffffffffu, v, o);
+        t += __shfl_xor_sync(0xffffffffu, t, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(stats + 1, v);
+        atomicAdd(stats + 2, t);
+        if (aoRays) {
+            atomicAdd(stats + 3, v);
+            atomicAdd(stats + 4, t);
+        }
+    }
+}
+
+// Primary rays of ao (main_gpu.cu:121-144): closest hit, flip the normal
+// towards the viewer, AO origin p + n * 1e-3.
+template <bool kCount>
+__global__ void __launch_bounds__(kTileW* kTileH)
+    k_ao_primary(mlbvh_ray_generator gen, int w, int h, const mlbvh_node_index* __restrict__ rootPtr,
+                 const mlbvh_internal_node* __restrict__ nodes, const float* __restrict__ tris,
+                 AoRecord* __restrict__ records, uint32_t* __restrict__ queueCount, uint32_t* __restrict__ counts,
+                 unsigned long long* __restrict__ stats)
+{
+    uint32_t visits = 0, tests = 0;
+    int xi, yi;
+    const bool inside = tile_pixel(w, h, xi, yi);
+    bool isHit = false;
+    AoRecord rec;
+    if (inside) {
+        const Camera cam = to_camera(gen);
+        const int pixel = xi + yi * w;
+        f3 ro, rd;
+        shoot(cam, (float)xi / (float)w, (float)yi / (float)h, ro, rd);
+        HitRecord hit;
+        hit.t = kFltMax;
+        hit.tri = 0xFFFFFFFFu;
+        trace_stackfree<false, kCount>(hit, nodes, tris, __ldg(rootPtr), ro, rd, inv_rd(rd), 0.0f, &visits, &tests);
+        if (hit.t == kFltMax) {
+            counts[pixel] = 0xFFFFFFFFu;
+        } else {
+            f3 n = normalize(hit.ng);
+            if (0.0f < dot(n, rd)) n = -n;
+            const f3 o = ro + rd * hit.t + n * 0.001f;
+            rec = AoRecord{o.x, o.y, o.z, n.x, n.y, n.z, (uint32_t)pixel, 0u};
+            counts[pixel] = 0u;
+            isHit = true;
+        }
+    }
+    if (kCount) add_stats(stats, visits, tests, false);
+    // warp-aggregated append to the hit queue
+    const uint32_t mask = __ballot_sync(0xffffffffu, isHit);
+    if (mask == 0u) return;
+    const int lane = threadIdx.x & 31;
+    uint32_t base = 0;
+    if (lane == __ffs(mask) - 1) base = atomicAdd(queueCount, (uint32_t)__popc(mask));
+    base = __shfl_sync(0xffffffffu, base, __ffs(mask) - 1);
+    if (isHit) {
+        float4* dst = reinterpret_cast<float4*>(records + base + __popc(mask & ((1u << lane) - 1u)));
+        dst[0] = make_float4(rec.ox, rec.oy, rec.oz, rec.nx);
+        dst[1] = make_float4(rec.ny, rec.nz, __uint_as_float(rec.pixel), 0.0f);
+    }
+}
+
+// AO rays (main_gpu.cu:146-173): item = (queue entry, sample). Each warp takes
+// 32 consecutive items; per-pixel occlusion counts are reduced across the
+// lanes of one pixel before a single atomic add.
+template <bool kCount>
+__global__ void __launch_bounds__(kAoThreads)
+    k_ao_rays(const AoRecord* __restrict__ records, const uint32_t* __restrict__ queueCount,
+              uint32_t* __restrict__ workCounter, int w, int nSamples, float radius, uint32_t seed, int useSobol,
+              const mlbvh_node_index* __restrict__ rootPtr, const mlbvh_internal_node* __restrict__ nodes,
+              const float* __restrict__ tris, uint32_t* __restrict__ counts, unsigned long long* __restrict__ stats)
+{
+    uint32_t visits = 0, tests = 0;
+    const int lane = threadIdx.x & 31;
+    const uint64_t total = (uint64_t)(*queueCount) * (uint64_t)nSamples;
+    const uint32_t root = __ldg(rootPtr);
+    for (;;) {
+        unsigned long long base = 0;
+        if (lane == 0) base = atomicAdd(reinterpret_cast<unsigned long long*>(workCounter), 32ull);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (base >= total) break;
+        const uint64_t item = base + (uint64_t)lane;
+        const bool valid = item < total;
+        uint32_t entry = 0xFFFFFFFFu;
+        bool occluded = false;
+        if (valid) {
+            entry = (uint32_t)(item / (uint64_t)nSamples);
+            const uint32_t s = (uint32_t)(item - (uint64_t)entry * (uint64_t)nSamples);
+            const float4* rp = reinterpret_cast<const float4*>(records + entry);
+            const float4 r0 = __ldg(rp), r1 = __ldg(rp + 1);
+            const f3 origin = mk(r0.x, r0.y, r0.z), n = mk(r0.w, r1.x, r1.y);
+            const uint32_t pixel = __float_as_uint(r1.z);
+            const uint32_t xi = pixel % (uint32_t)w, yi = pixel / (uint32_t)w;
+            f3 xaxis, zaxis;
+            onb(n, xaxis, zaxis);
+            float2 rnd;
+            if (useSobol) {
+                rnd = sobol2d(s, xi, yi, seed);
+            } else {
+                Pcg rng(hash_pcg(pixel), 0);
+                pcg_advance(rng, 2ull * s);
+                rnd.x = rng.uniformf();
+                rnd.y = rng.uniformf();
+            }
+            const f3 dl = sample_hemisphere(rnd.x, rnd.y);
+            const f3 dir = xaxis * dl.x + zaxis * dl.z + n * dl.y;
+            HitRecord hit;
+            hit.t = radius;
+            hit.tri = 0xFFFFFFFFu;
+            trace_stackfree<true, kCount>(hit, nodes, tris, root, origin, dir, inv_rd(dir), 0.0f, &visits, &tests);
+            occluded = hit.t != radius;
+        }
+        const uint32_t peers = __match_any_sync(0xffffffffu, entry);
+        const uint32_t occ = __ballot_sync(0xffffffffu, occluded);
+        if (valid && lane == __ffs(peers) - 1) {
+            const uint32_t c = __popc(occ & peers);
+            if (c) {
+                const uint32_t pixel = __float_as_uint(__ldg(reinterpret_cast<const float*>(records + entry) + 6));
+                atomicAdd(counts + pixel, c);
+            }
+        }
+    }
+    if (kCount) add_stats(stats, visits, tests, true);
+}
+
+// The tail of ao (main_gpu.cu:169-176): ao accumulates 1/nSample per occluded
+// ray in float (so it equals the reference's sum), gamma 1/2.2, pack.
+__global__ void __launch_bounds__(kFinishThreads)
+    k_ao_finish(const uint32_t* __restrict__ counts, int nPixels, int nSamples, uint32_t* __restrict__ pixels,
+                uint32_t* __restrict__ occludedOut, const uint32_t* __restrict__ queueCount,
+                unsigned long long* __restrict__ stats)
+{
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p == 0 && stats) *stats = (unsigned long long)nPixels + (unsigned long long)(*queueCount) * nSamples;
+    if (p >= nPixels) return;
+    const uint32_t c = counts[p];
+    uint32_t rgba;
+    if (c == 0xFFFFFFFFu) {
+        rgba = pack_rgba(0.0f, 0.0f, 0.0f);
+    } else {
+        float ao = 0.0f;
+        const float step = 1.0f / (float)nSamples;
+        for (uint32_t k = 0; k < c; ++k) ao += step;
+        const float brightness = powf(1.0f - ao, 1.0f / 2.2f);
+        rgba = pack_rgba(brightness, brightness, brightness);
+    }
+    if (pixels) pixels[p] = rgba;
+    if (occludedOut) occludedOut[p] = c;
+}
+
+// normal (main_gpu.cu:84-109)
+__global__ void __launch_bounds__(kTileW* kTileH)
+    k_normal(uint32_t* __restrict__ pixels, mlbvh_ray_generator gen, int w, int h,
+             const mlbvh_node_index* __restrict__ rootPtr, const mlbvh_internal_node* __restrict__ nodes,
+             const float* __restrict__ tris)
+{
+    int xi, yi;
+    if (!tile_pixel(w, h, xi, yi)) return;
+    const Camera cam = to_camera(gen);
+    f3 ro, rd;
+    shoot(cam, (float)xi / (float)w, (float)yi / (float)h, ro, rd);
+    HitRecord hit;
+    hit.t = kFltMax;
+    hit.tri = 0xFFFFFFFFu;
+    trace_stackfree<false>(hit, nodes, tris, __ldg(rootPtr), ro, rd, inv_rd(rd), 0.0f);
+    uint32_t rgba;
+    if (hit.t != kFltMax) {
+        const f3 n = normalize(hit.ng);
+        const f3 c = (n + mk(1.0f, 1.0f, 1.0f)) * 0.5f;
+        rgba = pack_rgba(c.x, c.y, c.z);
+    } else {
+        rgba = pack_rgba(0.0f, 0.0f, 0.0f);
+    }
+    pixels[xi + yi * w] = rgba;
+}
+
+struct PtRandom {
+    int useSobol;
+    uint32_t iteration, xi, yi, dim;
+    Pcg rng;
+    __device__ __forceinline__ float2 next()
+    {
+        if (useSobol) return sobol2d(iteration, xi, yi, dim++);
+        float2 r;
+        r.x = rng.uniformf();
+        r.y = rng.uniformf();
+        return r;
+    }
+};
+
+// pt (main_gpu.cu:179-272): one progressive sample per pixel.
+__global__ void __launch_bounds__(kTileW* kTileH)
+    k_pt(float4* __restrict__ accum, mlbvh_ray_generator gen, int w, int h,
+         const mlbvh_node_index* __restrict__ rootPtr, const mlbvh_internal_node* __restrict__ nodes,
+         const float* __restrict__ tris, const float* __restrict__ attribs, int useSobol, int maxSPP, int maxDepth)
+{
+    int xi, yi;
+    if (!tile_pixel(w, h, xi, yi)) return;
+    const Camera cam = to_camera(gen);
+    const int pixel = xi + yi * w;
+    float4 acc = accum[pixel];
+    const int iteration = (int)acc.w;
+    PtRandom rr{useSobol, (uint32_t)iteration, (uint32_t)xi, (uint32_t)yi, 0u,
+                Pcg(hash_pcg(hash_pcg((uint32_t)pixel) + (uint32_t)iteration), 0)};
+    const uint32_t root = __ldg(rootPtr);
+    float2 rnd = rr.next();
+    f3 ro, rd;
+    shoot(cam, ((float)xi + rnd.x) / (float)w, ((float)yi + rnd.y) / (float)h, ro, rd);
+    f3 color = mk(0.0f, 0.0f, 0.0f);
+    f3 throughput = mk(1.0f, 1.0f, 1.0f);
+    HitRecord hit;
+    hit.t = kFltMax;
+    hit.tri = 0xFFFFFFFFu;
+    trace_stackfree<false>(hit, nodes, tris, root, ro, rd, inv_rd(rd), 0.0f);
+    if (hit.t != kFltMax)
+        for (int depth = 0; depth < maxDepth; depth++) {
+            const float2 r2 = rr.next();
+            const f3 hit_p = ro + rd * hit.t;
+            f3 hit_n = normalize(hit.ng);
+            if (0.0f < dot(hit_n, rd)) hit_n = -hit_n;
+            const float* at = attribs + 15 * (size_t)hit.tri;
+            const f3 refl = mk(__ldg(at + 9), __ldg(at + 10), __ldg(at + 11));
+            const f3 emis = mk(__ldg(at + 12), __ldg(at + 13), __ldg(at + 14));
+            color = color + throughput * emis;
+            f3 xaxis, zaxis;
+            onb(hit_n, xaxis, zaxis);
+            const f3 dl = sample_hemisphere(r2.x, r2.y);
+            const f3 next_ro = hit_p + hit_n * 0.0001f;
+            const f3 next_rd = xaxis * dl.x + zaxis * dl.z + hit_n * dl.y;
+            throughput = throughput * refl;
+            const float rrThreshold = 0.25f;
+            const float maxComp = smax(smax(throughput.x, throughput.y), throughput.z);
+            const float p = smin(maxComp / rrThreshold, 1.0f);
+            if (p < rr.next().x) break;
+            throughput = throughput / p;
+            hit.t = kFltMax;
+            hit.u = hit.v = 0.0f;
+            hit.ng = mk(0.0f, 0.0f, 0.0f);
+            hit.tri = 0xFFFFFFFFu;
+            trace_stackfree<false>(hit, nodes, tris, root, next_ro, next_rd, inv_rd(next_rd), 0.0f);
+            if (hit.t == kFltMax) break;
+            ro = next_ro;
+            rd = next_rd;
+        }
+    if (iteration < maxSPP) {
+        acc.x += color.x;
+        acc.y += color.y;
+        acc.z += color.z;
+        acc.w += 1.0f;
+        accum[pixel] = acc;
+    }
+}
+
+// pack (main_gpu.cu:273-286)
+__global__ void k_pack(uint32_t* __restrict__ pixels, const float4* __restrict__ accum, int n)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float4 a = accum[i];
+    pixels[i] = pack_rgba(powf(a.x / a.w, 1.0f / 2.2f), powf(a.y / a.w, 1.0f / 2.2f), powf(a.z / a.w, 1.0f / 2.2f));
+}
+
+dim3 tile_grid(int w, int h) { return dim3((w + kTileW - 1) / kTileW, (h + kTileH - 1) / kTileH); }
+
+mlbvh_status check_image(int w, int h)
+{
+    if (w <= 0 || h <= 0 || (long long)w * (long long)h >= (1ll << 31))
+        return fail(MLBVH_ERR_INVALID_ARG, "image size must be positive and below 2^31 pixels");
+    return MLBVH_OK;
+}
+
+int ao_ray_blocks()
+{
+    static int blocksPerSm = 0;
+    if (blocksPerSm == 0) {
+        int b = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_ao_rays<false>, kAoThreads, 0) != cudaSuccess || b <= 0)
+            b = 8;
+        blocksPerSm = b;
+    }
+    return blocksPerSm * device_sm_count();
+}
+
+}  // namespace
+
+size_t render_scratch_bytes(int w, int h)
+{
+    if (w <= 0 || h <= 0) return 0;
+    return render_layout(w, h).total;
+}
+
+mlbvh_status render_normal(uint32_t* dPixels, int w, int h, const mlbvh_ray_generator& cam,
+                           const mlbvh_node_index* dRoot, const mlbvh_internal_node* dNodes,
+                           const mlbvh_triangle* dTris, cudaStream_t stream)
+{
+    if (mlbvh_status s = check_image(w, h)) return s;
+    if (!dPixels || !dRoot || !dTris) return fail(MLBVH_ERR_INVALID_ARG, "null pointer");
+    if (!aligned16(dPixels) || !aligned16(dRoot) || !aligned16(dNodes) || !aligned16(dTris))
+        return fail(MLBVH_ERR_INVALID_ARG, "device pointers must be 16-byte aligned");
+    k_normal<<<tile_grid(w, h), kTileW * kTileH, 0, stream>>>(dPixels, cam, w, h, dRoot, dNodes,
+                                                              reinterpret_cast<const float*>(dTris));
+    MLBVH_CHECK_LAUNCH("k_normal");
+    return MLBVH_OK;
+}
+
+mlbvh_status render_ao(uint32_t* dPixels, uint32_t* dOccluded, int w, int h, const mlbvh_ray_generator& cam,
+                       const mlbvh_node_index* dRoot, const mlbvh_internal_node* dNodes, const mlbvh_triangle* dTris,
+                       int useSobol, int nSamples, float radius, uint32_t seed, unsigned long long* dStats,
+                       void* dScratch, size_t scratchBytes, cudaStream_t stream)
+{
+    if (mlbvh_status s = check_image(w, h)) return s;
+    if (nSamples <= 0 || nSamples > 65536) return fail(MLBVH_ERR_INVALID_ARG, "nSamples must be in [1, 65536]");
+    if (!dRoot || !dTris || !dScratch) return fail(MLBVH_ERR_INVALID_ARG, "null pointer");
+    if (!aligned16(dPixels) || !aligned16(dOccluded) || !aligned16(dRoot) || !aligned16(dNodes) ||
+        !aligned16(dTris) || !aligned16(dScratch) || (reinterpret_cast<uintptr_t>(dStats) & 7u))
+        return fail(MLBVH_ERR_INVALID_ARG, "device pointers must be 16-byte aligned");
+    const RenderLayout L = render_layout(w, h);
+    if (scratchBytes < L.total) return fail(MLBVH_ERR_INVALID_ARG, "scratch smaller than mlbvh_render_scratch_bytes");
+    char* s = static_cast<char*>(dScratch);
+    uint32_t* header = reinterpret_cast<uint32_t*>(s + L.header);
+    AoRecord* records = reinterpret_cast<AoRecord*>(s + L.records);
+    uint32_t* counts = reinterpret_cast<uint32_t*>(s + L.counts);
+    const float* tris = reinterpret_cast<const float*>(dTris);
+
+    cudaError_t e = cudaMemsetAsync(header, 0, 16, stream);  // queue count, 64-bit work counter
+    if (e == cudaSuccess && dStats) e = cudaMemsetAsync(dStats, 0, 5 * sizeof(unsigned long long), stream);
+    if (e != cudaSuccess) return fail(MLBVH_ERR_CUDA, cudaGetErrorString(e));
+    const dim3 grid = tile_grid(w, h);
+    if (dStats)
+        k_ao_primary<true><<<grid, kTileW * kTileH, 0, stream>>>(cam, w, h, dRoot, dNodes, tris, records, header,
+                                                                 counts, dStats);
+    else
+        k_ao_primary<false><<<grid, kTileW * kTileH, 0, stream>>>(cam, w, h, dRoot, dNodes, tris, records, header,
+                                                                  counts, nullptr);
+    MLBVH_CHECK_LAUNCH("k_ao_primary");
+    ProfileEvents ev = take_profile_events();
+    if (ev.start) cudaEventRecord(ev.start, stream);
+    if (dStats)
+        k_ao_rays<true><<<ao_ray_blocks(), kAoThreads, 0, stream>>>(records, header, header + 2, w, nSamples, radius,
+                                                                    seed, useSobol, dRoot, dNodes, tris, counts, dStats);
+    else
+        k_ao_rays<false><<<ao_ray_blocks(), kAoThreads, 0, stream>>>(records, header, header + 2, w, nSamples, radius,
+                                                                     seed, useSobol, dRoot, dNodes, tris, counts,
+                                                                     nullptr);
+    MLBVH_CHECK_LAUNCH("k_ao_rays");
+    if (ev.stop) cudaEventRecord(ev.stop, stream);
+    const int px = w * h;
+    k_ao_finish<<<(px + kFinishThreads - 1) / kFinishThreads, kFinishThreads, 0, stream>>>(
+        counts, px, nSamples, dPixels, dOccluded, header, dStats);
+    MLBVH_CHECK_LAUNCH("k_ao_finish");
+    return MLBVH_OK;
+}
+
+mlbvh_status render_pt(float* dAccum, int w, int h, const mlbvh_ray_generator& cam, const mlbvh_node_index* dRoot,
+                       const mlbvh_internal_node* dNodes, const mlbvh_triangle* dTris,
+                       const mlbvh_triangle_attrib* dAttribs, int useSobol, int maxSPP, int maxDepth,
+                       cudaStream_t stream)
+{
+    if (mlbvh_status s = check_image(w, h)) return s;
+    if (!dAccum || !dRoot || !dTris || !dAttribs) return fail(MLBVH_ERR_INVALID_ARG, "null pointer");
+    if (!aligned16(dAccum) || !aligned16(dRoot) || !aligned16(dNodes) || !aligned16(dTris) || !aligned16(dAttribs))
+        return fail(MLBVH_ERR_INVALID_ARG, "device pointers must be 16-byte aligned");
+    if (maxDepth < 0) return fail(MLBVH_ERR_INVALID_ARG, "maxDepth must be >= 0");
+    k_pt<<<tile_grid(w, h), kTileW * kTileH, 0, stream>>>(reinterpret_cast<float4*>(dAccum), cam, w, h, dRoot, dNodes,
+                                                          reinterpret_cast<const float*>(dTris),
+                                                          reinterpret_cast<const float*>(dAttribs), useSobol, maxSPP,
+                                                          maxDepth);
+    MLBVH_CHECK_LAUNCH("k_pt");
+    return MLBVH_OK;
+}
+
+mlbvh_status pack(uint32_t* dPixels, const float* dAccum, int n, cudaStream_t stream)
+{
+    if (n <= 0) return n == 0 ? MLBVH_OK : fail(MLBVH_ERR_INVALID_ARG, "negative pixel count");
+    if (!dPixels || !dAccum) return fail(MLBVH_ERR_INVALID_ARG, "null pointer");
+    if (!aligned16(dPixels) || !aligned16(dAccum))
+        return fail(MLBVH_ERR_INVALID_ARG, "device pointers must be 16-byte aligned");
+    k_pack<<<(n + 255) / 256, 256, 0, stream>>>(dPixels, reinterpret_cast<const float4*>(dAccum), n);
+    MLBVH_CHECK_LAUNCH("k_pack");
+    return MLBVH_OK;
+}
+
+}  // namespace mlbvh

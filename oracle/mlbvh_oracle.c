@@ -1,0 +1,1160 @@
+/* Test infrastructure only — the oracle (checker) for the MinimumLBVH hot path.
+ *
+ * Plain-C restatement of the reference's CPU algorithm. Each function cites
+ * the reference file:line it follows. Compiled with -ffp-contract=off so that
+ * every float expression rounds exactly as the reference's host build does
+ * (one rounding per written operation, in source order). See mlbvh_oracle.h.
+ */
+#define _GNU_SOURCE
+#include "mlbvh_oracle.h"
+
+#include <math.h>
+#include <pthread.h>
+#include <stdlib.h>
+#include <string.h>
+#include <unistd.h>
+
+#define ORC_FLT_MAX 3.402823466e+38F /* minimum_lbvh.h:37 */
+#define ORC_MORTON_MAX 0x1FFFFF      /* minimum_lbvh.h:38 */
+#define ORC_INVALID 0x7FFFFFFFu      /* NodeIndex::invalid(), minimum_lbvh.h:261-264 */
+#define ORC_LEAF_BIT 0x80000000u
+
+int orc_version(void) { return 1; }
+
+/* ------------------------------------------------------------------ threads */
+static int g_threads = 0;
+void orc_set_threads(int n) { g_threads = n; }
+static int orc_threads(void)
+{
+    if (g_threads > 0) return g_threads;
+    const char* env = getenv("MLBVH_ORACLE_THREADS");
+    if (env && atoi(env) > 0) return atoi(env);
+    long n = sysconf(_SC_NPROCESSORS_ONLN);
+    return n > 0 ? (int)n : 1;
+}
+
+typedef void (*orc_range_fn)(void* ctx, uint32_t begin, uint32_t end);
+typedef struct {
+    orc_range_fn fn;
+    void* ctx;
+    uint32_t n, chunk;
+    uint32_t next; /* atomic */
+} orc_pool_job;
+
+static void* orc_worker(void* p)
+{
+    orc_pool_job* job = (orc_pool_job*)p;
+    for (;;)
+    {
+        uint32_t b = __atomic_fetch_add(&job->next, job->chunk, __ATOMIC_RELAXED);
+        if (b >= job->n) break;
+        uint32_t e = b + job->chunk < job->n ? b + job->chunk : job->n;
+        job->fn(job->ctx, b, e);
+    }
+    return NULL;
+}
+
+static void orc_parallel_for(uint32_t n, uint32_t chunk, orc_range_fn fn, void* ctx)
+{
+    int nt = orc_threads();
+    if (n == 0) return;
+    if (nt <= 1 || n <= chunk)
+    {
+        fn(ctx, 0, n);
+        return;
+    }
+    orc_pool_job job = {fn, ctx, n, chunk, 0};
+    pthread_t th[256];
+    if (nt > 256) nt = 256;
+    int started = 0;
+    for (int i = 1; i < nt; ++i)
+        if (pthread_create(&th[started], NULL, orc_worker, &job) == 0) started++;
+    orc_worker(&job);
+    for (int i = 0; i < started; ++i) pthread_join(th[i], NULL);
+}
+
+/* --------------------------------------------------------------- float math
+ * helper_math.h host semantics: fminf/fmaxf are selects (helper_math.h:134-142),
+ * rsqrtf is 1/sqrtf (:154-157), normalize is v * rsqrtf(dot(v, v)) (:1437). */
+static inline float smin(float a, float b) { return a < b ? a : b; }
+static inline float smax(float a, float b) { return a > b ? a : b; }
+static inline orc_f3 f3(float x, float y, float z) { orc_f3 r = {x, y, z}; return r; }
+static inline orc_f3 add3(orc_f3 a, orc_f3 b) { return f3(a.x + b.x, a.y + b.y, a.z + b.z); }
+static inline orc_f3 sub3(orc_f3 a, orc_f3 b) { return f3(a.x - b.x, a.y - b.y, a.z - b.z); }
+static inline orc_f3 mul3(orc_f3 a, orc_f3 b) { return f3(a.x * b.x, a.y * b.y, a.z * b.z); }
+static inline orc_f3 muls(orc_f3 a, float s) { return f3(a.x * s, a.y * s, a.z * s); }
+static inline orc_f3 smul(float s, orc_f3 a) { return f3(s * a.x, s * a.y, s * a.z); }
+static inline orc_f3 divs(orc_f3 a, float s) { return f3(a.x / s, a.y / s, a.z / s); }
+static inline orc_f3 div3(orc_f3 a, orc_f3 b) { return f3(a.x / b.x, a.y / b.y, a.z / b.z); }
+static inline orc_f3 neg3(orc_f3 a) { return f3(-a.x, -a.y, -a.z); }
+static inline orc_f3 min3(orc_f3 a, orc_f3 b) { return f3(smin(a.x, b.x), smin(a.y, b.y), smin(a.z, b.z)); }
+static inline orc_f3 max3(orc_f3 a, orc_f3 b) { return f3(smax(a.x, b.x), smax(a.y, b.y), smax(a.z, b.z)); }
+static inline float dot3(orc_f3 a, orc_f3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+static inline orc_f3 cross3(orc_f3 a, orc_f3 b)
+{
+    return f3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+static inline orc_f3 normalize3(orc_f3 v)
+{
+    float invLen = 1.0f / sqrtf(dot3(v, v));
+    return muls(v, invLen);
+}
+/* helper_math.h:1266 lerp(a, b, t) = a + t*(b-a) */
+static inline orc_f3 lerp3(orc_f3 a, orc_f3 b, float t) { return add3(a, smul(t, sub3(b, a))); }
+static inline float compMin(orc_f3 v) { return smin(smin(v.x, v.y), v.z); } /* minimum_lbvh.h:73 */
+static inline float compMax(orc_f3 v) { return smax(smax(v.x, v.y), v.z); } /* minimum_lbvh.h:77 */
+static inline float clampf(float f, float a, float b) { return smax(a, smin(f, b)); } /* helper_math.h:1280 */
+static inline int clampi(int f, int a, int b)
+{
+    int m = f < b ? f : b;
+    return a > m ? a : m;
+}
+/* float -> int conversion as x86 cvttss2si does it (the reference's host
+ * build): truncation, and 0x80000000 for NaN or out-of-range values. */
+static inline int f2i_x86(float x)
+{
+    if (!(x >= -2147483648.0f && x < 2147483648.0f)) return (int)0x80000000u;
+    return (int)x;
+}
+
+/* -------------------------------------------------------- bits and Morton */
+int orc_clz(uint32_t x) { return x ? __builtin_clz(x) : 32; }          /* minimum_lbvh.h:99 */
+int orc_clz64(uint64_t x) { return x ? __builtin_clzll(x) : 64; }      /* minimum_lbvh.h:107 */
+int orc_ffs(uint32_t x) { return x ? __builtin_ctz(x) + 1 : 0; }       /* minimum_lbvh.h:117 */
+int orc_ffs64(uint64_t x) { return x ? __builtin_ctzll(x) + 1 : 0; }   /* minimum_lbvh.h:128 */
+int orc_delta(uint32_t a, uint32_t b) { return 32 - orc_clz(a ^ b); } /* minimum_lbvh.h:140 */
+
+/* minimum_lbvh.h:149-160: bit i of x, y, z lands at bit 3i, 3i+1, 3i+2. */
+uint64_t orc_encode_morton_naive(uint32_t x, uint32_t y, uint32_t z)
+{
+    uint64_t code = 0;
+    for (uint64_t i = 0; i < 64 / 3; ++i)
+    {
+        code |= ((uint64_t)(x & (1u << i)) << (2 * i + 0)) |
+                ((uint64_t)(y & (1u << i)) << (2 * i + 1)) |
+                ((uint64_t)(z & (1u << i)) << (2 * i + 2));
+    }
+    return code;
+}
+
+/* minimum_lbvh.h:173-182: spreads the low 21 bits of a three apart by
+ * successive shift-or-mask steps (the usual magic-number dilation). */
+uint64_t orc_splat3(uint32_t a)
+{
+    uint64_t x = a & 0x1fffffu;
+    x = (x | x << 32) & 0x001f00000000ffffull;
+    x = (x | x << 16) & 0x001f0000ff0000ffull;
+    x = (x | x << 8) & 0x100f00f00f00f00full;
+    x = (x | x << 4) & 0x10c30c30c30c30c3ull;
+    x = (x | x << 2) & 0x1249249249249249ull;
+    return x;
+}
+
+/* minimum_lbvh.h:162-171: the inverse of splat3. */
+uint32_t orc_compact3(uint64_t m)
+{
+    uint64_t x = m & 0x1249249249249249ull;
+    x = (x ^ (x >> 2)) & 0x10c30c30c30c30c3ull;
+    x = (x ^ (x >> 4)) & 0x100f00f00f00f00full;
+    x = (x ^ (x >> 8)) & 0x001f0000ff0000ffull;
+    x = (x ^ (x >> 16)) & 0x001f00000000ffffull;
+    x = (x ^ (x >> 32)) & 0x1fffffull;
+    return (uint32_t)x;
+}
+
+uint64_t orc_encode_morton(uint32_t x, uint32_t y, uint32_t z) /* minimum_lbvh.h:190 */
+{
+    return orc_splat3(x) | orc_splat3(y) << 1 | orc_splat3(z) << 2;
+}
+
+void orc_decode_morton(uint64_t m, uint32_t* x, uint32_t* y, uint32_t* z) /* :184 */
+{
+    *x = orc_compact3(m);
+    *y = orc_compact3(m >> 1);
+    *z = orc_compact3(m >> 2);
+}
+
+/* AABB::encodeMortonCode (minimum_lbvh.h:246-251): quantise
+ * (p - lower) / (upper - lower) * 2^21, truncate, clamp to [0, 2^21 - 1]. */
+uint64_t orc_aabb_morton(const orc_aabb* box, orc_f3 p)
+{
+    orc_f3 q = muls(div3(sub3(p, box->lower), sub3(box->upper, box->lower)), (float)(ORC_MORTON_MAX + 1));
+    int cx = clampi(f2i_x86(q.x), 0, ORC_MORTON_MAX);
+    int cy = clampi(f2i_x86(q.y), 0, ORC_MORTON_MAX);
+    int cz = clampi(f2i_x86(q.z), 0, ORC_MORTON_MAX);
+    return orc_encode_morton((uint32_t)cx, (uint32_t)cy, (uint32_t)cz);
+}
+
+/* ------------------------------------------------------------------ build */
+static void aabb_set_empty(orc_aabb* b) /* minimum_lbvh.h:229-233 */
+{
+    b->lower = f3(ORC_FLT_MAX, ORC_FLT_MAX, ORC_FLT_MAX);
+    b->upper = f3(-ORC_FLT_MAX, -ORC_FLT_MAX, -ORC_FLT_MAX);
+}
+static void aabb_extend_p(orc_aabb* b, orc_f3 p) /* :234-238 */
+{
+    b->lower = min3(b->lower, p);
+    b->upper = max3(b->upper, p);
+}
+static void aabb_extend_b(orc_aabb* b, const orc_aabb* o) /* :240-244 */
+{
+    b->lower = min3(b->lower, o->lower);
+    b->upper = max3(b->upper, o->upper);
+}
+
+/* BVHCPUBuilder::build scene-AABB loop (minimum_lbvh.h:522-532). */
+void orc_scene_aabb(const orc_triangle* tris, uint32_t n, orc_aabb* out)
+{
+    orc_aabb s;
+    aabb_set_empty(&s);
+    for (uint32_t i = 0; i < n; i++)
+        for (int j = 0; j < 3; ++j) aabb_extend_p(&s, tris[i].v[j]);
+    *out = s;
+}
+
+/* Morton keys (minimum_lbvh.h:534-553; device twin minimum_lbvh.cu:68-92):
+ * centroid (v0 + v1 + v2) / 3, top 32 of the 63-bit code; with
+ * BUILD_OPTION_USE_NORMAL the low 6 bits are the normal's code. */
+void orc_morton_keys(const orc_triangle* tris, uint32_t n, uint32_t option,
+                     const orc_aabb* scene, uint32_t* keys)
+{
+    for (uint32_t i = 0; i < n; i++)
+    {
+        orc_triangle tri = tris[i];
+        orc_f3 center = divs(add3(add3(tri.v[0], tri.v[1]), tri.v[2]), 3.0f);
+        if (option & 1u)
+        {
+            orc_f3 ng = normalize3(cross3(sub3(tri.v[1], tri.v[0]), sub3(tri.v[2], tri.v[0])));
+            orc_aabb unit = {{-1, -1, -1}, {+1, +1, +1}};
+            uint32_t nMorton = (uint32_t)(orc_aabb_morton(&unit, ng) >> 31);
+            uint32_t pMorton = (uint32_t)(orc_aabb_morton(scene, center) >> 31);
+            keys[i] = (pMorton & 0xFFFFFFC0u) | (nMorton >> 26);
+        }
+        else
+        {
+            keys[i] = (uint32_t)(orc_aabb_morton(scene, center) >> 31);
+        }
+    }
+}
+
+/* Stable sort of (key, value) pairs by key: a four-pass LSD counting sort,
+ * i.e. the (morton, original index) order a stable sort of the reference's
+ * IndexedMorton array gives (minimum_lbvh.h:554 sorts with std::sort; the
+ * reference GPU path sorts the same array with a stable LSD radix sort,
+ * minimum_lbvh.h:833). */
+void orc_sort_pairs(uint32_t* keys, uint32_t* values, uint32_t n)
+{
+    uint32_t* k2 = (uint32_t*)malloc(sizeof(uint32_t) * (n ? n : 1));
+    uint32_t* v2 = (uint32_t*)malloc(sizeof(uint32_t) * (n ? n : 1));
+    uint32_t *ks = keys, *vs = values, *kd = k2, *vd = v2;
+    for (int pass = 0; pass < 4; ++pass)
+    {
+        uint32_t count[257];
+        memset(count, 0, sizeof(count));
+        int shift = pass * 8;
+        for (uint32_t i = 0; i < n; ++i) count[((ks[i] >> shift) & 255u) + 1]++;
+        for (int d = 0; d < 256; ++d) count[d + 1] += count[d];
+        for (uint32_t i = 0; i < n; ++i)
+        {
+            uint32_t d = (ks[i] >> shift) & 255u;
+            uint32_t o = count[d]++;
+            kd[o] = ks[i];
+            vd[o] = vs[i];
+        }
+        uint32_t* t = ks; ks = kd; kd = t;
+        t = vs; vs = vd; vd = t;
+    }
+    /* four passes: the result is back in the caller's arrays */
+    free(k2);
+    free(v2);
+}
+
+/* build_lbvh (minimum_lbvh.h:284-361): one walker per sorted leaf climbs
+ * bottom-up; at each step the parent is the internal node on the side with the
+ * smaller neighbouring delta (internal node i splits leaves i and i+1); the
+ * first walker to reach a parent leaves its range bound in `context` and stops,
+ * the second merges ranges and bounds and continues. Serial here: the result
+ * is the same for any walker order. */
+static void build_walk(uint32_t* rootNode, orc_node* internals, const orc_triangle* triangles,
+                       uint32_t nTriangles, const uint8_t* deltas, uint32_t i_leaf, uint32_t triangleIndex)
+{
+    uint32_t nInternals = nTriangles - 1;
+    uint32_t nDeltas = nInternals;
+    uint32_t leaf_lower = i_leaf, leaf_upper = i_leaf;
+    uint32_t node = triangleIndex | ORC_LEAF_BIT;
+
+    orc_aabb aabb;
+    aabb_set_empty(&aabb);
+    if (triangles)
+        for (int j = 0; j < 3; ++j) aabb_extend_p(&aabb, triangles[triangleIndex].v[j]);
+
+    int isRoot = 1;
+    while (leaf_upper - leaf_lower < nInternals)
+    {
+        uint32_t deltaL = 0 < leaf_lower ? deltas[leaf_lower - 1] : 0xFFFFFFFFu;
+        uint32_t deltaR = leaf_upper < nDeltas ? deltas[leaf_upper] : 0xFFFFFFFFu;
+        int goLeft = deltaL < deltaR ? 1 : 0;
+        uint32_t parent = goLeft ? (leaf_lower - 1) : leaf_upper;
+
+        internals[parent].children[goLeft] = node;
+        internals[parent].aabbs[goLeft] = aabb;
+        if (!(node & ORC_LEAF_BIT)) internals[node].parent = parent;
+
+        uint32_t index = goLeft ? leaf_upper : leaf_lower;
+        uint32_t old = internals[parent].context; /* the exchange (:330-336) */
+        internals[parent].context = index;
+        index = old;
+        if (index == 0xFFFFFFFFu)
+        {
+            isRoot = 0;
+            break;
+        }
+        leaf_lower = leaf_lower < index ? leaf_lower : index;
+        leaf_upper = leaf_upper < index ? index : leaf_upper;
+        internals[parent].context = leaf_upper < nInternals ? leaf_upper : 0xFFFFFFFFu;
+        node = parent;
+        orc_aabb other = internals[parent].aabbs[goLeft ^ 1];
+        aabb_extend_b(&aabb, &other);
+    }
+    if (isRoot)
+    {
+        *rootNode = node;
+        if (!(node & ORC_LEAF_BIT)) internals[node].parent = ORC_INVALID;
+    }
+}
+
+int orc_build_from_keys(const uint32_t* sorted_keys, const uint32_t* sorted_indices,
+                        const orc_triangle* tris, uint32_t n,
+                        orc_node* nodes, uint8_t* deltas, uint32_t* root)
+{
+    if (n == 0) return -1;
+    for (uint32_t i = 0; i + 1 < n; ++i)
+    {
+        memset(&nodes[i], 0, sizeof(orc_node));
+        nodes[i].context = 0xFFFFFFFFu; /* minimum_lbvh.h:514-519 */
+        deltas[i] = (uint8_t)orc_delta(sorted_keys[i], sorted_keys[i + 1]); /* :556-561 */
+    }
+    for (uint32_t i = 0; i < n; ++i)
+        build_walk(root, nodes, tris, n, deltas, i, sorted_indices[i]);
+    return 0;
+}
+
+/* BVHCPUBuilder::build (minimum_lbvh.h:512-592) with the stable key order. */
+int orc_build(const orc_triangle* tris, uint32_t n, uint32_t option,
+              orc_node* nodes, uint8_t* deltas, uint32_t* root,
+              uint32_t* keys_out, uint32_t* indices_out, orc_aabb* scene_out)
+{
+    if (n == 0) return -1;
+    orc_aabb scene;
+    orc_scene_aabb(tris, n, &scene);
+    uint32_t* keys = (uint32_t*)malloc(sizeof(uint32_t) * n);
+    uint32_t* idx = (uint32_t*)malloc(sizeof(uint32_t) * n);
+    orc_morton_keys(tris, n, option, &scene, keys);
+    for (uint32_t i = 0; i < n; ++i) idx[i] = i;
+    orc_sort_pairs(keys, idx, n);
+    int rc = orc_build_from_keys(keys, idx, tris, n, nodes, deltas, root);
+    if (keys_out) memcpy(keys_out, keys, sizeof(uint32_t) * n);
+    if (indices_out) memcpy(indices_out, idx, sizeof(uint32_t) * n);
+    if (scene_out) *scene_out = scene;
+    free(keys);
+    free(idx);
+    return rc;
+}
+
+/* validate_lbvh (minimum_lbvh.h:415-426), iterative; returns 1 when every
+ * child's split delta is <= its parent's. */
+int orc_validate(const orc_node* nodes, const uint8_t* deltas, uint32_t n, uint32_t root, int maxDelta)
+{
+    if (n <= 1) return 1;
+    uint32_t* stack = (uint32_t*)malloc(sizeof(uint32_t) * 2 * n);
+    int* limit = (int*)malloc(sizeof(int) * 2 * n);
+    size_t sp = 0;
+    int ok = 1;
+    stack[sp] = root;
+    limit[sp++] = maxDelta;
+    while (sp && ok)
+    {
+        --sp;
+        uint32_t node = stack[sp];
+        int lim = limit[sp];
+        if (node & ORC_LEAF_BIT) continue;
+        if (node >= n - 1) { ok = 0; break; }
+        int d = deltas[node];
+        if (d > lim) { ok = 0; break; }
+        for (int c = 0; c < 2; ++c)
+        {
+            stack[sp] = nodes[node].children[c];
+            limit[sp++] = d;
+        }
+    }
+    free(stack);
+    free(limit);
+    return ok;
+}
+
+/* Structural check: every leaf reached exactly once from the root, parent
+ * links consistent, each child's box inside its parent's, leaf boxes equal to
+ * their triangle's bounds. Returns 1 when all hold. */
+int orc_check_tree(const orc_node* nodes, const orc_triangle* tris, uint32_t n, uint32_t root)
+{
+    if (n == 1) return root == ORC_LEAF_BIT;
+    uint8_t* seen = (uint8_t*)calloc(n, 1);
+    uint32_t* stack = (uint32_t*)malloc(sizeof(uint32_t) * n);
+    size_t sp = 0;
+    int ok = (root & ORC_LEAF_BIT) == 0 && root < n - 1 && nodes[root].parent == ORC_INVALID;
+    uint32_t visited = 0;
+    if (ok) stack[sp++] = root;
+    while (sp && ok)
+    {
+        uint32_t node = stack[--sp];
+        visited++;
+        for (int c = 0; c < 2 && ok; ++c)
+        {
+            uint32_t ch = nodes[node].children[c];
+            const orc_aabb* b = &nodes[node].aabbs[c];
+            if (ch & ORC_LEAF_BIT)
+            {
+                uint32_t t = ch & ~ORC_LEAF_BIT;
+                if (t >= n || seen[t]) { ok = 0; break; }
+                seen[t] = 1;
+                orc_aabb tb;
+                aabb_set_empty(&tb);
+                for (int j = 0; j < 3; ++j) aabb_extend_p(&tb, tris[t].v[j]);
+                if (memcmp(&tb, b, sizeof(tb)) != 0) ok = 0;
+            }
+            else
+            {
+                if (ch >= n - 1 || nodes[ch].parent != node) { ok = 0; break; }
+                const orc_aabb* cb = &nodes[ch].aabbs[0];
+                const orc_aabb* cb1 = &nodes[ch].aabbs[1];
+                if (cb->lower.x < b->lower.x || cb->lower.y < b->lower.y || cb->lower.z < b->lower.z ||
+                    cb->upper.x > b->upper.x || cb->upper.y > b->upper.y || cb->upper.z > b->upper.z ||
+                    cb1->lower.x < b->lower.x || cb1->lower.y < b->lower.y || cb1->lower.z < b->lower.z ||
+                    cb1->upper.x > b->upper.x || cb1->upper.y > b->upper.y || cb1->upper.z > b->upper.z)
+                    ok = 0;
+                stack[sp++] = ch;
+            }
+        }
+    }
+    for (uint32_t i = 0; i < n && ok; ++i)
+        if (!seen[i]) ok = 0;
+    if (ok && visited != n - 1) ok = 0;
+    free(seen);
+    free(stack);
+    return ok;
+}
+
+/* ---------------------------------------------------------------- queries */
+/* slabs (minimum_lbvh.h:82-96): entry/exit of the ray against one box, the
+ * exit inflated by 1.00000024 (robust traversal), clipped to [0, knownHitT]. */
+static inline void slabs(orc_f3 ro, orc_f3 inv, const orc_aabb* b, float knownHitT, float* rmin, float* rmax)
+{
+    orc_f3 t0 = mul3(sub3(b->lower, ro), inv);
+    orc_f3 t1 = mul3(sub3(b->upper, ro), inv);
+    orc_f3 tmin = min3(t0, t1);
+    orc_f3 tmax = max3(t0, t1);
+    float region_min = compMax(tmin);
+    float region_max = compMin(tmax) * 1.00000024f;
+    region_min = smax(region_min, 0.0f);
+    region_max = smin(region_max, knownHitT);
+    *rmin = region_min;
+    *rmax = region_max;
+}
+
+/* intersectRayTriangle (minimum_lbvh.h:363-413). */
+static inline int intersect_tri(float* tOut, float* uOut, float* vOut, orc_f3* ngOut, float t_min, float t_max,
+                                orc_f3 ro, orc_f3 rd, orc_f3 v0, orc_f3 v1, orc_f3 v2)
+{
+    orc_f3 e0 = sub3(v1, v0);
+    orc_f3 e1 = sub3(v2, v1);
+    orc_f3 ng = cross3(e0, e1);
+    float t = dot3(sub3(v0, ro), ng) / dot3(ng, rd);
+    if (t_min <= t && t <= t_max)
+    {
+        orc_f3 e2 = sub3(v0, v2);
+        orc_f3 ro2 = muls(ro, 2.0f);
+        float u_vol = dot3(cross3(e2, sub3(add3(v0, v2), ro2)), rd);
+        float v_vol = dot3(cross3(e0, sub3(add3(v1, v0), ro2)), rd);
+        float w_vol = dot3(cross3(e1, sub3(add3(v2, v1), ro2)), rd);
+        if (smin(smin(u_vol, v_vol), w_vol) < 0.0f && 0.0f < smax(smax(u_vol, v_vol), w_vol)) return 0;
+        float vol = u_vol + v_vol + w_vol;
+        *tOut = t;
+        *uOut = u_vol / vol;
+        *vOut = v_vol / vol;
+        *ngOut = ng;
+        return 1;
+    }
+    return 0;
+}
+
+/* invRd (minimum_lbvh.h:898-901) */
+static inline orc_f3 inv_rd(orc_f3 rd)
+{
+    orc_f3 r = f3(1.0f / rd.x, 1.0f / rd.y, 1.0f / rd.z);
+    return f3(clampf(r.x, -ORC_FLT_MAX, ORC_FLT_MAX), clampf(r.y, -ORC_FLT_MAX, ORC_FLT_MAX),
+              clampf(r.z, -ORC_FLT_MAX, ORC_FLT_MAX));
+}
+
+static inline int is_leaf(uint32_t n) { return (n & ORC_LEAF_BIT) != 0; }
+static inline uint32_t idx_of(uint32_t n) { return n & ~ORC_LEAF_BIT; }
+
+static inline void leaf_test(orc_hit* hit, const orc_triangle* tris, uint32_t leaf, orc_f3 ro, orc_f3 rd,
+                             float tmin, int* hitOut, uint32_t* triTests)
+{
+    float t, u, v;
+    orc_f3 ng;
+    const orc_triangle* tri = &tris[idx_of(leaf)];
+    (*triTests)++;
+    *hitOut = 0;
+    if (intersect_tri(&t, &u, &v, &ng, tmin, hit->t, ro, rd, tri->v[0], tri->v[1], tri->v[2]))
+    {
+        hit->t = t;
+        hit->u = u;
+        hit->v = v;
+        hit->triangleIndex = idx_of(leaf);
+        hit->ng = ng;
+        *hitOut = 1;
+    }
+}
+
+/* intersect_stackfree (minimum_lbvh.h:981-1061): parent-pointer traversal.
+ * Coming from the parent, go to the near hit child (entry order, ties to the
+ * left) or back up; coming from the near child, go to the far child if both
+ * boxes are still hit, else up; coming from the far child, go up. */
+static void trace_stackfree(orc_hit* hit, const orc_node* nodes, const orc_triangle* tris, uint32_t root,
+                            orc_f3 ro, orc_f3 rd, orc_f3 inv, float tmin, int anyHit,
+                            uint32_t* nodeVisits, uint32_t* triTests)
+{
+    uint32_t curr = root, prev = ORC_INVALID;
+    while (curr != ORC_INVALID)
+    {
+        if (is_leaf(curr))
+        {
+            int h;
+            leaf_test(hit, tris, curr, ro, rd, tmin, &h, triTests);
+            if (h && anyHit) break;
+            uint32_t t = curr; curr = prev; prev = t;
+            continue;
+        }
+        (*nodeVisits)++;
+        const orc_node* nd = &nodes[curr];
+        float lmin, lmax, rmin, rmax;
+        slabs(ro, inv, &nd->aabbs[0], hit->t, &lmin, &lmax);
+        slabs(ro, inv, &nd->aabbs[1], hit->t, &rmin, &rmax);
+        lmin = smax(lmin, tmin);
+        rmin = smax(rmin, tmin);
+        int hitL = lmin <= lmax, hitR = rmin <= rmax;
+        uint32_t parent = nd->parent, near = nd->children[0], far = nd->children[1];
+        int nHits = 0;
+        if (hitL && hitR)
+        {
+            if (rmin < lmin) { uint32_t t = near; near = far; far = t; }
+            nHits = 2;
+        }
+        else if (hitL || hitR)
+        {
+            nHits = 1;
+            near = hitR ? far : near;
+        }
+        uint32_t next;
+        if (prev == parent) next = 0 < nHits ? near : parent;
+        else if (prev == near) next = nHits == 2 ? far : parent;
+        else next = parent;
+        prev = curr;
+        curr = next;
+    }
+}
+
+/* intersect_escape_link (minimum_lbvh.h:1063-1137): ropes through `context`
+ * (the index of the node covering the next leaf range). The reference reads
+ * nodes[prev] at a leaf; a leaf root (one triangle) is tested directly here. */
+static void trace_escape(orc_hit* hit, const orc_node* nodes, const orc_triangle* tris, uint32_t root,
+                         orc_f3 ro, orc_f3 rd, orc_f3 inv, float tmin, int anyHit,
+                         uint32_t* nodeVisits, uint32_t* triTests)
+{
+    if (is_leaf(root))
+    {
+        int h;
+        leaf_test(hit, tris, root, ro, rd, tmin, &h, triTests);
+        return;
+    }
+    uint32_t curr = root, prev = ORC_INVALID;
+    while (curr != ORC_INVALID)
+    {
+        if (is_leaf(curr))
+        {
+            int h;
+            leaf_test(hit, tris, curr, ro, rd, tmin, &h, triTests);
+            if (h && anyHit) break;
+            if (nodes[idx_of(prev)].children[0] == curr)
+            {
+                uint32_t t = curr; curr = prev; prev = t;
+                continue;
+            }
+            uint32_t ioi = nodes[idx_of(prev)].context;
+            uint32_t next = ioi != 0xFFFFFFFFu ? ioi : ORC_INVALID;
+            prev = curr;
+            curr = next;
+            continue;
+        }
+        (*nodeVisits)++;
+        const orc_node* nd = &nodes[curr];
+        uint32_t parent = nd->parent;
+        const orc_aabb* box;
+        uint32_t hitChild, miss;
+        if (prev == parent)
+        {
+            box = &nd->aabbs[0];
+            hitChild = nd->children[0];
+            miss = curr;
+        }
+        else
+        {
+            box = &nd->aabbs[1];
+            hitChild = nd->children[1];
+            uint32_t ioi = nd->context;
+            miss = ioi != 0xFFFFFFFFu ? ioi : ORC_INVALID;
+        }
+        float rmin, rmax;
+        slabs(ro, inv, box, hit->t, &rmin, &rmax);
+        rmin = smax(rmin, tmin);
+        uint32_t next = rmin <= rmax ? hitChild : miss;
+        prev = curr;
+        curr = next;
+    }
+}
+
+/* intersect_stackfull (minimum_lbvh.h:912-973): explicit stack, far child
+ * pushed. Closest hit only, as in the reference. */
+static void trace_stackfull(orc_hit* hit, const orc_node* nodes, const orc_triangle* tris, uint32_t root,
+                            orc_f3 ro, orc_f3 rd, orc_f3 inv, float tmin,
+                            uint32_t* nodeVisits, uint32_t* triTests)
+{
+    uint32_t stack[64];
+    int sp = 0;
+    uint32_t node = root;
+    while (node != ORC_INVALID)
+    {
+        if (is_leaf(node))
+        {
+            int h;
+            leaf_test(hit, tris, node, ro, rd, tmin, &h, triTests);
+            node = sp == 0 ? ORC_INVALID : stack[--sp];
+            continue;
+        }
+        (*nodeVisits)++;
+        const orc_node* nd = &nodes[node];
+        float lmin, lmax, rmin, rmax;
+        slabs(ro, inv, &nd->aabbs[0], hit->t, &lmin, &lmax);
+        slabs(ro, inv, &nd->aabbs[1], hit->t, &rmin, &rmax);
+        lmin = smax(lmin, tmin);
+        rmin = smax(rmin, tmin);
+        int hitL = lmin <= lmax, hitR = rmin <= rmax;
+        if (hitL && hitR)
+        {
+            uint32_t nearN = nd->children[0], farN = nd->children[1];
+            if (rmin < lmin) { uint32_t t = nearN; nearN = farN; farN = t; }
+            node = nearN;
+            if (sp < 64) stack[sp++] = farN;
+        }
+        else if (hitL || hitR)
+            node = nd->children[hitL ? 0 : 1];
+        else
+            node = sp == 0 ? ORC_INVALID : stack[--sp];
+    }
+}
+
+static inline void hit_init(orc_hit* h, float tmax)
+{
+    memset(h, 0, sizeof(*h));
+    h->t = tmax;
+    h->triangleIndex = 0xFFFFFFFFu;
+}
+
+typedef struct {
+    const orc_node* nodes;
+    const orc_triangle* tris;
+    uint32_t root;
+    const orc_ray* rays;
+    int query, mode;
+    orc_hit* hits;
+    uint32_t *nodeVisits, *triTests;
+} trace_ctx;
+
+static void trace_range(void* p, uint32_t b, uint32_t e)
+{
+    trace_ctx* c = (trace_ctx*)p;
+    for (uint32_t i = b; i < e; ++i)
+    {
+        const orc_ray* r = &c->rays[i];
+        orc_f3 ro = f3(r->ro[0], r->ro[1], r->ro[2]);
+        orc_f3 rd = f3(r->rd[0], r->rd[1], r->rd[2]);
+        orc_hit hit;
+        hit_init(&hit, r->tmax);
+        uint32_t nv = 0, nt = 0;
+        orc_f3 inv = inv_rd(rd);
+        if (c->mode == 1)
+            trace_escape(&hit, c->nodes, c->tris, c->root, ro, rd, inv, r->tmin, c->query == 1, &nv, &nt);
+        else if (c->mode == 2)
+            trace_stackfull(&hit, c->nodes, c->tris, c->root, ro, rd, inv, r->tmin, &nv, &nt);
+        else
+            trace_stackfree(&hit, c->nodes, c->tris, c->root, ro, rd, inv, r->tmin, c->query == 1, &nv, &nt);
+        c->hits[i] = hit;
+        if (c->nodeVisits) c->nodeVisits[i] = nv;
+        if (c->triTests) c->triTests[i] = nt;
+    }
+}
+
+void orc_trace(const orc_node* nodes, const orc_triangle* tris, uint32_t root,
+               const orc_ray* rays, uint32_t nRays, int query, int mode,
+               orc_hit* hits, uint32_t* nodeVisits, uint32_t* triTests)
+{
+    trace_ctx c = {nodes, tris, root, rays, query, mode, hits, nodeVisits, triTests};
+    orc_parallel_for(nRays, 1024, trace_range, &c);
+}
+
+/* ----------------------------------------------------------------- camera */
+/* RayGenerator::lookat (camera.h:10-22) */
+void orc_lookat(orc_f3 eye, orc_f3 center, orc_f3 up, float fovy, int w, int h, orc_camera* cam)
+{
+    orc_f3 f = normalize3(sub3(center, eye));
+    orc_f3 s = normalize3(cross3(f, up));
+    orc_f3 u = cross3(s, f);
+    float tanThetaY = tanf(fovy * 0.5f);
+    float tanThetaX = tanThetaY / (float)h * (float)w;
+    cam->origin = eye;
+    cam->right = muls(s, tanThetaX);
+    cam->up = muls(u, tanThetaY);
+}
+
+/* RayGenerator::shoot (camera.h:24-31) */
+void orc_shoot(const orc_camera* cam, float u, float v, orc_f3* ro, orc_f3* rd)
+{
+    orc_f3 from = cam->origin;
+    orc_f3 forward = normalize3(cross3(cam->up, cam->right));
+    orc_f3 to = add3(add3(add3(cam->origin, forward), lerp3(neg3(cam->right), cam->right, u)),
+                     lerp3(cam->up, neg3(cam->up), v));
+    *ro = from;
+    *rd = sub3(to, from);
+}
+
+/* ---------------------------------------------------------------- samples */
+static inline uint32_t reverse_bits(uint32_t v) /* sobol.h:18-30 */
+{
+    v = ((v >> 1) & 0x55555555u) | ((v & 0x55555555u) << 1);
+    v = ((v >> 2) & 0x33333333u) | ((v & 0x33333333u) << 2);
+    v = ((v >> 4) & 0x0F0F0F0Fu) | ((v & 0x0F0F0F0Fu) << 4);
+    v = ((v >> 8) & 0x00FF00FFu) | ((v & 0x00FF00FFu) << 8);
+    return (v >> 16) | (v << 16);
+}
+/* Laine-Karras style hash permutation (sobol.h:31-39, "Practical Hash-based
+ * Owen Scrambling", JCGT 2020). */
+static inline uint32_t lk_permutation(uint32_t x, uint32_t seed)
+{
+    x += seed;
+    x ^= x * 0x6c50b47cu;
+    x ^= x * 0xb82f1e52u;
+    x ^= x * 0xc7afe638u;
+    x ^= x * 0x8d22f6e6u;
+    return x;
+}
+static inline uint32_t nested_uniform_scramble(uint32_t x, uint32_t seed) /* sobol.h:40-46 */
+{
+    return reverse_bits(lk_permutation(reverse_bits(x), seed));
+}
+/* Pascal-matrix product giving Sobol's second dimension (sobol.h:51-59). */
+static inline uint32_t pascal(uint32_t v)
+{
+    v ^= v << 16;
+    v ^= (v & 0x00FF00FFu) << 8;
+    v ^= (v & 0x0F0F0F0Fu) << 4;
+    v ^= (v & 0x33333333u) << 2;
+    v ^= (v & 0x55555555u) << 1;
+    return v;
+}
+static inline float random_float(uint32_t u) /* sobol.h:62-72: top 24 bits / 2^24 */
+{
+    return (float)(u >> 8) / (float)((0xFFFFFFFFu >> 8) + 1);
+}
+uint32_t orc_hash_pcg(uint32_t v) /* sobol.h:76-81, minimum_lbvh.h:904-909 */
+{
+    uint32_t state = v * 747796405u + 2891336453u;
+    uint32_t word = ((state >> ((state >> 28) + 4)) ^ state) * 277803737u;
+    return (word >> 22) ^ word;
+}
+static inline void pcg3d(uint32_t* x, uint32_t* y, uint32_t* z) /* sobol.h:83-107 */
+{
+    uint32_t vx = *x * 1664525u + 1013904223u;
+    uint32_t vy = *y * 1664525u + 1013904223u;
+    uint32_t vz = *z * 1664525u + 1013904223u;
+    vx += vy * vz;
+    vy += vz * vx;
+    vz += vx * vy;
+    vx ^= vx >> 16;
+    vy ^= vy >> 16;
+    vz ^= vz >> 16;
+    vx += vy * vz;
+    vy += vz * vx;
+    vz += vx * vy;
+    *x = vx;
+    *y = vy;
+    *z = vz;
+}
+/* shuffled_scrambled_sobol_2d (sobol.h:119-129) */
+void orc_sobol(uint32_t index, uint32_t p0, uint32_t p1, uint32_t p2, float* x, float* y)
+{
+    pcg3d(&p0, &p1, &p2);
+    uint32_t v = lk_permutation(reverse_bits(index), p0);
+    *x = random_float(nested_uniform_scramble(v, p1));
+    *y = random_float(nested_uniform_scramble(pascal(v), p2));
+}
+
+/* PCG32 (main_gpu.cu:51-82, the pcg-random.org minimal generator). */
+typedef struct { uint64_t state, inc; } orc_pcg;
+static inline uint32_t pcg_next(orc_pcg* r)
+{
+    uint64_t old = r->state;
+    r->state = old * 6364136223846793005ULL + r->inc;
+    uint32_t xorshifted = (uint32_t)(((old >> 18u) ^ old) >> 27u);
+    uint32_t rot = (uint32_t)(old >> 59u);
+    return (xorshifted >> rot) | (xorshifted << ((-rot) & 31));
+}
+static inline void pcg_init(orc_pcg* r, uint64_t seed, uint64_t seq)
+{
+    r->state = 0;
+    r->inc = (seq << 1u) | 1u;
+    pcg_next(r);
+    r->state += seed;
+    pcg_next(r);
+}
+static inline float pcg_float(orc_pcg* r)
+{
+    uint32_t bits = (pcg_next(r) >> 9) | 0x3f800000u;
+    float v;
+    memcpy(&v, &bits, 4);
+    return v - 1.0f;
+}
+
+/* The project's portable FP32 sincos (shared formula with the CUDA kernels):
+ * Cody-Waite reduction by pi/2 split in three float parts, then the Taylor
+ * polynomials of sin (to r^9) and cos (to r^10) on [-pi/4, pi/4], evaluated
+ * with fused multiply-adds so that host and device round identically. */
+#define ORC_PIO2_HI 1.57079637050628662109375f
+#define ORC_PIO2_MID -4.371138828673792886547744274139404296875e-8f
+#define ORC_PIO2_LO -1.71512451000588187280393448475e-15f
+void orc_sincos(float phi, float* s, float* c)
+{
+    float k = rintf(phi * 0.636619772367581343f);
+    float r = fmaf(-k, ORC_PIO2_HI, phi);
+    r = fmaf(-k, ORC_PIO2_MID, r);
+    r = fmaf(-k, ORC_PIO2_LO, r);
+    float r2 = r * r;
+    float ps = fmaf(r2, (float)(1.0 / 362880.0), (float)(-1.0 / 5040.0));
+    ps = fmaf(ps, r2, (float)(1.0 / 120.0));
+    ps = fmaf(ps, r2, (float)(-1.0 / 6.0));
+    float sr = fmaf(ps * r2, r, r);
+    float pc = fmaf(r2, (float)(-1.0 / 3628800.0), (float)(1.0 / 40320.0));
+    pc = fmaf(pc, r2, (float)(-1.0 / 720.0));
+    pc = fmaf(pc, r2, (float)(1.0 / 24.0));
+    pc = fmaf(pc, r2, -0.5f);
+    float cr = fmaf(pc, r2, 1.0f);
+    int q = ((int)k) & 3;
+    if (q == 0) { *s = sr; *c = cr; }
+    else if (q == 1) { *s = cr; *c = -sr; }
+    else if (q == 2) { *s = -sr; *c = -cr; }
+    else { *s = -cr; *c = sr; }
+}
+
+#define ORC_PI 3.14159265358979323846f
+/* sampleHemisphereCosWeighted (main_gpu.cu:24-36) */
+static inline orc_f3 sample_hemisphere(float xi0, float xi1, int trig)
+{
+    float phi = xi0 * 2.0f * ORC_PI;
+    float r = sqrtf(xi1);
+    float sp, cp;
+    if (trig == ORC_TRIG_LIBM) { cp = cosf(phi); sp = sinf(phi); }
+    else orc_sincos(phi, &sp, &cp);
+    float x = cp * r;
+    float z = sp * r;
+    float y = sqrtf(fmaxf(1.0f - r * r, 0.0f));
+    return f3(x, y, z);
+}
+/* GetOrthonormalBasis (main_gpu.cu:39-45; Duff et al. 2017) */
+static inline void onb(orc_f3 z, orc_f3* xaxis, orc_f3* yaxis)
+{
+    const float sign = copysignf(1.0f, z.z);
+    const float a = -1.0f / (sign + z.z);
+    const float b = z.x * z.y * a;
+    *xaxis = f3(1.0f + sign * z.x * z.x * a, sign * b, -sign * z.x);
+    *yaxis = f3(b, sign + z.y * z.y * a, -z.y);
+}
+/* packRGBA (main_gpu.cu:17-22): (int)(c * 255 + 0.5) clamped, alpha not stored */
+static inline uint32_t pack_rgba(float r, float g, float b, float a)
+{
+    int x = clampi(f2i_x86(r * 255.0f + 0.5f), 0, 255);
+    int y = clampi(f2i_x86(g * 255.0f + 0.5f), 0, 255);
+    int z = clampi(f2i_x86(b * 255.0f + 0.5f), 0, 255);
+    (void)a;
+    return ((uint32_t)z << 16) | ((uint32_t)y << 8) | (uint32_t)x;
+}
+
+/* -------------------------------------------------------------------- AO */
+typedef struct {
+    uint32_t *pixels, *occluded;
+    int w, h;
+    const orc_camera* cam;
+    uint32_t root;
+    const orc_node* nodes;
+    const orc_triangle* tris;
+    int useSobol, nSamples;
+    float radius;
+    uint32_t seed;
+    int trig, rowBegin;
+    uint64_t* counters;
+} ao_ctx;
+
+/* ao (main_gpu.cu:111-177), per pixel, with nSample, ray length and the
+ * Sobol p2 seed as parameters (the reference fixes 16, 1.0 and 12345). */
+static void ao_rows(void* p, uint32_t b, uint32_t e)
+{
+    ao_ctx* c = (ao_ctx*)p;
+    uint64_t visits = 0, tests = 0, rays = 0;
+    for (uint32_t row = b; row < e; ++row)
+    {
+        int yi = c->rowBegin + (int)row;
+        for (int xi = 0; xi < c->w; ++xi)
+        {
+            int pixel = xi + yi * c->w;
+            orc_f3 ro, rd;
+            orc_shoot(c->cam, (float)xi / (float)c->w, (float)yi / (float)c->h, &ro, &rd);
+            orc_hit hit;
+            hit_init(&hit, ORC_FLT_MAX);
+            uint32_t nv = 0, nt = 0;
+            trace_stackfree(&hit, c->nodes, c->tris, c->root, ro, rd, inv_rd(rd), 0.0f, 0, &nv, &nt);
+            rays++;
+            if (hit.t == ORC_FLT_MAX)
+            {
+                if (c->pixels) c->pixels[pixel] = pack_rgba(0, 0, 0, 1);
+                if (c->occluded) c->occluded[pixel] = 0xFFFFFFFFu;
+                visits += nv;
+                tests += nt;
+                continue;
+            }
+            orc_f3 n = normalize3(hit.ng);
+            if (0.0f < dot3(n, rd)) n = neg3(n);
+            orc_f3 xaxis, zaxis;
+            onb(n, &xaxis, &zaxis);
+            orc_f3 ao_origin = add3(add3(ro, muls(rd, hit.t)), muls(n, 0.001f));
+            orc_pcg rng;
+            pcg_init(&rng, orc_hash_pcg((uint32_t)pixel), 0);
+            float ao = 0.0f;
+            uint32_t count = 0;
+            for (int i = 0; i < c->nSamples; i++)
+            {
+                float rx, ry;
+                if (c->useSobol == 1) orc_sobol((uint32_t)i, (uint32_t)xi, (uint32_t)yi, c->seed, &rx, &ry);
+                else if (c->useSobol == 2) { ry = pcg_float(&rng); rx = pcg_float(&rng); }
+                else { rx = pcg_float(&rng); ry = pcg_float(&rng); }
+                orc_f3 dl = sample_hemisphere(rx, ry, c->trig);
+                orc_f3 dir = add3(add3(muls(xaxis, dl.x), muls(zaxis, dl.z)), muls(n, dl.y));
+                orc_hit h2;
+                hit_init(&h2, c->radius);
+                trace_stackfree(&h2, c->nodes, c->tris, c->root, ao_origin, dir, inv_rd(dir), 0.0f, 1, &nv, &nt);
+                rays++;
+                if (h2.t != c->radius)
+                {
+                    ao += 1.0f / (float)c->nSamples;
+                    count++;
+                }
+            }
+            visits += nv;
+            tests += nt;
+            float brightness = powf(1.0f - ao, 1.0f / 2.2f);
+            if (c->pixels) c->pixels[pixel] = pack_rgba(brightness, brightness, brightness, 1.0f);
+            if (c->occluded) c->occluded[pixel] = count;
+        }
+    }
+    if (c->counters)
+    {
+        __atomic_fetch_add(&c->counters[0], visits, __ATOMIC_RELAXED);
+        __atomic_fetch_add(&c->counters[1], tests, __ATOMIC_RELAXED);
+        __atomic_fetch_add(&c->counters[2], rays, __ATOMIC_RELAXED);
+    }
+}
+
+void orc_render_ao(uint32_t* pixels, uint32_t* occluded, int w, int h, const orc_camera* cam,
+                   uint32_t root, const orc_node* nodes, const orc_triangle* tris,
+                   int useSobol, int nSamples, float radius, uint32_t seed, int trig,
+                   int rowBegin, int rowEnd, uint64_t* counters)
+{
+    if (rowEnd <= 0 || rowEnd > h) rowEnd = h;
+    if (rowBegin < 0) rowBegin = 0;
+    if (rowEnd <= rowBegin) return;
+    ao_ctx c = {pixels, occluded, w, h, cam, root, nodes, tris, useSobol, nSamples, radius, seed, trig, rowBegin, counters};
+    orc_parallel_for((uint32_t)(rowEnd - rowBegin), 1, ao_rows, &c);
+}
+
+/* ---------------------------------------------------------------- normal */
+typedef struct {
+    uint32_t* pixels;
+    int w, h;
+    const orc_camera* cam;
+    uint32_t root;
+    const orc_node* nodes;
+    const orc_triangle* tris;
+} normal_ctx;
+
+/* normal (main_gpu.cu:84-109) */
+static void normal_rows(void* p, uint32_t b, uint32_t e)
+{
+    normal_ctx* c = (normal_ctx*)p;
+    for (uint32_t yi = b; yi < e; ++yi)
+        for (int xi = 0; xi < c->w; ++xi)
+        {
+            int pixel = xi + (int)yi * c->w;
+            orc_f3 ro, rd;
+            orc_shoot(c->cam, (float)xi / (float)c->w, (float)yi / (float)c->h, &ro, &rd);
+            orc_hit hit;
+            hit_init(&hit, ORC_FLT_MAX);
+            uint32_t nv = 0, nt = 0;
+            trace_stackfree(&hit, c->nodes, c->tris, c->root, ro, rd, inv_rd(rd), 0.0f, 0, &nv, &nt);
+            if (hit.t != ORC_FLT_MAX)
+            {
+                orc_f3 n = normalize3(hit.ng);
+                orc_f3 col = muls(add3(n, f3(1.0f, 1.0f, 1.0f)), 0.5f);
+                c->pixels[pixel] = pack_rgba(col.x, col.y, col.z, 1.0f);
+            }
+            else
+                c->pixels[pixel] = pack_rgba(0, 0, 0, 1);
+        }
+}
+
+void orc_render_normal(uint32_t* pixels, int w, int h, const orc_camera* cam, uint32_t root,
+                       const orc_node* nodes, const orc_triangle* tris)
+{
+    normal_ctx c = {pixels, w, h, cam, root, nodes, tris};
+    orc_parallel_for((uint32_t)h, 1, normal_rows, &c);
+}
+
+/* -------------------------------------------------------------------- PT */
+typedef struct {
+    float* accum4;
+    int w, h;
+    const orc_camera* cam;
+    uint32_t root;
+    const orc_node* nodes;
+    const orc_triangle* tris;
+    const float* attribs;
+    int useSobol, maxSPP, maxDepth, trig;
+} pt_ctx;
+
+typedef struct {
+    int useSobol, iteration, xi, yi, dimLevel;
+    orc_pcg rng;
+} pt_random;
+
+static inline void pt_next(pt_random* r, float* x, float* y)
+{
+    if (r->useSobol == 1)
+        orc_sobol((uint32_t)r->iteration, (uint32_t)r->xi, (uint32_t)r->yi, (uint32_t)(r->dimLevel++), x, y);
+    else if (r->useSobol == 2)
+    {
+        *y = pcg_float(&r->rng);
+        *x = pcg_float(&r->rng);
+    }
+    else
+    {
+        *x = pcg_float(&r->rng);
+        *y = pcg_float(&r->rng);
+    }
+}
+
+/* pt (main_gpu.cu:179-272): one sample per pixel, emission accumulated along
+ * a cosine-sampled path, Russian roulette against max(throughput)/0.25. */
+static void pt_rows(void* p, uint32_t b, uint32_t e)
+{
+    pt_ctx* c = (pt_ctx*)p;
+    for (uint32_t yrow = b; yrow < e; ++yrow)
+        for (int xi = 0; xi < c->w; ++xi)
+        {
+            int yi = (int)yrow;
+            int pixel = xi + yi * c->w;
+            float* acc = c->accum4 + 4 * (size_t)pixel;
+            int iteration = (int)acc[3];
+            pt_random rr;
+            rr.useSobol = c->useSobol;
+            rr.iteration = iteration;
+            rr.xi = xi;
+            rr.yi = yi;
+            rr.dimLevel = 0;
+            pcg_init(&rr.rng, orc_hash_pcg(orc_hash_pcg((uint32_t)pixel) + (uint32_t)iteration), 0);
+            float rx, ry;
+            pt_next(&rr, &rx, &ry);
+            orc_f3 ro, rd;
+            orc_shoot(c->cam, ((float)xi + rx) / (float)c->w, ((float)yi + ry) / (float)c->h, &ro, &rd);
+            orc_f3 color = f3(0, 0, 0);
+            orc_f3 throughput = f3(1, 1, 1);
+            orc_hit hit;
+            hit_init(&hit, ORC_FLT_MAX);
+            uint32_t nv = 0, nt = 0;
+            trace_stackfree(&hit, c->nodes, c->tris, c->root, ro, rd, inv_rd(rd), 0.0f, 0, &nv, &nt);
+            if (hit.t != ORC_FLT_MAX)
+                for (int depth = 0; depth < c->maxDepth; depth++)
+                {
+                    float r0, r1;
+                    pt_next(&rr, &r0, &r1);
+                    orc_f3 hit_p = add3(ro, muls(rd, hit.t));
+                    orc_f3 hit_n = normalize3(hit.ng);
+                    if (0.0f < dot3(hit_n, rd)) hit_n = neg3(hit_n);
+                    const float* at = c->attribs + 15 * (size_t)hit.triangleIndex;
+                    orc_f3 refl = f3(at[9], at[10], at[11]);
+                    orc_f3 emis = f3(at[12], at[13], at[14]);
+                    color = add3(color, mul3(throughput, emis));
+                    orc_f3 xaxis, zaxis;
+                    onb(hit_n, &xaxis, &zaxis);
+                    orc_f3 dl = sample_hemisphere(r0, r1, c->trig);
+                    orc_f3 next_ro = add3(hit_p, muls(hit_n, 0.0001f));
+                    orc_f3 next_rd = add3(add3(muls(xaxis, dl.x), muls(zaxis, dl.z)), muls(hit_n, dl.y));
+                    throughput = mul3(throughput, refl);
+                    const float rrThreshold = 0.25f;
+                    float maxComp = smax(smax(throughput.x, throughput.y), throughput.z);
+                    float pr = smin(maxComp / rrThreshold, 1.0f);
+                    float q0, q1;
+                    pt_next(&rr, &q0, &q1);
+                    if (pr < q0) break;
+                    throughput = divs(throughput, pr);
+                    hit_init(&hit, ORC_FLT_MAX);
+                    trace_stackfree(&hit, c->nodes, c->tris, c->root, next_ro, next_rd, inv_rd(next_rd), 0.0f, 0,
+                                    &nv, &nt);
+                    if (hit.t == ORC_FLT_MAX) break;
+                    ro = next_ro;
+                    rd = next_rd;
+                }
+            if (iteration < c->maxSPP)
+            {
+                acc[0] += color.x;
+                acc[1] += color.y;
+                acc[2] += color.z;
+                acc[3] += 1.0f;
+            }
+        }
+}
+
+void orc_render_pt(float* accum4, int w, int h, const orc_camera* cam, uint32_t root,
+                   const orc_node* nodes, const orc_triangle* tris, const float* attribs15,
+                   int useSobol, int maxSPP, int maxDepth, int trig)
+{
+    pt_ctx c = {accum4, w, h, cam, root, nodes, tris, attribs15, useSobol, maxSPP, maxDepth, trig};
+    orc_parallel_for((uint32_t)h, 1, pt_rows, &c);
+}
+
+/* pack (main_gpu.cu:273-286) */
+void orc_pack(uint32_t* pixels, const float* accum4, int n)
+{
+    for (int i = 0; i < n; ++i)
+    {
+        const float* a = accum4 + 4 * (size_t)i;
+        pixels[i] = pack_rgba(powf(a[0] / a[3], 1.0f / 2.2f), powf(a[1] / a[3], 1.0f / 2.2f),
+                              powf(a[2] / a[3], 1.0f / 2.2f), 1.0f);
+    }
+}

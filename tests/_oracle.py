@@ -1,0 +1,223 @@
+"""ctypes access to the checkers: oracle/liboracle.so (the restatement) and
+oracle/_ref/libmlbvh_ref.so (the reference's own CPU code, when built).
+
+Test infrastructure only. Builds liboracle.so with gcc on first use if it is
+missing (gcc is the only requirement); the reference library cannot be
+rebuilt without the reference sources and is optional.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+ORACLE_DIR = os.path.join(ROOT, "oracle")
+ORACLE_LIB = os.path.join(ORACLE_DIR, "liboracle.so")
+REF_LIB = os.path.join(ORACLE_DIR, "_ref", "libmlbvh_ref.so")
+
+_vp = ctypes.c_void_p
+_u32, _i32, _f32, _u64 = ctypes.c_uint32, ctypes.c_int, ctypes.c_float, ctypes.c_uint64
+
+FLT_MAX = np.float32(3.402823466e38)
+LEAF = 0x80000000
+INVALID = 0x7FFFFFFF
+
+
+class F3(ctypes.Structure):
+    _fields_ = [("x", ctypes.c_float), ("y", ctypes.c_float), ("z", ctypes.c_float)]
+
+
+def P(a):
+    return None if a is None else a.ctypes.data_as(_vp)
+
+
+_oracle = None
+_ref = None
+
+
+def oracle() -> ctypes.CDLL:
+    global _oracle
+    if _oracle is None:
+        src = os.path.join(ORACLE_DIR, "mlbvh_oracle.c")
+        if not os.path.exists(ORACLE_LIB) or os.path.getmtime(ORACLE_LIB) < os.path.getmtime(src):
+            subprocess.run(["make", "-C", ORACLE_DIR, "liboracle.so"], check=True, capture_output=True)
+        L = ctypes.CDLL(ORACLE_LIB)
+        sig = {
+            "orc_version": (_i32, []),
+            "orc_set_threads": (None, [_i32]),
+            "orc_clz": (_i32, [_u32]), "orc_clz64": (_i32, [_u64]), "orc_ffs": (_i32, [_u32]),
+            "orc_ffs64": (_i32, [_u64]), "orc_delta": (_i32, [_u32, _u32]),
+            "orc_splat3": (_u64, [_u32]), "orc_compact3": (_u32, [_u64]),
+            "orc_encode_morton": (_u64, [_u32, _u32, _u32]), "orc_encode_morton_naive": (_u64, [_u32, _u32, _u32]),
+            "orc_decode_morton": (None, [_u64, _vp, _vp, _vp]),
+            "orc_scene_aabb": (None, [_vp, _u32, _vp]),
+            "orc_morton_keys": (None, [_vp, _u32, _u32, _vp, _vp]),
+            "orc_sort_pairs": (None, [_vp, _vp, _u32]),
+            "orc_build": (_i32, [_vp, _u32, _u32, _vp, _vp, _vp, _vp, _vp, _vp]),
+            "orc_build_from_keys": (_i32, [_vp, _vp, _vp, _u32, _vp, _vp, _vp]),
+            "orc_validate": (_i32, [_vp, _vp, _u32, _u32, _i32]),
+            "orc_check_tree": (_i32, [_vp, _vp, _u32, _u32]),
+            "orc_trace": (None, [_vp, _vp, _u32, _vp, _u32, _i32, _i32, _vp, _vp, _vp]),
+            "orc_lookat": (None, [F3, F3, F3, _f32, _i32, _i32, _vp]),
+            "orc_sobol": (None, [_u32, _u32, _u32, _u32, _vp, _vp]),
+            "orc_hash_pcg": (_u32, [_u32]),
+            "orc_sincos": (None, [_f32, _vp, _vp]),
+            "orc_render_ao": (None, [_vp, _vp, _i32, _i32, _vp, _u32, _vp, _vp, _i32, _i32, _f32, _u32, _i32,
+                                     _i32, _i32, _vp]),
+            "orc_render_pt": (None, [_vp, _i32, _i32, _vp, _u32, _vp, _vp, _vp, _i32, _i32, _i32, _i32]),
+            "orc_pack": (None, [_vp, _vp, _i32]),
+            "orc_render_normal": (None, [_vp, _i32, _i32, _vp, _u32, _vp, _vp]),
+        }
+        for name, (res, args) in sig.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _oracle = L
+    return _oracle
+
+
+def ref_available() -> bool:
+    return os.path.exists(REF_LIB)
+
+
+def ref() -> ctypes.CDLL:
+    global _ref
+    if _ref is None:
+        L = ctypes.CDLL(REF_LIB)
+        sig = {
+            "ref_version": (_i32, []), "ref_threads": (_i32, []),
+            "ref_cpu_builder": (None, [_vp, _i32, _u32, _vp, _vp, _vp]),
+            "ref_build_stable": (None, [_vp, _i32, _u32, _vp, _vp, _vp, _vp, _vp, _vp, _i32]),
+            "ref_toy_tree": (None, [_vp, _i32, _vp, _vp, _vp]),
+            "ref_trace": (None, [_vp, _vp, _u32, _vp, _i32, _i32, _i32, _vp]),
+            "ref_lookat": (None, [_vp, _vp, _vp, _f32, _i32, _i32, _vp]),
+            "ref_shoot": (None, [_vp, _i32, _i32, _i32, _i32, _vp, _vp]),
+            "ref_ao": (None, [_vp, _i32, _i32, _vp, _u32, _vp, _vp, _i32]),
+            "ref_ao_param": (None, [_vp, _i32, _i32, _vp, _u32, _vp, _vp, _i32, _f32, _u32, _i32, _i32, _vp]),
+            "ref_normal": (None, [_vp, _i32, _i32, _vp, _u32, _vp, _vp]),
+            "ref_pt": (None, [_vp, _vp, _i32, _i32, _vp, _u32, _vp, _vp, _vp, _i32, _i32]),
+            "ref_pack": (None, [_vp, _vp, _i32]),
+            "ref_sobol": (None, [_u32, _u32, _u32, _u32, _vp]),
+            "ref_splat3": (_u64, [_u32]), "ref_compact3": (_u32, [_u64]),
+            "ref_encode_morton": (_u64, [_u32, _u32, _u32]), "ref_encode_morton_naive": (_u64, [_u32, _u32, _u32]),
+            "ref_clz": (_i32, [_u32]), "ref_clz64": (_i32, [_u64]), "ref_ffs": (_i32, [_u32]),
+            "ref_ffs64": (_i32, [_u64]), "ref_hash_pcg": (_u32, [_u32]),
+            "ref_aabb_morton": (_u64, [_vp, _vp, _vp]),
+        }
+        for name, (res, args) in sig.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _ref = L
+    return _ref
+
+
+# ------------------------------------------------------------ oracle wrappers
+def build(tris: np.ndarray, option: int = 0):
+    """Oracle build: dict of nodes (n-1, 16) u32, deltas, root, keys, indices, scene."""
+    tris = np.ascontiguousarray(tris, np.float32).reshape(-1, 9)
+    n = tris.shape[0]
+    nodes = np.zeros((max(n - 1, 1), 16), np.uint32)
+    deltas = np.zeros(max(n - 1, 1), np.uint8)
+    root = np.zeros(1, np.uint32)
+    keys = np.zeros(n, np.uint32)
+    idx = np.zeros(n, np.uint32)
+    scene = np.zeros(6, np.float32)
+    rc = oracle().orc_build(P(tris), n, option, P(nodes), P(deltas), P(root), P(keys), P(idx), P(scene))
+    assert rc == 0
+    return dict(nodes=nodes[: n - 1], deltas=deltas[: n - 1], root=int(root[0]), keys=keys, indices=idx, scene=scene)
+
+
+def ref_build(tris: np.ndarray, option: int = 0, parallel: int = 0):
+    tris = np.ascontiguousarray(tris, np.float32).reshape(-1, 9)
+    n = tris.shape[0]
+    nodes = np.zeros((max(n - 1, 1), 16), np.uint32)
+    deltas = np.zeros(max(n - 1, 1), np.uint8)
+    root = np.zeros(1, np.uint32)
+    keys = np.zeros(n, np.uint32)
+    idx = np.zeros(n, np.uint32)
+    scene = np.zeros(6, np.float32)
+    ref().ref_build_stable(P(tris), n, option, P(nodes), P(deltas), P(root), P(keys), P(idx), P(scene), parallel)
+    return dict(nodes=nodes[: n - 1], deltas=deltas[: n - 1], root=int(root[0]), keys=keys, indices=idx, scene=scene)
+
+
+def trace(nodes, tris, root, rays, query=0, mode=0, counters=False):
+    rays = np.ascontiguousarray(rays, np.float32).reshape(-1, 8)
+    n = rays.shape[0]
+    hits = np.zeros((n, 8), np.uint32)
+    nv = np.zeros(n, np.uint32) if counters else None
+    nt = np.zeros(n, np.uint32) if counters else None
+    nodes_c = np.ascontiguousarray(nodes, np.uint32) if len(nodes) else np.zeros((1, 16), np.uint32)
+    oracle().orc_trace(P(nodes_c), P(np.ascontiguousarray(tris, np.float32)), root, P(rays), n, query, mode,
+                       P(hits), P(nv), P(nt))
+    if counters:
+        return hits, nv, nt
+    return hits
+
+
+def ref_trace(nodes, tris, root, rays, query=0, mode=0):
+    rays = np.ascontiguousarray(rays, np.float32).reshape(-1, 8)
+    n = rays.shape[0]
+    hits = np.zeros((n, 8), np.uint32)
+    nodes_c = np.ascontiguousarray(nodes, np.uint32) if len(nodes) else np.zeros((1, 16), np.uint32)
+    ref().ref_trace(P(nodes_c), P(np.ascontiguousarray(tris, np.float32)), root, P(rays), n, query, mode, P(hits))
+    return hits
+
+
+def lookat(eye, center, up, fovy, w, h) -> np.ndarray:
+    cam = np.zeros(9, np.float32)
+    oracle().orc_lookat(F3(*eye), F3(*center), F3(*up), float(fovy), w, h, P(cam))
+    return cam
+
+
+def render_ao(cam, root, nodes, tris, w, h, n_samples=16, radius=1.0, seed=12345, use_sobol=1, trig=1,
+              rows=None, counters=False):
+    pixels = np.zeros(w * h, np.uint32)
+    occ = np.zeros(w * h, np.uint32)
+    cnt = np.zeros(3, np.uint64)
+    rb, re = (0, h) if rows is None else rows
+    nodes_c = np.ascontiguousarray(nodes, np.uint32) if len(nodes) else np.zeros((1, 16), np.uint32)
+    oracle().orc_render_ao(P(pixels), P(occ), w, h, P(np.ascontiguousarray(cam, np.float32)), root, P(nodes_c),
+                           P(np.ascontiguousarray(tris, np.float32)), use_sobol, n_samples, float(radius), seed,
+                           trig, rb, re, P(cnt))
+    if counters:
+        return pixels, occ, cnt
+    return pixels, occ
+
+
+def ref_ao(cam, root, nodes, tris, w, h, use_sobol=1):
+    pixels = np.zeros(w * h, np.uint32)
+    ref().ref_ao(P(pixels), w, h, P(np.ascontiguousarray(cam, np.float32)), root,
+                 P(np.ascontiguousarray(nodes, np.uint32)), P(np.ascontiguousarray(tris, np.float32)), use_sobol)
+    return pixels
+
+
+def render_pt(accum, cam, root, nodes, tris, attribs, w, h, use_sobol=1, max_spp=1 << 30, max_depth=1024, trig=1):
+    oracle().orc_render_pt(P(accum), w, h, P(np.ascontiguousarray(cam, np.float32)), root,
+                           P(np.ascontiguousarray(nodes, np.uint32)), P(np.ascontiguousarray(tris, np.float32)),
+                           P(np.ascontiguousarray(attribs, np.float32)), use_sobol, max_spp, max_depth, trig)
+    return accum
+
+
+def ref_pt(accum, cam, root, nodes, tris, attribs, w, h, use_sobol=1, max_spp=1 << 30):
+    pixels = np.zeros(w * h, np.uint32)
+    ref().ref_pt(P(pixels), P(accum), w, h, P(np.ascontiguousarray(cam, np.float32)), root,
+                 P(np.ascontiguousarray(nodes, np.uint32)), P(np.ascontiguousarray(tris, np.float32)),
+                 P(np.ascontiguousarray(attribs, np.float32)), use_sobol, max_spp)
+    return accum
+
+
+def render_normal(cam, root, nodes, tris, w, h):
+    pixels = np.zeros(w * h, np.uint32)
+    oracle().orc_render_normal(P(pixels), w, h, P(np.ascontiguousarray(cam, np.float32)), root,
+                               P(np.ascontiguousarray(nodes, np.uint32)), P(np.ascontiguousarray(tris, np.float32)))
+    return pixels
+
+
+def pack(accum, n):
+    pixels = np.zeros(n, np.uint32)
+    oracle().orc_pack(P(pixels), P(np.ascontiguousarray(accum, np.float32)), n)
+    return pixels
