@@ -20,7 +20,7 @@
 #include <cstring>
 
 #include "capi_internal.h"
-#include "common.cuh"
+#include "../../include/mlbvh_device.cuh"
 
 namespace mlbvh {
 
@@ -186,7 +186,7 @@ __global__ void __launch_bounds__(kKeysThreads)
 {
     __shared__ float s_scene[6];
     __shared__ uint32_t s_hist[4][256];
-    __shared__ float s_tri[kKeysThreads * 9];
+    __shared__ __align__(16) float s_tri[kKeysThreads * 9];  // written with 16-byte stores
 
     for (int i = threadIdx.x; i < 4 * 256; i += blockDim.x) (&s_hist[0][0])[i] = 0u;
     if (threadIdx.x < 32) {

@@ -10,7 +10,7 @@
 #include <algorithm>
 
 #include "capi_internal.h"
-#include "common.cuh"
+#include "../../include/mlbvh_device.cuh"
 
 namespace mlbvh {
 

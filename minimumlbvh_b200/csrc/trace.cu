@@ -5,126 +5,13 @@
 // (:912-973) with a single launch. Rays and hits move as 2 x 16-byte vectors,
 // nodes as 4 x 16-byte read-only loads.
 #include "capi_internal.h"
-#include "common.cuh"
+#include "../../include/mlbvh_device.cuh"
 
 namespace mlbvh {
 
 namespace {
 
 constexpr int kTraceThreads = 128;
-
-// intersect_escape_link (minimum_lbvh.h:1063-1137): after a left child the
-// walk moves to the right child through the parent; after a right child it
-// follows the rope in `context` (the node whose left subtree starts the next
-// leaf range). A one-leaf tree is tested directly (the reference would read
-// nodes[invalid] there).
-template <bool kAny>
-__device__ __forceinline__ void trace_escape(HitRecord& hit, const mlbvh_internal_node* __restrict__ nodes,
-                                             const float* __restrict__ tris, uint32_t root, f3 ro, f3 rd, f3 inv,
-                                             float tmin)
-{
-    auto leaf = [&](uint32_t n) -> bool {
-        uint32_t ti = n & ~kLeafBit;
-        f3 v0, v1, v2;
-        load_triangle(tris, ti, v0, v1, v2);
-        float t, u, v;
-        f3 ng;
-        if (intersect_triangle(t, u, v, ng, tmin, hit.t, ro, rd, v0, v1, v2)) {
-            hit.t = t;
-            hit.u = u;
-            hit.v = v;
-            hit.ng = ng;
-            hit.tri = ti;
-            return true;
-        }
-        return false;
-    };
-    if (root & kLeafBit) {
-        leaf(root);
-        return;
-    }
-    uint32_t curr = root, prev = kInvalid, steps = 0;
-    while (curr != kInvalid && ++steps < kMaxTraversalSteps) {
-        if (curr & kLeafBit) {
-            if (leaf(curr) && kAny) break;
-            const NodeView pn = load_node(nodes, prev & ~kLeafBit);
-            if (pn.c0 == curr) {
-                uint32_t s = curr;
-                curr = prev;
-                prev = s;
-                continue;
-            }
-            uint32_t next = pn.context != 0xFFFFFFFFu ? pn.context : kInvalid;
-            prev = curr;
-            curr = next;
-            continue;
-        }
-        const NodeView nd = load_node(nodes, curr);
-        f3 lo, hi;
-        uint32_t hitChild, miss;
-        if (prev == nd.parent) {
-            lo = nd.lo0;
-            hi = nd.hi0;
-            hitChild = nd.c0;
-            miss = curr;
-        } else {
-            lo = nd.lo1;
-            hi = nd.hi1;
-            hitChild = nd.c1;
-            miss = nd.context != 0xFFFFFFFFu ? nd.context : kInvalid;
-        }
-        float2 r = slab(ro, inv, lo, hi, tmin, hit.t);
-        uint32_t next = r.x <= r.y ? hitChild : miss;
-        prev = curr;
-        curr = next;
-    }
-}
-
-// intersect_stackfull (minimum_lbvh.h:912-973): explicit per-thread stack of
-// far children; closest hit only, as in the reference.
-__device__ __forceinline__ void trace_stackfull(HitRecord& hit, const mlbvh_internal_node* __restrict__ nodes,
-                                                const float* __restrict__ tris, uint32_t root, f3 ro, f3 rd, f3 inv,
-                                                float tmin)
-{
-    uint32_t stack[64];
-    int sp = 0;
-    uint32_t node = root, steps = 0;
-    while (node != kInvalid && ++steps < kMaxTraversalSteps) {
-        if (node & kLeafBit) {
-            uint32_t ti = node & ~kLeafBit;
-            f3 v0, v1, v2;
-            load_triangle(tris, ti, v0, v1, v2);
-            float t, u, v;
-            f3 ng;
-            if (intersect_triangle(t, u, v, ng, tmin, hit.t, ro, rd, v0, v1, v2)) {
-                hit.t = t;
-                hit.u = u;
-                hit.v = v;
-                hit.ng = ng;
-                hit.tri = ti;
-            }
-            node = sp == 0 ? kInvalid : stack[--sp];
-            continue;
-        }
-        const NodeView nd = load_node(nodes, node);
-        float2 rl = slab(ro, inv, nd.lo0, nd.hi0, tmin, hit.t);
-        float2 rr = slab(ro, inv, nd.lo1, nd.hi1, tmin, hit.t);
-        bool hitL = rl.x <= rl.y, hitR = rr.x <= rr.y;
-        if (hitL && hitR) {
-            uint32_t nearN = nd.c0, farN = nd.c1;
-            if (rr.x < rl.x) {
-                nearN = nd.c1;
-                farN = nd.c0;
-            }
-            node = nearN;
-            if (sp < 64) stack[sp++] = farN;
-        } else if (hitL || hitR) {
-            node = hitL ? nd.c0 : nd.c1;
-        } else {
-            node = sp == 0 ? kInvalid : stack[--sp];
-        }
-    }
-}
 
 template <int kMode, bool kAny>
 __global__ void __launch_bounds__(kTraceThreads)
@@ -144,12 +31,14 @@ __global__ void __launch_bounds__(kTraceThreads)
     hit.tri = 0xFFFFFFFFu;
     const uint32_t root = __ldg(rootPtr);
     const f3 inv = inv_rd(rd);
-    if (kMode == MLBVH_TRAVERSAL_ESCAPE_LINK)
+    if (kMode == MLBVH_TRAVERSAL_ESCAPE_LINK) {
         trace_escape<kAny>(hit, nodes, tris, root, ro, rd, inv, tmin);
-    else if (kMode == MLBVH_TRAVERSAL_STACKFULL)
-        trace_stackfull(hit, nodes, tris, root, ro, rd, inv, tmin);
-    else
+    } else if (kMode == MLBVH_TRAVERSAL_STACKFULL) {
+        uint32_t stack[64];
+        trace_stackfull(hit, nodes, tris, root, ro, rd, inv, tmin, stack, 64);
+    } else {
         trace_stackfree<kAny>(hit, nodes, tris, root, ro, rd, inv, tmin);
+    }
     hits[2 * (size_t)i] = make_float4(hit.t, 0.0f, hit.u, hit.v);
     hits[2 * (size_t)i + 1] = make_float4(hit.ng.x, hit.ng.y, hit.ng.z, __uint_as_float(hit.tri));
 }
