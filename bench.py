@@ -233,8 +233,11 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=8.0, help="wall time of the CPU-baseline AO sample")
     ap.add_argument("--ref-seconds", type=float, default=4.0, help="wall time of one reference-arm step")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--image", default=None, help="override the frame size, WxH (small cases for ncu captures)")
     args = ap.parse_args()
-    wl = WORKLOADS[args.workload]
+    wl = dict(WORKLOADS[args.workload])
+    if args.image:
+        wl["w"], wl["h"] = (int(v) for v in args.image.lower().split("x"))
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
     local = int(os.environ.get("LOCAL_RANK", 0))

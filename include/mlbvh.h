@@ -83,6 +83,35 @@ typedef struct mlbvh_triangle_attrib {
     float emissive[3];
 } mlbvh_triangle_attrib;
 
+/* The quantised tree (no reference counterpart; a replacement node format for
+ * the same topology, 32 bytes instead of 64):
+ *   origin     the node's box lower corner (FP32), the min of both child boxes
+ *   q[c*6+0..2], q[c*6+3..5]  child c's lower / upper corner in steps of
+ *              2^(eBase - k_axis) above origin, rounded down / up, so the
+ *              decoded box always contains the exact one
+ *   child[c]   bit 31 leaf flag; bits 0-22 internal-node index or leaf
+ *              position; bits 23-30 carry the three 5-bit axis codes k_axis
+ *              (child[0]: k_x | k_y bits 0-2; child[1]: k_y bits 3-4 | k_z)
+ * Parents live in a separate array (read only when the walk moves up).
+ * Leaves are stored in sorted (leaf) order as mlbvh_qtri: the triangle's three
+ * FP32 corners, unchanged, and its original index. */
+typedef struct mlbvh_qnode {
+    float origin[3];
+    uint8_t q[12];
+    uint32_t child[2];
+} mlbvh_qnode;
+typedef struct mlbvh_qtri {
+    float v[9];
+    uint32_t triangleIndex;
+    uint32_t _pad[2];
+} mlbvh_qtri;
+typedef struct mlbvh_qheader {
+    uint32_t root; /* bit 31 leaf flag, bits 0-22 index */
+    int32_t eBase; /* step exponent of code k = 0 */
+    uint32_t nTriangles;
+    uint32_t _pad;
+} mlbvh_qheader;
+
 /* Library version (MLBVH_VERSION) and the message of the last error raised on
  * the calling host thread ("" if none). */
 MLBVH_API int mlbvh_version(void);
@@ -129,6 +158,30 @@ MLBVH_API mlbvh_status mlbvh_trace(const mlbvh_internal_node* dInternals, const 
                          const mlbvh_triangle* dTriangles, const mlbvh_ray* dRays, mlbvh_hit* dHits,
                          uint32_t nRays, int rayQuery, int traversal, void* stream);
 
+/* ------------------------------------------------------- quantised form ---
+ * No reference counterpart. mlbvh_quantise converts a tree built by
+ * mlbvh_build (same topology) into 32-byte nodes with 8-bit child boxes
+ * rounded outward, a parent array and leaf-ordered triangles:
+ * dQNodes nTriangles-1 entries, dQParents nTriangles-1, dQTris nTriangles,
+ * one dQHeader. 1 <= nTriangles <= 2^23. The triangle test stays FP32 and
+ * identical, so closest hits equal the FP32 tree's except where two triangles
+ * return bit-identical t (the later-visited wins in both). */
+MLBVH_API mlbvh_status mlbvh_quantise(const mlbvh_internal_node* dInternals, const mlbvh_node_index* dRootNode,
+                                      const mlbvh_triangle* dTriangles, uint32_t nTriangles, mlbvh_qnode* dQNodes,
+                                      uint32_t* dQParents, mlbvh_qtri* dQTris, mlbvh_qheader* dQHeader, void* stream);
+/* mlbvh_trace over the quantised tree (stack-free, as intersect_stackfree). */
+MLBVH_API mlbvh_status mlbvh_trace_quantised(const mlbvh_qnode* dQNodes, const uint32_t* dQParents,
+                                             const mlbvh_qtri* dQTris, const mlbvh_qheader* dQHeader,
+                                             const mlbvh_ray* dRays, mlbvh_hit* dHits, uint32_t nRays, int rayQuery,
+                                             void* stream);
+/* mlbvh_render_ao over the quantised tree; same arguments otherwise. */
+MLBVH_API mlbvh_status mlbvh_render_ao_quantised(uint32_t* dPixels, uint32_t* dOccluded, int width, int height,
+                                                 const mlbvh_ray_generator* camera, const mlbvh_qnode* dQNodes,
+                                                 const uint32_t* dQParents, const mlbvh_qtri* dQTris,
+                                                 const mlbvh_qheader* dQHeader, int useSobol, int nSamples,
+                                                 float radius, uint32_t sobolSeed, unsigned long long* dStats,
+                                                 void* dScratch, size_t scratchBytes, void* stream);
+
 /* --------------------------------------------------------------- shading ---
  * The reference's shading kernels (main_gpu.cu), one launch chain each.
  * `camera` is a HOST pointer (passed by value to the kernels, as the
@@ -147,10 +200,11 @@ MLBVH_API mlbvh_status mlbvh_render_normal(uint32_t* dPixels, int width, int hei
  * dOccluded / nSamples. The sample directions use this library's FP32 sincos
  * instead of CUDA's cosf/sinf, so that the host oracle can reproduce them bit
  * for bit. dScratch holds mlbvh_render_scratch_bytes(width, height) bytes.
- * dStats (may be NULL; 5 device uint64) receives {rays traced (primary + AO),
+ * dStats (may be NULL; 8 device uint64) receives {rays traced (primary + AO),
  * internal-node visits, triangle tests, the AO rays' share of those visits,
- * the AO rays' share of those tests}; counting runs a slower kernel variant,
- * so leave it NULL when timing. */
+ * the AO rays' share of those tests, parent-word loads (quantised tree only),
+ * the AO rays' share of those, 0}; counting runs a slower kernel variant, so
+ * leave it NULL when timing. */
 MLBVH_API size_t mlbvh_render_scratch_bytes(int width, int height);
 MLBVH_API mlbvh_status mlbvh_render_ao(uint32_t* dPixels, uint32_t* dOccluded, int width, int height,
                              const mlbvh_ray_generator* camera, const mlbvh_node_index* dRootNode,

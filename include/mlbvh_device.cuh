@@ -547,4 +547,143 @@ __device__ __forceinline__ void shoot(const Camera& cam, float u, float v, f3& r
     rd = to - from;
 }
 
+// ------------------------------------------------------------ quantised tree
+// 32-byte nodes with 8-bit child boxes (see mlbvh_qnode in mlbvh.h). Boxes
+// are decoded with directed rounding (lower corners down, upper corners up),
+// so every decoded box contains the FP32 box it came from and the traversal
+// visits every leaf the FP32 traversal would need.
+constexpr uint32_t kQIndexMask = 0x7FFFFFu;  // 23-bit index / leaf position
+constexpr uint32_t kQMaxLeaves = 1u << 23;
+
+__device__ __forceinline__ float pow2f(int e) { return __int_as_float((127 + e) << 23); }  // e in [-126, 127]
+
+// The step exponent e of one axis: the smallest e with 255 * 2^e >= d
+// (d >= 0, already rounded up), at least -126.
+__device__ __forceinline__ int step_exponent(float d)
+{
+    if (!(d >= 1.17549435e-38f)) return -126;  // zero, subnormal (or NaN)
+    int x = (int)((__float_as_uint(d) >> 23) & 0xFFu) - 126;  // d = m * 2^x, m in [0.5, 1)
+    int e = x - 8;
+    if (e < -126) e = -126;
+    if (255.0f * pow2f(e) < d) e += 1;
+    return e;
+}
+
+struct QBox {
+    f3 lo0, hi0, lo1, hi1;
+};
+
+__device__ __forceinline__ void decode_steps(uint32_t c0, uint32_t c1, int eBase, float& sx, float& sy, float& sz)
+{
+    const uint32_t code = ((c0 >> 23) & 0xFFu) | (((c1 >> 23) & 0xFFu) << 8);
+    int ex = eBase - (int)(code & 31u), ey = eBase - (int)((code >> 5) & 31u), ez = eBase - (int)((code >> 10) & 31u);
+    sx = pow2f(max(ex, -126));
+    sy = pow2f(max(ey, -126));
+    sz = pow2f(max(ez, -126));
+}
+
+__device__ __forceinline__ float qlo(float o, uint32_t q, float s) { return __fadd_rd(o, (float)q * s); }
+__device__ __forceinline__ float qhi(float o, uint32_t q, float s) { return __fadd_ru(o, (float)q * s); }
+
+struct QNodeView {
+    uint32_t c0, c1;  // leaf flag | 23-bit index
+    QBox box;
+};
+__device__ __forceinline__ QNodeView load_qnode(const mlbvh_qnode* __restrict__ qnodes, uint32_t i, int eBase)
+{
+    const float4* p = reinterpret_cast<const float4*>(qnodes + i);
+    const float4 a = __ldg(p), b = __ldg(p + 1);
+    const uint32_t w0 = __float_as_uint(a.w), w1 = __float_as_uint(b.x), w2 = __float_as_uint(b.y);
+    const uint32_t c0 = __float_as_uint(b.z), c1 = __float_as_uint(b.w);
+    float sx, sy, sz;
+    decode_steps(c0, c1, eBase, sx, sy, sz);
+    const f3 o = mk(a.x, a.y, a.z);
+    QNodeView n;
+    n.c0 = c0 & (kLeafBit | kQIndexMask);
+    n.c1 = c1 & (kLeafBit | kQIndexMask);
+    // q bytes: w0 = q0..q3, w1 = q4..q7, w2 = q8..q11
+    n.box.lo0 = mk(qlo(o.x, w0 & 255u, sx), qlo(o.y, (w0 >> 8) & 255u, sy), qlo(o.z, (w0 >> 16) & 255u, sz));
+    n.box.hi0 = mk(qhi(o.x, w0 >> 24, sx), qhi(o.y, w1 & 255u, sy), qhi(o.z, (w1 >> 8) & 255u, sz));
+    n.box.lo1 = mk(qlo(o.x, (w1 >> 16) & 255u, sx), qlo(o.y, w1 >> 24, sy), qlo(o.z, w2 & 255u, sz));
+    n.box.hi1 = mk(qhi(o.x, (w2 >> 8) & 255u, sx), qhi(o.y, (w2 >> 16) & 255u, sy), qhi(o.z, w2 >> 24, sz));
+    return n;
+}
+
+// Stack-free walk over the quantised tree: the state machine of
+// intersect_stackfree (minimum_lbvh.h:981-1061), with "came from the parent"
+// recognised as "came from neither child" so that the parent word is read
+// only when the walk moves up.
+template <bool kAny, bool kCount = false>
+__device__ __forceinline__ void trace_quantised(HitRecord& hit, const mlbvh_qnode* __restrict__ qnodes,
+                                                const uint32_t* __restrict__ parents,
+                                                const mlbvh_qtri* __restrict__ qtris, uint32_t root, int eBase, f3 ro,
+                                                f3 rd, f3 inv, float tmin, uint32_t* visits = nullptr,
+                                                uint32_t* tests = nullptr, uint32_t* ups = nullptr)
+{
+    uint32_t curr = root, prev = kInvalid;
+    uint32_t nv = 0, nt = 0, nu = 0, steps = 0;
+    while (curr != kInvalid && ++steps < kMaxTraversalSteps) {
+        if (curr & kLeafBit) {
+            if (kCount) ++nt;
+            const float4* t = reinterpret_cast<const float4*>(qtris + (curr & kQIndexMask));
+            const float4 a = __ldg(t), b = __ldg(t + 1), c = __ldg(t + 2);
+            float tt, u, v;
+            f3 ng;
+            if (intersect_triangle(tt, u, v, ng, tmin, hit.t, ro, rd, mk(a.x, a.y, a.z), mk(a.w, b.x, b.y),
+                                   mk(b.z, b.w, c.x))) {
+                hit.t = tt;
+                hit.u = u;
+                hit.v = v;
+                hit.ng = ng;
+                hit.tri = __float_as_uint(c.y);
+                if (kAny) break;
+            }
+            const uint32_t s = curr;
+            curr = prev;
+            prev = s;
+            continue;
+        }
+        if (kCount) ++nv;
+        const QNodeView nd = load_qnode(qnodes, curr, eBase);
+        const float2 rl = slab(ro, inv, nd.box.lo0, nd.box.hi0, tmin, hit.t);
+        const float2 rr = slab(ro, inv, nd.box.lo1, nd.box.hi1, tmin, hit.t);
+        const bool hitL = rl.x <= rl.y, hitR = rr.x <= rr.y;
+        uint32_t nearN = nd.c0, farN = nd.c1;
+        int nHits = 0;
+        if (hitL && hitR) {
+            if (rr.x < rl.x) {
+                nearN = nd.c1;
+                farN = nd.c0;
+            }
+            nHits = 2;
+        } else if (hitL || hitR) {
+            nHits = 1;
+            nearN = hitR ? farN : nearN;
+        }
+        const bool fromParent = prev != nd.c0 && prev != nd.c1;
+        uint32_t next = kInvalid;
+        bool up;
+        if (fromParent) {
+            up = nHits == 0;
+            next = nearN;
+        } else if (prev == nearN) {
+            up = nHits != 2;
+            next = farN;
+        } else {
+            up = true;
+        }
+        if (up) {
+            if (kCount) ++nu;
+            next = __ldg(parents + curr);
+        }
+        prev = curr;
+        curr = next;
+    }
+    if (kCount) {
+        *visits += nv;
+        *tests += nt;
+        *ups += nu;
+    }
+}
+
 }  // namespace mlbvh

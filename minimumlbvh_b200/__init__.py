@@ -21,6 +21,7 @@ __all__ = [
     "RAY_QUERY_CLOSEST", "RAY_QUERY_ANY", "TRAVERSAL_STACKFREE", "TRAVERSAL_ESCAPE_LINK",
     "TRAVERSAL_STACKFULL", "OnesweepSort", "BVHGPUBuilder", "RayGenerator", "intersect",
     "render_normal", "render_ao", "render_pt", "pack", "profile_events", "FLT_MAX", "INVALID_NODE",
+    "QuantisedBVH", "intersect_quantised", "render_ao_quantised",
 ]
 
 BUILD_OPTION_USE_NORMAL = 1   # minimum_lbvh.h:44
@@ -75,6 +76,10 @@ def lib() -> ctypes.CDLL:
             "mlbvh_render_pt": (i32, [_vp, i32, i32, _vp, _vp, _vp, _vp, _vp, i32, i32, i32, _vp]),
             "mlbvh_pack": (i32, [_vp, _vp, i32, _vp]),
             "mlbvh_profile_events": (None, [_vp, _vp]),
+            "mlbvh_quantise": (i32, [_vp, _vp, _vp, u32, _vp, _vp, _vp, _vp, _vp]),
+            "mlbvh_trace_quantised": (i32, [_vp, _vp, _vp, _vp, _vp, _vp, u32, i32, _vp]),
+            "mlbvh_render_ao_quantised": (i32, [_vp, _vp, i32, i32, _vp, _vp, _vp, _vp, _vp, i32, i32, f32, u32,
+                                                _vp, _vp, sz, _vp]),
             "mlbvh_camera_lookat": (i32, [_vp, _vp, _vp, _vp, f32, i32, i32]),
         }
         for name, (res, args) in sig.items():
@@ -264,6 +269,9 @@ _render_scratch = {}
 def profile_events(start=None, stop=None):
     """Make the next render_ao / BVHGPUBuilder.build on this thread record
     the torch.cuda.Event pair around its dominant kernel."""
+    for e in (start, stop):
+        if e is not None and not e.cuda_event:
+            e.record()  # torch creates the CUDA event on first record; the hook re-records it
     lib().mlbvh_profile_events(None if start is None else start.cuda_event,
                                None if stop is None else stop.cuda_event)
 
@@ -306,4 +314,61 @@ def render_pt(accumulators, imageSize, rayGenerator: RayGenerator, rootNode, int
 def pack(pixels, accumulators, n: int, stream=None):
     """pack (main_gpu.cu:273-286)."""
     _check(lib().mlbvh_pack(_ptr(pixels), _ptr(accumulators), int(n), _stream(stream)))
+    return pixels
+
+
+class QuantisedBVH:
+    """The quantised form of a built tree (no reference counterpart):
+    32-byte nodes with 8-bit child boxes rounded outward, a parent array and
+    leaf-ordered triangles. ``from_builder`` converts a BVHGPUBuilder's tree
+    on the GPU (mlbvh_quantise)."""
+
+    def __init__(self, qnodes, parents, qtris, header, n):
+        self.qnodes, self.parents, self.qtris, self.header, self.nTriangles = qnodes, parents, qtris, header, n
+
+    @classmethod
+    def from_builder(cls, builder: BVHGPUBuilder, triangles, stream=None) -> "QuantisedBVH":
+        import torch
+        n = builder.m_nTriangles
+        dev = triangles.device
+        qnodes = torch.empty((max(n - 1, 1), 8), dtype=torch.int32, device=dev)
+        parents = torch.empty(max(n - 1, 1) + 3, dtype=torch.int32, device=dev)
+        qtris = torch.empty((n, 12), dtype=torch.int32, device=dev)
+        header = torch.empty(4, dtype=torch.int32, device=dev)
+        _check(lib().mlbvh_quantise(_ptr(builder.m_internals), _ptr(builder.m_rootNode), _ptr(triangles), n,
+                                    _ptr(qnodes), _ptr(parents), _ptr(qtris), _ptr(header), _stream(stream)))
+        return cls(qnodes, parents, qtris, header, n)
+
+
+def intersect_quantised(q: QuantisedBVH, rays, rayQuery: int = RAY_QUERY_CLOSEST, hits=None, stream=None):
+    """Stack-free closest/any hit over the quantised tree (same Hit records)."""
+    import torch
+    _require_cuda(rays, "rays")
+    n = rays.numel() // 8
+    if hits is None:
+        hits = torch.empty((n, 8), dtype=torch.int32, device=rays.device)
+    _check(lib().mlbvh_trace_quantised(_ptr(q.qnodes), _ptr(q.parents), _ptr(q.qtris), _ptr(q.header), _ptr(rays),
+                                       _ptr(hits), n, int(rayQuery), _stream(stream)))
+    return hits
+
+
+def render_ao_quantised(pixels, imageSize, rayGenerator: RayGenerator, q: QuantisedBVH, useSobol: int = 1,
+                        nSamples: int = 16, radius: float = 1.0, seed: int = 12345, occluded=None, stats=None,
+                        scratch=None, stream=None):
+    """render_ao over the quantised tree."""
+    import torch
+    w, h = imageSize
+    need = lib().mlbvh_render_scratch_bytes(int(w), int(h))
+    if scratch is None:
+        key = (pixels.device.index, need)
+        scratch = _render_scratch.get(key)
+        if scratch is None:
+            scratch = torch.empty(need, dtype=torch.uint8, device=pixels.device)
+            _render_scratch.clear()
+            _render_scratch[key] = scratch
+    cam = rayGenerator._cstruct()
+    _check(lib().mlbvh_render_ao_quantised(_ptr(pixels), _ptr(occluded), int(w), int(h), ctypes.addressof(cam),
+                                           _ptr(q.qnodes), _ptr(q.parents), _ptr(q.qtris), _ptr(q.header),
+                                           int(useSobol), int(nSamples), float(radius), int(seed), _ptr(stats),
+                                           _ptr(scratch), scratch.numel(), _stream(stream)))
     return pixels

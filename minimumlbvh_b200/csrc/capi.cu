@@ -124,6 +124,37 @@ mlbvh_status mlbvh_render_pt(float* dAccumulators, int width, int height, const 
                      maxSPP, maxDepth, as_stream(stream));
 }
 
+mlbvh_status mlbvh_quantise(const mlbvh_internal_node* dInternals, const mlbvh_node_index* dRootNode,
+                            const mlbvh_triangle* dTriangles, uint32_t nTriangles, mlbvh_qnode* dQNodes,
+                            uint32_t* dQParents, mlbvh_qtri* dQTris, mlbvh_qheader* dQHeader, void* stream)
+{
+    clear_error();
+    return quantise(dInternals, dRootNode, dTriangles, nTriangles, dQNodes, dQParents, dQTris, dQHeader,
+                    as_stream(stream));
+}
+
+mlbvh_status mlbvh_trace_quantised(const mlbvh_qnode* dQNodes, const uint32_t* dQParents, const mlbvh_qtri* dQTris,
+                                   const mlbvh_qheader* dQHeader, const mlbvh_ray* dRays, mlbvh_hit* dHits,
+                                   uint32_t nRays, int rayQuery, void* stream)
+{
+    clear_error();
+    return trace_quantised(dQNodes, dQParents, dQTris, dQHeader, dRays, dHits, nRays, rayQuery, as_stream(stream));
+}
+
+mlbvh_status mlbvh_render_ao_quantised(uint32_t* dPixels, uint32_t* dOccluded, int width, int height,
+                                       const mlbvh_ray_generator* camera, const mlbvh_qnode* dQNodes,
+                                       const uint32_t* dQParents, const mlbvh_qtri* dQTris,
+                                       const mlbvh_qheader* dQHeader, int useSobol, int nSamples, float radius,
+                                       uint32_t sobolSeed, unsigned long long* dStats, void* dScratch,
+                                       size_t scratchBytes, void* stream)
+{
+    clear_error();
+    if (!camera) return fail(MLBVH_ERR_INVALID_ARG, "null camera");
+    return render_ao_quantised(dPixels, dOccluded, width, height, *camera, dQNodes, dQParents, dQTris, dQHeader,
+                               useSobol, nSamples, radius, sobolSeed, dStats, dScratch, scratchBytes,
+                               as_stream(stream));
+}
+
 void mlbvh_profile_events(void* startEvent, void* stopEvent)
 {
     set_profile_events(reinterpret_cast<cudaEvent_t>(startEvent), reinterpret_cast<cudaEvent_t>(stopEvent));

@@ -48,6 +48,17 @@ mlbvh_status render_ao(uint32_t* dPixels, uint32_t* dOccluded, int w, int h, con
                        const mlbvh_node_index* dRoot, const mlbvh_internal_node* dNodes, const mlbvh_triangle* dTris,
                        int useSobol, int nSamples, float radius, uint32_t seed, unsigned long long* dStats,
                        void* dScratch, size_t scratchBytes, cudaStream_t stream);
+mlbvh_status render_ao_quantised(uint32_t* dPixels, uint32_t* dOccluded, int w, int h, const mlbvh_ray_generator& cam,
+                                 const mlbvh_qnode* dQNodes, const uint32_t* dQParents, const mlbvh_qtri* dQTris,
+                                 const mlbvh_qheader* dQHeader, int useSobol, int nSamples, float radius,
+                                 uint32_t seed, unsigned long long* dStats, void* dScratch, size_t scratchBytes,
+                                 cudaStream_t stream);
+mlbvh_status quantise(const mlbvh_internal_node* dNodes, const mlbvh_node_index* dRoot, const mlbvh_triangle* dTris,
+                      uint32_t n, mlbvh_qnode* dQNodes, uint32_t* dQParents, mlbvh_qtri* dQTris,
+                      mlbvh_qheader* dQHeader, cudaStream_t stream);
+mlbvh_status trace_quantised(const mlbvh_qnode* dQNodes, const uint32_t* dQParents, const mlbvh_qtri* dQTris,
+                             const mlbvh_qheader* dQHeader, const mlbvh_ray* dRays, mlbvh_hit* dHits, uint32_t nRays,
+                             int rayQuery, cudaStream_t stream);
 mlbvh_status render_pt(float* dAccum, int w, int h, const mlbvh_ray_generator& cam, const mlbvh_node_index* dRoot,
                        const mlbvh_internal_node* dNodes, const mlbvh_triangle* dTris,
                        const mlbvh_triangle_attrib* dAttribs, int useSobol, int maxSPP, int maxDepth,

@@ -1,0 +1,196 @@
+// The quantised tree: 32-byte nodes with 8-bit child boxes (no reference
+// counterpart), made from a tree built by build.cu, and its ray query.
+//
+// k_quantise: one thread per internal node. The node's origin is the min of
+// its two child boxes; per axis the step is the smallest power of two 2^e with
+// 255 * 2^e >= the node's extent (rounded up), coded as k = eBase - e in 5 bits
+// where eBase is the step of the root's extent. Child corners are quantised
+// down (lower) and up (upper) and checked against the same directed-rounding
+// decode the traversal uses, so every decoded box contains its FP32 box.
+// Leaves move to sorted (leaf) order: a left leaf child of node j is leaf j,
+// a right leaf child is leaf j+1 (node j splits leaves j and j+1).
+#include "capi_internal.h"
+#include "../../include/mlbvh_device.cuh"
+
+namespace mlbvh {
+
+namespace {
+
+constexpr int kQuantiseThreads = 256;
+constexpr int kTraceThreads = 128;
+
+__device__ __forceinline__ void leaf_box(const float* __restrict__ tris, uint32_t t, f3& lo, f3& hi)
+{
+    f3 v0, v1, v2;
+    load_triangle(tris, t, v0, v1, v2);
+    lo = smin3(smin3(smin3(mk(kFltMax, kFltMax, kFltMax), v0), v1), v2);
+    hi = smax3(smax3(smax3(mk(-kFltMax, -kFltMax, -kFltMax), v0), v1), v2);
+}
+
+// Step exponent of the whole tree: that of the largest root-box extent.
+__device__ __forceinline__ int tree_ebase(const mlbvh_internal_node* __restrict__ nodes,
+                                          const float* __restrict__ tris, uint32_t root)
+{
+    f3 lo, hi;
+    if (root & kLeafBit) {
+        leaf_box(tris, root & ~kLeafBit, lo, hi);
+    } else {
+        const NodeView nd = load_node(nodes, root);
+        lo = smin3(nd.lo0, nd.lo1);
+        hi = smax3(nd.hi0, nd.hi1);
+    }
+    const float d = fmaxf(fmaxf(__fsub_ru(hi.x, lo.x), __fsub_ru(hi.y, lo.y)), __fsub_ru(hi.z, lo.z));
+    return step_exponent(d);
+}
+
+__device__ __forceinline__ uint32_t quantise_lo(float v, float o, float s)
+{
+    float q = floorf(__fsub_rd(v, o) / s);
+    uint32_t qi = q <= 0.0f ? 0u : (q >= 255.0f ? 255u : (uint32_t)q);
+    while (qi > 0u && qlo(o, qi, s) > v) --qi;
+    return qi;
+}
+__device__ __forceinline__ uint32_t quantise_hi(float v, float o, float s)
+{
+    float q = ceilf(__fsub_ru(v, o) / s);
+    uint32_t qi = q <= 0.0f ? 0u : (q >= 255.0f ? 255u : (uint32_t)q);
+    while (qi < 255u && qhi(o, qi, s) < v) ++qi;
+    return qi;
+}
+
+__device__ __forceinline__ void write_qtri(mlbvh_qtri* __restrict__ qtris, uint32_t pos, const float* __restrict__ tris,
+                                           uint32_t t)
+{
+    const float* src = tris + 9ull * t;
+    float4* dst = reinterpret_cast<float4*>(qtris + pos);
+    dst[0] = make_float4(__ldg(src + 0), __ldg(src + 1), __ldg(src + 2), __ldg(src + 3));
+    dst[1] = make_float4(__ldg(src + 4), __ldg(src + 5), __ldg(src + 6), __ldg(src + 7));
+    dst[2] = make_float4(__ldg(src + 8), __uint_as_float(t), 0.0f, 0.0f);
+}
+
+__global__ void __launch_bounds__(kQuantiseThreads)
+    k_quantise(const mlbvh_internal_node* __restrict__ nodes, const mlbvh_node_index* __restrict__ rootPtr,
+               const float* __restrict__ tris, uint32_t n, mlbvh_qnode* __restrict__ qnodes,
+               uint32_t* __restrict__ parents, mlbvh_qtri* __restrict__ qtris, mlbvh_qheader* __restrict__ header)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t root = __ldg(rootPtr);
+    const int eBase = tree_ebase(nodes, tris, root);
+    if (i == 0) {
+        header->root = (root & kLeafBit) ? kLeafBit : root;
+        header->eBase = eBase;
+        header->nTriangles = n;
+        header->_pad = 0;
+        if (root & kLeafBit) write_qtri(qtris, 0, tris, root & ~kLeafBit);
+    }
+    if (i + 1 >= n) return;
+    const NodeView nd = load_node(nodes, i);
+    const f3 o = smin3(nd.lo0, nd.lo1);
+    const f3 top = smax3(nd.hi0, nd.hi1);
+    const float ext[3] = {__fsub_ru(top.x, o.x), __fsub_ru(top.y, o.y), __fsub_ru(top.z, o.z)};
+    uint32_t code = 0;
+    float step[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        int e = max(step_exponent(ext[a]), eBase - 31);
+        int k = eBase - e;
+        if (k < 0) k = 0;  // cannot happen: every node lies inside the root box
+        code |= (uint32_t)k << (5 * a);
+        step[a] = pow2f(max(eBase - k, -126));
+    }
+    const float lo0[3] = {nd.lo0.x, nd.lo0.y, nd.lo0.z}, hi0[3] = {nd.hi0.x, nd.hi0.y, nd.hi0.z};
+    const float lo1[3] = {nd.lo1.x, nd.lo1.y, nd.lo1.z}, hi1[3] = {nd.hi1.x, nd.hi1.y, nd.hi1.z};
+    const float oo[3] = {o.x, o.y, o.z};
+    uint32_t q[12];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        q[a] = quantise_lo(lo0[a], oo[a], step[a]);
+        q[3 + a] = quantise_hi(hi0[a], oo[a], step[a]);
+        q[6 + a] = quantise_lo(lo1[a], oo[a], step[a]);
+        q[9 + a] = quantise_hi(hi1[a], oo[a], step[a]);
+    }
+    uint32_t c0 = nd.c0, c1 = nd.c1;
+    if (c0 & kLeafBit) {
+        write_qtri(qtris, i, tris, c0 & ~kLeafBit);
+        c0 = kLeafBit | i;
+    }
+    if (c1 & kLeafBit) {
+        write_qtri(qtris, i + 1, tris, c1 & ~kLeafBit);
+        c1 = kLeafBit | (i + 1);
+    }
+    c0 |= (code & 0xFFu) << 23;
+    c1 |= ((code >> 8) & 0xFFu) << 23;
+    float4* dst = reinterpret_cast<float4*>(qnodes + i);
+    dst[0] = make_float4(o.x, o.y, o.z, __uint_as_float(q[0] | q[1] << 8 | q[2] << 16 | q[3] << 24));
+    dst[1] = make_float4(__uint_as_float(q[4] | q[5] << 8 | q[6] << 16 | q[7] << 24),
+                         __uint_as_float(q[8] | q[9] << 8 | q[10] << 16 | q[11] << 24), __uint_as_float(c0),
+                         __uint_as_float(c1));
+    parents[i] = nd.parent;
+}
+
+template <bool kAny>
+__global__ void __launch_bounds__(kTraceThreads)
+    k_trace_quantised(const mlbvh_qnode* __restrict__ qnodes, const uint32_t* __restrict__ parents,
+                      const mlbvh_qtri* __restrict__ qtris, const mlbvh_qheader* __restrict__ header,
+                      const float4* __restrict__ rays, float4* __restrict__ hits, uint32_t n)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float4 a = __ldg(rays + 2 * (size_t)i), b = __ldg(rays + 2 * (size_t)i + 1);
+    const f3 ro = mk(a.x, a.y, a.z), rd = mk(b.x, b.y, b.z);
+    HitRecord hit;
+    hit.t = b.w;
+    hit.u = 0.0f;
+    hit.v = 0.0f;
+    hit.ng = mk(0.0f, 0.0f, 0.0f);
+    hit.tri = 0xFFFFFFFFu;
+    trace_quantised<kAny>(hit, qnodes, parents, qtris, __ldg(&header->root), __ldg(&header->eBase), ro, rd, inv_rd(rd),
+                          a.w);
+    hits[2 * (size_t)i] = make_float4(hit.t, 0.0f, hit.u, hit.v);
+    hits[2 * (size_t)i + 1] = make_float4(hit.ng.x, hit.ng.y, hit.ng.z, __uint_as_float(hit.tri));
+}
+
+}  // namespace
+
+mlbvh_status quantise(const mlbvh_internal_node* dNodes, const mlbvh_node_index* dRoot, const mlbvh_triangle* dTris,
+                      uint32_t n, mlbvh_qnode* dQNodes, uint32_t* dQParents, mlbvh_qtri* dQTris,
+                      mlbvh_qheader* dQHeader, cudaStream_t stream)
+{
+    if (n == 0 || n > kQMaxLeaves) return fail(MLBVH_ERR_INVALID_ARG, "nTriangles must be in [1, 2^23]");
+    if (!dRoot || !dTris || !dQTris || !dQHeader || (n > 1 && (!dNodes || !dQNodes || !dQParents)))
+        return fail(MLBVH_ERR_INVALID_ARG, "null pointer");
+    if (!aligned16(dNodes) || !aligned16(dRoot) || !aligned16(dTris) || !aligned16(dQNodes) || !aligned16(dQParents) ||
+        !aligned16(dQTris) || !aligned16(dQHeader))
+        return fail(MLBVH_ERR_INVALID_ARG, "device pointers must be 16-byte aligned");
+    const uint32_t threads = n > 1 ? n - 1 : 1;
+    k_quantise<<<(threads + kQuantiseThreads - 1) / kQuantiseThreads, kQuantiseThreads, 0, stream>>>(
+        dNodes, dRoot, reinterpret_cast<const float*>(dTris), n, dQNodes, dQParents, dQTris, dQHeader);
+    MLBVH_CHECK_LAUNCH("k_quantise");
+    return MLBVH_OK;
+}
+
+mlbvh_status trace_quantised(const mlbvh_qnode* dQNodes, const uint32_t* dQParents, const mlbvh_qtri* dQTris,
+                             const mlbvh_qheader* dQHeader, const mlbvh_ray* dRays, mlbvh_hit* dHits, uint32_t nRays,
+                             int rayQuery, cudaStream_t stream)
+{
+    if (nRays == 0) return MLBVH_OK;
+    if (!dQTris || !dQHeader || !dRays || !dHits) return fail(MLBVH_ERR_INVALID_ARG, "null pointer");
+    if (!aligned16(dQNodes) || !aligned16(dQParents) || !aligned16(dQTris) || !aligned16(dQHeader) ||
+        !aligned16(dRays) || !aligned16(dHits))
+        return fail(MLBVH_ERR_INVALID_ARG, "device pointers must be 16-byte aligned");
+    if (rayQuery != MLBVH_RAY_QUERY_CLOSEST && rayQuery != MLBVH_RAY_QUERY_ANY)
+        return fail(MLBVH_ERR_INVALID_ARG, "rayQuery must be MLBVH_RAY_QUERY_CLOSEST or MLBVH_RAY_QUERY_ANY");
+    const unsigned blocks = (nRays + kTraceThreads - 1) / kTraceThreads;
+    const float4* rays = reinterpret_cast<const float4*>(dRays);
+    float4* hits = reinterpret_cast<float4*>(dHits);
+    if (rayQuery == MLBVH_RAY_QUERY_ANY)
+        k_trace_quantised<true><<<blocks, kTraceThreads, 0, stream>>>(dQNodes, dQParents, dQTris, dQHeader, rays, hits,
+                                                                      nRays);
+    else
+        k_trace_quantised<false><<<blocks, kTraceThreads, 0, stream>>>(dQNodes, dQParents, dQTris, dQHeader, rays, hits,
+                                                                       nRays);
+    MLBVH_CHECK_LAUNCH("k_trace_quantised");
+    return MLBVH_OK;
+}
+
+}  // namespace mlbvh

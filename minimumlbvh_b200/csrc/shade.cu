@@ -79,36 +79,79 @@ __device__ __forceinline__ void pcg_advance(Pcg& r, uint64_t delta)
     r.state = accMult * r.state + accPlus;
 }
 
-// Adds per-thread traversal counts to stats[1] (node visits) and stats[2]
-// (triangle tests) with one atomic per warp; AO rays also to stats[3], [4].
-__device__ __forceinline__ void add_stats(unsigned long long* stats, uint32_t visits, uint32_t tests, bool aoRays)
+// Traversal counters of the counting variants: visits = internal-node loads,
+// tests = triangle tests, ups = parent-word loads (quantised tree only).
+struct Counts {
+    uint32_t visits = 0, tests = 0, ups = 0;
+};
+
+// Adds per-thread counts to stats[1] (node visits), [2] (triangle tests) and
+// [5] (parent loads) with one atomic per warp; AO rays also to [3], [4], [6].
+__device__ __forceinline__ void add_stats(unsigned long long* stats, const Counts& c, bool aoRays)
 {
-    unsigned long long v = visits, t = tests;
+    unsigned long long v = c.visits, t = c.tests, u = c.ups;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
         v += __shfl_xor_sync(0xffffffffu, v, o);
         t += __shfl_xor_sync(0xffffffffu, t, o);
+        u += __shfl_xor_sync(0xffffffffu, u, o);
     }
     if ((threadIdx.x & 31) == 0) {
         atomicAdd(stats + 1, v);
         atomicAdd(stats + 2, t);
+        atomicAdd(stats + 5, u);
         if (aoRays) {
             atomicAdd(stats + 3, v);
             atomicAdd(stats + 4, t);
+            atomicAdd(stats + 6, u);
         }
     }
 }
 
+// The two tree formats the AO kernels run over.
+struct PlainTree {
+    const mlbvh_internal_node* nodes;
+    const float* tris;
+    const mlbvh_node_index* rootPtr;
+    struct Ctx {
+        uint32_t root;
+    };
+    __device__ __forceinline__ Ctx context() const { return Ctx{__ldg(rootPtr)}; }
+    template <bool kAny, bool kCount>
+    __device__ __forceinline__ void trace(const Ctx& c, HitRecord& hit, f3 ro, f3 rd, Counts& n) const
+    {
+        trace_stackfree<kAny, kCount>(hit, nodes, tris, c.root, ro, rd, inv_rd(rd), 0.0f, &n.visits, &n.tests);
+    }
+};
+struct QuantTree {
+    const mlbvh_qnode* qnodes;
+    const uint32_t* parents;
+    const mlbvh_qtri* qtris;
+    const mlbvh_qheader* header;
+    struct Ctx {
+        uint32_t root;
+        int eBase;
+    };
+    __device__ __forceinline__ Ctx context() const
+    {
+        return Ctx{__ldg(&header->root), __ldg(&header->eBase)};
+    }
+    template <bool kAny, bool kCount>
+    __device__ __forceinline__ void trace(const Ctx& c, HitRecord& hit, f3 ro, f3 rd, Counts& n) const
+    {
+        trace_quantised<kAny, kCount>(hit, qnodes, parents, qtris, c.root, c.eBase, ro, rd, inv_rd(rd), 0.0f,
+                                      &n.visits, &n.tests, &n.ups);
+    }
+};
+
 // Primary rays of ao (main_gpu.cu:121-144): closest hit, flip the normal
 // towards the viewer, AO origin p + n * 1e-3.
-template <bool kCount>
+template <class Tree, bool kCount>
 __global__ void __launch_bounds__(kTileW* kTileH)
-    k_ao_primary(mlbvh_ray_generator gen, int w, int h, const mlbvh_node_index* __restrict__ rootPtr,
-                 const mlbvh_internal_node* __restrict__ nodes, const float* __restrict__ tris,
-                 AoRecord* __restrict__ records, uint32_t* __restrict__ queueCount, uint32_t* __restrict__ counts,
-                 unsigned long long* __restrict__ stats)
+    k_ao_primary(mlbvh_ray_generator gen, int w, int h, Tree tree, AoRecord* __restrict__ records,
+                 uint32_t* __restrict__ queueCount, uint32_t* __restrict__ counts, unsigned long long* __restrict__ stats)
 {
-    uint32_t visits = 0, tests = 0;
+    Counts cnt;
     int xi, yi;
     const bool inside = tile_pixel(w, h, xi, yi);
     bool isHit = false;
@@ -121,7 +164,7 @@ __global__ void __launch_bounds__(kTileW* kTileH)
         HitRecord hit;
         hit.t = kFltMax;
         hit.tri = 0xFFFFFFFFu;
-        trace_stackfree<false, kCount>(hit, nodes, tris, __ldg(rootPtr), ro, rd, inv_rd(rd), 0.0f, &visits, &tests);
+        tree.template trace<false, kCount>(tree.context(), hit, ro, rd, cnt);
         if (hit.t == kFltMax) {
             counts[pixel] = 0xFFFFFFFFu;
         } else {
@@ -133,7 +176,7 @@ __global__ void __launch_bounds__(kTileW* kTileH)
             isHit = true;
         }
     }
-    if (kCount) add_stats(stats, visits, tests, false);
+    if (kCount) add_stats(stats, cnt, false);
     // warp-aggregated append to the hit queue
     const uint32_t mask = __ballot_sync(0xffffffffu, isHit);
     if (mask == 0u) return;
@@ -151,17 +194,16 @@ __global__ void __launch_bounds__(kTileW* kTileH)
 // AO rays (main_gpu.cu:146-173): item = (queue entry, sample). Each warp takes
 // 32 consecutive items; per-pixel occlusion counts are reduced across the
 // lanes of one pixel before a single atomic add.
-template <bool kCount>
+template <class Tree, bool kCount>
 __global__ void __launch_bounds__(kAoThreads)
     k_ao_rays(const AoRecord* __restrict__ records, const uint32_t* __restrict__ queueCount,
               uint32_t* __restrict__ workCounter, int w, int nSamples, float radius, uint32_t seed, int useSobol,
-              const mlbvh_node_index* __restrict__ rootPtr, const mlbvh_internal_node* __restrict__ nodes,
-              const float* __restrict__ tris, uint32_t* __restrict__ counts, unsigned long long* __restrict__ stats)
+              Tree tree, uint32_t* __restrict__ counts, unsigned long long* __restrict__ stats)
 {
-    uint32_t visits = 0, tests = 0;
+    Counts cnt;
     const int lane = threadIdx.x & 31;
     const uint64_t total = (uint64_t)(*queueCount) * (uint64_t)nSamples;
-    const uint32_t root = __ldg(rootPtr);
+    const typename Tree::Ctx ctx = tree.context();
     for (;;) {
         unsigned long long base = 0;
         if (lane == 0) base = atomicAdd(reinterpret_cast<unsigned long long*>(workCounter), 32ull);
@@ -195,7 +237,7 @@ __global__ void __launch_bounds__(kAoThreads)
             HitRecord hit;
             hit.t = radius;
             hit.tri = 0xFFFFFFFFu;
-            trace_stackfree<true, kCount>(hit, nodes, tris, root, origin, dir, inv_rd(dir), 0.0f, &visits, &tests);
+            tree.template trace<true, kCount>(ctx, hit, origin, dir, cnt);
             occluded = hit.t != radius;
         }
         const uint32_t peers = __match_any_sync(0xffffffffu, entry);
@@ -208,7 +250,7 @@ __global__ void __launch_bounds__(kAoThreads)
             }
         }
     }
-    if (kCount) add_stats(stats, visits, tests, true);
+    if (kCount) add_stats(stats, cnt, true);
 }
 
 // The tail of ao (main_gpu.cu:169-176): ao accumulates 1/nSample per occluded
@@ -357,16 +399,70 @@ mlbvh_status check_image(int w, int h)
     return MLBVH_OK;
 }
 
+template <class Tree>
 int ao_ray_blocks()
 {
     static int blocksPerSm = 0;
     if (blocksPerSm == 0) {
         int b = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_ao_rays<false>, kAoThreads, 0) != cudaSuccess || b <= 0)
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_ao_rays<Tree, false>, kAoThreads, 0) != cudaSuccess ||
+            b <= 0)
             b = 8;
         blocksPerSm = b;
     }
     return blocksPerSm * device_sm_count();
+}
+
+// The AO launch chain over either tree format (arguments already checked).
+template <class Tree>
+mlbvh_status launch_ao(uint32_t* dPixels, uint32_t* dOccluded, int w, int h, const mlbvh_ray_generator& cam,
+                       const Tree& tree, int useSobol, int nSamples, float radius, uint32_t seed,
+                       unsigned long long* dStats, void* dScratch, size_t scratchBytes, cudaStream_t stream)
+{
+    const RenderLayout L = render_layout(w, h);
+    if (scratchBytes < L.total) return fail(MLBVH_ERR_INVALID_ARG, "scratch smaller than mlbvh_render_scratch_bytes");
+    char* s = static_cast<char*>(dScratch);
+    uint32_t* header = reinterpret_cast<uint32_t*>(s + L.header);
+    AoRecord* records = reinterpret_cast<AoRecord*>(s + L.records);
+    uint32_t* counts = reinterpret_cast<uint32_t*>(s + L.counts);
+
+    cudaError_t e = cudaMemsetAsync(header, 0, 16, stream);  // queue count, 64-bit work counter
+    if (e == cudaSuccess && dStats) e = cudaMemsetAsync(dStats, 0, 8 * sizeof(unsigned long long), stream);
+    if (e != cudaSuccess) return fail(MLBVH_ERR_CUDA, cudaGetErrorString(e));
+    const dim3 grid = tile_grid(w, h);
+    if (dStats)
+        k_ao_primary<Tree, true><<<grid, kTileW * kTileH, 0, stream>>>(cam, w, h, tree, records, header, counts, dStats);
+    else
+        k_ao_primary<Tree, false><<<grid, kTileW * kTileH, 0, stream>>>(cam, w, h, tree, records, header, counts,
+                                                                        nullptr);
+    MLBVH_CHECK_LAUNCH("k_ao_primary");
+    ProfileEvents ev = take_profile_events();
+    if (ev.start) cudaEventRecord(ev.start, stream);
+    if (dStats)
+        k_ao_rays<Tree, true><<<ao_ray_blocks<Tree>(), kAoThreads, 0, stream>>>(
+            records, header, header + 2, w, nSamples, radius, seed, useSobol, tree, counts, dStats);
+    else
+        k_ao_rays<Tree, false><<<ao_ray_blocks<Tree>(), kAoThreads, 0, stream>>>(
+            records, header, header + 2, w, nSamples, radius, seed, useSobol, tree, counts, nullptr);
+    MLBVH_CHECK_LAUNCH("k_ao_rays");
+    if (ev.stop) cudaEventRecord(ev.stop, stream);
+    const int px = w * h;
+    k_ao_finish<<<(px + kFinishThreads - 1) / kFinishThreads, kFinishThreads, 0, stream>>>(
+        counts, px, nSamples, dPixels, dOccluded, header, dStats);
+    MLBVH_CHECK_LAUNCH("k_ao_finish");
+    return MLBVH_OK;
+}
+
+mlbvh_status check_ao_args(int w, int h, int nSamples, const void* dPixels, const void* dOccluded,
+                           const void* dScratch, const unsigned long long* dStats)
+{
+    if (mlbvh_status s = check_image(w, h)) return s;
+    if (nSamples <= 0 || nSamples > 65536) return fail(MLBVH_ERR_INVALID_ARG, "nSamples must be in [1, 65536]");
+    if (!dScratch) return fail(MLBVH_ERR_INVALID_ARG, "null scratch pointer");
+    if (!aligned16(dPixels) || !aligned16(dOccluded) || !aligned16(dScratch) ||
+        (reinterpret_cast<uintptr_t>(dStats) & 7u))
+        return fail(MLBVH_ERR_INVALID_ARG, "device pointers must be 16-byte aligned");
+    return MLBVH_OK;
 }
 
 }  // namespace
@@ -396,47 +492,28 @@ mlbvh_status render_ao(uint32_t* dPixels, uint32_t* dOccluded, int w, int h, con
                        int useSobol, int nSamples, float radius, uint32_t seed, unsigned long long* dStats,
                        void* dScratch, size_t scratchBytes, cudaStream_t stream)
 {
-    if (mlbvh_status s = check_image(w, h)) return s;
-    if (nSamples <= 0 || nSamples > 65536) return fail(MLBVH_ERR_INVALID_ARG, "nSamples must be in [1, 65536]");
-    if (!dRoot || !dTris || !dScratch) return fail(MLBVH_ERR_INVALID_ARG, "null pointer");
-    if (!aligned16(dPixels) || !aligned16(dOccluded) || !aligned16(dRoot) || !aligned16(dNodes) ||
-        !aligned16(dTris) || !aligned16(dScratch) || (reinterpret_cast<uintptr_t>(dStats) & 7u))
+    if (mlbvh_status s = check_ao_args(w, h, nSamples, dPixels, dOccluded, dScratch, dStats)) return s;
+    if (!dRoot || !dTris) return fail(MLBVH_ERR_INVALID_ARG, "null pointer");
+    if (!aligned16(dRoot) || !aligned16(dNodes) || !aligned16(dTris))
         return fail(MLBVH_ERR_INVALID_ARG, "device pointers must be 16-byte aligned");
-    const RenderLayout L = render_layout(w, h);
-    if (scratchBytes < L.total) return fail(MLBVH_ERR_INVALID_ARG, "scratch smaller than mlbvh_render_scratch_bytes");
-    char* s = static_cast<char*>(dScratch);
-    uint32_t* header = reinterpret_cast<uint32_t*>(s + L.header);
-    AoRecord* records = reinterpret_cast<AoRecord*>(s + L.records);
-    uint32_t* counts = reinterpret_cast<uint32_t*>(s + L.counts);
-    const float* tris = reinterpret_cast<const float*>(dTris);
+    const PlainTree tree{dNodes, reinterpret_cast<const float*>(dTris), dRoot};
+    return launch_ao(dPixels, dOccluded, w, h, cam, tree, useSobol, nSamples, radius, seed, dStats, dScratch,
+                     scratchBytes, stream);
+}
 
-    cudaError_t e = cudaMemsetAsync(header, 0, 16, stream);  // queue count, 64-bit work counter
-    if (e == cudaSuccess && dStats) e = cudaMemsetAsync(dStats, 0, 5 * sizeof(unsigned long long), stream);
-    if (e != cudaSuccess) return fail(MLBVH_ERR_CUDA, cudaGetErrorString(e));
-    const dim3 grid = tile_grid(w, h);
-    if (dStats)
-        k_ao_primary<true><<<grid, kTileW * kTileH, 0, stream>>>(cam, w, h, dRoot, dNodes, tris, records, header,
-                                                                 counts, dStats);
-    else
-        k_ao_primary<false><<<grid, kTileW * kTileH, 0, stream>>>(cam, w, h, dRoot, dNodes, tris, records, header,
-                                                                  counts, nullptr);
-    MLBVH_CHECK_LAUNCH("k_ao_primary");
-    ProfileEvents ev = take_profile_events();
-    if (ev.start) cudaEventRecord(ev.start, stream);
-    if (dStats)
-        k_ao_rays<true><<<ao_ray_blocks(), kAoThreads, 0, stream>>>(records, header, header + 2, w, nSamples, radius,
-                                                                    seed, useSobol, dRoot, dNodes, tris, counts, dStats);
-    else
-        k_ao_rays<false><<<ao_ray_blocks(), kAoThreads, 0, stream>>>(records, header, header + 2, w, nSamples, radius,
-                                                                     seed, useSobol, dRoot, dNodes, tris, counts,
-                                                                     nullptr);
-    MLBVH_CHECK_LAUNCH("k_ao_rays");
-    if (ev.stop) cudaEventRecord(ev.stop, stream);
-    const int px = w * h;
-    k_ao_finish<<<(px + kFinishThreads - 1) / kFinishThreads, kFinishThreads, 0, stream>>>(
-        counts, px, nSamples, dPixels, dOccluded, header, dStats);
-    MLBVH_CHECK_LAUNCH("k_ao_finish");
-    return MLBVH_OK;
+mlbvh_status render_ao_quantised(uint32_t* dPixels, uint32_t* dOccluded, int w, int h, const mlbvh_ray_generator& cam,
+                                 const mlbvh_qnode* dQNodes, const uint32_t* dQParents, const mlbvh_qtri* dQTris,
+                                 const mlbvh_qheader* dQHeader, int useSobol, int nSamples, float radius,
+                                 uint32_t seed, unsigned long long* dStats, void* dScratch, size_t scratchBytes,
+                                 cudaStream_t stream)
+{
+    if (mlbvh_status s = check_ao_args(w, h, nSamples, dPixels, dOccluded, dScratch, dStats)) return s;
+    if (!dQTris || !dQHeader) return fail(MLBVH_ERR_INVALID_ARG, "null pointer");
+    if (!aligned16(dQNodes) || !aligned16(dQParents) || !aligned16(dQTris) || !aligned16(dQHeader))
+        return fail(MLBVH_ERR_INVALID_ARG, "device pointers must be 16-byte aligned");
+    const QuantTree tree{dQNodes, dQParents, dQTris, dQHeader};
+    return launch_ao(dPixels, dOccluded, w, h, cam, tree, useSobol, nSamples, radius, seed, dStats, dScratch,
+                     scratchBytes, stream);
 }
 
 mlbvh_status render_pt(float* dAccum, int w, int h, const mlbvh_ray_generator& cam, const mlbvh_node_index* dRoot,

@@ -1158,3 +1158,284 @@ void orc_pack(uint32_t* pixels, const float* accum4, int n)
                               powf(a[2] / a[3], 1.0f / 2.2f), 1.0f);
     }
 }
+
+/* ------------------------------------------------------------ quantised tree
+ * Restates csrc/quantise.cu and trace_quantised of the device header (this
+ * node format has no reference counterpart; its checker is this code plus
+ * the FP32 traversal above, whose closest hits it must reproduce).
+ * Directed-rounding sums are formed exactly with the TwoSum error term
+ * (Knuth), so they equal CUDA's __fadd_rd / __fadd_ru except possibly in the
+ * sign of a zero result, which no comparison here can see. */
+#define ORC_QMASK 0x7FFFFFu
+
+static inline float two_sum_err(float a, float b, float s)
+{
+    float bp = s - a;
+    float ap = s - bp;
+    return (a - ap) + (b - bp);
+}
+static inline float add_rd(float a, float b)
+{
+    float s = a + b;
+    return two_sum_err(a, b, s) < 0.0f ? nextafterf(s, -INFINITY) : s;
+}
+static inline float add_ru(float a, float b)
+{
+    float s = a + b;
+    return two_sum_err(a, b, s) > 0.0f ? nextafterf(s, INFINITY) : s;
+}
+static inline float pow2f_(int e)
+{
+    uint32_t b = (uint32_t)(127 + e) << 23;
+    float f;
+    memcpy(&f, &b, 4);
+    return f;
+}
+static inline int step_exponent(float d)
+{
+    if (!(d >= 1.17549435e-38f)) return -126;
+    uint32_t bits;
+    memcpy(&bits, &d, 4);
+    int e = (int)((bits >> 23) & 0xFFu) - 126 - 8;
+    if (e < -126) e = -126;
+    if (255.0f * pow2f_(e) < d) e += 1;
+    return e;
+}
+static inline float qdec_lo(float o, uint32_t q, float s) { return add_rd(o, (float)q * s); }
+static inline float qdec_hi(float o, uint32_t q, float s) { return add_ru(o, (float)q * s); }
+static inline uint32_t quant_lo(float v, float o, float s)
+{
+    float q = floorf(add_rd(v, -o) / s);
+    uint32_t qi = q <= 0.0f ? 0u : (q >= 255.0f ? 255u : (uint32_t)q);
+    while (qi > 0u && qdec_lo(o, qi, s) > v) --qi;
+    return qi;
+}
+static inline uint32_t quant_hi(float v, float o, float s)
+{
+    float q = ceilf(add_ru(v, -o) / s);
+    uint32_t qi = q <= 0.0f ? 0u : (q >= 255.0f ? 255u : (uint32_t)q);
+    while (qi < 255u && qdec_hi(o, qi, s) < v) ++qi;
+    return qi;
+}
+static void tri_box(const orc_triangle* t, orc_aabb* b)
+{
+    aabb_set_empty(b);
+    for (int j = 0; j < 3; ++j) aabb_extend_p(b, t->v[j]);
+}
+
+/* k_quantise (csrc/quantise.cu). qnodes: 8 words per node; qtris: 12 words
+ * per leaf; header: 4 words. Returns 0. */
+int orc_quantise(const orc_node* nodes, uint32_t root, const orc_triangle* tris, uint32_t n,
+                 uint32_t* qnodes, uint32_t* parents, uint32_t* qtris, uint32_t* header)
+{
+    orc_aabb rb;
+    if (root & ORC_LEAF_BIT) tri_box(&tris[root & ~ORC_LEAF_BIT], &rb);
+    else
+    {
+        rb.lower = min3(nodes[root].aabbs[0].lower, nodes[root].aabbs[1].lower);
+        rb.upper = max3(nodes[root].aabbs[0].upper, nodes[root].aabbs[1].upper);
+    }
+    float d = fmaxf(fmaxf(add_ru(rb.upper.x, -rb.lower.x), add_ru(rb.upper.y, -rb.lower.y)),
+                    add_ru(rb.upper.z, -rb.lower.z));
+    int eBase = step_exponent(d);
+    header[0] = (root & ORC_LEAF_BIT) ? ORC_LEAF_BIT : root;
+    memcpy(&header[1], &eBase, 4);
+    header[2] = n;
+    header[3] = 0;
+#define PUT_QTRI(pos, t)                                                  \
+    do {                                                                  \
+        memcpy(qtris + 12 * (size_t)(pos), &tris[t], 36);                 \
+        qtris[12 * (size_t)(pos) + 9] = (t);                              \
+        qtris[12 * (size_t)(pos) + 10] = 0;                               \
+        qtris[12 * (size_t)(pos) + 11] = 0;                               \
+    } while (0)
+    if (root & ORC_LEAF_BIT) PUT_QTRI(0, root & ~ORC_LEAF_BIT);
+    for (uint32_t i = 0; i + 1 < n; ++i)
+    {
+        const orc_node* nd = &nodes[i];
+        orc_f3 o = min3(nd->aabbs[0].lower, nd->aabbs[1].lower);
+        orc_f3 top = max3(nd->aabbs[0].upper, nd->aabbs[1].upper);
+        float oo[3] = {o.x, o.y, o.z}, tt[3] = {top.x, top.y, top.z};
+        float lo[2][3] = {{nd->aabbs[0].lower.x, nd->aabbs[0].lower.y, nd->aabbs[0].lower.z},
+                          {nd->aabbs[1].lower.x, nd->aabbs[1].lower.y, nd->aabbs[1].lower.z}};
+        float hi[2][3] = {{nd->aabbs[0].upper.x, nd->aabbs[0].upper.y, nd->aabbs[0].upper.z},
+                          {nd->aabbs[1].upper.x, nd->aabbs[1].upper.y, nd->aabbs[1].upper.z}};
+        uint32_t code = 0, q[12];
+        for (int a = 0; a < 3; ++a)
+        {
+            int e = step_exponent(add_ru(tt[a], -oo[a]));
+            if (e < eBase - 31) e = eBase - 31;
+            int k = eBase - e;
+            if (k < 0) k = 0;
+            code |= (uint32_t)k << (5 * a);
+            int es = eBase - k;
+            float s = pow2f_(es < -126 ? -126 : es);
+            q[a] = quant_lo(lo[0][a], oo[a], s);
+            q[3 + a] = quant_hi(hi[0][a], oo[a], s);
+            q[6 + a] = quant_lo(lo[1][a], oo[a], s);
+            q[9 + a] = quant_hi(hi[1][a], oo[a], s);
+        }
+        uint32_t c0 = nd->children[0], c1 = nd->children[1];
+        if (c0 & ORC_LEAF_BIT) { PUT_QTRI(i, c0 & ~ORC_LEAF_BIT); c0 = ORC_LEAF_BIT | i; }
+        if (c1 & ORC_LEAF_BIT) { PUT_QTRI(i + 1, c1 & ~ORC_LEAF_BIT); c1 = ORC_LEAF_BIT | (i + 1); }
+        c0 |= (code & 0xFFu) << 23;
+        c1 |= ((code >> 8) & 0xFFu) << 23;
+        uint32_t* w = qnodes + 8 * (size_t)i;
+        memcpy(&w[0], &o, 12);
+        w[3] = q[0] | q[1] << 8 | q[2] << 16 | q[3] << 24;
+        w[4] = q[4] | q[5] << 8 | q[6] << 16 | q[7] << 24;
+        w[5] = q[8] | q[9] << 8 | q[10] << 16 | q[11] << 24;
+        w[6] = c0;
+        w[7] = c1;
+        parents[i] = nd->parent;
+    }
+#undef PUT_QTRI
+    return 0;
+}
+
+static inline void qnode_boxes(const uint32_t* w, int eBase, orc_aabb* b0, orc_aabb* b1)
+{
+    uint32_t code = ((w[6] >> 23) & 0xFFu) | (((w[7] >> 23) & 0xFFu) << 8);
+    int ex = eBase - (int)(code & 31u), ey = eBase - (int)((code >> 5) & 31u), ez = eBase - (int)((code >> 10) & 31u);
+    float sx = pow2f_(ex < -126 ? -126 : ex), sy = pow2f_(ey < -126 ? -126 : ey), sz = pow2f_(ez < -126 ? -126 : ez);
+    float o[3];
+    memcpy(o, w, 12);
+    uint32_t w0 = w[3], w1 = w[4], w2 = w[5];
+    b0->lower = f3(qdec_lo(o[0], w0 & 255u, sx), qdec_lo(o[1], (w0 >> 8) & 255u, sy), qdec_lo(o[2], (w0 >> 16) & 255u, sz));
+    b0->upper = f3(qdec_hi(o[0], w0 >> 24, sx), qdec_hi(o[1], w1 & 255u, sy), qdec_hi(o[2], (w1 >> 8) & 255u, sz));
+    b1->lower = f3(qdec_lo(o[0], (w1 >> 16) & 255u, sx), qdec_lo(o[1], w1 >> 24, sy), qdec_lo(o[2], w2 & 255u, sz));
+    b1->upper = f3(qdec_hi(o[0], (w2 >> 8) & 255u, sx), qdec_hi(o[1], (w2 >> 16) & 255u, sy), qdec_hi(o[2], w2 >> 24, sz));
+}
+
+/* Checks that every decoded child box of the quantised tree contains the
+ * FP32 child box of the same node. Returns 1 when all do. */
+int orc_check_quantised(const orc_node* nodes, uint32_t n, const uint32_t* qnodes, const uint32_t* header)
+{
+    int eBase;
+    memcpy(&eBase, &header[1], 4);
+    for (uint32_t i = 0; i + 1 < n; ++i)
+    {
+        orc_aabb b[2];
+        qnode_boxes(qnodes + 8 * (size_t)i, eBase, &b[0], &b[1]);
+        for (int c = 0; c < 2; ++c)
+        {
+            const orc_aabb* e = &nodes[i].aabbs[c];
+            if (b[c].lower.x > e->lower.x || b[c].lower.y > e->lower.y || b[c].lower.z > e->lower.z ||
+                b[c].upper.x < e->upper.x || b[c].upper.y < e->upper.y || b[c].upper.z < e->upper.z)
+                return 0;
+        }
+    }
+    return 1;
+}
+
+typedef struct {
+    const uint32_t *qnodes, *parents, *qtris;
+    uint32_t root;
+    int eBase;
+    const orc_ray* rays;
+    int query;
+    orc_hit* hits;
+    uint32_t *visits, *tests, *ups;
+} qtrace_ctx;
+
+/* trace_quantised (include/mlbvh_device.cuh): the stack-free state machine
+ * over quantised nodes; "came from the parent" is "came from neither child",
+ * and the parent word is read only when moving up. */
+static void qtrace_one(const qtrace_ctx* c, orc_hit* hit, orc_f3 ro, orc_f3 rd, float tmin, uint32_t* nv, uint32_t* nt,
+                       uint32_t* nu)
+{
+    orc_f3 inv = inv_rd(rd);
+    uint32_t curr = c->root, prev = ORC_INVALID;
+    while (curr != ORC_INVALID)
+    {
+        if (curr & ORC_LEAF_BIT)
+        {
+            (*nt)++;
+            const uint32_t* q = c->qtris + 12 * (size_t)(curr & ORC_QMASK);
+            orc_f3 v[3];
+            memcpy(v, q, 36);
+            float t, u, vv;
+            orc_f3 ng;
+            if (intersect_tri(&t, &u, &vv, &ng, tmin, hit->t, ro, rd, v[0], v[1], v[2]))
+            {
+                hit->t = t;
+                hit->u = u;
+                hit->v = vv;
+                hit->ng = ng;
+                hit->triangleIndex = q[9];
+                if (c->query == 1) break;
+            }
+            uint32_t s = curr;
+            curr = prev;
+            prev = s;
+            continue;
+        }
+        (*nv)++;
+        const uint32_t* w = c->qnodes + 8 * (size_t)curr;
+        orc_aabb b0, b1;
+        qnode_boxes(w, c->eBase, &b0, &b1);
+        uint32_t c0 = w[6] & (ORC_LEAF_BIT | ORC_QMASK), c1 = w[7] & (ORC_LEAF_BIT | ORC_QMASK);
+        float lmin, lmax, rmin, rmax;
+        slabs(ro, inv, &b0, hit->t, &lmin, &lmax);
+        slabs(ro, inv, &b1, hit->t, &rmin, &rmax);
+        lmin = smax(lmin, tmin);
+        rmin = smax(rmin, tmin);
+        int hitL = lmin <= lmax, hitR = rmin <= rmax;
+        uint32_t nearN = c0, farN = c1;
+        int nHits = 0;
+        if (hitL && hitR)
+        {
+            if (rmin < lmin) { nearN = c1; farN = c0; }
+            nHits = 2;
+        }
+        else if (hitL || hitR)
+        {
+            nHits = 1;
+            nearN = hitR ? farN : nearN;
+        }
+        int fromParent = prev != c0 && prev != c1, up;
+        uint32_t next = ORC_INVALID;
+        if (fromParent) { up = nHits == 0; next = nearN; }
+        else if (prev == nearN) { up = nHits != 2; next = farN; }
+        else up = 1;
+        if (up) { (*nu)++; next = c->parents[curr]; }
+        prev = curr;
+        curr = next;
+    }
+}
+
+static void qtrace_range(void* p, uint32_t b, uint32_t e)
+{
+    qtrace_ctx* c = (qtrace_ctx*)p;
+    for (uint32_t i = b; i < e; ++i)
+    {
+        const orc_ray* r = &c->rays[i];
+        orc_hit hit;
+        hit_init(&hit, r->tmax);
+        uint32_t nv = 0, nt = 0, nu = 0;
+        qtrace_one(c, &hit, f3(r->ro[0], r->ro[1], r->ro[2]), f3(r->rd[0], r->rd[1], r->rd[2]), r->tmin, &nv, &nt, &nu);
+        c->hits[i] = hit;
+        if (c->visits) c->visits[i] = nv;
+        if (c->tests) c->tests[i] = nt;
+        if (c->ups) c->ups[i] = nu;
+    }
+}
+
+void orc_trace_quantised(const uint32_t* qnodes, const uint32_t* parents, const uint32_t* qtris, const uint32_t* header,
+                         const orc_ray* rays, uint32_t nRays, int query, orc_hit* hits, uint32_t* visits,
+                         uint32_t* tests, uint32_t* ups)
+{
+    qtrace_ctx c;
+    c.qnodes = qnodes;
+    c.parents = parents;
+    c.qtris = qtris;
+    c.root = header[0];
+    memcpy(&c.eBase, &header[1], 4);
+    c.rays = rays;
+    c.query = query;
+    c.hits = hits;
+    c.visits = visits;
+    c.tests = tests;
+    c.ups = ups;
+    orc_parallel_for(nRays, 1024, qtrace_range, &c);
+}

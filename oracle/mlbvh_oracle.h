@@ -120,6 +120,16 @@ void orc_pack(uint32_t* pixels, const float* accum4, int n);
 void orc_render_normal(uint32_t* pixels, int w, int h, const orc_camera* cam, uint32_t root,
                        const orc_node* nodes, const orc_triangle* tris);
 
+/* Quantised tree (no reference counterpart): the conversion and traversal of
+ * csrc/quantise.cu and the device header, word for word. qnodes 8 words per
+ * internal node, parents 1, qtris 12 words per leaf, header 4 words. */
+int orc_quantise(const orc_node* nodes, uint32_t root, const orc_triangle* tris, uint32_t n,
+                 uint32_t* qnodes, uint32_t* parents, uint32_t* qtris, uint32_t* header);
+int orc_check_quantised(const orc_node* nodes, uint32_t n, const uint32_t* qnodes, const uint32_t* header);
+void orc_trace_quantised(const uint32_t* qnodes, const uint32_t* parents, const uint32_t* qtris, const uint32_t* header,
+                         const orc_ray* rays, uint32_t nRays, int query, orc_hit* hits, uint32_t* visits,
+                         uint32_t* tests, uint32_t* ups);
+
 #ifdef __cplusplus
 }
 #endif

@@ -70,6 +70,9 @@ def oracle() -> ctypes.CDLL:
             "orc_render_pt": (None, [_vp, _i32, _i32, _vp, _u32, _vp, _vp, _vp, _i32, _i32, _i32, _i32]),
             "orc_pack": (None, [_vp, _vp, _i32]),
             "orc_render_normal": (None, [_vp, _i32, _i32, _vp, _u32, _vp, _vp]),
+            "orc_quantise": (_i32, [_vp, _u32, _vp, _u32, _vp, _vp, _vp, _vp]),
+            "orc_check_quantised": (_i32, [_vp, _u32, _vp, _vp]),
+            "orc_trace_quantised": (None, [_vp, _vp, _vp, _vp, _vp, _u32, _i32, _vp, _vp, _vp, _vp]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -221,3 +224,34 @@ def pack(accum, n):
     pixels = np.zeros(n, np.uint32)
     oracle().orc_pack(P(pixels), P(np.ascontiguousarray(accum, np.float32)), n)
     return pixels
+
+
+def quantise(b: dict, tris: np.ndarray):
+    """Oracle quantised tree of an oracle build: dict of qnodes (n-1, 8),
+    parents (n-1,), qtris (n, 12) and header (4,), all uint32."""
+    tris = np.ascontiguousarray(tris, np.float32).reshape(-1, 9)
+    n = len(tris)
+    qn = np.zeros((max(n - 1, 1), 8), np.uint32)
+    par = np.zeros(max(n - 1, 1), np.uint32)
+    qt = np.zeros((n, 12), np.uint32)
+    hd = np.zeros(4, np.uint32)
+    nodes_c = np.ascontiguousarray(b["nodes"], np.uint32) if n > 1 else np.zeros((1, 16), np.uint32)
+    oracle().orc_quantise(P(nodes_c), b["root"], P(tris), n, P(qn), P(par), P(qt), P(hd))
+    return dict(qnodes=qn[: n - 1], parents=par[: n - 1], qtris=qt, header=hd)
+
+
+def trace_quantised(q: dict, rays, query=0, counters=False):
+    rays = np.ascontiguousarray(rays, np.float32).reshape(-1, 8)
+    n = rays.shape[0]
+    hits = np.zeros((n, 8), np.uint32)
+    nv = np.zeros(n, np.uint32) if counters else None
+    nt = np.zeros(n, np.uint32) if counters else None
+    nu = np.zeros(n, np.uint32) if counters else None
+    qn = q["qnodes"] if len(q["qnodes"]) else np.zeros((1, 8), np.uint32)
+    par = q["parents"] if len(q["parents"]) else np.zeros(1, np.uint32)
+    oracle().orc_trace_quantised(P(np.ascontiguousarray(qn)), P(np.ascontiguousarray(par)),
+                                 P(np.ascontiguousarray(q["qtris"])), P(q["header"]), P(rays), n, query, P(hits), P(nv),
+                                 P(nt), P(nu))
+    if counters:
+        return hits, nv, nt, nu
+    return hits

@@ -1,0 +1,93 @@
+"""The quantised form (8-bit child boxes, 32-byte nodes; no reference
+counterpart). The GPU conversion must equal the oracle's word for word, every
+decoded box must contain its FP32 box, GPU traversal must equal the oracle's
+quantised traversal bit for bit, and its hits must equal the FP32 tree's."""
+import numpy as np
+import pytest
+
+import _gpu as G
+import _oracle as O
+import minimumlbvh_b200 as mb
+from minimumlbvh_b200 import scenes
+
+pytestmark = pytest.mark.gpu
+
+
+def quantise_both(tris):
+    b, t, out = G.build(tris)
+    q = mb.QuantisedBVH.from_builder(b, t)
+    n = len(tris)
+    gq = dict(qnodes=G.host(q.qnodes, np.uint32)[: n - 1], parents=G.host(q.parents, np.uint32)[: n - 1],
+              qtris=G.host(q.qtris, np.uint32), header=G.host(q.header, np.uint32))
+    ref = O.quantise(out, tris)
+    return b, t, out, q, gq, ref
+
+
+@pytest.mark.parametrize("n", [1, 2, 3, 257, 4097, 100000])
+def test_quantise_matches_oracle(cuda, n):
+    tris = scenes.gaussian_soup(n, clusters=4, seed=300 + n)
+    _, _, out, _, gq, ref = quantise_both(tris)
+    for k in ("qnodes", "parents", "qtris", "header"):
+        np.testing.assert_array_equal(gq[k], ref[k], err_msg=k)
+    if n > 1:
+        assert O.oracle().orc_check_quantised(O.P(out["nodes"]), n, O.P(gq["qnodes"]), O.P(gq["header"])) == 1
+
+
+@pytest.fixture(scope="module")
+def heightfield_q(cuda):
+    tris = scenes.heightfield_icospheres()
+    return (tris,) + quantise_both(tris)
+
+
+def test_quantise_heightfield_conservative(heightfield_q):
+    tris, _, _, out, _, gq, ref = heightfield_q
+    for k in ("qnodes", "parents", "qtris", "header"):
+        np.testing.assert_array_equal(gq[k], ref[k], err_msg=k)
+    assert O.oracle().orc_check_quantised(O.P(out["nodes"]), len(tris), O.P(gq["qnodes"]), O.P(gq["header"])) == 1
+
+
+@pytest.mark.parametrize("q", [0, 1])
+def test_quantised_trace_heightfield(heightfield_q, q):
+    tris, b, t, out, qb, gq, ref = heightfield_q
+    rays = scenes.random_rays(200000, [-1, -0.3, -1], [1, 0.7, 1], seed=41)
+    rays[1::3, 7] = 0.25
+    got = G.host(mb.intersect_quantised(qb, G.dev(rays), q), np.uint32)
+    np.testing.assert_array_equal(got, O.trace_quantised(ref, rays, q))
+    plain = O.trace(out["nodes"], tris, out["root"], rays, q, 0)
+    if q == 0:
+        np.testing.assert_array_equal(got[:, 7], plain[:, 7])  # hit ids
+        np.testing.assert_array_equal(got[:, 0], plain[:, 0])  # t
+    else:
+        np.testing.assert_array_equal(got[:, 7] == 0xFFFFFFFF, plain[:, 7] == 0xFFFFFFFF)
+
+
+def test_quantised_ao_equals_plain(heightfield_q):
+    import torch
+    tris, b, t, out, qb, gq, ref = heightfield_q
+    eye, c, up, fovy = scenes.camera_heightfield()
+    w, h = 512, 512
+    cam = mb.RayGenerator().lookat(eye, c, up, fovy, w, h)
+    px0 = torch.zeros(w * h, dtype=torch.int32, device="cuda")
+    px1 = torch.zeros_like(px0)
+    occ0 = torch.zeros_like(px0)
+    occ1 = torch.zeros_like(px0)
+    st = torch.zeros(8, dtype=torch.int64, device="cuda")
+    mb.render_ao(px0, (w, h), cam, b.m_rootNode, b.m_internals, t, 1, 16, 0.25, occluded=occ0)
+    mb.render_ao_quantised(px1, (w, h), cam, qb, 1, 16, 0.25, occluded=occ1, stats=st)
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(G.host(occ1), G.host(occ0))
+    np.testing.assert_array_equal(G.host(px1), G.host(px0))
+    assert int(G.host(st)[0]) > w * h
+
+
+def test_quantised_full_size_soup(cuda):
+    tris = scenes.gaussian_soup()
+    b, t, out, qb, gq, ref = quantise_both(tris)
+    for k in ("qnodes", "parents", "qtris", "header"):
+        np.testing.assert_array_equal(gq[k], ref[k], err_msg=k)
+    rays = scenes.random_rays(100000, [0, 0, 0], [1, 1, 1], seed=19)
+    rays[::2, 7] = 0.1
+    got = G.host(mb.intersect_quantised(qb, G.dev(rays), 0), np.uint32)
+    np.testing.assert_array_equal(got, O.trace_quantised(ref, rays, 0))
+    plain = O.trace(out["nodes"], tris, out["root"], rays, 0, 0)
+    np.testing.assert_array_equal(got[:, 7], plain[:, 7])
