@@ -276,7 +276,7 @@ def main():
     cam = mb.RayGenerator().lookat(eye, c, up, fovy, w, h)
     pixels = torch.zeros(w * h, dtype=torch.int32, device=dev)
     host_pixels = torch.empty(w * h, dtype=torch.int32).pin_memory()
-    stats = torch.zeros(5, dtype=torch.int64, device=dev)
+    stats = torch.zeros(8, dtype=torch.int64, device=dev)
     stream = torch.cuda.current_stream()
 
     def ao_frame(with_stats=False):
@@ -319,6 +319,32 @@ def main():
         ao_ms = [a.elapsed_time(b) for a, b in ev]
         kernel_ms = [a.elapsed_time(b) for a, b in kev]
         ao_total_s = max_over_ranks(sum(ao_ms) / 1e3)
+
+        # ---- the chosen form: the same frames over the 8-bit quantised tree
+        qtree = mb.QuantisedBVH.from_builder(builder, d_tris)
+        occ_plain = torch.empty(w * h, dtype=torch.int32, device=dev)
+        occ_q = torch.empty_like(occ_plain)
+        qstats = torch.zeros(8, dtype=torch.int64, device=dev)
+        mb.render_ao(pixels, (w, h), cam, builder.m_rootNode, builder.m_internals, d_tris, 1, wl["ns"], wl["radius"],
+                     12345, occluded=occ_plain)
+        mb.render_ao_quantised(pixels, (w, h), cam, qtree, 1, wl["ns"], wl["radius"], 12345, occluded=occ_q,
+                               stats=qstats)
+        for _ in range(args.warmup):
+            mb.render_ao_quantised(pixels, (w, h), cam, qtree, 1, wl["ns"], wl["radius"], 12345)
+        qev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+        barrier()
+        torch.cuda.synchronize()
+        for i in range(args.steps):
+            if flush is not None:
+                flush.zero_()
+            qev[i][0].record(stream)
+            mb.render_ao_quantised(pixels, (w, h), cam, qtree, 1, wl["ns"], wl["radius"], 12345)
+            qev[i][1].record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        q_total_s = max_over_ranks(sum(a.elapsed_time(b) for a, b in qev) / 1e3)
+        q_agree = float((occ_plain == occ_q).float().mean().item())
+        qst = qstats.cpu().numpy()
 
         # ---- builds
         bev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
@@ -365,7 +391,7 @@ def main():
                    "ao_rays": ao_rays, "parallelism": "replicas" if world > 1 else "single GPU",
                    "l2": "inputs larger than L2 (nodes + triangles 419 MB)" if wl["scene"] == "soup"
                    else "L2 flushed (256 MB write) between timed frames"},
-        "gpu_launches": args.steps * 3 + args.steps * 7 + args.steps * 10,
+        "gpu_launches": args.steps * (3 + 3 + 7 + 10),  # AO, quantised AO, build, e2e (build + AO) steps
         "clocks": clocks,
     }
     # roofline of the dominant kernel (k_ao_rays): algorithmic bytes of its rays
@@ -386,6 +412,15 @@ def main():
     line["e2e"] = {"value": rays_per_frame * args.steps * world / e2e_s / 1e6, "unit": "Mrays/s",
                    "h2d_bytes_per_step": int(host_tris.numel() * 4), "d2h_bytes_per_step": int(w * h * 4),
                    "ms_per_step": e2e_s * 1e3 / args.steps}
+    q_rays = int(qst[0])
+    line["chosen"] = {
+        "form": "quantised 8-bit child boxes (32-byte nodes)", "value": q_rays * args.steps * world / q_total_s / 1e6,
+        "unit": "Mrays/s", "ms_per_step": q_total_s * 1e3 / args.steps, "vs_plain": ao_total_s / q_total_s,
+        "occlusion_agreement": q_agree, "rays_per_frame": q_rays,
+        "node_bytes_per_ray": (32 * int(qst[1]) + 4 * int(qst[5])) / max(q_rays, 1),
+        "plain_node_bytes_per_ray": 64 * visits / max(rays_per_frame, 1),
+        "tri_bytes_per_ray": 48 * int(qst[2]) / max(q_rays, 1),
+        "plain_tri_bytes_per_ray": 36 * tests / max(rays_per_frame, 1)}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         out = {"nodes": builder.m_internals.cpu().numpy().view(np.uint32)[: n - 1],
                "root": int(builder.m_rootNode.cpu().numpy().view(np.uint32)[0])}

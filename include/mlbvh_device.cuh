@@ -198,65 +198,76 @@ __device__ __forceinline__ NodeView load_node(const mlbvh_internal_node* __restr
 // left child) or back up; from the near child go to the far child when both
 // boxes are still hit, else up; from the far child go up. Both child boxes
 // are re-tested on every visit against the current closest t.
-// With kCount, *visits and *tests receive the internal-node visits and
-// triangle tests of the walk (the traffic model of the roofline).
+//
+// stackfree_step advances the walk (curr, prev) by one leaf test or one
+// internal-node visit and returns true when the walk is over. With kCount,
+// nv and nt count internal-node visits and triangle tests (the traffic
+// model of the roofline).
+template <bool kAny, bool kCount>
+__device__ __forceinline__ bool stackfree_step(uint32_t& curr, uint32_t& prev, HitRecord& hit,
+                                               const mlbvh_internal_node* __restrict__ nodes,
+                                               const float* __restrict__ tris, f3 ro, f3 rd, f3 inv, float tmin,
+                                               uint32_t& nv, uint32_t& nt)
+{
+    if (curr & kLeafBit) {
+        if (kCount) ++nt;
+        const uint32_t ti = curr & ~kLeafBit;
+        f3 v0, v1, v2;
+        load_triangle(tris, ti, v0, v1, v2);
+        float t, u, v;
+        f3 ng;
+        if (intersect_triangle(t, u, v, ng, tmin, hit.t, ro, rd, v0, v1, v2)) {
+            hit.t = t;
+            hit.u = u;
+            hit.v = v;
+            hit.ng = ng;
+            hit.tri = ti;
+            if (kAny) return true;
+        }
+        const uint32_t s = curr;
+        curr = prev;
+        prev = s;
+        return curr == kInvalid;
+    }
+    if (kCount) ++nv;
+    const NodeView nd = load_node(nodes, curr);
+    const float2 rl = slab(ro, inv, nd.lo0, nd.hi0, tmin, hit.t);
+    const float2 rr = slab(ro, inv, nd.lo1, nd.hi1, tmin, hit.t);
+    const bool hitL = rl.x <= rl.y;
+    const bool hitR = rr.x <= rr.y;
+    uint32_t nearN = nd.c0, farN = nd.c1;
+    int nHits = 0;
+    if (hitL && hitR) {
+        if (rr.x < rl.x) {
+            nearN = nd.c1;
+            farN = nd.c0;
+        }
+        nHits = 2;
+    } else if (hitL || hitR) {
+        nHits = 1;
+        nearN = hitR ? farN : nearN;
+    }
+    uint32_t next;
+    if (prev == nd.parent)
+        next = 0 < nHits ? nearN : nd.parent;
+    else if (prev == nearN)
+        next = nHits == 2 ? farN : nd.parent;
+    else
+        next = nd.parent;
+    prev = curr;
+    curr = next;
+    return curr == kInvalid;
+}
+
 template <bool kAny, bool kCount = false>
 __device__ __forceinline__ void trace_stackfree(HitRecord& hit, const mlbvh_internal_node* __restrict__ nodes,
                                                 const float* __restrict__ tris, uint32_t root, f3 ro, f3 rd,
                                                 f3 inv, float tmin, uint32_t* visits = nullptr,
                                                 uint32_t* tests = nullptr)
 {
-    uint32_t curr = root, prev = kInvalid;
-    uint32_t nv = 0, nt = 0, steps = 0;
-    while (curr != kInvalid && ++steps < kMaxTraversalSteps) {
-        if (curr & kLeafBit) {
-            if (kCount) ++nt;
-            uint32_t ti = curr & ~kLeafBit;
-            f3 v0, v1, v2;
-            load_triangle(tris, ti, v0, v1, v2);
-            float t, u, v;
-            f3 ng;
-            if (intersect_triangle(t, u, v, ng, tmin, hit.t, ro, rd, v0, v1, v2)) {
-                hit.t = t;
-                hit.u = u;
-                hit.v = v;
-                hit.ng = ng;
-                hit.tri = ti;
-                if (kAny) break;
-            }
-            uint32_t s = curr;
-            curr = prev;
-            prev = s;
-            continue;
-        }
-        if (kCount) ++nv;
-        NodeView nd = load_node(nodes, curr);
-        float2 rl = slab(ro, inv, nd.lo0, nd.hi0, tmin, hit.t);
-        float2 rr = slab(ro, inv, nd.lo1, nd.hi1, tmin, hit.t);
-        bool hitL = rl.x <= rl.y;
-        bool hitR = rr.x <= rr.y;
-        uint32_t nearN = nd.c0, farN = nd.c1;
-        int nHits = 0;
-        if (hitL && hitR) {
-            if (rr.x < rl.x) {
-                nearN = nd.c1;
-                farN = nd.c0;
-            }
-            nHits = 2;
-        } else if (hitL || hitR) {
-            nHits = 1;
-            nearN = hitR ? farN : nearN;
-        }
-        uint32_t next;
-        if (prev == nd.parent)
-            next = 0 < nHits ? nearN : nd.parent;
-        else if (prev == nearN)
-            next = nHits == 2 ? farN : nd.parent;
-        else
-            next = nd.parent;
-        prev = curr;
-        curr = next;
-    }
+    uint32_t curr = root, prev = kInvalid, nv = 0, nt = 0;
+    for (uint32_t steps = 1; steps < kMaxTraversalSteps; ++steps)
+        if (stackfree_step<kAny, kCount>(curr, prev, hit, nodes, tris, ro, rd, inv, tmin, nv, nt)) break;
     if (kCount) {
         *visits += nv;
         *tests += nt;
@@ -612,7 +623,74 @@ __device__ __forceinline__ QNodeView load_qnode(const mlbvh_qnode* __restrict__ 
 // Stack-free walk over the quantised tree: the state machine of
 // intersect_stackfree (minimum_lbvh.h:981-1061), with "came from the parent"
 // recognised as "came from neither child" so that the parent word is read
-// only when the walk moves up.
+// only when the walk moves up. quantised_step advances it by one leaf test or
+// internal-node visit and returns true when the walk is over; nu counts
+// parent-word loads.
+template <bool kAny, bool kCount>
+__device__ __forceinline__ bool quantised_step(uint32_t& curr, uint32_t& prev, HitRecord& hit,
+                                               const mlbvh_qnode* __restrict__ qnodes,
+                                               const uint32_t* __restrict__ parents,
+                                               const mlbvh_qtri* __restrict__ qtris, int eBase, f3 ro, f3 rd, f3 inv,
+                                               float tmin, uint32_t& nv, uint32_t& nt, uint32_t& nu)
+{
+    if (curr & kLeafBit) {
+        if (kCount) ++nt;
+        const float4* t = reinterpret_cast<const float4*>(qtris + (curr & kQIndexMask));
+        const float4 a = __ldg(t), b = __ldg(t + 1), c = __ldg(t + 2);
+        float tt, u, v;
+        f3 ng;
+        if (intersect_triangle(tt, u, v, ng, tmin, hit.t, ro, rd, mk(a.x, a.y, a.z), mk(a.w, b.x, b.y),
+                               mk(b.z, b.w, c.x))) {
+            hit.t = tt;
+            hit.u = u;
+            hit.v = v;
+            hit.ng = ng;
+            hit.tri = __float_as_uint(c.y);
+            if (kAny) return true;
+        }
+        const uint32_t s = curr;
+        curr = prev;
+        prev = s;
+        return curr == kInvalid;
+    }
+    if (kCount) ++nv;
+    const QNodeView nd = load_qnode(qnodes, curr, eBase);
+    const float2 rl = slab(ro, inv, nd.box.lo0, nd.box.hi0, tmin, hit.t);
+    const float2 rr = slab(ro, inv, nd.box.lo1, nd.box.hi1, tmin, hit.t);
+    const bool hitL = rl.x <= rl.y, hitR = rr.x <= rr.y;
+    uint32_t nearN = nd.c0, farN = nd.c1;
+    int nHits = 0;
+    if (hitL && hitR) {
+        if (rr.x < rl.x) {
+            nearN = nd.c1;
+            farN = nd.c0;
+        }
+        nHits = 2;
+    } else if (hitL || hitR) {
+        nHits = 1;
+        nearN = hitR ? farN : nearN;
+    }
+    const bool fromParent = prev != nd.c0 && prev != nd.c1;
+    uint32_t next = kInvalid;
+    bool up;
+    if (fromParent) {
+        up = nHits == 0;
+        next = nearN;
+    } else if (prev == nearN) {
+        up = nHits != 2;
+        next = farN;
+    } else {
+        up = true;
+    }
+    if (up) {
+        if (kCount) ++nu;
+        next = __ldg(parents + curr);
+    }
+    prev = curr;
+    curr = next;
+    return curr == kInvalid;
+}
+
 template <bool kAny, bool kCount = false>
 __device__ __forceinline__ void trace_quantised(HitRecord& hit, const mlbvh_qnode* __restrict__ qnodes,
                                                 const uint32_t* __restrict__ parents,
@@ -620,65 +698,11 @@ __device__ __forceinline__ void trace_quantised(HitRecord& hit, const mlbvh_qnod
                                                 f3 rd, f3 inv, float tmin, uint32_t* visits = nullptr,
                                                 uint32_t* tests = nullptr, uint32_t* ups = nullptr)
 {
-    uint32_t curr = root, prev = kInvalid;
-    uint32_t nv = 0, nt = 0, nu = 0, steps = 0;
-    while (curr != kInvalid && ++steps < kMaxTraversalSteps) {
-        if (curr & kLeafBit) {
-            if (kCount) ++nt;
-            const float4* t = reinterpret_cast<const float4*>(qtris + (curr & kQIndexMask));
-            const float4 a = __ldg(t), b = __ldg(t + 1), c = __ldg(t + 2);
-            float tt, u, v;
-            f3 ng;
-            if (intersect_triangle(tt, u, v, ng, tmin, hit.t, ro, rd, mk(a.x, a.y, a.z), mk(a.w, b.x, b.y),
-                                   mk(b.z, b.w, c.x))) {
-                hit.t = tt;
-                hit.u = u;
-                hit.v = v;
-                hit.ng = ng;
-                hit.tri = __float_as_uint(c.y);
-                if (kAny) break;
-            }
-            const uint32_t s = curr;
-            curr = prev;
-            prev = s;
-            continue;
-        }
-        if (kCount) ++nv;
-        const QNodeView nd = load_qnode(qnodes, curr, eBase);
-        const float2 rl = slab(ro, inv, nd.box.lo0, nd.box.hi0, tmin, hit.t);
-        const float2 rr = slab(ro, inv, nd.box.lo1, nd.box.hi1, tmin, hit.t);
-        const bool hitL = rl.x <= rl.y, hitR = rr.x <= rr.y;
-        uint32_t nearN = nd.c0, farN = nd.c1;
-        int nHits = 0;
-        if (hitL && hitR) {
-            if (rr.x < rl.x) {
-                nearN = nd.c1;
-                farN = nd.c0;
-            }
-            nHits = 2;
-        } else if (hitL || hitR) {
-            nHits = 1;
-            nearN = hitR ? farN : nearN;
-        }
-        const bool fromParent = prev != nd.c0 && prev != nd.c1;
-        uint32_t next = kInvalid;
-        bool up;
-        if (fromParent) {
-            up = nHits == 0;
-            next = nearN;
-        } else if (prev == nearN) {
-            up = nHits != 2;
-            next = farN;
-        } else {
-            up = true;
-        }
-        if (up) {
-            if (kCount) ++nu;
-            next = __ldg(parents + curr);
-        }
-        prev = curr;
-        curr = next;
-    }
+    uint32_t curr = root, prev = kInvalid, nv = 0, nt = 0, nu = 0;
+    for (uint32_t steps = 1; steps < kMaxTraversalSteps; ++steps)
+        if (quantised_step<kAny, kCount>(curr, prev, hit, qnodes, parents, qtris, eBase, ro, rd, inv, tmin, nv, nt,
+                                         nu))
+            break;
     if (kCount) {
         *visits += nv;
         *tests += nt;

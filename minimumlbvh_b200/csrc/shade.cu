@@ -1,12 +1,13 @@
 // Shading on B200: the reference's normal / ao / pt / pack kernels
 // (main_gpu.cu:84-286) restated over this library's traversal.
 //
-// AO is ray-major instead of pixel-major: k_ao_primary traces one closest-hit
-// ray per pixel and appends each hit pixel (AO origin and facing normal) to a
-// queue; k_ao_rays is a persistent kernel whose warps take 32 consecutive
-// (pixel, sample) items at a time from an atomic work counter, so a warp's
-// any-hit rays share one origin and the SMs never idle on missed pixels;
-// k_ao_finish turns the per-pixel occlusion counts into the packed image.
+// AO runs in three kernels: k_ao_primary traces one closest-hit ray per pixel
+// and appends each hit pixel (AO origin and facing normal) to a queue, so no
+// later work is spent on missed pixels; k_ao_rays is a persistent kernel in
+// which every lane owns one queued pixel at a time and steps its any-hit rays
+// one node per iteration, refilling idle lanes from the queue (no lane waits
+// for the longest ray of its warp); k_ao_finish turns the per-pixel occlusion
+// counts into the packed image.
 #include <algorithm>
 
 #include "capi_internal.h"
@@ -28,7 +29,7 @@ struct AoRecord {
 };
 
 struct RenderLayout {
-    size_t header;  // u32 queueCount, u32 workCounter
+    size_t header;  // u32 queue count, u32 pad, u32 work counter
     size_t records;
     size_t counts;
     size_t total;
@@ -122,6 +123,12 @@ struct PlainTree {
     {
         trace_stackfree<kAny, kCount>(hit, nodes, tris, c.root, ro, rd, inv_rd(rd), 0.0f, &n.visits, &n.tests);
     }
+    template <bool kAny, bool kCount>
+    __device__ __forceinline__ bool step(const Ctx&, uint32_t& curr, uint32_t& prev, HitRecord& hit, f3 ro, f3 rd,
+                                         f3 inv, Counts& n) const
+    {
+        return stackfree_step<kAny, kCount>(curr, prev, hit, nodes, tris, ro, rd, inv, 0.0f, n.visits, n.tests);
+    }
 };
 struct QuantTree {
     const mlbvh_qnode* qnodes;
@@ -141,6 +148,13 @@ struct QuantTree {
     {
         trace_quantised<kAny, kCount>(hit, qnodes, parents, qtris, c.root, c.eBase, ro, rd, inv_rd(rd), 0.0f,
                                       &n.visits, &n.tests, &n.ups);
+    }
+    template <bool kAny, bool kCount>
+    __device__ __forceinline__ bool step(const Ctx& c, uint32_t& curr, uint32_t& prev, HitRecord& hit, f3 ro, f3 rd,
+                                         f3 inv, Counts& n) const
+    {
+        return quantised_step<kAny, kCount>(curr, prev, hit, qnodes, parents, qtris, c.eBase, ro, rd, inv, 0.0f,
+                                            n.visits, n.tests, n.ups);
     }
 };
 
@@ -191,9 +205,15 @@ __global__ void __launch_bounds__(kTileW* kTileH)
     }
 }
 
-// AO rays (main_gpu.cu:146-173): item = (queue entry, sample). Each warp takes
-// 32 consecutive items; per-pixel occlusion counts are reduced across the
-// lanes of one pixel before a single atomic add.
+// AO rays (main_gpu.cu:146-173), scheduled per lane. Each lane owns one hit
+// pixel at a time and traces its nSamples any-hit rays one after another,
+// advancing its walk one node (or leaf) per loop iteration; a lane whose
+// pixel is done takes the next pixel from the queue, in warp-wide batches
+// (one atomic per batch) once a quarter of the warp is idle or the warp has
+// nothing left. So lanes never wait for the longest ray of their warp, and
+// each pixel's occlusion count is written once, by its owner, without atomics.
+constexpr int kRefillBatch = 8;
+
 template <class Tree, bool kCount>
 __global__ void __launch_bounds__(kAoThreads)
     k_ao_rays(const AoRecord* __restrict__ records, const uint32_t* __restrict__ queueCount,
@@ -202,27 +222,47 @@ __global__ void __launch_bounds__(kAoThreads)
 {
     Counts cnt;
     const int lane = threadIdx.x & 31;
-    const uint64_t total = (uint64_t)(*queueCount) * (uint64_t)nSamples;
+    const uint32_t lanesBelow = (1u << lane) - 1u;
+    const uint32_t total = *queueCount;
     const typename Tree::Ctx ctx = tree.context();
+    bool exhausted = false;  // warp-uniform: the queue has no pixel left
+    bool owns = false;       // this lane owns a pixel
+    bool live = false;       // this lane has a ray in flight
+    uint32_t pixel = 0, s = 0, occ = 0, xi = 0, yi = 0, curr = 0, prev = 0, steps = 0;
+    f3 origin = mk(0, 0, 0), n = origin, xaxis = origin, zaxis = origin, dir = origin, inv = origin;
+    HitRecord hit;
+    hit.t = radius;
     for (;;) {
-        unsigned long long base = 0;
-        if (lane == 0) base = atomicAdd(reinterpret_cast<unsigned long long*>(workCounter), 32ull);
-        base = __shfl_sync(0xffffffffu, base, 0);
-        if (base >= total) break;
-        const uint64_t item = base + (uint64_t)lane;
-        const bool valid = item < total;
-        uint32_t entry = 0xFFFFFFFFu;
-        bool occluded = false;
-        if (valid) {
-            entry = (uint32_t)(item / (uint64_t)nSamples);
-            const uint32_t s = (uint32_t)(item - (uint64_t)entry * (uint64_t)nSamples);
-            const float4* rp = reinterpret_cast<const float4*>(records + entry);
-            const float4 r0 = __ldg(rp), r1 = __ldg(rp + 1);
-            const f3 origin = mk(r0.x, r0.y, r0.z), n = mk(r0.w, r1.x, r1.y);
-            const uint32_t pixel = __float_as_uint(r1.z);
-            const uint32_t xi = pixel % (uint32_t)w, yi = pixel / (uint32_t)w;
-            f3 xaxis, zaxis;
-            onb(n, xaxis, zaxis);
+        const uint32_t idle = __ballot_sync(0xffffffffu, !owns);
+        if (!exhausted && (__popc(idle) >= kRefillBatch || idle == 0xffffffffu)) {
+            const int leader = __ffs(idle) - 1;
+            uint32_t base = 0;
+            if (lane == leader) base = atomicAdd(workCounter, (uint32_t)__popc(idle));
+            base = __shfl_sync(0xffffffffu, base, leader);
+            if (base + (uint32_t)__popc(idle) >= total) exhausted = true;
+            if (!owns) {
+                const uint32_t entry = base + __popc(idle & lanesBelow);
+                if (entry < total) {
+                    const float4* rp = reinterpret_cast<const float4*>(records + entry);
+                    const float4 r0 = __ldg(rp), r1 = __ldg(rp + 1);
+                    origin = mk(r0.x, r0.y, r0.z);
+                    n = mk(r0.w, r1.x, r1.y);
+                    pixel = __float_as_uint(r1.z);
+                    xi = pixel % (uint32_t)w;
+                    yi = pixel / (uint32_t)w;
+                    onb(n, xaxis, zaxis);
+                    s = 0;
+                    occ = 0;
+                    owns = true;
+                    live = false;
+                }
+            }
+        }
+        if (!__any_sync(0xffffffffu, owns)) {
+            if (exhausted) break;
+            continue;
+        }
+        if (owns && !live) {  // start sample s of this lane's pixel
             float2 rnd;
             if (useSobol) {
                 rnd = sobol2d(s, xi, yi, seed);
@@ -233,20 +273,24 @@ __global__ void __launch_bounds__(kAoThreads)
                 rnd.y = rng.uniformf();
             }
             const f3 dl = sample_hemisphere(rnd.x, rnd.y);
-            const f3 dir = xaxis * dl.x + zaxis * dl.z + n * dl.y;
-            HitRecord hit;
+            dir = xaxis * dl.x + zaxis * dl.z + n * dl.y;
+            inv = inv_rd(dir);
             hit.t = radius;
             hit.tri = 0xFFFFFFFFu;
-            tree.template trace<true, kCount>(ctx, hit, origin, dir, cnt);
-            occluded = hit.t != radius;
+            curr = ctx.root;
+            prev = kInvalid;
+            steps = 0;
+            live = true;
         }
-        const uint32_t peers = __match_any_sync(0xffffffffu, entry);
-        const uint32_t occ = __ballot_sync(0xffffffffu, occluded);
-        if (valid && lane == __ffs(peers) - 1) {
-            const uint32_t c = __popc(occ & peers);
-            if (c) {
-                const uint32_t pixel = __float_as_uint(__ldg(reinterpret_cast<const float*>(records + entry) + 6));
-                atomicAdd(counts + pixel, c);
+        if (live) {
+            if (tree.template step<true, kCount>(ctx, curr, prev, hit, origin, dir, inv, cnt) ||
+                ++steps >= kMaxTraversalSteps) {
+                live = false;
+                if (hit.t != radius) ++occ;
+                if (++s == (uint32_t)nSamples) {
+                    counts[pixel] = occ;
+                    owns = false;
+                }
             }
         }
     }

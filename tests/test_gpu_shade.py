@@ -25,7 +25,7 @@ def gpu_ao(b, t, cam, w, h, ns, radius, seed=12345, sobol=1):
     import torch
     px = torch.zeros(w * h, dtype=torch.int32, device="cuda")
     occ = torch.zeros(w * h, dtype=torch.int32, device="cuda")
-    stats = torch.zeros(5, dtype=torch.int64, device="cuda")
+    stats = torch.zeros(8, dtype=torch.int64, device="cuda")
     mb.render_ao(px, (w, h), mb.RayGenerator.from_array(cam), b.m_rootNode, b.m_internals, t, sobol, ns, radius,
                  seed, occluded=occ, stats=stats)
     torch.cuda.synchronize()
