@@ -143,6 +143,25 @@ MLBVH_API mlbvh_status mlbvh_build_ex(const mlbvh_triangle* dTriangles, uint32_t
                             mlbvh_aabb* dSceneAABB, uint32_t* dSortedKeys, uint32_t* dSortedIndices,
                             uint8_t* dDeltas, void* dScratch, size_t scratchBytes, void* stream);
 
+/* mlbvh_build without the scratch argument, for callers that must not
+ * allocate device memory: plugins whose host application owns all GPU memory
+ * through its own allocator, and real-time loops that cannot afford
+ * cudaMalloc's implicit device synchronisation or its failure mid-frame. This
+ * entry point has no counterpart in the reference (whose builder allocates
+ * and frees its temporaries on every build).
+ * Its scratch is a fixed 2 MiB device array inside this library, held by
+ * every GPU that loads the library until the process exits; it limits the
+ * build to nTriangles <= 65536 (larger sizes return MLBVH_ERR_INVALID_ARG).
+ * The caller still passes the triangles and the output buffers. The first
+ * call on a device looks up the array's device address (cudaGetSymbolAddress,
+ * with that device current); make that first call before any stream capture.
+ * Every call shares the one array, which keeps the last call's contents:
+ * calls that overlap on the GPU (e.g. on two streams) race and must be
+ * serialised by the caller. Nothing is allocated or freed. */
+MLBVH_API mlbvh_status mlbvh_build_noalloc(const mlbvh_triangle* dTriangles, uint32_t nTriangles,
+                                           uint32_t buildOption, mlbvh_internal_node* dInternals,
+                                           mlbvh_node_index* dRootNode, mlbvh_aabb* dSceneAABB, void* stream);
+
 /* Synchronises `stream`, then reports MLBVH_ERR_TIMEOUT if a bounded wait of
  * the last build that used dScratch gave up (its output is then unusable),
  * else MLBVH_OK. */
