@@ -205,13 +205,15 @@ __global__ void __launch_bounds__(kTileW* kTileH)
     }
 }
 
-// AO rays (main_gpu.cu:146-173), scheduled per lane. Each lane owns one hit
-// pixel at a time and traces its nSamples any-hit rays one after another,
-// advancing its walk one node (or leaf) per loop iteration; a lane whose
-// pixel is done takes the next pixel from the queue, in warp-wide batches
-// (one atomic per batch) once a quarter of the warp is idle or the warp has
-// nothing left. So lanes never wait for the longest ray of their warp, and
-// each pixel's occlusion count is written once, by its owner, without atomics.
+// AO rays (main_gpu.cu:146-173), scheduled per lane. A work item is a run of
+// consecutive samples of one hit pixel (all nSamples when there are enough
+// pixels to fill the grid eight times over, else halved down to 4 samples).
+// Each lane owns one item at a time and traces its any-hit rays one after
+// another, advancing its walk one node (or leaf) per loop iteration; lanes
+// that finish take new items from the queue in warp-wide batches (one atomic
+// per batch) once a quarter of the warp is idle or the warp has nothing left.
+// So lanes never wait for the longest ray of their warp. A finished item adds
+// its occlusion count to its pixel's.
 constexpr int kRefillBatch = 8;
 
 template <class Tree, bool kCount>
@@ -223,12 +225,18 @@ __global__ void __launch_bounds__(kAoThreads)
     Counts cnt;
     const int lane = threadIdx.x & 31;
     const uint32_t lanesBelow = (1u << lane) - 1u;
-    const uint32_t total = *queueCount;
+    const uint32_t pixels = *queueCount;
+    const uint64_t lanes = (uint64_t)gridDim.x * blockDim.x;
+    uint32_t chunk = (uint32_t)nSamples;
+    while (chunk > 4 && (uint64_t)pixels * ((nSamples + chunk - 1) / chunk) < 8 * lanes) chunk = (chunk + 1) / 2;
+    if ((uint64_t)pixels * ((nSamples + chunk - 1) / chunk) > 0xFFFFFFFFull) chunk = (uint32_t)nSamples;
+    const uint32_t itemsPerPixel = (nSamples + chunk - 1) / chunk;
+    const uint32_t total = pixels * itemsPerPixel;
     const typename Tree::Ctx ctx = tree.context();
-    bool exhausted = false;  // warp-uniform: the queue has no pixel left
-    bool owns = false;       // this lane owns a pixel
+    bool exhausted = false;  // warp-uniform: the queue has no item left
+    bool owns = false;       // this lane owns an item
     bool live = false;       // this lane has a ray in flight
-    uint32_t pixel = 0, s = 0, occ = 0, xi = 0, yi = 0, curr = 0, prev = 0, steps = 0;
+    uint32_t pixel = 0, s = 0, sEnd = 0, occ = 0, xi = 0, yi = 0, curr = 0, prev = 0, steps = 0;
     f3 origin = mk(0, 0, 0), n = origin, xaxis = origin, zaxis = origin, dir = origin, inv = origin;
     HitRecord hit;
     hit.t = radius;
@@ -241,8 +249,11 @@ __global__ void __launch_bounds__(kAoThreads)
             base = __shfl_sync(0xffffffffu, base, leader);
             if (base + (uint32_t)__popc(idle) >= total) exhausted = true;
             if (!owns) {
-                const uint32_t entry = base + __popc(idle & lanesBelow);
-                if (entry < total) {
+                const uint32_t item = base + __popc(idle & lanesBelow);
+                if (item < total) {
+                    const uint32_t entry = item / itemsPerPixel;
+                    s = (item - entry * itemsPerPixel) * chunk;
+                    sEnd = min(s + chunk, (uint32_t)nSamples);
                     const float4* rp = reinterpret_cast<const float4*>(records + entry);
                     const float4 r0 = __ldg(rp), r1 = __ldg(rp + 1);
                     origin = mk(r0.x, r0.y, r0.z);
@@ -251,7 +262,6 @@ __global__ void __launch_bounds__(kAoThreads)
                     xi = pixel % (uint32_t)w;
                     yi = pixel / (uint32_t)w;
                     onb(n, xaxis, zaxis);
-                    s = 0;
                     occ = 0;
                     owns = true;
                     live = false;
@@ -287,8 +297,8 @@ __global__ void __launch_bounds__(kAoThreads)
                 ++steps >= kMaxTraversalSteps) {
                 live = false;
                 if (hit.t != radius) ++occ;
-                if (++s == (uint32_t)nSamples) {
-                    counts[pixel] = occ;
+                if (++s == sEnd) {
+                    if (occ) atomicAdd(counts + pixel, occ);
                     owns = false;
                 }
             }
