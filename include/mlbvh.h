@@ -6,7 +6,9 @@
  * stream-ordered: device buffers are owned by the caller, nothing is
  * allocated, and nothing synchronises unless stated. `stream` is a
  * cudaStream_t passed as void* (NULL = the legacy default stream). Device
- * pointers must be 16-byte aligned (checked; MLBVH_ERR_INVALID_ARG).
+ * pointers must be 16-byte aligned, and node arrays that a query reads
+ * (mlbvh_internal_node, mlbvh_qnode) 32-byte aligned, as cudaMalloc returns
+ * them (checked; MLBVH_ERR_INVALID_ARG).
  *
  * Data layouts are byte-identical to the reference's minimum_lbvh.h types so
  * that buffers built here can be handed to code written against it:
@@ -238,6 +240,26 @@ MLBVH_API mlbvh_status mlbvh_render_pt(float* dAccumulators, int width, int heig
                              const mlbvh_node_index* dRootNode, const mlbvh_internal_node* dInternals,
                              const mlbvh_triangle* dTriangles, const mlbvh_triangle_attrib* dAttribs,
                              int useSobol, int maxSPP, int maxDepth, void* stream);
+
+/* ------------------------------------------------ differentiable path trace ---
+ * No reference counterpart (the reference's pt, main_gpu.cu:179-272, is not
+ * differentiable). A fixed-depth, Russian-roulette-free variant of pt with
+ * grey per-triangle albedo dAlbedo[t] and emission dEmission[t]:
+ *   I_p = 1/spp sum_s sum_{d=0..bounces} e(t_d) prod_{j<d} a(t_j)
+ * over spp Owen-Sobol paths per pixel (dimension 0 jitters the pixel,
+ * dimension 1 + d samples bounce d). mlbvh_pt_diff_render writes the float
+ * image; mlbvh_pt_diff_adjoint ADDS dLoss/dAlbedo to dGradAlbedo (zero it
+ * first) given dLoss/dImage, by replaying every path from its sample index
+ * instead of storing it (path replay). 0 <= bounces <= 8. */
+MLBVH_API mlbvh_status mlbvh_pt_diff_render(float* dImage, int width, int height, int spp, int bounces,
+                                            const mlbvh_ray_generator* camera, const mlbvh_node_index* dRootNode,
+                                            const mlbvh_internal_node* dInternals, const mlbvh_triangle* dTriangles,
+                                            const float* dAlbedo, const float* dEmission, void* stream);
+MLBVH_API mlbvh_status mlbvh_pt_diff_adjoint(float* dGradAlbedo, const float* dGradImage, int width, int height,
+                                             int spp, int bounces, const mlbvh_ray_generator* camera,
+                                             const mlbvh_node_index* dRootNode, const mlbvh_internal_node* dInternals,
+                                             const mlbvh_triangle* dTriangles, const float* dAlbedo,
+                                             const float* dEmission, void* stream);
 
 /* pack (main_gpu.cu:273-286): accumulator / spp, gamma 1/2.2, RGBA8. */
 MLBVH_API mlbvh_status mlbvh_pack(uint32_t* dPixels, const float* dAccumulators, int n, void* stream);

@@ -177,10 +177,31 @@ struct NodeView {
     uint32_t c0, c1, parent, context;
     f3 lo0, hi0, lo1, hi1;
 };
+// 32 bytes through the read-only path in one instruction (ld.global.nc.v8,
+// sm_100 and later); p must be 32-byte aligned.
+__device__ __forceinline__ void ldg32(const void* p, float4& a, float4& b)
+{
+    asm("ld.global.nc.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+        : "=f"(a.x), "=f"(a.y), "=f"(a.z), "=f"(a.w), "=f"(b.x), "=f"(b.y), "=f"(b.z), "=f"(b.w)
+        : "l"(p));
+}
+
+// kWide: two 32-byte loads (the node array must be 32-byte aligned, as the
+// library's entry points check); otherwise four 16-byte loads.
+template <bool kWide = false>
 __device__ __forceinline__ NodeView load_node(const mlbvh_internal_node* __restrict__ nodes, uint32_t i)
 {
     const float4* p = reinterpret_cast<const float4*>(nodes + i);
-    float4 a = __ldg(p + 0), b = __ldg(p + 1), c = __ldg(p + 2), d = __ldg(p + 3);
+    float4 a, b, c, d;
+    if (kWide) {
+        ldg32(p, a, b);
+        ldg32(p + 2, c, d);
+    } else {
+        a = __ldg(p + 0);
+        b = __ldg(p + 1);
+        c = __ldg(p + 2);
+        d = __ldg(p + 3);
+    }
     NodeView n;
     n.c0 = __float_as_uint(a.x);
     n.c1 = __float_as_uint(a.y);
@@ -202,8 +223,8 @@ __device__ __forceinline__ NodeView load_node(const mlbvh_internal_node* __restr
 // stackfree_step advances the walk (curr, prev) by one leaf test or one
 // internal-node visit and returns true when the walk is over. With kCount,
 // nv and nt count internal-node visits and triangle tests (the traffic
-// model of the roofline).
-template <bool kAny, bool kCount>
+// model of the roofline). kWide selects 32-byte node loads (see load_node).
+template <bool kAny, bool kCount, bool kWide = false>
 __device__ __forceinline__ bool stackfree_step(uint32_t& curr, uint32_t& prev, HitRecord& hit,
                                                const mlbvh_internal_node* __restrict__ nodes,
                                                const float* __restrict__ tris, f3 ro, f3 rd, f3 inv, float tmin,
@@ -230,7 +251,7 @@ __device__ __forceinline__ bool stackfree_step(uint32_t& curr, uint32_t& prev, H
         return curr == kInvalid;
     }
     if (kCount) ++nv;
-    const NodeView nd = load_node(nodes, curr);
+    const NodeView nd = load_node<kWide>(nodes, curr);
     const float2 rl = slab(ro, inv, nd.lo0, nd.hi0, tmin, hit.t);
     const float2 rr = slab(ro, inv, nd.lo1, nd.hi1, tmin, hit.t);
     const bool hitL = rl.x <= rl.y;
@@ -259,7 +280,7 @@ __device__ __forceinline__ bool stackfree_step(uint32_t& curr, uint32_t& prev, H
     return curr == kInvalid;
 }
 
-template <bool kAny, bool kCount = false>
+template <bool kAny, bool kCount = false, bool kWide = false>
 __device__ __forceinline__ void trace_stackfree(HitRecord& hit, const mlbvh_internal_node* __restrict__ nodes,
                                                 const float* __restrict__ tris, uint32_t root, f3 ro, f3 rd,
                                                 f3 inv, float tmin, uint32_t* visits = nullptr,
@@ -267,7 +288,7 @@ __device__ __forceinline__ void trace_stackfree(HitRecord& hit, const mlbvh_inte
 {
     uint32_t curr = root, prev = kInvalid, nv = 0, nt = 0;
     for (uint32_t steps = 1; steps < kMaxTraversalSteps; ++steps)
-        if (stackfree_step<kAny, kCount>(curr, prev, hit, nodes, tris, ro, rd, inv, tmin, nv, nt)) break;
+        if (stackfree_step<kAny, kCount, kWide>(curr, prev, hit, nodes, tris, ro, rd, inv, tmin, nv, nt)) break;
     if (kCount) {
         *visits += nv;
         *tests += nt;
@@ -600,10 +621,17 @@ struct QNodeView {
     uint32_t c0, c1;  // leaf flag | 23-bit index
     QBox box;
 };
+template <bool kWide = false>
 __device__ __forceinline__ QNodeView load_qnode(const mlbvh_qnode* __restrict__ qnodes, uint32_t i, int eBase)
 {
     const float4* p = reinterpret_cast<const float4*>(qnodes + i);
-    const float4 a = __ldg(p), b = __ldg(p + 1);
+    float4 a, b;
+    if (kWide) {
+        ldg32(p, a, b);
+    } else {
+        a = __ldg(p);
+        b = __ldg(p + 1);
+    }
     const uint32_t w0 = __float_as_uint(a.w), w1 = __float_as_uint(b.x), w2 = __float_as_uint(b.y);
     const uint32_t c0 = __float_as_uint(b.z), c1 = __float_as_uint(b.w);
     float sx, sy, sz;
@@ -625,8 +653,8 @@ __device__ __forceinline__ QNodeView load_qnode(const mlbvh_qnode* __restrict__ 
 // recognised as "came from neither child" so that the parent word is read
 // only when the walk moves up. quantised_step advances it by one leaf test or
 // internal-node visit and returns true when the walk is over; nu counts
-// parent-word loads.
-template <bool kAny, bool kCount>
+// parent-word loads. kWide: one 32-byte node load (32-byte aligned array).
+template <bool kAny, bool kCount, bool kWide = false>
 __device__ __forceinline__ bool quantised_step(uint32_t& curr, uint32_t& prev, HitRecord& hit,
                                                const mlbvh_qnode* __restrict__ qnodes,
                                                const uint32_t* __restrict__ parents,
@@ -654,7 +682,7 @@ __device__ __forceinline__ bool quantised_step(uint32_t& curr, uint32_t& prev, H
         return curr == kInvalid;
     }
     if (kCount) ++nv;
-    const QNodeView nd = load_qnode(qnodes, curr, eBase);
+    const QNodeView nd = load_qnode<kWide>(qnodes, curr, eBase);
     const float2 rl = slab(ro, inv, nd.box.lo0, nd.box.hi0, tmin, hit.t);
     const float2 rr = slab(ro, inv, nd.box.lo1, nd.box.hi1, tmin, hit.t);
     const bool hitL = rl.x <= rl.y, hitR = rr.x <= rr.y;
@@ -691,7 +719,7 @@ __device__ __forceinline__ bool quantised_step(uint32_t& curr, uint32_t& prev, H
     return curr == kInvalid;
 }
 
-template <bool kAny, bool kCount = false>
+template <bool kAny, bool kCount = false, bool kWide = false>
 __device__ __forceinline__ void trace_quantised(HitRecord& hit, const mlbvh_qnode* __restrict__ qnodes,
                                                 const uint32_t* __restrict__ parents,
                                                 const mlbvh_qtri* __restrict__ qtris, uint32_t root, int eBase, f3 ro,
@@ -700,8 +728,8 @@ __device__ __forceinline__ void trace_quantised(HitRecord& hit, const mlbvh_qnod
 {
     uint32_t curr = root, prev = kInvalid, nv = 0, nt = 0, nu = 0;
     for (uint32_t steps = 1; steps < kMaxTraversalSteps; ++steps)
-        if (quantised_step<kAny, kCount>(curr, prev, hit, qnodes, parents, qtris, eBase, ro, rd, inv, tmin, nv, nt,
-                                         nu))
+        if (quantised_step<kAny, kCount, kWide>(curr, prev, hit, qnodes, parents, qtris, eBase, ro, rd, inv, tmin, nv,
+                                                nt, nu))
             break;
     if (kCount) {
         *visits += nv;

@@ -21,7 +21,7 @@ __all__ = [
     "RAY_QUERY_CLOSEST", "RAY_QUERY_ANY", "TRAVERSAL_STACKFREE", "TRAVERSAL_ESCAPE_LINK",
     "TRAVERSAL_STACKFULL", "OnesweepSort", "BVHGPUBuilder", "RayGenerator", "intersect",
     "render_normal", "render_ao", "render_pt", "pack", "profile_events", "FLT_MAX", "INVALID_NODE",
-    "QuantisedBVH", "intersect_quantised", "render_ao_quantised",
+    "QuantisedBVH", "intersect_quantised", "render_ao_quantised", "pt_diff_render", "pt_diff_adjoint",
 ]
 
 BUILD_OPTION_USE_NORMAL = 1   # minimum_lbvh.h:44
@@ -81,6 +81,8 @@ def lib() -> ctypes.CDLL:
             "mlbvh_render_ao_quantised": (i32, [_vp, _vp, i32, i32, _vp, _vp, _vp, _vp, _vp, i32, i32, f32, u32,
                                                 _vp, _vp, sz, _vp]),
             "mlbvh_camera_lookat": (i32, [_vp, _vp, _vp, _vp, f32, i32, i32]),
+            "mlbvh_pt_diff_render": (i32, [_vp, i32, i32, i32, i32, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+            "mlbvh_pt_diff_adjoint": (i32, [_vp, _vp, i32, i32, i32, i32, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -372,3 +374,27 @@ def render_ao_quantised(pixels, imageSize, rayGenerator: RayGenerator, q: Quanti
                                            int(useSobol), int(nSamples), float(radius), int(seed), _ptr(stats),
                                            _ptr(scratch), scratch.numel(), _stream(stream)))
     return pixels
+
+
+def pt_diff_render(image, imageSize, rayGenerator: RayGenerator, builder: BVHGPUBuilder, triangles, albedo, emission,
+                   spp: int, bounces: int = 3, stream=None):
+    """Fixed-depth differentiable path trace (float image, one value per
+    pixel) with per-triangle grey albedo and emission."""
+    w, h = imageSize
+    cam = rayGenerator._cstruct()
+    _check(lib().mlbvh_pt_diff_render(_ptr(image), int(w), int(h), int(spp), int(bounces), ctypes.addressof(cam),
+                                      _ptr(builder.m_rootNode), _ptr(builder.m_internals), _ptr(triangles),
+                                      _ptr(albedo), _ptr(emission), _stream(stream)))
+    return image
+
+
+def pt_diff_adjoint(grad_albedo, grad_image, imageSize, rayGenerator: RayGenerator, builder: BVHGPUBuilder, triangles,
+                    albedo, emission, spp: int, bounces: int = 3, stream=None):
+    """Path-replay adjoint: ADDS dLoss/dAlbedo to grad_albedo given
+    dLoss/dImage."""
+    w, h = imageSize
+    cam = rayGenerator._cstruct()
+    _check(lib().mlbvh_pt_diff_adjoint(_ptr(grad_albedo), _ptr(grad_image), int(w), int(h), int(spp), int(bounces),
+                                       ctypes.addressof(cam), _ptr(builder.m_rootNode), _ptr(builder.m_internals),
+                                       _ptr(triangles), _ptr(albedo), _ptr(emission), _stream(stream)))
+    return grad_albedo

@@ -1,0 +1,178 @@
+// Differentiable path tracing with a path-replay adjoint (no reference
+// counterpart): the gradient of an image loss with respect to per-triangle
+// albedo, for the fixed-depth, Russian-roulette-free estimator
+//
+//   I_p = 1/spp * sum_s L(path_s),   L = sum_{d=0..B} e(t_d) * prod_{j<d} a(t_j)
+//
+// where t_0 is the primary hit, t_1..t_B the hits after B cosine-sampled
+// bounces, e the per-triangle emission and a the per-triangle (grey) albedo.
+// Path geometry is that of pt (main_gpu.cu:179-272): Owen-Sobol sample
+// streams (dimension 0 for the pixel jitter, 1 + d for bounce d), normals
+// facing the incoming ray, origin offset n * 1e-4, Lambertian bounce whose
+// cosine/pdf cancels so the throughput is multiplied by the albedo.
+//
+// The adjoint replays every path from its sample index (paths are never
+// stored; Vicini et al., "Path Replay Backpropagation", 2021): with c_d the
+// radiance collected at vertex d, dL/da(t_j) = (sum_{d>j} c_d) / a(t_j), and
+// grad[t_j] += dLoss/dI_p / spp * that, scattered with atomic adds.
+#include "capi_internal.h"
+#include "../../include/mlbvh_device.cuh"
+
+namespace mlbvh {
+
+namespace {
+
+constexpr int kDiffThreads = 128;
+constexpr int kMaxBounces = 8;
+
+struct PathVertex {
+    uint32_t tri;
+    float collected;  // throughput * emission at this vertex
+};
+
+// Traces the path of sample s of pixel (xi, yi); returns its vertex count
+// and fills v (at most bounces + 1 vertices).
+__device__ __forceinline__ int trace_path(PathVertex* v, int bounces, uint32_t s, int xi, int yi, int w, int h,
+                                          const Camera& cam, uint32_t root, const mlbvh_internal_node* __restrict__ nodes,
+                                          const float* __restrict__ tris, const float* __restrict__ albedo,
+                                          const float* __restrict__ emission)
+{
+    const float2 jitter = sobol2d(s, (uint32_t)xi, (uint32_t)yi, 0u);
+    f3 ro, rd;
+    shoot(cam, ((float)xi + jitter.x) / (float)w, ((float)yi + jitter.y) / (float)h, ro, rd);
+    HitRecord hit;
+    hit.t = kFltMax;
+    hit.tri = 0xFFFFFFFFu;
+    trace_stackfree<false, false, true>(hit, nodes, tris, root, ro, rd, inv_rd(rd), 0.0f);
+    if (hit.t == kFltMax) return 0;
+    float throughput = 1.0f;
+    int count = 0;
+    for (int d = 0; d <= bounces; ++d) {
+        const uint32_t t = hit.tri;
+        v[count].tri = t;
+        v[count].collected = throughput * __ldg(emission + t);
+        ++count;
+        if (d == bounces) break;
+        const f3 p = ro + rd * hit.t;
+        f3 n = normalize(hit.ng);
+        if (0.0f < dot(n, rd)) n = -n;
+        f3 xaxis, zaxis;
+        onb(n, xaxis, zaxis);
+        const float2 r = sobol2d(s, (uint32_t)xi, (uint32_t)yi, (uint32_t)(1 + d));
+        const f3 dl = sample_hemisphere(r.x, r.y);
+        ro = p + n * 0.0001f;
+        rd = xaxis * dl.x + zaxis * dl.z + n * dl.y;
+        throughput = throughput * __ldg(albedo + t);
+        hit.t = kFltMax;
+        hit.tri = 0xFFFFFFFFu;
+        trace_stackfree<false, false, true>(hit, nodes, tris, root, ro, rd, inv_rd(rd), 0.0f);
+        if (hit.t == kFltMax) break;
+    }
+    return count;
+}
+
+__device__ __forceinline__ Camera camera_of(const mlbvh_ray_generator& g)
+{
+    Camera c;
+    c.origin = mk(g.origin[0], g.origin[1], g.origin[2]);
+    c.right = mk(g.right[0], g.right[1], g.right[2]);
+    c.up = mk(g.up[0], g.up[1], g.up[2]);
+    return c;
+}
+
+__global__ void __launch_bounds__(kDiffThreads)
+    k_pt_diff_render(float* __restrict__ image, int w, int h, int spp, int bounces, mlbvh_ray_generator gen,
+                     const mlbvh_node_index* __restrict__ rootPtr, const mlbvh_internal_node* __restrict__ nodes,
+                     const float* __restrict__ tris, const float* __restrict__ albedo,
+                     const float* __restrict__ emission)
+{
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= w * h) return;
+    const int xi = p % w, yi = p / w;
+    const Camera cam = camera_of(gen);
+    const uint32_t root = __ldg(rootPtr);
+    PathVertex v[kMaxBounces + 1];
+    float sum = 0.0f;
+    for (int s = 0; s < spp; ++s) {
+        const int n = trace_path(v, bounces, (uint32_t)s, xi, yi, w, h, cam, root, nodes, tris, albedo, emission);
+        float L = 0.0f;
+        for (int d = 0; d < n; ++d) L += v[d].collected;
+        sum += L;
+    }
+    image[p] = sum / (float)spp;
+}
+
+__global__ void __launch_bounds__(kDiffThreads)
+    k_pt_diff_adjoint(float* __restrict__ grad, const float* __restrict__ gradImage, int w, int h, int spp,
+                      int bounces, mlbvh_ray_generator gen, const mlbvh_node_index* __restrict__ rootPtr,
+                      const mlbvh_internal_node* __restrict__ nodes, const float* __restrict__ tris,
+                      const float* __restrict__ albedo, const float* __restrict__ emission)
+{
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= w * h) return;
+    const float g = __ldg(gradImage + p) / (float)spp;
+    if (g == 0.0f) return;
+    const int xi = p % w, yi = p / w;
+    const Camera cam = camera_of(gen);
+    const uint32_t root = __ldg(rootPtr);
+    PathVertex v[kMaxBounces + 1];
+    for (int s = 0; s < spp; ++s) {
+        const int n = trace_path(v, bounces, (uint32_t)s, xi, yi, w, h, cam, root, nodes, tris, albedo, emission);
+        // suffix sums of the collected radiance: the part of L that depends on
+        // the albedo of vertex j is everything collected after it
+        float after = 0.0f;
+        for (int j = n - 1; j >= 0; --j) {
+            if (j < bounces && after != 0.0f) {
+                const uint32_t t = v[j].tri;
+                atomicAdd(grad + t, g * after / __ldg(albedo + t));
+            }
+            after += v[j].collected;
+        }
+    }
+}
+
+mlbvh_status check_diff_args(int w, int h, int spp, int bounces, const void* a, const void* b, const void* c,
+                             const void* d, const void* e)
+{
+    if (w <= 0 || h <= 0 || (long long)w * h >= (1ll << 31)) return fail(MLBVH_ERR_INVALID_ARG, "bad image size");
+    if (spp <= 0) return fail(MLBVH_ERR_INVALID_ARG, "spp must be positive");
+    if (bounces < 0 || bounces > kMaxBounces) return fail(MLBVH_ERR_INVALID_ARG, "bounces must be in [0, 8]");
+    if (!a || !b || !c || !d || !e) return fail(MLBVH_ERR_INVALID_ARG, "null pointer");
+    if (!aligned16(a) || !aligned16(b) || !aligned16(c) || !aligned16(d) || !aligned16(e))
+        return fail(MLBVH_ERR_INVALID_ARG, "device pointers must be 16-byte aligned");
+    return MLBVH_OK;
+}
+
+}  // namespace
+
+mlbvh_status pt_diff_render(float* dImage, int w, int h, int spp, int bounces, const mlbvh_ray_generator& cam,
+                            const mlbvh_node_index* dRoot, const mlbvh_internal_node* dNodes,
+                            const mlbvh_triangle* dTris, const float* dAlbedo, const float* dEmission,
+                            cudaStream_t stream)
+{
+    if (mlbvh_status s = check_diff_args(w, h, spp, bounces, dImage, dRoot, dTris, dAlbedo, dEmission)) return s;
+    if (!aligned32(dNodes)) return fail(MLBVH_ERR_INVALID_ARG, "device pointers must be 16-byte aligned");
+    const int px = w * h;
+    k_pt_diff_render<<<(px + kDiffThreads - 1) / kDiffThreads, kDiffThreads, 0, stream>>>(
+        dImage, w, h, spp, bounces, cam, dRoot, dNodes, reinterpret_cast<const float*>(dTris), dAlbedo, dEmission);
+    MLBVH_CHECK_LAUNCH("k_pt_diff_render");
+    return MLBVH_OK;
+}
+
+mlbvh_status pt_diff_adjoint(float* dGrad, const float* dGradImage, int w, int h, int spp, int bounces,
+                             const mlbvh_ray_generator& cam, const mlbvh_node_index* dRoot,
+                             const mlbvh_internal_node* dNodes, const mlbvh_triangle* dTris, const float* dAlbedo,
+                             const float* dEmission, cudaStream_t stream)
+{
+    if (mlbvh_status s = check_diff_args(w, h, spp, bounces, dGrad, dRoot, dTris, dAlbedo, dEmission)) return s;
+    if (!dGradImage || !aligned16(dGradImage) || !aligned32(dNodes))
+        return fail(MLBVH_ERR_INVALID_ARG, "null or misaligned pointer");
+    const int px = w * h;
+    k_pt_diff_adjoint<<<(px + kDiffThreads - 1) / kDiffThreads, kDiffThreads, 0, stream>>>(
+        dGrad, dGradImage, w, h, spp, bounces, cam, dRoot, dNodes, reinterpret_cast<const float*>(dTris), dAlbedo,
+        dEmission);
+    MLBVH_CHECK_LAUNCH("k_pt_diff_adjoint");
+    return MLBVH_OK;
+}
+
+}  // namespace mlbvh

@@ -155,6 +155,28 @@ mlbvh_status mlbvh_render_ao_quantised(uint32_t* dPixels, uint32_t* dOccluded, i
                                as_stream(stream));
 }
 
+mlbvh_status mlbvh_pt_diff_render(float* dImage, int width, int height, int spp, int bounces,
+                                  const mlbvh_ray_generator* camera, const mlbvh_node_index* dRootNode,
+                                  const mlbvh_internal_node* dInternals, const mlbvh_triangle* dTriangles,
+                                  const float* dAlbedo, const float* dEmission, void* stream)
+{
+    clear_error();
+    if (!camera) return fail(MLBVH_ERR_INVALID_ARG, "null camera");
+    return pt_diff_render(dImage, width, height, spp, bounces, *camera, dRootNode, dInternals, dTriangles, dAlbedo,
+                          dEmission, as_stream(stream));
+}
+
+mlbvh_status mlbvh_pt_diff_adjoint(float* dGradAlbedo, const float* dGradImage, int width, int height, int spp,
+                                   int bounces, const mlbvh_ray_generator* camera, const mlbvh_node_index* dRootNode,
+                                   const mlbvh_internal_node* dInternals, const mlbvh_triangle* dTriangles,
+                                   const float* dAlbedo, const float* dEmission, void* stream)
+{
+    clear_error();
+    if (!camera) return fail(MLBVH_ERR_INVALID_ARG, "null camera");
+    return pt_diff_adjoint(dGradAlbedo, dGradImage, width, height, spp, bounces, *camera, dRootNode, dInternals,
+                           dTriangles, dAlbedo, dEmission, as_stream(stream));
+}
+
 void mlbvh_profile_events(void* startEvent, void* stopEvent)
 {
     set_profile_events(reinterpret_cast<cudaEvent_t>(startEvent), reinterpret_cast<cudaEvent_t>(stopEvent));

@@ -14,6 +14,8 @@ namespace mlbvh {
 mlbvh_status fail(mlbvh_status status, const char* message);
 void clear_error();
 inline bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
+// Node arrays are read with 32-byte loads.
+inline bool aligned32(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 31u) == 0; }
 int device_sm_count();
 
 // CUDA events (cudaEvent_t) that the next render_ao / build call on this host
@@ -64,5 +66,13 @@ mlbvh_status render_pt(float* dAccum, int w, int h, const mlbvh_ray_generator& c
                        const mlbvh_triangle_attrib* dAttribs, int useSobol, int maxSPP, int maxDepth,
                        cudaStream_t stream);
 mlbvh_status pack(uint32_t* dPixels, const float* dAccum, int n, cudaStream_t stream);
+mlbvh_status pt_diff_render(float* dImage, int w, int h, int spp, int bounces, const mlbvh_ray_generator& cam,
+                            const mlbvh_node_index* dRoot, const mlbvh_internal_node* dNodes,
+                            const mlbvh_triangle* dTris, const float* dAlbedo, const float* dEmission,
+                            cudaStream_t stream);
+mlbvh_status pt_diff_adjoint(float* dGrad, const float* dGradImage, int w, int h, int spp, int bounces,
+                             const mlbvh_ray_generator& cam, const mlbvh_node_index* dRoot,
+                             const mlbvh_internal_node* dNodes, const mlbvh_triangle* dTris, const float* dAlbedo,
+                             const float* dEmission, cudaStream_t stream);
 
 }  // namespace mlbvh

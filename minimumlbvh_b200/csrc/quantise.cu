@@ -144,7 +144,7 @@ __global__ void __launch_bounds__(kTraceThreads)
     hit.v = 0.0f;
     hit.ng = mk(0.0f, 0.0f, 0.0f);
     hit.tri = 0xFFFFFFFFu;
-    trace_quantised<kAny>(hit, qnodes, parents, qtris, __ldg(&header->root), __ldg(&header->eBase), ro, rd, inv_rd(rd),
+    trace_quantised<kAny, false, true>(hit, qnodes, parents, qtris, __ldg(&header->root), __ldg(&header->eBase), ro, rd, inv_rd(rd),
                           a.w);
     hits[2 * (size_t)i] = make_float4(hit.t, 0.0f, hit.u, hit.v);
     hits[2 * (size_t)i + 1] = make_float4(hit.ng.x, hit.ng.y, hit.ng.z, __uint_as_float(hit.tri));
@@ -159,9 +159,9 @@ mlbvh_status quantise(const mlbvh_internal_node* dNodes, const mlbvh_node_index*
     if (n == 0 || n > kQMaxLeaves) return fail(MLBVH_ERR_INVALID_ARG, "nTriangles must be in [1, 2^23]");
     if (!dRoot || !dTris || !dQTris || !dQHeader || (n > 1 && (!dNodes || !dQNodes || !dQParents)))
         return fail(MLBVH_ERR_INVALID_ARG, "null pointer");
-    if (!aligned16(dNodes) || !aligned16(dRoot) || !aligned16(dTris) || !aligned16(dQNodes) || !aligned16(dQParents) ||
+    if (!aligned16(dNodes) || !aligned16(dRoot) || !aligned16(dTris) || !aligned32(dQNodes) || !aligned16(dQParents) ||
         !aligned16(dQTris) || !aligned16(dQHeader))
-        return fail(MLBVH_ERR_INVALID_ARG, "device pointers must be 16-byte aligned");
+        return fail(MLBVH_ERR_INVALID_ARG, "device pointers must be 16-byte aligned (node arrays 32-byte)");
     const uint32_t threads = n > 1 ? n - 1 : 1;
     k_quantise<<<(threads + kQuantiseThreads - 1) / kQuantiseThreads, kQuantiseThreads, 0, stream>>>(
         dNodes, dRoot, reinterpret_cast<const float*>(dTris), n, dQNodes, dQParents, dQTris, dQHeader);
@@ -175,7 +175,7 @@ mlbvh_status trace_quantised(const mlbvh_qnode* dQNodes, const uint32_t* dQParen
 {
     if (nRays == 0) return MLBVH_OK;
     if (!dQTris || !dQHeader || !dRays || !dHits) return fail(MLBVH_ERR_INVALID_ARG, "null pointer");
-    if (!aligned16(dQNodes) || !aligned16(dQParents) || !aligned16(dQTris) || !aligned16(dQHeader) ||
+    if (!aligned32(dQNodes) || !aligned16(dQParents) || !aligned16(dQTris) || !aligned16(dQHeader) ||
         !aligned16(dRays) || !aligned16(dHits))
         return fail(MLBVH_ERR_INVALID_ARG, "device pointers must be 16-byte aligned");
     if (rayQuery != MLBVH_RAY_QUERY_CLOSEST && rayQuery != MLBVH_RAY_QUERY_ANY)

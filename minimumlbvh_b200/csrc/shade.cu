@@ -121,13 +121,13 @@ struct PlainTree {
     template <bool kAny, bool kCount>
     __device__ __forceinline__ void trace(const Ctx& c, HitRecord& hit, f3 ro, f3 rd, Counts& n) const
     {
-        trace_stackfree<kAny, kCount>(hit, nodes, tris, c.root, ro, rd, inv_rd(rd), 0.0f, &n.visits, &n.tests);
+        trace_stackfree<kAny, kCount, true>(hit, nodes, tris, c.root, ro, rd, inv_rd(rd), 0.0f, &n.visits, &n.tests);
     }
     template <bool kAny, bool kCount>
     __device__ __forceinline__ bool step(const Ctx&, uint32_t& curr, uint32_t& prev, HitRecord& hit, f3 ro, f3 rd,
                                          f3 inv, Counts& n) const
     {
-        return stackfree_step<kAny, kCount>(curr, prev, hit, nodes, tris, ro, rd, inv, 0.0f, n.visits, n.tests);
+        return stackfree_step<kAny, kCount, true>(curr, prev, hit, nodes, tris, ro, rd, inv, 0.0f, n.visits, n.tests);
     }
 };
 struct QuantTree {
@@ -146,14 +146,14 @@ struct QuantTree {
     template <bool kAny, bool kCount>
     __device__ __forceinline__ void trace(const Ctx& c, HitRecord& hit, f3 ro, f3 rd, Counts& n) const
     {
-        trace_quantised<kAny, kCount>(hit, qnodes, parents, qtris, c.root, c.eBase, ro, rd, inv_rd(rd), 0.0f,
+        trace_quantised<kAny, kCount, true>(hit, qnodes, parents, qtris, c.root, c.eBase, ro, rd, inv_rd(rd), 0.0f,
                                       &n.visits, &n.tests, &n.ups);
     }
     template <bool kAny, bool kCount>
     __device__ __forceinline__ bool step(const Ctx& c, uint32_t& curr, uint32_t& prev, HitRecord& hit, f3 ro, f3 rd,
                                          f3 inv, Counts& n) const
     {
-        return quantised_step<kAny, kCount>(curr, prev, hit, qnodes, parents, qtris, c.eBase, ro, rd, inv, 0.0f,
+        return quantised_step<kAny, kCount, true>(curr, prev, hit, qnodes, parents, qtris, c.eBase, ro, rd, inv, 0.0f,
                                             n.visits, n.tests, n.ups);
     }
 };
@@ -217,7 +217,7 @@ __global__ void __launch_bounds__(kTileW* kTileH)
 constexpr int kRefillBatch = 8;
 
 template <class Tree, bool kCount>
-__global__ void __launch_bounds__(kAoThreads)
+__global__ void __launch_bounds__(kAoThreads, 8)  // at most 64 registers: 32 warps per SM
     k_ao_rays(const AoRecord* __restrict__ records, const uint32_t* __restrict__ queueCount,
               uint32_t* __restrict__ workCounter, int w, int nSamples, float radius, uint32_t seed, int useSobol,
               Tree tree, uint32_t* __restrict__ counts, unsigned long long* __restrict__ stats)
@@ -346,7 +346,7 @@ __global__ void __launch_bounds__(kTileW* kTileH)
     HitRecord hit;
     hit.t = kFltMax;
     hit.tri = 0xFFFFFFFFu;
-    trace_stackfree<false>(hit, nodes, tris, __ldg(rootPtr), ro, rd, inv_rd(rd), 0.0f);
+    trace_stackfree<false, false, true>(hit, nodes, tris, __ldg(rootPtr), ro, rd, inv_rd(rd), 0.0f);
     uint32_t rgba;
     if (hit.t != kFltMax) {
         const f3 n = normalize(hit.ng);
@@ -395,7 +395,7 @@ __global__ void __launch_bounds__(kTileW* kTileH)
     HitRecord hit;
     hit.t = kFltMax;
     hit.tri = 0xFFFFFFFFu;
-    trace_stackfree<false>(hit, nodes, tris, root, ro, rd, inv_rd(rd), 0.0f);
+    trace_stackfree<false, false, true>(hit, nodes, tris, root, ro, rd, inv_rd(rd), 0.0f);
     if (hit.t != kFltMax)
         for (int depth = 0; depth < maxDepth; depth++) {
             const float2 r2 = rr.next();
@@ -421,7 +421,7 @@ __global__ void __launch_bounds__(kTileW* kTileH)
             hit.u = hit.v = 0.0f;
             hit.ng = mk(0.0f, 0.0f, 0.0f);
             hit.tri = 0xFFFFFFFFu;
-            trace_stackfree<false>(hit, nodes, tris, root, next_ro, next_rd, inv_rd(next_rd), 0.0f);
+            trace_stackfree<false, false, true>(hit, nodes, tris, root, next_ro, next_rd, inv_rd(next_rd), 0.0f);
             if (hit.t == kFltMax) break;
             ro = next_ro;
             rd = next_rd;
@@ -533,7 +533,7 @@ mlbvh_status render_normal(uint32_t* dPixels, int w, int h, const mlbvh_ray_gene
 {
     if (mlbvh_status s = check_image(w, h)) return s;
     if (!dPixels || !dRoot || !dTris) return fail(MLBVH_ERR_INVALID_ARG, "null pointer");
-    if (!aligned16(dPixels) || !aligned16(dRoot) || !aligned16(dNodes) || !aligned16(dTris))
+    if (!aligned16(dPixels) || !aligned16(dRoot) || !aligned32(dNodes) || !aligned16(dTris))
         return fail(MLBVH_ERR_INVALID_ARG, "device pointers must be 16-byte aligned");
     k_normal<<<tile_grid(w, h), kTileW * kTileH, 0, stream>>>(dPixels, cam, w, h, dRoot, dNodes,
                                                               reinterpret_cast<const float*>(dTris));
@@ -548,7 +548,7 @@ mlbvh_status render_ao(uint32_t* dPixels, uint32_t* dOccluded, int w, int h, con
 {
     if (mlbvh_status s = check_ao_args(w, h, nSamples, dPixels, dOccluded, dScratch, dStats)) return s;
     if (!dRoot || !dTris) return fail(MLBVH_ERR_INVALID_ARG, "null pointer");
-    if (!aligned16(dRoot) || !aligned16(dNodes) || !aligned16(dTris))
+    if (!aligned16(dRoot) || !aligned32(dNodes) || !aligned16(dTris))
         return fail(MLBVH_ERR_INVALID_ARG, "device pointers must be 16-byte aligned");
     const PlainTree tree{dNodes, reinterpret_cast<const float*>(dTris), dRoot};
     return launch_ao(dPixels, dOccluded, w, h, cam, tree, useSobol, nSamples, radius, seed, dStats, dScratch,
@@ -563,7 +563,7 @@ mlbvh_status render_ao_quantised(uint32_t* dPixels, uint32_t* dOccluded, int w, 
 {
     if (mlbvh_status s = check_ao_args(w, h, nSamples, dPixels, dOccluded, dScratch, dStats)) return s;
     if (!dQTris || !dQHeader) return fail(MLBVH_ERR_INVALID_ARG, "null pointer");
-    if (!aligned16(dQNodes) || !aligned16(dQParents) || !aligned16(dQTris) || !aligned16(dQHeader))
+    if (!aligned32(dQNodes) || !aligned16(dQParents) || !aligned16(dQTris) || !aligned16(dQHeader))
         return fail(MLBVH_ERR_INVALID_ARG, "device pointers must be 16-byte aligned");
     const QuantTree tree{dQNodes, dQParents, dQTris, dQHeader};
     return launch_ao(dPixels, dOccluded, w, h, cam, tree, useSobol, nSamples, radius, seed, dStats, dScratch,
@@ -577,7 +577,7 @@ mlbvh_status render_pt(float* dAccum, int w, int h, const mlbvh_ray_generator& c
 {
     if (mlbvh_status s = check_image(w, h)) return s;
     if (!dAccum || !dRoot || !dTris || !dAttribs) return fail(MLBVH_ERR_INVALID_ARG, "null pointer");
-    if (!aligned16(dAccum) || !aligned16(dRoot) || !aligned16(dNodes) || !aligned16(dTris) || !aligned16(dAttribs))
+    if (!aligned16(dAccum) || !aligned16(dRoot) || !aligned32(dNodes) || !aligned16(dTris) || !aligned16(dAttribs))
         return fail(MLBVH_ERR_INVALID_ARG, "device pointers must be 16-byte aligned");
     if (maxDepth < 0) return fail(MLBVH_ERR_INVALID_ARG, "maxDepth must be >= 0");
     k_pt<<<tile_grid(w, h), kTileW * kTileH, 0, stream>>>(reinterpret_cast<float4*>(dAccum), cam, w, h, dRoot, dNodes,

@@ -37,7 +37,7 @@ __global__ void __launch_bounds__(kTraceThreads)
         uint32_t stack[64];
         trace_stackfull(hit, nodes, tris, root, ro, rd, inv, tmin, stack, 64);
     } else {
-        trace_stackfree<kAny>(hit, nodes, tris, root, ro, rd, inv, tmin);
+        trace_stackfree<kAny, false, true>(hit, nodes, tris, root, ro, rd, inv, tmin);
     }
     hits[2 * (size_t)i] = make_float4(hit.t, 0.0f, hit.u, hit.v);
     hits[2 * (size_t)i + 1] = make_float4(hit.ng.x, hit.ng.y, hit.ng.z, __uint_as_float(hit.tri));
@@ -51,8 +51,8 @@ mlbvh_status trace(const mlbvh_internal_node* dNodes, const mlbvh_node_index* dR
 {
     if (nRays == 0) return MLBVH_OK;
     if (!dRoot || !dTris || !dRays || !dHits) return fail(MLBVH_ERR_INVALID_ARG, "null pointer");
-    if (!aligned16(dNodes) || !aligned16(dRoot) || !aligned16(dTris) || !aligned16(dRays) || !aligned16(dHits))
-        return fail(MLBVH_ERR_INVALID_ARG, "device pointers must be 16-byte aligned");
+    if (!aligned32(dNodes) || !aligned16(dRoot) || !aligned16(dTris) || !aligned16(dRays) || !aligned16(dHits))
+        return fail(MLBVH_ERR_INVALID_ARG, "device pointers must be 16-byte aligned (node arrays 32-byte)");
     if (rayQuery != MLBVH_RAY_QUERY_CLOSEST && rayQuery != MLBVH_RAY_QUERY_ANY)
         return fail(MLBVH_ERR_INVALID_ARG, "rayQuery must be MLBVH_RAY_QUERY_CLOSEST or MLBVH_RAY_QUERY_ANY");
     const bool any = rayQuery == MLBVH_RAY_QUERY_ANY;

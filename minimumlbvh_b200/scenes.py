@@ -27,6 +27,9 @@ __all__ = [
     "camera_heightfield",
     "camera_soup",
     "pt_attributes",
+    "quad_light",
+    "diff_scene",
+    "albedo",
 ]
 
 
@@ -156,3 +159,26 @@ def pt_attributes(n: int, seed: int = 3, light_fraction: float = 0.002) -> np.nd
     emit = rng.random(n) < light_fraction
     a[emit, 12:15] = 10.0
     return a
+
+
+def quad_light(y: float = 1.4, half: float = 0.25) -> np.ndarray:
+    """A 0.5 x 0.5 horizontal quad (two triangles) centred above the
+    heightfield at height y: float32 (2, 9)."""
+    a, b, c, d = (-half, y, -half), (half, y, -half), (half, y, half), (-half, y, half)
+    return np.array([a + b + c, a + c + d], dtype=np.float32)
+
+
+def diff_scene(seed: int = 0, albedo_seed: int = 1, light_radiance: float = 10.0):
+    """The differentiable-rendering scene: the 212,992-triangle heightfield +
+    icospheres with a quad light of radiance 10 appended (212,994 triangles),
+    per-triangle grey albedo uniform in [0.1, 0.9] (seeded) and emission
+    (light_radiance on the two light triangles, 0 elsewhere)."""
+    tris = np.concatenate([heightfield_icospheres(seed), quad_light()])
+    emission = np.zeros(len(tris), np.float32)
+    emission[-2:] = light_radiance
+    return tris, albedo(len(tris), albedo_seed), emission
+
+
+def albedo(n: int, seed: int) -> np.ndarray:
+    """Per-triangle grey albedo uniform in [0.1, 0.9] (float32)."""
+    return np.random.default_rng(seed).uniform(0.1, 0.9, n).astype(np.float32)

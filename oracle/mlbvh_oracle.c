@@ -1439,3 +1439,147 @@ void orc_trace_quantised(const uint32_t* qnodes, const uint32_t* parents, const 
     c.ups = ups;
     orc_parallel_for(nRays, 1024, qtrace_range, &c);
 }
+
+/* ------------------------------------------------ differentiable path trace
+ * Restates csrc/adjoint.cu (no reference counterpart). The path geometry
+ * (hits, directions) is computed in FP32 exactly as the kernels do, so the
+ * paths are the GPU's; the radiance and the gradient are accumulated either
+ * in FP32 in the kernels' order (for bit-exact image parity) or in FP64 (the
+ * FP64 host adjoint and the finite differences). */
+#define ORC_MAX_BOUNCES 8
+
+static int diff_path(uint32_t* tri, int bounces, uint32_t s, int xi, int yi, int w, int h, const orc_camera* cam,
+                     uint32_t root, const orc_node* nodes, const orc_triangle* tris)
+{
+    float jx, jy;
+    orc_sobol(s, (uint32_t)xi, (uint32_t)yi, 0u, &jx, &jy);
+    orc_f3 ro, rd;
+    orc_shoot(cam, ((float)xi + jx) / (float)w, ((float)yi + jy) / (float)h, &ro, &rd);
+    orc_hit hit;
+    hit_init(&hit, ORC_FLT_MAX);
+    uint32_t nv = 0, nt = 0;
+    trace_stackfree(&hit, nodes, tris, root, ro, rd, inv_rd(rd), 0.0f, 0, &nv, &nt);
+    if (hit.t == ORC_FLT_MAX) return 0;
+    int count = 0;
+    for (int d = 0; d <= bounces; ++d)
+    {
+        tri[count++] = hit.triangleIndex;
+        if (d == bounces) break;
+        orc_f3 p = add3(ro, muls(rd, hit.t));
+        orc_f3 n = normalize3(hit.ng);
+        if (0.0f < dot3(n, rd)) n = neg3(n);
+        orc_f3 xaxis, zaxis;
+        onb(n, &xaxis, &zaxis);
+        float r0, r1;
+        orc_sobol(s, (uint32_t)xi, (uint32_t)yi, (uint32_t)(1 + d), &r0, &r1);
+        orc_f3 dl = sample_hemisphere(r0, r1, ORC_TRIG_PORTABLE);
+        ro = add3(p, muls(n, 0.0001f));
+        rd = add3(add3(muls(xaxis, dl.x), muls(zaxis, dl.z)), muls(n, dl.y));
+        hit_init(&hit, ORC_FLT_MAX);
+        trace_stackfree(&hit, nodes, tris, root, ro, rd, inv_rd(rd), 0.0f, 0, &nv, &nt);
+        if (hit.t == ORC_FLT_MAX) break;
+    }
+    return count;
+}
+
+typedef struct {
+    int w, h, spp, bounces;
+    const orc_camera* cam;
+    uint32_t root;
+    const orc_node* nodes;
+    const orc_triangle* tris;
+    const float* albedo32;
+    const float* emission32;
+    const double* albedo64;
+    const double* emission64;
+    float* image32;
+    double* image64;
+    const double* gradImage;
+    double* grad;
+} diff_ctx;
+
+static void atomic_add_double(double* p, double v)
+{
+    uint64_t old = __atomic_load_n((uint64_t*)p, __ATOMIC_RELAXED), upd;
+    do
+    {
+        double cur;
+        memcpy(&cur, &old, 8);
+        cur += v;
+        memcpy(&upd, &cur, 8);
+    } while (!__atomic_compare_exchange_n((uint64_t*)p, &old, upd, 1, __ATOMIC_RELAXED, __ATOMIC_RELAXED));
+}
+
+static void diff_rows(void* p, uint32_t b, uint32_t e)
+{
+    diff_ctx* c = (diff_ctx*)p;
+    uint32_t tri[ORC_MAX_BOUNCES + 1];
+    for (uint32_t y = b; y < e; ++y)
+        for (int x = 0; x < c->w; ++x)
+        {
+            int px = x + (int)y * c->w;
+            float sum32 = 0.0f;
+            double sum64 = 0.0;
+            double g = c->gradImage ? c->gradImage[px] / (double)c->spp : 0.0;
+            for (int s = 0; s < c->spp; ++s)
+            {
+                int n = diff_path(tri, c->bounces, (uint32_t)s, x, (int)y, c->w, c->h, c->cam, c->root, c->nodes, c->tris);
+                if (c->image32)
+                {
+                    float thr = 1.0f, L = 0.0f;
+                    float coll[ORC_MAX_BOUNCES + 1];
+                    for (int d = 0; d < n; ++d)
+                    {
+                        coll[d] = thr * c->emission32[tri[d]];
+                        if (d < c->bounces) thr = thr * c->albedo32[tri[d]];
+                    }
+                    for (int d = 0; d < n; ++d) L += coll[d];
+                    sum32 += L;
+                }
+                if (c->image64 || c->grad)
+                {
+                    double thr = 1.0, coll[ORC_MAX_BOUNCES + 1];
+                    for (int d = 0; d < n; ++d)
+                    {
+                        coll[d] = thr * c->emission64[tri[d]];
+                        thr *= c->albedo64[tri[d]];
+                    }
+                    if (c->image64)
+                        for (int d = 0; d < n; ++d) sum64 += coll[d];
+                    if (c->grad && g != 0.0)
+                    {
+                        double after = 0.0;
+                        for (int j = n - 1; j >= 0; --j)
+                        {
+                            if (j < c->bounces && after != 0.0)
+                                atomic_add_double(&c->grad[tri[j]], g * after / c->albedo64[tri[j]]);
+                            after += coll[j];
+                        }
+                    }
+                }
+            }
+            if (c->image32) c->image32[px] = sum32 / (float)c->spp;
+            if (c->image64) c->image64[px] = sum64 / (double)c->spp;
+        }
+}
+
+/* k_pt_diff_render in FP32 (bit-exact with the kernel) and/or FP64. */
+void orc_pt_diff_render(float* image32, double* image64, int w, int h, int spp, int bounces, const orc_camera* cam,
+                        uint32_t root, const orc_node* nodes, const orc_triangle* tris, const float* albedo32,
+                        const float* emission32, const double* albedo64, const double* emission64)
+{
+    diff_ctx c = {w, h, spp, bounces, cam, root, nodes, tris, albedo32, emission32, albedo64, emission64,
+                  image32, image64, NULL, NULL};
+    orc_parallel_for((uint32_t)h, 1, diff_rows, &c);
+}
+
+/* The FP64 host adjoint: grad[t] += sum over paths of dLoss/dI_p / spp *
+ * (radiance collected after each scattering at t) / albedo[t]. */
+void orc_pt_diff_adjoint(double* grad, const double* gradImage, int w, int h, int spp, int bounces,
+                         const orc_camera* cam, uint32_t root, const orc_node* nodes, const orc_triangle* tris,
+                         const double* albedo64, const double* emission64)
+{
+    diff_ctx c = {w, h, spp, bounces, cam, root, nodes, tris, NULL, NULL, albedo64, emission64, NULL, NULL,
+                  gradImage, grad};
+    orc_parallel_for((uint32_t)h, 1, diff_rows, &c);
+}

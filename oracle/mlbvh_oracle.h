@@ -130,6 +130,17 @@ void orc_trace_quantised(const uint32_t* qnodes, const uint32_t* parents, const 
                          const orc_ray* rays, uint32_t nRays, int query, orc_hit* hits, uint32_t* visits,
                          uint32_t* tests, uint32_t* ups);
 
+/* Differentiable path tracing (no reference counterpart): the render and
+ * path-replay adjoint of csrc/adjoint.cu. image32 (nullable) is the kernel's
+ * FP32 image bit for bit; image64 (nullable) and the adjoint accumulate in
+ * FP64 over the same FP32 path geometry. */
+void orc_pt_diff_render(float* image32, double* image64, int w, int h, int spp, int bounces, const orc_camera* cam,
+                        uint32_t root, const orc_node* nodes, const orc_triangle* tris, const float* albedo32,
+                        const float* emission32, const double* albedo64, const double* emission64);
+void orc_pt_diff_adjoint(double* grad, const double* gradImage, int w, int h, int spp, int bounces,
+                         const orc_camera* cam, uint32_t root, const orc_node* nodes, const orc_triangle* tris,
+                         const double* albedo64, const double* emission64);
+
 #ifdef __cplusplus
 }
 #endif

@@ -73,6 +73,8 @@ def oracle() -> ctypes.CDLL:
             "orc_quantise": (_i32, [_vp, _u32, _vp, _u32, _vp, _vp, _vp, _vp]),
             "orc_check_quantised": (_i32, [_vp, _u32, _vp, _vp]),
             "orc_trace_quantised": (None, [_vp, _vp, _vp, _vp, _vp, _u32, _i32, _vp, _vp, _vp, _vp]),
+            "orc_pt_diff_render": (None, [_vp, _vp, _i32, _i32, _i32, _i32, _vp, _u32, _vp, _vp, _vp, _vp, _vp, _vp]),
+            "orc_pt_diff_adjoint": (None, [_vp, _vp, _i32, _i32, _i32, _i32, _vp, _u32, _vp, _vp, _vp, _vp]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -255,3 +257,28 @@ def trace_quantised(q: dict, rays, query=0, counters=False):
     if counters:
         return hits, nv, nt, nu
     return hits
+
+
+def diff_render(b, tris, cam, w, h, spp, bounces, albedo, emission, fp64=False):
+    """Oracle differentiable render: FP32 image (the kernel's, bit for bit) or
+    FP64 image over the same path geometry."""
+    img32 = None if fp64 else np.zeros(w * h, np.float32)
+    img64 = np.zeros(w * h, np.float64) if fp64 else None
+    oracle().orc_pt_diff_render(P(img32), P(img64), w, h, spp, bounces, P(np.ascontiguousarray(cam, np.float32)),
+                                b["root"], P(np.ascontiguousarray(b["nodes"], np.uint32)),
+                                P(np.ascontiguousarray(tris, np.float32)), P(np.ascontiguousarray(albedo, np.float32)),
+                                P(np.ascontiguousarray(emission, np.float32)),
+                                P(np.ascontiguousarray(albedo, np.float64)),
+                                P(np.ascontiguousarray(emission, np.float64)))
+    return img64 if fp64 else img32
+
+
+def diff_adjoint(b, tris, cam, w, h, spp, bounces, albedo, emission, grad_image):
+    """The FP64 host adjoint: dLoss/dAlbedo given dLoss/dImage."""
+    grad = np.zeros(len(tris), np.float64)
+    oracle().orc_pt_diff_adjoint(P(grad), P(np.ascontiguousarray(grad_image, np.float64)), w, h, spp, bounces,
+                                 P(np.ascontiguousarray(cam, np.float32)), b["root"],
+                                 P(np.ascontiguousarray(b["nodes"], np.uint32)), P(np.ascontiguousarray(tris, np.float32)),
+                                 P(np.ascontiguousarray(albedo, np.float64)),
+                                 P(np.ascontiguousarray(emission, np.float64)))
+    return grad
