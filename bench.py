@@ -191,6 +191,97 @@ def cpu_build_baseline(tris):
     return {"mtri_s": n / dt / 1e6, "ms": dt * 1e3, "kind": "port", "what": "oracle build (serial)"}
 
 
+def bench_batched(args, dev, stream, barrier, max_over_ranks, world):
+    """The batched workload: 1,024 meshes with log-uniform 64..262,144
+    triangles (30.8M in all) and log-uniform 4,096..1,048,576 incoherent rays
+    each (169M), generated on the device. Build + traversal run as one CUDA
+    graph launch with autotuned parameters; the plain form is the same work as
+    1,024 mlbvh_build + 1,024 mlbvh_trace calls. Inputs are larger than L2."""
+    import torch
+    import minimumlbvh_b200 as mb
+    from minimumlbvh_b200 import scenes
+    tris, offsets = scenes.batched_soup(1024, 64, 262_144, seed=7, device=dev)
+    rays, roff = scenes.batched_rays(tris, offsets, 4096, 1_048_576, seed=8)
+    nm, n, nr = len(offsets) - 1, int(offsets[-1]), int(roff[-1])
+    bb = mb.BatchedBVH(tris, torch.as_tensor(offsets.astype(np.int32), device=dev), nm)
+    bb.set_rays(rays, torch.as_tensor(roff.astype(np.int32), device=dev))
+    params, tune_build_ms, tune_trace_ms = bb.autotune()
+    bb.status()
+    graph = bb.graph(params, stages=3)
+    steps = max(1, args.steps)
+    for _ in range(args.warmup):
+        graph.launch()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    bev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    tev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    barrier()
+    torch.cuda.synchronize()
+    for i in range(steps):
+        ev[i][0].record(stream)
+        graph.launch()
+        ev[i][1].record(stream)
+    for i in range(steps):
+        bev[i][0].record(stream)
+        bb.build(params)
+        bev[i][1].record(stream)
+        tev[i][0].record(stream)
+        bb.trace(params)
+        tev[i][1].record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    bb.status()
+    graph.close()
+    graph_s = max_over_ranks(sum(a.elapsed_time(b) for a, b in ev) / 1e3 / steps)
+    build_s = max_over_ranks(sum(a.elapsed_time(b) for a, b in bev) / 1e3 / steps)
+    trace_s = max_over_ranks(sum(a.elapsed_time(b) for a, b in tev) / 1e3 / steps)
+    hits = bb.hits.clone()
+
+    # the plain form: the same meshes and rays, one mesh per call
+    meshes = [tris[int(offsets[m]):int(offsets[m + 1])].clone() for m in range(nm)]
+    builders = [mb.BVHGPUBuilder() for _ in range(nm)]
+    sorter = mb.OnesweepSort(dev.index)
+    sorter.reserve(mb.lib().mlbvh_build_scratch_bytes(int(np.diff(offsets).max())))
+    plain_hits = torch.empty_like(hits)
+
+    def plain_build():
+        for m in range(nm):
+            builders[m].build(meshes[m], meshes[m].shape[0], 0, sorter)
+
+    def plain_trace():
+        for m in range(nm):
+            r0, r1 = int(roff[m]), int(roff[m + 1])
+            mb.intersect(builders[m], meshes[m], rays[r0:r1], hits=plain_hits[r0:r1])
+
+    plain_build()
+    plain_trace()
+    torch.cuda.synchronize()
+    pev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    barrier()
+    torch.cuda.synchronize()
+    pev[0].record(stream)
+    plain_build()
+    pev[1].record(stream)
+    plain_trace()
+    pev[2].record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    pb_s = max_over_ranks(pev[0].elapsed_time(pev[1]) / 1e3)
+    pt_s = max_over_ranks(pev[1].elapsed_time(pev[2]) / 1e3)
+    agree = float((plain_hits == hits).all(1).float().mean().item())
+    return {
+        "workload": "batched1024", "meshes": nm, "triangles": n, "rays": nr,
+        "value": nr * world / trace_s / 1e6, "unit": "Mrays/s (persistent queue traversal)",
+        "build_ms": build_s * 1e3, "build_mtri_s": n * world / build_s / 1e6, "trace_ms": trace_s * 1e3,
+        "graph_ms": graph_s * 1e3, "graph_mrays_s": nr * world / graph_s / 1e6,
+        "plain_build_ms": pb_s * 1e3, "plain_trace_ms": pt_s * 1e3, "plain_mrays_s": nr * world / pt_s / 1e6,
+        "vs_plain_trace": pt_s / trace_s, "vs_plain_build": pb_s / build_s,
+        "vs_plain_build_plus_trace": (pb_s + pt_s) / graph_s, "hit_agreement": agree,
+        "params": params.as_dict(), "autotune_ms": {"build": tune_build_ms, "trace": tune_trace_ms},
+        # graph (8 build kernels + traversal) and direct build + traversal per step; the plain loop once
+        "launches": steps * 18 + 8 * nm,
+    }
+
+
 def run_reference(args, wl, rank):
     """The reference's own CPU implementation of the path, all host threads."""
     if rank != 0:
@@ -234,6 +325,7 @@ def main():
     ap.add_argument("--ref-seconds", type=float, default=4.0, help="wall time of one reference-arm step")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--image", default=None, help="override the frame size, WxH (small cases for ncu captures)")
+    ap.add_argument("--no-batched", action="store_true", help="skip the batched (1,024-mesh) workload")
     args = ap.parse_args()
     wl = dict(WORKLOADS[args.workload])
     if args.image:
@@ -376,6 +468,7 @@ def main():
         torch.cuda.synchronize()
         barrier()
         e2e_s = max_over_ranks(eev[0].elapsed_time(eev[1]) / 1e3)
+        batched = None if args.no_batched else bench_batched(args, dev, stream, barrier, max_over_ranks, world)
     clocks = sampler.summary()
 
     ms_per_step = ao_total_s * 1e3 / args.steps
@@ -421,6 +514,9 @@ def main():
         "plain_node_bytes_per_ray": 64 * visits / max(rays_per_frame, 1),
         "tri_bytes_per_ray": 48 * int(qst[2]) / max(q_rays, 1),
         "plain_tri_bytes_per_ray": 36 * tests / max(rays_per_frame, 1)}
+    if batched is not None:
+        line["batched"] = batched
+        line["gpu_launches"] += batched["launches"]
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         out = {"nodes": builder.m_internals.cpu().numpy().view(np.uint32)[: n - 1],
                "root": int(builder.m_rootNode.cpu().numpy().view(np.uint32)[0])}

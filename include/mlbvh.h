@@ -203,6 +203,77 @@ MLBVH_API mlbvh_status mlbvh_render_ao_quantised(uint32_t* dPixels, uint32_t* dO
                                                  float radius, uint32_t sobolSeed, unsigned long long* dStats,
                                                  void* dScratch, size_t scratchBytes, void* stream);
 
+/* --------------------------------------------------------- batched form ---
+ * No reference counterpart (the reference builds one mesh per
+ * BVHGPUBuilder::build call). Many independent meshes of uneven size, laid
+ * out back to back, are built by one launch chain, and a batch of rays, each
+ * aimed at one mesh, is drained by one persistent work-queue kernel.
+ *
+ * Layout: mesh m owns triangles [o[m], o[m+1]) of dTriangles (o =
+ * dMeshTriangleOffsets, nMeshes + 1 device words, o[0] = 0, o[nMeshes] =
+ * nTriangles, every mesh at least one triangle), internal nodes
+ * [o[m] - m, o[m+1] - m - 1) of dInternals (nTriangles - nMeshes nodes in
+ * all), and dRootNodes[m]. Node and leaf indices inside a tree are local to
+ * its mesh, and every tree is bit-identical to mlbvh_build of that mesh alone.
+ * Rays [r[m], r[m+1]) of dRays (r = dMeshRayOffsets, nondecreasing, r[0] = 0,
+ * r[nMeshes] = nRays) query mesh m; dHits[i] is ray i's hit as mlbvh_trace
+ * writes it, with the triangle index local to the mesh.
+ * Bad triangle offsets are detected on the device: nothing is built or
+ * traced, and mlbvh_scratch_status(dScratch) reports MLBVH_ERR_INVALID_ARG. */
+typedef struct mlbvh_batch {
+    const mlbvh_triangle* dTriangles;
+    const uint32_t* dMeshTriangleOffsets;
+    uint32_t nMeshes;    /* 1 .. 2^20 */
+    uint32_t nTriangles; /* nMeshes .. 2^30 - 1 */
+    uint32_t buildOption;
+    int rayQuery;        /* MLBVH_RAY_QUERY_CLOSEST or _ANY */
+    mlbvh_internal_node* dInternals;
+    mlbvh_node_index* dRootNodes;
+    mlbvh_aabb* dMeshAABBs; /* nMeshes, may be NULL */
+    const mlbvh_ray* dRays;
+    const uint32_t* dMeshRayOffsets;
+    uint32_t nRays;         /* below 2^31 */
+    uint32_t _pad;
+    mlbvh_hit* dHits;
+    void* dScratch;         /* mlbvh_batch_scratch_bytes(nMeshes, nTriangles); build and trace of one batch share it */
+    size_t scratchBytes;
+} mlbvh_batch;
+
+/* Launch parameters, chosen by mlbvh_batch_autotune; results do not depend
+ * on them (only the time does). */
+typedef struct mlbvh_batch_params {
+    int digitBits;   /* radix digit width of the build's sort: 8 (4 passes) or 11 (3 passes) */
+    int traceBlock;  /* threads per CTA of the traversal kernel: 64, 128, 256 or 512 */
+    int queueChunk;  /* rays a warp takes from the queue per atomic: 1 .. 65536 */
+    int refillLanes; /* idle lanes of a warp that trigger taking more rays: 1 .. 32 */
+} mlbvh_batch_params;
+
+typedef struct mlbvh_batch_graph mlbvh_batch_graph; /* opaque */
+
+MLBVH_API size_t mlbvh_batch_scratch_bytes(uint32_t nMeshes, uint32_t nTriangles);
+/* Defaults: 8-bit digits, 128 threads, chunks of 64 rays, refill at 8 idle lanes. */
+MLBVH_API void mlbvh_batch_params_default(mlbvh_batch_params* params);
+/* Builds every mesh's tree (params may be NULL: the defaults). */
+MLBVH_API mlbvh_status mlbvh_build_batched(const mlbvh_batch* batch, const mlbvh_batch_params* params, void* stream);
+/* Traces every ray against its mesh's tree (built by mlbvh_build_batched with
+ * the same dScratch, whose header it reads). */
+MLBVH_API mlbvh_status mlbvh_trace_batched(const mlbvh_batch* batch, const mlbvh_batch_params* params, void* stream);
+/* Times candidate parameters on this batch (the digit width on the build,
+ * then block size, queue chunk and refill threshold on the traversal, one at
+ * a time) and writes the fastest to *params; *buildMs / *traceMs (may be
+ * NULL) receive their median times. Runs the build and the traversal many
+ * times, overwriting the outputs, and synchronises `stream`. */
+MLBVH_API mlbvh_status mlbvh_batch_autotune(const mlbvh_batch* batch, mlbvh_batch_params* params, float* buildMs,
+                                            float* traceMs, void* stream);
+/* Captures the build (stages = 1), the traversal (2) or both (3) of this
+ * batch into a CUDA graph. The graph keeps the batch's pointers and sizes;
+ * each launch reads the buffers' contents at that time, so new triangles or
+ * rays of the same sizes need no new capture. */
+MLBVH_API mlbvh_status mlbvh_batch_graph_create(const mlbvh_batch* batch, const mlbvh_batch_params* params,
+                                                int stages, mlbvh_batch_graph** graph);
+MLBVH_API mlbvh_status mlbvh_batch_graph_launch(mlbvh_batch_graph* graph, void* stream);
+MLBVH_API void mlbvh_batch_graph_destroy(mlbvh_batch_graph* graph);
+
 /* --------------------------------------------------------------- shading ---
  * The reference's shading kernels (main_gpu.cu), one launch chain each.
  * `camera` is a HOST pointer (passed by value to the kernels, as the

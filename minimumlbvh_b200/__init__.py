@@ -22,6 +22,7 @@ __all__ = [
     "TRAVERSAL_STACKFULL", "OnesweepSort", "BVHGPUBuilder", "RayGenerator", "intersect",
     "render_normal", "render_ao", "render_pt", "pack", "profile_events", "FLT_MAX", "INVALID_NODE",
     "QuantisedBVH", "intersect_quantised", "render_ao_quantised", "pt_diff_render", "pt_diff_adjoint",
+    "BatchParams", "BatchedBVH",
 ]
 
 BUILD_OPTION_USE_NORMAL = 1   # minimum_lbvh.h:44
@@ -83,6 +84,14 @@ def lib() -> ctypes.CDLL:
             "mlbvh_camera_lookat": (i32, [_vp, _vp, _vp, _vp, f32, i32, i32]),
             "mlbvh_pt_diff_render": (i32, [_vp, i32, i32, i32, i32, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
             "mlbvh_pt_diff_adjoint": (i32, [_vp, _vp, i32, i32, i32, i32, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+            "mlbvh_batch_scratch_bytes": (sz, [u32, u32]),
+            "mlbvh_batch_params_default": (None, [_vp]),
+            "mlbvh_build_batched": (i32, [_vp, _vp, _vp]),
+            "mlbvh_trace_batched": (i32, [_vp, _vp, _vp]),
+            "mlbvh_batch_autotune": (i32, [_vp, _vp, _vp, _vp, _vp]),
+            "mlbvh_batch_graph_create": (i32, [_vp, _vp, i32, _vp]),
+            "mlbvh_batch_graph_launch": (i32, [_vp, _vp]),
+            "mlbvh_batch_graph_destroy": (None, [_vp]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -398,3 +407,130 @@ def pt_diff_adjoint(grad_albedo, grad_image, imageSize, rayGenerator: RayGenerat
                                        ctypes.addressof(cam), _ptr(builder.m_rootNode), _ptr(builder.m_internals),
                                        _ptr(triangles), _ptr(albedo), _ptr(emission), _stream(stream)))
     return grad_albedo
+
+
+class BatchParams(ctypes.Structure):
+    """mlbvh_batch_params: launch parameters of the batched form."""
+    _fields_ = [("digitBits", ctypes.c_int), ("traceBlock", ctypes.c_int), ("queueChunk", ctypes.c_int),
+                ("refillLanes", ctypes.c_int)]
+
+    @classmethod
+    def default(cls) -> "BatchParams":
+        p = cls()
+        lib().mlbvh_batch_params_default(ctypes.byref(p))
+        return p
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class _Batch(ctypes.Structure):
+    _fields_ = [("dTriangles", _vp), ("dMeshTriangleOffsets", _vp), ("nMeshes", ctypes.c_uint32),
+                ("nTriangles", ctypes.c_uint32), ("buildOption", ctypes.c_uint32), ("rayQuery", ctypes.c_int),
+                ("dInternals", _vp), ("dRootNodes", _vp), ("dMeshAABBs", _vp), ("dRays", _vp),
+                ("dMeshRayOffsets", _vp), ("nRays", ctypes.c_uint32), ("_pad", ctypes.c_uint32), ("dHits", _vp),
+                ("dScratch", _vp), ("scratchBytes", ctypes.c_size_t)]
+
+
+class BatchedBVH:
+    """Many meshes built in one launch chain and traced by one persistent
+    kernel (mlbvh_build_batched / mlbvh_trace_batched; no reference
+    counterpart). ``triangles`` is float32 (nTriangles, 9) with the meshes back
+    to back; ``tri_offsets`` (nMeshes + 1, int32 on the device) bounds them.
+    After ``build``, ``internals`` (nTriangles - nMeshes rows of 16 words),
+    ``roots`` (nMeshes) and ``mesh_aabbs`` (nMeshes x 6) hold the trees: mesh
+    m's nodes start at row tri_offsets[m] - m."""
+
+    def __init__(self, triangles, tri_offsets, n_meshes: int, buildOption: int = 0):
+        import torch
+        _require_cuda(triangles, "triangles")
+        _require_cuda(tri_offsets, "tri_offsets")
+        dev = triangles.device
+        self.triangles, self.tri_offsets = triangles, tri_offsets
+        self.nMeshes, self.nTriangles = int(n_meshes), triangles.numel() // 9
+        nbytes = lib().mlbvh_batch_scratch_bytes(self.nMeshes, self.nTriangles)
+        if nbytes == 0:
+            raise MlbvhError(1, "nMeshes must be in [1, 2^20] and nTriangles in [nMeshes, 2^30)")
+        self.scratch = torch.empty(nbytes, dtype=torch.uint8, device=dev)
+        self.internals = torch.empty((max(self.nTriangles - self.nMeshes, 1), 16), dtype=torch.int32, device=dev)
+        self.roots = torch.empty(max(self.nMeshes, 4), dtype=torch.int32, device=dev)
+        self.mesh_aabbs = torch.empty((self.nMeshes, 6), dtype=torch.float32, device=dev)
+        self.rays = self.ray_offsets = self.hits = None
+        self.nRays = 0
+        self._desc = _Batch()
+        d = self._desc
+        d.dTriangles, d.dMeshTriangleOffsets = _ptr(triangles), _ptr(tri_offsets)
+        d.nMeshes, d.nTriangles, d.buildOption = self.nMeshes, self.nTriangles, int(buildOption)
+        d.dInternals, d.dRootNodes, d.dMeshAABBs = _ptr(self.internals), _ptr(self.roots), _ptr(self.mesh_aabbs)
+        d.dScratch, d.scratchBytes = _ptr(self.scratch), self.scratch.numel()
+        self._graphs = []
+
+    def set_rays(self, rays, ray_offsets, rayQuery: int = RAY_QUERY_CLOSEST, hits=None):
+        """Rays float32 (nRays, 8) (ro.xyz, tmin, rd.xyz, tmax), mesh after
+        mesh; ray_offsets (nMeshes + 1, int32 on the device)."""
+        import torch
+        _require_cuda(rays, "rays")
+        _require_cuda(ray_offsets, "ray_offsets")
+        self.rays, self.ray_offsets, self.nRays = rays, ray_offsets, rays.numel() // 8
+        if hits is None:
+            hits = torch.empty((max(self.nRays, 1), 8), dtype=torch.int32, device=rays.device)
+        self.hits = hits
+        d = self._desc
+        d.dRays, d.dMeshRayOffsets, d.nRays, d.rayQuery, d.dHits = (_ptr(rays), _ptr(ray_offsets), self.nRays,
+                                                                    int(rayQuery), _ptr(hits))
+        return self
+
+    def build(self, params: BatchParams | None = None, stream=None):
+        _check(lib().mlbvh_build_batched(ctypes.byref(self._desc), None if params is None else ctypes.byref(params),
+                                         _stream(stream)))
+        return self
+
+    def trace(self, params: BatchParams | None = None, stream=None):
+        _check(lib().mlbvh_trace_batched(ctypes.byref(self._desc), None if params is None else ctypes.byref(params),
+                                         _stream(stream)))
+        return self.hits
+
+    def status(self, stream=None) -> None:
+        """Synchronise; raise on bad offsets or a bounded wait that gave up."""
+        _check(lib().mlbvh_scratch_status(_ptr(self.scratch), _stream(stream)))
+
+    def autotune(self, stream=None):
+        """Returns (BatchParams, build ms, trace ms) of the fastest candidates."""
+        p = BatchParams()
+        b, t = ctypes.c_float(0), ctypes.c_float(0)
+        _check(lib().mlbvh_batch_autotune(ctypes.byref(self._desc), ctypes.byref(p), ctypes.byref(b),
+                                          ctypes.byref(t), _stream(stream)))
+        return p, b.value, t.value
+
+    def graph(self, params: BatchParams | None = None, stages: int = 3) -> "BatchGraph":
+        g = _vp()
+        _check(lib().mlbvh_batch_graph_create(ctypes.byref(self._desc),
+                                              None if params is None else ctypes.byref(params), int(stages),
+                                              ctypes.byref(g)))
+        return BatchGraph(g)
+
+    def mesh_nodes(self, m: int, offsets_host) -> tuple:
+        """(node rows, triangle range) of mesh m given the host offsets."""
+        a, b = int(offsets_host[m]), int(offsets_host[m + 1])
+        return self.internals[a - m: b - m - 1], (a, b)
+
+
+class BatchGraph:
+    """A CUDA graph of a batch's build and/or traversal."""
+
+    def __init__(self, handle):
+        self._h = handle
+
+    def launch(self, stream=None):
+        _check(lib().mlbvh_batch_graph_launch(self._h, _stream(stream)))
+
+    def close(self):
+        if self._h:
+            lib().mlbvh_batch_graph_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

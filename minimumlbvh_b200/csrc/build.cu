@@ -21,6 +21,8 @@
 
 #include "capi_internal.h"
 #include "../../include/mlbvh_device.cuh"
+#include "climb.cuh"
+#include "onesweep.cuh"
 
 namespace mlbvh {
 
@@ -29,14 +31,8 @@ namespace {
 constexpr int kBoundsThreads = 256;
 constexpr int kBoundsMaxBlocks = 1024;
 constexpr int kKeysThreads = 256;
-constexpr int kSortThreads = 256;
-constexpr int kSortItems = 16;
-constexpr int kSortTile = kSortThreads * kSortItems;  // 4096 keys per tile
-constexpr int kSortWarps = kSortThreads / 32;
+constexpr int kSortTile = sort::kTile;  // 4096 keys per tile
 constexpr int kBuildThreads = 256;
-constexpr uint32_t kFlagAggregate = 1u << 30;
-constexpr uint32_t kFlagPrefix = 2u << 30;
-constexpr uint32_t kValueMask = (1u << 30) - 1;
 constexpr uint32_t kDefaultSpinLimit = 1u << 22;
 
 // Scratch layout of one build (offsets from the caller's dScratch). The
@@ -84,40 +80,6 @@ BuildLayout build_layout(uint32_t n)
     return L;
 }
 
-__device__ __forceinline__ uint32_t ld_relaxed(const uint32_t* p)
-{
-    uint32_t v;
-    asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-    return v;
-}
-__device__ __forceinline__ void st_relaxed(uint32_t* p, uint32_t v)
-{
-    asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
-}
-__device__ __forceinline__ uint32_t exch_acq_rel(uint32_t* p, uint32_t v)
-{
-    uint32_t old;
-    asm volatile("atom.acq_rel.gpu.global.exch.b32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
-    return old;
-}
-
-// Exclusive scan of one value per thread over a 256-thread block.
-__device__ __forceinline__ uint32_t block_exclusive_scan256(uint32_t v, uint32_t* s_warp /*8 entries*/)
-{
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    uint32_t inc = v;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        uint32_t y = __shfl_up_sync(0xffffffffu, inc, o);
-        if (lane >= o) inc += y;
-    }
-    if (lane == 31) s_warp[warp] = inc;
-    __syncthreads();
-    uint32_t base = 0;
-    for (int w = 0; w < warp; ++w) base += s_warp[w];
-    __syncthreads();
-    return base + inc - v;
-}
 
 // ------------------------------------------------------------ kernels
 
@@ -255,141 +217,8 @@ __global__ void __launch_bounds__(kKeysThreads)
     }
 }
 
-// One stable counting pass of the LSD sort over digit (key >> shift) & 255.
-// Tile t (4096 keys, ticketed in launch order so every tile a CTA waits on has
-// already started) ranks its keys with an 8-ballot warp multisplit, publishes
-// its per-digit counts, and resolves its global offsets by decoupled look-back
-// over earlier tiles (Merrill & Garland; Adinets & Merrill, "Onesweep", 2022).
-// Every wait is bounded: on expiry the error word is set and the pass goes on
-// with a wrong prefix instead of hanging.
-template <bool kFirst>
-__global__ void __launch_bounds__(kSortThreads)
-    k_onesweep(const uint32_t* __restrict__ keysIn, uint32_t* __restrict__ keysOut,
-               const uint32_t* __restrict__ valsIn, uint32_t* __restrict__ valsOut, uint32_t n, int shift,
-               const uint32_t* __restrict__ digitCounts, uint32_t* __restrict__ lookback,
-               uint32_t* __restrict__ tileCounter, uint32_t* __restrict__ errorWord, uint32_t spinLimit)
-{
-    __shared__ uint32_t s_tile;
-    __shared__ uint32_t s_warpHist[kSortWarps][256];
-    __shared__ uint32_t s_tileExcl[256];
-    __shared__ uint32_t s_dest[256];
-    __shared__ uint32_t s_scan[kSortWarps];
-    __shared__ uint32_t s_keys[kSortTile];
-    __shared__ uint32_t s_vals[kSortTile];
 
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    if (tid == 0) s_tile = atomicAdd(tileCounter, 1u);
-    for (int i = tid; i < kSortWarps * 256; i += kSortThreads) (&s_warpHist[0][0])[i] = 0u;
-    // global base offset of each digit for this pass
-    const uint32_t digitBase = block_exclusive_scan256(digitCounts[tid], s_scan);
-    __syncthreads();
-    const uint32_t tile = s_tile;
-    const uint32_t base = tile * (uint32_t)kSortTile + (uint32_t)warp * (kSortItems * 32);
-
-    uint32_t key[kSortItems], val[kSortItems], rank[kSortItems];
-#pragma unroll
-    for (int k = 0; k < kSortItems; ++k) {
-        const uint32_t idx = base + k * 32 + lane;
-        const bool valid = idx < n;
-        key[k] = valid ? __ldg(keysIn + idx) : 0xFFFFFFFFu;
-        val[k] = kFirst ? idx : (valid ? __ldg(valsIn + idx) : 0u);
-    }
-    const uint32_t lanesBelow = (1u << lane) - 1u;
-#pragma unroll
-    for (int k = 0; k < kSortItems; ++k) {
-        const uint32_t idx = base + k * 32 + lane;
-        const uint32_t d = (key[k] >> shift) & 255u;
-        uint32_t peers = __ballot_sync(0xffffffffu, idx < n);
-#pragma unroll
-        for (int b = 0; b < 8; ++b) {
-            const uint32_t bit = (d >> b) & 1u;
-            const uint32_t m = __ballot_sync(0xffffffffu, bit);
-            peers &= bit ? m : ~m;
-        }
-        const uint32_t before = s_warpHist[warp][d];
-        rank[k] = before + __popc(peers & lanesBelow);
-        __syncwarp();
-        if (idx < n && lane == __ffs(peers) - 1) s_warpHist[warp][d] = before + __popc(peers);
-        __syncwarp();
-    }
-    __syncthreads();
-
-    // per digit (one per thread): warp offsets and the tile's count
-    const uint32_t d = (uint32_t)tid;
-    uint32_t count = 0;
-#pragma unroll
-    for (int w = 0; w < kSortWarps; ++w) {
-        const uint32_t c = s_warpHist[w][d];
-        s_warpHist[w][d] = count;
-        count += c;
-    }
-    uint32_t* myWord = lookback + (size_t)tile * 256 + d;
-    uint32_t prefix = 0;
-    if (tile == 0) {
-        st_relaxed(myWord, kFlagPrefix | count);
-    } else {
-        st_relaxed(myWord, kFlagAggregate | count);
-        int t = (int)tile - 1;
-        while (t >= 0) {
-            const uint32_t* w = lookback + (size_t)t * 256 + d;
-            uint32_t word = ld_relaxed(w);
-            uint32_t spins = 0;
-            while ((word >> 30) == 0u) {
-                if (++spins > spinLimit) {
-                    atomicOr(errorWord, 1u);
-                    word = kFlagPrefix;
-                    break;
-                }
-                __nanosleep(32);
-                word = ld_relaxed(w);
-            }
-            prefix += word & kValueMask;
-            if ((word >> 30) == 2u) break;
-            --t;
-        }
-        st_relaxed(myWord, kFlagPrefix | ((prefix + count) & kValueMask));
-    }
-    const uint32_t excl = block_exclusive_scan256(count, s_scan);
-    s_tileExcl[d] = excl;
-    s_dest[d] = digitBase + prefix - excl;
-    __syncthreads();
-
-    // place every key at its tile-sorted position in shared memory
-#pragma unroll
-    for (int k = 0; k < kSortItems; ++k) {
-        const uint32_t idx = base + k * 32 + lane;
-        if (idx < n) {
-            const uint32_t dk = (key[k] >> shift) & 255u;
-            const uint32_t pos = s_tileExcl[dk] + s_warpHist[warp][dk] + rank[k];
-            s_keys[pos] = key[k];
-            s_vals[pos] = val[k];
-        }
-    }
-    __syncthreads();
-    const uint32_t tileStart = tile * (uint32_t)kSortTile;
-    const uint32_t count_in_tile = min((uint32_t)kSortTile, n - tileStart);
-    for (uint32_t i = tid; i < count_in_tile; i += kSortThreads) {
-        const uint32_t k = s_keys[i];
-        const uint32_t dst = s_dest[(k >> shift) & 255u] + i;
-        if (dst < n) {  // always true unless a bounded wait gave up (error word set)
-            keysOut[dst] = k;
-            valsOut[dst] = s_vals[i];
-        }
-    }
-}
-
-__device__ __forceinline__ uint32_t delta_at(const uint32_t* __restrict__ keys, uint32_t i)
-{
-    return split_delta(keys[i], keys[i + 1]);
-}
-
-// build_lbvh (minimum_lbvh.h:284-361), one thread per sorted leaf. The
-// hand-off word per internal node lives in its own array (reset by k_keys)
-// and is exchanged with acquire-release semantics, so the first walker's
-// child slot is visible to the second; the sibling bounds are then read from
-// L2. The merged box is formed as max/min(box of child 1, box of child 0)
-// whichever walker arrives second, which is the order the reference's serial
-// CPU build produces (its second arrival always comes from the right).
+// One thread per sorted leaf of the single-mesh build.
 __global__ void __launch_bounds__(kBuildThreads)
     k_build(const float* __restrict__ tris, uint32_t n, const uint32_t* __restrict__ sortedKeys,
             const uint32_t* __restrict__ sortedIdx, mlbvh_internal_node* __restrict__ nodes,
@@ -397,60 +226,7 @@ __global__ void __launch_bounds__(kBuildThreads)
 {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    const uint32_t nInternals = n - 1;
-    const uint32_t tri = sortedIdx[i];
-    if (tri >= n) return;  // only after a sort whose bounded wait gave up (error word set)
-    if (deltas && i < nInternals) deltas[i] = (uint8_t)delta_at(sortedKeys, i);
-
-    f3 v0, v1, v2;
-    load_triangle(tris, tri, v0, v1, v2);
-    f3 lo = mk(kFltMax, kFltMax, kFltMax), hi = mk(-kFltMax, -kFltMax, -kFltMax);
-    lo = smin3(lo, v0);
-    hi = smax3(hi, v0);
-    lo = smin3(lo, v1);
-    hi = smax3(hi, v1);
-    lo = smin3(lo, v2);
-    hi = smax3(hi, v2);
-
-    uint32_t leafLower = i, leafUpper = i;
-    uint32_t node = tri | kLeafBit;
-    while (leafUpper - leafLower < nInternals) {
-        const uint32_t deltaL = 0 < leafLower ? delta_at(sortedKeys, leafLower - 1) : 0xFFFFFFFFu;
-        const uint32_t deltaR = leafUpper < nInternals ? delta_at(sortedKeys, leafUpper) : 0xFFFFFFFFu;
-        const int goLeft = deltaL < deltaR ? 1 : 0;
-        const uint32_t parent = goLeft ? leafLower - 1 : leafUpper;
-
-        mlbvh_internal_node* p = nodes + parent;
-        p->children[goLeft] = node;
-        float* box = p->aabbs[goLeft].lower;
-        box[0] = lo.x;
-        box[1] = lo.y;
-        box[2] = lo.z;
-        box[3] = hi.x;
-        box[4] = hi.y;
-        box[5] = hi.z;
-        if (!(node & kLeafBit)) nodes[node].parent = parent;
-
-        uint32_t other = exch_acq_rel(handoff + parent, goLeft ? leafUpper : leafLower);
-        if (other == 0xFFFFFFFFu) return;  // first arrival: the sibling finishes this node
-
-        leafLower = min(leafLower, other);
-        leafUpper = max(leafUpper, other);
-        p->context = leafUpper < nInternals ? leafUpper : 0xFFFFFFFFu;
-        const float* ob = p->aabbs[goLeft ^ 1].lower;
-        const f3 olo = mk(__ldcg(ob + 0), __ldcg(ob + 1), __ldcg(ob + 2));
-        const f3 ohi = mk(__ldcg(ob + 3), __ldcg(ob + 4), __ldcg(ob + 5));
-        if (goLeft) {  // this walker is child 1
-            lo = smin3(lo, olo);
-            hi = smax3(hi, ohi);
-        } else {
-            lo = smin3(olo, lo);
-            hi = smax3(ohi, hi);
-        }
-        node = parent;
-    }
-    *root = node;
-    if (!(node & kLeafBit)) nodes[node].parent = kInvalid;
+    climb(tris, n, i, sortedKeys, sortedIdx, nodes, handoff, root, deltas);
 }
 
 }  // namespace
@@ -500,17 +276,20 @@ mlbvh_status build(const mlbvh_triangle* dTris, uint32_t n, uint32_t option, mlb
 
     uint32_t* kin = keysA;
     uint32_t* vin = valsA;
+    constexpr size_t kSmem = sort::Shape<8>::kSmemBytes;
     for (int pass = 0; pass < 4; ++pass) {
         uint32_t* kout = (pass == 3) ? keysFinal : (pass % 2 == 0 ? keysB : keysA);
         uint32_t* vout = (pass == 3) ? valsFinal : (pass % 2 == 0 ? valsB : valsA);
+        const sort::SingleSegment seg{n, L.tiles, hist + 256 * pass};
+        uint32_t* lb = lookback + (size_t)pass * L.tiles * 256;
         if (pass == 0)
-            k_onesweep<true><<<L.tiles, kSortThreads, 0, stream>>>(kin, kout, nullptr, vout, n, 8 * pass,
-                                                                    hist + 256 * pass, lookback + (size_t)pass * L.tiles * 256,
-                                                                    header + 1 + pass, header, spinLimit);
+            sort::k_onesweep<8, true><<<L.tiles, sort::kThreads, kSmem, stream>>>(kin, kout, nullptr, vout, 8 * pass,
+                                                                                seg, lb, header + 1 + pass, header,
+                                                                                spinLimit);
         else
-            k_onesweep<false><<<L.tiles, kSortThreads, 0, stream>>>(kin, kout, vin, vout, n, 8 * pass,
-                                                                     hist + 256 * pass, lookback + (size_t)pass * L.tiles * 256,
-                                                                     header + 1 + pass, header, spinLimit);
+            sort::k_onesweep<8, false><<<L.tiles, sort::kThreads, kSmem, stream>>>(kin, kout, vin, vout, 8 * pass,
+                                                                                 seg, lb, header + 1 + pass, header,
+                                                                                 spinLimit);
         MLBVH_CHECK_LAUNCH("k_onesweep");
         kin = kout;
         vin = vout;
@@ -531,6 +310,9 @@ mlbvh_status scratch_status(const void* dScratch, cudaStream_t stream)
     cudaError_t e = cudaMemcpyAsync(&word, dScratch, sizeof(word), cudaMemcpyDeviceToHost, stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
     if (e != cudaSuccess) return fail(MLBVH_ERR_CUDA, cudaGetErrorString(e));
+    if (word & 2u)
+        return fail(MLBVH_ERR_INVALID_ARG, "batch triangle offsets are not 0 = o[0] < o[1] < ... < o[nMeshes] = "
+                                           "nTriangles; nothing was built");
     if (word) return fail(MLBVH_ERR_TIMEOUT, "a bounded device wait gave up; the output of that call is unusable");
     return MLBVH_OK;
 }

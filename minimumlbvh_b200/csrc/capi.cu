@@ -177,6 +177,64 @@ mlbvh_status mlbvh_pt_diff_adjoint(float* dGradAlbedo, const float* dGradImage, 
                            dTriangles, dAlbedo, dEmission, as_stream(stream));
 }
 
+size_t mlbvh_batch_scratch_bytes(uint32_t nMeshes, uint32_t nTriangles)
+{
+    return batch_scratch_bytes(nMeshes, nTriangles);
+}
+
+void mlbvh_batch_params_default(mlbvh_batch_params* params)
+{
+    if (params) batch_params_default(params);
+}
+
+static const mlbvh_batch_params& params_or_default(const mlbvh_batch_params* p, mlbvh_batch_params& storage)
+{
+    if (p) return *p;
+    batch_params_default(&storage);
+    return storage;
+}
+
+mlbvh_status mlbvh_build_batched(const mlbvh_batch* batch, const mlbvh_batch_params* params, void* stream)
+{
+    clear_error();
+    if (!batch) return fail(MLBVH_ERR_INVALID_ARG, "null batch");
+    mlbvh_batch_params d;
+    return build_batched(*batch, params_or_default(params, d), as_stream(stream));
+}
+
+mlbvh_status mlbvh_trace_batched(const mlbvh_batch* batch, const mlbvh_batch_params* params, void* stream)
+{
+    clear_error();
+    if (!batch) return fail(MLBVH_ERR_INVALID_ARG, "null batch");
+    mlbvh_batch_params d;
+    return trace_batched(*batch, params_or_default(params, d), as_stream(stream));
+}
+
+mlbvh_status mlbvh_batch_autotune(const mlbvh_batch* batch, mlbvh_batch_params* params, float* buildMs,
+                                  float* traceMs, void* stream)
+{
+    clear_error();
+    if (!batch) return fail(MLBVH_ERR_INVALID_ARG, "null batch");
+    return batch_autotune(*batch, params, buildMs, traceMs, as_stream(stream));
+}
+
+mlbvh_status mlbvh_batch_graph_create(const mlbvh_batch* batch, const mlbvh_batch_params* params, int stages,
+                                      mlbvh_batch_graph** graph)
+{
+    clear_error();
+    if (!batch) return fail(MLBVH_ERR_INVALID_ARG, "null batch");
+    mlbvh_batch_params d;
+    return batch_graph_create(*batch, params_or_default(params, d), stages, graph);
+}
+
+mlbvh_status mlbvh_batch_graph_launch(mlbvh_batch_graph* graph, void* stream)
+{
+    clear_error();
+    return batch_graph_launch(graph, as_stream(stream));
+}
+
+void mlbvh_batch_graph_destroy(mlbvh_batch_graph* graph) { batch_graph_destroy(graph); }
+
 void mlbvh_profile_events(void* startEvent, void* stopEvent)
 {
     set_profile_events(reinterpret_cast<cudaEvent_t>(startEvent), reinterpret_cast<cudaEvent_t>(stopEvent));

@@ -75,4 +75,15 @@ mlbvh_status pt_diff_adjoint(float* dGrad, const float* dGradImage, int w, int h
                              const mlbvh_internal_node* dNodes, const mlbvh_triangle* dTris, const float* dAlbedo,
                              const float* dEmission, cudaStream_t stream);
 
+size_t batch_scratch_bytes(uint32_t nMeshes, uint32_t n);
+void batch_params_default(mlbvh_batch_params* p);
+mlbvh_status build_batched(const mlbvh_batch& B, const mlbvh_batch_params& P, cudaStream_t stream);
+mlbvh_status trace_batched(const mlbvh_batch& B, const mlbvh_batch_params& P, cudaStream_t stream);
+mlbvh_status batch_autotune(const mlbvh_batch& B, mlbvh_batch_params* out, float* bestBuildMs, float* bestTraceMs,
+                            cudaStream_t stream);
+mlbvh_status batch_graph_create(const mlbvh_batch& B, const mlbvh_batch_params& P, int stages,
+                                mlbvh_batch_graph** out);
+mlbvh_status batch_graph_launch(mlbvh_batch_graph* g, cudaStream_t stream);
+void batch_graph_destroy(mlbvh_batch_graph* g);
+
 }  // namespace mlbvh

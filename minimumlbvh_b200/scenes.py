@@ -12,7 +12,15 @@ here are synthetic and fully determined by their seed (numpy PCG64):
   the unit cube, sigma 0.02); each triangle is equilateral with a lognormal
   edge length (median 0.004, sigma 0.5) and a uniformly random orientation.
 
-Both return float32 arrays of shape (n, 9): v0.xyz, v1.xyz, v2.xyz per
+* ``batched_soup`` — the batched workload: meshes with triangle counts
+  log-uniform in [lo, hi], each a Gaussian-cluster soup as above in its own
+  unit box, laid out back to back; ``batched_rays`` gives every mesh a
+  log-uniform number of rays with origins uniform in the mesh's bounding box
+  expanded by 10% and directions uniform on the sphere. Both are generated
+  with torch (seeded generator on the given device), so the 32M-triangle
+  batch can be made directly in device memory.
+
+Triangle arrays are float32 of shape (n, 9): v0.xyz, v1.xyz, v2.xyz per
 triangle, the byte layout of minimum_lbvh::Triangle.
 """
 from __future__ import annotations
@@ -30,6 +38,9 @@ __all__ = [
     "quad_light",
     "diff_scene",
     "albedo",
+    "log_uniform_counts",
+    "batched_soup",
+    "batched_rays",
 ]
 
 
@@ -182,3 +193,92 @@ def diff_scene(seed: int = 0, albedo_seed: int = 1, light_radiance: float = 10.0
 def albedo(n: int, seed: int) -> np.ndarray:
     """Per-triangle grey albedo uniform in [0.1, 0.9] (float32)."""
     return np.random.default_rng(seed).uniform(0.1, 0.9, n).astype(np.float32)
+
+
+def log_uniform_counts(n: int, lo: int, hi: int, seed: int) -> np.ndarray:
+    """n integers log-uniform in [lo, hi] (int64)."""
+    rng = np.random.default_rng(seed)
+    c = np.exp(rng.uniform(np.log(lo), np.log(hi), n))
+    return np.clip(np.rint(c), lo, hi).astype(np.int64)
+
+
+def _soup_torch(counts, clusters: int, sigma: float, median_edge: float, edge_sigma: float, gen, device):
+    """Gaussian-cluster soups (see gaussian_soup) for every mesh of ``counts``,
+    back to back, generated with torch: float32 tensor (sum(counts), 9)."""
+    import torch
+    nm = len(counts)
+    n = int(np.sum(counts))
+    mesh = torch.repeat_interleave(torch.arange(nm, device=device),
+                                   torch.as_tensor(np.asarray(counts), device=device))
+    starts = torch.as_tensor(np.concatenate([[0], np.cumsum(counts)[:-1]]), device=device)
+    local = torch.arange(n, device=device) - starts[mesh]
+    centres = torch.rand((nm, clusters, 3), generator=gen, device=device, dtype=torch.float64)
+    out = torch.empty((n, 9), dtype=torch.float32, device=device)
+    base = torch.tensor([[1.0, 0.0, 0.0], [-0.5, 0.75**0.5, 0.0], [-0.5, -(0.75**0.5), 0.0]],
+                        dtype=torch.float64, device=device) / 3.0**0.5
+    chunk = 1 << 22
+    for s in range(0, n, chunk):
+        e = min(n, s + chunk)
+        m = e - s
+        c = centres[mesh[s:e], local[s:e] % clusters] + sigma * torch.randn((m, 3), generator=gen, device=device,
+                                                                          dtype=torch.float64)
+        edge = torch.exp(np.log(median_edge) + edge_sigma * torch.randn(m, generator=gen, device=device,
+                                                                        dtype=torch.float64))
+        q = torch.randn((m, 4), generator=gen, device=device, dtype=torch.float64)
+        q = q / q.norm(dim=1, keepdim=True)
+        w, x, y, z = q.unbind(1)
+        r = torch.stack([1 - 2 * (y * y + z * z), 2 * (x * y - z * w), 2 * (x * z + y * w),
+                         2 * (x * y + z * w), 1 - 2 * (x * x + z * z), 2 * (y * z - x * w),
+                         2 * (x * z - y * w), 2 * (y * z + x * w), 1 - 2 * (x * x + y * y)], 1).view(m, 3, 3)
+        v = torch.einsum("mij,vj->mvi", r, base) * edge[:, None, None] + c[:, None, :]
+        out[s:e] = v.reshape(m, 9).to(torch.float32)
+    return out
+
+
+def batched_soup(n_meshes: int = 1024, lo: int = 64, hi: int = 262_144, seed: int = 7, device="cpu",
+                 clusters: int = 64, sigma: float = 0.02, median_edge: float = 0.004, edge_sigma: float = 0.5):
+    """The batched workload's meshes (see module doc). Returns (triangles
+    float32 tensor (n, 9) on ``device``, triangle offsets int64 numpy array of
+    n_meshes + 1)."""
+    import torch
+    counts = log_uniform_counts(n_meshes, lo, hi, seed)
+    gen = torch.Generator(device=device).manual_seed(seed)
+    tris = _soup_torch(counts, clusters, sigma, median_edge, edge_sigma, gen, device)
+    return tris, np.concatenate([[0], np.cumsum(counts)]).astype(np.int64)
+
+
+def batched_rays(tris, tri_offsets: np.ndarray, lo: int = 4096, hi: int = 1_048_576, seed: int = 8, counts=None,
+                 tmax: float = 3.402823466e38):
+    """Rays of the batched workload: mesh m gets counts[m] rays (log-uniform
+    in [lo, hi] unless given) with origins uniform in its bounding box
+    expanded by 10% and directions uniform on the sphere. Returns (rays
+    float32 tensor (R, 8) on the triangles' device, ray offsets int64 numpy
+    array of n_meshes + 1)."""
+    import torch
+    device = tris.device
+    nm = len(tri_offsets) - 1
+    if counts is None:
+        counts = log_uniform_counts(nm, lo, hi, seed)
+    counts = np.asarray(counts, np.int64)
+    tmesh = torch.repeat_interleave(torch.arange(nm, device=device),
+                                    torch.as_tensor(np.diff(tri_offsets), device=device))
+    pts = tris.view(-1, 3, 3)
+    bmin = torch.full((nm, 3), float("inf"), device=device).scatter_reduce(
+        0, tmesh[:, None].expand(-1, 3), pts.amin(1), "amin")
+    bmax = torch.full((nm, 3), float("-inf"), device=device).scatter_reduce(
+        0, tmesh[:, None].expand(-1, 3), pts.amax(1), "amax")
+    rmesh = torch.repeat_interleave(torch.arange(nm, device=device), torch.as_tensor(counts, device=device))
+    gen = torch.Generator(device=device).manual_seed(seed)
+    n = int(counts.sum())
+    rays = torch.zeros((n, 8), dtype=torch.float32, device=device)
+    chunk = 1 << 24
+    for s in range(0, n, chunk):
+        e = min(n, s + chunk)
+        lo3, hi3 = bmin[rmesh[s:e]].double(), bmax[rmesh[s:e]].double()
+        ext = (hi3 - lo3) * 0.1
+        u = torch.rand((e - s, 3), generator=gen, device=device, dtype=torch.float64)
+        rays[s:e, 0:3] = (lo3 - ext + u * (hi3 - lo3 + 2 * ext)).float()
+        d = torch.randn((e - s, 3), generator=gen, device=device, dtype=torch.float64)
+        rays[s:e, 4:7] = (d / d.norm(dim=1, keepdim=True)).float()
+    rays[:, 7] = float(np.float32(tmax))
+    return rays, np.concatenate([[0], np.cumsum(counts)]).astype(np.int64)

@@ -91,3 +91,54 @@ def test_camera_lookat_matches_reference():
             O.ref().ref_lookat(O.P(np.array(eye, np.float32)), O.P(np.array(c, np.float32)),
                                O.P(np.array(up, np.float32)), float(np.float32(fovy)), w, h, O.P(r))
             np.testing.assert_array_equal(g, r)
+
+
+def _fake_batch(**kw):
+    d = mb._Batch()
+    p = 256
+    d.dTriangles = d.dMeshTriangleOffsets = d.dInternals = d.dRootNodes = d.dScratch = p
+    d.dRays = d.dMeshRayOffsets = d.dHits = p
+    d.nMeshes, d.nTriangles, d.nRays, d.scratchBytes = 4, 100, 10, 1 << 40
+    for k, v in kw.items():
+        setattr(d, k, v)
+    return d
+
+
+def test_batched_entry_points_reject_bad_arguments():
+    L = mb.lib()
+    by = ctypes.byref
+    assert L.mlbvh_build_batched(None, None, None) == 1
+    assert L.mlbvh_build_batched(by(_fake_batch(nMeshes=0)), None, None) == 1
+    assert L.mlbvh_build_batched(by(_fake_batch(nTriangles=3)), None, None) == 1  # fewer triangles than meshes
+    assert L.mlbvh_build_batched(by(_fake_batch(dTriangles=260)), None, None) == 1
+    assert b"aligned" in L.mlbvh_last_error_string()
+    assert L.mlbvh_build_batched(by(_fake_batch(scratchBytes=64)), None, None) == 1
+    assert b"scratch" in L.mlbvh_last_error_string()
+    p = mb.BatchParams.default()
+    for field, bad in (("digitBits", 9), ("traceBlock", 96), ("queueChunk", 0), ("refillLanes", 33)):
+        q = mb.BatchParams.default()
+        setattr(q, field, bad)
+        assert L.mlbvh_build_batched(by(_fake_batch()), by(q), None) == 1, field
+        assert field in L.mlbvh_last_error_string().decode()
+    assert L.mlbvh_trace_batched(by(_fake_batch(rayQuery=3)), by(p), None) == 1
+    assert L.mlbvh_trace_batched(by(_fake_batch(nRays=1 << 31)), by(p), None) == 1
+    assert L.mlbvh_trace_batched(by(_fake_batch(nRays=0)), by(p), None) == 0  # nothing to do
+    g = ctypes.c_void_p()
+    assert L.mlbvh_batch_graph_create(by(_fake_batch()), by(p), 0, by(g)) == 1
+    assert L.mlbvh_batch_graph_create(by(_fake_batch()), by(p), 3, None) == 1
+    assert L.mlbvh_batch_graph_launch(None, None) == 1
+    L.mlbvh_batch_graph_destroy(None)
+
+
+def test_batch_scratch_sizes():
+    L = mb.lib()
+    assert L.mlbvh_batch_scratch_bytes(0, 10) == 0
+    assert L.mlbvh_batch_scratch_bytes(10, 9) == 0
+    assert L.mlbvh_batch_scratch_bytes(1 << 21, 1 << 22) == 0
+    prev = 0
+    for nm, n in ((1, 1), (1, 4097), (16, 100000), (1024, 30_779_048)):
+        s = L.mlbvh_batch_scratch_bytes(nm, n)
+        assert s % 256 == 0 and s > prev and s >= 20 * n
+        prev = s
+    # the 1-mesh batch needs no less than the single-mesh build
+    assert L.mlbvh_batch_scratch_bytes(1, 1 << 20) >= L.mlbvh_build_scratch_bytes(1 << 20)
