@@ -191,7 +191,7 @@ def cpu_build_baseline(tris):
     return {"mtri_s": n / dt / 1e6, "ms": dt * 1e3, "kind": "port", "what": "oracle build (serial)"}
 
 
-def bench_batched(args, dev, stream, barrier, max_over_ranks, world):
+def bench_batched(args, dev, stream, barrier, max_over_ranks, world, n_meshes=1024, autotune=True):
     """The batched workload: 1,024 meshes with log-uniform 64..262,144
     triangles (30.8M in all) and log-uniform 4,096..1,048,576 incoherent rays
     each (169M), generated on the device. Build + traversal run as one CUDA
@@ -200,12 +200,16 @@ def bench_batched(args, dev, stream, barrier, max_over_ranks, world):
     import torch
     import minimumlbvh_b200 as mb
     from minimumlbvh_b200 import scenes
-    tris, offsets = scenes.batched_soup(1024, 64, 262_144, seed=7, device=dev)
+    tris, offsets = scenes.batched_soup(n_meshes, 64, 262_144, seed=7, device=dev)
     rays, roff = scenes.batched_rays(tris, offsets, 4096, 1_048_576, seed=8)
     nm, n, nr = len(offsets) - 1, int(offsets[-1]), int(roff[-1])
     bb = mb.BatchedBVH(tris, torch.as_tensor(offsets.astype(np.int32), device=dev), nm)
     bb.set_rays(rays, torch.as_tensor(roff.astype(np.int32), device=dev))
-    params, tune_build_ms, tune_trace_ms = bb.autotune()
+    if autotune:
+        params, tune_build_ms, tune_trace_ms = bb.autotune()
+    else:
+        params, tune_build_ms, tune_trace_ms = mb.BatchParams.default(), None, None
+        bb.build(params)
     bb.status()
     graph = bb.graph(params, stages=3)
     steps = max(1, args.steps)
@@ -269,7 +273,7 @@ def bench_batched(args, dev, stream, barrier, max_over_ranks, world):
     pt_s = max_over_ranks(pev[1].elapsed_time(pev[2]) / 1e3)
     agree = float((plain_hits == hits).all(1).float().mean().item())
     return {
-        "workload": "batched1024", "meshes": nm, "triangles": n, "rays": nr,
+        "workload": f"batched{nm}", "meshes": nm, "triangles": n, "rays": nr,
         "value": nr * world / trace_s / 1e6, "unit": "Mrays/s (persistent queue traversal)",
         "build_ms": build_s * 1e3, "build_mtri_s": n * world / build_s / 1e6, "trace_ms": trace_s * 1e3,
         "graph_ms": graph_s * 1e3, "graph_mrays_s": nr * world / graph_s / 1e6,
@@ -326,6 +330,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--image", default=None, help="override the frame size, WxH (small cases for ncu captures)")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched (1,024-mesh) workload")
+    ap.add_argument("--batched-meshes", type=int, default=1024, help="meshes of the batched workload (small cases)")
+    ap.add_argument("--no-autotune", action="store_true", help="batched workload with default launch parameters")
     args = ap.parse_args()
     wl = dict(WORKLOADS[args.workload])
     if args.image:
@@ -468,7 +474,8 @@ def main():
         torch.cuda.synchronize()
         barrier()
         e2e_s = max_over_ranks(eev[0].elapsed_time(eev[1]) / 1e3)
-        batched = None if args.no_batched else bench_batched(args, dev, stream, barrier, max_over_ranks, world)
+        batched = None if args.no_batched else bench_batched(args, dev, stream, barrier, max_over_ranks,
+                                                                   world, args.batched_meshes, not args.no_autotune)
     clocks = sampler.summary()
 
     ms_per_step = ao_total_s * 1e3 / args.steps

@@ -1336,16 +1336,15 @@ typedef struct {
     int query;
     orc_hit* hits;
     uint32_t *visits, *tests, *ups;
+    int stackDepth; /* 0: stack-free walk; 1..64: replay walk with that many stack entries */
 } qtrace_ctx;
 
 /* trace_quantised (include/mlbvh_device.cuh): the stack-free state machine
  * over quantised nodes; "came from the parent" is "came from neither child",
  * and the parent word is read only when moving up. */
-static void qtrace_one(const qtrace_ctx* c, orc_hit* hit, orc_f3 ro, orc_f3 rd, float tmin, uint32_t* nv, uint32_t* nt,
-                       uint32_t* nu)
+static void qtrace_walk(const qtrace_ctx* c, orc_hit* hit, orc_f3 ro, orc_f3 rd, orc_f3 inv, float tmin, uint32_t curr,
+                        uint32_t prev, uint32_t* nv, uint32_t* nt, uint32_t* nu)
 {
-    orc_f3 inv = inv_rd(rd);
-    uint32_t curr = c->root, prev = ORC_INVALID;
     while (curr != ORC_INVALID)
     {
         if (curr & ORC_LEAF_BIT)
@@ -1404,6 +1403,97 @@ static void qtrace_one(const qtrace_ctx* c, orc_hit* hit, orc_f3 ro, orc_f3 rd, 
     }
 }
 
+static void qtrace_one(const qtrace_ctx* c, orc_hit* hit, orc_f3 ro, orc_f3 rd, float tmin, uint32_t* nv, uint32_t* nt,
+                       uint32_t* nu)
+{
+    qtrace_walk(c, hit, ro, rd, inv_rd(rd), tmin, c->root, ORC_INVALID, nv, nt, nu);
+}
+
+/* quantised_replay_step (include/mlbvh_device.cuh): the same walk with a
+ * stack of pending far children (node, entry distance) instead of revisits.
+ * At a node whose two child boxes are hit, the far child is pushed and the
+ * near child entered; when a subtree is done, entries are popped and an entry
+ * is entered iff its entry distance is still <= hit.t, which is exactly when
+ * the stack-free walk, back at the parent, finds both boxes still hit (the
+ * near entry never exceeds the far one). So leaves are tested in the same
+ * order against the same hit.t. A push onto a full stack (depth entries)
+ * hands the walk to the stack-free state machine at (near child, parent),
+ * which re-derives every pending entry on its way up. */
+static void qreplay_one(const qtrace_ctx* c, int depth, orc_hit* hit, orc_f3 ro, orc_f3 rd, float tmin, uint32_t* nv,
+                        uint32_t* nt, uint32_t* nu)
+{
+    orc_f3 inv = inv_rd(rd);
+    uint32_t stackNode[64];
+    float stackEntry[64];
+    int top = 0;
+    uint32_t curr = c->root;
+    for (;;)
+    {
+        int pop = 0;
+        if (curr & ORC_LEAF_BIT)
+        {
+            (*nt)++;
+            const uint32_t* q = c->qtris + 12 * (size_t)(curr & ORC_QMASK);
+            orc_f3 v[3];
+            memcpy(v, q, 36);
+            float t, u, vv;
+            orc_f3 ng;
+            if (intersect_tri(&t, &u, &vv, &ng, tmin, hit->t, ro, rd, v[0], v[1], v[2]))
+            {
+                hit->t = t;
+                hit->u = u;
+                hit->v = vv;
+                hit->ng = ng;
+                hit->triangleIndex = q[9];
+                if (c->query == 1) return;
+            }
+            pop = 1;
+        }
+        else
+        {
+            (*nv)++;
+            const uint32_t* w = c->qnodes + 8 * (size_t)curr;
+            orc_aabb b0, b1;
+            qnode_boxes(w, c->eBase, &b0, &b1);
+            uint32_t c0 = w[6] & (ORC_LEAF_BIT | ORC_QMASK), c1 = w[7] & (ORC_LEAF_BIT | ORC_QMASK);
+            float lmin, lmax, rmin, rmax;
+            slabs(ro, inv, &b0, hit->t, &lmin, &lmax);
+            slabs(ro, inv, &b1, hit->t, &rmin, &rmax);
+            lmin = smax(lmin, tmin);
+            rmin = smax(rmin, tmin);
+            int hitL = lmin <= lmax, hitR = rmin <= rmax;
+            if (hitL && hitR)
+            {
+                uint32_t nearN = c0, farN = c1;
+                float farEntry = rmin;
+                if (rmin < lmin) { nearN = c1; farN = c0; farEntry = lmin; }
+                if (top == depth)
+                {
+                    qtrace_walk(c, hit, ro, rd, inv, tmin, nearN, curr, nv, nt, nu);
+                    return;
+                }
+                stackNode[top] = farN;
+                stackEntry[top] = farEntry;
+                ++top;
+                curr = nearN;
+            }
+            else if (hitL || hitR)
+                curr = hitL ? c0 : c1;
+            else
+                pop = 1;
+        }
+        if (pop)
+        {
+            for (;;)
+            {
+                if (top == 0) return;
+                --top;
+                if (stackEntry[top] <= hit->t) { curr = stackNode[top]; break; }
+            }
+        }
+    }
+}
+
 static void qtrace_range(void* p, uint32_t b, uint32_t e)
 {
     qtrace_ctx* c = (qtrace_ctx*)p;
@@ -1413,7 +1503,12 @@ static void qtrace_range(void* p, uint32_t b, uint32_t e)
         orc_hit hit;
         hit_init(&hit, r->tmax);
         uint32_t nv = 0, nt = 0, nu = 0;
-        qtrace_one(c, &hit, f3(r->ro[0], r->ro[1], r->ro[2]), f3(r->rd[0], r->rd[1], r->rd[2]), r->tmin, &nv, &nt, &nu);
+        if (c->stackDepth > 0)
+            qreplay_one(c, c->stackDepth, &hit, f3(r->ro[0], r->ro[1], r->ro[2]), f3(r->rd[0], r->rd[1], r->rd[2]),
+                        r->tmin, &nv, &nt, &nu);
+        else
+            qtrace_one(c, &hit, f3(r->ro[0], r->ro[1], r->ro[2]), f3(r->rd[0], r->rd[1], r->rd[2]), r->tmin, &nv, &nt,
+                       &nu);
         c->hits[i] = hit;
         if (c->visits) c->visits[i] = nv;
         if (c->tests) c->tests[i] = nt;
@@ -1437,6 +1532,27 @@ void orc_trace_quantised(const uint32_t* qnodes, const uint32_t* parents, const 
     c.visits = visits;
     c.tests = tests;
     c.ups = ups;
+    c.stackDepth = 0;
+    orc_parallel_for(nRays, 1024, qtrace_range, &c);
+}
+
+void orc_trace_quantised_replay(const uint32_t* qnodes, const uint32_t* parents, const uint32_t* qtris,
+                                const uint32_t* header, const orc_ray* rays, uint32_t nRays, int query, int stackDepth,
+                                orc_hit* hits, uint32_t* visits, uint32_t* tests, uint32_t* ups)
+{
+    qtrace_ctx c;
+    c.qnodes = qnodes;
+    c.parents = parents;
+    c.qtris = qtris;
+    c.root = header[0];
+    memcpy(&c.eBase, &header[1], 4);
+    c.rays = rays;
+    c.query = query;
+    c.hits = hits;
+    c.visits = visits;
+    c.tests = tests;
+    c.ups = ups;
+    c.stackDepth = stackDepth < 1 ? 1 : stackDepth > 64 ? 64 : stackDepth;
     orc_parallel_for(nRays, 1024, qtrace_range, &c);
 }
 

@@ -129,6 +129,12 @@ int orc_check_quantised(const orc_node* nodes, uint32_t n, const uint32_t* qnode
 void orc_trace_quantised(const uint32_t* qnodes, const uint32_t* parents, const uint32_t* qtris, const uint32_t* header,
                          const orc_ray* rays, uint32_t nRays, int query, orc_hit* hits, uint32_t* visits,
                          uint32_t* tests, uint32_t* ups);
+/* The quantised walk with a stack of stackDepth (1..64) pending far children
+ * replacing the revisits (quantised_replay_step); same hits as
+ * orc_trace_quantised, fewer node visits. */
+void orc_trace_quantised_replay(const uint32_t* qnodes, const uint32_t* parents, const uint32_t* qtris,
+                                const uint32_t* header, const orc_ray* rays, uint32_t nRays, int query, int stackDepth,
+                                orc_hit* hits, uint32_t* visits, uint32_t* tests, uint32_t* ups);
 
 /* Differentiable path tracing (no reference counterpart): the render and
  * path-replay adjoint of csrc/adjoint.cu. image32 (nullable) is the kernel's

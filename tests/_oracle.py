@@ -73,6 +73,7 @@ def oracle() -> ctypes.CDLL:
             "orc_quantise": (_i32, [_vp, _u32, _vp, _u32, _vp, _vp, _vp, _vp]),
             "orc_check_quantised": (_i32, [_vp, _u32, _vp, _vp]),
             "orc_trace_quantised": (None, [_vp, _vp, _vp, _vp, _vp, _u32, _i32, _vp, _vp, _vp, _vp]),
+            "orc_trace_quantised_replay": (None, [_vp, _vp, _vp, _vp, _vp, _u32, _i32, _i32, _vp, _vp, _vp, _vp]),
             "orc_pt_diff_render": (None, [_vp, _vp, _i32, _i32, _i32, _i32, _vp, _u32, _vp, _vp, _vp, _vp, _vp, _vp]),
             "orc_pt_diff_adjoint": (None, [_vp, _vp, _i32, _i32, _i32, _i32, _vp, _u32, _vp, _vp, _vp, _vp]),
         }
@@ -242,7 +243,7 @@ def quantise(b: dict, tris: np.ndarray):
     return dict(qnodes=qn[: n - 1], parents=par[: n - 1], qtris=qt, header=hd)
 
 
-def trace_quantised(q: dict, rays, query=0, counters=False):
+def trace_quantised(q: dict, rays, query=0, counters=False, stack_depth=0):
     rays = np.ascontiguousarray(rays, np.float32).reshape(-1, 8)
     n = rays.shape[0]
     hits = np.zeros((n, 8), np.uint32)
@@ -251,9 +252,14 @@ def trace_quantised(q: dict, rays, query=0, counters=False):
     nu = np.zeros(n, np.uint32) if counters else None
     qn = q["qnodes"] if len(q["qnodes"]) else np.zeros((1, 8), np.uint32)
     par = q["parents"] if len(q["parents"]) else np.zeros(1, np.uint32)
-    oracle().orc_trace_quantised(P(np.ascontiguousarray(qn)), P(np.ascontiguousarray(par)),
-                                 P(np.ascontiguousarray(q["qtris"])), P(q["header"]), P(rays), n, query, P(hits), P(nv),
-                                 P(nt), P(nu))
+    if stack_depth > 0:  # the replay walk with a stack of pending far children
+        oracle().orc_trace_quantised_replay(P(np.ascontiguousarray(qn)), P(np.ascontiguousarray(par)),
+                                            P(np.ascontiguousarray(q["qtris"])), P(q["header"]), P(rays), n, query,
+                                            stack_depth, P(hits), P(nv), P(nt), P(nu))
+    else:
+        oracle().orc_trace_quantised(P(np.ascontiguousarray(qn)), P(np.ascontiguousarray(par)),
+                                     P(np.ascontiguousarray(q["qtris"])), P(q["header"]), P(rays), n, query, P(hits),
+                                     P(nv), P(nt), P(nu))
     if counters:
         return hits, nv, nt, nu
     return hits
