@@ -190,11 +190,23 @@ MLBVH_API mlbvh_status mlbvh_trace(const mlbvh_internal_node* dInternals, const 
 MLBVH_API mlbvh_status mlbvh_quantise(const mlbvh_internal_node* dInternals, const mlbvh_node_index* dRootNode,
                                       const mlbvh_triangle* dTriangles, uint32_t nTriangles, mlbvh_qnode* dQNodes,
                                       uint32_t* dQParents, mlbvh_qtri* dQTris, mlbvh_qheader* dQHeader, void* stream);
-/* mlbvh_trace over the quantised tree (stack-free, as intersect_stackfree). */
+/* mlbvh_trace over the quantised tree. The walk visits leaves in the order
+ * of intersect_stackfree's state machine; a 16-entry stack of pending far
+ * children per ray replaces its revisits (same Hit records, fewer node loads). */
 MLBVH_API mlbvh_status mlbvh_trace_quantised(const mlbvh_qnode* dQNodes, const uint32_t* dQParents,
                                              const mlbvh_qtri* dQTris, const mlbvh_qheader* dQHeader,
                                              const mlbvh_ray* dRays, mlbvh_hit* dHits, uint32_t nRays, int rayQuery,
                                              void* stream);
+/* mlbvh_trace_quantised with the walk chosen: stackDepth 0 = the stack-free
+ * walk (parent loads instead of a stack), 1, 4 or 16 = that many stack entries
+ * per ray (a full stack hands over to the stack-free walk). All give the same
+ * Hit records. dCounts (may be NULL; 3 * nRays words, nRays < 2^30) receives
+ * per ray the internal-node visits, triangle tests and parent loads at
+ * [i], [nRays + i], [2 nRays + i]. */
+MLBVH_API mlbvh_status mlbvh_trace_quantised_ex(const mlbvh_qnode* dQNodes, const uint32_t* dQParents,
+                                                const mlbvh_qtri* dQTris, const mlbvh_qheader* dQHeader,
+                                                const mlbvh_ray* dRays, mlbvh_hit* dHits, uint32_t nRays,
+                                                int rayQuery, int stackDepth, uint32_t* dCounts, void* stream);
 /* mlbvh_render_ao over the quantised tree; same arguments otherwise. */
 MLBVH_API mlbvh_status mlbvh_render_ao_quantised(uint32_t* dPixels, uint32_t* dOccluded, int width, int height,
                                                  const mlbvh_ray_generator* camera, const mlbvh_qnode* dQNodes,

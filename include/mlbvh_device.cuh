@@ -614,8 +614,14 @@ __device__ __forceinline__ void decode_steps(uint32_t c0, uint32_t c1, int eBase
     sz = pow2f(max(ez, -126));
 }
 
-__device__ __forceinline__ float qlo(float o, uint32_t q, float s) { return __fadd_rd(o, (float)q * s); }
-__device__ __forceinline__ float qhi(float o, uint32_t q, float s) { return __fadd_ru(o, (float)q * s); }
+__device__ __forceinline__ float qlo(float o, float q, float s) { return __fadd_rd(o, q * s); }
+__device__ __forceinline__ float qhi(float o, float q, float s) { return __fadd_ru(o, q * s); }
+// Byte k of w as a float, exactly: the byte permute builds 0x4B0000qq, which
+// is 2^23 + q as a float, and the subtraction of 2^23 is exact.
+__device__ __forceinline__ float qbyte(uint32_t w, int k)
+{
+    return __uint_as_float(__byte_perm(w, 0x4B000000u, 0x7540u + (uint32_t)k)) - 8388608.0f;
+}
 
 struct QNodeView {
     uint32_t c0, c1;  // leaf flag | 23-bit index
@@ -641,10 +647,10 @@ __device__ __forceinline__ QNodeView load_qnode(const mlbvh_qnode* __restrict__ 
     n.c0 = c0 & (kLeafBit | kQIndexMask);
     n.c1 = c1 & (kLeafBit | kQIndexMask);
     // q bytes: w0 = q0..q3, w1 = q4..q7, w2 = q8..q11
-    n.box.lo0 = mk(qlo(o.x, w0 & 255u, sx), qlo(o.y, (w0 >> 8) & 255u, sy), qlo(o.z, (w0 >> 16) & 255u, sz));
-    n.box.hi0 = mk(qhi(o.x, w0 >> 24, sx), qhi(o.y, w1 & 255u, sy), qhi(o.z, (w1 >> 8) & 255u, sz));
-    n.box.lo1 = mk(qlo(o.x, (w1 >> 16) & 255u, sx), qlo(o.y, w1 >> 24, sy), qlo(o.z, w2 & 255u, sz));
-    n.box.hi1 = mk(qhi(o.x, (w2 >> 8) & 255u, sx), qhi(o.y, (w2 >> 16) & 255u, sy), qhi(o.z, w2 >> 24, sz));
+    n.box.lo0 = mk(qlo(o.x, qbyte(w0, 0), sx), qlo(o.y, qbyte(w0, 1), sy), qlo(o.z, qbyte(w0, 2), sz));
+    n.box.hi0 = mk(qhi(o.x, qbyte(w0, 3), sx), qhi(o.y, qbyte(w1, 0), sy), qhi(o.z, qbyte(w1, 1), sz));
+    n.box.lo1 = mk(qlo(o.x, qbyte(w1, 2), sx), qlo(o.y, qbyte(w1, 3), sy), qlo(o.z, qbyte(w2, 0), sz));
+    n.box.hi1 = mk(qhi(o.x, qbyte(w2, 1), sx), qhi(o.y, qbyte(w2, 2), sy), qhi(o.z, qbyte(w2, 3), sz));
     return n;
 }
 
@@ -717,6 +723,83 @@ __device__ __forceinline__ bool quantised_step(uint32_t& curr, uint32_t& prev, H
     prev = curr;
     curr = next;
     return curr == kInvalid;
+}
+
+// The same walk with a stack of pending far children instead of revisits.
+// At a node whose two child boxes are hit, the far child and its entry
+// distance are pushed and the near child is entered; when a subtree is done,
+// entries are popped and an entry is entered iff its entry distance is still
+// <= hit.t. That is exactly when the stack-free walk, back at the parent from
+// the near child, finds both boxes still hit: a box's entry distance does not
+// depend on hit.t, and the near entry never exceeds the far one. So leaves
+// are tested in the same order against the same hit.t and the Hit record is
+// the stack-free walk's bit for bit, with each internal node loaded once
+// instead of up to three times and no parent loads.
+//
+// The stack holds kDepth entries of this thread at stack[d * stride]
+// (shared memory, one column per thread). A push onto a full stack hands the
+// walk to the stack-free state machine at (near child, this node), marked by
+// depth = -1; climbing through the parents, it re-derives every entry still
+// on the stack. Start a walk with curr = root, depth = 0.
+template <bool kAny, bool kCount, int kDepth>
+__device__ __forceinline__ bool quantised_replay_step(uint32_t& curr, uint32_t& prev, int& depth, uint2* stack,
+                                                      int stride, HitRecord& hit,
+                                                      const mlbvh_qnode* __restrict__ qnodes,
+                                                      const uint32_t* __restrict__ parents,
+                                                      const mlbvh_qtri* __restrict__ qtris, int eBase, f3 ro, f3 rd,
+                                                      f3 inv, float tmin, uint32_t& nv, uint32_t& nt, uint32_t& nu)
+{
+    if (depth < 0)
+        return quantised_step<kAny, kCount, true>(curr, prev, hit, qnodes, parents, qtris, eBase, ro, rd, inv, tmin, nv,
+                                                  nt, nu);
+    if (curr & kLeafBit) {
+        if (kCount) ++nt;
+        const float4* t = reinterpret_cast<const float4*>(qtris + (curr & kQIndexMask));
+        const float4 a = __ldg(t), b = __ldg(t + 1), c = __ldg(t + 2);
+        float tt, u, v;
+        f3 ng;
+        if (intersect_triangle(tt, u, v, ng, tmin, hit.t, ro, rd, mk(a.x, a.y, a.z), mk(a.w, b.x, b.y),
+                               mk(b.z, b.w, c.x))) {
+            hit.t = tt;
+            hit.u = u;
+            hit.v = v;
+            hit.ng = ng;
+            hit.tri = __float_as_uint(c.y);
+            if (kAny) return true;
+        }
+    } else {
+        if (kCount) ++nv;
+        const QNodeView nd = load_qnode<true>(qnodes, curr, eBase);
+        const float2 rl = slab(ro, inv, nd.box.lo0, nd.box.hi0, tmin, hit.t);
+        const float2 rr = slab(ro, inv, nd.box.lo1, nd.box.hi1, tmin, hit.t);
+        const bool hitL = rl.x <= rl.y, hitR = rr.x <= rr.y;
+        if (hitL && hitR) {
+            const bool swap = rr.x < rl.x;
+            const uint32_t nearN = swap ? nd.c1 : nd.c0, farN = swap ? nd.c0 : nd.c1;
+            if (depth == kDepth) {  // full: continue as the stack-free walk
+                depth = -1;
+                prev = curr;
+                curr = nearN;
+                return false;
+            }
+            stack[depth * stride] = make_uint2(farN, __float_as_uint(swap ? rl.x : rr.x));
+            ++depth;
+            curr = nearN;
+            return false;
+        }
+        if (hitL || hitR) {
+            curr = hitL ? nd.c0 : nd.c1;
+            return false;
+        }
+    }
+    while (depth > 0) {
+        const uint2 e = stack[--depth * stride];
+        if (__uint_as_float(e.y) <= hit.t) {
+            curr = e.x;
+            return false;
+        }
+    }
+    return true;
 }
 
 template <bool kAny, bool kCount = false, bool kWide = false>

@@ -79,6 +79,7 @@ def lib() -> ctypes.CDLL:
             "mlbvh_profile_events": (None, [_vp, _vp]),
             "mlbvh_quantise": (i32, [_vp, _vp, _vp, u32, _vp, _vp, _vp, _vp, _vp]),
             "mlbvh_trace_quantised": (i32, [_vp, _vp, _vp, _vp, _vp, _vp, u32, i32, _vp]),
+            "mlbvh_trace_quantised_ex": (i32, [_vp, _vp, _vp, _vp, _vp, _vp, u32, i32, i32, _vp, _vp]),
             "mlbvh_render_ao_quantised": (i32, [_vp, _vp, i32, i32, _vp, _vp, _vp, _vp, _vp, i32, i32, f32, u32,
                                                 _vp, _vp, sz, _vp]),
             "mlbvh_camera_lookat": (i32, [_vp, _vp, _vp, _vp, f32, i32, i32]),
@@ -351,15 +352,26 @@ class QuantisedBVH:
         return cls(qnodes, parents, qtris, header, n)
 
 
-def intersect_quantised(q: QuantisedBVH, rays, rayQuery: int = RAY_QUERY_CLOSEST, hits=None, stream=None):
-    """Stack-free closest/any hit over the quantised tree (same Hit records)."""
+def intersect_quantised(q: QuantisedBVH, rays, rayQuery: int = RAY_QUERY_CLOSEST, hits=None, stream=None,
+                        stack_depth: int | None = None, counts=None):
+    """Closest/any hit over the quantised tree (the stack-free walk's Hit
+    records). ``stack_depth`` None: the library's default walk; 0: the
+    stack-free walk; 1, 4 or 16: the replay walk with that many stack
+    entries. ``counts`` (int32 CUDA tensor of 3 * nRays) receives per-ray
+    node visits, triangle tests and parent loads."""
     import torch
     _require_cuda(rays, "rays")
     n = rays.numel() // 8
     if hits is None:
         hits = torch.empty((n, 8), dtype=torch.int32, device=rays.device)
-    _check(lib().mlbvh_trace_quantised(_ptr(q.qnodes), _ptr(q.parents), _ptr(q.qtris), _ptr(q.header), _ptr(rays),
-                                       _ptr(hits), n, int(rayQuery), _stream(stream)))
+    if stack_depth is None and counts is None:
+        _check(lib().mlbvh_trace_quantised(_ptr(q.qnodes), _ptr(q.parents), _ptr(q.qtris), _ptr(q.header),
+                                           _ptr(rays), _ptr(hits), n, int(rayQuery), _stream(stream)))
+    else:
+        _check(lib().mlbvh_trace_quantised_ex(_ptr(q.qnodes), _ptr(q.parents), _ptr(q.qtris), _ptr(q.header),
+                                              _ptr(rays), _ptr(hits), n, int(rayQuery),
+                                              16 if stack_depth is None else int(stack_depth), _ptr(counts),
+                                              _stream(stream)))
     return hits
 
 

@@ -138,7 +138,17 @@ mlbvh_status mlbvh_trace_quantised(const mlbvh_qnode* dQNodes, const uint32_t* d
                                    uint32_t nRays, int rayQuery, void* stream)
 {
     clear_error();
-    return trace_quantised(dQNodes, dQParents, dQTris, dQHeader, dRays, dHits, nRays, rayQuery, as_stream(stream));
+    return trace_quantised(dQNodes, dQParents, dQTris, dQHeader, dRays, dHits, nRays, rayQuery, 16, nullptr,
+                           as_stream(stream));
+}
+
+mlbvh_status mlbvh_trace_quantised_ex(const mlbvh_qnode* dQNodes, const uint32_t* dQParents, const mlbvh_qtri* dQTris,
+                                      const mlbvh_qheader* dQHeader, const mlbvh_ray* dRays, mlbvh_hit* dHits,
+                                      uint32_t nRays, int rayQuery, int stackDepth, uint32_t* dCounts, void* stream)
+{
+    clear_error();
+    return trace_quantised(dQNodes, dQParents, dQTris, dQHeader, dRays, dHits, nRays, rayQuery, stackDepth, dCounts,
+                           as_stream(stream));
 }
 
 mlbvh_status mlbvh_render_ao_quantised(uint32_t* dPixels, uint32_t* dOccluded, int width, int height,

@@ -60,7 +60,7 @@ mlbvh_status quantise(const mlbvh_internal_node* dNodes, const mlbvh_node_index*
                       mlbvh_qheader* dQHeader, cudaStream_t stream);
 mlbvh_status trace_quantised(const mlbvh_qnode* dQNodes, const uint32_t* dQParents, const mlbvh_qtri* dQTris,
                              const mlbvh_qheader* dQHeader, const mlbvh_ray* dRays, mlbvh_hit* dHits, uint32_t nRays,
-                             int rayQuery, cudaStream_t stream);
+                             int rayQuery, int stackDepth, uint32_t* dCounts, cudaStream_t stream);
 mlbvh_status render_pt(float* dAccum, int w, int h, const mlbvh_ray_generator& cam, const mlbvh_node_index* dRoot,
                        const mlbvh_internal_node* dNodes, const mlbvh_triangle* dTris,
                        const mlbvh_triangle_attrib* dAttribs, int useSobol, int maxSPP, int maxDepth,

@@ -128,12 +128,19 @@ __global__ void __launch_bounds__(kQuantiseThreads)
     parents[i] = nd.parent;
 }
 
-template <bool kAny>
+// One thread per ray. kDepth = 0: the stack-free walk (trace_quantised);
+// otherwise the replay walk with a kDepth-entry stack per thread in shared
+// memory (quantised_replay_step), which returns the same Hit records.
+// counts (may be null): per ray, internal-node visits, triangle tests and
+// parent loads at counts[i], counts[n + i], counts[2n + i].
+template <bool kAny, int kDepth, bool kCount>
 __global__ void __launch_bounds__(kTraceThreads)
     k_trace_quantised(const mlbvh_qnode* __restrict__ qnodes, const uint32_t* __restrict__ parents,
                       const mlbvh_qtri* __restrict__ qtris, const mlbvh_qheader* __restrict__ header,
-                      const float4* __restrict__ rays, float4* __restrict__ hits, uint32_t n)
+                      const float4* __restrict__ rays, float4* __restrict__ hits, uint32_t n,
+                      uint32_t* __restrict__ counts)
 {
+    __shared__ uint2 s_stack[kDepth > 0 ? kDepth : 1][kTraceThreads];
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const float4 a = __ldg(rays + 2 * (size_t)i), b = __ldg(rays + 2 * (size_t)i + 1);
@@ -144,10 +151,53 @@ __global__ void __launch_bounds__(kTraceThreads)
     hit.v = 0.0f;
     hit.ng = mk(0.0f, 0.0f, 0.0f);
     hit.tri = 0xFFFFFFFFu;
-    trace_quantised<kAny, false, true>(hit, qnodes, parents, qtris, __ldg(&header->root), __ldg(&header->eBase), ro, rd, inv_rd(rd),
-                          a.w);
+    const uint32_t root = __ldg(&header->root);
+    const int eBase = __ldg(&header->eBase);
+    const f3 inv = inv_rd(rd);
+    uint32_t nv = 0, nt = 0, nu = 0;
+    if (kDepth == 0) {
+        trace_quantised<kAny, kCount, true>(hit, qnodes, parents, qtris, root, eBase, ro, rd, inv, a.w, &nv, &nt, &nu);
+    } else {
+        uint32_t curr = root, prev = kInvalid;
+        int depth = 0;
+        for (uint32_t steps = 1; steps < kMaxTraversalSteps; ++steps)
+            if (quantised_replay_step<kAny, kCount, kDepth>(curr, prev, depth, &s_stack[0][threadIdx.x],
+                                                            kTraceThreads, hit, qnodes, parents, qtris, eBase, ro, rd,
+                                                            inv, a.w, nv, nt, nu))
+                break;
+    }
     hits[2 * (size_t)i] = make_float4(hit.t, 0.0f, hit.u, hit.v);
     hits[2 * (size_t)i + 1] = make_float4(hit.ng.x, hit.ng.y, hit.ng.z, __uint_as_float(hit.tri));
+    if (kCount) {
+        counts[i] = nv;
+        counts[n + i] = nt;
+        counts[2 * (size_t)n + i] = nu;
+    }
+}
+
+template <bool kAny, int kDepth>
+void launch_trace_quantised(unsigned blocks, cudaStream_t stream, const mlbvh_qnode* q, const uint32_t* p,
+                            const mlbvh_qtri* t, const mlbvh_qheader* h, const float4* rays, float4* hits, uint32_t n,
+                            uint32_t* counts)
+{
+    if (counts)
+        k_trace_quantised<kAny, kDepth, true><<<blocks, kTraceThreads, 0, stream>>>(q, p, t, h, rays, hits, n, counts);
+    else
+        k_trace_quantised<kAny, kDepth, false><<<blocks, kTraceThreads, 0, stream>>>(q, p, t, h, rays, hits, n,
+                                                                                    nullptr);
+}
+
+template <bool kAny>
+void launch_trace_quantised_depth(int depth, unsigned blocks, cudaStream_t stream, const mlbvh_qnode* q,
+                                  const uint32_t* p, const mlbvh_qtri* t, const mlbvh_qheader* h, const float4* rays,
+                                  float4* hits, uint32_t n, uint32_t* counts)
+{
+    switch (depth) {
+    case 0: launch_trace_quantised<kAny, 0>(blocks, stream, q, p, t, h, rays, hits, n, counts); break;
+    case 1: launch_trace_quantised<kAny, 1>(blocks, stream, q, p, t, h, rays, hits, n, counts); break;
+    case 4: launch_trace_quantised<kAny, 4>(blocks, stream, q, p, t, h, rays, hits, n, counts); break;
+    default: launch_trace_quantised<kAny, 16>(blocks, stream, q, p, t, h, rays, hits, n, counts); break;
+    }
 }
 
 }  // namespace
@@ -171,24 +221,27 @@ mlbvh_status quantise(const mlbvh_internal_node* dNodes, const mlbvh_node_index*
 
 mlbvh_status trace_quantised(const mlbvh_qnode* dQNodes, const uint32_t* dQParents, const mlbvh_qtri* dQTris,
                              const mlbvh_qheader* dQHeader, const mlbvh_ray* dRays, mlbvh_hit* dHits, uint32_t nRays,
-                             int rayQuery, cudaStream_t stream)
+                             int rayQuery, int stackDepth, uint32_t* dCounts, cudaStream_t stream)
 {
     if (nRays == 0) return MLBVH_OK;
     if (!dQTris || !dQHeader || !dRays || !dHits) return fail(MLBVH_ERR_INVALID_ARG, "null pointer");
     if (!aligned32(dQNodes) || !aligned16(dQParents) || !aligned16(dQTris) || !aligned16(dQHeader) ||
-        !aligned16(dRays) || !aligned16(dHits))
+        !aligned16(dRays) || !aligned16(dHits) || !aligned16(dCounts))
         return fail(MLBVH_ERR_INVALID_ARG, "device pointers must be 16-byte aligned");
     if (rayQuery != MLBVH_RAY_QUERY_CLOSEST && rayQuery != MLBVH_RAY_QUERY_ANY)
         return fail(MLBVH_ERR_INVALID_ARG, "rayQuery must be MLBVH_RAY_QUERY_CLOSEST or MLBVH_RAY_QUERY_ANY");
+    if (stackDepth != 0 && stackDepth != 1 && stackDepth != 4 && stackDepth != 16)
+        return fail(MLBVH_ERR_INVALID_ARG, "stackDepth must be 0, 1, 4 or 16");
+    if (nRays >= (1u << 30) && dCounts) return fail(MLBVH_ERR_INVALID_ARG, "nRays must be below 2^30 with counts");
     const unsigned blocks = (nRays + kTraceThreads - 1) / kTraceThreads;
     const float4* rays = reinterpret_cast<const float4*>(dRays);
     float4* hits = reinterpret_cast<float4*>(dHits);
     if (rayQuery == MLBVH_RAY_QUERY_ANY)
-        k_trace_quantised<true><<<blocks, kTraceThreads, 0, stream>>>(dQNodes, dQParents, dQTris, dQHeader, rays, hits,
-                                                                      nRays);
+        launch_trace_quantised_depth<true>(stackDepth, blocks, stream, dQNodes, dQParents, dQTris, dQHeader, rays, hits,
+                                           nRays, dCounts);
     else
-        k_trace_quantised<false><<<blocks, kTraceThreads, 0, stream>>>(dQNodes, dQParents, dQTris, dQHeader, rays, hits,
-                                                                       nRays);
+        launch_trace_quantised_depth<false>(stackDepth, blocks, stream, dQNodes, dQParents, dQTris, dQHeader, rays,
+                                            hits, nRays, dCounts);
     MLBVH_CHECK_LAUNCH("k_trace_quantised");
     return MLBVH_OK;
 }

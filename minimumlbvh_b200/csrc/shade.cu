@@ -123,9 +123,11 @@ struct PlainTree {
     {
         trace_stackfree<kAny, kCount, true>(hit, nodes, tris, c.root, ro, rd, inv_rd(rd), 0.0f, &n.visits, &n.tests);
     }
+    // the reference's stack-free walk: no stack
+    static constexpr int kStack = 0;
     template <bool kAny, bool kCount>
-    __device__ __forceinline__ bool step(const Ctx&, uint32_t& curr, uint32_t& prev, HitRecord& hit, f3 ro, f3 rd,
-                                         f3 inv, Counts& n) const
+    __device__ __forceinline__ bool step(const Ctx&, uint32_t& curr, uint32_t& prev, int&, uint2*, HitRecord& hit,
+                                         f3 ro, f3 rd, f3 inv, Counts& n) const
     {
         return stackfree_step<kAny, kCount, true>(curr, prev, hit, nodes, tris, ro, rd, inv, 0.0f, n.visits, n.tests);
     }
@@ -149,12 +151,16 @@ struct QuantTree {
         trace_quantised<kAny, kCount, true>(hit, qnodes, parents, qtris, c.root, c.eBase, ro, rd, inv_rd(rd), 0.0f,
                                       &n.visits, &n.tests, &n.ups);
     }
+    // the replay walk: the stack-free walk's leaf order with a stack of
+    // kStack pending far children per lane (shared memory) instead of revisits
+    static constexpr int kStack = 16;
     template <bool kAny, bool kCount>
-    __device__ __forceinline__ bool step(const Ctx& c, uint32_t& curr, uint32_t& prev, HitRecord& hit, f3 ro, f3 rd,
-                                         f3 inv, Counts& n) const
+    __device__ __forceinline__ bool step(const Ctx& c, uint32_t& curr, uint32_t& prev, int& depth, uint2* stack,
+                                         HitRecord& hit, f3 ro, f3 rd, f3 inv, Counts& n) const
     {
-        return quantised_step<kAny, kCount, true>(curr, prev, hit, qnodes, parents, qtris, c.eBase, ro, rd, inv, 0.0f,
-                                            n.visits, n.tests, n.ups);
+        return quantised_replay_step<kAny, kCount, kStack>(curr, prev, depth, stack, kAoThreads, hit, qnodes, parents,
+                                                           qtris, c.eBase, ro, rd, inv, 0.0f, n.visits, n.tests,
+                                                           n.ups);
     }
 };
 
@@ -214,7 +220,13 @@ __global__ void __launch_bounds__(kTileW* kTileH)
 // per batch) once a quarter of the warp is idle or the warp has nothing left.
 // So lanes never wait for the longest ray of their warp. A finished item adds
 // its occlusion count to its pixel's.
+// Setting up a ray (Sobol point, hemisphere direction, reciprocal direction)
+// costs about as much as several traversal steps; a lane whose ray is done
+// waits until kStartBatch lanes of its warp need a new ray (or no lane has a
+// ray in flight), so that the set-up runs for many lanes at once instead of
+// once per finishing lane.
 constexpr int kRefillBatch = 8;
+constexpr int kStartBatch = 4;
 
 template <class Tree, bool kCount>
 __global__ void __launch_bounds__(kAoThreads, 8)  // at most 64 registers: 32 warps per SM
@@ -233,6 +245,9 @@ __global__ void __launch_bounds__(kAoThreads, 8)  // at most 64 registers: 32 wa
     const uint32_t itemsPerPixel = (nSamples + chunk - 1) / chunk;
     const uint32_t total = pixels * itemsPerPixel;
     const typename Tree::Ctx ctx = tree.context();
+    __shared__ uint2 s_stack[Tree::kStack > 0 ? Tree::kStack : 1][kAoThreads];
+    uint2* const stack = &s_stack[0][threadIdx.x];
+    int depth = 0;
     bool exhausted = false;  // warp-uniform: the queue has no item left
     bool owns = false;       // this lane owns an item
     bool live = false;       // this lane has a ray in flight
@@ -272,7 +287,10 @@ __global__ void __launch_bounds__(kAoThreads, 8)  // at most 64 registers: 32 wa
             if (exhausted) break;
             continue;
         }
-        if (owns && !live) {  // start sample s of this lane's pixel
+        const uint32_t starters = __ballot_sync(0xffffffffu, owns && !live);
+        const uint32_t inFlight = __ballot_sync(0xffffffffu, live);
+        if (owns && !live && (__popc(starters) >= kStartBatch || inFlight == 0u)) {
+            // start sample s of this lane's pixel
             float2 rnd;
             if (useSobol) {
                 rnd = sobol2d(s, xi, yi, seed);
@@ -289,11 +307,12 @@ __global__ void __launch_bounds__(kAoThreads, 8)  // at most 64 registers: 32 wa
             hit.tri = 0xFFFFFFFFu;
             curr = ctx.root;
             prev = kInvalid;
+            depth = 0;
             steps = 0;
             live = true;
         }
         if (live) {
-            if (tree.template step<true, kCount>(ctx, curr, prev, hit, origin, dir, inv, cnt) ||
+            if (tree.template step<true, kCount>(ctx, curr, prev, depth, stack, hit, origin, dir, inv, cnt) ||
                 ++steps >= kMaxTraversalSteps) {
                 live = false;
                 if (hit.t != radius) ++occ;

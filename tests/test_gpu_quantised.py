@@ -91,3 +91,39 @@ def test_quantised_full_size_soup(cuda):
     np.testing.assert_array_equal(got, O.trace_quantised(ref, rays, 0))
     plain = O.trace(out["nodes"], tris, out["root"], rays, 0, 0)
     np.testing.assert_array_equal(got[:, 7], plain[:, 7])
+
+
+@pytest.mark.parametrize("q", [0, 1])
+@pytest.mark.parametrize("depth", [0, 1, 4, 16])
+def test_quantised_walks_match_oracle_with_counts(heightfield_q, q, depth):
+    """Every walk (stack-free, or the replay walk with 1, 4 or 16 stack
+    entries, overflowing to the stack-free walk) returns the oracle's Hit
+    records, and per ray the oracle's node visits, triangle tests and parent
+    loads for that walk."""
+    import torch
+    tris, b, t, out, qb, gq, ref = heightfield_q
+    rays = scenes.random_rays(60000, [-1, -0.3, -1], [1, 0.7, 1], seed=43)
+    rays[1::3, 7] = 0.25
+    n = len(rays)
+    counts = torch.zeros(3 * n, dtype=torch.int32, device="cuda")
+    got = G.host(mb.intersect_quantised(qb, G.dev(rays), q, stack_depth=depth, counts=counts), np.uint32)
+    hits, nv, nt, nu = O.trace_quantised(ref, rays, q, counters=True, stack_depth=depth)
+    np.testing.assert_array_equal(got, hits)
+    c = G.host(counts, np.uint32)
+    np.testing.assert_array_equal(c[:n], nv, err_msg="node visits")
+    np.testing.assert_array_equal(c[n:2 * n], nt, err_msg="triangle tests")
+    np.testing.assert_array_equal(c[2 * n:], nu, err_msg="parent loads")
+    if depth == 0:
+        np.testing.assert_array_equal(got, O.trace_quantised(ref, rays, q))
+
+
+def test_quantised_replay_on_duplicate_chains(cuda):
+    """A tree of long equal-key chains (deep) overflows small stacks: still the
+    stack-free walk's Hit records."""
+    tris = np.tile(scenes.gaussian_soup(3, seed=6), (3000, 1))
+    b, t, out, qb, gq, ref = quantise_both(tris)
+    rays = scenes.random_rays(20000, [0, 0, 0], [1, 1, 1], seed=44)
+    want = O.trace_quantised(ref, rays, 0)
+    for depth in (0, 1, 4, 16):
+        got = G.host(mb.intersect_quantised(qb, G.dev(rays), 0, stack_depth=depth), np.uint32)
+        np.testing.assert_array_equal(got, want, err_msg=f"depth {depth}")
