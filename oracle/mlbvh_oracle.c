@@ -521,11 +521,10 @@ static inline void leaf_test(orc_hit* hit, const orc_triangle* tris, uint32_t le
  * Coming from the parent, go to the near hit child (entry order, ties to the
  * left) or back up; coming from the near child, go to the far child if both
  * boxes are still hit, else up; coming from the far child, go up. */
-static void trace_stackfree(orc_hit* hit, const orc_node* nodes, const orc_triangle* tris, uint32_t root,
-                            orc_f3 ro, orc_f3 rd, orc_f3 inv, float tmin, int anyHit,
-                            uint32_t* nodeVisits, uint32_t* triTests)
+static void stackfree_walk(orc_hit* hit, const orc_node* nodes, const orc_triangle* tris, uint32_t curr,
+                           uint32_t prev, orc_f3 ro, orc_f3 rd, orc_f3 inv, float tmin, int anyHit,
+                           uint32_t* nodeVisits, uint32_t* triTests)
 {
-    uint32_t curr = root, prev = ORC_INVALID;
     while (curr != ORC_INVALID)
     {
         if (is_leaf(curr))
@@ -562,6 +561,82 @@ static void trace_stackfree(orc_hit* hit, const orc_node* nodes, const orc_trian
         else next = parent;
         prev = curr;
         curr = next;
+    }
+}
+
+static void trace_stackfree(orc_hit* hit, const orc_node* nodes, const orc_triangle* tris, uint32_t root,
+                            orc_f3 ro, orc_f3 rd, orc_f3 inv, float tmin, int anyHit,
+                            uint32_t* nodeVisits, uint32_t* triTests)
+{
+    stackfree_walk(hit, nodes, tris, root, ORC_INVALID, ro, rd, inv, tmin, anyHit, nodeVisits, triTests);
+}
+
+/* stackfree_replay_step (include/mlbvh_device.cuh): intersect_stackfree's
+ * leaf order and hit.t updates without its revisits. Where both child boxes
+ * are hit, the far child and its entry distance are pushed and the near child
+ * entered; when a subtree is done, entries are popped, and an entry is entered
+ * iff its entry distance is still <= hit.t -- exactly when the stack-free
+ * walk, back at the parent from the near child, finds both boxes still hit
+ * (an entry distance does not depend on hit.t, and the near entry never
+ * exceeds the far one). A push onto a full stack (depth entries) hands over
+ * to the stack-free walk at (near child, this node). */
+static void trace_replay(orc_hit* hit, const orc_node* nodes, const orc_triangle* tris, uint32_t root, orc_f3 ro,
+                         orc_f3 rd, orc_f3 inv, float tmin, int anyHit, int depth, uint32_t* nodeVisits,
+                         uint32_t* triTests)
+{
+    uint32_t stackNode[64];
+    float stackEntry[64];
+    int top = 0;
+    uint32_t curr = root;
+    for (;;)
+    {
+        int pop = 0;
+        if (is_leaf(curr))
+        {
+            int h;
+            leaf_test(hit, tris, curr, ro, rd, tmin, &h, triTests);
+            if (h && anyHit) return;
+            pop = 1;
+        }
+        else
+        {
+            (*nodeVisits)++;
+            const orc_node* nd = &nodes[curr];
+            float lmin, lmax, rmin, rmax;
+            slabs(ro, inv, &nd->aabbs[0], hit->t, &lmin, &lmax);
+            slabs(ro, inv, &nd->aabbs[1], hit->t, &rmin, &rmax);
+            lmin = smax(lmin, tmin);
+            rmin = smax(rmin, tmin);
+            int hitL = lmin <= lmax, hitR = rmin <= rmax;
+            if (hitL && hitR)
+            {
+                uint32_t nearN = nd->children[0], farN = nd->children[1];
+                float farEntry = rmin;
+                if (rmin < lmin) { nearN = nd->children[1]; farN = nd->children[0]; farEntry = lmin; }
+                if (top == depth)
+                {
+                    stackfree_walk(hit, nodes, tris, nearN, curr, ro, rd, inv, tmin, anyHit, nodeVisits, triTests);
+                    return;
+                }
+                stackNode[top] = farN;
+                stackEntry[top] = farEntry;
+                ++top;
+                curr = nearN;
+            }
+            else if (hitL || hitR)
+                curr = nd->children[hitL ? 0 : 1];
+            else
+                pop = 1;
+        }
+        if (pop)
+        {
+            for (;;)
+            {
+                if (top == 0) return;
+                --top;
+                if (stackEntry[top] <= hit->t) { curr = stackNode[top]; break; }
+            }
+        }
     }
 }
 
@@ -679,6 +754,7 @@ typedef struct {
     int query, mode;
     orc_hit* hits;
     uint32_t *nodeVisits, *triTests;
+    int depth; /* stack entries of the replay walk (mode 3) */
 } trace_ctx;
 
 static void trace_range(void* p, uint32_t b, uint32_t e)
@@ -697,6 +773,8 @@ static void trace_range(void* p, uint32_t b, uint32_t e)
             trace_escape(&hit, c->nodes, c->tris, c->root, ro, rd, inv, r->tmin, c->query == 1, &nv, &nt);
         else if (c->mode == 2)
             trace_stackfull(&hit, c->nodes, c->tris, c->root, ro, rd, inv, r->tmin, &nv, &nt);
+        else if (c->mode == 3)
+            trace_replay(&hit, c->nodes, c->tris, c->root, ro, rd, inv, r->tmin, c->query == 1, c->depth, &nv, &nt);
         else
             trace_stackfree(&hit, c->nodes, c->tris, c->root, ro, rd, inv, r->tmin, c->query == 1, &nv, &nt);
         c->hits[i] = hit;
@@ -709,7 +787,15 @@ void orc_trace(const orc_node* nodes, const orc_triangle* tris, uint32_t root,
                const orc_ray* rays, uint32_t nRays, int query, int mode,
                orc_hit* hits, uint32_t* nodeVisits, uint32_t* triTests)
 {
-    trace_ctx c = {nodes, tris, root, rays, query, mode, hits, nodeVisits, triTests};
+    trace_ctx c = {nodes, tris, root, rays, query, mode, hits, nodeVisits, triTests, 16};
+    orc_parallel_for(nRays, 1024, trace_range, &c);
+}
+
+void orc_trace_replay(const orc_node* nodes, const orc_triangle* tris, uint32_t root, const orc_ray* rays,
+                      uint32_t nRays, int query, int depth, orc_hit* hits, uint32_t* nodeVisits, uint32_t* triTests)
+{
+    trace_ctx c = {nodes, tris, root, rays, query, 3, hits, nodeVisits, triTests,
+                   depth < 1 ? 1 : depth > 64 ? 64 : depth};
     orc_parallel_for(nRays, 1024, trace_range, &c);
 }
 

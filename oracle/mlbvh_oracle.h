@@ -87,6 +87,11 @@ int orc_check_tree(const orc_node* nodes, const orc_triangle* tris, uint32_t n, 
 void orc_trace(const orc_node* nodes, const orc_triangle* tris, uint32_t root,
                const orc_ray* rays, uint32_t nRays, int query, int mode,
                orc_hit* hits, uint32_t* nodeVisits, uint32_t* triTests);
+/* The replay walk (stackfree_replay_step): intersect_stackfree's hits with a
+ * stack of `depth` (1..64) pending far children instead of revisits. mode 3
+ * of orc_trace is this walk with 16 entries. */
+void orc_trace_replay(const orc_node* nodes, const orc_triangle* tris, uint32_t root, const orc_ray* rays,
+                      uint32_t nRays, int query, int depth, orc_hit* hits, uint32_t* nodeVisits, uint32_t* triTests);
 
 /* Camera (camera.h:10-31) */
 void orc_lookat(orc_f3 eye, orc_f3 center, orc_f3 up, float fovy, int w, int h, orc_camera* cam);

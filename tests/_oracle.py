@@ -61,6 +61,7 @@ def oracle() -> ctypes.CDLL:
             "orc_validate": (_i32, [_vp, _vp, _u32, _u32, _i32]),
             "orc_check_tree": (_i32, [_vp, _vp, _u32, _u32]),
             "orc_trace": (None, [_vp, _vp, _u32, _vp, _u32, _i32, _i32, _vp, _vp, _vp]),
+            "orc_trace_replay": (None, [_vp, _vp, _u32, _vp, _u32, _i32, _i32, _vp, _vp, _vp]),
             "orc_lookat": (None, [F3, F3, F3, _f32, _i32, _i32, _vp]),
             "orc_sobol": (None, [_u32, _u32, _u32, _u32, _vp, _vp]),
             "orc_hash_pcg": (_u32, [_u32]),
@@ -159,6 +160,22 @@ def trace(nodes, tris, root, rays, query=0, mode=0, counters=False):
     nodes_c = np.ascontiguousarray(nodes, np.uint32) if len(nodes) else np.zeros((1, 16), np.uint32)
     oracle().orc_trace(P(nodes_c), P(np.ascontiguousarray(tris, np.float32)), root, P(rays), n, query, mode,
                        P(hits), P(nv), P(nt))
+    if counters:
+        return hits, nv, nt
+    return hits
+
+
+def trace_replay(nodes, tris, root, rays, query=0, depth=16, counters=False):
+    """The replay walk over the reference node layout (same hits as trace
+    mode 0, fewer node visits)."""
+    rays = np.ascontiguousarray(rays, np.float32).reshape(-1, 8)
+    n = rays.shape[0]
+    hits = np.zeros((n, 8), np.uint32)
+    nv = np.zeros(n, np.uint32) if counters else None
+    nt = np.zeros(n, np.uint32) if counters else None
+    nodes_c = np.ascontiguousarray(nodes, np.uint32) if len(nodes) else np.zeros((1, 16), np.uint32)
+    oracle().orc_trace_replay(P(nodes_c), P(np.ascontiguousarray(tris, np.float32)), root, P(rays), n, query, depth,
+                              P(hits), P(nv), P(nt))
     if counters:
         return hits, nv, nt
     return hits

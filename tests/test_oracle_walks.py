@@ -1,4 +1,6 @@
-"""The quantised form on the oracle (CPU only): decoded child boxes contain
+"""The replay walk and the quantised form on the oracle (CPU only). The
+replay walk over the reference node layout returns intersect_stackfree's Hit
+records bit for bit at every stack depth. Decoded quantised child boxes contain
 the FP32 boxes, the quantised stack-free walk returns the FP32 tree's closest
 hits, and the replay walk (a stack of pending far children instead of
 revisits, with the stack-free walk taking over when the stack is full)
@@ -53,4 +55,17 @@ def test_replay_walk_equals_stackfree_walk(case, query, depth):
     np.testing.assert_array_equal(nt1, nt0)
     assert (nv1 <= nv0).all()
     if depth >= 16 and query == 0 and name != "duplicates":  # deep chains overflow the stack
+        assert nv1.sum() < 0.75 * nv0.sum()
+
+
+@pytest.mark.parametrize("query", [0, 1])
+@pytest.mark.parametrize("depth", [1, 2, 5, 16, 64])
+def test_replay_walk_equals_stackfree_on_fp32_nodes(case, query, depth):
+    name, tris, b, _, rays = case
+    ref, nv0, nt0 = O.trace(b["nodes"], tris, b["root"], rays, query, 0, counters=True)
+    got, nv1, nt1 = O.trace_replay(b["nodes"], tris, b["root"], rays, query, depth, counters=True)
+    np.testing.assert_array_equal(got, ref)
+    np.testing.assert_array_equal(nt1, nt0)  # the same leaves, in the same order
+    assert (nv1 <= nv0).all()
+    if depth >= 16 and query == 0 and name != "duplicates":
         assert nv1.sum() < 0.75 * nv0.sum()
