@@ -418,31 +418,42 @@ def main():
         kernel_ms = [a.elapsed_time(b) for a, b in kev]
         ao_total_s = max_over_ranks(sum(ao_ms) / 1e3)
 
-        # ---- the chosen form: the same frames over the 8-bit quantised tree
+        # ---- the other forms, at equal results: the replay walk over the same
+        # FP32 nodes, and the replay walk over the 8-bit quantised tree
         qtree = mb.QuantisedBVH.from_builder(builder, d_tris)
         occ_plain = torch.empty(w * h, dtype=torch.int32, device=dev)
-        occ_q = torch.empty_like(occ_plain)
-        qstats = torch.zeros(8, dtype=torch.int64, device=dev)
         mb.render_ao(pixels, (w, h), cam, builder.m_rootNode, builder.m_internals, d_tris, 1, wl["ns"], wl["radius"],
                      12345, occluded=occ_plain)
-        mb.render_ao_quantised(pixels, (w, h), cam, qtree, 1, wl["ns"], wl["radius"], 12345, occluded=occ_q,
-                               stats=qstats)
-        for _ in range(args.warmup):
-            mb.render_ao_quantised(pixels, (w, h), cam, qtree, 1, wl["ns"], wl["radius"], 12345)
-        qev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-        barrier()
-        torch.cuda.synchronize()
-        for i in range(args.steps):
-            if flush is not None:
-                flush.zero_()
-            qev[i][0].record(stream)
-            mb.render_ao_quantised(pixels, (w, h), cam, qtree, 1, wl["ns"], wl["radius"], 12345)
-            qev[i][1].record(stream)
-        torch.cuda.synchronize()
-        barrier()
-        q_total_s = max_over_ranks(sum(a.elapsed_time(b) for a, b in qev) / 1e3)
-        q_agree = float((occ_plain == occ_q).float().mean().item())
-        qst = qstats.cpu().numpy()
+
+        def replay_frame(occluded=None, stats=None):
+            mb.render_ao(pixels, (w, h), cam, builder.m_rootNode, builder.m_internals, d_tris, 1, wl["ns"],
+                         wl["radius"], 12345, occluded=occluded, stats=stats, traversal=mb.TRAVERSAL_REPLAY)
+
+        def quantised_frame(occluded=None, stats=None):
+            mb.render_ao_quantised(pixels, (w, h), cam, qtree, 1, wl["ns"], wl["radius"], 12345, occluded=occluded,
+                                   stats=stats)
+
+        forms = {}
+        for name, frame in (("replay", replay_frame), ("quantised", quantised_frame)):
+            occ = torch.empty_like(occ_plain)
+            fst = torch.zeros(8, dtype=torch.int64, device=dev)
+            frame(occluded=occ, stats=fst)
+            for _ in range(args.warmup):
+                frame()
+            fev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+                   for _ in range(args.steps)]
+            barrier()
+            torch.cuda.synchronize()
+            for i in range(args.steps):
+                if flush is not None:
+                    flush.zero_()
+                fev[i][0].record(stream)
+                frame()
+                fev[i][1].record(stream)
+            torch.cuda.synchronize()
+            barrier()
+            forms[name] = (max_over_ranks(sum(a.elapsed_time(b) for a, b in fev) / 1e3),
+                           float((occ_plain == occ).float().mean().item()), fst.cpu().numpy())
 
         # ---- builds
         bev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
@@ -491,7 +502,7 @@ def main():
                    "ao_rays": ao_rays, "parallelism": "replicas" if world > 1 else "single GPU",
                    "l2": "inputs larger than L2 (nodes + triangles 419 MB)" if wl["scene"] == "soup"
                    else "L2 flushed (256 MB write) between timed frames"},
-        "gpu_launches": args.steps * (3 + 3 + 7 + 10),  # AO, quantised AO, build, e2e (build + AO) steps
+        "gpu_launches": args.steps * (3 + 3 + 3 + 7 + 10),  # AO, replay AO, quantised AO, build, e2e steps
         "clocks": clocks,
     }
     # roofline of the dominant kernel (k_ao_rays): algorithmic bytes of its rays
@@ -512,15 +523,25 @@ def main():
     line["e2e"] = {"value": rays_per_frame * args.steps * world / e2e_s / 1e6, "unit": "Mrays/s",
                    "h2d_bytes_per_step": int(host_tris.numel() * 4), "d2h_bytes_per_step": int(w * h * 4),
                    "ms_per_step": e2e_s * 1e3 / args.steps}
-    q_rays = int(qst[0])
-    line["chosen"] = {
-        "form": "quantised 8-bit child boxes (32-byte nodes)", "value": q_rays * args.steps * world / q_total_s / 1e6,
-        "unit": "Mrays/s", "ms_per_step": q_total_s * 1e3 / args.steps, "vs_plain": ao_total_s / q_total_s,
-        "occlusion_agreement": q_agree, "rays_per_frame": q_rays,
-        "node_bytes_per_ray": (32 * int(qst[1]) + 4 * int(qst[5])) / max(q_rays, 1),
-        "plain_node_bytes_per_ray": 64 * visits / max(rays_per_frame, 1),
-        "tri_bytes_per_ray": 48 * int(qst[2]) / max(q_rays, 1),
-        "plain_tri_bytes_per_ray": 36 * tests / max(rays_per_frame, 1)}
+    form_lines = {}
+    for name, (total_s, agree, fst) in forms.items():
+        f_rays = int(fst[0])
+        node_bytes = (64 * int(fst[1])) if name == "replay" else (32 * int(fst[1]) + 4 * int(fst[5]))
+        tri_bytes = (36 if name == "replay" else 48) * int(fst[2])
+        form_lines[name] = {
+            "form": "FP32 nodes, replay walk (stack of pending far children)" if name == "replay"
+            else "quantised 8-bit child boxes (32-byte nodes), replay walk",
+            "value": f_rays * args.steps * world / total_s / 1e6, "unit": "Mrays/s",
+            "ms_per_step": total_s * 1e3 / args.steps, "vs_plain": ao_total_s / total_s,
+            "occlusion_agreement": agree, "rays_per_frame": f_rays,
+            "node_visits_per_ray": int(fst[1]) / max(f_rays, 1),
+            "node_bytes_per_ray": node_bytes / max(f_rays, 1), "tri_bytes_per_ray": tri_bytes / max(f_rays, 1)}
+    exact = [k for k, v in form_lines.items() if v["occlusion_agreement"] == 1.0]
+    best = max(exact, key=lambda k: form_lines[k]["value"]) if exact else None
+    line["chosen"] = dict(form_lines[best]) if best else {"form": None, "note": "no form agreed with the plain one"}
+    line["chosen"]["plain_node_visits_per_ray"] = visits / max(rays_per_frame, 1)
+    line["chosen"]["plain_node_bytes_per_ray"] = 64 * visits / max(rays_per_frame, 1)
+    line["forms"] = form_lines
     if batched is not None:
         line["batched"] = batched
         line["gpu_launches"] += batched["launches"]

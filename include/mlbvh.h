@@ -56,7 +56,11 @@ enum { MLBVH_RAY_QUERY_CLOSEST = 0, MLBVH_RAY_QUERY_ANY = 1 }; /* RAY_QUERY, min
 enum {
     MLBVH_TRAVERSAL_STACKFREE = 0,   /* intersect_stackfree,   minimum_lbvh.h:981  */
     MLBVH_TRAVERSAL_ESCAPE_LINK = 1, /* intersect_escape_link, minimum_lbvh.h:1063 */
-    MLBVH_TRAVERSAL_STACKFULL = 2    /* intersect_stackfull,   minimum_lbvh.h:912  */
+    MLBVH_TRAVERSAL_STACKFULL = 2,   /* intersect_stackfull,   minimum_lbvh.h:912  */
+    /* intersect_stackfree's Hit records (bit for bit, ties included) from a walk
+     * that keeps pending far children on a 16-entry stack instead of revisiting
+     * nodes through their parents; no reference counterpart */
+    MLBVH_TRAVERSAL_REPLAY = 3
 };
 
 typedef struct mlbvh_triangle { float vs[3][3]; } mlbvh_triangle;
@@ -315,6 +319,17 @@ MLBVH_API mlbvh_status mlbvh_render_ao(uint32_t* dPixels, uint32_t* dOccluded, i
                              const mlbvh_internal_node* dInternals, const mlbvh_triangle* dTriangles,
                              int useSobol, int nSamples, float radius, uint32_t sobolSeed,
                              unsigned long long* dStats, void* dScratch, size_t scratchBytes, void* stream);
+
+/* mlbvh_render_ao with the walk of its rays chosen: MLBVH_TRAVERSAL_STACKFREE
+ * (what mlbvh_render_ao runs) or MLBVH_TRAVERSAL_REPLAY (the same occlusion
+ * counts and pixels from fewer node loads). No reference counterpart. With
+ * dStats, node visits are those of the chosen walk. */
+MLBVH_API mlbvh_status mlbvh_render_ao_ex(uint32_t* dPixels, uint32_t* dOccluded, int width, int height,
+                                          const mlbvh_ray_generator* camera, const mlbvh_node_index* dRootNode,
+                                          const mlbvh_internal_node* dInternals, const mlbvh_triangle* dTriangles,
+                                          int useSobol, int nSamples, float radius, uint32_t sobolSeed, int traversal,
+                                          unsigned long long* dStats, void* dScratch, size_t scratchBytes,
+                                          void* stream);
 
 /* One progressive path-tracing pass (pt, main_gpu.cu:179-272): reads and
  * updates dAccumulators (float4 per pixel, w = samples so far). maxDepth is

@@ -280,6 +280,80 @@ __device__ __forceinline__ bool stackfree_step(uint32_t& curr, uint32_t& prev, H
     return curr == kInvalid;
 }
 
+// intersect_stackfree's leaf order and hit.t updates without its revisits
+// (the replay walk). Where both child boxes are hit, the far child and its
+// entry distance are pushed and the near child is entered; when a subtree is
+// done, entries are popped and an entry is entered iff its entry distance is
+// still <= hit.t. That is exactly when the stack-free walk, back at the parent
+// from the near child, finds both boxes still hit: a box's entry distance does
+// not depend on hit.t, and the near entry never exceeds the far one. So the
+// same leaves are tested in the same order against the same hit.t, and the
+// Hit record is the stack-free walk's bit for bit, ties included, while every
+// internal node is loaded once instead of up to three times.
+//
+// The stack holds kDepth entries of this thread at stack[d * stride]
+// (shared memory, one column per thread). A push onto a full stack hands the
+// walk to stackfree_step at (near child, this node), marked by depth = -1;
+// climbing through the parent links, it re-derives every entry still on the
+// stack. Start a walk with curr = root, depth = 0.
+template <bool kAny, bool kCount, int kDepth>
+__device__ __forceinline__ bool stackfree_replay_step(uint32_t& curr, uint32_t& prev, int& depth, uint2* stack,
+                                                      int stride, HitRecord& hit,
+                                                      const mlbvh_internal_node* __restrict__ nodes,
+                                                      const float* __restrict__ tris, f3 ro, f3 rd, f3 inv, float tmin,
+                                                      uint32_t& nv, uint32_t& nt)
+{
+    if (depth < 0) return stackfree_step<kAny, kCount, true>(curr, prev, hit, nodes, tris, ro, rd, inv, tmin, nv, nt);
+    if (curr & kLeafBit) {
+        if (kCount) ++nt;
+        const uint32_t ti = curr & ~kLeafBit;
+        f3 v0, v1, v2;
+        load_triangle(tris, ti, v0, v1, v2);
+        float t, u, v;
+        f3 ng;
+        if (intersect_triangle(t, u, v, ng, tmin, hit.t, ro, rd, v0, v1, v2)) {
+            hit.t = t;
+            hit.u = u;
+            hit.v = v;
+            hit.ng = ng;
+            hit.tri = ti;
+            if (kAny) return true;
+        }
+    } else {
+        if (kCount) ++nv;
+        const NodeView nd = load_node<true>(nodes, curr);
+        const float2 rl = slab(ro, inv, nd.lo0, nd.hi0, tmin, hit.t);
+        const float2 rr = slab(ro, inv, nd.lo1, nd.hi1, tmin, hit.t);
+        const bool hitL = rl.x <= rl.y, hitR = rr.x <= rr.y;
+        if (hitL && hitR) {
+            const bool swap = rr.x < rl.x;
+            const uint32_t nearN = swap ? nd.c1 : nd.c0, farN = swap ? nd.c0 : nd.c1;
+            if (depth == kDepth) {  // full: continue as the stack-free walk
+                depth = -1;
+                prev = curr;
+                curr = nearN;
+                return false;
+            }
+            stack[depth * stride] = make_uint2(farN, __float_as_uint(swap ? rl.x : rr.x));
+            ++depth;
+            curr = nearN;
+            return false;
+        }
+        if (hitL || hitR) {
+            curr = hitL ? nd.c0 : nd.c1;
+            return false;
+        }
+    }
+    while (depth > 0) {
+        const uint2 e = stack[--depth * stride];
+        if (__uint_as_float(e.y) <= hit.t) {
+            curr = e.x;
+            return false;
+        }
+    }
+    return true;
+}
+
 template <bool kAny, bool kCount = false, bool kWide = false>
 __device__ __forceinline__ void trace_stackfree(HitRecord& hit, const mlbvh_internal_node* __restrict__ nodes,
                                                 const float* __restrict__ tris, uint32_t root, f3 ro, f3 rd,

@@ -19,7 +19,7 @@ import numpy as np
 __all__ = [
     "lib", "library_path", "MlbvhError", "BUILD_OPTION_USE_NORMAL", "BUILD_OPTION_CPU_PARALLEL",
     "RAY_QUERY_CLOSEST", "RAY_QUERY_ANY", "TRAVERSAL_STACKFREE", "TRAVERSAL_ESCAPE_LINK",
-    "TRAVERSAL_STACKFULL", "OnesweepSort", "BVHGPUBuilder", "RayGenerator", "intersect",
+    "TRAVERSAL_STACKFULL", "TRAVERSAL_REPLAY", "OnesweepSort", "BVHGPUBuilder", "RayGenerator", "intersect",
     "render_normal", "render_ao", "render_pt", "pack", "profile_events", "FLT_MAX", "INVALID_NODE",
     "QuantisedBVH", "intersect_quantised", "render_ao_quantised", "pt_diff_render", "pt_diff_adjoint",
     "BatchParams", "BatchedBVH",
@@ -32,6 +32,7 @@ RAY_QUERY_ANY = 1              # minimum_lbvh.h:978
 TRAVERSAL_STACKFREE = 0
 TRAVERSAL_ESCAPE_LINK = 1
 TRAVERSAL_STACKFULL = 2
+TRAVERSAL_REPLAY = 3  # intersect_stackfree's hits from a stack of pending far children (no revisits)
 FLT_MAX = float(np.float32(3.402823466e38))
 INVALID_NODE = 0x7FFFFFFF
 
@@ -75,6 +76,8 @@ def lib() -> ctypes.CDLL:
             "mlbvh_render_ao": (i32, [_vp, _vp, i32, i32, _vp, _vp, _vp, _vp, i32, i32, f32, u32, _vp, _vp, sz,
                                       _vp]),
             "mlbvh_render_pt": (i32, [_vp, i32, i32, _vp, _vp, _vp, _vp, _vp, i32, i32, i32, _vp]),
+            "mlbvh_render_ao_ex": (i32, [_vp, _vp, i32, i32, _vp, _vp, _vp, _vp, i32, i32, f32, u32, i32, _vp, _vp,
+                                         sz, _vp]),
             "mlbvh_pack": (i32, [_vp, _vp, i32, _vp]),
             "mlbvh_profile_events": (None, [_vp, _vp]),
             "mlbvh_quantise": (i32, [_vp, _vp, _vp, u32, _vp, _vp, _vp, _vp, _vp]),
@@ -290,10 +293,11 @@ def profile_events(start=None, stop=None):
 
 def render_ao(pixels, imageSize, rayGenerator: RayGenerator, rootNode, internals, triangles, useSobol: int = 1,
               nSamples: int = 16, radius: float = 1.0, seed: int = 12345, occluded=None, stats=None,
-              scratch=None, stream=None):
+              scratch=None, stream=None, traversal: int = TRAVERSAL_STACKFREE):
     """ao (main_gpu.cu:111-177) with sample count, radius and Sobol seed as
     parameters (the reference fixes 16, 1.0, 12345). ``stats`` (int64 CUDA
-    tensor of 3) receives rays traced, node visits and triangle tests."""
+    tensor of 8) receives rays traced, node visits and triangle tests.
+    ``traversal`` TRAVERSAL_REPLAY gives the same result from the replay walk."""
     import torch
     w, h = imageSize
     need = lib().mlbvh_render_scratch_bytes(int(w), int(h))
@@ -305,10 +309,16 @@ def render_ao(pixels, imageSize, rayGenerator: RayGenerator, rootNode, internals
             _render_scratch.clear()
             _render_scratch[key] = scratch
     cam = rayGenerator._cstruct()
-    _check(lib().mlbvh_render_ao(_ptr(pixels), _ptr(occluded), int(w), int(h), ctypes.addressof(cam),
-                                 _ptr(rootNode), _ptr(internals), _ptr(triangles), int(useSobol), int(nSamples),
-                                 float(radius), int(seed), _ptr(stats), _ptr(scratch), scratch.numel(),
-                                 _stream(stream)))
+    if traversal == TRAVERSAL_STACKFREE:
+        _check(lib().mlbvh_render_ao(_ptr(pixels), _ptr(occluded), int(w), int(h), ctypes.addressof(cam),
+                                     _ptr(rootNode), _ptr(internals), _ptr(triangles), int(useSobol), int(nSamples),
+                                     float(radius), int(seed), _ptr(stats), _ptr(scratch), scratch.numel(),
+                                     _stream(stream)))
+    else:
+        _check(lib().mlbvh_render_ao_ex(_ptr(pixels), _ptr(occluded), int(w), int(h), ctypes.addressof(cam),
+                                        _ptr(rootNode), _ptr(internals), _ptr(triangles), int(useSobol),
+                                        int(nSamples), float(radius), int(seed), int(traversal), _ptr(stats),
+                                        _ptr(scratch), scratch.numel(), _stream(stream)))
     return pixels
 
 

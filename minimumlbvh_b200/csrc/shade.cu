@@ -109,8 +109,12 @@ __device__ __forceinline__ void add_stats(unsigned long long* stats, const Count
     }
 }
 
-// The two tree formats the AO kernels run over.
-struct PlainTree {
+// The tree formats and walks the AO kernels run over: the reference node
+// layout with the stack-free walk (kReplay false) or the replay walk (kReplay
+// true: the same Hit records from a stack of pending far children), and the
+// quantised tree with the replay walk.
+template <bool kReplay>
+struct PlainTreeT {
     const mlbvh_internal_node* nodes;
     const float* tris;
     const mlbvh_node_index* rootPtr;
@@ -123,15 +127,20 @@ struct PlainTree {
     {
         trace_stackfree<kAny, kCount, true>(hit, nodes, tris, c.root, ro, rd, inv_rd(rd), 0.0f, &n.visits, &n.tests);
     }
-    // the reference's stack-free walk: no stack
-    static constexpr int kStack = 0;
+    static constexpr int kStack = kReplay ? 16 : 0;
     template <bool kAny, bool kCount>
-    __device__ __forceinline__ bool step(const Ctx&, uint32_t& curr, uint32_t& prev, int&, uint2*, HitRecord& hit,
-                                         f3 ro, f3 rd, f3 inv, Counts& n) const
+    __device__ __forceinline__ bool step(const Ctx&, uint32_t& curr, uint32_t& prev, int& depth, uint2* stack,
+                                         HitRecord& hit, f3 ro, f3 rd, f3 inv, Counts& n) const
     {
+        if (kReplay)
+            return stackfree_replay_step<kAny, kCount, kReplay ? 16 : 1>(curr, prev, depth, stack, kAoThreads, hit,
+                                                                         nodes, tris, ro, rd, inv, 0.0f, n.visits,
+                                                                         n.tests);
         return stackfree_step<kAny, kCount, true>(curr, prev, hit, nodes, tris, ro, rd, inv, 0.0f, n.visits, n.tests);
     }
 };
+using PlainTree = PlainTreeT<false>;
+using PlainReplayTree = PlainTreeT<true>;
 struct QuantTree {
     const mlbvh_qnode* qnodes;
     const uint32_t* parents;
@@ -563,12 +572,19 @@ mlbvh_status render_normal(uint32_t* dPixels, int w, int h, const mlbvh_ray_gene
 mlbvh_status render_ao(uint32_t* dPixels, uint32_t* dOccluded, int w, int h, const mlbvh_ray_generator& cam,
                        const mlbvh_node_index* dRoot, const mlbvh_internal_node* dNodes, const mlbvh_triangle* dTris,
                        int useSobol, int nSamples, float radius, uint32_t seed, unsigned long long* dStats,
-                       void* dScratch, size_t scratchBytes, cudaStream_t stream)
+                       void* dScratch, size_t scratchBytes, int traversal, cudaStream_t stream)
 {
     if (mlbvh_status s = check_ao_args(w, h, nSamples, dPixels, dOccluded, dScratch, dStats)) return s;
     if (!dRoot || !dTris) return fail(MLBVH_ERR_INVALID_ARG, "null pointer");
     if (!aligned16(dRoot) || !aligned32(dNodes) || !aligned16(dTris))
         return fail(MLBVH_ERR_INVALID_ARG, "device pointers must be 16-byte aligned");
+    if (traversal == MLBVH_TRAVERSAL_REPLAY) {
+        const PlainReplayTree tree{dNodes, reinterpret_cast<const float*>(dTris), dRoot};
+        return launch_ao(dPixels, dOccluded, w, h, cam, tree, useSobol, nSamples, radius, seed, dStats, dScratch,
+                         scratchBytes, stream);
+    }
+    if (traversal != MLBVH_TRAVERSAL_STACKFREE)
+        return fail(MLBVH_ERR_INVALID_ARG, "AO traversal must be MLBVH_TRAVERSAL_STACKFREE or MLBVH_TRAVERSAL_REPLAY");
     const PlainTree tree{dNodes, reinterpret_cast<const float*>(dTris), dRoot};
     return launch_ao(dPixels, dOccluded, w, h, cam, tree, useSobol, nSamples, radius, seed, dStats, dScratch,
                      scratchBytes, stream);

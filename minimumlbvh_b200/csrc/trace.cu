@@ -2,7 +2,8 @@
 //
 // Replaces the per-ray device calls of intersect_stackfree (minimum_lbvh.h:
 // 981-1061), intersect_escape_link (:1063-1137) and intersect_stackfull
-// (:912-973) with a single launch. Rays and hits move as 2 x 16-byte vectors,
+// (:912-973) with a single launch; MLBVH_TRAVERSAL_REPLAY gives
+// intersect_stackfree's Hit records through the replay walk. Rays and hits move as 2 x 16-byte vectors,
 // nodes as 4 x 16-byte read-only loads.
 #include "capi_internal.h"
 #include "../../include/mlbvh_device.cuh"
@@ -13,11 +14,14 @@ namespace {
 
 constexpr int kTraceThreads = 128;
 
+constexpr int kReplayDepth = 16;  // stack entries per ray of the replay walk
+
 template <int kMode, bool kAny>
 __global__ void __launch_bounds__(kTraceThreads)
     k_trace(const mlbvh_internal_node* __restrict__ nodes, const mlbvh_node_index* __restrict__ rootPtr,
             const float* __restrict__ tris, const float4* __restrict__ rays, float4* __restrict__ hits, uint32_t n)
 {
+    __shared__ uint2 s_stack[kMode == MLBVH_TRAVERSAL_REPLAY ? kReplayDepth : 1][kTraceThreads];
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const float4 a = __ldg(rays + 2 * (size_t)i), b = __ldg(rays + 2 * (size_t)i + 1);
@@ -33,6 +37,14 @@ __global__ void __launch_bounds__(kTraceThreads)
     const f3 inv = inv_rd(rd);
     if (kMode == MLBVH_TRAVERSAL_ESCAPE_LINK) {
         trace_escape<kAny>(hit, nodes, tris, root, ro, rd, inv, tmin);
+    } else if (kMode == MLBVH_TRAVERSAL_REPLAY) {
+        uint32_t curr = root, prev = kInvalid, nv = 0, nt = 0;
+        int depth = 0;
+        for (uint32_t steps = 1; steps < kMaxTraversalSteps; ++steps)
+            if (stackfree_replay_step<kAny, false, kReplayDepth>(curr, prev, depth, &s_stack[0][threadIdx.x],
+                                                                 kTraceThreads, hit, nodes, tris, ro, rd, inv, tmin,
+                                                                 nv, nt))
+                break;
     } else if (kMode == MLBVH_TRAVERSAL_STACKFULL) {
         uint32_t stack[64];
         trace_stackfull(hit, nodes, tris, root, ro, rd, inv, tmin, stack, 64);
@@ -72,6 +84,12 @@ mlbvh_status trace(const mlbvh_internal_node* dNodes, const mlbvh_node_index* dR
             k_trace<MLBVH_TRAVERSAL_ESCAPE_LINK, true><<<blocks, kTraceThreads, 0, stream>>>(dNodes, dRoot, tris, rays, hits, nRays);
         else
             k_trace<MLBVH_TRAVERSAL_ESCAPE_LINK, false><<<blocks, kTraceThreads, 0, stream>>>(dNodes, dRoot, tris, rays, hits, nRays);
+        break;
+    case MLBVH_TRAVERSAL_REPLAY:
+        if (any)
+            k_trace<MLBVH_TRAVERSAL_REPLAY, true><<<blocks, kTraceThreads, 0, stream>>>(dNodes, dRoot, tris, rays, hits, nRays);
+        else
+            k_trace<MLBVH_TRAVERSAL_REPLAY, false><<<blocks, kTraceThreads, 0, stream>>>(dNodes, dRoot, tris, rays, hits, nRays);
         break;
     case MLBVH_TRAVERSAL_STACKFULL:
         k_trace<MLBVH_TRAVERSAL_STACKFULL, false><<<blocks, kTraceThreads, 0, stream>>>(dNodes, dRoot, tris, rays, hits, nRays);

@@ -21,13 +21,13 @@ def channels(p):
     return np.stack([(p >> s) & 255 for s in (0, 8, 16, 24)], -1).astype(np.int32)
 
 
-def gpu_ao(b, t, cam, w, h, ns, radius, seed=12345, sobol=1):
+def gpu_ao(b, t, cam, w, h, ns, radius, seed=12345, sobol=1, traversal=mb.TRAVERSAL_STACKFREE):
     import torch
     px = torch.zeros(w * h, dtype=torch.int32, device="cuda")
     occ = torch.zeros(w * h, dtype=torch.int32, device="cuda")
     stats = torch.zeros(8, dtype=torch.int64, device="cuda")
     mb.render_ao(px, (w, h), mb.RayGenerator.from_array(cam), b.m_rootNode, b.m_internals, t, sobol, ns, radius,
-                 seed, occluded=occ, stats=stats)
+                 seed, occluded=occ, stats=stats, traversal=traversal)
     torch.cuda.synchronize()
     st = G.host(stats)
     return G.host(px, np.uint32), G.host(occ, np.uint32), (int(st[0]), int(st[1]), int(st[2]))
@@ -69,6 +69,22 @@ def test_ao_heightfield_config(cuda):
     assert st == (int(cnt[2]), int(cnt[0]), int(cnt[1]))
 
 
+@pytest.mark.parametrize("sobol", [1, 0])
+def test_ao_replay_walk_equals_stackfree(cuda, sobol):
+    """The replay walk gives every pixel's occlusion count of the stack-free
+    walk (which the oracle pins), with fewer internal-node visits."""
+    tris = scenes.heightfield_icospheres()
+    b, t, out = G.build(tris)
+    eye, c, up, fovy = scenes.camera_heightfield()
+    cam = O.lookat(eye, c, up, fovy, 512, 512)
+    px0, occ0, st0 = gpu_ao(b, t, cam, 512, 512, 16, 0.25, sobol=sobol)
+    px1, occ1, st1 = gpu_ao(b, t, cam, 512, 512, 16, 0.25, sobol=sobol, traversal=mb.TRAVERSAL_REPLAY)
+    np.testing.assert_array_equal(occ1, occ0)
+    np.testing.assert_array_equal(px1, px0)
+    assert st1[0] == st0[0] and st1[2] == st0[2]  # rays and triangle tests: the same leaves
+    assert st1[1] < st0[1]
+
+
 def test_ao_soup_config_rows(cuda):
     """4M-triangle soup, 1920 x 1080, 64 AO rays per hit, radius 0.1: the
     whole frame on the GPU, three row bands checked against the oracle."""
@@ -78,6 +94,8 @@ def test_ao_soup_config_rows(cuda):
     w, h = 1920, 1080
     cam = O.lookat(eye, c, up, fovy, w, h)
     px, occ, _ = gpu_ao(b, t, cam, w, h, 64, 0.1)
+    _, occ_replay, _ = gpu_ao(b, t, cam, w, h, 64, 0.1, traversal=mb.TRAVERSAL_REPLAY)
+    np.testing.assert_array_equal(occ_replay, occ)
     for r0 in (300, 540, 700):
         rpx, rocc = O.render_ao(cam, out["root"], out["nodes"], tris, w, h, 64, 0.1, 12345, 1, trig=1,
                                 rows=(r0, r0 + 4))
