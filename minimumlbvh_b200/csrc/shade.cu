@@ -29,7 +29,7 @@ struct AoRecord {
 };
 
 struct RenderLayout {
-    size_t header;  // u32 queue count, u32 pad, u32 work counter
+    size_t header;  // u32 queue count, u32 pad, u64 work counter
     size_t records;
     size_t counts;
     size_t total;
@@ -220,116 +220,113 @@ __global__ void __launch_bounds__(kTileW* kTileH)
     }
 }
 
-// AO rays (main_gpu.cu:146-173), scheduled per lane. A work item is a run of
-// consecutive samples of one hit pixel (all nSamples when there are enough
-// pixels to fill the grid eight times over, else halved down to 4 samples).
-// Each lane owns one item at a time and traces its any-hit rays one after
-// another, advancing its walk one node (or leaf) per loop iteration; lanes
-// that finish take new items from the queue in warp-wide batches (one atomic
-// per batch) once a quarter of the warp is idle or the warp has nothing left.
-// So lanes never wait for the longest ray of their warp. A finished item adds
-// its occlusion count to its pixel's.
-// Setting up a ray (Sobol point, hemisphere direction, reciprocal direction)
-// costs about as much as several traversal steps; a lane whose ray is done
-// waits until kStartBatch lanes of its warp need a new ray (or no lane has a
-// ray in flight), so that the set-up runs for many lanes at once instead of
-// once per finishing lane.
-constexpr int kRefillBatch = 8;
+// AO rays (main_gpu.cu:146-173), scheduled per lane. A work item is one AO
+// sample of one hit pixel, item i = (queue entry i / nSamples, sample
+// i % nSamples). A warp takes kChunk consecutive items per atomic on the work
+// counter, so its lanes mostly trace samples of the same pixel: rays from one
+// origin share their upper paths, and the warp's node loads coalesce. Each
+// lane traces its own ray one node (or leaf) per loop iteration and takes the
+// next item as soon as it is free, so lanes never wait for the longest ray of
+// their warp. Setting a ray up (Sobol point, hemisphere direction, reciprocal
+// direction) costs about as much as several traversal steps, so free lanes
+// take items once kStartBatch of them are free (or none is busy), and the
+// set-up runs for many lanes at once. An occluded ray adds one to its pixel's
+// count; the lanes of a warp add per pixel with one atomic.
+constexpr int kChunk = 64;
 constexpr int kStartBatch = 4;
 
 template <class Tree, bool kCount>
 __global__ void __launch_bounds__(kAoThreads, 8)  // at most 64 registers: 32 warps per SM
     k_ao_rays(const AoRecord* __restrict__ records, const uint32_t* __restrict__ queueCount,
-              uint32_t* __restrict__ workCounter, int w, int nSamples, float radius, uint32_t seed, int useSobol,
-              Tree tree, uint32_t* __restrict__ counts, unsigned long long* __restrict__ stats)
+              unsigned long long* __restrict__ workCounter, int w, int nSamples, float radius, uint32_t seed,
+              int useSobol, Tree tree, uint32_t* __restrict__ counts, unsigned long long* __restrict__ stats)
 {
     Counts cnt;
     const int lane = threadIdx.x & 31;
     const uint32_t lanesBelow = (1u << lane) - 1u;
-    const uint32_t pixels = *queueCount;
-    const uint64_t lanes = (uint64_t)gridDim.x * blockDim.x;
-    uint32_t chunk = (uint32_t)nSamples;
-    while (chunk > 4 && (uint64_t)pixels * ((nSamples + chunk - 1) / chunk) < 8 * lanes) chunk = (chunk + 1) / 2;
-    if ((uint64_t)pixels * ((nSamples + chunk - 1) / chunk) > 0xFFFFFFFFull) chunk = (uint32_t)nSamples;
-    const uint32_t itemsPerPixel = (nSamples + chunk - 1) / chunk;
-    const uint32_t total = pixels * itemsPerPixel;
+    const unsigned long long total = (unsigned long long)(*queueCount) * (unsigned long long)nSamples;
     const typename Tree::Ctx ctx = tree.context();
     __shared__ uint2 s_stack[Tree::kStack > 0 ? Tree::kStack : 1][kAoThreads];
     uint2* const stack = &s_stack[0][threadIdx.x];
+    unsigned long long poolNext = 0, poolEnd = 0;  // warp-uniform: items taken, not yet handed out
+    bool exhausted = false;                        // warp-uniform: the work counter is past the end
+    bool live = false;                             // this lane has a ray in flight
+    uint32_t pixel = 0, curr = 0, prev = 0, steps = 0;
     int depth = 0;
-    bool exhausted = false;  // warp-uniform: the queue has no item left
-    bool owns = false;       // this lane owns an item
-    bool live = false;       // this lane has a ray in flight
-    uint32_t pixel = 0, s = 0, sEnd = 0, occ = 0, xi = 0, yi = 0, curr = 0, prev = 0, steps = 0;
-    f3 origin = mk(0, 0, 0), n = origin, xaxis = origin, zaxis = origin, dir = origin, inv = origin;
+    f3 origin = mk(0, 0, 0), dir = origin, inv = origin;
     HitRecord hit;
     hit.t = radius;
     for (;;) {
-        const uint32_t idle = __ballot_sync(0xffffffffu, !owns);
-        if (!exhausted && (__popc(idle) >= kRefillBatch || idle == 0xffffffffu)) {
-            const int leader = __ffs(idle) - 1;
-            uint32_t base = 0;
-            if (lane == leader) base = atomicAdd(workCounter, (uint32_t)__popc(idle));
-            base = __shfl_sync(0xffffffffu, base, leader);
-            if (base + (uint32_t)__popc(idle) >= total) exhausted = true;
-            if (!owns) {
-                const uint32_t item = base + __popc(idle & lanesBelow);
-                if (item < total) {
-                    const uint32_t entry = item / itemsPerPixel;
-                    s = (item - entry * itemsPerPixel) * chunk;
-                    sEnd = min(s + chunk, (uint32_t)nSamples);
+        const uint32_t idle = __ballot_sync(0xffffffffu, !live);
+        if (idle == 0xffffffffu || (uint32_t)__popc(idle) >= (uint32_t)kStartBatch) {
+            if (poolNext >= poolEnd && !exhausted) {
+                unsigned long long base = 0;
+                if (lane == 0) base = atomicAdd(workCounter, (unsigned long long)kChunk);
+                base = __shfl_sync(0xffffffffu, base, 0);
+                if (base >= total) {
+                    exhausted = true;
+                } else {
+                    poolNext = base;
+                    poolEnd = min(base + (unsigned long long)kChunk, total);
+                }
+            }
+            if (poolNext < poolEnd) {
+                const unsigned long long avail = poolEnd - poolNext;
+                const uint32_t rank = __popc(idle & lanesBelow);
+                if (!live && rank < avail) {  // start item poolNext + rank
+                    const unsigned long long item = poolNext + rank;
+                    const uint32_t entry = (uint32_t)(item / (uint32_t)nSamples);
+                    const uint32_t s = (uint32_t)(item - (unsigned long long)entry * (uint32_t)nSamples);
                     const float4* rp = reinterpret_cast<const float4*>(records + entry);
                     const float4 r0 = __ldg(rp), r1 = __ldg(rp + 1);
                     origin = mk(r0.x, r0.y, r0.z);
-                    n = mk(r0.w, r1.x, r1.y);
+                    const f3 n = mk(r0.w, r1.x, r1.y);
                     pixel = __float_as_uint(r1.z);
-                    xi = pixel % (uint32_t)w;
-                    yi = pixel / (uint32_t)w;
+                    f3 xaxis, zaxis;
                     onb(n, xaxis, zaxis);
-                    occ = 0;
-                    owns = true;
-                    live = false;
+                    float2 rnd;
+                    if (useSobol) {
+                        rnd = sobol2d(s, pixel % (uint32_t)w, pixel / (uint32_t)w, seed);
+                    } else {
+                        Pcg rng(hash_pcg(pixel), 0);
+                        pcg_advance(rng, 2ull * s);
+                        rnd.x = rng.uniformf();
+                        rnd.y = rng.uniformf();
+                    }
+                    const f3 dl = sample_hemisphere(rnd.x, rnd.y);
+                    dir = xaxis * dl.x + zaxis * dl.z + n * dl.y;
+                    inv = inv_rd(dir);
+                    hit.t = radius;
+                    hit.tri = 0xFFFFFFFFu;
+                    curr = ctx.root;
+                    prev = kInvalid;
+                    depth = 0;
+                    steps = 0;
+                    live = true;
                 }
+                poolNext += min((unsigned long long)__popc(idle), avail);
             }
         }
-        if (!__any_sync(0xffffffffu, owns)) {
+        if (!__any_sync(0xffffffffu, live)) {
             if (exhausted) break;
             continue;
         }
-        const uint32_t starters = __ballot_sync(0xffffffffu, owns && !live);
-        const uint32_t inFlight = __ballot_sync(0xffffffffu, live);
-        if (owns && !live && (__popc(starters) >= kStartBatch || inFlight == 0u)) {
-            // start sample s of this lane's pixel
-            float2 rnd;
-            if (useSobol) {
-                rnd = sobol2d(s, xi, yi, seed);
-            } else {
-                Pcg rng(hash_pcg(pixel), 0);
-                pcg_advance(rng, 2ull * s);
-                rnd.x = rng.uniformf();
-                rnd.y = rng.uniformf();
-            }
-            const f3 dl = sample_hemisphere(rnd.x, rnd.y);
-            dir = xaxis * dl.x + zaxis * dl.z + n * dl.y;
-            inv = inv_rd(dir);
-            hit.t = radius;
-            hit.tri = 0xFFFFFFFFu;
-            curr = ctx.root;
-            prev = kInvalid;
-            depth = 0;
-            steps = 0;
-            live = true;
-        }
+        bool occluded = false;
         if (live) {
             if (tree.template step<true, kCount>(ctx, curr, prev, depth, stack, hit, origin, dir, inv, cnt) ||
                 ++steps >= kMaxTraversalSteps) {
                 live = false;
-                if (hit.t != radius) ++occ;
-                if (++s == sEnd) {
-                    if (occ) atomicAdd(counts + pixel, occ);
-                    owns = false;
-                }
+                occluded = hit.t != radius;
             }
+        }
+        // one atomic per pixel among the lanes whose ray just ended occluded
+        uint32_t pending = __ballot_sync(0xffffffffu, occluded);
+        while (pending) {
+            const int leader = __ffs(pending) - 1;
+            const uint32_t p = __shfl_sync(0xffffffffu, pixel, leader);
+            const uint32_t same = __ballot_sync(0xffffffffu, occluded && pixel == p);
+            if (lane == leader) atomicAdd(counts + p, (uint32_t)__popc(same));
+            pending &= ~same;
         }
     }
     if (kCount) add_stats(stats, cnt, true);
@@ -507,6 +504,7 @@ mlbvh_status launch_ao(uint32_t* dPixels, uint32_t* dOccluded, int w, int h, con
     uint32_t* header = reinterpret_cast<uint32_t*>(s + L.header);
     AoRecord* records = reinterpret_cast<AoRecord*>(s + L.records);
     uint32_t* counts = reinterpret_cast<uint32_t*>(s + L.counts);
+    unsigned long long* work = reinterpret_cast<unsigned long long*>(s + L.header + 8);
 
     cudaError_t e = cudaMemsetAsync(header, 0, 16, stream);  // queue count, 64-bit work counter
     if (e == cudaSuccess && dStats) e = cudaMemsetAsync(dStats, 0, 8 * sizeof(unsigned long long), stream);
@@ -522,10 +520,10 @@ mlbvh_status launch_ao(uint32_t* dPixels, uint32_t* dOccluded, int w, int h, con
     if (ev.start) cudaEventRecord(ev.start, stream);
     if (dStats)
         k_ao_rays<Tree, true><<<ao_ray_blocks<Tree>(), kAoThreads, 0, stream>>>(
-            records, header, header + 2, w, nSamples, radius, seed, useSobol, tree, counts, dStats);
+            records, header, work, w, nSamples, radius, seed, useSobol, tree, counts, dStats);
     else
         k_ao_rays<Tree, false><<<ao_ray_blocks<Tree>(), kAoThreads, 0, stream>>>(
-            records, header, header + 2, w, nSamples, radius, seed, useSobol, tree, counts, nullptr);
+            records, header, work, w, nSamples, radius, seed, useSobol, tree, counts, nullptr);
     MLBVH_CHECK_LAUNCH("k_ao_rays");
     if (ev.stop) cudaEventRecord(ev.stop, stream);
     const int px = w * h;
