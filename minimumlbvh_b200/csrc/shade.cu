@@ -233,7 +233,7 @@ __global__ void __launch_bounds__(kTileW* kTileH)
 // set-up runs for many lanes at once. An occluded ray adds one to its pixel's
 // count; the lanes of a warp add per pixel with one atomic.
 constexpr int kChunk = 64;
-constexpr int kStartBatch = 4;
+constexpr int kStartBatch = 8;
 
 template <class Tree, bool kCount>
 __global__ void __launch_bounds__(kAoThreads, 8)  // at most 64 registers: 32 warps per SM
