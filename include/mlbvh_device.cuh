@@ -280,6 +280,19 @@ __device__ __forceinline__ bool stackfree_step(uint32_t& curr, uint32_t& prev, H
     return curr == kInvalid;
 }
 
+// Stack entries of the replay walks. A closest-hit walk keeps the pending far
+// child and its entry distance; an any-hit walk keeps the child alone: its
+// hit.t does not change before the first hit, which ends the walk, so every
+// pending child still passes the entry test when it is popped.
+template <bool kAny>
+struct ReplayStack {
+    using Entry = uint2;
+};
+template <>
+struct ReplayStack<true> {
+    using Entry = uint32_t;
+};
+
 // intersect_stackfree's leaf order and hit.t updates without its revisits
 // (the replay walk). Where both child boxes are hit, the far child and its
 // entry distance are pushed and the near child is entered; when a subtree is
@@ -297,7 +310,8 @@ __device__ __forceinline__ bool stackfree_step(uint32_t& curr, uint32_t& prev, H
 // climbing through the parent links, it re-derives every entry still on the
 // stack. Start a walk with curr = root, depth = 0.
 template <bool kAny, bool kCount, int kDepth>
-__device__ __forceinline__ bool stackfree_replay_step(uint32_t& curr, uint32_t& prev, int& depth, uint2* stack,
+__device__ __forceinline__ bool stackfree_replay_step(uint32_t& curr, uint32_t& prev, int& depth,
+                                                      typename ReplayStack<kAny>::Entry* stack,
                                                       int stride, HitRecord& hit,
                                                       const mlbvh_internal_node* __restrict__ nodes,
                                                       const float* __restrict__ tris, f3 ro, f3 rd, f3 inv, float tmin,
@@ -334,7 +348,10 @@ __device__ __forceinline__ bool stackfree_replay_step(uint32_t& curr, uint32_t& 
                 curr = nearN;
                 return false;
             }
-            stack[depth * stride] = make_uint2(farN, __float_as_uint(swap ? rl.x : rr.x));
+            if constexpr (kAny)
+                stack[depth * stride] = farN;
+            else
+                stack[depth * stride] = make_uint2(farN, __float_as_uint(swap ? rl.x : rr.x));
             ++depth;
             curr = nearN;
             return false;
@@ -344,14 +361,20 @@ __device__ __forceinline__ bool stackfree_replay_step(uint32_t& curr, uint32_t& 
             return false;
         }
     }
-    while (depth > 0) {
-        const uint2 e = stack[--depth * stride];
-        if (__uint_as_float(e.y) <= hit.t) {
-            curr = e.x;
-            return false;
+    if constexpr (kAny) {
+        if (depth == 0) return true;
+        curr = stack[--depth * stride];
+        return false;
+    } else {
+        while (depth > 0) {
+            const uint2 e = stack[--depth * stride];
+            if (__uint_as_float(e.y) <= hit.t) {
+                curr = e.x;
+                return false;
+            }
         }
+        return true;
     }
-    return true;
 }
 
 template <bool kAny, bool kCount = false, bool kWide = false>
@@ -816,7 +839,8 @@ __device__ __forceinline__ bool quantised_step(uint32_t& curr, uint32_t& prev, H
 // depth = -1; climbing through the parents, it re-derives every entry still
 // on the stack. Start a walk with curr = root, depth = 0.
 template <bool kAny, bool kCount, int kDepth>
-__device__ __forceinline__ bool quantised_replay_step(uint32_t& curr, uint32_t& prev, int& depth, uint2* stack,
+__device__ __forceinline__ bool quantised_replay_step(uint32_t& curr, uint32_t& prev, int& depth,
+                                                      typename ReplayStack<kAny>::Entry* stack,
                                                       int stride, HitRecord& hit,
                                                       const mlbvh_qnode* __restrict__ qnodes,
                                                       const uint32_t* __restrict__ parents,
@@ -856,7 +880,10 @@ __device__ __forceinline__ bool quantised_replay_step(uint32_t& curr, uint32_t& 
                 curr = nearN;
                 return false;
             }
-            stack[depth * stride] = make_uint2(farN, __float_as_uint(swap ? rl.x : rr.x));
+            if constexpr (kAny)
+                stack[depth * stride] = farN;
+            else
+                stack[depth * stride] = make_uint2(farN, __float_as_uint(swap ? rl.x : rr.x));
             ++depth;
             curr = nearN;
             return false;
@@ -866,14 +893,20 @@ __device__ __forceinline__ bool quantised_replay_step(uint32_t& curr, uint32_t& 
             return false;
         }
     }
-    while (depth > 0) {
-        const uint2 e = stack[--depth * stride];
-        if (__uint_as_float(e.y) <= hit.t) {
-            curr = e.x;
-            return false;
+    if constexpr (kAny) {
+        if (depth == 0) return true;
+        curr = stack[--depth * stride];
+        return false;
+    } else {
+        while (depth > 0) {
+            const uint2 e = stack[--depth * stride];
+            if (__uint_as_float(e.y) <= hit.t) {
+                curr = e.x;
+                return false;
+            }
         }
+        return true;
     }
-    return true;
 }
 
 template <bool kAny, bool kCount = false, bool kWide = false>

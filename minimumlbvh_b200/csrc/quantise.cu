@@ -140,7 +140,7 @@ __global__ void __launch_bounds__(kTraceThreads)
                       const float4* __restrict__ rays, float4* __restrict__ hits, uint32_t n,
                       uint32_t* __restrict__ counts)
 {
-    __shared__ uint2 s_stack[kDepth > 0 ? kDepth : 1][kTraceThreads];
+    __shared__ typename ReplayStack<kAny>::Entry s_stack[kDepth > 0 ? kDepth : 1][kTraceThreads];
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const float4 a = __ldg(rays + 2 * (size_t)i), b = __ldg(rays + 2 * (size_t)i + 1);

@@ -129,7 +129,7 @@ struct PlainTreeT {
     }
     static constexpr int kStack = kReplay ? 16 : 0;
     template <bool kAny, bool kCount>
-    __device__ __forceinline__ bool step(const Ctx&, uint32_t& curr, uint32_t& prev, int& depth, uint2* stack,
+    __device__ __forceinline__ bool step(const Ctx&, uint32_t& curr, uint32_t& prev, int& depth, uint32_t* stack,
                                          HitRecord& hit, f3 ro, f3 rd, f3 inv, Counts& n) const
     {
         if (kReplay)
@@ -161,10 +161,11 @@ struct QuantTree {
                                       &n.visits, &n.tests, &n.ups);
     }
     // the replay walk: the stack-free walk's leaf order with a stack of
-    // kStack pending far children per lane (shared memory) instead of revisits
+    // kStack pending far children per lane (shared memory) instead of revisits;
+    // only any-hit steps are taken (AO rays)
     static constexpr int kStack = 16;
     template <bool kAny, bool kCount>
-    __device__ __forceinline__ bool step(const Ctx& c, uint32_t& curr, uint32_t& prev, int& depth, uint2* stack,
+    __device__ __forceinline__ bool step(const Ctx& c, uint32_t& curr, uint32_t& prev, int& depth, uint32_t* stack,
                                          HitRecord& hit, f3 ro, f3 rd, f3 inv, Counts& n) const
     {
         return quantised_replay_step<kAny, kCount, kStack>(curr, prev, depth, stack, kAoThreads, hit, qnodes, parents,
@@ -246,8 +247,8 @@ __global__ void __launch_bounds__(kAoThreads, 8)  // at most 64 registers: 32 wa
     const uint32_t lanesBelow = (1u << lane) - 1u;
     const unsigned long long total = (unsigned long long)(*queueCount) * (unsigned long long)nSamples;
     const typename Tree::Ctx ctx = tree.context();
-    __shared__ uint2 s_stack[Tree::kStack > 0 ? Tree::kStack : 1][kAoThreads];
-    uint2* const stack = &s_stack[0][threadIdx.x];
+    __shared__ uint32_t s_stack[Tree::kStack > 0 ? Tree::kStack : 1][kAoThreads];  // AO rays are any-hit
+    uint32_t* const stack = &s_stack[0][threadIdx.x];
     unsigned long long poolNext = 0, poolEnd = 0;  // warp-uniform: items taken, not yet handed out
     bool exhausted = false;                        // warp-uniform: the work counter is past the end
     bool live = false;                             // this lane has a ray in flight

@@ -21,7 +21,8 @@ __global__ void __launch_bounds__(kTraceThreads)
     k_trace(const mlbvh_internal_node* __restrict__ nodes, const mlbvh_node_index* __restrict__ rootPtr,
             const float* __restrict__ tris, const float4* __restrict__ rays, float4* __restrict__ hits, uint32_t n)
 {
-    __shared__ uint2 s_stack[kMode == MLBVH_TRAVERSAL_REPLAY ? kReplayDepth : 1][kTraceThreads];
+    __shared__ typename ReplayStack<kAny>::Entry s_stack[kMode == MLBVH_TRAVERSAL_REPLAY ? kReplayDepth : 1]
+                                                        [kTraceThreads];
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const float4 a = __ldg(rays + 2 * (size_t)i), b = __ldg(rays + 2 * (size_t)i + 1);
