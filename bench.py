@@ -425,9 +425,12 @@ def main():
         mb.render_ao(pixels, (w, h), cam, builder.m_rootNode, builder.m_internals, d_tris, 1, wl["ns"], wl["radius"],
                      12345, occluded=occ_plain)
 
+        leaf_tris = mb.leaf_triangles(builder, d_tris)
+
         def replay_frame(occluded=None, stats=None):
             mb.render_ao(pixels, (w, h), cam, builder.m_rootNode, builder.m_internals, d_tris, 1, wl["ns"],
-                         wl["radius"], 12345, occluded=occluded, stats=stats, traversal=mb.TRAVERSAL_REPLAY)
+                         wl["radius"], 12345, occluded=occluded, stats=stats, traversal=mb.TRAVERSAL_REPLAY,
+                         leaf_triangles=leaf_tris)
 
         def quantised_frame(occluded=None, stats=None):
             mb.render_ao_quantised(pixels, (w, h), cam, qtree, 1, wl["ns"], wl["radius"], 12345, occluded=occluded,
@@ -527,9 +530,10 @@ def main():
     for name, (total_s, agree, fst) in forms.items():
         f_rays = int(fst[0])
         node_bytes = (64 * int(fst[1])) if name == "replay" else (32 * int(fst[1]) + 4 * int(fst[5]))
-        tri_bytes = (36 if name == "replay" else 48) * int(fst[2])
+        tri_bytes = 48 * int(fst[2])
         form_lines[name] = {
-            "form": "FP32 nodes, replay walk (stack of pending far children)" if name == "replay"
+            "form": "FP32 nodes, replay walk (stack of pending far children), leaf-ordered 48-byte triangles"
+            if name == "replay"
             else "quantised 8-bit child boxes (32-byte nodes), replay walk",
             "value": f_rays * args.steps * world / total_s / 1e6, "unit": "Mrays/s",
             "ms_per_step": total_s * 1e3 / args.steps, "vs_plain": ao_total_s / total_s,

@@ -322,14 +322,24 @@ MLBVH_API mlbvh_status mlbvh_render_ao(uint32_t* dPixels, uint32_t* dOccluded, i
 
 /* mlbvh_render_ao with the walk of its rays chosen: MLBVH_TRAVERSAL_STACKFREE
  * (what mlbvh_render_ao runs) or MLBVH_TRAVERSAL_REPLAY (the same occlusion
- * counts and pixels from fewer node loads). No reference counterpart. With
+ * counts and pixels from fewer node loads; primary rays too). With REPLAY,
+ * dLeafTriangles (may be NULL) is the tree's triangles in leaf order from
+ * mlbvh_leaf_triangles: 16-byte aligned records read with three vector loads
+ * instead of nine scalar ones, same results. No reference counterpart. With
  * dStats, node visits are those of the chosen walk. */
 MLBVH_API mlbvh_status mlbvh_render_ao_ex(uint32_t* dPixels, uint32_t* dOccluded, int width, int height,
                                           const mlbvh_ray_generator* camera, const mlbvh_node_index* dRootNode,
                                           const mlbvh_internal_node* dInternals, const mlbvh_triangle* dTriangles,
                                           int useSobol, int nSamples, float radius, uint32_t sobolSeed, int traversal,
-                                          unsigned long long* dStats, void* dScratch, size_t scratchBytes,
-                                          void* stream);
+                                          const mlbvh_qtri* dLeafTriangles, unsigned long long* dStats,
+                                          void* dScratch, size_t scratchBytes, void* stream);
+/* The triangles of a built tree in leaf (sorted) order as 48-byte mlbvh_qtri
+ * records (corners and original index), nTriangles of them: leaf j is the
+ * left leaf child of internal node j or the right leaf child of node j - 1.
+ * The same array mlbvh_quantise writes. No reference counterpart. */
+MLBVH_API mlbvh_status mlbvh_leaf_triangles(const mlbvh_internal_node* dInternals, const mlbvh_node_index* dRootNode,
+                                            const mlbvh_triangle* dTriangles, uint32_t nTriangles,
+                                            mlbvh_qtri* dLeafTriangles, void* stream);
 
 /* One progressive path-tracing pass (pt, main_gpu.cu:179-272): reads and
  * updates dAccumulators (float4 per pixel, w = samples so far). maxDepth is

@@ -377,6 +377,83 @@ __device__ __forceinline__ bool stackfree_replay_step(uint32_t& curr, uint32_t& 
     }
 }
 
+// The replay walk over leaf-ordered triangles: mlbvh_qtri records (48 bytes,
+// 16-byte aligned, corners + original index) in sorted leaf order. A leaf
+// child of internal node j is leaf j (left child) or leaf j + 1 (right child),
+// so the walk names a leaf by its position (kLeafBit | position) and reads its
+// triangle with three 16-byte loads; the Hit record reports the original
+// index stored in the record. Same leaves, same order, same Hit records as
+// stackfree_replay_step. After a stack overflow the stack-free walk continues
+// over the original leaf names and the reference triangle array `tris`.
+template <bool kAny, bool kCount, int kDepth>
+__device__ __forceinline__ bool stackfree_replay_step_lo(uint32_t& curr, uint32_t& prev, int& depth,
+                                                         typename ReplayStack<kAny>::Entry* stack, int stride,
+                                                         HitRecord& hit, const mlbvh_internal_node* __restrict__ nodes,
+                                                         const float* __restrict__ tris,
+                                                         const mlbvh_qtri* __restrict__ leafTris, f3 ro, f3 rd,
+                                                         f3 inv, float tmin, uint32_t& nv, uint32_t& nt)
+{
+    if (depth < 0) return stackfree_step<kAny, kCount, true>(curr, prev, hit, nodes, tris, ro, rd, inv, tmin, nv, nt);
+    if (curr & kLeafBit) {
+        if (kCount) ++nt;
+        const float4* t = reinterpret_cast<const float4*>(leafTris + (curr & ~kLeafBit));
+        const float4 a = __ldg(t), b = __ldg(t + 1), c = __ldg(t + 2);
+        float tt, u, v;
+        f3 ng;
+        if (intersect_triangle(tt, u, v, ng, tmin, hit.t, ro, rd, mk(a.x, a.y, a.z), mk(a.w, b.x, b.y),
+                               mk(b.z, b.w, c.x))) {
+            hit.t = tt;
+            hit.u = u;
+            hit.v = v;
+            hit.ng = ng;
+            hit.tri = __float_as_uint(c.y);
+            if (kAny) return true;
+        }
+    } else {
+        if (kCount) ++nv;
+        const NodeView nd = load_node<true>(nodes, curr);
+        const float2 rl = slab(ro, inv, nd.lo0, nd.hi0, tmin, hit.t);
+        const float2 rr = slab(ro, inv, nd.lo1, nd.hi1, tmin, hit.t);
+        const bool hitL = rl.x <= rl.y, hitR = rr.x <= rr.y;
+        const uint32_t e0 = (nd.c0 & kLeafBit) ? (kLeafBit | curr) : nd.c0;
+        const uint32_t e1 = (nd.c1 & kLeafBit) ? (kLeafBit | (curr + 1)) : nd.c1;
+        if (hitL && hitR) {
+            const bool swap = rr.x < rl.x;
+            if (depth == kDepth) {  // full: continue as the stack-free walk, over the original leaf names
+                depth = -1;
+                prev = curr;
+                curr = swap ? nd.c1 : nd.c0;
+                return false;
+            }
+            if constexpr (kAny)
+                stack[depth * stride] = swap ? e0 : e1;
+            else
+                stack[depth * stride] = make_uint2(swap ? e0 : e1, __float_as_uint(swap ? rl.x : rr.x));
+            ++depth;
+            curr = swap ? e1 : e0;
+            return false;
+        }
+        if (hitL || hitR) {
+            curr = hitL ? e0 : e1;
+            return false;
+        }
+    }
+    if constexpr (kAny) {
+        if (depth == 0) return true;
+        curr = stack[--depth * stride];
+        return false;
+    } else {
+        while (depth > 0) {
+            const uint2 e = stack[--depth * stride];
+            if (__uint_as_float(e.y) <= hit.t) {
+                curr = e.x;
+                return false;
+            }
+        }
+        return true;
+    }
+}
+
 template <bool kAny, bool kCount = false, bool kWide = false>
 __device__ __forceinline__ void trace_stackfree(HitRecord& hit, const mlbvh_internal_node* __restrict__ nodes,
                                                 const float* __restrict__ tris, uint32_t root, f3 ro, f3 rd,

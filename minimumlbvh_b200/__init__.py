@@ -22,7 +22,7 @@ __all__ = [
     "TRAVERSAL_STACKFULL", "TRAVERSAL_REPLAY", "OnesweepSort", "BVHGPUBuilder", "RayGenerator", "intersect",
     "render_normal", "render_ao", "render_pt", "pack", "profile_events", "FLT_MAX", "INVALID_NODE",
     "QuantisedBVH", "intersect_quantised", "render_ao_quantised", "pt_diff_render", "pt_diff_adjoint",
-    "BatchParams", "BatchedBVH",
+    "BatchParams", "BatchedBVH", "leaf_triangles",
 ]
 
 BUILD_OPTION_USE_NORMAL = 1   # minimum_lbvh.h:44
@@ -77,7 +77,8 @@ def lib() -> ctypes.CDLL:
                                       _vp]),
             "mlbvh_render_pt": (i32, [_vp, i32, i32, _vp, _vp, _vp, _vp, _vp, i32, i32, i32, _vp]),
             "mlbvh_render_ao_ex": (i32, [_vp, _vp, i32, i32, _vp, _vp, _vp, _vp, i32, i32, f32, u32, i32, _vp, _vp,
-                                         sz, _vp]),
+                                         _vp, sz, _vp]),
+            "mlbvh_leaf_triangles": (i32, [_vp, _vp, _vp, u32, _vp, _vp]),
             "mlbvh_pack": (i32, [_vp, _vp, i32, _vp]),
             "mlbvh_profile_events": (None, [_vp, _vp]),
             "mlbvh_quantise": (i32, [_vp, _vp, _vp, u32, _vp, _vp, _vp, _vp, _vp]),
@@ -293,11 +294,12 @@ def profile_events(start=None, stop=None):
 
 def render_ao(pixels, imageSize, rayGenerator: RayGenerator, rootNode, internals, triangles, useSobol: int = 1,
               nSamples: int = 16, radius: float = 1.0, seed: int = 12345, occluded=None, stats=None,
-              scratch=None, stream=None, traversal: int = TRAVERSAL_STACKFREE):
+              scratch=None, stream=None, traversal: int = TRAVERSAL_STACKFREE, leaf_triangles=None):
     """ao (main_gpu.cu:111-177) with sample count, radius and Sobol seed as
     parameters (the reference fixes 16, 1.0, 12345). ``stats`` (int64 CUDA
     tensor of 8) receives rays traced, node visits and triangle tests.
-    ``traversal`` TRAVERSAL_REPLAY gives the same result from the replay walk."""
+    ``traversal`` TRAVERSAL_REPLAY gives the same result from the replay walk,
+    reading ``leaf_triangles`` (from ``leaf_triangles()``) when given."""
     import torch
     w, h = imageSize
     need = lib().mlbvh_render_scratch_bytes(int(w), int(h))
@@ -317,9 +319,22 @@ def render_ao(pixels, imageSize, rayGenerator: RayGenerator, rootNode, internals
     else:
         _check(lib().mlbvh_render_ao_ex(_ptr(pixels), _ptr(occluded), int(w), int(h), ctypes.addressof(cam),
                                         _ptr(rootNode), _ptr(internals), _ptr(triangles), int(useSobol),
-                                        int(nSamples), float(radius), int(seed), int(traversal), _ptr(stats),
-                                        _ptr(scratch), scratch.numel(), _stream(stream)))
+                                        int(nSamples), float(radius), int(seed), int(traversal),
+                                        _ptr(leaf_triangles), _ptr(stats), _ptr(scratch), scratch.numel(),
+                                        _stream(stream)))
     return pixels
+
+
+def leaf_triangles(builder: "BVHGPUBuilder", triangles, out=None, stream=None):
+    """The built tree's triangles in leaf order as 48-byte records (int32
+    (n, 12): corners, original index, padding), mlbvh_leaf_triangles."""
+    import torch
+    n = builder.m_nTriangles
+    if out is None:
+        out = torch.empty((n, 12), dtype=torch.int32, device=triangles.device)
+    _check(lib().mlbvh_leaf_triangles(_ptr(builder.m_internals), _ptr(builder.m_rootNode), _ptr(triangles), n,
+                                      _ptr(out), _stream(stream)))
+    return out
 
 
 def render_pt(accumulators, imageSize, rayGenerator: RayGenerator, rootNode, internals, triangles,

@@ -110,19 +110,29 @@ mlbvh_status mlbvh_render_ao(uint32_t* dPixels, uint32_t* dOccluded, int width, 
     clear_error();
     if (!camera) return fail(MLBVH_ERR_INVALID_ARG, "null camera");
     return render_ao(dPixels, dOccluded, width, height, *camera, dRootNode, dInternals, dTriangles, useSobol, nSamples,
-                     radius, sobolSeed, dStats, dScratch, scratchBytes, MLBVH_TRAVERSAL_STACKFREE, as_stream(stream));
+                     radius, sobolSeed, dStats, dScratch, scratchBytes, MLBVH_TRAVERSAL_STACKFREE, nullptr,
+                     as_stream(stream));
 }
 
 mlbvh_status mlbvh_render_ao_ex(uint32_t* dPixels, uint32_t* dOccluded, int width, int height,
                                 const mlbvh_ray_generator* camera, const mlbvh_node_index* dRootNode,
                                 const mlbvh_internal_node* dInternals, const mlbvh_triangle* dTriangles, int useSobol,
                                 int nSamples, float radius, uint32_t sobolSeed, int traversal,
-                                unsigned long long* dStats, void* dScratch, size_t scratchBytes, void* stream)
+                                const mlbvh_qtri* dLeafTriangles, unsigned long long* dStats, void* dScratch,
+                                size_t scratchBytes, void* stream)
 {
     clear_error();
     if (!camera) return fail(MLBVH_ERR_INVALID_ARG, "null camera");
     return render_ao(dPixels, dOccluded, width, height, *camera, dRootNode, dInternals, dTriangles, useSobol, nSamples,
-                     radius, sobolSeed, dStats, dScratch, scratchBytes, traversal, as_stream(stream));
+                     radius, sobolSeed, dStats, dScratch, scratchBytes, traversal, dLeafTriangles, as_stream(stream));
+}
+
+mlbvh_status mlbvh_leaf_triangles(const mlbvh_internal_node* dInternals, const mlbvh_node_index* dRootNode,
+                                  const mlbvh_triangle* dTriangles, uint32_t nTriangles, mlbvh_qtri* dLeafTriangles,
+                                  void* stream)
+{
+    clear_error();
+    return leaf_triangles(dInternals, dRootNode, dTriangles, nTriangles, dLeafTriangles, as_stream(stream));
 }
 
 mlbvh_status mlbvh_render_pt(float* dAccumulators, int width, int height, const mlbvh_ray_generator* camera,

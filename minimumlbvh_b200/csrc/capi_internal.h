@@ -49,7 +49,10 @@ mlbvh_status render_normal(uint32_t* dPixels, int w, int h, const mlbvh_ray_gene
 mlbvh_status render_ao(uint32_t* dPixels, uint32_t* dOccluded, int w, int h, const mlbvh_ray_generator& cam,
                        const mlbvh_node_index* dRoot, const mlbvh_internal_node* dNodes, const mlbvh_triangle* dTris,
                        int useSobol, int nSamples, float radius, uint32_t seed, unsigned long long* dStats,
-                       void* dScratch, size_t scratchBytes, int traversal, cudaStream_t stream);
+                       void* dScratch, size_t scratchBytes, int traversal, const mlbvh_qtri* dLeafTris,
+                       cudaStream_t stream);
+mlbvh_status leaf_triangles(const mlbvh_internal_node* dNodes, const mlbvh_node_index* dRoot,
+                            const mlbvh_triangle* dTris, uint32_t n, mlbvh_qtri* dLeafTris, cudaStream_t stream);
 mlbvh_status render_ao_quantised(uint32_t* dPixels, uint32_t* dOccluded, int w, int h, const mlbvh_ray_generator& cam,
                                  const mlbvh_qnode* dQNodes, const uint32_t* dQParents, const mlbvh_qtri* dQTris,
                                  const mlbvh_qheader* dQHeader, int useSobol, int nSamples, float radius,

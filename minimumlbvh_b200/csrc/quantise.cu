@@ -128,6 +128,23 @@ __global__ void __launch_bounds__(kQuantiseThreads)
     parents[i] = nd.parent;
 }
 
+// Leaf-ordered triangles alone (the qtris of k_quantise): one thread per
+// internal node j writes its leaf children, leaf j (left) and j + 1 (right).
+__global__ void __launch_bounds__(kQuantiseThreads)
+    k_leaf_tris(const mlbvh_internal_node* __restrict__ nodes, const mlbvh_node_index* __restrict__ rootPtr,
+                const float* __restrict__ tris, uint32_t n, mlbvh_qtri* __restrict__ leafTris)
+{
+    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n == 1) {
+        if (j == 0) write_qtri(leafTris, 0, tris, __ldg(rootPtr) & ~kLeafBit);
+        return;
+    }
+    if (j + 1 >= n) return;
+    const uint32_t c0 = __ldg(&nodes[j].children[0]), c1 = __ldg(&nodes[j].children[1]);
+    if (c0 & kLeafBit) write_qtri(leafTris, j, tris, c0 & ~kLeafBit);
+    if (c1 & kLeafBit) write_qtri(leafTris, j + 1, tris, c1 & ~kLeafBit);
+}
+
 // One thread per ray. kDepth = 0: the stack-free walk (trace_quantised);
 // otherwise the replay walk with a kDepth-entry stack per thread in shared
 // memory (quantised_replay_step), which returns the same Hit records.
@@ -216,6 +233,20 @@ mlbvh_status quantise(const mlbvh_internal_node* dNodes, const mlbvh_node_index*
     k_quantise<<<(threads + kQuantiseThreads - 1) / kQuantiseThreads, kQuantiseThreads, 0, stream>>>(
         dNodes, dRoot, reinterpret_cast<const float*>(dTris), n, dQNodes, dQParents, dQTris, dQHeader);
     MLBVH_CHECK_LAUNCH("k_quantise");
+    return MLBVH_OK;
+}
+
+mlbvh_status leaf_triangles(const mlbvh_internal_node* dNodes, const mlbvh_node_index* dRoot,
+                            const mlbvh_triangle* dTris, uint32_t n, mlbvh_qtri* dLeafTris, cudaStream_t stream)
+{
+    if (n == 0 || n >= (1u << 31)) return fail(MLBVH_ERR_INVALID_ARG, "nTriangles must be in [1, 2^31)");
+    if (!dRoot || !dTris || !dLeafTris || (n > 1 && !dNodes)) return fail(MLBVH_ERR_INVALID_ARG, "null pointer");
+    if (!aligned16(dNodes) || !aligned16(dRoot) || !aligned16(dTris) || !aligned16(dLeafTris))
+        return fail(MLBVH_ERR_INVALID_ARG, "device pointers must be 16-byte aligned");
+    const uint32_t threads = n > 1 ? n - 1 : 1;
+    k_leaf_tris<<<(threads + kQuantiseThreads - 1) / kQuantiseThreads, kQuantiseThreads, 0, stream>>>(
+        dNodes, dRoot, reinterpret_cast<const float*>(dTris), n, dLeafTris);
+    MLBVH_CHECK_LAUNCH("k_leaf_tris");
     return MLBVH_OK;
 }
 

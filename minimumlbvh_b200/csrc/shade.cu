@@ -110,37 +110,69 @@ __device__ __forceinline__ void add_stats(unsigned long long* stats, const Count
 }
 
 // The tree formats and walks the AO kernels run over: the reference node
-// layout with the stack-free walk (kReplay false) or the replay walk (kReplay
-// true: the same Hit records from a stack of pending far children), and the
-// quantised tree with the replay walk.
-template <bool kReplay>
+// layout with the stack-free walk (kWalk 0), the replay walk (kWalk 1: the
+// same Hit records from a stack of pending far children), or the replay walk
+// over leaf-ordered 48-byte triangles (kWalk 2); and the quantised tree with
+// the replay walk. Primary rays of the replay forms take the closest-hit
+// replay walk (pstack: 16 entries per thread in shared memory).
+constexpr int kReplayDepth = 16;
+template <int kWalk>
 struct PlainTreeT {
     const mlbvh_internal_node* nodes;
     const float* tris;
     const mlbvh_node_index* rootPtr;
+    const mlbvh_qtri* leafTris;  // kWalk 2 only
     struct Ctx {
-        uint32_t root;
+        uint32_t root;  // kWalk 2: a leaf root is named by its position, 0
     };
-    __device__ __forceinline__ Ctx context() const { return Ctx{__ldg(rootPtr)}; }
-    template <bool kAny, bool kCount>
-    __device__ __forceinline__ void trace(const Ctx& c, HitRecord& hit, f3 ro, f3 rd, Counts& n) const
+    __device__ __forceinline__ Ctx context() const
     {
-        trace_stackfree<kAny, kCount, true>(hit, nodes, tris, c.root, ro, rd, inv_rd(rd), 0.0f, &n.visits, &n.tests);
+        const uint32_t r = __ldg(rootPtr);
+        return Ctx{(kWalk == 2 && (r & kLeafBit)) ? kLeafBit : r};
     }
-    static constexpr int kStack = kReplay ? 16 : 0;
+    static constexpr int kStack = kWalk > 0 ? kReplayDepth : 0;
+    template <bool kAny, bool kCount, class Entry>
+    __device__ __forceinline__ bool walk(uint32_t& curr, uint32_t& prev, int& depth, Entry* stack, int stride,
+                                         HitRecord& hit, f3 ro, f3 rd, f3 inv, Counts& n) const
+    {
+        if constexpr (kWalk == 2)
+            return stackfree_replay_step_lo<kAny, kCount, kReplayDepth>(curr, prev, depth, stack, stride, hit, nodes,
+                                                                        tris, leafTris, ro, rd, inv, 0.0f, n.visits,
+                                                                        n.tests);
+        else if constexpr (kWalk == 1)
+            return stackfree_replay_step<kAny, kCount, kReplayDepth>(curr, prev, depth, stack, stride, hit, nodes, tris,
+                                                                     ro, rd, inv, 0.0f, n.visits, n.tests);
+        else
+            return stackfree_step<kAny, kCount, true>(curr, prev, hit, nodes, tris, ro, rd, inv, 0.0f, n.visits,
+                                                      n.tests);
+    }
+    template <bool kAny, bool kCount>
+    __device__ __forceinline__ void trace(const Ctx& c, HitRecord& hit, f3 ro, f3 rd, Counts& n, uint2* pstack,
+                                          int stride) const
+    {
+        if constexpr (kWalk == 0) {
+            trace_stackfree<kAny, kCount, true>(hit, nodes, tris, c.root, ro, rd, inv_rd(rd), 0.0f, &n.visits,
+                                                &n.tests);
+        } else {
+            static_assert(!kAny, "primary rays are closest-hit");
+            const f3 inv = inv_rd(rd);
+            uint32_t curr = c.root, prev = kInvalid;
+            int depth = 0;
+            for (uint32_t steps = 1; steps < kMaxTraversalSteps; ++steps)
+                if (walk<false, kCount>(curr, prev, depth, pstack, stride, hit, ro, rd, inv, n)) break;
+        }
+    }
     template <bool kAny, bool kCount>
     __device__ __forceinline__ bool step(const Ctx&, uint32_t& curr, uint32_t& prev, int& depth, uint32_t* stack,
                                          HitRecord& hit, f3 ro, f3 rd, f3 inv, Counts& n) const
     {
-        if (kReplay)
-            return stackfree_replay_step<kAny, kCount, kReplay ? 16 : 1>(curr, prev, depth, stack, kAoThreads, hit,
-                                                                         nodes, tris, ro, rd, inv, 0.0f, n.visits,
-                                                                         n.tests);
-        return stackfree_step<kAny, kCount, true>(curr, prev, hit, nodes, tris, ro, rd, inv, 0.0f, n.visits, n.tests);
+        static_assert(kWalk == 0 || kAny, "AO rays are any-hit");
+        return walk<kAny, kCount>(curr, prev, depth, stack, kAoThreads, hit, ro, rd, inv, n);
     }
 };
-using PlainTree = PlainTreeT<false>;
-using PlainReplayTree = PlainTreeT<true>;
+using PlainTree = PlainTreeT<0>;
+using PlainReplayTree = PlainTreeT<1>;
+using PlainReplayLeafTree = PlainTreeT<2>;
 struct QuantTree {
     const mlbvh_qnode* qnodes;
     const uint32_t* parents;
@@ -155,10 +187,18 @@ struct QuantTree {
         return Ctx{__ldg(&header->root), __ldg(&header->eBase)};
     }
     template <bool kAny, bool kCount>
-    __device__ __forceinline__ void trace(const Ctx& c, HitRecord& hit, f3 ro, f3 rd, Counts& n) const
+    __device__ __forceinline__ void trace(const Ctx& c, HitRecord& hit, f3 ro, f3 rd, Counts& n, uint2* pstack,
+                                          int stride) const
     {
-        trace_quantised<kAny, kCount, true>(hit, qnodes, parents, qtris, c.root, c.eBase, ro, rd, inv_rd(rd), 0.0f,
-                                      &n.visits, &n.tests, &n.ups);
+        static_assert(!kAny, "primary rays are closest-hit");
+        const f3 inv = inv_rd(rd);
+        uint32_t curr = c.root, prev = kInvalid;
+        int depth = 0;
+        for (uint32_t steps = 1; steps < kMaxTraversalSteps; ++steps)
+            if (quantised_replay_step<false, kCount, kStack>(curr, prev, depth, pstack, stride, hit, qnodes, parents,
+                                                            qtris, c.eBase, ro, rd, inv, 0.0f, n.visits, n.tests,
+                                                            n.ups))
+                break;
     }
     // the replay walk: the stack-free walk's leaf order with a stack of
     // kStack pending far children per lane (shared memory) instead of revisits;
@@ -181,6 +221,7 @@ __global__ void __launch_bounds__(kTileW* kTileH)
     k_ao_primary(mlbvh_ray_generator gen, int w, int h, Tree tree, AoRecord* __restrict__ records,
                  uint32_t* __restrict__ queueCount, uint32_t* __restrict__ counts, unsigned long long* __restrict__ stats)
 {
+    __shared__ uint2 s_pstack[Tree::kStack > 0 ? Tree::kStack : 1][kTileW * kTileH];
     Counts cnt;
     int xi, yi;
     const bool inside = tile_pixel(w, h, xi, yi);
@@ -194,7 +235,8 @@ __global__ void __launch_bounds__(kTileW* kTileH)
         HitRecord hit;
         hit.t = kFltMax;
         hit.tri = 0xFFFFFFFFu;
-        tree.template trace<false, kCount>(tree.context(), hit, ro, rd, cnt);
+        tree.template trace<false, kCount>(tree.context(), hit, ro, rd, cnt, &s_pstack[0][threadIdx.x],
+                                           kTileW * kTileH);
         if (hit.t == kFltMax) {
             counts[pixel] = 0xFFFFFFFFu;
         } else {
@@ -571,20 +613,27 @@ mlbvh_status render_normal(uint32_t* dPixels, int w, int h, const mlbvh_ray_gene
 mlbvh_status render_ao(uint32_t* dPixels, uint32_t* dOccluded, int w, int h, const mlbvh_ray_generator& cam,
                        const mlbvh_node_index* dRoot, const mlbvh_internal_node* dNodes, const mlbvh_triangle* dTris,
                        int useSobol, int nSamples, float radius, uint32_t seed, unsigned long long* dStats,
-                       void* dScratch, size_t scratchBytes, int traversal, cudaStream_t stream)
+                       void* dScratch, size_t scratchBytes, int traversal, const mlbvh_qtri* dLeafTris,
+                       cudaStream_t stream)
 {
     if (mlbvh_status s = check_ao_args(w, h, nSamples, dPixels, dOccluded, dScratch, dStats)) return s;
     if (!dRoot || !dTris) return fail(MLBVH_ERR_INVALID_ARG, "null pointer");
     if (!aligned16(dRoot) || !aligned32(dNodes) || !aligned16(dTris))
         return fail(MLBVH_ERR_INVALID_ARG, "device pointers must be 16-byte aligned");
+    if (!aligned16(dLeafTris)) return fail(MLBVH_ERR_INVALID_ARG, "device pointers must be 16-byte aligned");
+    if (traversal == MLBVH_TRAVERSAL_REPLAY && dLeafTris) {
+        const PlainReplayLeafTree tree{dNodes, reinterpret_cast<const float*>(dTris), dRoot, dLeafTris};
+        return launch_ao(dPixels, dOccluded, w, h, cam, tree, useSobol, nSamples, radius, seed, dStats, dScratch,
+                         scratchBytes, stream);
+    }
     if (traversal == MLBVH_TRAVERSAL_REPLAY) {
-        const PlainReplayTree tree{dNodes, reinterpret_cast<const float*>(dTris), dRoot};
+        const PlainReplayTree tree{dNodes, reinterpret_cast<const float*>(dTris), dRoot, nullptr};
         return launch_ao(dPixels, dOccluded, w, h, cam, tree, useSobol, nSamples, radius, seed, dStats, dScratch,
                          scratchBytes, stream);
     }
     if (traversal != MLBVH_TRAVERSAL_STACKFREE)
         return fail(MLBVH_ERR_INVALID_ARG, "AO traversal must be MLBVH_TRAVERSAL_STACKFREE or MLBVH_TRAVERSAL_REPLAY");
-    const PlainTree tree{dNodes, reinterpret_cast<const float*>(dTris), dRoot};
+    const PlainTree tree{dNodes, reinterpret_cast<const float*>(dTris), dRoot, nullptr};
     return launch_ao(dPixels, dOccluded, w, h, cam, tree, useSobol, nSamples, radius, seed, dStats, dScratch,
                      scratchBytes, stream);
 }

@@ -26,9 +26,11 @@ def quantise_both(tris):
 @pytest.mark.parametrize("n", [1, 2, 3, 257, 4097, 100000])
 def test_quantise_matches_oracle(cuda, n):
     tris = scenes.gaussian_soup(n, clusters=4, seed=300 + n)
-    _, _, out, _, gq, ref = quantise_both(tris)
+    b, t, out, _, gq, ref = quantise_both(tris)
     for k in ("qnodes", "parents", "qtris", "header"):
         np.testing.assert_array_equal(gq[k], ref[k], err_msg=k)
+    # mlbvh_leaf_triangles writes the same leaf-ordered triangles
+    np.testing.assert_array_equal(G.host(mb.leaf_triangles(b, t), np.uint32), ref["qtris"])
     if n > 1:
         assert O.oracle().orc_check_quantised(O.P(out["nodes"]), n, O.P(gq["qnodes"]), O.P(gq["header"])) == 1
 

@@ -21,13 +21,13 @@ def channels(p):
     return np.stack([(p >> s) & 255 for s in (0, 8, 16, 24)], -1).astype(np.int32)
 
 
-def gpu_ao(b, t, cam, w, h, ns, radius, seed=12345, sobol=1, traversal=mb.TRAVERSAL_STACKFREE):
+def gpu_ao(b, t, cam, w, h, ns, radius, seed=12345, sobol=1, traversal=mb.TRAVERSAL_STACKFREE, leaf_tris=None):
     import torch
     px = torch.zeros(w * h, dtype=torch.int32, device="cuda")
     occ = torch.zeros(w * h, dtype=torch.int32, device="cuda")
     stats = torch.zeros(8, dtype=torch.int64, device="cuda")
     mb.render_ao(px, (w, h), mb.RayGenerator.from_array(cam), b.m_rootNode, b.m_internals, t, sobol, ns, radius,
-                 seed, occluded=occ, stats=stats, traversal=traversal)
+                 seed, occluded=occ, stats=stats, traversal=traversal, leaf_triangles=leaf_tris)
     torch.cuda.synchronize()
     st = G.host(stats)
     return G.host(px, np.uint32), G.host(occ, np.uint32), (int(st[0]), int(st[1]), int(st[2]))
@@ -83,6 +83,12 @@ def test_ao_replay_walk_equals_stackfree(cuda, sobol):
     np.testing.assert_array_equal(px1, px0)
     assert st1[0] == st0[0] and st1[2] == st0[2]  # rays and triangle tests: the same leaves
     assert st1[1] < st0[1]
+    # the same walk over leaf-ordered 48-byte triangles
+    lt = mb.leaf_triangles(b, t)
+    px2, occ2, st2 = gpu_ao(b, t, cam, 512, 512, 16, 0.25, sobol=sobol, traversal=mb.TRAVERSAL_REPLAY, leaf_tris=lt)
+    np.testing.assert_array_equal(occ2, occ0)
+    np.testing.assert_array_equal(px2, px0)
+    assert st2 == st1
 
 
 def test_ao_soup_config_rows(cuda):
@@ -94,7 +100,8 @@ def test_ao_soup_config_rows(cuda):
     w, h = 1920, 1080
     cam = O.lookat(eye, c, up, fovy, w, h)
     px, occ, _ = gpu_ao(b, t, cam, w, h, 64, 0.1)
-    _, occ_replay, _ = gpu_ao(b, t, cam, w, h, 64, 0.1, traversal=mb.TRAVERSAL_REPLAY)
+    _, occ_replay, _ = gpu_ao(b, t, cam, w, h, 64, 0.1, traversal=mb.TRAVERSAL_REPLAY,
+                              leaf_tris=mb.leaf_triangles(b, t))
     np.testing.assert_array_equal(occ_replay, occ)
     for r0 in (300, 540, 700):
         rpx, rocc = O.render_ao(cam, out["root"], out["nodes"], tris, w, h, 64, 0.1, 12345, 1, trig=1,
