@@ -828,6 +828,21 @@ __device__ __forceinline__ QNodeView load_qnode(const mlbvh_qnode* __restrict__ 
     return n;
 }
 
+// The reference's own test of a leaf: its slabs (minimum_lbvh.h:82-96) on the
+// triangle's FP32 box, as its parent node stores it. A quantised walk reaches
+// every leaf the FP32 walk reaches and a few more (its boxes are larger); a
+// hit it finds counts only if the triangle's exact box passes, which makes the
+// hits it can find those of the FP32 walk: for FP32 boxes the slab test is
+// monotone, so a leaf box that passes implies every ancestor box passes too.
+// A miss needs no check, so the check runs on hits only.
+__device__ __forceinline__ bool leaf_box_passes(f3 ro, f3 inv, f3 v0, f3 v1, f3 v2, float tmin, float hitT)
+{
+    const f3 lo = smin3(smin3(smin3(mk(kFltMax, kFltMax, kFltMax), v0), v1), v2);
+    const f3 hi = smax3(smax3(smax3(mk(-kFltMax, -kFltMax, -kFltMax), v0), v1), v2);
+    const float2 t = slab(ro, inv, lo, hi, tmin, hitT);
+    return t.x <= t.y;
+}
+
 // Stack-free walk over the quantised tree: the state machine of
 // intersect_stackfree (minimum_lbvh.h:981-1061), with "came from the parent"
 // recognised as "came from neither child" so that the parent word is read
@@ -845,10 +860,11 @@ __device__ __forceinline__ bool quantised_step(uint32_t& curr, uint32_t& prev, H
         if (kCount) ++nt;
         const float4* t = reinterpret_cast<const float4*>(qtris + (curr & kQIndexMask));
         const float4 a = __ldg(t), b = __ldg(t + 1), c = __ldg(t + 2);
+        const f3 v0 = mk(a.x, a.y, a.z), v1 = mk(a.w, b.x, b.y), v2 = mk(b.z, b.w, c.x);
         float tt, u, v;
         f3 ng;
-        if (intersect_triangle(tt, u, v, ng, tmin, hit.t, ro, rd, mk(a.x, a.y, a.z), mk(a.w, b.x, b.y),
-                               mk(b.z, b.w, c.x))) {
+        if (intersect_triangle(tt, u, v, ng, tmin, hit.t, ro, rd, v0, v1, v2) &&
+            leaf_box_passes(ro, inv, v0, v1, v2, tmin, hit.t)) {
             hit.t = tt;
             hit.u = u;
             hit.v = v;
@@ -931,10 +947,11 @@ __device__ __forceinline__ bool quantised_replay_step(uint32_t& curr, uint32_t& 
         if (kCount) ++nt;
         const float4* t = reinterpret_cast<const float4*>(qtris + (curr & kQIndexMask));
         const float4 a = __ldg(t), b = __ldg(t + 1), c = __ldg(t + 2);
+        const f3 v0 = mk(a.x, a.y, a.z), v1 = mk(a.w, b.x, b.y), v2 = mk(b.z, b.w, c.x);
         float tt, u, v;
         f3 ng;
-        if (intersect_triangle(tt, u, v, ng, tmin, hit.t, ro, rd, mk(a.x, a.y, a.z), mk(a.w, b.x, b.y),
-                               mk(b.z, b.w, c.x))) {
+        if (intersect_triangle(tt, u, v, ng, tmin, hit.t, ro, rd, v0, v1, v2) &&
+            leaf_box_passes(ro, inv, v0, v1, v2, tmin, hit.t)) {
             hit.t = tt;
             hit.u = u;
             hit.v = v;

@@ -1425,6 +1425,19 @@ typedef struct {
     int stackDepth; /* 0: stack-free walk; 1..64: replay walk with that many stack entries */
 } qtrace_ctx;
 
+/* leaf_box_passes (include/mlbvh_device.cuh): on a hit in a quantised walk,
+ * the reference's slabs on the triangle's FP32 box must pass as well. */
+static int leaf_box_passes(orc_f3 ro, orc_f3 inv, const orc_f3* v, float tmin, float hitT)
+{
+    orc_aabb b;
+    aabb_set_empty(&b);
+    for (int j = 0; j < 3; ++j) aabb_extend_p(&b, v[j]);
+    float e, x;
+    slabs(ro, inv, &b, hitT, &e, &x);
+    e = smax(e, tmin);
+    return e <= x;
+}
+
 /* trace_quantised (include/mlbvh_device.cuh): the stack-free state machine
  * over quantised nodes; "came from the parent" is "came from neither child",
  * and the parent word is read only when moving up. */
@@ -1441,7 +1454,8 @@ static void qtrace_walk(const qtrace_ctx* c, orc_hit* hit, orc_f3 ro, orc_f3 rd,
             memcpy(v, q, 36);
             float t, u, vv;
             orc_f3 ng;
-            if (intersect_tri(&t, &u, &vv, &ng, tmin, hit->t, ro, rd, v[0], v[1], v[2]))
+            if (intersect_tri(&t, &u, &vv, &ng, tmin, hit->t, ro, rd, v[0], v[1], v[2]) &&
+                leaf_box_passes(ro, inv, v, tmin, hit->t))
             {
                 hit->t = t;
                 hit->u = u;
@@ -1524,7 +1538,8 @@ static void qreplay_one(const qtrace_ctx* c, int depth, orc_hit* hit, orc_f3 ro,
             memcpy(v, q, 36);
             float t, u, vv;
             orc_f3 ng;
-            if (intersect_tri(&t, &u, &vv, &ng, tmin, hit->t, ro, rd, v[0], v[1], v[2]))
+            if (intersect_tri(&t, &u, &vv, &ng, tmin, hit->t, ro, rd, v[0], v[1], v[2]) &&
+                leaf_box_passes(ro, inv, v, tmin, hit->t))
             {
                 hit->t = t;
                 hit->u = u;
