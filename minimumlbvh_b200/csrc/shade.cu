@@ -25,7 +25,7 @@ struct AoRecord {
     float ox, oy, oz;
     float nx, ny, nz;
     uint32_t pixel;
-    uint32_t pad;
+    uint32_t pad;  // replay forms: the node AO rays of this pixel start from (ball_start)
 };
 
 struct RenderLayout {
@@ -109,6 +109,25 @@ __device__ __forceinline__ void add_stats(unsigned long long* stats, const Count
     }
 }
 
+// The cube around an AO origin that holds every point an AO ray of length
+// radius can reach (directions are unit vectors), widened by 0.1% of the
+// radius plus 1e-6 of the coordinates' magnitude and rounded outward, so
+// that it also holds the hit points the triangle test can report.
+struct AoBall {
+    f3 lo, hi;
+};
+__device__ __forceinline__ AoBall ao_ball(f3 o, float radius)
+{
+    const float mag = __fadd_ru(__fadd_ru(fabsf(o.x), fabsf(o.y)), __fadd_ru(fabsf(o.z), radius));
+    const float r = __fadd_ru(__fmul_ru(radius, 1.001f), __fmul_ru(mag, 1e-6f));
+    return AoBall{mk(__fsub_rd(o.x, r), __fsub_rd(o.y, r), __fsub_rd(o.z, r)),
+                  mk(__fadd_ru(o.x, r), __fadd_ru(o.y, r), __fadd_ru(o.z, r))};
+}
+__device__ __forceinline__ bool box_meets(f3 lo, f3 hi, const AoBall& b)
+{
+    return lo.x <= b.hi.x && lo.y <= b.hi.y && lo.z <= b.hi.z && hi.x >= b.lo.x && hi.y >= b.lo.y && hi.z >= b.lo.z;
+}
+
 // The tree formats and walks the AO kernels run over: the reference node
 // layout with the stack-free walk (kWalk 0), the replay walk (kWalk 1: the
 // same Hit records from a stack of pending far children), or the replay walk
@@ -131,6 +150,24 @@ struct PlainTreeT {
         return Ctx{(kWalk == 2 && (r & kLeafBit)) ? kLeafBit : r};
     }
     static constexpr int kStack = kWalk > 0 ? kReplayDepth : 0;
+    // Replay forms: the node where AO rays from the ball's centre start. From
+    // the root, while exactly one child's box meets the ball, go down into it;
+    // stop where both do (or at a leaf). Every leaf an AO ray of the pixel can
+    // hit lies below that node; kInvalid: no box meets the ball, nothing can be
+    // hit. Leaves are named as the walk names them.
+    __device__ __forceinline__ uint32_t ball_start(const Ctx& c, const AoBall& b) const
+    {
+        uint32_t curr = c.root;
+        for (uint32_t steps = 0; !(curr & kLeafBit) && steps < kMaxTraversalSteps; ++steps) {
+            const NodeView nd = load_node<true>(nodes, curr);
+            const bool m0 = box_meets(nd.lo0, nd.hi0, b), m1 = box_meets(nd.lo1, nd.hi1, b);
+            if (m0 && m1) return curr;
+            if (!m0 && !m1) return kInvalid;
+            const uint32_t child = m0 ? nd.c0 : nd.c1;
+            curr = (kWalk == 2 && (child & kLeafBit)) ? (kLeafBit | (curr + (m0 ? 0u : 1u))) : child;
+        }
+        return curr;
+    }
     template <bool kAny, bool kCount, class Entry>
     __device__ __forceinline__ bool walk(uint32_t& curr, uint32_t& prev, int& depth, Entry* stack, int stride,
                                          HitRecord& hit, f3 ro, f3 rd, f3 inv, Counts& n) const
@@ -204,6 +241,18 @@ struct QuantTree {
     // kStack pending far children per lane (shared memory) instead of revisits;
     // only any-hit steps are taken (AO rays)
     static constexpr int kStack = 16;
+    __device__ __forceinline__ uint32_t ball_start(const Ctx& c, const AoBall& b) const
+    {
+        uint32_t curr = c.root;
+        for (uint32_t steps = 0; !(curr & kLeafBit) && steps < kMaxTraversalSteps; ++steps) {
+            const QNodeView nd = load_qnode<true>(qnodes, curr, c.eBase);
+            const bool m0 = box_meets(nd.box.lo0, nd.box.hi0, b), m1 = box_meets(nd.box.lo1, nd.box.hi1, b);
+            if (m0 && m1) return curr;
+            if (!m0 && !m1) return kInvalid;
+            curr = m0 ? nd.c0 : nd.c1;
+        }
+        return curr;
+    }
     template <bool kAny, bool kCount>
     __device__ __forceinline__ bool step(const Ctx& c, uint32_t& curr, uint32_t& prev, int& depth, uint32_t* stack,
                                          HitRecord& hit, f3 ro, f3 rd, f3 inv, Counts& n) const
@@ -218,7 +267,7 @@ struct QuantTree {
 // towards the viewer, AO origin p + n * 1e-3.
 template <class Tree, bool kCount>
 __global__ void __launch_bounds__(kTileW* kTileH)
-    k_ao_primary(mlbvh_ray_generator gen, int w, int h, Tree tree, AoRecord* __restrict__ records,
+    k_ao_primary(mlbvh_ray_generator gen, int w, int h, float radius, Tree tree, AoRecord* __restrict__ records,
                  uint32_t* __restrict__ queueCount, uint32_t* __restrict__ counts, unsigned long long* __restrict__ stats)
 {
     __shared__ uint2 s_pstack[Tree::kStack > 0 ? Tree::kStack : 1][kTileW * kTileH];
@@ -243,7 +292,9 @@ __global__ void __launch_bounds__(kTileW* kTileH)
             f3 n = normalize(hit.ng);
             if (0.0f < dot(n, rd)) n = -n;
             const f3 o = ro + rd * hit.t + n * 0.001f;
-            rec = AoRecord{o.x, o.y, o.z, n.x, n.y, n.z, (uint32_t)pixel, 0u};
+            uint32_t start = 0u;
+            if constexpr (Tree::kStack > 0) start = tree.ball_start(tree.context(), ao_ball(o, radius));
+            rec = AoRecord{o.x, o.y, o.z, n.x, n.y, n.z, (uint32_t)pixel, start};
             counts[pixel] = 0u;
             isHit = true;
         }
@@ -259,7 +310,7 @@ __global__ void __launch_bounds__(kTileW* kTileH)
     if (isHit) {
         float4* dst = reinterpret_cast<float4*>(records + base + __popc(mask & ((1u << lane) - 1u)));
         dst[0] = make_float4(rec.ox, rec.oy, rec.oz, rec.nx);
-        dst[1] = make_float4(rec.ny, rec.nz, __uint_as_float(rec.pixel), 0.0f);
+        dst[1] = make_float4(rec.ny, rec.nz, __uint_as_float(rec.pixel), __uint_as_float(rec.pad));
     }
 }
 
@@ -325,6 +376,7 @@ __global__ void __launch_bounds__(kAoThreads, 8)  // at most 64 registers: 32 wa
                     origin = mk(r0.x, r0.y, r0.z);
                     const f3 n = mk(r0.w, r1.x, r1.y);
                     pixel = __float_as_uint(r1.z);
+                    const uint32_t start = Tree::kStack > 0 ? __float_as_uint(r1.w) : ctx.root;
                     f3 xaxis, zaxis;
                     onb(n, xaxis, zaxis);
                     float2 rnd;
@@ -341,11 +393,11 @@ __global__ void __launch_bounds__(kAoThreads, 8)  // at most 64 registers: 32 wa
                     inv = inv_rd(dir);
                     hit.t = radius;
                     hit.tri = 0xFFFFFFFFu;
-                    curr = ctx.root;
+                    curr = start;
                     prev = kInvalid;
                     depth = 0;
                     steps = 0;
-                    live = true;
+                    live = start != kInvalid;  // kInvalid: no box within the AO radius, the ray misses
                 }
                 poolNext += min((unsigned long long)__popc(idle), avail);
             }
@@ -554,9 +606,10 @@ mlbvh_status launch_ao(uint32_t* dPixels, uint32_t* dOccluded, int w, int h, con
     if (e != cudaSuccess) return fail(MLBVH_ERR_CUDA, cudaGetErrorString(e));
     const dim3 grid = tile_grid(w, h);
     if (dStats)
-        k_ao_primary<Tree, true><<<grid, kTileW * kTileH, 0, stream>>>(cam, w, h, tree, records, header, counts, dStats);
+        k_ao_primary<Tree, true><<<grid, kTileW * kTileH, 0, stream>>>(cam, w, h, radius, tree, records, header, counts,
+                                                                       dStats);
     else
-        k_ao_primary<Tree, false><<<grid, kTileW * kTileH, 0, stream>>>(cam, w, h, tree, records, header, counts,
+        k_ao_primary<Tree, false><<<grid, kTileW * kTileH, 0, stream>>>(cam, w, h, radius, tree, records, header, counts,
                                                                         nullptr);
     MLBVH_CHECK_LAUNCH("k_ao_primary");
     ProfileEvents ev = take_profile_events();
