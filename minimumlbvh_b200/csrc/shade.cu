@@ -328,6 +328,7 @@ __global__ void __launch_bounds__(kTileW* kTileH)
 // count; the lanes of a warp add per pixel with one atomic.
 constexpr int kChunk = 64;
 constexpr int kStartBatch = 8;
+constexpr int kStepsPerRound = 3;
 
 template <class Tree, bool kCount>
 __global__ void __launch_bounds__(kAoThreads, 8)  // at most 64 registers: 32 warps per SM
@@ -406,14 +407,18 @@ __global__ void __launch_bounds__(kAoThreads, 8)  // at most 64 registers: 32 wa
             if (exhausted) break;
             continue;
         }
+        // up to kStepsPerRound steps per loop iteration: the refill and vote
+        // overhead of an iteration is shared by several steps
         bool occluded = false;
-        if (live) {
-            if (tree.template step<true, kCount>(ctx, curr, prev, depth, stack, hit, origin, dir, inv, cnt) ||
-                ++steps >= kMaxTraversalSteps) {
-                live = false;
-                occluded = hit.t != radius;
+#pragma unroll
+        for (int rep = 0; rep < kStepsPerRound; ++rep)
+            if (live) {
+                if (tree.template step<true, kCount>(ctx, curr, prev, depth, stack, hit, origin, dir, inv, cnt) ||
+                    ++steps >= kMaxTraversalSteps) {
+                    live = false;
+                    occluded = hit.t != radius;
+                }
             }
-        }
         // one atomic per pixel among the lanes whose ray just ended occluded
         uint32_t pending = __ballot_sync(0xffffffffu, occluded);
         while (pending) {
