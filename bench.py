@@ -346,24 +346,12 @@ def main():
     import torch
     import minimumlbvh_b200 as mb
 
+    from minimumlbvh_b200.replicas import Replicas
+
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    dist = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
-
-    def barrier():
-        if dist is not None:
-            dist.barrier()
-
-    def max_over_ranks(x: float) -> float:
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    reps = Replicas("nccl", device=dev)
+    barrier, max_over_ranks = reps.barrier, reps.max
 
     tris, (eye, c, up, fovy) = make_scene(wl)
     n, w, h = len(tris), wl["w"], wl["h"]
@@ -556,9 +544,8 @@ def main():
         cb, _ = cpu_sample_ao(wl, tris, cam_arr, out, args.cpu_seconds)
         cb["build"] = cpu_build_baseline(tris)
         line["cpu_baseline"] = cb
-    if dist is not None:
-        dist.destroy_process_group()
-    if rank == 0:
+    reps.close()
+    if reps.is_root:
         print(json.dumps(line), flush=True)
 
 
