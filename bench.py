@@ -286,6 +286,51 @@ def bench_batched(args, dev, stream, barrier, max_over_ranks, world, n_meshes=10
     }
 
 
+def bench_precision(args, builder, qtree, d_tris, tris, cam, w, h, dev, stream, max_over_ranks):
+    """The precision configuration: closest hits of 1M camera rays of the
+    frame (every other pixel) over the FP32 and the quantised tree: hit-ID
+    agreement, t equality, the largest t error against the FP64 evaluation of
+    the ray-plane formula (with its stated bound, fp64check), node bytes per
+    ray, and Mrays/s of both traversals (rays resident, CUDA events)."""
+    import torch
+    import minimumlbvh_b200 as mb
+    from minimumlbvh_b200 import fp64check, scenes
+    rays_h = scenes.camera_rays(cam.m_origin, cam.m_right, cam.m_up, w, h, 2)
+    n = len(rays_h)
+    rays = torch.from_numpy(rays_h).to(dev)
+    hp = torch.empty((n, 8), dtype=torch.int32, device=dev)
+    hq = torch.empty_like(hp)
+    counts = torch.zeros(3 * n, dtype=torch.int32, device=dev)
+    mb.intersect_quantised(qtree, rays, 0, hits=hq, stack_depth=16, counts=counts)
+
+    def run(fn):
+        for _ in range(args.warmup):
+            fn()
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+        torch.cuda.synchronize()
+        ev[0].record(stream)
+        for _ in range(args.steps):
+            fn()
+        ev[1].record(stream)
+        torch.cuda.synchronize()
+        return max_over_ranks(ev[0].elapsed_time(ev[1]) / 1e3 / args.steps)
+
+    tp = run(lambda: mb.intersect(builder, d_tris, rays, hits=hp))
+    tq = run(lambda: mb.intersect_quantised(qtree, rays, 0, hits=hq))
+    a = hp.cpu().numpy().view(np.uint32)
+    b = hq.cpu().numpy().view(np.uint32)
+    c = counts.cpu().numpy().astype(np.int64)
+    chk = fp64check.check_hits(tris, rays_h, b)
+    return {
+        "rays": n, "rays_desc": f"camera rays of every other pixel of the {w}x{h} frame, closest hit",
+        "hit_id_agreement": float((a[:, 7] == b[:, 7]).mean()), "t_equal": float((a[:, 0] == b[:, 0]).mean()),
+        "hits": chk["hits"], "max_abs_t_err_vs_fp64": chk["max_abs_err"], "max_rel_t_err_vs_fp64": chk["max_rel_err"],
+        "max_t_err_over_bound": chk["max_bound_ratio"],
+        "node_bytes_per_ray": (32 * c[:n].sum() + 4 * c[2 * n:].sum()) / n,
+        "quantised_mrays_s": n / tq / 1e6, "plain_mrays_s": n / tp / 1e6, "vs_plain": tp / tq,
+    }
+
+
 def run_reference(args, wl, rank):
     """The reference's own CPU implementation of the path, all host threads."""
     if rank != 0:
@@ -476,6 +521,7 @@ def main():
         torch.cuda.synchronize()
         barrier()
         e2e_s = max_over_ranks(eev[0].elapsed_time(eev[1]) / 1e3)
+        precision = bench_precision(args, builder, qtree, d_tris, tris, cam, w, h, dev, stream, max_over_ranks)
         batched = None if args.no_batched else bench_batched(args, dev, stream, barrier, max_over_ranks,
                                                                    world, args.batched_meshes, not args.no_autotune)
     clocks = sampler.summary()
@@ -534,6 +580,8 @@ def main():
     line["chosen"]["plain_node_visits_per_ray"] = visits / max(rays_per_frame, 1)
     line["chosen"]["plain_node_bytes_per_ray"] = 64 * visits / max(rays_per_frame, 1)
     line["forms"] = form_lines
+    line["precision"] = precision
+    line["gpu_launches"] += 2 * (args.warmup + args.steps) + 1
     if batched is not None:
         line["batched"] = batched
         line["gpu_launches"] += batched["launches"]

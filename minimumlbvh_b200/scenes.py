@@ -41,6 +41,7 @@ __all__ = [
     "log_uniform_counts",
     "batched_soup",
     "batched_rays",
+    "camera_rays",
 ]
 
 
@@ -282,3 +283,20 @@ def batched_rays(tris, tri_offsets: np.ndarray, lo: int = 4096, hi: int = 1_048_
         rays[s:e, 4:7] = (d / d.norm(dim=1, keepdim=True)).float()
     rays[:, 7] = float(np.float32(tmax))
     return rays, np.concatenate([[0], np.cumsum(counts)]).astype(np.int64)
+
+
+def camera_rays(origin, right, up, w: int, h: int, step: int = 2) -> np.ndarray:
+    """Pinhole rays (RayGenerator::shoot, camera.h:24-31, in FP64 numpy) of
+    every `step`-th pixel of a w x h frame: float32 (n, 8) with tmin 0 and
+    tmax FLT_MAX."""
+    o, right, up = (np.asarray(x, np.float64) for x in (origin, right, up))
+    fwd = np.cross(up, right)
+    fwd /= np.linalg.norm(fwd)
+    ys, xs = np.divmod(np.arange(0, w * h, step), w)
+    u, v = (xs / w)[:, None], (ys / h)[:, None]
+    to = o + fwd + (-right + u * 2 * right) + (up - v * 2 * up)
+    rays = np.zeros((len(xs), 8), np.float32)
+    rays[:, 0:3] = o
+    rays[:, 4:7] = to - o
+    rays[:, 7] = np.float32(3.402823466e38)
+    return rays

@@ -69,3 +69,15 @@ def test_replay_walk_equals_stackfree_on_fp32_nodes(case, query, depth):
     assert (nv1 <= nv0).all()
     if depth >= 16 and query == 0 and name != "duplicates":
         assert nv1.sum() < 0.75 * nv0.sum()
+
+
+def test_fp32_hit_distances_within_fp64_bound(case):
+    """Every closest hit's FP32 t is within the stated forward error bound of
+    the FP64 evaluation of the same ray-plane formula (fp64check)."""
+    from minimumlbvh_b200 import fp64check as F
+    name, tris, b, q, rays = case
+    hits = O.trace(b["nodes"], tris, b["root"], rays, 0, 0)
+    r = F.check_hits(tris, rays, hits)
+    assert (r["hits"] > 0 or name == "duplicates") and r["max_bound_ratio"] <= 1.0, r
+    rq = F.check_hits(tris, rays, O.trace_quantised(q, rays, 0))
+    assert rq == r
