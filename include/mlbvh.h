@@ -262,12 +262,13 @@ typedef struct mlbvh_batch_params {
     int traceBlock;  /* threads per CTA of the traversal kernel: 64, 128, 256 or 512 */
     int queueChunk;  /* rays a warp takes from the queue per atomic: 1 .. 65536 */
     int refillLanes; /* idle lanes of a warp that trigger taking more rays: 1 .. 32 */
+    int walk;        /* 0: intersect_stackfree's walk; 1: the replay walk (same Hit records, fewer node loads) */
 } mlbvh_batch_params;
 
 typedef struct mlbvh_batch_graph mlbvh_batch_graph; /* opaque */
 
 MLBVH_API size_t mlbvh_batch_scratch_bytes(uint32_t nMeshes, uint32_t nTriangles);
-/* Defaults: 8-bit digits, 128 threads, chunks of 64 rays, refill at 8 idle lanes. */
+/* Defaults: 8-bit digits, 128 threads, chunks of 64 rays, refill at 8 idle lanes, replay walk. */
 MLBVH_API void mlbvh_batch_params_default(mlbvh_batch_params* params);
 /* Builds every mesh's tree (params may be NULL: the defaults). */
 MLBVH_API mlbvh_status mlbvh_build_batched(const mlbvh_batch* batch, const mlbvh_batch_params* params, void* stream);
@@ -275,7 +276,7 @@ MLBVH_API mlbvh_status mlbvh_build_batched(const mlbvh_batch* batch, const mlbvh
  * the same dScratch, whose header it reads). */
 MLBVH_API mlbvh_status mlbvh_trace_batched(const mlbvh_batch* batch, const mlbvh_batch_params* params, void* stream);
 /* Times candidate parameters on this batch (the digit width on the build,
- * then block size, queue chunk and refill threshold on the traversal, one at
+ * then walk, block size, queue chunk and refill threshold on the traversal, one at
  * a time) and writes the fastest to *params; *buildMs / *traceMs (may be
  * NULL) receive their median times. Runs the build and the traversal many
  * times, overwriting the outputs, and synchronises `stream`. */

@@ -449,7 +449,7 @@ def pt_diff_adjoint(grad_albedo, grad_image, imageSize, rayGenerator: RayGenerat
 class BatchParams(ctypes.Structure):
     """mlbvh_batch_params: launch parameters of the batched form."""
     _fields_ = [("digitBits", ctypes.c_int), ("traceBlock", ctypes.c_int), ("queueChunk", ctypes.c_int),
-                ("refillLanes", ctypes.c_int)]
+                ("refillLanes", ctypes.c_int), ("walk", ctypes.c_int)]
 
     @classmethod
     def default(cls) -> "BatchParams":

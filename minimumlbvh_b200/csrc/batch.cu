@@ -25,9 +25,10 @@
 // Traversal: k_batch_trace is persistent (one grid of resident CTAs). A warp
 // takes `queueChunk` consecutive rays per atomic on the queue counter and
 // hands them to its idle lanes; every lane walks its own ray one node per
-// loop iteration (the stack-free walk of intersect_stackfree) and takes the
-// next ray as soon as it finishes, so lanes never wait for the longest ray of
-// the warp. Rays find their mesh through the ray offsets.
+// loop iteration (the stack-free walk of intersect_stackfree, or the replay
+// walk that gives the same Hit records from a stack of pending far children)
+// and takes the next ray as soon as it finishes, so lanes never wait for the
+// longest ray of the warp. Rays find their mesh through the ray offsets.
 #include <algorithm>
 #include <cstring>
 #include <vector>
@@ -377,7 +378,9 @@ __global__ void __launch_bounds__(kBuildThreads)
 // The persistent traversal (see the file comment). Hits are written as
 // mlbvh_trace writes them; ray i of the batch belongs to the mesh m with
 // rayOff[m] <= i < rayOff[m+1].
-template <bool kAny>
+constexpr int kBatchReplayDepth = 16;  // stack entries per lane of the replay walk
+
+template <bool kAny, bool kReplay>
 __global__ void __launch_bounds__(512)
     k_batch_trace(const mlbvh_internal_node* __restrict__ nodes, const mlbvh_node_index* __restrict__ roots,
                   const float* __restrict__ tris, const uint32_t* __restrict__ triOff,
@@ -386,6 +389,11 @@ __global__ void __launch_bounds__(512)
                   const uint32_t* __restrict__ header, uint32_t chunk, uint32_t refill)
 {
     if (__ldcg(header + kHdrError)) return;  // the build failed: its trees must not be walked
+    // replay walk: kBatchReplayDepth stack entries per lane in dynamic shared memory, one column per thread
+    extern __shared__ __align__(16) unsigned char s_replay[];
+    using Entry = typename ReplayStack<kAny>::Entry;
+    Entry* const stack = reinterpret_cast<Entry*>(s_replay) + threadIdx.x;
+    int depth = 0;
     const int lane = threadIdx.x & 31;
     const uint32_t lanesBelow = (1u << lane) - 1u;
     uint32_t poolNext = 0, poolEnd = 0, poolMesh = 0;  // warp-uniform: rays taken, not yet handed out
@@ -440,6 +448,7 @@ __global__ void __launch_bounds__(512)
                     hit.tri = 0xFFFFFFFFu;
                     curr = __ldg(roots + m);
                     prev = kInvalid;
+                    depth = 0;
                     steps = 0;
                     live = true;
                 }
@@ -453,14 +462,36 @@ __global__ void __launch_bounds__(512)
         if (live) {
             // an index outside the mesh's tree (possible only in a corrupt tree) ends the walk
             const bool inTree = (curr & kLeafBit) ? (curr & ~kLeafBit) < leaves : curr + 1 < leaves;
-            if (!inTree || stackfree_step<kAny, false, true>(curr, prev, hit, mn, mt, ro, rd, inv, tmin, nv, nt) ||
-                ++steps >= kMaxTraversalSteps) {
+            bool done = !inTree;
+            if (!done) {
+                if constexpr (kReplay)
+                    done = stackfree_replay_step<kAny, false, kBatchReplayDepth>(curr, prev, depth, stack, blockDim.x,
+                                                                                  hit, mn, mt, ro, rd, inv, tmin, nv,
+                                                                                  nt);
+                else
+                    done = stackfree_step<kAny, false, true>(curr, prev, hit, mn, mt, ro, rd, inv, tmin, nv, nt);
+            }
+            if (done || ++steps >= kMaxTraversalSteps) {
                 hits[2 * (size_t)ray] = make_float4(hit.t, 0.0f, hit.u, hit.v);
                 hits[2 * (size_t)ray + 1] = make_float4(hit.ng.x, hit.ng.y, hit.ng.z, __uint_as_float(hit.tri));
                 live = false;
             }
         }
     }
+}
+
+// The replay traversal's dynamic shared memory can exceed 48 KB (512 threads,
+// closest hit: 64 KB); allow it once per device.
+void prepare_trace()
+{
+    static bool done[64] = {};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev >= 0 && dev < 64 && done[dev]) return;
+    const int smem = kBatchReplayDepth * 512 * 8;
+    cudaFuncSetAttribute(k_batch_trace<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    cudaFuncSetAttribute(k_batch_trace<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (dev >= 0 && dev < 64) done[dev] = true;
 }
 
 template <int kBits>
@@ -537,6 +568,7 @@ mlbvh_status check_params(const mlbvh_batch_params& p)
         return fail(MLBVH_ERR_INVALID_ARG, "traceBlock must be 64, 128, 256 or 512");
     if (p.queueChunk < 1 || p.queueChunk > 65536) return fail(MLBVH_ERR_INVALID_ARG, "queueChunk must be in [1, 65536]");
     if (p.refillLanes < 1 || p.refillLanes > 32) return fail(MLBVH_ERR_INVALID_ARG, "refillLanes must be in [1, 32]");
+    if (p.walk != 0 && p.walk != 1) return fail(MLBVH_ERR_INVALID_ARG, "walk must be 0 (stack-free) or 1 (replay)");
     return MLBVH_OK;
 }
 
@@ -568,6 +600,7 @@ void batch_params_default(mlbvh_batch_params* p)
     p->traceBlock = 128;
     p->queueChunk = 64;
     p->refillLanes = 8;
+    p->walk = 1;
 }
 
 mlbvh_status build_batched(const mlbvh_batch& B, const mlbvh_batch_params& P, cudaStream_t stream)
@@ -598,12 +631,16 @@ mlbvh_status trace_batched(const mlbvh_batch& B, const mlbvh_batch_params& P, cu
     cudaError_t e = cudaMemsetAsync(header + kHdrQueue, 0, sizeof(uint32_t), stream);
     if (e != cudaSuccess) return fail(MLBVH_ERR_CUDA, cudaGetErrorString(e));
     const bool any = B.rayQuery == MLBVH_RAY_QUERY_ANY;
-    auto kernel = any ? k_batch_trace<true> : k_batch_trace<false>;
+    const bool replay = P.walk == 1;
+    auto kernel = any ? (replay ? k_batch_trace<true, true> : k_batch_trace<true, false>)
+                      : (replay ? k_batch_trace<false, true> : k_batch_trace<false, false>);
+    const size_t smem = replay ? (size_t)kBatchReplayDepth * P.traceBlock * (any ? 4 : 8) : 0;
+    prepare_trace();
     int perSm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, kernel, P.traceBlock, 0) != cudaSuccess || perSm <= 0)
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, kernel, P.traceBlock, smem) != cudaSuccess || perSm <= 0)
         perSm = 1;
     const int grid = perSm * device_sm_count();
-    kernel<<<grid, P.traceBlock, 0, stream>>>(B.dInternals, B.dRootNodes, reinterpret_cast<const float*>(B.dTriangles),
+    kernel<<<grid, P.traceBlock, smem, stream>>>(B.dInternals, B.dRootNodes, reinterpret_cast<const float*>(B.dTriangles),
                                               B.dMeshTriangleOffsets, reinterpret_cast<const float4*>(B.dRays),
                                               B.dMeshRayOffsets, B.nMeshes, B.nRays,
                                               reinterpret_cast<float4*>(B.dHits), header + kHdrQueue, header,
@@ -632,6 +669,7 @@ mlbvh_status batch_graph_create(const mlbvh_batch& B, const mlbvh_batch_params& 
     if (mlbvh_status s = check_geometry(B)) return s;
     if (mlbvh_status s = check_params(P)) return s;
     // kernel attributes are set outside the capture
+    prepare_trace();
     if (P.digitBits == 11)
         prepare_sort<11>();
     else
@@ -752,13 +790,14 @@ mlbvh_status batch_autotune(const mlbvh_batch& B, mlbvh_batch_params* out, float
             return time_median([&] { return trace_batched(B, p, stream); }, stream, 1, ms);
         };
         if (mlbvh_status s = try_trace(best, &bestT)) return s;
-        const int blocks[] = {64, 128, 256, 512}, chunks[] = {32, 64, 128, 256, 512}, refills[] = {1, 4, 8, 16};
-        for (int axis = 0; axis < 3; ++axis) {
-            const int* vals = axis == 0 ? blocks : axis == 1 ? chunks : refills;
-            const int count = axis == 0 ? 4 : axis == 1 ? 5 : 4;
+        const int walks[] = {0, 1}, blocks[] = {64, 128, 256, 512}, chunks[] = {32, 64, 128, 256, 512},
+                  refills[] = {1, 4, 8, 16};
+        for (int axis = 0; axis < 4; ++axis) {
+            const int* vals = axis == 0 ? walks : axis == 1 ? blocks : axis == 2 ? chunks : refills;
+            const int count = axis == 0 ? 2 : axis == 1 ? 4 : axis == 2 ? 5 : 4;
             for (int k = 0; k < count; ++k) {
                 mlbvh_batch_params p = best;
-                int& field = axis == 0 ? p.traceBlock : axis == 1 ? p.queueChunk : p.refillLanes;
+                int& field = axis == 0 ? p.walk : axis == 1 ? p.traceBlock : axis == 2 ? p.queueChunk : p.refillLanes;
                 if (field == vals[k]) continue;
                 field = vals[k];
                 float ms = 0.0f;

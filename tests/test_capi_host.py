@@ -115,7 +115,7 @@ def test_batched_entry_points_reject_bad_arguments():
     assert L.mlbvh_build_batched(by(_fake_batch(scratchBytes=64)), None, None) == 1
     assert b"scratch" in L.mlbvh_last_error_string()
     p = mb.BatchParams.default()
-    for field, bad in (("digitBits", 9), ("traceBlock", 96), ("queueChunk", 0), ("refillLanes", 33)):
+    for field, bad in (("digitBits", 9), ("traceBlock", 96), ("queueChunk", 0), ("refillLanes", 33), ("walk", 2)):
         q = mb.BatchParams.default()
         setattr(q, field, bad)
         assert L.mlbvh_build_batched(by(_fake_batch()), by(q), None) == 1, field

@@ -94,9 +94,10 @@ def _rays_for(tris_t, offsets, counts, seed=5):
     return rays.numpy(), roff
 
 
+@pytest.mark.parametrize("walk", [0, 1])
 @pytest.mark.parametrize("query", [mb.RAY_QUERY_CLOSEST, mb.RAY_QUERY_ANY])
 @pytest.mark.parametrize("chunk,block,refill", [(64, 128, 8), (1, 64, 1), (512, 512, 32)])
-def test_batched_trace_matches_oracle(cuda, query, chunk, block, refill):
+def test_batched_trace_matches_oracle(cuda, query, chunk, block, refill, walk):
     tris, offsets = _small_batch(seed=21)
     bb = _batch(tris, offsets)
     bb.build()
@@ -108,7 +109,7 @@ def test_batched_trace_matches_oracle(cuda, query, chunk, block, refill):
     rays, roff = _rays_for(bb.triangles, offsets, counts)
     bb.set_rays(G.dev(rays), G.dev(roff.astype(np.int32)), query)
     p = mb.BatchParams.default()
-    p.queueChunk, p.traceBlock, p.refillLanes = chunk, block, refill
+    p.queueChunk, p.traceBlock, p.refillLanes, p.walk = chunk, block, refill, walk
     hits = G.host(bb.trace(p), np.uint32)
     bb.status()
     nodes = G.host(bb.internals, np.uint32)
@@ -185,7 +186,7 @@ def test_batched_autotune_keeps_results(cuda):
     ref_hits = bb.trace().clone()
     ref_nodes = bb.internals.clone()
     p, build_ms, trace_ms = bb.autotune()
-    assert p.digitBits in (8, 11) and p.traceBlock in (64, 128, 256, 512)
+    assert p.digitBits in (8, 11) and p.traceBlock in (64, 128, 256, 512) and p.walk in (0, 1)
     assert build_ms > 0 and trace_ms > 0
     bb.build(p)
     hits = bb.trace(p)
