@@ -373,6 +373,22 @@ MLBVH_API mlbvh_status mlbvh_pt_diff_adjoint(float* dGradAlbedo, const float* dG
 /* pack (main_gpu.cu:273-286): accumulator / spp, gamma 1/2.2, RGBA8. */
 MLBVH_API mlbvh_status mlbvh_pack(uint32_t* dPixels, const float* dAccumulators, int n, void* stream);
 
+/* ------------------------------------------------------------ OBJ scenes ---
+ * A host-side OBJ / MTL reader giving the path tracer's input as the
+ * reference's scene loop does (main_gpu.cpp:209-282, over a third-party OBJ
+ * library there): one triangle and one TriangleAttrib per triangle, with the
+ * corner normals, reflectance = the material's Kd, emissive = its Ke, or
+ * reflectance 0.5 and no emission without a material. Quads are split along
+ * the shorter diagonal, larger faces into fans. The mesh lives in host memory
+ * until mlbvh_obj_free; copy the arrays to the device for mlbvh_build and
+ * mlbvh_render_pt. Errors: MLBVH_ERR_INVALID_ARG (file missing, bad corner). */
+typedef struct mlbvh_obj_mesh mlbvh_obj_mesh; /* opaque */
+MLBVH_API mlbvh_status mlbvh_obj_load(const char* path, mlbvh_obj_mesh** mesh);
+MLBVH_API uint32_t mlbvh_obj_triangle_count(const mlbvh_obj_mesh* mesh);
+MLBVH_API const mlbvh_triangle* mlbvh_obj_triangles(const mlbvh_obj_mesh* mesh);
+MLBVH_API const mlbvh_triangle_attrib* mlbvh_obj_attribs(const mlbvh_obj_mesh* mesh);
+MLBVH_API void mlbvh_obj_free(mlbvh_obj_mesh* mesh);
+
 /* Profiling hook (no reference counterpart; the reference times whole calls
  * with its DeviceStopwatch, minimum_lbvh.h:693-724): the next mlbvh_render_ao
  * or mlbvh_build on this host thread records the two cudaEvent_t handles

@@ -22,7 +22,7 @@ __all__ = [
     "TRAVERSAL_STACKFULL", "TRAVERSAL_REPLAY", "OnesweepSort", "BVHGPUBuilder", "RayGenerator", "intersect",
     "render_normal", "render_ao", "render_pt", "pack", "profile_events", "FLT_MAX", "INVALID_NODE",
     "QuantisedBVH", "intersect_quantised", "render_ao_quantised", "pt_diff_render", "pt_diff_adjoint",
-    "BatchParams", "BatchedBVH", "leaf_triangles",
+    "BatchParams", "BatchedBVH", "leaf_triangles", "load_obj",
 ]
 
 BUILD_OPTION_USE_NORMAL = 1   # minimum_lbvh.h:44
@@ -79,6 +79,11 @@ def lib() -> ctypes.CDLL:
             "mlbvh_render_ao_ex": (i32, [_vp, _vp, i32, i32, _vp, _vp, _vp, _vp, i32, i32, f32, u32, i32, _vp, _vp,
                                          _vp, sz, _vp]),
             "mlbvh_leaf_triangles": (i32, [_vp, _vp, _vp, u32, _vp, _vp]),
+            "mlbvh_obj_load": (i32, [ctypes.c_char_p, _vp]),
+            "mlbvh_obj_triangle_count": (u32, [_vp]),
+            "mlbvh_obj_triangles": (_vp, [_vp]),
+            "mlbvh_obj_attribs": (_vp, [_vp]),
+            "mlbvh_obj_free": (None, [_vp]),
             "mlbvh_pack": (i32, [_vp, _vp, i32, _vp]),
             "mlbvh_profile_events": (None, [_vp, _vp]),
             "mlbvh_quantise": (i32, [_vp, _vp, _vp, u32, _vp, _vp, _vp, _vp, _vp]),
@@ -571,3 +576,22 @@ class BatchGraph:
             self.close()
         except Exception:
             pass
+
+
+def load_obj(path: str):
+    """mlbvh_obj_load: (triangles float32 (n, 9), attributes float32 (n, 15)
+    as TriangleAttrib: shading normals, reflectance, emissive), host arrays."""
+    L = lib()
+    h = _vp()
+    _check(L.mlbvh_obj_load(os.fsencode(path), ctypes.byref(h)))
+    try:
+        n = L.mlbvh_obj_triangle_count(h)
+        if n == 0:
+            return np.zeros((0, 9), np.float32), np.zeros((0, 15), np.float32)
+        tp = ctypes.cast(L.mlbvh_obj_triangles(h), ctypes.POINTER(ctypes.c_float))
+        ap = ctypes.cast(L.mlbvh_obj_attribs(h), ctypes.POINTER(ctypes.c_float))
+        tris = np.ctypeslib.as_array(tp, shape=(n, 9)).copy()
+        attribs = np.ctypeslib.as_array(ap, shape=(n, 15)).copy()
+    finally:
+        L.mlbvh_obj_free(h)
+    return tris, attribs

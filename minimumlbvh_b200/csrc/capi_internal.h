@@ -88,5 +88,6 @@ mlbvh_status batch_graph_create(const mlbvh_batch& B, const mlbvh_batch_params& 
                                 mlbvh_batch_graph** out);
 mlbvh_status batch_graph_launch(mlbvh_batch_graph* g, cudaStream_t stream);
 void batch_graph_destroy(mlbvh_batch_graph* g);
+mlbvh_status obj_load(const char* path, mlbvh_obj_mesh** out);
 
 }  // namespace mlbvh
