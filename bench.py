@@ -469,8 +469,23 @@ def main():
             mb.render_ao_quantised(pixels, (w, h), cam, qtree, 1, wl["ns"], wl["radius"], 12345, occluded=occluded,
                                    stats=stats)
 
+        # the 4-wide tree for the AO rays: regrouping + leaf-ordered triangles,
+        # timed as the form's preparation per build
+        wide = mb.WideBVH.from_builder(builder, d_tris)
+        wev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+        for i in range(args.steps):
+            wev[i][0].record(stream)
+            wide.update(stream)
+            wev[i][1].record(stream)
+        torch.cuda.synchronize()
+        wide_prep_ms = float(np.mean([a.elapsed_time(b) for a, b in wev]))
+
+        def wide_frame(occluded=None, stats=None):
+            mb.render_ao_wide(pixels, (w, h), cam, wide, 1, wl["ns"], wl["radius"], 12345, occluded=occluded,
+                              stats=stats)
+
         forms = {}
-        for name, frame in (("replay", replay_frame), ("quantised", quantised_frame)):
+        for name, frame in (("replay", replay_frame), ("quantised", quantised_frame), ("wide", wide_frame)):
             occ = torch.empty_like(occ_plain)
             fst = torch.zeros(8, dtype=torch.int64, device=dev)
             frame(occluded=occ, stats=fst)
@@ -539,7 +554,8 @@ def main():
                    "ao_rays": ao_rays, "parallelism": "replicas" if world > 1 else "single GPU",
                    "l2": "inputs larger than L2 (nodes + triangles 419 MB)" if wl["scene"] == "soup"
                    else "L2 flushed (256 MB write) between timed frames"},
-        "gpu_launches": args.steps * (3 + 3 + 3 + 7 + 10),  # AO, replay AO, quantised AO, build, e2e steps
+        "gpu_launches": args.steps * (3 + 3 + 3 + 3 + 2 + 7 + 10),  # AO, replay, quantised, wide AO, wide prep,
+        # build, e2e steps
         "clocks": clocks,
     }
     # roofline of the dominant kernel (k_ao_rays): algorithmic bytes of its rays
@@ -561,19 +577,31 @@ def main():
                    "h2d_bytes_per_step": int(host_tris.numel() * 4), "d2h_bytes_per_step": int(w * h * 4),
                    "ms_per_step": e2e_s * 1e3 / args.steps}
     form_lines = {}
+    form_desc = {
+        "replay": "FP32 nodes, replay walk (stack of pending far children), leaf-ordered 48-byte triangles",
+        "quantised": "quantised 8-bit child boxes (32-byte nodes), replay walk",
+        "wide": "AO rays over the 4-wide regrouping of the FP32 tree (128-byte nodes, any-hit), "
+                "primary rays on the replay walk, leaf-ordered 48-byte triangles",
+    }
     for name, (total_s, agree, fst) in forms.items():
         f_rays = int(fst[0])
-        node_bytes = (64 * int(fst[1])) if name == "replay" else (32 * int(fst[1]) + 4 * int(fst[5]))
+        if name == "replay":
+            node_bytes = 64 * int(fst[1])
+        elif name == "quantised":
+            node_bytes = 32 * int(fst[1]) + 4 * int(fst[5])
+        else:  # primary rays visit 64-byte binary nodes, AO rays 128-byte wide nodes
+            node_bytes = 64 * (int(fst[1]) - int(fst[3])) + 128 * int(fst[3])
         tri_bytes = 48 * int(fst[2])
         form_lines[name] = {
-            "form": "FP32 nodes, replay walk (stack of pending far children), leaf-ordered 48-byte triangles"
-            if name == "replay"
-            else "quantised 8-bit child boxes (32-byte nodes), replay walk",
+            "form": form_desc[name],
             "value": f_rays * args.steps * world / total_s / 1e6, "unit": "Mrays/s",
             "ms_per_step": total_s * 1e3 / args.steps, "vs_plain": ao_total_s / total_s,
             "occlusion_agreement": agree, "rays_per_frame": f_rays,
             "node_visits_per_ray": int(fst[1]) / max(f_rays, 1),
             "node_bytes_per_ray": node_bytes / max(f_rays, 1), "tri_bytes_per_ray": tri_bytes / max(f_rays, 1)}
+        if name == "wide":
+            form_lines[name]["prep_ms_per_build"] = wide_prep_ms
+            form_lines[name]["restarts"] = int(fst[6])
     exact = [k for k, v in form_lines.items() if v["occlusion_agreement"] == 1.0]
     best = max(exact, key=lambda k: form_lines[k]["value"]) if exact else None
     line["chosen"] = dict(form_lines[best]) if best else {"form": None, "note": "no form agreed with the plain one"}

@@ -118,6 +118,27 @@ typedef struct mlbvh_qheader {
     uint32_t _pad;
 } mlbvh_qheader;
 
+/* The 4-wide tree for any-hit rays (no reference counterpart): a 4-wide
+ * regrouping of the same binary tree. Slot i holds the expansion of binary
+ * internal node i: its two children, then repeatedly the internal child of
+ * largest surface area replaced by its two children, until four children or
+ * only leaves are left. Child boxes are the binary tree's own (exact FP32),
+ * stored per axis (axis[a].lo[c], axis[a].hi[c] for child c). child[c] is an
+ * internal-node index (which is also the slot of that node's expansion), a
+ * leaf position with bit 31 set (leaf j = left leaf child of binary node j or
+ * right leaf child of node j - 1, as in mlbvh_leaf_triangles), or 0xFFFFFFFF
+ * for an empty slot. Every leaf whose box passes a ray's slab test is reached
+ * through boxes that pass too (a box contains its descendants' boxes and the
+ * slab test is monotone in the box), so an any-hit walk over this tree finds
+ * a hit exactly when intersect_stackfree's any-hit walk does. */
+typedef struct mlbvh_wnode {
+    struct {
+        float lo[4], hi[4];
+    } axis[3];         /* axis[a].lo[c], axis[a].hi[c]: 32 bytes per axis */
+    uint32_t child[4];
+    uint32_t _pad[4];  /* zero */
+} mlbvh_wnode;         /* 128 bytes, 128-byte aligned */
+
 /* Library version (MLBVH_VERSION) and the message of the last error raised on
  * the calling host thread ("" if none). */
 MLBVH_API int mlbvh_version(void);
@@ -341,6 +362,36 @@ MLBVH_API mlbvh_status mlbvh_render_ao_ex(uint32_t* dPixels, uint32_t* dOccluded
 MLBVH_API mlbvh_status mlbvh_leaf_triangles(const mlbvh_internal_node* dInternals, const mlbvh_node_index* dRootNode,
                                             const mlbvh_triangle* dTriangles, uint32_t nTriangles,
                                             mlbvh_qtri* dLeafTriangles, void* stream);
+
+/* The 4-wide tree of a built tree: nTriangles - 1 mlbvh_wnode slots (none
+ * for one triangle), 128-byte aligned. No reference counterpart. */
+MLBVH_API mlbvh_status mlbvh_build_wide(const mlbvh_internal_node* dInternals, const mlbvh_node_index* dRootNode,
+                                        uint32_t nTriangles, mlbvh_wnode* dWideNodes, void* stream);
+/* Any-hit rays over the 4-wide tree (rayQuery must be MLBVH_RAY_QUERY_ANY):
+ * a ray has a hit exactly when mlbvh_trace's any-hit walk finds one; the Hit
+ * record is that of the first triangle this walk finds (the reference's walk
+ * may stop at another one). dLeafTriangles from mlbvh_leaf_triangles. A
+ * ray whose stack (24 entries) would overflow restarts with the stack-free
+ * walk over dInternals / dTriangles. dCounts (may be NULL; 3 * nRays words,
+ * nRays < 2^30) receives per ray the node visits (wide nodes, then binary
+ * nodes after a restart), triangle tests and restarts at [i], [nRays + i],
+ * [2 nRays + i]. */
+MLBVH_API mlbvh_status mlbvh_trace_wide(const mlbvh_wnode* dWideNodes, const mlbvh_internal_node* dInternals,
+                                        const mlbvh_node_index* dRootNode, const mlbvh_triangle* dTriangles,
+                                        const mlbvh_qtri* dLeafTriangles, const mlbvh_ray* dRays, mlbvh_hit* dHits,
+                                        uint32_t nRays, int rayQuery, uint32_t* dCounts, void* stream);
+/* mlbvh_render_ao with the AO rays over the 4-wide tree (any-hit, so every
+ * occlusion count is mlbvh_render_ao's) and the primary rays on the replay
+ * walk over the binary tree (the stack-free walk's Hit records). AO rays of a
+ * pixel start at the deepest wide node whose subtree holds every leaf within
+ * their reach. With dStats, node visits count wide nodes for AO rays. */
+MLBVH_API mlbvh_status mlbvh_render_ao_wide(uint32_t* dPixels, uint32_t* dOccluded, int width, int height,
+                                            const mlbvh_ray_generator* camera, const mlbvh_node_index* dRootNode,
+                                            const mlbvh_internal_node* dInternals, const mlbvh_triangle* dTriangles,
+                                            const mlbvh_wnode* dWideNodes, const mlbvh_qtri* dLeafTriangles,
+                                            int useSobol, int nSamples, float radius, uint32_t sobolSeed,
+                                            unsigned long long* dStats, void* dScratch, size_t scratchBytes,
+                                            void* stream);
 
 /* One progressive path-tracing pass (pt, main_gpu.cu:179-272): reads and
  * updates dAccumulators (float4 per pixel, w = samples so far). maxDepth is

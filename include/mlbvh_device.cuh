@@ -454,6 +454,102 @@ __device__ __forceinline__ bool stackfree_replay_step_lo(uint32_t& curr, uint32_
     }
 }
 
+// ------------------------------------------------------- the 4-wide tree
+// mlbvh_wnode (include/mlbvh.h): slot i is the expansion of binary internal
+// node i into at most four children with the binary tree's own boxes. Only
+// any-hit rays walk it: a leaf whose box passes the slab test is reached
+// through boxes that contain it and therefore pass too (the slab test is
+// monotone in the box: every operation rounds to nearest, which preserves
+// order), and only leaves whose own box passes are tested, so a ray finds a
+// hit exactly when intersect_stackfree's any-hit walk does.
+constexpr uint32_t kWideEmpty = 0xFFFFFFFFu;  // an empty child slot
+constexpr int kWideDepth = 24;                // stack entries per ray
+
+__device__ __forceinline__ float wpick(const float4& v, int k)
+{
+    return k == 0 ? v.x : k == 1 ? v.y : k == 2 ? v.z : v.w;
+}
+__device__ __forceinline__ uint32_t wpick(const uint4& v, int k)
+{
+    return k == 0 ? v.x : k == 1 ? v.y : k == 2 ? v.z : v.w;
+}
+
+// One step of the any-hit walk over the wide tree: a leaf test (leaf-ordered
+// triangles) or a wide-node visit. At a node, every non-empty child whose box
+// passes the slab test is taken: the nearest entry first (ties to the lower
+// slot), the others pushed in slot order. A node whose pushes would overflow
+// the stack (kWideDepth entries, shared memory, `stride` apart) restarts the
+// ray with the stack-free walk over the binary tree from `binaryRoot`
+// (depth < 0 from then on; ++nr). Returns true when the walk is over (a hit,
+// or nothing left).
+template <bool kCount>
+__device__ __forceinline__ bool wide_any_step(uint32_t& curr, uint32_t& prev, int& depth, uint32_t* stack, int stride,
+                                              HitRecord& hit, const mlbvh_wnode* __restrict__ wnodes,
+                                              const mlbvh_internal_node* __restrict__ nodes,
+                                              const float* __restrict__ tris, const mlbvh_qtri* __restrict__ leafTris,
+                                              uint32_t binaryRoot, f3 ro, f3 rd, f3 inv, float tmin, uint32_t& nv,
+                                              uint32_t& nt, uint32_t& nr)
+{
+    if (depth < 0) return stackfree_step<true, kCount, true>(curr, prev, hit, nodes, tris, ro, rd, inv, tmin, nv, nt);
+    if (curr & kLeafBit) {
+        if (kCount) ++nt;
+        const float4* t = reinterpret_cast<const float4*>(leafTris + (curr & ~kLeafBit));
+        const float4 a = __ldg(t), b = __ldg(t + 1), c = __ldg(t + 2);
+        float tt, u, v;
+        f3 ng;
+        if (intersect_triangle(tt, u, v, ng, tmin, hit.t, ro, rd, mk(a.x, a.y, a.z), mk(a.w, b.x, b.y),
+                               mk(b.z, b.w, c.x))) {
+            hit.t = tt;
+            hit.u = u;
+            hit.v = v;
+            hit.ng = ng;
+            hit.tri = __float_as_uint(c.y);
+            return true;
+        }
+    } else {
+        if (kCount) ++nv;
+        const float4* p = reinterpret_cast<const float4*>(wnodes + curr);
+        float4 lx, hx, ly, hy, lz, hz;
+        ldg32(p, lx, hx);
+        ldg32(p + 2, ly, hy);
+        ldg32(p + 4, lz, hz);
+        const uint4 ch = __ldg(reinterpret_cast<const uint4*>(p + 6));
+        uint32_t pass = 0;
+        int best = -1;
+        float bestT = 0.0f;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const float2 r = slab(ro, inv, mk(wpick(lx, k), wpick(ly, k), wpick(lz, k)),
+                                  mk(wpick(hx, k), wpick(hy, k), wpick(hz, k)), tmin, hit.t);
+            if (wpick(ch, k) != kWideEmpty && r.x <= r.y) {
+                pass |= 1u << k;
+                if (best < 0 || r.x < bestT) {
+                    best = k;
+                    bestT = r.x;
+                }
+            }
+        }
+        if (pass) {
+            const uint32_t others = pass & ~(1u << best);
+            if (depth + __popc(others) > kWideDepth) {
+                if (kCount) ++nr;
+                depth = -1;
+                curr = binaryRoot;
+                prev = kInvalid;
+                return false;
+            }
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+                if (others & (1u << k)) stack[depth++ * stride] = wpick(ch, k);
+            curr = wpick(ch, best);
+            return false;
+        }
+    }
+    if (depth == 0) return true;
+    curr = stack[--depth * stride];
+    return false;
+}
+
 template <bool kAny, bool kCount = false, bool kWide = false>
 __device__ __forceinline__ void trace_stackfree(HitRecord& hit, const mlbvh_internal_node* __restrict__ nodes,
                                                 const float* __restrict__ tris, uint32_t root, f3 ro, f3 rd,

@@ -20,6 +20,7 @@ __all__ = [
     "lib", "library_path", "MlbvhError", "BUILD_OPTION_USE_NORMAL", "BUILD_OPTION_CPU_PARALLEL",
     "RAY_QUERY_CLOSEST", "RAY_QUERY_ANY", "TRAVERSAL_STACKFREE", "TRAVERSAL_ESCAPE_LINK",
     "TRAVERSAL_STACKFULL", "TRAVERSAL_REPLAY", "OnesweepSort", "BVHGPUBuilder", "RayGenerator", "intersect",
+    "WideBVH", "intersect_wide", "render_ao_wide",
     "render_normal", "render_ao", "render_pt", "pack", "profile_events", "FLT_MAX", "INVALID_NODE",
     "QuantisedBVH", "intersect_quantised", "render_ao_quantised", "pt_diff_render", "pt_diff_adjoint",
     "BatchParams", "BatchedBVH", "leaf_triangles", "load_obj",
@@ -79,6 +80,10 @@ def lib() -> ctypes.CDLL:
             "mlbvh_render_ao_ex": (i32, [_vp, _vp, i32, i32, _vp, _vp, _vp, _vp, i32, i32, f32, u32, i32, _vp, _vp,
                                          _vp, sz, _vp]),
             "mlbvh_leaf_triangles": (i32, [_vp, _vp, _vp, u32, _vp, _vp]),
+            "mlbvh_build_wide": (i32, [_vp, _vp, u32, _vp, _vp]),
+            "mlbvh_trace_wide": (i32, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, u32, i32, _vp, _vp]),
+            "mlbvh_render_ao_wide": (i32, [_vp, _vp, i32, i32, _vp, _vp, _vp, _vp, _vp, _vp, i32, i32, f32, u32, _vp,
+                                           _vp, sz, _vp]),
             "mlbvh_obj_load": (i32, [ctypes.c_char_p, _vp]),
             "mlbvh_obj_triangle_count": (u32, [_vp]),
             "mlbvh_obj_triangles": (_vp, [_vp]),
@@ -297,6 +302,21 @@ def profile_events(start=None, stop=None):
                                None if stop is None else stop.cuda_event)
 
 
+def _ao_scratch(pixels, w: int, h: int, scratch=None):
+    """The caller's AO scratch, or a cached device buffer of the needed size."""
+    import torch
+    if scratch is not None:
+        return scratch
+    need = lib().mlbvh_render_scratch_bytes(int(w), int(h))
+    key = (pixels.device.index, need)
+    scratch = _render_scratch.get(key)
+    if scratch is None:
+        scratch = torch.empty(need, dtype=torch.uint8, device=pixels.device)
+        _render_scratch.clear()
+        _render_scratch[key] = scratch
+    return scratch
+
+
 def render_ao(pixels, imageSize, rayGenerator: RayGenerator, rootNode, internals, triangles, useSobol: int = 1,
               nSamples: int = 16, radius: float = 1.0, seed: int = 12345, occluded=None, stats=None,
               scratch=None, stream=None, traversal: int = TRAVERSAL_STACKFREE, leaf_triangles=None):
@@ -305,16 +325,8 @@ def render_ao(pixels, imageSize, rayGenerator: RayGenerator, rootNode, internals
     tensor of 8) receives rays traced, node visits and triangle tests.
     ``traversal`` TRAVERSAL_REPLAY gives the same result from the replay walk,
     reading ``leaf_triangles`` (from ``leaf_triangles()``) when given."""
-    import torch
     w, h = imageSize
-    need = lib().mlbvh_render_scratch_bytes(int(w), int(h))
-    if scratch is None:
-        key = (pixels.device.index, need)
-        scratch = _render_scratch.get(key)
-        if scratch is None:
-            scratch = torch.empty(need, dtype=torch.uint8, device=pixels.device)
-            _render_scratch.clear()
-            _render_scratch[key] = scratch
+    scratch = _ao_scratch(pixels, w, h, scratch)
     cam = rayGenerator._cstruct()
     if traversal == TRAVERSAL_STACKFREE:
         _check(lib().mlbvh_render_ao(_ptr(pixels), _ptr(occluded), int(w), int(h), ctypes.addressof(cam),
@@ -340,6 +352,67 @@ def leaf_triangles(builder: "BVHGPUBuilder", triangles, out=None, stream=None):
     _check(lib().mlbvh_leaf_triangles(_ptr(builder.m_internals), _ptr(builder.m_rootNode), _ptr(triangles), n,
                                       _ptr(out), _stream(stream)))
     return out
+
+
+class WideBVH:
+    """The 4-wide tree of a built tree (mlbvh_build_wide) with the triangles
+    in leaf order (mlbvh_leaf_triangles): any-hit rays over it find a hit
+    exactly when the stack-free any-hit walk does, loading half as many
+    nodes in a chain. Holds the builder's arrays for primary rays and for the
+    restart of a ray whose stack would overflow."""
+
+    def __init__(self, builder: "BVHGPUBuilder", triangles, wide, leaf_tris):
+        self.builder, self.triangles, self.wide, self.leaf_triangles = builder, triangles, wide, leaf_tris
+
+    @classmethod
+    def from_builder(cls, builder: "BVHGPUBuilder", triangles, stream=None) -> "WideBVH":
+        import torch
+        n = builder.m_nTriangles
+        wide = torch.empty((max(n - 1, 1), 32), dtype=torch.int32, device=triangles.device)
+        _check(lib().mlbvh_build_wide(_ptr(builder.m_internals), _ptr(builder.m_rootNode), n, _ptr(wide),
+                                      _stream(stream)))
+        return cls(builder, triangles, wide, leaf_triangles(builder, triangles, stream=stream))
+
+    def update(self, stream=None) -> "WideBVH":
+        """Regroup again after the builder rebuilt its tree (same triangle
+        count): the wide slots and the leaf-ordered triangles, in place."""
+        n = self.builder.m_nTriangles
+        _check(lib().mlbvh_build_wide(_ptr(self.builder.m_internals), _ptr(self.builder.m_rootNode), n,
+                                      _ptr(self.wide), _stream(stream)))
+        leaf_triangles(self.builder, self.triangles, out=self.leaf_triangles, stream=stream)
+        return self
+
+
+def intersect_wide(w: WideBVH, rays, hits=None, counts=None, stream=None):
+    """Any-hit rays over the 4-wide tree (mlbvh_trace_wide). ``counts``
+    (int32 CUDA tensor of 3 * nRays) receives per-ray node visits, triangle
+    tests and restarts."""
+    import torch
+    _require_cuda(rays, "rays")
+    n = rays.numel() // 8
+    if hits is None:
+        hits = torch.empty((n, 8), dtype=torch.int32, device=rays.device)
+    b = w.builder
+    _check(lib().mlbvh_trace_wide(_ptr(w.wide), _ptr(b.m_internals), _ptr(b.m_rootNode), _ptr(w.triangles),
+                                  _ptr(w.leaf_triangles), _ptr(rays), _ptr(hits), n, RAY_QUERY_ANY, _ptr(counts),
+                                  _stream(stream)))
+    return hits
+
+
+def render_ao_wide(pixels, imageSize, rayGenerator: RayGenerator, w: WideBVH, useSobol: int = 1,
+                   nSamples: int = 16, radius: float = 1.0, seed: int = 12345, occluded=None, stats=None,
+                   scratch=None, stream=None):
+    """render_ao with the AO rays over the 4-wide tree (same occlusion
+    counts) and primary rays on the replay walk (the same Hit records)."""
+    width, height = imageSize
+    scratch = _ao_scratch(pixels, width, height, scratch)
+    cam = rayGenerator._cstruct()
+    b = w.builder
+    _check(lib().mlbvh_render_ao_wide(_ptr(pixels), _ptr(occluded), int(width), int(height), ctypes.addressof(cam),
+                                      _ptr(b.m_rootNode), _ptr(b.m_internals), _ptr(w.triangles), _ptr(w.wide),
+                                      _ptr(w.leaf_triangles), int(useSobol), int(nSamples), float(radius), int(seed),
+                                      _ptr(stats), _ptr(scratch), scratch.numel(), _stream(stream)))
+    return pixels
 
 
 def render_pt(accumulators, imageSize, rayGenerator: RayGenerator, rootNode, internals, triangles,
@@ -409,16 +482,8 @@ def render_ao_quantised(pixels, imageSize, rayGenerator: RayGenerator, q: Quanti
                         nSamples: int = 16, radius: float = 1.0, seed: int = 12345, occluded=None, stats=None,
                         scratch=None, stream=None):
     """render_ao over the quantised tree."""
-    import torch
     w, h = imageSize
-    need = lib().mlbvh_render_scratch_bytes(int(w), int(h))
-    if scratch is None:
-        key = (pixels.device.index, need)
-        scratch = _render_scratch.get(key)
-        if scratch is None:
-            scratch = torch.empty(need, dtype=torch.uint8, device=pixels.device)
-            _render_scratch.clear()
-            _render_scratch[key] = scratch
+    scratch = _ao_scratch(pixels, w, h, scratch)
     cam = rayGenerator._cstruct()
     _check(lib().mlbvh_render_ao_quantised(_ptr(pixels), _ptr(occluded), int(w), int(h), ctypes.addressof(cam),
                                            _ptr(q.qnodes), _ptr(q.parents), _ptr(q.qtris), _ptr(q.header),

@@ -135,6 +135,37 @@ mlbvh_status mlbvh_leaf_triangles(const mlbvh_internal_node* dInternals, const m
     return leaf_triangles(dInternals, dRootNode, dTriangles, nTriangles, dLeafTriangles, as_stream(stream));
 }
 
+mlbvh_status mlbvh_build_wide(const mlbvh_internal_node* dInternals, const mlbvh_node_index* dRootNode,
+                              uint32_t nTriangles, mlbvh_wnode* dWideNodes, void* stream)
+{
+    clear_error();
+    return build_wide(dInternals, dRootNode, nTriangles, dWideNodes, as_stream(stream));
+}
+
+mlbvh_status mlbvh_trace_wide(const mlbvh_wnode* dWideNodes, const mlbvh_internal_node* dInternals,
+                              const mlbvh_node_index* dRootNode, const mlbvh_triangle* dTriangles,
+                              const mlbvh_qtri* dLeafTriangles, const mlbvh_ray* dRays, mlbvh_hit* dHits,
+                              uint32_t nRays, int rayQuery, uint32_t* dCounts, void* stream)
+{
+    clear_error();
+    return trace_wide(dWideNodes, dInternals, dRootNode, dTriangles, dLeafTriangles, dRays, dHits, nRays, rayQuery,
+                      dCounts, as_stream(stream));
+}
+
+mlbvh_status mlbvh_render_ao_wide(uint32_t* dPixels, uint32_t* dOccluded, int width, int height,
+                                  const mlbvh_ray_generator* camera, const mlbvh_node_index* dRootNode,
+                                  const mlbvh_internal_node* dInternals, const mlbvh_triangle* dTriangles,
+                                  const mlbvh_wnode* dWideNodes, const mlbvh_qtri* dLeafTriangles, int useSobol,
+                                  int nSamples, float radius, uint32_t sobolSeed, unsigned long long* dStats,
+                                  void* dScratch, size_t scratchBytes, void* stream)
+{
+    clear_error();
+    if (!camera) return fail(MLBVH_ERR_INVALID_ARG, "null camera");
+    return render_ao_wide(dPixels, dOccluded, width, height, *camera, dRootNode, dInternals, dTriangles, dWideNodes,
+                          dLeafTriangles, useSobol, nSamples, radius, sobolSeed, dStats, dScratch, scratchBytes,
+                          as_stream(stream));
+}
+
 mlbvh_status mlbvh_render_pt(float* dAccumulators, int width, int height, const mlbvh_ray_generator* camera,
                              const mlbvh_node_index* dRootNode, const mlbvh_internal_node* dInternals,
                              const mlbvh_triangle* dTriangles, const mlbvh_triangle_attrib* dAttribs, int useSobol,

@@ -53,6 +53,16 @@ mlbvh_status render_ao(uint32_t* dPixels, uint32_t* dOccluded, int w, int h, con
                        cudaStream_t stream);
 mlbvh_status leaf_triangles(const mlbvh_internal_node* dNodes, const mlbvh_node_index* dRoot,
                             const mlbvh_triangle* dTris, uint32_t n, mlbvh_qtri* dLeafTris, cudaStream_t stream);
+mlbvh_status build_wide(const mlbvh_internal_node* dNodes, const mlbvh_node_index* dRoot, uint32_t n,
+                        mlbvh_wnode* dWide, cudaStream_t stream);
+mlbvh_status trace_wide(const mlbvh_wnode* dWide, const mlbvh_internal_node* dNodes, const mlbvh_node_index* dRoot,
+                        const mlbvh_triangle* dTris, const mlbvh_qtri* dLeafTris, const mlbvh_ray* dRays,
+                        mlbvh_hit* dHits, uint32_t nRays, int rayQuery, uint32_t* dCounts, cudaStream_t stream);
+mlbvh_status render_ao_wide(uint32_t* dPixels, uint32_t* dOccluded, int w, int h, const mlbvh_ray_generator& cam,
+                            const mlbvh_node_index* dRoot, const mlbvh_internal_node* dNodes,
+                            const mlbvh_triangle* dTris, const mlbvh_wnode* dWide, const mlbvh_qtri* dLeafTris,
+                            int useSobol, int nSamples, float radius, uint32_t seed, unsigned long long* dStats,
+                            void* dScratch, size_t scratchBytes, cudaStream_t stream);
 mlbvh_status render_ao_quantised(uint32_t* dPixels, uint32_t* dOccluded, int w, int h, const mlbvh_ray_generator& cam,
                                  const mlbvh_qnode* dQNodes, const uint32_t* dQParents, const mlbvh_qtri* dQTris,
                                  const mlbvh_qheader* dQHeader, int useSobol, int nSamples, float radius,

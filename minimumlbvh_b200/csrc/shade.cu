@@ -150,6 +150,7 @@ struct PlainTreeT {
         return Ctx{(kWalk == 2 && (r & kLeafBit)) ? kLeafBit : r};
     }
     static constexpr int kStack = kWalk > 0 ? kReplayDepth : 0;
+    static constexpr int kPrimaryStack = kStack;  // closest-hit replay stack of primary rays
     // Replay forms: the node where AO rays from the ball's centre start. From
     // the root, while exactly one child's box meets the ball, go down into it;
     // stop where both do (or at a leaf). Every leaf an AO ray of the pixel can
@@ -241,6 +242,7 @@ struct QuantTree {
     // kStack pending far children per lane (shared memory) instead of revisits;
     // only any-hit steps are taken (AO rays)
     static constexpr int kStack = 16;
+    static constexpr int kPrimaryStack = kStack;
     __device__ __forceinline__ uint32_t ball_start(const Ctx& c, const AoBall& b) const
     {
         uint32_t curr = c.root;
@@ -263,6 +265,67 @@ struct QuantTree {
     }
 };
 
+// The 4-wide tree for AO rays (any-hit, wide_any_step), the binary tree's
+// replay walk over leaf-ordered triangles for primary rays (closest hit, the
+// stack-free walk's Hit records). Context: the walk's root (a leaf root is
+// leaf position 0) and the binary root as the reference names it (the
+// restart of a ray whose wide stack would overflow).
+struct WideTree {
+    PlainReplayLeafTree binary;
+    const mlbvh_wnode* wnodes;
+    struct Ctx {
+        uint32_t root, binaryRoot;
+    };
+    static constexpr int kStack = kWideDepth;
+    static constexpr int kPrimaryStack = PlainReplayLeafTree::kStack;
+    __device__ __forceinline__ Ctx context() const
+    {
+        const uint32_t r = __ldg(binary.rootPtr);
+        return Ctx{(r & kLeafBit) ? kLeafBit : r, r};
+    }
+    template <bool kAny, bool kCount>
+    __device__ __forceinline__ void trace(const Ctx& c, HitRecord& hit, f3 ro, f3 rd, Counts& n, uint2* pstack,
+                                          int stride) const
+    {
+        binary.template trace<kAny, kCount>(PlainReplayLeafTree::Ctx{c.root}, hit, ro, rd, n, pstack, stride);
+    }
+    // From the root, while exactly one child's box meets the ball, go down
+    // into it; stop where several do (or at a leaf); kInvalid where none does.
+    __device__ __forceinline__ uint32_t ball_start(const Ctx& c, const AoBall& b) const
+    {
+        uint32_t curr = c.root;
+        for (uint32_t steps = 0; !(curr & kLeafBit) && steps < kMaxTraversalSteps; ++steps) {
+            const float4* p = reinterpret_cast<const float4*>(wnodes + curr);
+            float4 lx, hx, ly, hy, lz, hz;
+            ldg32(p, lx, hx);
+            ldg32(p + 2, ly, hy);
+            ldg32(p + 4, lz, hz);
+            const uint4 ch = __ldg(reinterpret_cast<const uint4*>(p + 6));
+            int meets = 0;
+            uint32_t only = kInvalid;
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+                if (wpick(ch, k) != kWideEmpty && box_meets(mk(wpick(lx, k), wpick(ly, k), wpick(lz, k)),
+                                                            mk(wpick(hx, k), wpick(hy, k), wpick(hz, k)), b)) {
+                    ++meets;
+                    only = wpick(ch, k);
+                }
+            if (meets == 0) return kInvalid;
+            if (meets > 1) return curr;
+            curr = only;
+        }
+        return curr;
+    }
+    template <bool kAny, bool kCount>
+    __device__ __forceinline__ bool step(const Ctx& c, uint32_t& curr, uint32_t& prev, int& depth, uint32_t* stack,
+                                         HitRecord& hit, f3 ro, f3 rd, f3 inv, Counts& n) const
+    {
+        static_assert(kAny, "AO rays are any-hit");
+        return wide_any_step<kCount>(curr, prev, depth, stack, kAoThreads, hit, wnodes, binary.nodes, binary.tris,
+                                     binary.leafTris, c.binaryRoot, ro, rd, inv, 0.0f, n.visits, n.tests, n.ups);
+    }
+};
+
 // Primary rays of ao (main_gpu.cu:121-144): closest hit, flip the normal
 // towards the viewer, AO origin p + n * 1e-3.
 template <class Tree, bool kCount>
@@ -270,7 +333,7 @@ __global__ void __launch_bounds__(kTileW* kTileH)
     k_ao_primary(mlbvh_ray_generator gen, int w, int h, float radius, Tree tree, AoRecord* __restrict__ records,
                  uint32_t* __restrict__ queueCount, uint32_t* __restrict__ counts, unsigned long long* __restrict__ stats)
 {
-    __shared__ uint2 s_pstack[Tree::kStack > 0 ? Tree::kStack : 1][kTileW * kTileH];
+    __shared__ uint2 s_pstack[Tree::kPrimaryStack > 0 ? Tree::kPrimaryStack : 1][kTileW * kTileH];
     Counts cnt;
     int xi, yi;
     const bool inside = tile_pixel(w, h, xi, yi);
@@ -692,6 +755,22 @@ mlbvh_status render_ao(uint32_t* dPixels, uint32_t* dOccluded, int w, int h, con
     if (traversal != MLBVH_TRAVERSAL_STACKFREE)
         return fail(MLBVH_ERR_INVALID_ARG, "AO traversal must be MLBVH_TRAVERSAL_STACKFREE or MLBVH_TRAVERSAL_REPLAY");
     const PlainTree tree{dNodes, reinterpret_cast<const float*>(dTris), dRoot, nullptr};
+    return launch_ao(dPixels, dOccluded, w, h, cam, tree, useSobol, nSamples, radius, seed, dStats, dScratch,
+                     scratchBytes, stream);
+}
+
+mlbvh_status render_ao_wide(uint32_t* dPixels, uint32_t* dOccluded, int w, int h, const mlbvh_ray_generator& cam,
+                            const mlbvh_node_index* dRoot, const mlbvh_internal_node* dNodes,
+                            const mlbvh_triangle* dTris, const mlbvh_wnode* dWide, const mlbvh_qtri* dLeafTris,
+                            int useSobol, int nSamples, float radius, uint32_t seed, unsigned long long* dStats,
+                            void* dScratch, size_t scratchBytes, cudaStream_t stream)
+{
+    if (mlbvh_status s = check_ao_args(w, h, nSamples, dPixels, dOccluded, dScratch, dStats)) return s;
+    if (!dRoot || !dTris || !dLeafTris) return fail(MLBVH_ERR_INVALID_ARG, "null pointer");
+    if (!aligned16(dRoot) || !aligned32(dNodes) || !aligned16(dTris) || !aligned16(dLeafTris) ||
+        (reinterpret_cast<uintptr_t>(dWide) & 127u))
+        return fail(MLBVH_ERR_INVALID_ARG, "device pointers misaligned (wide nodes 128 B, nodes 32 B, others 16 B)");
+    const WideTree tree{PlainReplayLeafTree{dNodes, reinterpret_cast<const float*>(dTris), dRoot, dLeafTris}, dWide};
     return launch_ao(dPixels, dOccluded, w, h, cam, tree, useSobol, nSamples, radius, seed, dStats, dScratch,
                      scratchBytes, stream);
 }

@@ -1,0 +1,178 @@
+// The 4-wide tree for any-hit rays (no reference counterpart): a regrouping
+// of the binary tree that intersect_stackfree walks (minimum_lbvh.h:981-1061)
+// with the same leaves and the same boxes, so that an any-hit ray loads half
+// as many nodes in a chain. Slot i of the wide array is the expansion of
+// binary internal node i, written by one thread with no order between slots:
+// the walk starts at the root's slot and only ever follows child indices,
+// which name the slots of their own expansions.
+#include "capi_internal.h"
+#include "../../include/mlbvh_device.cuh"
+
+namespace mlbvh {
+namespace {
+
+constexpr int kWideThreads = 256;
+constexpr int kWideTraceThreads = 128;
+
+struct WideKid {
+    uint32_t name;  // internal index, kLeafBit | leaf position, or kWideEmpty
+    f3 lo, hi;
+};
+
+__device__ __forceinline__ float half_area(f3 lo, f3 hi)
+{
+    const float dx = hi.x - lo.x, dy = hi.y - lo.y, dz = hi.z - lo.z;
+    float a = dx * dy;
+    a = a + dy * dz;
+    a = a + dz * dx;
+    return a;
+}
+
+// Leaf children of binary node p are named by leaf position: the left one is
+// leaf p, the right one leaf p + 1 (mlbvh_leaf_triangles' order).
+__device__ __forceinline__ void binary_children(const mlbvh_internal_node* __restrict__ nodes, uint32_t p, WideKid& a,
+                                                WideKid& b)
+{
+    const NodeView nd = load_node<true>(nodes, p);
+    a = WideKid{(nd.c0 & kLeafBit) ? (kLeafBit | p) : nd.c0, nd.lo0, nd.hi0};
+    b = WideKid{(nd.c1 & kLeafBit) ? (kLeafBit | (p + 1)) : nd.c1, nd.lo1, nd.hi1};
+}
+
+// Slot i: start from binary node i's two children; twice, replace the
+// internal child of largest surface area (ties: the lower slot) by its two
+// children, keeping the left-to-right leaf order. The area is summed in the
+// fixed order dx dy + dy dz + dz dx (the oracle does the same), so the
+// regrouping, and with it every slot, is deterministic.
+__global__ void __launch_bounds__(kWideThreads)
+    k_wide_collapse(const mlbvh_internal_node* __restrict__ nodes, uint32_t nInternal, mlbvh_wnode* __restrict__ out)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nInternal) return;
+    WideKid kid[4];
+    binary_children(nodes, i, kid[0], kid[1]);
+    kid[2].name = kid[3].name = kWideEmpty;
+    kid[2].lo = kid[2].hi = kid[3].lo = kid[3].hi = mk(0.0f, 0.0f, 0.0f);
+    int count = 2;
+#pragma unroll
+    for (int round = 0; round < 2; ++round) {
+        int pick = -1;
+        float best = 0.0f;
+#pragma unroll
+        for (int k = 0; k < 3 + round; ++k)
+            if (k < count && !(kid[k].name & kLeafBit)) {
+                const float a = half_area(kid[k].lo, kid[k].hi);
+                if (pick < 0 || a > best) {
+                    pick = k;
+                    best = a;
+                }
+            }
+        if (pick < 0) break;
+        WideKid a, b;
+        uint32_t p = 0;
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+            if (k == pick) p = kid[k].name;
+        binary_children(nodes, p, a, b);
+#pragma unroll
+        for (int k = 3; k >= 1; --k)
+            if (k > pick + 1 && k <= count) kid[k] = kid[k - 1];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            if (k == pick) kid[k] = a;
+            if (k == pick + 1) kid[k] = b;
+        }
+        ++count;
+    }
+    float4* dst = reinterpret_cast<float4*>(out + i);
+    dst[0] = make_float4(kid[0].lo.x, kid[1].lo.x, kid[2].lo.x, kid[3].lo.x);
+    dst[1] = make_float4(kid[0].hi.x, kid[1].hi.x, kid[2].hi.x, kid[3].hi.x);
+    dst[2] = make_float4(kid[0].lo.y, kid[1].lo.y, kid[2].lo.y, kid[3].lo.y);
+    dst[3] = make_float4(kid[0].hi.y, kid[1].hi.y, kid[2].hi.y, kid[3].hi.y);
+    dst[4] = make_float4(kid[0].lo.z, kid[1].lo.z, kid[2].lo.z, kid[3].lo.z);
+    dst[5] = make_float4(kid[0].hi.z, kid[1].hi.z, kid[2].hi.z, kid[3].hi.z);
+    reinterpret_cast<uint4*>(dst)[6] = make_uint4(kid[0].name, kid[1].name, kid[2].name, kid[3].name);
+    reinterpret_cast<uint4*>(dst)[7] = make_uint4(0u, 0u, 0u, 0u);
+}
+
+// One thread per ray, any-hit. counts (may be null): per ray, node visits,
+// triangle tests and restarts at counts[i], counts[n + i], counts[2n + i].
+template <bool kCount>
+__global__ void __launch_bounds__(kWideTraceThreads)
+    k_trace_wide(const mlbvh_wnode* __restrict__ wnodes, const mlbvh_internal_node* __restrict__ nodes,
+                 const mlbvh_node_index* __restrict__ rootPtr, const float* __restrict__ tris,
+                 const mlbvh_qtri* __restrict__ leafTris, const float4* __restrict__ rays, float4* __restrict__ hits,
+                 uint32_t n, uint32_t* __restrict__ counts)
+{
+    __shared__ uint32_t s_stack[kWideDepth][kWideTraceThreads];
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float4 a = __ldg(rays + 2 * (size_t)i), b = __ldg(rays + 2 * (size_t)i + 1);
+    const f3 ro = mk(a.x, a.y, a.z), rd = mk(b.x, b.y, b.z);
+    HitRecord hit;
+    hit.t = b.w;
+    hit.u = 0.0f;
+    hit.v = 0.0f;
+    hit.ng = mk(0.0f, 0.0f, 0.0f);
+    hit.tri = 0xFFFFFFFFu;
+    const uint32_t root = __ldg(rootPtr);
+    const f3 inv = inv_rd(rd);
+    uint32_t nv = 0, nt = 0, nr = 0;
+    uint32_t curr = (root & kLeafBit) ? kLeafBit : root, prev = kInvalid;
+    int depth = 0;
+    for (uint32_t steps = 1; steps < kMaxTraversalSteps; ++steps)
+        if (wide_any_step<kCount>(curr, prev, depth, &s_stack[0][threadIdx.x], kWideTraceThreads, hit, wnodes, nodes,
+                                  tris, leafTris, root, ro, rd, inv, a.w, nv, nt, nr))
+            break;
+    hits[2 * (size_t)i] = make_float4(hit.t, 0.0f, hit.u, hit.v);
+    hits[2 * (size_t)i + 1] = make_float4(hit.ng.x, hit.ng.y, hit.ng.z, __uint_as_float(hit.tri));
+    if (kCount) {
+        counts[i] = nv;
+        counts[n + i] = nt;
+        counts[2 * (size_t)n + i] = nr;
+    }
+}
+
+inline bool aligned128(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 127u) == 0; }
+
+}  // namespace
+
+mlbvh_status build_wide(const mlbvh_internal_node* dNodes, const mlbvh_node_index* dRoot, uint32_t n,
+                        mlbvh_wnode* dWide, cudaStream_t stream)
+{
+    if (n == 0) return fail(MLBVH_ERR_INVALID_ARG, "no triangles");
+    if (n == 1) return MLBVH_OK;
+    if (!dNodes || !dRoot || !dWide) return fail(MLBVH_ERR_INVALID_ARG, "null pointer");
+    if (!aligned32(dNodes) || !aligned16(dRoot) || !aligned128(dWide))
+        return fail(MLBVH_ERR_INVALID_ARG, "nodes must be 32-byte and wide nodes 128-byte aligned");
+    const uint32_t m = n - 1;
+    k_wide_collapse<<<(m + kWideThreads - 1) / kWideThreads, kWideThreads, 0, stream>>>(dNodes, m, dWide);
+    MLBVH_CHECK_LAUNCH("k_wide_collapse");
+    return MLBVH_OK;
+}
+
+mlbvh_status trace_wide(const mlbvh_wnode* dWide, const mlbvh_internal_node* dNodes, const mlbvh_node_index* dRoot,
+                        const mlbvh_triangle* dTris, const mlbvh_qtri* dLeafTris, const mlbvh_ray* dRays,
+                        mlbvh_hit* dHits, uint32_t nRays, int rayQuery, uint32_t* dCounts, cudaStream_t stream)
+{
+    if (nRays == 0) return MLBVH_OK;
+    if (rayQuery != MLBVH_RAY_QUERY_ANY) return fail(MLBVH_ERR_INVALID_ARG, "the wide tree takes any-hit rays only");
+    if (!dRoot || !dTris || !dLeafTris || !dRays || !dHits) return fail(MLBVH_ERR_INVALID_ARG, "null pointer");
+    if (!aligned128(dWide) || !aligned32(dNodes) || !aligned16(dRoot) || !aligned16(dTris) || !aligned16(dLeafTris) ||
+        !aligned16(dRays) || !aligned16(dHits) || !aligned16(dCounts))
+        return fail(MLBVH_ERR_INVALID_ARG, "device pointers misaligned (wide nodes 128 B, nodes 32 B, others 16 B)");
+    if (nRays >= (1u << 30) && dCounts) return fail(MLBVH_ERR_INVALID_ARG, "nRays must be below 2^30 with counts");
+    const unsigned blocks = (nRays + kWideTraceThreads - 1) / kWideTraceThreads;
+    const float4* rays = reinterpret_cast<const float4*>(dRays);
+    float4* hits = reinterpret_cast<float4*>(dHits);
+    const float* tris = reinterpret_cast<const float*>(dTris);
+    if (dCounts)
+        k_trace_wide<true><<<blocks, kWideTraceThreads, 0, stream>>>(dWide, dNodes, dRoot, tris, dLeafTris, rays, hits,
+                                                                     nRays, dCounts);
+    else
+        k_trace_wide<false><<<blocks, kWideTraceThreads, 0, stream>>>(dWide, dNodes, dRoot, tris, dLeafTris, rays,
+                                                                      hits, nRays, nullptr);
+    MLBVH_CHECK_LAUNCH("k_trace_wide");
+    return MLBVH_OK;
+}
+
+}  // namespace mlbvh

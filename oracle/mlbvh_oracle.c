@@ -799,6 +799,203 @@ void orc_trace_replay(const orc_node* nodes, const orc_triangle* tris, uint32_t 
     orc_parallel_for(nRays, 1024, trace_range, &c);
 }
 
+/* ------------------------------------------------------- the 4-wide tree */
+/* No reference counterpart: csrc/wide.cu (k_wide_collapse) and
+ * wide_any_step (include/mlbvh_device.cuh). A wide node is 32 words: per
+ * axis a, words 8a..8a+3 the lower and 8a+4..8a+7 the upper bounds of
+ * children 0-3; words 24-27 the children (internal index, leaf position with
+ * bit 31, or 0xFFFFFFFF for an empty slot); 28-31 zero. */
+#define ORC_WIDE_EMPTY 0xFFFFFFFFu
+#define ORC_WIDE_DEPTH 24
+
+typedef struct {
+    uint32_t name;
+    orc_aabb box;
+} wide_kid;
+
+static float wide_area(const orc_aabb* b)
+{
+    float dx = b->upper.x - b->lower.x, dy = b->upper.y - b->lower.y, dz = b->upper.z - b->lower.z;
+    float a = dx * dy;
+    a = a + dy * dz;
+    a = a + dz * dx;
+    return a;
+}
+
+static wide_kid wide_child(const orc_node* nodes, uint32_t p, int side)
+{
+    wide_kid k;
+    uint32_t c = nodes[p].children[side];
+    k.name = is_leaf(c) ? (ORC_LEAF_BIT | (p + (uint32_t)side)) : c;
+    k.box = nodes[p].aabbs[side];
+    return k;
+}
+
+/* Slot i: binary node i's children; twice, the internal child of largest
+ * area (ties: the lower slot) replaced by its two children in place. */
+void orc_build_wide(const orc_node* nodes, uint32_t n, uint32_t* out)
+{
+    for (uint32_t i = 0; i + 1 < n; ++i)
+    {
+        wide_kid kid[4];
+        int count = 2;
+        kid[0] = wide_child(nodes, i, 0);
+        kid[1] = wide_child(nodes, i, 1);
+        for (int round = 0; round < 2; ++round)
+        {
+            int pick = -1;
+            float best = 0.0f;
+            for (int k = 0; k < count; ++k)
+            {
+                if (is_leaf(kid[k].name)) continue;
+                float a = wide_area(&kid[k].box);
+                if (pick < 0 || a > best) { pick = k; best = a; }
+            }
+            if (pick < 0) break;
+            uint32_t p = kid[pick].name;
+            for (int k = count; k > pick + 1; --k) kid[k] = kid[k - 1];
+            kid[pick] = wide_child(nodes, p, 0);
+            kid[pick + 1] = wide_child(nodes, p, 1);
+            ++count;
+        }
+        uint32_t* w = out + 32 * (size_t)i;
+        memset(w, 0, 32 * sizeof(uint32_t));
+        for (int k = 0; k < 4; ++k)
+        {
+            if (k >= count) { w[24 + k] = ORC_WIDE_EMPTY; continue; }
+            const float lo[3] = {kid[k].box.lower.x, kid[k].box.lower.y, kid[k].box.lower.z};
+            const float hi[3] = {kid[k].box.upper.x, kid[k].box.upper.y, kid[k].box.upper.z};
+            for (int a = 0; a < 3; ++a)
+            {
+                memcpy(&w[8 * a + k], &lo[a], 4);
+                memcpy(&w[8 * a + 4 + k], &hi[a], 4);
+            }
+            w[24 + k] = kid[k].name;
+        }
+    }
+}
+
+/* The any-hit walk over the wide tree from `start` (a wide slot or leaf
+ * position; ORC_INVALID: nothing to test). leafIndex maps leaf positions to
+ * triangle indices. Children whose box passes: the nearest entry first (ties
+ * to the lower slot), the others pushed in slot order; a visit whose pushes
+ * would overflow ORC_WIDE_DEPTH entries restarts with the stack-free walk
+ * from binaryRoot. */
+static void trace_wide_any(orc_hit* hit, const uint32_t* wide, const orc_node* nodes, const orc_triangle* tris,
+                           const uint32_t* leafIndex, uint32_t start, uint32_t binaryRoot, orc_f3 ro, orc_f3 rd,
+                           orc_f3 inv, float tmin, uint32_t* visits, uint32_t* tests, uint32_t* restarts)
+{
+    uint32_t stack[ORC_WIDE_DEPTH];
+    int top = 0;
+    uint32_t curr = start;
+    if (start == ORC_INVALID) return;
+    for (;;)
+    {
+        if (is_leaf(curr))
+        {
+            int h;
+            leaf_test(hit, tris, ORC_LEAF_BIT | leafIndex[idx_of(curr)], ro, rd, tmin, &h, tests);
+            if (h) return;
+        }
+        else
+        {
+            (*visits)++;
+            const uint32_t* w = wide + 32 * (size_t)curr;
+            int best = -1, npass = 0, pass[4] = {0, 0, 0, 0};
+            float bestT = 0.0f;
+            for (int k = 0; k < 4; ++k)
+            {
+                if (w[24 + k] == ORC_WIDE_EMPTY) continue;
+                orc_aabb b;
+                memcpy(&b.lower.x, &w[k], 4);
+                memcpy(&b.upper.x, &w[4 + k], 4);
+                memcpy(&b.lower.y, &w[8 + k], 4);
+                memcpy(&b.upper.y, &w[12 + k], 4);
+                memcpy(&b.lower.z, &w[16 + k], 4);
+                memcpy(&b.upper.z, &w[20 + k], 4);
+                float rmin, rmax;
+                slabs(ro, inv, &b, hit->t, &rmin, &rmax);
+                rmin = smax(rmin, tmin);
+                if (rmin <= rmax)
+                {
+                    pass[k] = 1;
+                    ++npass;
+                    if (best < 0 || rmin < bestT) { best = k; bestT = rmin; }
+                }
+            }
+            if (best >= 0)
+            {
+                if (top + npass - 1 > ORC_WIDE_DEPTH)
+                {
+                    (*restarts)++;
+                    stackfree_walk(hit, nodes, tris, binaryRoot, ORC_INVALID, ro, rd, inv, tmin, 1, visits, tests);
+                    return;
+                }
+                for (int k = 0; k < 4; ++k)
+                    if (pass[k] && k != best) stack[top++] = w[24 + k];
+                curr = w[24 + best];
+                continue;
+            }
+        }
+        if (top == 0) return;
+        curr = stack[--top];
+    }
+}
+
+/* leaf position -> triangle index of a built tree (n leaves) */
+static void leaf_positions(const orc_node* nodes, uint32_t n, uint32_t root, uint32_t* leafIndex)
+{
+    if (n == 1) { leafIndex[0] = idx_of(root); return; }
+    for (uint32_t j = 0; j + 1 < n; ++j)
+    {
+        if (is_leaf(nodes[j].children[0])) leafIndex[j] = idx_of(nodes[j].children[0]);
+        if (is_leaf(nodes[j].children[1])) leafIndex[j + 1] = idx_of(nodes[j].children[1]);
+    }
+}
+
+typedef struct {
+    const uint32_t* wide;
+    const orc_node* nodes;
+    const orc_triangle* tris;
+    const uint32_t* leafIndex;
+    uint32_t root;
+    const orc_ray* rays;
+    orc_hit* hits;
+    uint32_t *visits, *tests, *restarts;
+} wide_ctx;
+
+static void wide_range(void* p, uint32_t b, uint32_t e)
+{
+    wide_ctx* c = (wide_ctx*)p;
+    for (uint32_t i = b; i < e; ++i)
+    {
+        const orc_ray* r = &c->rays[i];
+        orc_f3 ro = f3(r->ro[0], r->ro[1], r->ro[2]);
+        orc_f3 rd = f3(r->rd[0], r->rd[1], r->rd[2]);
+        orc_hit hit;
+        hit_init(&hit, r->tmax);
+        uint32_t nv = 0, nt = 0, nr = 0;
+        uint32_t start = is_leaf(c->root) ? ORC_LEAF_BIT : c->root;
+        trace_wide_any(&hit, c->wide, c->nodes, c->tris, c->leafIndex, start, c->root, ro, rd, inv_rd(rd), r->tmin,
+                       &nv, &nt, &nr);
+        c->hits[i] = hit;
+        if (c->visits) c->visits[i] = nv;
+        if (c->tests) c->tests[i] = nt;
+        if (c->restarts) c->restarts[i] = nr;
+    }
+}
+
+void orc_trace_wide(const uint32_t* wide, const orc_node* nodes, const orc_triangle* tris, uint32_t n, uint32_t root,
+                    const orc_ray* rays, uint32_t nRays, orc_hit* hits, uint32_t* visits, uint32_t* tests,
+                    uint32_t* restarts)
+{
+    uint32_t* leafIndex = (uint32_t*)malloc(sizeof(uint32_t) * (n ? n : 1));
+    leaf_positions(nodes, n, root, leafIndex);
+    wide_ctx c = {wide, nodes, tris, leafIndex, root, rays, hits, visits, tests, restarts};
+    orc_parallel_for(nRays, 1024, wide_range, &c);
+    free(leafIndex);
+}
+
 /* ----------------------------------------------------------------- camera */
 /* RayGenerator::lookat (camera.h:10-22) */
 void orc_lookat(orc_f3 eye, orc_f3 center, orc_f3 up, float fovy, int w, int h, orc_camera* cam)

@@ -62,6 +62,8 @@ def oracle() -> ctypes.CDLL:
             "orc_check_tree": (_i32, [_vp, _vp, _u32, _u32]),
             "orc_trace": (None, [_vp, _vp, _u32, _vp, _u32, _i32, _i32, _vp, _vp, _vp]),
             "orc_trace_replay": (None, [_vp, _vp, _u32, _vp, _u32, _i32, _i32, _vp, _vp, _vp]),
+            "orc_build_wide": (None, [_vp, _u32, _vp]),
+            "orc_trace_wide": (None, [_vp, _vp, _vp, _u32, _u32, _vp, _u32, _vp, _vp, _vp, _vp]),
             "orc_lookat": (None, [F3, F3, F3, _f32, _i32, _i32, _vp]),
             "orc_sobol": (None, [_u32, _u32, _u32, _u32, _vp, _vp]),
             "orc_hash_pcg": (_u32, [_u32]),
@@ -179,6 +181,28 @@ def trace_replay(nodes, tris, root, rays, query=0, depth=16, counters=False):
     if counters:
         return hits, nv, nt
     return hits
+
+
+def build_wide(nodes, n):
+    """The 4-wide tree of a built tree: (n - 1, 32) uint32 slots."""
+    out = np.zeros((max(n - 1, 0), 32), np.uint32)
+    if n > 1:
+        oracle().orc_build_wide(P(np.ascontiguousarray(nodes, np.uint32)), n, P(out))
+    return out
+
+
+def trace_wide(wide, nodes, tris, root, rays):
+    """Any-hit rays over the 4-wide tree: hits and per-ray (visits, tests,
+    restarts)."""
+    rays = np.ascontiguousarray(rays, np.float32).reshape(-1, 8)
+    tris = np.ascontiguousarray(tris, np.float32).reshape(-1, 9)
+    n, m = len(tris), rays.shape[0]
+    hits = np.zeros((m, 8), np.uint32)
+    nv, nt, nr = (np.zeros(m, np.uint32) for _ in range(3))
+    wide_c = np.ascontiguousarray(wide, np.uint32) if len(wide) else np.zeros((1, 32), np.uint32)
+    nodes_c = np.ascontiguousarray(nodes, np.uint32) if len(nodes) else np.zeros((1, 16), np.uint32)
+    oracle().orc_trace_wide(P(wide_c), P(nodes_c), P(tris), n, root, P(rays), m, P(hits), P(nv), P(nt), P(nr))
+    return hits, nv, nt, nr
 
 
 def ref_trace(nodes, tris, root, rays, query=0, mode=0):

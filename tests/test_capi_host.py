@@ -142,3 +142,21 @@ def test_batch_scratch_sizes():
         prev = s
     # the 1-mesh batch needs no less than the single-mesh build
     assert L.mlbvh_batch_scratch_bytes(1, 1 << 20) >= L.mlbvh_build_scratch_bytes(1 << 20)
+
+
+def test_wide_entry_points_reject_bad_arguments():
+    L = mb.lib()
+    p, odd = ctypes.c_void_p(256), ctypes.c_void_p(256 + 64)
+    assert L.mlbvh_build_wide(p, p, 0, p, None) == 1  # no triangles
+    assert L.mlbvh_build_wide(p, p, 1, None, None) == 0  # one triangle: no slots, nothing to do
+    assert L.mlbvh_build_wide(p, p, 10, odd, None) == 1  # wide nodes must be 128-byte aligned
+    assert b"aligned" in L.mlbvh_last_error_string()
+    assert L.mlbvh_trace_wide(p, p, p, p, p, p, p, 4, 0, None, None) == 1  # closest hit: not on this tree
+    assert b"any-hit" in L.mlbvh_last_error_string()
+    assert L.mlbvh_trace_wide(odd, p, p, p, p, p, p, 4, 1, None, None) == 1
+    assert L.mlbvh_trace_wide(p, p, p, p, p, p, p, 0, 1, None, None) == 0  # nothing to do
+    cam = (ctypes.c_float * 9)()
+    assert L.mlbvh_render_ao_wide(p, None, 8, 8, ctypes.addressof(cam), p, p, p, odd, p, 1, 16, 1.0, 1, None, p,
+                                  1 << 30, None) == 1
+    assert L.mlbvh_render_ao_wide(p, None, 8, 8, ctypes.addressof(cam), p, p, p, p, None, 1, 16, 1.0, 1, None, p,
+                                  1 << 30, None) == 1

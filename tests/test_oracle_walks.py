@@ -81,3 +81,99 @@ def test_fp32_hit_distances_within_fp64_bound(case):
     assert (r["hits"] > 0 or name == "duplicates") and r["max_bound_ratio"] <= 1.0, r
     rq = F.check_hits(tris, rays, O.trace_quantised(q, rays, 0))
     assert rq == r
+
+
+MISS = 0xFFFFFFFF
+
+
+def _binary_boxes(nodes, n):
+    """Box of every internal node (from its parent) and of every leaf
+    position, as uint32 words."""
+    box_int, box_leaf = {}, {}
+    for j in range(n - 1):
+        for s in (0, 1):
+            c = int(nodes[j, s])
+            box = nodes[j, 2 + 6 * s: 8 + 6 * s]
+            if c & O.LEAF:
+                box_leaf[j + s] = box
+            else:
+                box_int[c] = box
+    return box_int, box_leaf
+
+
+def test_wide_tree_regroups_the_binary_tree(case):
+    """From the root, the wide slots reach every leaf position exactly once,
+    each child with the binary tree's own box, two to four children a slot
+    (non-empty slots first)."""
+    _, tris, b, _, _ = case
+    n = len(tris)
+    wide = O.build_wide(b["nodes"], n)
+    box_int, box_leaf = _binary_boxes(b["nodes"], n)
+    seen = np.zeros(n, np.int64)
+    todo, visited = [int(b["root"])], 0
+    while todo:
+        w = todo.pop()
+        visited += 1
+        kids = wide[w, 24:28]
+        filled = kids != MISS
+        assert filled.sum() >= 2 and (filled[:filled.sum()]).all()
+        assert (wide[w, 28:] == 0).all()
+        for k in np.nonzero(filled)[0]:
+            c = int(kids[k])
+            got = np.array([wide[w, k], wide[w, 8 + k], wide[w, 16 + k], wide[w, 4 + k], wide[w, 12 + k],
+                            wide[w, 20 + k]], np.uint32)
+            ref = box_leaf[c & ~O.LEAF] if c & O.LEAF else box_int[c]
+            np.testing.assert_array_equal(got, ref)
+            if c & O.LEAF:
+                seen[c & ~O.LEAF] += 1
+            else:
+                todo.append(c)
+    assert (seen == 1).all()
+    assert visited < 0.6 * (n - 1)  # about half the binary nodes are slots the walk uses
+
+
+def test_wide_any_hit_equals_stackfree(case):
+    """Any-hit rays over the wide tree hit exactly when the stack-free walk's
+    any-hit rays do, with fewer node visits; every reported hit is a real one."""
+    name, tris, b, _, rays = case
+    n = len(tris)
+    wide = O.build_wide(b["nodes"], n)
+    got, nv, nt, nr = O.trace_wide(wide, b["nodes"], tris, b["root"], rays)
+    ref, nv0, _ = O.trace(b["nodes"], tris, b["root"], rays, 1, 0, counters=True)
+    np.testing.assert_array_equal(got[:, 7] == MISS, ref[:, 7] == MISS)
+    hit = got[:, 7] != MISS
+    t = got[hit, 0].view(np.float32)
+    assert (t >= rays[hit, 3]).all() and (t <= rays[hit, 7]).all()
+    # the reported triangle, tested alone, gives the same t
+    for i in np.nonzero(hit)[0][:50]:
+        one = O.trace(np.zeros((0, 16), np.uint32), tris[got[i, 7]][None], O.LEAF, rays[i][None], 1, 0)
+        assert one[0, 0] == got[i, 0]
+    if name != "duplicates":
+        assert nv.sum() < 0.7 * nv0.sum()
+        assert nr.sum() == 0
+
+
+def test_wide_stack_overflow_restarts_with_stackfree_walk():
+    """Rays parallel to a triangle duplicated 400 times pass all its copies'
+    boxes and miss them all: the wide stack overflows, the ray restarts with
+    the stack-free walk, and hit/miss still equal the stack-free walk's."""
+    base = scenes.gaussian_soup(3, seed=6)
+    tris = np.tile(base, (400, 1))
+    b = O.build(tris)
+    wide = O.build_wide(b["nodes"], len(tris))
+    v = base[0].reshape(3, 3).astype(np.float64)
+    nrm = np.cross(v[1] - v[0], v[2] - v[1])
+    nrm /= np.linalg.norm(nrm)
+    c = v.mean(0)
+    rng = np.random.default_rng(3)
+    rays = np.zeros((64, 8), np.float32)
+    for i in range(64):
+        d = np.cross(nrm, rng.standard_normal(3))
+        d /= np.linalg.norm(d)
+        rays[i, 0:3] = c + nrm * 1e-5 - d * 0.01
+        rays[i, 4:7] = d
+        rays[i, 7] = 0.02
+    got, nv, nt, nr = O.trace_wide(wide, b["nodes"], tris, b["root"], rays)
+    ref = O.trace(b["nodes"], tris, b["root"], rays, 1, 0)
+    np.testing.assert_array_equal(got[:, 7] == MISS, ref[:, 7] == MISS)
+    assert nr.sum() > 0
