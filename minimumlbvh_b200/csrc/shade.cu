@@ -19,6 +19,17 @@ namespace {
 
 constexpr int kTileW = 16, kTileH = 8;  // 128-thread pixel tile: 4 warps of 8 x 4 pixels
 constexpr int kAoThreads = 128;
+
+// Build-time overrides for tuning sweeps (-DMLBVH_AO_START_BATCH=...).
+#ifndef MLBVH_AO_START_BATCH
+#define MLBVH_AO_START_BATCH 8
+#endif
+#ifndef MLBVH_AO_STEPS_PER_ROUND
+#define MLBVH_AO_STEPS_PER_ROUND 3
+#endif
+#ifndef MLBVH_AO_WIDE_STEPS_PER_ROUND
+#define MLBVH_AO_WIDE_STEPS_PER_ROUND 2
+#endif
 constexpr int kFinishThreads = 256;
 
 struct AoRecord {
@@ -278,6 +289,7 @@ struct WideTree {
     };
     static constexpr int kStack = kWideDepth;
     static constexpr int kPrimaryStack = PlainReplayLeafTree::kStack;
+    static constexpr int kSteps = MLBVH_AO_WIDE_STEPS_PER_ROUND;
     __device__ __forceinline__ Ctx context() const
     {
         const uint32_t r = __ldg(binary.rootPtr);
@@ -390,8 +402,18 @@ __global__ void __launch_bounds__(kTileW* kTileH)
 // set-up runs for many lanes at once. An occluded ray adds one to its pixel's
 // count; the lanes of a warp add per pixel with one atomic.
 constexpr int kChunk = 64;
-constexpr int kStartBatch = 8;
-constexpr int kStepsPerRound = 3;
+constexpr int kStartBatch = MLBVH_AO_START_BATCH;
+// Traversal steps per lane between two refill checks: a tree's kSteps (the
+// wide tree's steps are about twice as long), else kStepsPerRound.
+constexpr int kStepsPerRound = MLBVH_AO_STEPS_PER_ROUND;
+template <class Tree, class = void>
+struct StepsOf {
+    static constexpr int value = kStepsPerRound;
+};
+template <class Tree>
+struct StepsOf<Tree, decltype((void)Tree::kSteps)> {
+    static constexpr int value = Tree::kSteps;
+};
 
 template <class Tree, bool kCount>
 __global__ void __launch_bounds__(kAoThreads, 8)  // at most 64 registers: 32 warps per SM
@@ -470,11 +492,11 @@ __global__ void __launch_bounds__(kAoThreads, 8)  // at most 64 registers: 32 wa
             if (exhausted) break;
             continue;
         }
-        // up to kStepsPerRound steps per loop iteration: the refill and vote
+        // up to StepsOf<Tree> steps per loop iteration: the refill and vote
         // overhead of an iteration is shared by several steps
         bool occluded = false;
 #pragma unroll
-        for (int rep = 0; rep < kStepsPerRound; ++rep)
+        for (int rep = 0; rep < StepsOf<Tree>::value; ++rep)
             if (live) {
                 if (tree.template step<true, kCount>(ctx, curr, prev, depth, stack, hit, origin, dir, inv, cnt) ||
                     ++steps >= kMaxTraversalSteps) {
