@@ -484,8 +484,24 @@ def main():
             mb.render_ao_wide(pixels, (w, h), cam, wide, 1, wl["ns"], wl["radius"], 12345, occluded=occluded,
                               stats=stats)
 
+        # its 8-bit quantised slots (64 bytes instead of 128)
+        wide.quantise()
+        qev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+        for i in range(args.steps):
+            qev[i][0].record(stream)
+            wide.quantise(stream)
+            qev[i][1].record(stream)
+        torch.cuda.synchronize()
+        wide_quant_ms = float(np.mean([a.elapsed_time(b) for a, b in qev]))
+        quant_status = int(wide.status[0].item())
+
+        def wide_quantised_frame(occluded=None, stats=None):
+            mb.render_ao_wide(pixels, (w, h), cam, wide, 1, wl["ns"], wl["radius"], 12345, occluded=occluded,
+                              stats=stats, quantised=True)
+
         forms = {}
-        for name, frame in (("replay", replay_frame), ("quantised", quantised_frame), ("wide", wide_frame)):
+        for name, frame in (("replay", replay_frame), ("quantised", quantised_frame), ("wide", wide_frame),
+                            ("wide_quantised", wide_quantised_frame)):
             occ = torch.empty_like(occ_plain)
             fst = torch.zeros(8, dtype=torch.int64, device=dev)
             frame(occluded=occ, stats=fst)
@@ -554,7 +570,8 @@ def main():
                    "ao_rays": ao_rays, "parallelism": "replicas" if world > 1 else "single GPU",
                    "l2": "inputs larger than L2 (nodes + triangles 419 MB)" if wl["scene"] == "soup"
                    else "L2 flushed (256 MB write) between timed frames"},
-        "gpu_launches": args.steps * (3 + 3 + 3 + 3 + 2 + 7 + 10),  # AO, replay, quantised, wide AO, wide prep,
+        "gpu_launches": args.steps * (3 + 3 + 3 + 3 + 3 + 2 + 1 + 7 + 10),  # AO, replay, quantised, wide, wide
+        # quantised AO, wide prep, quantisation,
         # build, e2e steps
         "clocks": clocks,
     }
@@ -582,6 +599,8 @@ def main():
         "quantised": "quantised 8-bit child boxes (32-byte nodes), replay walk",
         "wide": "AO rays over the 4-wide regrouping of the FP32 tree (128-byte nodes, any-hit), "
                 "primary rays on the replay walk, leaf-ordered 48-byte triangles",
+        "wide_quantised": "AO rays over the 4-wide tree with 8-bit child planes rounded outward (64-byte nodes, "
+                          "any-hit, exact leaf-box check on hits), primary rays on the replay walk",
     }
     for name, (total_s, agree, fst) in forms.items():
         f_rays = int(fst[0])
@@ -589,8 +608,8 @@ def main():
             node_bytes = 64 * int(fst[1])
         elif name == "quantised":
             node_bytes = 32 * int(fst[1]) + 4 * int(fst[5])
-        else:  # primary rays visit 64-byte binary nodes, AO rays 128-byte wide nodes
-            node_bytes = 64 * (int(fst[1]) - int(fst[3])) + 128 * int(fst[3])
+        else:  # primary rays visit 64-byte binary nodes, AO rays 128-byte (64-byte quantised) wide nodes
+            node_bytes = 64 * (int(fst[1]) - int(fst[3])) + (128 if name == "wide" else 64) * int(fst[3])
         tri_bytes = 48 * int(fst[2])
         form_lines[name] = {
             "form": form_desc[name],
@@ -602,6 +621,10 @@ def main():
         if name == "wide":
             form_lines[name]["prep_ms_per_build"] = wide_prep_ms
             form_lines[name]["restarts"] = int(fst[6])
+        if name == "wide_quantised":
+            form_lines[name]["prep_ms_per_build"] = wide_prep_ms + wide_quant_ms
+            form_lines[name]["restarts"] = int(fst[6])
+            form_lines[name]["quantisation_status"] = quant_status
     exact = [k for k, v in form_lines.items() if v["occlusion_agreement"] == 1.0]
     best = max(exact, key=lambda k: form_lines[k]["value"]) if exact else None
     line["chosen"] = dict(form_lines[best]) if best else {"form": None, "note": "no form agreed with the plain one"}

@@ -139,6 +139,18 @@ typedef struct mlbvh_wnode {
     uint32_t _pad[4];  /* zero */
 } mlbvh_wnode;         /* 128 bytes, 128-byte aligned */
 
+/* The 4-wide tree with 8-bit child planes (no reference counterpart): the
+ * slots of mlbvh_wnode in 64 bytes. Per axis a, a base and a power of two
+ * scale; plane code q stands for base[a] + scale[a] * (1 + q / 32768). Lower
+ * plane codes are rounded down and upper ones up (and decoded with the same
+ * directed rounding), so a decoded child box contains the exact one. */
+typedef struct mlbvh_qwnode {
+    float base[3];
+    float scale[3];
+    uint8_t q[3][2][4]; /* q[a][0][c], q[a][1][c]: lower, upper plane of child c on axis a */
+    uint32_t child[4];  /* as in mlbvh_wnode */
+} mlbvh_qwnode;         /* 64 bytes, 32-byte aligned */
+
 /* Library version (MLBVH_VERSION) and the message of the last error raised on
  * the calling host thread ("" if none). */
 MLBVH_API int mlbvh_version(void);
@@ -380,6 +392,32 @@ MLBVH_API mlbvh_status mlbvh_trace_wide(const mlbvh_wnode* dWideNodes, const mlb
                                         const mlbvh_node_index* dRootNode, const mlbvh_triangle* dTriangles,
                                         const mlbvh_qtri* dLeafTriangles, const mlbvh_ray* dRays, mlbvh_hit* dHits,
                                         uint32_t nRays, int rayQuery, uint32_t* dCounts, void* stream);
+/* The quantised slots of a 4-wide tree: nTriangles - 1 mlbvh_qwnode (none for
+ * one triangle), 32-byte aligned, from the FP32 slots of mlbvh_build_wide.
+ * *dStatus (one device word) becomes 0 when every slot was quantised, 1 when
+ * one could not be (non-finite planes, or extents beyond about 1e36); the
+ * quantised walks then take the stack-free walk over the binary tree for
+ * every ray (the same answers, slower). No reference counterpart. */
+MLBVH_API mlbvh_status mlbvh_quantise_wide(const mlbvh_wnode* dWideNodes, uint32_t nTriangles,
+                                           mlbvh_qwnode* dQWideNodes, uint32_t* dStatus, void* stream);
+/* mlbvh_trace_wide over the quantised slots (any-hit only; a hit counts only
+ * where the triangle's exact box passes the slab test as well). */
+MLBVH_API mlbvh_status mlbvh_trace_wide_quantised(const mlbvh_qwnode* dQWideNodes, const uint32_t* dStatus,
+                                                  const mlbvh_internal_node* dInternals,
+                                                  const mlbvh_node_index* dRootNode, const mlbvh_triangle* dTriangles,
+                                                  const mlbvh_qtri* dLeafTriangles, const mlbvh_ray* dRays,
+                                                  mlbvh_hit* dHits, uint32_t nRays, int rayQuery, uint32_t* dCounts,
+                                                  void* stream);
+/* mlbvh_render_ao_wide over the quantised slots (the same occlusion counts). */
+MLBVH_API mlbvh_status mlbvh_render_ao_wide_quantised(uint32_t* dPixels, uint32_t* dOccluded, int width, int height,
+                                                      const mlbvh_ray_generator* camera,
+                                                      const mlbvh_node_index* dRootNode,
+                                                      const mlbvh_internal_node* dInternals,
+                                                      const mlbvh_triangle* dTriangles,
+                                                      const mlbvh_qwnode* dQWideNodes, const uint32_t* dStatus,
+                                                      const mlbvh_qtri* dLeafTriangles, int useSobol, int nSamples,
+                                                      float radius, uint32_t sobolSeed, unsigned long long* dStats,
+                                                      void* dScratch, size_t scratchBytes, void* stream);
 /* mlbvh_render_ao with the AO rays over the 4-wide tree (any-hit, so every
  * occlusion count is mlbvh_render_ao's) and the primary rays on the replay
  * walk over the binary tree (the stack-free walk's Hit records). AO rays of a

@@ -152,16 +152,22 @@ __device__ __forceinline__ f3 inv_rd(f3 rd)
 // entry is clipped to tmin (0 in the reference) and the exit, inflated by
 // 1.00000024, to knownHitT. Only the sign of a zero can differ between
 // fminf/fmaxf and the host selects here, and no comparison below sees it.
-__device__ __forceinline__ float2 slab(f3 ro, f3 inv, f3 lo, f3 hi, float tmin, float knownHitT)
+// slab_offsets takes the planes already relative to the ray origin (lo - ro,
+// hi - ro); slab is slab_offsets(lo - ro, hi - ro, ...), the same operations.
+__device__ __forceinline__ float2 slab_offsets(f3 dlo, f3 dhi, f3 inv, float tmin, float knownHitT)
 {
-    f3 t0 = (lo - ro) * inv;
-    f3 t1 = (hi - ro) * inv;
+    f3 t0 = dlo * inv;
+    f3 t1 = dhi * inv;
     float rmin = fmaxf(fmaxf(fminf(t0.x, t1.x), fminf(t0.y, t1.y)), fminf(t0.z, t1.z));
     float rmax = fminf(fminf(fmaxf(t0.x, t1.x), fmaxf(t0.y, t1.y)), fmaxf(t0.z, t1.z)) * 1.00000024f;
     rmin = fmaxf(rmin, 0.0f);
     rmin = fmaxf(rmin, tmin);
     rmax = fminf(rmax, knownHitT);
     return make_float2(rmin, rmax);
+}
+__device__ __forceinline__ float2 slab(f3 ro, f3 inv, f3 lo, f3 hi, float tmin, float knownHitT)
+{
+    return slab_offsets(lo - ro, hi - ro, inv, tmin, knownHitT);
 }
 
 struct HitRecord {
@@ -452,102 +458,6 @@ __device__ __forceinline__ bool stackfree_replay_step_lo(uint32_t& curr, uint32_
         }
         return true;
     }
-}
-
-// ------------------------------------------------------- the 4-wide tree
-// mlbvh_wnode (include/mlbvh.h): slot i is the expansion of binary internal
-// node i into at most four children with the binary tree's own boxes. Only
-// any-hit rays walk it: a leaf whose box passes the slab test is reached
-// through boxes that contain it and therefore pass too (the slab test is
-// monotone in the box: every operation rounds to nearest, which preserves
-// order), and only leaves whose own box passes are tested, so a ray finds a
-// hit exactly when intersect_stackfree's any-hit walk does.
-constexpr uint32_t kWideEmpty = 0xFFFFFFFFu;  // an empty child slot
-constexpr int kWideDepth = 24;                // stack entries per ray
-
-__device__ __forceinline__ float wpick(const float4& v, int k)
-{
-    return k == 0 ? v.x : k == 1 ? v.y : k == 2 ? v.z : v.w;
-}
-__device__ __forceinline__ uint32_t wpick(const uint4& v, int k)
-{
-    return k == 0 ? v.x : k == 1 ? v.y : k == 2 ? v.z : v.w;
-}
-
-// One step of the any-hit walk over the wide tree: a leaf test (leaf-ordered
-// triangles) or a wide-node visit. At a node, every non-empty child whose box
-// passes the slab test is taken: the nearest entry first (ties to the lower
-// slot), the others pushed in slot order. A node whose pushes would overflow
-// the stack (kWideDepth entries, shared memory, `stride` apart) restarts the
-// ray with the stack-free walk over the binary tree from `binaryRoot`
-// (depth < 0 from then on; ++nr). Returns true when the walk is over (a hit,
-// or nothing left).
-template <bool kCount>
-__device__ __forceinline__ bool wide_any_step(uint32_t& curr, uint32_t& prev, int& depth, uint32_t* stack, int stride,
-                                              HitRecord& hit, const mlbvh_wnode* __restrict__ wnodes,
-                                              const mlbvh_internal_node* __restrict__ nodes,
-                                              const float* __restrict__ tris, const mlbvh_qtri* __restrict__ leafTris,
-                                              uint32_t binaryRoot, f3 ro, f3 rd, f3 inv, float tmin, uint32_t& nv,
-                                              uint32_t& nt, uint32_t& nr)
-{
-    if (depth < 0) return stackfree_step<true, kCount, true>(curr, prev, hit, nodes, tris, ro, rd, inv, tmin, nv, nt);
-    if (curr & kLeafBit) {
-        if (kCount) ++nt;
-        const float4* t = reinterpret_cast<const float4*>(leafTris + (curr & ~kLeafBit));
-        const float4 a = __ldg(t), b = __ldg(t + 1), c = __ldg(t + 2);
-        float tt, u, v;
-        f3 ng;
-        if (intersect_triangle(tt, u, v, ng, tmin, hit.t, ro, rd, mk(a.x, a.y, a.z), mk(a.w, b.x, b.y),
-                               mk(b.z, b.w, c.x))) {
-            hit.t = tt;
-            hit.u = u;
-            hit.v = v;
-            hit.ng = ng;
-            hit.tri = __float_as_uint(c.y);
-            return true;
-        }
-    } else {
-        if (kCount) ++nv;
-        const float4* p = reinterpret_cast<const float4*>(wnodes + curr);
-        float4 lx, hx, ly, hy, lz, hz;
-        ldg32(p, lx, hx);
-        ldg32(p + 2, ly, hy);
-        ldg32(p + 4, lz, hz);
-        const uint4 ch = __ldg(reinterpret_cast<const uint4*>(p + 6));
-        uint32_t pass = 0;
-        int best = -1;
-        float bestT = 0.0f;
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            const float2 r = slab(ro, inv, mk(wpick(lx, k), wpick(ly, k), wpick(lz, k)),
-                                  mk(wpick(hx, k), wpick(hy, k), wpick(hz, k)), tmin, hit.t);
-            if (wpick(ch, k) != kWideEmpty && r.x <= r.y) {
-                pass |= 1u << k;
-                if (best < 0 || r.x < bestT) {
-                    best = k;
-                    bestT = r.x;
-                }
-            }
-        }
-        if (pass) {
-            const uint32_t others = pass & ~(1u << best);
-            if (depth + __popc(others) > kWideDepth) {
-                if (kCount) ++nr;
-                depth = -1;
-                curr = binaryRoot;
-                prev = kInvalid;
-                return false;
-            }
-#pragma unroll
-            for (int k = 0; k < 4; ++k)
-                if (others & (1u << k)) stack[depth++ * stride] = wpick(ch, k);
-            curr = wpick(ch, best);
-            return false;
-        }
-    }
-    if (depth == 0) return true;
-    curr = stack[--depth * stride];
-    return false;
 }
 
 template <bool kAny, bool kCount = false, bool kWide = false>
@@ -1116,6 +1026,168 @@ __device__ __forceinline__ void trace_quantised(HitRecord& hit, const mlbvh_qnod
         *tests += nt;
         *ups += nu;
     }
+}
+
+
+// ------------------------------------------------------- the 4-wide tree
+// mlbvh_wnode / mlbvh_qwnode (include/mlbvh.h): slot i is the expansion of
+// binary internal node i into at most four children with the binary tree's
+// own boxes (mlbvh_wnode), or those boxes with 8-bit planes rounded outward
+// (mlbvh_qwnode). Only any-hit rays walk it: a leaf whose box passes the
+// slab test is reached through boxes that contain it and therefore pass too
+// (the slab test is monotone in the box: every operation rounds to nearest,
+// which preserves order), and only leaves whose own box passes are tested (on
+// the quantised slots, a hit counts only if the leaf's exact box passes,
+// leaf_box_passes), so a ray finds a hit exactly when intersect_stackfree's
+// any-hit walk does.
+constexpr uint32_t kWideEmpty = 0xFFFFFFFFu;  // an empty child slot
+constexpr int kWideDepth = 24;                // stack entries per ray
+
+__device__ __forceinline__ float wpick(const float4& v, int k)
+{
+    return k == 0 ? v.x : k == 1 ? v.y : k == 2 ? v.z : v.w;
+}
+__device__ __forceinline__ uint32_t wpick(const uint4& v, int k)
+{
+    return k == 0 ? v.x : k == 1 ? v.y : k == 2 ? v.z : v.w;
+}
+
+// One visit: which non-empty children pass (bit mask), the nearest of them
+// (entry distance, ties to the lower slot; -1 if none) and the child words.
+struct WideVisit {
+    uint32_t pass;
+    int best;
+    uint4 ch;
+};
+// FP32 slot: three 32-byte plane loads and the 16-byte child words.
+__device__ __forceinline__ WideVisit wide_visit(const mlbvh_wnode* __restrict__ wnodes, uint32_t i, f3 ro, f3 inv,
+                                                float tmin, float hitT)
+{
+    const float4* p = reinterpret_cast<const float4*>(wnodes + i);
+    float4 lx, hx, ly, hy, lz, hz;
+    ldg32(p, lx, hx);
+    ldg32(p + 2, ly, hy);
+    ldg32(p + 4, lz, hz);
+    WideVisit w{0u, -1, __ldg(reinterpret_cast<const uint4*>(p + 6))};
+    float bestT = 0.0f;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const float2 r = slab(ro, inv, mk(wpick(lx, k), wpick(ly, k), wpick(lz, k)),
+                              mk(wpick(hx, k), wpick(hy, k), wpick(hz, k)), tmin, hitT);
+        if (wpick(w.ch, k) != kWideEmpty && r.x <= r.y) {
+            w.pass |= 1u << k;
+            if (w.best < 0 || r.x < bestT) {
+                w.best = k;
+                bestT = r.x;
+            }
+        }
+    }
+    return w;
+}
+
+// Quantised slot (two 32-byte loads). Plane code q of axis a stands for
+// base[a] + scale[a] * (1 + q / 2^15): one byte permute writes q into
+// mantissa byte 1 of the power of two scale[a]. Relative to the ray origin,
+// lower planes are base - ro rounded down plus that value rounded down, upper
+// planes the same rounded up, so they lie at or outside the exact planes (the
+// codes were rounded outward too) and the slab test on them passes wherever
+// it passes on the exact box.
+__device__ __forceinline__ float qw_value(uint32_t codes, uint32_t scaleBits, int k)
+{
+    return __uint_as_float(__byte_perm(codes, scaleBits, 0x7604u | ((uint32_t)k << 4)));
+}
+__device__ __forceinline__ WideVisit qwide_visit(const mlbvh_qwnode* __restrict__ qw, uint32_t i, f3 ro, f3 inv,
+                                                 float tmin, float hitT)
+{
+    const float4* p = reinterpret_cast<const float4*>(qw + i);
+    float4 a, b, c, d;
+    ldg32(p, a, b);
+    ldg32(p + 2, c, d);
+    const f3 dlo = mk(__fsub_rd(a.x, ro.x), __fsub_rd(a.y, ro.y), __fsub_rd(a.z, ro.z));
+    const f3 dhi = mk(__fsub_ru(a.x, ro.x), __fsub_ru(a.y, ro.y), __fsub_ru(a.z, ro.z));
+    const uint32_t sx = __float_as_uint(a.w), sy = __float_as_uint(b.x), sz = __float_as_uint(b.y);
+    const uint32_t qxl = __float_as_uint(b.z), qxh = __float_as_uint(b.w), qyl = __float_as_uint(c.x),
+                   qyh = __float_as_uint(c.y), qzl = __float_as_uint(c.z), qzh = __float_as_uint(c.w);
+    WideVisit w{0u, -1, make_uint4(__float_as_uint(d.x), __float_as_uint(d.y), __float_as_uint(d.z),
+                                   __float_as_uint(d.w))};
+    float bestT = 0.0f;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const f3 lo = mk(__fadd_rd(dlo.x, qw_value(qxl, sx, k)), __fadd_rd(dlo.y, qw_value(qyl, sy, k)),
+                         __fadd_rd(dlo.z, qw_value(qzl, sz, k)));
+        const f3 hi = mk(__fadd_ru(dhi.x, qw_value(qxh, sx, k)), __fadd_ru(dhi.y, qw_value(qyh, sy, k)),
+                         __fadd_ru(dhi.z, qw_value(qzh, sz, k)));
+        const float2 r = slab_offsets(lo, hi, inv, tmin, hitT);
+        if (wpick(w.ch, k) != kWideEmpty && r.x <= r.y) {
+            w.pass |= 1u << k;
+            if (w.best < 0 || r.x < bestT) {
+                w.best = k;
+                bestT = r.x;
+            }
+        }
+    }
+    return w;
+}
+
+// One step of the any-hit walk over the wide tree (FP32 slots, or quantised
+// slots with kQuant): a leaf test (leaf-ordered triangles) or a slot visit.
+// At a slot, every non-empty child whose box passes is taken: the nearest
+// entry first, the others pushed in slot order. A visit whose pushes would
+// overflow the stack (kWideDepth entries, shared memory, `stride` apart)
+// restarts the ray with the stack-free walk over the binary tree from
+// `binaryRoot` (depth < 0 from then on; ++nr). Returns true when the walk is
+// over (a hit, or nothing left).
+template <bool kCount, bool kQuant, class Slot>
+__device__ __forceinline__ bool wide_any_step(uint32_t& curr, uint32_t& prev, int& depth, uint32_t* stack, int stride,
+                                              HitRecord& hit, const Slot* __restrict__ slots,
+                                              const mlbvh_internal_node* __restrict__ nodes,
+                                              const float* __restrict__ tris, const mlbvh_qtri* __restrict__ leafTris,
+                                              uint32_t binaryRoot, f3 ro, f3 rd, f3 inv, float tmin, uint32_t& nv,
+                                              uint32_t& nt, uint32_t& nr)
+{
+    if (depth < 0) return stackfree_step<true, kCount, true>(curr, prev, hit, nodes, tris, ro, rd, inv, tmin, nv, nt);
+    if (curr & kLeafBit) {
+        if (kCount) ++nt;
+        const float4* t = reinterpret_cast<const float4*>(leafTris + (curr & ~kLeafBit));
+        const float4 a = __ldg(t), b = __ldg(t + 1), c = __ldg(t + 2);
+        const f3 v0 = mk(a.x, a.y, a.z), v1 = mk(a.w, b.x, b.y), v2 = mk(b.z, b.w, c.x);
+        float tt, u, v;
+        f3 ng;
+        if (intersect_triangle(tt, u, v, ng, tmin, hit.t, ro, rd, v0, v1, v2) &&
+            (!kQuant || leaf_box_passes(ro, inv, v0, v1, v2, tmin, hit.t))) {
+            hit.t = tt;
+            hit.u = u;
+            hit.v = v;
+            hit.ng = ng;
+            hit.tri = __float_as_uint(c.y);
+            return true;
+        }
+    } else {
+        if (kCount) ++nv;
+        WideVisit w;
+        if constexpr (kQuant)
+            w = qwide_visit(slots, curr, ro, inv, tmin, hit.t);
+        else
+            w = wide_visit(slots, curr, ro, inv, tmin, hit.t);
+        if (w.pass) {
+            const uint32_t others = w.pass & ~(1u << w.best);
+            if (depth + __popc(others) > kWideDepth) {
+                if (kCount) ++nr;
+                depth = -1;
+                curr = binaryRoot;
+                prev = kInvalid;
+                return false;
+            }
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+                if (others & (1u << k)) stack[depth++ * stride] = wpick(w.ch, k);
+            curr = wpick(w.ch, w.best);
+            return false;
+        }
+    }
+    if (depth == 0) return true;
+    curr = stack[--depth * stride];
+    return false;
 }
 
 }  // namespace mlbvh

@@ -84,6 +84,10 @@ def lib() -> ctypes.CDLL:
             "mlbvh_trace_wide": (i32, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, u32, i32, _vp, _vp]),
             "mlbvh_render_ao_wide": (i32, [_vp, _vp, i32, i32, _vp, _vp, _vp, _vp, _vp, _vp, i32, i32, f32, u32, _vp,
                                            _vp, sz, _vp]),
+            "mlbvh_quantise_wide": (i32, [_vp, u32, _vp, _vp, _vp]),
+            "mlbvh_trace_wide_quantised": (i32, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, u32, i32, _vp, _vp]),
+            "mlbvh_render_ao_wide_quantised": (i32, [_vp, _vp, i32, i32, _vp, _vp, _vp, _vp, _vp, _vp, _vp, i32, i32,
+                                                     f32, u32, _vp, _vp, sz, _vp]),
             "mlbvh_obj_load": (i32, [ctypes.c_char_p, _vp]),
             "mlbvh_obj_triangle_count": (u32, [_vp]),
             "mlbvh_obj_triangles": (_vp, [_vp]),
@@ -363,6 +367,19 @@ class WideBVH:
 
     def __init__(self, builder: "BVHGPUBuilder", triangles, wide, leaf_tris):
         self.builder, self.triangles, self.wide, self.leaf_triangles = builder, triangles, wide, leaf_tris
+        self.qwide = None   # quantised slots (quantise())
+        self.status = None  # int32 device word: 1 when a slot could not be quantised
+
+    def quantise(self, stream=None) -> "WideBVH":
+        """The 64-byte quantised slots (mlbvh_quantise_wide), kept beside the
+        FP32 ones."""
+        import torch
+        n = self.builder.m_nTriangles
+        if self.qwide is None:
+            self.qwide = torch.empty((max(n - 1, 1), 16), dtype=torch.int32, device=self.wide.device)
+            self.status = torch.zeros(4, dtype=torch.int32, device=self.wide.device)
+        _check(lib().mlbvh_quantise_wide(_ptr(self.wide), n, _ptr(self.qwide), _ptr(self.status), _stream(stream)))
+        return self
 
     @classmethod
     def from_builder(cls, builder: "BVHGPUBuilder", triangles, stream=None) -> "WideBVH":
@@ -380,38 +397,56 @@ class WideBVH:
         _check(lib().mlbvh_build_wide(_ptr(self.builder.m_internals), _ptr(self.builder.m_rootNode), n,
                                       _ptr(self.wide), _stream(stream)))
         leaf_triangles(self.builder, self.triangles, out=self.leaf_triangles, stream=stream)
+        if self.qwide is not None:
+            self.quantise(stream)
         return self
 
 
-def intersect_wide(w: WideBVH, rays, hits=None, counts=None, stream=None):
-    """Any-hit rays over the 4-wide tree (mlbvh_trace_wide). ``counts``
-    (int32 CUDA tensor of 3 * nRays) receives per-ray node visits, triangle
-    tests and restarts."""
+def intersect_wide(w: WideBVH, rays, hits=None, counts=None, stream=None, quantised: bool = False):
+    """Any-hit rays over the 4-wide tree (mlbvh_trace_wide, or with
+    ``quantised`` mlbvh_trace_wide_quantised over ``w.quantise()``'s slots).
+    ``counts`` (int32 CUDA tensor of 3 * nRays) receives per-ray node visits,
+    triangle tests and restarts."""
     import torch
     _require_cuda(rays, "rays")
     n = rays.numel() // 8
     if hits is None:
         hits = torch.empty((n, 8), dtype=torch.int32, device=rays.device)
     b = w.builder
-    _check(lib().mlbvh_trace_wide(_ptr(w.wide), _ptr(b.m_internals), _ptr(b.m_rootNode), _ptr(w.triangles),
-                                  _ptr(w.leaf_triangles), _ptr(rays), _ptr(hits), n, RAY_QUERY_ANY, _ptr(counts),
-                                  _stream(stream)))
+    if quantised:
+        _check(lib().mlbvh_trace_wide_quantised(_ptr(w.qwide), _ptr(w.status), _ptr(b.m_internals),
+                                                _ptr(b.m_rootNode), _ptr(w.triangles), _ptr(w.leaf_triangles),
+                                                _ptr(rays), _ptr(hits), n, RAY_QUERY_ANY, _ptr(counts),
+                                                _stream(stream)))
+    else:
+        _check(lib().mlbvh_trace_wide(_ptr(w.wide), _ptr(b.m_internals), _ptr(b.m_rootNode), _ptr(w.triangles),
+                                      _ptr(w.leaf_triangles), _ptr(rays), _ptr(hits), n, RAY_QUERY_ANY, _ptr(counts),
+                                      _stream(stream)))
     return hits
 
 
 def render_ao_wide(pixels, imageSize, rayGenerator: RayGenerator, w: WideBVH, useSobol: int = 1,
                    nSamples: int = 16, radius: float = 1.0, seed: int = 12345, occluded=None, stats=None,
-                   scratch=None, stream=None):
+                   scratch=None, stream=None, quantised: bool = False):
     """render_ao with the AO rays over the 4-wide tree (same occlusion
-    counts) and primary rays on the replay walk (the same Hit records)."""
+    counts; ``quantised``: over ``w.quantise()``'s 64-byte slots) and primary
+    rays on the replay walk (the same Hit records)."""
     width, height = imageSize
     scratch = _ao_scratch(pixels, width, height, scratch)
     cam = rayGenerator._cstruct()
     b = w.builder
-    _check(lib().mlbvh_render_ao_wide(_ptr(pixels), _ptr(occluded), int(width), int(height), ctypes.addressof(cam),
-                                      _ptr(b.m_rootNode), _ptr(b.m_internals), _ptr(w.triangles), _ptr(w.wide),
-                                      _ptr(w.leaf_triangles), int(useSobol), int(nSamples), float(radius), int(seed),
-                                      _ptr(stats), _ptr(scratch), scratch.numel(), _stream(stream)))
+    if quantised:
+        _check(lib().mlbvh_render_ao_wide_quantised(
+            _ptr(pixels), _ptr(occluded), int(width), int(height), ctypes.addressof(cam), _ptr(b.m_rootNode),
+            _ptr(b.m_internals), _ptr(w.triangles), _ptr(w.qwide), _ptr(w.status), _ptr(w.leaf_triangles),
+            int(useSobol), int(nSamples), float(radius), int(seed), _ptr(stats), _ptr(scratch), scratch.numel(),
+            _stream(stream)))
+    else:
+        _check(lib().mlbvh_render_ao_wide(_ptr(pixels), _ptr(occluded), int(width), int(height),
+                                          ctypes.addressof(cam), _ptr(b.m_rootNode), _ptr(b.m_internals),
+                                          _ptr(w.triangles), _ptr(w.wide), _ptr(w.leaf_triangles), int(useSobol),
+                                          int(nSamples), float(radius), int(seed), _ptr(stats), _ptr(scratch),
+                                          scratch.numel(), _stream(stream)))
     return pixels
 
 

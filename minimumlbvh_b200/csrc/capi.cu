@@ -166,6 +166,39 @@ mlbvh_status mlbvh_render_ao_wide(uint32_t* dPixels, uint32_t* dOccluded, int wi
                           as_stream(stream));
 }
 
+mlbvh_status mlbvh_quantise_wide(const mlbvh_wnode* dWideNodes, uint32_t nTriangles, mlbvh_qwnode* dQWideNodes,
+                                 uint32_t* dStatus, void* stream)
+{
+    clear_error();
+    return quantise_wide(dWideNodes, nTriangles, dQWideNodes, dStatus, as_stream(stream));
+}
+
+mlbvh_status mlbvh_trace_wide_quantised(const mlbvh_qwnode* dQWideNodes, const uint32_t* dStatus,
+                                        const mlbvh_internal_node* dInternals, const mlbvh_node_index* dRootNode,
+                                        const mlbvh_triangle* dTriangles, const mlbvh_qtri* dLeafTriangles,
+                                        const mlbvh_ray* dRays, mlbvh_hit* dHits, uint32_t nRays, int rayQuery,
+                                        uint32_t* dCounts, void* stream)
+{
+    clear_error();
+    return trace_wide_quantised(dQWideNodes, dStatus, dInternals, dRootNode, dTriangles, dLeafTriangles, dRays, dHits,
+                                nRays, rayQuery, dCounts, as_stream(stream));
+}
+
+mlbvh_status mlbvh_render_ao_wide_quantised(uint32_t* dPixels, uint32_t* dOccluded, int width, int height,
+                                            const mlbvh_ray_generator* camera, const mlbvh_node_index* dRootNode,
+                                            const mlbvh_internal_node* dInternals, const mlbvh_triangle* dTriangles,
+                                            const mlbvh_qwnode* dQWideNodes, const uint32_t* dStatus,
+                                            const mlbvh_qtri* dLeafTriangles, int useSobol, int nSamples,
+                                            float radius, uint32_t sobolSeed, unsigned long long* dStats,
+                                            void* dScratch, size_t scratchBytes, void* stream)
+{
+    clear_error();
+    if (!camera) return fail(MLBVH_ERR_INVALID_ARG, "null camera");
+    return render_ao_wide_quantised(dPixels, dOccluded, width, height, *camera, dRootNode, dInternals, dTriangles,
+                                    dQWideNodes, dStatus, dLeafTriangles, useSobol, nSamples, radius, sobolSeed,
+                                    dStats, dScratch, scratchBytes, as_stream(stream));
+}
+
 mlbvh_status mlbvh_render_pt(float* dAccumulators, int width, int height, const mlbvh_ray_generator* camera,
                              const mlbvh_node_index* dRootNode, const mlbvh_internal_node* dInternals,
                              const mlbvh_triangle* dTriangles, const mlbvh_triangle_attrib* dAttribs, int useSobol,

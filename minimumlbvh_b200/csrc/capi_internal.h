@@ -58,6 +58,20 @@ mlbvh_status build_wide(const mlbvh_internal_node* dNodes, const mlbvh_node_inde
 mlbvh_status trace_wide(const mlbvh_wnode* dWide, const mlbvh_internal_node* dNodes, const mlbvh_node_index* dRoot,
                         const mlbvh_triangle* dTris, const mlbvh_qtri* dLeafTris, const mlbvh_ray* dRays,
                         mlbvh_hit* dHits, uint32_t nRays, int rayQuery, uint32_t* dCounts, cudaStream_t stream);
+mlbvh_status quantise_wide(const mlbvh_wnode* dWide, uint32_t n, mlbvh_qwnode* dQWide, uint32_t* dStatus,
+                           cudaStream_t stream);
+mlbvh_status trace_wide_quantised(const mlbvh_qwnode* dQWide, const uint32_t* dStatus,
+                                  const mlbvh_internal_node* dNodes, const mlbvh_node_index* dRoot,
+                                  const mlbvh_triangle* dTris, const mlbvh_qtri* dLeafTris, const mlbvh_ray* dRays,
+                                  mlbvh_hit* dHits, uint32_t nRays, int rayQuery, uint32_t* dCounts,
+                                  cudaStream_t stream);
+mlbvh_status render_ao_wide_quantised(uint32_t* dPixels, uint32_t* dOccluded, int w, int h,
+                                      const mlbvh_ray_generator& cam, const mlbvh_node_index* dRoot,
+                                      const mlbvh_internal_node* dNodes, const mlbvh_triangle* dTris,
+                                      const mlbvh_qwnode* dQWide, const uint32_t* dStatus,
+                                      const mlbvh_qtri* dLeafTris, int useSobol, int nSamples, float radius,
+                                      uint32_t seed, unsigned long long* dStats, void* dScratch, size_t scratchBytes,
+                                      cudaStream_t stream);
 mlbvh_status render_ao_wide(uint32_t* dPixels, uint32_t* dOccluded, int w, int h, const mlbvh_ray_generator& cam,
                             const mlbvh_node_index* dRoot, const mlbvh_internal_node* dNodes,
                             const mlbvh_triangle* dTris, const mlbvh_wnode* dWide, const mlbvh_qtri* dLeafTris,

@@ -10,6 +10,8 @@
 // counts into the packed image.
 #include <algorithm>
 
+#include <type_traits>
+
 #include "capi_internal.h"
 #include "../../include/mlbvh_device.cuh"
 
@@ -276,16 +278,22 @@ struct QuantTree {
     }
 };
 
-// The 4-wide tree for AO rays (any-hit, wide_any_step), the binary tree's
-// replay walk over leaf-ordered triangles for primary rays (closest hit, the
-// stack-free walk's Hit records). Context: the walk's root (a leaf root is
-// leaf position 0) and the binary root as the reference names it (the
-// restart of a ray whose wide stack would overflow).
-struct WideTree {
+// The 4-wide tree for AO rays (any-hit, wide_any_step) over FP32 slots or
+// (kQuant) quantised slots; primary rays on the binary tree's replay walk over
+// leaf-ordered triangles (closest hit, the stack-free walk's Hit records).
+// Context: the walk's root (a leaf root is leaf position 0), the binary root
+// as the reference names it (the restart of a ray whose wide stack would
+// overflow) and, for quantised slots, whether they are unusable (every AO ray
+// then takes the stack-free walk over the binary tree).
+template <bool kQuant>
+struct WideTreeT {
+    using Slot = typename std::conditional<kQuant, mlbvh_qwnode, mlbvh_wnode>::type;
     PlainReplayLeafTree binary;
-    const mlbvh_wnode* wnodes;
+    const Slot* slots;
+    const uint32_t* status;  // quantised slots only
     struct Ctx {
         uint32_t root, binaryRoot;
+        bool fallback;
     };
     static constexpr int kStack = kWideDepth;
     static constexpr int kPrimaryStack = PlainReplayLeafTree::kStack;
@@ -293,7 +301,7 @@ struct WideTree {
     __device__ __forceinline__ Ctx context() const
     {
         const uint32_t r = __ldg(binary.rootPtr);
-        return Ctx{(r & kLeafBit) ? kLeafBit : r, r};
+        return Ctx{(r & kLeafBit) ? kLeafBit : r, r, kQuant && __ldg(status) != 0u};
     }
     template <bool kAny, bool kCount>
     __device__ __forceinline__ void trace(const Ctx& c, HitRecord& hit, f3 ro, f3 rd, Counts& n, uint2* pstack,
@@ -303,25 +311,50 @@ struct WideTree {
     }
     // From the root, while exactly one child's box meets the ball, go down
     // into it; stop where several do (or at a leaf); kInvalid where none does.
+    // Quantised slots are tested on their decoded boxes, which contain the
+    // exact ones.
     __device__ __forceinline__ uint32_t ball_start(const Ctx& c, const AoBall& b) const
     {
+        if (c.fallback) return c.root;
         uint32_t curr = c.root;
         for (uint32_t steps = 0; !(curr & kLeafBit) && steps < kMaxTraversalSteps; ++steps) {
-            const float4* p = reinterpret_cast<const float4*>(wnodes + curr);
-            float4 lx, hx, ly, hy, lz, hz;
-            ldg32(p, lx, hx);
-            ldg32(p + 2, ly, hy);
-            ldg32(p + 4, lz, hz);
-            const uint4 ch = __ldg(reinterpret_cast<const uint4*>(p + 6));
+            const float4* p = reinterpret_cast<const float4*>(slots + curr);
             int meets = 0;
             uint32_t only = kInvalid;
+            if constexpr (kQuant) {
+                float4 a, q, c2, d;
+                ldg32(p, a, q);
+                ldg32(p + 2, c2, d);
+                const uint32_t sx = __float_as_uint(a.w), sy = __float_as_uint(q.x), sz = __float_as_uint(q.y);
+                const uint4 ch = make_uint4(__float_as_uint(d.x), __float_as_uint(d.y), __float_as_uint(d.z),
+                                            __float_as_uint(d.w));
 #pragma unroll
-            for (int k = 0; k < 4; ++k)
-                if (wpick(ch, k) != kWideEmpty && box_meets(mk(wpick(lx, k), wpick(ly, k), wpick(lz, k)),
-                                                            mk(wpick(hx, k), wpick(hy, k), wpick(hz, k)), b)) {
-                    ++meets;
-                    only = wpick(ch, k);
+                for (int k = 0; k < 4; ++k) {
+                    const f3 lo = mk(__fadd_rd(a.x, qw_value(__float_as_uint(q.z), sx, k)),
+                                     __fadd_rd(a.y, qw_value(__float_as_uint(c2.x), sy, k)),
+                                     __fadd_rd(a.z, qw_value(__float_as_uint(c2.z), sz, k)));
+                    const f3 hi = mk(__fadd_ru(a.x, qw_value(__float_as_uint(q.w), sx, k)),
+                                     __fadd_ru(a.y, qw_value(__float_as_uint(c2.y), sy, k)),
+                                     __fadd_ru(a.z, qw_value(__float_as_uint(c2.w), sz, k)));
+                    if (wpick(ch, k) != kWideEmpty && box_meets(lo, hi, b)) {
+                        ++meets;
+                        only = wpick(ch, k);
+                    }
                 }
+            } else {
+                float4 lx, hx, ly, hy, lz, hz;
+                ldg32(p, lx, hx);
+                ldg32(p + 2, ly, hy);
+                ldg32(p + 4, lz, hz);
+                const uint4 ch = __ldg(reinterpret_cast<const uint4*>(p + 6));
+#pragma unroll
+                for (int k = 0; k < 4; ++k)
+                    if (wpick(ch, k) != kWideEmpty && box_meets(mk(wpick(lx, k), wpick(ly, k), wpick(lz, k)),
+                                                                mk(wpick(hx, k), wpick(hy, k), wpick(hz, k)), b)) {
+                        ++meets;
+                        only = wpick(ch, k);
+                    }
+            }
             if (meets == 0) return kInvalid;
             if (meets > 1) return curr;
             curr = only;
@@ -333,10 +366,18 @@ struct WideTree {
                                          HitRecord& hit, f3 ro, f3 rd, f3 inv, Counts& n) const
     {
         static_assert(kAny, "AO rays are any-hit");
-        return wide_any_step<kCount>(curr, prev, depth, stack, kAoThreads, hit, wnodes, binary.nodes, binary.tris,
-                                     binary.leafTris, c.binaryRoot, ro, rd, inv, 0.0f, n.visits, n.tests, n.ups);
+        if (kQuant && c.fallback && depth >= 0) {  // unusable slots: the stack-free walk from the binary root
+            depth = -1;
+            curr = c.binaryRoot;
+            prev = kInvalid;
+        }
+        return wide_any_step<kCount, kQuant>(curr, prev, depth, stack, kAoThreads, hit, slots, binary.nodes,
+                                             binary.tris, binary.leafTris, c.binaryRoot, ro, rd, inv, 0.0f, n.visits,
+                                             n.tests, n.ups);
     }
 };
+using WideTree = WideTreeT<false>;
+using QuantWideTree = WideTreeT<true>;
 
 // Primary rays of ao (main_gpu.cu:121-144): closest hit, flip the normal
 // towards the viewer, AO origin p + n * 1e-3.
@@ -792,7 +833,27 @@ mlbvh_status render_ao_wide(uint32_t* dPixels, uint32_t* dOccluded, int w, int h
     if (!aligned16(dRoot) || !aligned32(dNodes) || !aligned16(dTris) || !aligned16(dLeafTris) ||
         (reinterpret_cast<uintptr_t>(dWide) & 127u))
         return fail(MLBVH_ERR_INVALID_ARG, "device pointers misaligned (wide nodes 128 B, nodes 32 B, others 16 B)");
-    const WideTree tree{PlainReplayLeafTree{dNodes, reinterpret_cast<const float*>(dTris), dRoot, dLeafTris}, dWide};
+    const WideTree tree{PlainReplayLeafTree{dNodes, reinterpret_cast<const float*>(dTris), dRoot, dLeafTris}, dWide,
+                        nullptr};
+    return launch_ao(dPixels, dOccluded, w, h, cam, tree, useSobol, nSamples, radius, seed, dStats, dScratch,
+                     scratchBytes, stream);
+}
+
+mlbvh_status render_ao_wide_quantised(uint32_t* dPixels, uint32_t* dOccluded, int w, int h,
+                                      const mlbvh_ray_generator& cam, const mlbvh_node_index* dRoot,
+                                      const mlbvh_internal_node* dNodes, const mlbvh_triangle* dTris,
+                                      const mlbvh_qwnode* dQWide, const uint32_t* dStatus,
+                                      const mlbvh_qtri* dLeafTris, int useSobol, int nSamples, float radius,
+                                      uint32_t seed, unsigned long long* dStats, void* dScratch, size_t scratchBytes,
+                                      cudaStream_t stream)
+{
+    if (mlbvh_status s = check_ao_args(w, h, nSamples, dPixels, dOccluded, dScratch, dStats)) return s;
+    if (!dRoot || !dTris || !dLeafTris || !dStatus) return fail(MLBVH_ERR_INVALID_ARG, "null pointer");
+    if (!aligned16(dRoot) || !aligned32(dNodes) || !aligned16(dTris) || !aligned16(dLeafTris) ||
+        !aligned16(dStatus) || !aligned32(dQWide))
+        return fail(MLBVH_ERR_INVALID_ARG, "device pointers misaligned (quantised slots and nodes 32 B, others 16 B)");
+    const QuantWideTree tree{PlainReplayLeafTree{dNodes, reinterpret_cast<const float*>(dTris), dRoot, dLeafTris},
+                             dQWide, dStatus};
     return launch_ao(dPixels, dOccluded, w, h, cam, tree, useSobol, nSamples, radius, seed, dStats, dScratch,
                      scratchBytes, stream);
 }

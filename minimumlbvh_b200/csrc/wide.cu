@@ -94,14 +94,94 @@ __global__ void __launch_bounds__(kWideThreads)
     reinterpret_cast<uint4*>(dst)[7] = make_uint4(0u, 0u, 0u, 0u);
 }
 
-// One thread per ray, any-hit. counts (may be null): per ray, node visits,
-// triangle tests and restarts at counts[i], counts[n + i], counts[2n + i].
-template <bool kCount>
+// Quantises one axis of a slot: base, power-of-two scale 2^E and the codes
+// of the children in `valid` (byte k of qlo / qhi). A lower code q satisfies
+// base + 2^E (1 + q / 2^15) <= lo and an upper code >= hi, in exact
+// arithmetic: every step rounds toward that side. E is the smallest exponent
+// (>= -111, so that 2^(E-15) stays a normal number) whose codes fit 8 bits.
+__device__ __forceinline__ bool quantise_axis(const float lo[4], const float hi[4], uint32_t valid, float& base,
+                                              float& scale, uint32_t& qlo, uint32_t& qhi)
+{
+    base = scale = 0.0f;
+    qlo = qhi = 0u;
+    float nlo = kFltMax, nhi = -kFltMax;
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+        if (valid & (1u << k)) {
+            nlo = fminf(nlo, lo[k]);
+            nhi = fmaxf(nhi, hi[k]);
+        }
+    if (!(isfinite(nlo) && isfinite(nhi) && nlo <= nhi)) return false;
+    const float m = __fdiv_ru(__fsub_ru(nhi, nlo), 255.0f);  // >= extent / 255
+    int e = -111;
+    if (m > 0.0f) {
+        int k;
+        const float f = frexpf(m, &k);  // m = f 2^k, f in [0.5, 1)
+        e = max(e, (f == 0.5f ? k - 1 : k) + 15);
+    }
+    for (; e <= 127; ++e) {
+        scale = pow2f(e);
+        base = __fsub_rd(nlo, scale);
+        if (!isfinite(base)) return false;
+        const float toCode = pow2f(15 - e);
+        bool fits = true;
+        qlo = qhi = 0u;
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+            if (valid & (1u << k)) {
+                const float ql = floorf(__fmul_rd(__fsub_rd(__fsub_rd(lo[k], base), scale), toCode));
+                const float qh = ceilf(__fmul_ru(__fsub_ru(__fsub_ru(hi[k], base), scale), toCode));
+                if (!(qh <= 255.0f)) fits = false;
+                qlo |= (uint32_t)fminf(fmaxf(ql, 0.0f), 255.0f) << (8 * k);
+                qhi |= (uint32_t)fminf(fmaxf(qh, 0.0f), 255.0f) << (8 * k);
+            }
+        if (fits) return true;
+    }
+    return false;
+}
+
+// One thread per slot: the FP32 slot's planes quantised axis by axis; a slot
+// that cannot be quantised sets *status.
+__global__ void __launch_bounds__(kWideThreads)
+    k_wide_quantise(const mlbvh_wnode* __restrict__ wnodes, uint32_t nSlots, mlbvh_qwnode* __restrict__ out,
+                    uint32_t* __restrict__ status)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nSlots) return;
+    const float4* p = reinterpret_cast<const float4*>(wnodes + i);
+    const uint4 ch = __ldg(reinterpret_cast<const uint4*>(p + 6));
+    uint32_t valid = 0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+        if (wpick(ch, k) != kWideEmpty) valid |= 1u << k;
+    float base[3], scale[3];
+    uint32_t q[6];
+    bool ok = true;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const float4 l = __ldg(p + 2 * a), h = __ldg(p + 2 * a + 1);
+        const float lo[4] = {l.x, l.y, l.z, l.w}, hi[4] = {h.x, h.y, h.z, h.w};
+        ok = quantise_axis(lo, hi, valid, base[a], scale[a], q[2 * a], q[2 * a + 1]) && ok;
+    }
+    if (!ok) atomicOr(status, 1u);
+    float4* dst = reinterpret_cast<float4*>(out + i);
+    dst[0] = make_float4(base[0], base[1], base[2], scale[0]);
+    dst[1] = make_float4(scale[1], scale[2], __uint_as_float(q[0]), __uint_as_float(q[1]));
+    dst[2] = make_float4(__uint_as_float(q[2]), __uint_as_float(q[3]), __uint_as_float(q[4]), __uint_as_float(q[5]));
+    reinterpret_cast<uint4*>(dst)[3] = ch;
+}
+
+// One thread per ray, any-hit, over FP32 slots or (kQuant) quantised slots.
+// counts (may be null): per ray, node visits, triangle tests and restarts at
+// counts[i], counts[n + i], counts[2n + i]. status (quantised slots): nonzero
+// sends every ray to the stack-free walk over the binary tree.
+template <bool kCount, bool kQuant, class Slot>
 __global__ void __launch_bounds__(kWideTraceThreads)
-    k_trace_wide(const mlbvh_wnode* __restrict__ wnodes, const mlbvh_internal_node* __restrict__ nodes,
-                 const mlbvh_node_index* __restrict__ rootPtr, const float* __restrict__ tris,
-                 const mlbvh_qtri* __restrict__ leafTris, const float4* __restrict__ rays, float4* __restrict__ hits,
-                 uint32_t n, uint32_t* __restrict__ counts)
+    k_trace_wide(const Slot* __restrict__ slots, const uint32_t* __restrict__ status,
+                 const mlbvh_internal_node* __restrict__ nodes, const mlbvh_node_index* __restrict__ rootPtr,
+                 const float* __restrict__ tris, const mlbvh_qtri* __restrict__ leafTris,
+                 const float4* __restrict__ rays, float4* __restrict__ hits, uint32_t n,
+                 uint32_t* __restrict__ counts)
 {
     __shared__ uint32_t s_stack[kWideDepth][kWideTraceThreads];
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -119,9 +199,13 @@ __global__ void __launch_bounds__(kWideTraceThreads)
     uint32_t nv = 0, nt = 0, nr = 0;
     uint32_t curr = (root & kLeafBit) ? kLeafBit : root, prev = kInvalid;
     int depth = 0;
+    if (kQuant && __ldg(status) != 0u) {
+        curr = root;
+        depth = -1;
+    }
     for (uint32_t steps = 1; steps < kMaxTraversalSteps; ++steps)
-        if (wide_any_step<kCount>(curr, prev, depth, &s_stack[0][threadIdx.x], kWideTraceThreads, hit, wnodes, nodes,
-                                  tris, leafTris, root, ro, rd, inv, a.w, nv, nt, nr))
+        if (wide_any_step<kCount, kQuant>(curr, prev, depth, &s_stack[0][threadIdx.x], kWideTraceThreads, hit, slots,
+                                          nodes, tris, leafTris, root, ro, rd, inv, a.w, nv, nt, nr))
             break;
     hits[2 * (size_t)i] = make_float4(hit.t, 0.0f, hit.u, hit.v);
     hits[2 * (size_t)i + 1] = make_float4(hit.ng.x, hit.ng.y, hit.ng.z, __uint_as_float(hit.tri));
@@ -150,28 +234,73 @@ mlbvh_status build_wide(const mlbvh_internal_node* dNodes, const mlbvh_node_inde
     return MLBVH_OK;
 }
 
-mlbvh_status trace_wide(const mlbvh_wnode* dWide, const mlbvh_internal_node* dNodes, const mlbvh_node_index* dRoot,
-                        const mlbvh_triangle* dTris, const mlbvh_qtri* dLeafTris, const mlbvh_ray* dRays,
-                        mlbvh_hit* dHits, uint32_t nRays, int rayQuery, uint32_t* dCounts, cudaStream_t stream)
+namespace {
+
+template <bool kQuant, class Slot>
+mlbvh_status launch_trace_wide(const Slot* dSlots, const uint32_t* dStatus, const mlbvh_internal_node* dNodes,
+                               const mlbvh_node_index* dRoot, const mlbvh_triangle* dTris,
+                               const mlbvh_qtri* dLeafTris, const mlbvh_ray* dRays, mlbvh_hit* dHits, uint32_t nRays,
+                               int rayQuery, uint32_t* dCounts, cudaStream_t stream)
 {
     if (nRays == 0) return MLBVH_OK;
     if (rayQuery != MLBVH_RAY_QUERY_ANY) return fail(MLBVH_ERR_INVALID_ARG, "the wide tree takes any-hit rays only");
-    if (!dRoot || !dTris || !dLeafTris || !dRays || !dHits) return fail(MLBVH_ERR_INVALID_ARG, "null pointer");
-    if (!aligned128(dWide) || !aligned32(dNodes) || !aligned16(dRoot) || !aligned16(dTris) || !aligned16(dLeafTris) ||
-        !aligned16(dRays) || !aligned16(dHits) || !aligned16(dCounts))
-        return fail(MLBVH_ERR_INVALID_ARG, "device pointers misaligned (wide nodes 128 B, nodes 32 B, others 16 B)");
+    if (!dRoot || !dTris || !dLeafTris || !dRays || !dHits || (kQuant && !dStatus))
+        return fail(MLBVH_ERR_INVALID_ARG, "null pointer");
+    if (!(kQuant ? aligned32(dSlots) : aligned128(dSlots)) || !aligned32(dNodes) || !aligned16(dRoot) ||
+        !aligned16(dTris) || !aligned16(dLeafTris) || !aligned16(dRays) || !aligned16(dHits) || !aligned16(dCounts) ||
+        !aligned16(dStatus))
+        return fail(MLBVH_ERR_INVALID_ARG,
+                    "device pointers misaligned (wide slots 128 B, quantised slots and nodes 32 B, others 16 B)");
     if (nRays >= (1u << 30) && dCounts) return fail(MLBVH_ERR_INVALID_ARG, "nRays must be below 2^30 with counts");
     const unsigned blocks = (nRays + kWideTraceThreads - 1) / kWideTraceThreads;
     const float4* rays = reinterpret_cast<const float4*>(dRays);
     float4* hits = reinterpret_cast<float4*>(dHits);
     const float* tris = reinterpret_cast<const float*>(dTris);
     if (dCounts)
-        k_trace_wide<true><<<blocks, kWideTraceThreads, 0, stream>>>(dWide, dNodes, dRoot, tris, dLeafTris, rays, hits,
-                                                                     nRays, dCounts);
+        k_trace_wide<true, kQuant><<<blocks, kWideTraceThreads, 0, stream>>>(dSlots, dStatus, dNodes, dRoot, tris,
+                                                                             dLeafTris, rays, hits, nRays, dCounts);
     else
-        k_trace_wide<false><<<blocks, kWideTraceThreads, 0, stream>>>(dWide, dNodes, dRoot, tris, dLeafTris, rays,
-                                                                      hits, nRays, nullptr);
+        k_trace_wide<false, kQuant><<<blocks, kWideTraceThreads, 0, stream>>>(dSlots, dStatus, dNodes, dRoot, tris,
+                                                                              dLeafTris, rays, hits, nRays, nullptr);
     MLBVH_CHECK_LAUNCH("k_trace_wide");
+    return MLBVH_OK;
+}
+
+}  // namespace
+
+mlbvh_status trace_wide(const mlbvh_wnode* dWide, const mlbvh_internal_node* dNodes, const mlbvh_node_index* dRoot,
+                        const mlbvh_triangle* dTris, const mlbvh_qtri* dLeafTris, const mlbvh_ray* dRays,
+                        mlbvh_hit* dHits, uint32_t nRays, int rayQuery, uint32_t* dCounts, cudaStream_t stream)
+{
+    return launch_trace_wide<false>(dWide, static_cast<const uint32_t*>(nullptr), dNodes, dRoot, dTris, dLeafTris,
+                                    dRays, dHits, nRays, rayQuery, dCounts, stream);
+}
+
+mlbvh_status trace_wide_quantised(const mlbvh_qwnode* dQWide, const uint32_t* dStatus,
+                                  const mlbvh_internal_node* dNodes, const mlbvh_node_index* dRoot,
+                                  const mlbvh_triangle* dTris, const mlbvh_qtri* dLeafTris, const mlbvh_ray* dRays,
+                                  mlbvh_hit* dHits, uint32_t nRays, int rayQuery, uint32_t* dCounts,
+                                  cudaStream_t stream)
+{
+    return launch_trace_wide<true>(dQWide, dStatus, dNodes, dRoot, dTris, dLeafTris, dRays, dHits, nRays, rayQuery,
+                                   dCounts, stream);
+}
+
+mlbvh_status quantise_wide(const mlbvh_wnode* dWide, uint32_t n, mlbvh_qwnode* dQWide, uint32_t* dStatus,
+                           cudaStream_t stream)
+{
+    if (n == 0) return fail(MLBVH_ERR_INVALID_ARG, "no triangles");
+    if (!dStatus) return fail(MLBVH_ERR_INVALID_ARG, "null pointer");
+    if (!aligned16(dStatus)) return fail(MLBVH_ERR_INVALID_ARG, "device pointers must be 16-byte aligned");
+    cudaError_t e = cudaMemsetAsync(dStatus, 0, sizeof(uint32_t), stream);
+    if (e != cudaSuccess) return fail(MLBVH_ERR_CUDA, cudaGetErrorString(e));
+    if (n == 1) return MLBVH_OK;
+    if (!dWide || !dQWide) return fail(MLBVH_ERR_INVALID_ARG, "null pointer");
+    if (!aligned128(dWide) || !aligned32(dQWide))
+        return fail(MLBVH_ERR_INVALID_ARG, "wide slots must be 128-byte and quantised slots 32-byte aligned");
+    const uint32_t m = n - 1;
+    k_wide_quantise<<<(m + kWideThreads - 1) / kWideThreads, kWideThreads, 0, stream>>>(dWide, m, dQWide, dStatus);
+    MLBVH_CHECK_LAUNCH("k_wide_quantise");
     return MLBVH_OK;
 }
 

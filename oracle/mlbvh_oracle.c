@@ -875,15 +875,149 @@ void orc_build_wide(const orc_node* nodes, uint32_t n, uint32_t* out)
     }
 }
 
+/* ----- quantised slots (csrc/wide.cu: quantise_axis, k_wide_quantise) */
+static int leaf_box_passes(orc_f3 ro, orc_f3 inv, const orc_f3* v, float tmin, float hitT);
+
+/* a + b rounded down (up != 0: up), as __fadd_rd / __fadd_ru: the nearest sum
+ * and its exact error (TwoSum) decide the step. */
+static float add_dir(float a, float b, int up)
+{
+    float s = a + b;
+    if (!isfinite(s)) return s;
+    /* an exact zero sum is -0 when rounding down unless both operands are +0
+     * (IEEE 754); rounding up gives the nearest sum's zero */
+    if (s == 0.0f && !up && (a != 0.0f || b != 0.0f || signbit(a) || signbit(b))) return -0.0f;
+    float bb = s - a;
+    float err = (a - (s - bb)) + (b - bb);
+    if (up) return err > 0.0f ? nextafterf(s, INFINITY) : s;
+    return err < 0.0f ? nextafterf(s, -INFINITY) : s;
+}
+/* a * b rounded down / up (the double product of two floats is exact) */
+static float mul_dir(float a, float b, int up)
+{
+    double p = (double)a * (double)b;
+    float f = (float)p;
+    if (up) return (double)f < p ? nextafterf(f, INFINITY) : f;
+    return (double)f > p ? nextafterf(f, -INFINITY) : f;
+}
+/* a / b rounded up (b = 255 here: the product q * 255 is exact in double) */
+static float div_up(float a, float b)
+{
+    float q = a / b;
+    return (double)q * (double)b < (double)a ? nextafterf(q, INFINITY) : q;
+}
+static float pow2_of(int e)
+{
+    uint32_t u = (uint32_t)(127 + e) << 23;
+    float f;
+    memcpy(&f, &u, 4);
+    return f;
+}
+/* the plane value of code q under scale 2^E: 2^E (1 + q / 2^15) */
+static float qw_value(uint32_t codes, uint32_t scaleBits, int k)
+{
+    uint32_t u = scaleBits | (((codes >> (8 * k)) & 255u) << 8);
+    float f;
+    memcpy(&f, &u, 4);
+    return f;
+}
+
+static int quantise_axis(const float lo[4], const float hi[4], uint32_t valid, float* base, float* scale,
+                         uint32_t* qlo, uint32_t* qhi)
+{
+    *base = *scale = 0.0f;
+    *qlo = *qhi = 0u;
+    float nlo = ORC_FLT_MAX, nhi = -ORC_FLT_MAX;
+    for (int k = 0; k < 4; ++k)
+        if (valid & (1u << k))
+        {
+            nlo = fminf(nlo, lo[k]);
+            nhi = fmaxf(nhi, hi[k]);
+        }
+    if (!(isfinite(nlo) && isfinite(nhi) && nlo <= nhi)) return 0;
+    float m = div_up(add_dir(nhi, -nlo, 1), 255.0f);
+    int e = -111;
+    if (m > 0.0f)
+    {
+        int k;
+        float f = frexpf(m, &k);
+        int c = (f == 0.5f ? k - 1 : k) + 15;
+        if (c > e) e = c;
+    }
+    for (; e <= 127; ++e)
+    {
+        float sc = pow2_of(e);
+        float b = add_dir(nlo, -sc, 0);
+        if (!isfinite(b)) return 0;
+        float toCode = pow2_of(15 - e);
+        int fits = 1;
+        uint32_t ql_all = 0, qh_all = 0;
+        for (int k = 0; k < 4; ++k)
+        {
+            if (!(valid & (1u << k))) continue;
+            float ql = floorf(mul_dir(add_dir(add_dir(lo[k], -b, 0), -sc, 0), toCode, 0));
+            float qh = ceilf(mul_dir(add_dir(add_dir(hi[k], -b, 1), -sc, 1), toCode, 1));
+            if (!(qh <= 255.0f)) fits = 0;
+            ql_all |= (uint32_t)fminf(fmaxf(ql, 0.0f), 255.0f) << (8 * k);
+            qh_all |= (uint32_t)fminf(fmaxf(qh, 0.0f), 255.0f) << (8 * k);
+        }
+        *base = b;
+        *scale = sc;
+        *qlo = ql_all;
+        *qhi = qh_all;
+        if (fits) return 1;
+    }
+    return 0;
+}
+
+/* 16 words per slot: base x y z, scale x y z, codes (x lo, x hi, y lo, y hi,
+ * z lo, z hi), children. Returns 1 when every slot was quantised. */
+int orc_quantise_wide(const uint32_t* wide, uint32_t n, uint32_t* out)
+{
+    int ok = 1;
+    for (uint32_t i = 0; i + 1 < n; ++i)
+    {
+        const uint32_t* w = wide + 32 * (size_t)i;
+        uint32_t* o = out + 16 * (size_t)i;
+        uint32_t valid = 0;
+        for (int k = 0; k < 4; ++k)
+            if (w[24 + k] != ORC_WIDE_EMPTY) valid |= 1u << k;
+        for (int a = 0; a < 3; ++a)
+        {
+            float lo[4], hi[4], b, sc;
+            memcpy(lo, &w[8 * a], 16);
+            memcpy(hi, &w[8 * a + 4], 16);
+            ok &= quantise_axis(lo, hi, valid, &b, &sc, &o[6 + 2 * a], &o[7 + 2 * a]);
+            memcpy(&o[a], &b, 4);
+            memcpy(&o[3 + a], &sc, 4);
+        }
+        memcpy(&o[12], &w[24], 16);
+    }
+    return ok;
+}
+
+/* The slab test on planes given relative to the ray origin (slabs with
+ * lower - ro, upper - ro already formed). */
+static inline void slabs_offsets(orc_f3 dlo, orc_f3 dhi, orc_f3 inv, float knownHitT, float* rmin, float* rmax)
+{
+    orc_f3 t0 = mul3(dlo, inv);
+    orc_f3 t1 = mul3(dhi, inv);
+    float region_min = compMax(min3(t0, t1));
+    float region_max = compMin(max3(t0, t1)) * 1.00000024f;
+    *rmin = smax(region_min, 0.0f);
+    *rmax = smin(region_max, knownHitT);
+}
+
 /* The any-hit walk over the wide tree from `start` (a wide slot or leaf
  * position; ORC_INVALID: nothing to test). leafIndex maps leaf positions to
  * triangle indices. Children whose box passes: the nearest entry first (ties
  * to the lower slot), the others pushed in slot order; a visit whose pushes
  * would overflow ORC_WIDE_DEPTH entries restarts with the stack-free walk
  * from binaryRoot. */
-static void trace_wide_any(orc_hit* hit, const uint32_t* wide, const orc_node* nodes, const orc_triangle* tris,
-                           const uint32_t* leafIndex, uint32_t start, uint32_t binaryRoot, orc_f3 ro, orc_f3 rd,
-                           orc_f3 inv, float tmin, uint32_t* visits, uint32_t* tests, uint32_t* restarts)
+static void trace_wide_any(orc_hit* hit, const uint32_t* wide, const uint32_t* qwide, const orc_node* nodes,
+                           const orc_triangle* tris, const uint32_t* leafIndex, uint32_t start, uint32_t binaryRoot,
+                           orc_f3 ro, orc_f3 rd, orc_f3 inv, float tmin, uint32_t* visits, uint32_t* tests,
+                           uint32_t* restarts)
 {
     uint32_t stack[ORC_WIDE_DEPTH];
     int top = 0;
@@ -893,28 +1027,51 @@ static void trace_wide_any(orc_hit* hit, const uint32_t* wide, const orc_node* n
     {
         if (is_leaf(curr))
         {
+            const orc_triangle* tri = &tris[leafIndex[idx_of(curr)]];
+            orc_hit probe = *hit;
             int h;
-            leaf_test(hit, tris, ORC_LEAF_BIT | leafIndex[idx_of(curr)], ro, rd, tmin, &h, tests);
-            if (h) return;
+            leaf_test(&probe, tris, ORC_LEAF_BIT | leafIndex[idx_of(curr)], ro, rd, tmin, &h, tests);
+            if (h && (!qwide || leaf_box_passes(ro, inv, tri->v, tmin, hit->t)))
+            {
+                *hit = probe;
+                return;
+            }
         }
         else
         {
             (*visits)++;
-            const uint32_t* w = wide + 32 * (size_t)curr;
+            const uint32_t* w = qwide ? qwide + 16 * (size_t)curr : wide + 32 * (size_t)curr;
+            const uint32_t* ch = qwide ? w + 12 : w + 24;
             int best = -1, npass = 0, pass[4] = {0, 0, 0, 0};
             float bestT = 0.0f;
             for (int k = 0; k < 4; ++k)
             {
-                if (w[24 + k] == ORC_WIDE_EMPTY) continue;
-                orc_aabb b;
-                memcpy(&b.lower.x, &w[k], 4);
-                memcpy(&b.upper.x, &w[4 + k], 4);
-                memcpy(&b.lower.y, &w[8 + k], 4);
-                memcpy(&b.upper.y, &w[12 + k], 4);
-                memcpy(&b.lower.z, &w[16 + k], 4);
-                memcpy(&b.upper.z, &w[20 + k], 4);
+                if (ch[k] == ORC_WIDE_EMPTY) continue;
                 float rmin, rmax;
-                slabs(ro, inv, &b, hit->t, &rmin, &rmax);
+                if (qwide)
+                {
+                    float base[3];
+                    memcpy(base, w, 12);
+                    const float r[3] = {ro.x, ro.y, ro.z};
+                    float dl[3], dh[3];
+                    for (int a = 0; a < 3; ++a)
+                    {
+                        dl[a] = add_dir(add_dir(base[a], -r[a], 0), qw_value(w[6 + 2 * a], w[3 + a], k), 0);
+                        dh[a] = add_dir(add_dir(base[a], -r[a], 1), qw_value(w[7 + 2 * a], w[3 + a], k), 1);
+                    }
+                    slabs_offsets(f3(dl[0], dl[1], dl[2]), f3(dh[0], dh[1], dh[2]), inv, hit->t, &rmin, &rmax);
+                }
+                else
+                {
+                    orc_aabb b;
+                    memcpy(&b.lower.x, &w[k], 4);
+                    memcpy(&b.upper.x, &w[4 + k], 4);
+                    memcpy(&b.lower.y, &w[8 + k], 4);
+                    memcpy(&b.upper.y, &w[12 + k], 4);
+                    memcpy(&b.lower.z, &w[16 + k], 4);
+                    memcpy(&b.upper.z, &w[20 + k], 4);
+                    slabs(ro, inv, &b, hit->t, &rmin, &rmax);
+                }
                 rmin = smax(rmin, tmin);
                 if (rmin <= rmax)
                 {
@@ -932,8 +1089,8 @@ static void trace_wide_any(orc_hit* hit, const uint32_t* wide, const orc_node* n
                     return;
                 }
                 for (int k = 0; k < 4; ++k)
-                    if (pass[k] && k != best) stack[top++] = w[24 + k];
-                curr = w[24 + best];
+                    if (pass[k] && k != best) stack[top++] = ch[k];
+                curr = ch[best];
                 continue;
             }
         }
@@ -955,6 +1112,8 @@ static void leaf_positions(const orc_node* nodes, uint32_t n, uint32_t root, uin
 
 typedef struct {
     const uint32_t* wide;
+    const uint32_t* qwide; /* quantised slots, or NULL */
+    int fallback;          /* the quantised slots are unusable: the stack-free walk for every ray */
     const orc_node* nodes;
     const orc_triangle* tris;
     const uint32_t* leafIndex;
@@ -976,8 +1135,11 @@ static void wide_range(void* p, uint32_t b, uint32_t e)
         hit_init(&hit, r->tmax);
         uint32_t nv = 0, nt = 0, nr = 0;
         uint32_t start = is_leaf(c->root) ? ORC_LEAF_BIT : c->root;
-        trace_wide_any(&hit, c->wide, c->nodes, c->tris, c->leafIndex, start, c->root, ro, rd, inv_rd(rd), r->tmin,
-                       &nv, &nt, &nr);
+        if (c->fallback)
+            stackfree_walk(&hit, c->nodes, c->tris, c->root, ORC_INVALID, ro, rd, inv_rd(rd), r->tmin, 1, &nv, &nt);
+        else
+            trace_wide_any(&hit, c->wide, c->qwide, c->nodes, c->tris, c->leafIndex, start, c->root, ro, rd,
+                           inv_rd(rd), r->tmin, &nv, &nt, &nr);
         c->hits[i] = hit;
         if (c->visits) c->visits[i] = nv;
         if (c->tests) c->tests[i] = nt;
@@ -991,7 +1153,18 @@ void orc_trace_wide(const uint32_t* wide, const orc_node* nodes, const orc_trian
 {
     uint32_t* leafIndex = (uint32_t*)malloc(sizeof(uint32_t) * (n ? n : 1));
     leaf_positions(nodes, n, root, leafIndex);
-    wide_ctx c = {wide, nodes, tris, leafIndex, root, rays, hits, visits, tests, restarts};
+    wide_ctx c = {wide, NULL, 0, nodes, tris, leafIndex, root, rays, hits, visits, tests, restarts};
+    orc_parallel_for(nRays, 1024, wide_range, &c);
+    free(leafIndex);
+}
+
+void orc_trace_wide_quantised(const uint32_t* qwide, int fallback, const orc_node* nodes, const orc_triangle* tris,
+                              uint32_t n, uint32_t root, const orc_ray* rays, uint32_t nRays, orc_hit* hits,
+                              uint32_t* visits, uint32_t* tests, uint32_t* restarts)
+{
+    uint32_t* leafIndex = (uint32_t*)malloc(sizeof(uint32_t) * (n ? n : 1));
+    leaf_positions(nodes, n, root, leafIndex);
+    wide_ctx c = {NULL, qwide, fallback, nodes, tris, leafIndex, root, rays, hits, visits, tests, restarts};
     orc_parallel_for(nRays, 1024, wide_range, &c);
     free(leafIndex);
 }

@@ -101,6 +101,14 @@ void orc_build_wide(const orc_node* nodes, uint32_t n, uint32_t* out);
 void orc_trace_wide(const uint32_t* wide, const orc_node* nodes, const orc_triangle* tris, uint32_t n, uint32_t root,
                     const orc_ray* rays, uint32_t nRays, orc_hit* hits, uint32_t* visits, uint32_t* tests,
                     uint32_t* restarts);
+/* Quantised slots (16 words each; csrc/wide.cu): returns 1 when every slot
+ * was quantised. orc_trace_wide_quantised walks them (a hit counts only where
+ * the triangle's exact box passes too); fallback != 0: the stack-free walk
+ * for every ray, as the kernels do when a slot could not be quantised. */
+int orc_quantise_wide(const uint32_t* wide, uint32_t n, uint32_t* out);
+void orc_trace_wide_quantised(const uint32_t* qwide, int fallback, const orc_node* nodes, const orc_triangle* tris,
+                              uint32_t n, uint32_t root, const orc_ray* rays, uint32_t nRays, orc_hit* hits,
+                              uint32_t* visits, uint32_t* tests, uint32_t* restarts);
 
 /* Camera (camera.h:10-31) */
 void orc_lookat(orc_f3 eye, orc_f3 center, orc_f3 up, float fovy, int w, int h, orc_camera* cam);

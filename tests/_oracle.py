@@ -64,6 +64,8 @@ def oracle() -> ctypes.CDLL:
             "orc_trace_replay": (None, [_vp, _vp, _u32, _vp, _u32, _i32, _i32, _vp, _vp, _vp]),
             "orc_build_wide": (None, [_vp, _u32, _vp]),
             "orc_trace_wide": (None, [_vp, _vp, _vp, _u32, _u32, _vp, _u32, _vp, _vp, _vp, _vp]),
+            "orc_quantise_wide": (_i32, [_vp, _u32, _vp]),
+            "orc_trace_wide_quantised": (None, [_vp, _i32, _vp, _vp, _u32, _u32, _vp, _u32, _vp, _vp, _vp, _vp]),
             "orc_lookat": (None, [F3, F3, F3, _f32, _i32, _i32, _vp]),
             "orc_sobol": (None, [_u32, _u32, _u32, _u32, _vp, _vp]),
             "orc_hash_pcg": (_u32, [_u32]),
@@ -202,6 +204,29 @@ def trace_wide(wide, nodes, tris, root, rays):
     wide_c = np.ascontiguousarray(wide, np.uint32) if len(wide) else np.zeros((1, 32), np.uint32)
     nodes_c = np.ascontiguousarray(nodes, np.uint32) if len(nodes) else np.zeros((1, 16), np.uint32)
     oracle().orc_trace_wide(P(wide_c), P(nodes_c), P(tris), n, root, P(rays), m, P(hits), P(nv), P(nt), P(nr))
+    return hits, nv, nt, nr
+
+
+def quantise_wide(wide, n):
+    """Quantised slots of a 4-wide tree: ((n - 1, 16) uint32, all quantised?)."""
+    out = np.zeros((max(n - 1, 0), 16), np.uint32)
+    ok = 1
+    if n > 1:
+        ok = oracle().orc_quantise_wide(P(np.ascontiguousarray(wide, np.uint32)), n, P(out))
+    return out, bool(ok)
+
+
+def trace_wide_quantised(qwide, nodes, tris, root, rays, fallback=False):
+    """Any-hit rays over quantised wide slots: hits, visits, tests, restarts."""
+    rays = np.ascontiguousarray(rays, np.float32).reshape(-1, 8)
+    tris = np.ascontiguousarray(tris, np.float32).reshape(-1, 9)
+    n, m = len(tris), rays.shape[0]
+    hits = np.zeros((m, 8), np.uint32)
+    nv, nt, nr = (np.zeros(m, np.uint32) for _ in range(3))
+    q_c = np.ascontiguousarray(qwide, np.uint32) if len(qwide) else np.zeros((1, 16), np.uint32)
+    nodes_c = np.ascontiguousarray(nodes, np.uint32) if len(nodes) else np.zeros((1, 16), np.uint32)
+    oracle().orc_trace_wide_quantised(P(q_c), int(fallback), P(nodes_c), P(tris), n, root, P(rays), m, P(hits),
+                                      P(nv), P(nt), P(nr))
     return hits, nv, nt, nr
 
 

@@ -160,3 +160,11 @@ def test_wide_entry_points_reject_bad_arguments():
                                   1 << 30, None) == 1
     assert L.mlbvh_render_ao_wide(p, None, 8, 8, ctypes.addressof(cam), p, p, p, p, None, 1, 16, 1.0, 1, None, p,
                                   1 << 30, None) == 1
+    # quantised wide slots
+    assert L.mlbvh_quantise_wide(p, 10, p, None, None) == 1  # no status word
+    assert L.mlbvh_quantise_wide(p, 0, p, p, None) == 1      # no triangles
+    assert L.mlbvh_trace_wide_quantised(p, p, p, p, p, p, p, p, 4, 0, None, None) == 1  # closest hit
+    assert L.mlbvh_trace_wide_quantised(p, None, p, p, p, p, p, p, 4, 1, None, None) == 1  # no status word
+    assert L.mlbvh_trace_wide_quantised(ctypes.c_void_p(256 + 16), p, p, p, p, p, p, p, 4, 1, None, None) == 1
+    assert L.mlbvh_render_ao_wide_quantised(p, None, 8, 8, ctypes.addressof(cam), p, p, p, p, None, p, 1, 16, 1.0, 1,
+                                            None, p, 1 << 30, None) == 1

@@ -136,3 +136,79 @@ def test_ao_wide_equals_plain_soup(cuda):
     _, occ1, st1 = _ao(mb.render_ao_wide, 1920, 1080, 64, 0.1, 1, cam, w)
     np.testing.assert_array_equal(occ1, occ0)
     assert (occ0 != MISS).mean() > 0.05
+
+
+def test_quantised_wide_slots_match_oracle(wcase):
+    import torch
+    _, tris, _, _, out, w, _ = wcase
+    n = len(tris)
+    w.quantise()
+    torch.cuda.synchronize()
+    assert int(G.host(w.status)[0]) == 0
+    if n == 1:
+        return
+    got = G.host(w.qwide, np.uint32)[: n - 1]
+    ref, ok = O.quantise_wide(O.build_wide(out["nodes"], n), n)
+    assert ok
+    bad = np.nonzero((got != ref).any(1))[0]
+    assert bad.size == 0, f"{bad.size} slots differ, first {bad[:4]}: {got[bad[:1]]} vs {ref[bad[:1]]}"
+
+
+def test_trace_wide_quantised_matches_oracle(wcase):
+    import torch
+    name, tris, b, t, out, w, rays = wcase
+    w.quantise()
+    counts = torch.zeros(3 * len(rays), dtype=torch.int32, device="cuda")
+    hits = G.host(mb.intersect_wide(w, G.dev(rays), counts=counts, quantised=True), np.uint32)
+    c = G.host(counts, np.uint32).reshape(3, -1)
+    q, _ = O.quantise_wide(O.build_wide(out["nodes"], len(tris)), len(tris))
+    ref, nv, nt, nr = O.trace_wide_quantised(q, out["nodes"], tris, out["root"], rays)
+    np.testing.assert_array_equal(hits, ref)
+    np.testing.assert_array_equal(c[0], nv)
+    np.testing.assert_array_equal(c[1], nt)
+    np.testing.assert_array_equal(c[2], nr)
+    plain = G.trace(b, t, rays, mb.RAY_QUERY_ANY)
+    np.testing.assert_array_equal(hits[:, 7] == MISS, plain[:, 7] == MISS)
+
+
+def test_quantised_wide_fallback_on_huge_extents(cuda):
+    """Coordinates spread over about 1e37 cannot be quantised: the status
+    word is set and every ray takes the stack-free walk (the oracle's hits)."""
+    rng = np.random.default_rng(9)
+    tris = (rng.random((200, 9)).astype(np.float32) - np.float32(0.5)) * np.float32(2e37)
+    b, t, out = G.build(tris)
+    w = mb.WideBVH.from_builder(b, t).quantise()
+    rays = scenes.random_rays(500, [-1e37, -1e37, -1e37], [1e37, 1e37, 1e37], seed=2)
+    rays[:, 7] = np.float32(3e37)
+    hits = G.host(mb.intersect_wide(w, G.dev(rays), quantised=True), np.uint32)
+    assert int(G.host(w.status)[0]) == 1
+    ref = O.trace(out["nodes"], tris, out["root"], rays, 1, 0)
+    np.testing.assert_array_equal(hits, ref)
+
+
+@pytest.mark.parametrize("sobol", [1, 0])
+def test_ao_quantised_wide_equals_plain_heightfield(cuda, sobol):
+    tris = scenes.heightfield_icospheres()
+    b, t, out = G.build(tris)
+    eye, c, up, fovy = scenes.camera_heightfield()
+    cam = mb.RayGenerator.from_array(O.lookat(eye, c, up, fovy, 512, 512))
+    px0, occ0, st0 = _ao(lambda *a, **k: mb.render_ao(a[0], a[1], a[2], b.m_rootNode, b.m_internals, t, *a[3:], **k),
+                         512, 512, 16, 0.25, sobol, cam)
+    w = mb.WideBVH.from_builder(b, t).quantise()
+    px1, occ1, st1 = _ao(lambda *a, **k: mb.render_ao_wide(*a, quantised=True, **k), 512, 512, 16, 0.25, sobol, cam,
+                         w)
+    np.testing.assert_array_equal(occ1, occ0)
+    np.testing.assert_array_equal(px1, px0)
+    assert st1[0] == st0[0] and st1[3] < 0.5 * st0[3]
+
+
+def test_ao_quantised_wide_equals_plain_soup(cuda):
+    tris = scenes.gaussian_soup()
+    b, t, out = G.build(tris)
+    eye, c, up, fovy = scenes.camera_soup()
+    cam = mb.RayGenerator.from_array(O.lookat(eye, c, up, fovy, 1920, 1080))
+    _, occ0, _ = _ao(lambda *a, **k: mb.render_ao(a[0], a[1], a[2], b.m_rootNode, b.m_internals, t, *a[3:], **k),
+                     1920, 1080, 64, 0.1, 1, cam)
+    w = mb.WideBVH.from_builder(b, t).quantise()
+    _, occ1, _ = _ao(lambda *a, **k: mb.render_ao_wide(*a, quantised=True, **k), 1920, 1080, 64, 0.1, 1, cam, w)
+    np.testing.assert_array_equal(occ1, occ0)

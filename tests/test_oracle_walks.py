@@ -177,3 +177,76 @@ def test_wide_stack_overflow_restarts_with_stackfree_walk():
     ref = O.trace(b["nodes"], tris, b["root"], rays, 1, 0)
     np.testing.assert_array_equal(got[:, 7] == MISS, ref[:, 7] == MISS)
     assert nr.sum() > 0
+
+
+def _decode_slot_planes(q):
+    """Per slot, child and axis: (lower, upper) plane values base + v(code)
+    in float64 (exact for these scenes; checked), and the children."""
+    base = q[:, 0:3].view(np.float32).astype(np.float64)
+    scale_bits = q[:, 3:6]
+    planes = np.zeros((len(q), 4, 3, 2))
+    for a in range(3):
+        for side in range(2):
+            codes = q[:, 6 + 2 * a + side]
+            for k in range(4):
+                code = (codes >> (8 * k)) & 255
+                v = (scale_bits[:, a] | (code << 8)).astype(np.uint32).view(np.float32).astype(np.float64)
+                s = base[:, a] + v
+                assert ((s - base[:, a]) == v).all()  # the float64 sum is exact
+                planes[:, k, a, side] = s
+    return planes
+
+
+def test_quantised_wide_slots_contain_fp32_slots(case):
+    """Every decoded child box of every quantised slot contains the FP32
+    slot's box; children are carried over unchanged."""
+    _, tris, b, _, _ = case
+    n = len(tris)
+    wide = O.build_wide(b["nodes"], n)
+    q, ok = O.quantise_wide(wide, n)
+    assert ok
+    np.testing.assert_array_equal(q[:, 12:16], wide[:, 24:28])
+    planes = _decode_slot_planes(q)
+    wf = wide.view(np.float32).astype(np.float64)
+    for k in range(4):
+        filled = wide[:, 24 + k] != MISS
+        for a in range(3):
+            lo, hi = wf[:, 8 * a + k], wf[:, 8 * a + 4 + k]
+            assert (planes[filled, k, a, 0] <= lo[filled]).all()
+            assert (planes[filled, k, a, 1] >= hi[filled]).all()
+    # the codes use the 8 bits: the mean upper-minus-lower gap is far below the node
+    # extent (a few codes per child plane, not the whole range)
+    ext = planes[:, :, :, 1].max(1) - planes[:, :, :, 0].min(1)
+    assert (ext > 0).mean() > 0.9
+
+
+def test_quantised_wide_any_hit_equals_stackfree(case):
+    name, tris, b, _, rays = case
+    n = len(tris)
+    wide = O.build_wide(b["nodes"], n)
+    q, _ = O.quantise_wide(wide, n)
+    got, nv, nt, nr = O.trace_wide_quantised(q, b["nodes"], tris, b["root"], rays)
+    ref = O.trace(b["nodes"], tris, b["root"], rays, 1, 0)
+    np.testing.assert_array_equal(got[:, 7] == MISS, ref[:, 7] == MISS)
+    fp32, nv32, _, _ = O.trace_wide(wide, b["nodes"], tris, b["root"], rays)
+    if name != "duplicates":
+        # decoded boxes contain the exact ones: at least the FP32 walk's visits, not many more
+        assert nv.sum() >= nv32.sum() and nv.sum() < 1.3 * nv32.sum()
+
+
+def test_quantised_wide_fallback_for_huge_extents():
+    """Coordinates spread over about 1e37 cannot be quantised (codes beyond
+    8 bits at every scale up to 2^127): the slots are flagged and every ray
+    takes the stack-free walk, with the same hits."""
+    rng = np.random.default_rng(9)
+    tris = (rng.random((200, 9)).astype(np.float32) - np.float32(0.5)) * np.float32(2e37)
+    b = O.build(tris)
+    wide = O.build_wide(b["nodes"], len(tris))
+    _, ok = O.quantise_wide(wide, len(tris))
+    assert not ok
+    rays = scenes.random_rays(500, [-1e37, -1e37, -1e37], [1e37, 1e37, 1e37], seed=2)
+    rays[:, 7] = np.float32(3e37)
+    got, _, _, _ = O.trace_wide_quantised(np.zeros((len(tris) - 1, 16), np.uint32), b["nodes"], tris, b["root"],
+                                          rays, fallback=True)
+    ref = O.trace(b["nodes"], tris, b["root"], rays, 1, 0)
+    np.testing.assert_array_equal(got, ref)
