@@ -410,9 +410,10 @@ def main():
     stats = torch.zeros(8, dtype=torch.int64, device=dev)
     stream = torch.cuda.current_stream()
 
-    def ao_frame(with_stats=False):
-        mb.render_ao(pixels, (w, h), cam, builder.m_rootNode, builder.m_internals, d_tris, 1, wl["ns"], wl["radius"],
-                     12345, stats=stats if with_stats else None)
+    def ao_frame(with_stats=False, tris_buf=None):
+        mb.render_ao(pixels, (w, h), cam, builder.m_rootNode, builder.m_internals,
+                     d_tris if tris_buf is None else tris_buf, 1, wl["ns"], wl["radius"], 12345,
+                     stats=stats if with_stats else None)
 
     # counting pass: rays, node visits and triangle tests of one frame (the
     # traversal is deterministic, so every timed frame does the same work)
@@ -509,18 +510,22 @@ def main():
                 frame()
             fev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
                    for _ in range(args.steps)]
+            fkev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+                    for _ in range(args.steps)]
             barrier()
             torch.cuda.synchronize()
             for i in range(args.steps):
                 if flush is not None:
                     flush.zero_()
                 fev[i][0].record(stream)
+                mb.profile_events(*fkev[i])
                 frame()
                 fev[i][1].record(stream)
             torch.cuda.synchronize()
             barrier()
             forms[name] = (max_over_ranks(sum(a.elapsed_time(b) for a, b in fev) / 1e3),
-                           float((occ_plain == occ).float().mean().item()), fst.cpu().numpy())
+                           float((occ_plain == occ).float().mean().item()), fst.cpu().numpy(),
+                           float(np.mean([a.elapsed_time(b) for a, b in fkev])) / 1e3)
 
         # ---- builds
         bev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
@@ -538,19 +543,36 @@ def main():
         build_total_s = max_over_ranks(sum(build_ms) / 1e3)
         builder.status()
 
-        # ---- end to end through the C ABI from host buffers
+        # ---- end to end through the C ABI from host buffers: every step uploads
+        # its triangles from pinned host memory, builds, renders and reads the
+        # image back. Two device triangle buffers: step i + 1's upload (copy
+        # stream) overlaps step i's build and frame; a buffer is refilled only
+        # after the step that read it is done.
         eev = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+        copy_stream = torch.cuda.Stream(device=dev)
+        bufs = (d_tris, torch.empty_like(d_tris))
+        ready = [torch.cuda.Event() for _ in range(args.steps)]
+        done = [torch.cuda.Event() for _ in range(args.steps)]
         barrier()
         torch.cuda.synchronize()
         eev[0].record(stream)
+        copy_stream.wait_event(eev[0])
         for i in range(args.steps):
-            d_tris.copy_(host_tris, non_blocking=True)
-            builder.build(d_tris, n, 0, sorter)
-            ao_frame()
+            buf = bufs[i % 2]
+            if i >= 2:
+                copy_stream.wait_event(done[i - 2])
+            with torch.cuda.stream(copy_stream):
+                buf.copy_(host_tris, non_blocking=True)
+            ready[i].record(copy_stream)
+            stream.wait_event(ready[i])
+            builder.build(buf, n, 0, sorter)
+            ao_frame(tris_buf=buf)
             host_pixels.copy_(pixels, non_blocking=True)
+            done[i].record(stream)
         eev[1].record(stream)
         torch.cuda.synchronize()
         barrier()
+        builder.build(d_tris, n, 0, sorter)
         e2e_s = max_over_ranks(eev[0].elapsed_time(eev[1]) / 1e3)
         precision = bench_precision(args, builder, qtree, d_tris, tris, cam, w, h, dev, stream, max_over_ranks)
         batched = None if args.no_batched else bench_batched(args, dev, stream, barrier, max_over_ranks,
@@ -592,7 +614,8 @@ def main():
                      "frac": n * BUILD_BYTES_PER_TRI / build_s / 1e9 / peak, "bytes_per_tri": BUILD_BYTES_PER_TRI}
     line["e2e"] = {"value": rays_per_frame * args.steps * world / e2e_s / 1e6, "unit": "Mrays/s",
                    "h2d_bytes_per_step": int(host_tris.numel() * 4), "d2h_bytes_per_step": int(w * h * 4),
-                   "ms_per_step": e2e_s * 1e3 / args.steps}
+                   "ms_per_step": e2e_s * 1e3 / args.steps,
+                   "pipeline": "upload of step i+1 overlaps build + frame of step i (two device triangle buffers)"}
     form_lines = {}
     form_desc = {
         "replay": "FP32 nodes, replay walk (stack of pending far children), leaf-ordered 48-byte triangles",
@@ -602,7 +625,7 @@ def main():
         "wide_quantised": "AO rays over the 4-wide tree with 8-bit child planes rounded outward (64-byte nodes, "
                           "any-hit, exact leaf-box check on hits), primary rays on the replay walk",
     }
-    for name, (total_s, agree, fst) in forms.items():
+    for name, (total_s, agree, fst, f_kernel_s) in forms.items():
         f_rays = int(fst[0])
         if name == "replay":
             node_bytes = 64 * int(fst[1])
@@ -611,13 +634,27 @@ def main():
         else:  # primary rays visit 64-byte binary nodes, AO rays 128-byte (64-byte quantised) wide nodes
             node_bytes = 64 * (int(fst[1]) - int(fst[3])) + (128 if name == "wide" else 64) * int(fst[3])
         tri_bytes = 48 * int(fst[2])
+        # the AO-ray kernel of this form: its algorithmic bytes (node bytes of
+        # its AO-ray visits + 48 B per AO-ray triangle test) per launch over its
+        # event-timed duration
+        if name == "replay":
+            ao_node_bytes = 64 * int(fst[3])
+        elif name == "quantised":
+            ao_node_bytes = 32 * int(fst[3]) + 4 * int(fst[6])
+        else:
+            ao_node_bytes = (128 if name == "wide" else 64) * int(fst[3])
+        f_kernel_bytes = ao_node_bytes + 48 * int(fst[4])
+        f_achieved = f_kernel_bytes / f_kernel_s / 1e9
+        form_lines_roof = {"kernel_ms": f_kernel_s * 1e3, "achieved": f_achieved, "peak": peak, "unit": "GB/s",
+                           "frac": f_achieved / peak, "kernel_bytes": f_kernel_bytes}
         form_lines[name] = {
             "form": form_desc[name],
             "value": f_rays * args.steps * world / total_s / 1e6, "unit": "Mrays/s",
             "ms_per_step": total_s * 1e3 / args.steps, "vs_plain": ao_total_s / total_s,
             "occlusion_agreement": agree, "rays_per_frame": f_rays,
             "node_visits_per_ray": int(fst[1]) / max(f_rays, 1),
-            "node_bytes_per_ray": node_bytes / max(f_rays, 1), "tri_bytes_per_ray": tri_bytes / max(f_rays, 1)}
+            "node_bytes_per_ray": node_bytes / max(f_rays, 1), "tri_bytes_per_ray": tri_bytes / max(f_rays, 1),
+            "ao_kernel_roofline": form_lines_roof}
         if name == "wide":
             form_lines[name]["prep_ms_per_build"] = wide_prep_ms
             form_lines[name]["restarts"] = int(fst[6])

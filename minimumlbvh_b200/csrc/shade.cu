@@ -32,6 +32,9 @@ constexpr int kAoThreads = 128;
 #ifndef MLBVH_AO_WIDE_STEPS_PER_ROUND
 #define MLBVH_AO_WIDE_STEPS_PER_ROUND 2
 #endif
+#ifndef MLBVH_AO_MIN_BLOCKS
+#define MLBVH_AO_MIN_BLOCKS 8
+#endif
 constexpr int kFinishThreads = 256;
 
 struct AoRecord {
@@ -457,7 +460,7 @@ struct StepsOf<Tree, decltype((void)Tree::kSteps)> {
 };
 
 template <class Tree, bool kCount>
-__global__ void __launch_bounds__(kAoThreads, 8)  // at most 64 registers: 32 warps per SM
+__global__ void __launch_bounds__(kAoThreads, MLBVH_AO_MIN_BLOCKS)  // 8: at most 64 registers, 32 warps per SM
     k_ao_rays(const AoRecord* __restrict__ records, const uint32_t* __restrict__ queueCount,
               unsigned long long* __restrict__ workCounter, int w, int nSamples, float radius, uint32_t seed,
               int useSobol, Tree tree, uint32_t* __restrict__ counts, unsigned long long* __restrict__ stats)
