@@ -66,22 +66,22 @@ __global__ void __launch_bounds__(kWideThreads)
                     best = a;
                 }
             }
-        if (pick < 0) break;
-        WideKid a, b;
-        uint32_t p = 0;
+        if (pick >= 0) {
+            WideKid a, b;
+            uint32_t p = 0;
 #pragma unroll
-        for (int k = 0; k < 4; ++k)
-            if (k == pick) p = kid[k].name;
-        binary_children(nodes, p, a, b);
+            for (int k = 0; k < 4; ++k)
+                if (k == pick) p = kid[k].name;
+            binary_children(nodes, p, a, b);
+            // kid[pick] becomes a, b; the kids after it move one slot up
+            WideKid next[4];
 #pragma unroll
-        for (int k = 3; k >= 1; --k)
-            if (k > pick + 1 && k <= count) kid[k] = kid[k - 1];
+            for (int k = 0; k < 4; ++k)
+                next[k] = k < pick ? kid[k] : k == pick ? a : k == pick + 1 ? b : kid[k > 0 ? k - 1 : 0];
 #pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            if (k == pick) kid[k] = a;
-            if (k == pick + 1) kid[k] = b;
+            for (int k = 0; k < 4; ++k) kid[k] = next[k];
+            ++count;
         }
-        ++count;
     }
     float4* dst = reinterpret_cast<float4*>(out + i);
     dst[0] = make_float4(kid[0].lo.x, kid[1].lo.x, kid[2].lo.x, kid[3].lo.x);
