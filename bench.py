@@ -331,6 +331,123 @@ def bench_precision(args, builder, qtree, d_tris, tris, cam, w, h, dev, stream, 
     }
 
 
+REF_GPU_LIB = os.path.join(ROOT, "oracle", "_ref", "libmlbvh_ref_gpu.so")
+
+
+def bench_reference_gpu(args, builder, sorter, d_tris, n, cam, w, h, dev, stream, max_over_ranks):
+    """Baseline leg: the reference's OWN GPU kernels, compiled unmodified for
+    sm_100a (oracle/_ref/libmlbvh_ref_gpu.so, built from the reference sources
+    by oracle/Makefile), against this project's kernels on the same B200.
+
+    Build: the reference's getSceneAABB + buildMortons, and computeDeltas +
+    0xFF fill + build over sorted pairs. Its Onesweep sort is not run (its waits
+    are unbounded; see oracle/ref_gpu_launch.cu): the pairs come from this
+    project's sort, which produces the reference's stable order, so the sort is
+    excluded from the reference's time and included in ours. AO: the
+    reference's ao kernel, which fixes 16 Owen-Sobol samples of length 1.0
+    (main_gpu.cu:148, 165), over the validated tree, against the plain and the
+    4-wide forms at the same 16 samples and radius 1.0. The reference's grid
+    also covers the rows up to the next multiple of 16 (a padded buffer takes
+    its writes); only the frame's rays are counted."""
+    import ctypes
+    import torch
+    import minimumlbvh_b200 as mb
+    if not os.path.exists(REF_GPU_LIB):
+        return {"unavailable": "oracle/_ref/libmlbvh_ref_gpu.so is not built (it needs the reference sources)"}
+    L = ctypes.CDLL(REF_GPU_LIB)
+    vp, i32, i64, u32 = ctypes.c_void_p, ctypes.c_int, ctypes.c_longlong, ctypes.c_uint32
+    L.refgpu_scene_aabb.argtypes = [vp, vp, i32, vp]
+    L.refgpu_mortons.argtypes = [vp, vp, i32, vp, u32, vp]
+    L.refgpu_deltas_and_build.argtypes = [vp, vp, vp, i32, vp, vp, vp]
+    L.refgpu_ao.argtypes = [vp, i64, i32, i32, vp, vp, vp, vp, i32, vp]
+    for f in (L.refgpu_scene_aabb, L.refgpu_mortons, L.refgpu_deltas_and_build, L.refgpu_ao):
+        f.restype = i32
+    if (n - 1) % 256 == 0:
+        return {"unavailable": "n - 1 is a multiple of 256: the reference's build grid would skip a leaf"}
+    sp = stream.cuda_stream
+    ptr = mb._ptr
+
+    def check(rc, what):
+        if rc != 0:
+            raise RuntimeError(f"reference GPU {what}: status {rc}")
+
+    # our build with the sorted pairs kept: the reference's input to computeDeltas + build
+    builder.build(d_tris, n, 0, sorter, keep_keys=True)
+    builder.status()
+    pairs = torch.stack([builder.m_sortedKeys, builder.m_sortedIndices], 1).contiguous()
+    scene = torch.empty(8, dtype=torch.float32, device=dev)
+    mortons = torch.empty((n, 2), dtype=torch.int32, device=dev)
+    deltas = torch.empty(n, dtype=torch.uint8, device=dev)
+    nodes = torch.empty((n - 1, 16), dtype=torch.int32, device=dev)
+    root = torch.empty(4, dtype=torch.int32, device=dev)
+
+    def ref_build():
+        check(L.refgpu_scene_aabb(ptr(scene), ptr(d_tris), n, sp), "getSceneAABB")
+        check(L.refgpu_mortons(ptr(mortons), ptr(d_tris), n, ptr(scene), 0, sp), "buildMortons")
+        check(L.refgpu_deltas_and_build(ptr(root), ptr(nodes), ptr(d_tris), n, ptr(deltas), ptr(pairs), sp),
+              "computeDeltas/build")
+
+    def timed(fn, steps):
+        for _ in range(args.warmup):
+            fn()
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+        torch.cuda.synchronize()
+        for i in range(steps):
+            ev[i][0].record(stream)
+            fn()
+            ev[i][1].record(stream)
+        torch.cuda.synchronize()
+        return max_over_ranks(float(np.mean([a.elapsed_time(b) for a, b in ev])) / 1e3)
+
+    ref_build_s = timed(ref_build, args.steps)
+    ours_build_s = timed(lambda: builder.build(d_tris, n, 0, sorter), args.steps)
+    # the reference's keys (unsorted, from its buildMortons) sorted stably must be ours
+    ref_keys = mortons[:, 0].cpu().numpy().view(np.uint32)
+    our_keys = pairs[:, 0].cpu().numpy().view(np.uint32)
+    keys_equal = bool((np.sort(ref_keys, kind="stable") == our_keys).all())
+    tree_equal = bool(torch.equal(nodes, builder.m_internals[: n - 1]) and torch.equal(root[:1], builder.m_rootNode[:1]))
+
+    # AO at the reference's fixed parameters, over this project's tree (the
+    # reference's own only if identical): 16 samples, length 1.0
+    pw, ph = -(-w // 16) * 16, -(-h // 16) * 16
+    ref_px = torch.zeros(pw * ph, dtype=torch.int32, device=dev)
+    cam_arr = np.ascontiguousarray(cam.as_array(), np.float32)
+    src_nodes = nodes if tree_equal else builder.m_internals
+    src_root = root if tree_equal else builder.m_rootNode
+    ref_ao_s = timed(lambda: check(L.refgpu_ao(ptr(ref_px), pw * ph, w, h, cam_arr.ctypes.data, ptr(src_root),
+                                              ptr(src_nodes), ptr(d_tris), 1, sp), "ao"), args.steps)
+    px = torch.zeros(w * h, dtype=torch.int32, device=dev)
+    occ = torch.zeros(w * h, dtype=torch.int32, device=dev)
+    plain_s = timed(lambda: mb.render_ao(px, (w, h), cam, builder.m_rootNode, builder.m_internals, d_tris, 1, 16, 1.0,
+                                         12345, occluded=occ), args.steps)
+    plain_px = px.clone()
+    wide = mb.WideBVH.from_builder(builder, d_tris)
+    wide_s = timed(lambda: mb.render_ao_wide(px, (w, h), cam, wide, 1, 16, 1.0, 12345), args.steps)
+    torch.cuda.synchronize()
+    rays = w * h + 16 * int((occ != -1).sum().item())
+    a = ref_px.cpu().numpy().view(np.uint32)[: w * h]
+    b = plain_px.cpu().numpy().view(np.uint32)
+    ch = np.abs(np.stack([(a >> k) & 255 for k in (0, 8, 16)], 1).astype(np.int32)
+                - np.stack([(b >> k) & 255 for k in (0, 8, 16)], 1).astype(np.int32)).max(1)
+    return {
+        "what": "the reference's own CUDA kernels (minimum_lbvh.cu, main_gpu.cu) compiled unmodified for sm_100a "
+                "and launched with its own grids, on the same B200 and inputs",
+        "build": {"reference_ms": ref_build_s * 1e3, "ours_ms": ours_build_s * 1e3,
+                  "vs_reference": ref_build_s / ours_build_s, "reference_tree_equal": tree_equal,
+                  "reference_keys_equal": keys_equal,
+                  "note": "reference time excludes its Onesweep sort (not run: unbounded waits); ours includes our "
+                          "sort"},
+        "ao": {"samples": 16, "radius": 1.0, "rays_per_frame": rays,
+               "reference_ms": ref_ao_s * 1e3, "reference_mrays_s": rays / ref_ao_s / 1e6,
+               "plain_ms": plain_s * 1e3, "plain_mrays_s": rays / plain_s / 1e6, "plain_vs_reference": ref_ao_s / plain_s,
+               "wide_ms": wide_s * 1e3, "wide_mrays_s": rays / wide_s / 1e6, "wide_vs_reference": ref_ao_s / wide_s,
+               "pixels_equal": float((ch == 0).mean()), "max_channel_diff": int(ch.max()),
+               "note": "the reference samples directions with CUDA's cosf/sinf, the plain form with its own FP32 "
+                       "sincos: a few AO rays flip; the reference's grid also traces the padding rows "
+                       f"{h}..{ph - 1} (uncounted)"},
+    }
+
+
 def run_reference(args, wl, rank):
     """The reference's own CPU implementation of the path, all host threads."""
     if rank != 0:
@@ -377,6 +494,8 @@ def main():
     ap.add_argument("--no-batched", action="store_true", help="skip the batched (1,024-mesh) workload")
     ap.add_argument("--batched-meshes", type=int, default=1024, help="meshes of the batched workload (small cases)")
     ap.add_argument("--no-autotune", action="store_true", help="batched workload with default launch parameters")
+    ap.add_argument("--no-reference-gpu", action="store_true",
+                    help="skip the baseline leg running the reference's own GPU kernels")
     args = ap.parse_args()
     wl = dict(WORKLOADS[args.workload])
     if args.image:
@@ -575,6 +694,10 @@ def main():
         builder.build(d_tris, n, 0, sorter)
         e2e_s = max_over_ranks(eev[0].elapsed_time(eev[1]) / 1e3)
         precision = bench_precision(args, builder, qtree, d_tris, tris, cam, w, h, dev, stream, max_over_ranks)
+        reference_gpu = None
+        if not args.no_reference_gpu and rank == 0 and world == 1:
+            reference_gpu = bench_reference_gpu(args, builder, sorter, d_tris, n, cam, w, h, dev, stream,
+                                                lambda x: x)
         batched = None if args.no_batched else bench_batched(args, dev, stream, barrier, max_over_ranks,
                                                                    world, args.batched_meshes, not args.no_autotune)
     clocks = sampler.summary()
@@ -669,6 +792,10 @@ def main():
     line["chosen"]["plain_node_bytes_per_ray"] = 64 * visits / max(rays_per_frame, 1)
     line["forms"] = form_lines
     line["precision"] = precision
+    if reference_gpu is not None:
+        line["reference_gpu_baseline"] = reference_gpu
+        if "ao" in reference_gpu:  # our kernels launched in that leg: plain (3) and wide (3) frames, 2 builds
+            line["gpu_launches"] += (args.warmup + args.steps) * (3 + 3 + 7) + 2
     line["gpu_launches"] += 2 * (args.warmup + args.steps) + 1
     if batched is not None:
         line["batched"] = batched
