@@ -21,6 +21,34 @@ __device__ __forceinline__ uint32_t delta_at(const uint32_t* __restrict__ keys, 
     return split_delta(keys[i], keys[i + 1]);
 }
 
+// A triangle's three corners with three 16-byte loads: the 48-byte window
+// from the triangle's address rounded down to 16 bytes holds its 36 bytes;
+// the corners are picked out by the triangle's offset in that window. A
+// window that would reach past `end` (the last triangles) takes nine scalar
+// loads instead, so nothing is read outside the array.
+__device__ __forceinline__ void load_triangle_v(const float* __restrict__ t, const float* end, f3& v0, f3& v1,
+                                                f3& v2)
+{
+    const uintptr_t a = reinterpret_cast<uintptr_t>(t);
+    const uintptr_t a0 = a & ~uintptr_t(15);
+    if (a0 + 48 > reinterpret_cast<uintptr_t>(end)) {
+        v0 = mk(__ldg(t + 0), __ldg(t + 1), __ldg(t + 2));
+        v1 = mk(__ldg(t + 3), __ldg(t + 4), __ldg(t + 5));
+        v2 = mk(__ldg(t + 6), __ldg(t + 7), __ldg(t + 8));
+        return;
+    }
+    const float4* q = reinterpret_cast<const float4*>(a0);
+    const float4 q0 = __ldg(q), q1 = __ldg(q + 1), q2 = __ldg(q + 2);
+    const float f[12] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w, q2.x, q2.y, q2.z, q2.w};
+    const int off = (int)((a - a0) >> 2);  // 0..3
+    float c[9];
+#pragma unroll
+    for (int j = 0; j < 9; ++j) c[j] = off == 0 ? f[j] : off == 1 ? f[j + 1] : off == 2 ? f[j + 2] : f[j + 3];
+    v0 = mk(c[0], c[1], c[2]);
+    v1 = mk(c[3], c[4], c[5]);
+    v2 = mk(c[6], c[7], c[8]);
+}
+
 // build_lbvh (minimum_lbvh.h:284-361) for sorted leaf i of a tree of n
 // leaves: climbs from the leaf to the root. The hand-off word per internal
 // node lives in its own array (reset before the build) and is exchanged with
@@ -28,7 +56,10 @@ __device__ __forceinline__ uint32_t delta_at(const uint32_t* __restrict__ keys, 
 // the second; the sibling bounds are then read from L2. The merged box is
 // formed as max/min(box of child 1, box of child 0) whichever walker arrives
 // second, which is the order the reference's serial CPU build produces (its
-// second arrival always comes from the right).
+// second arrival always comes from the right). A child slot is written with
+// two vector stores (children word apart), the sibling's box read with two
+// vector loads; of the two key deltas at the range's ends only the one at the
+// end that moved is recomputed. The node array must be 16-byte aligned.
 __device__ __forceinline__ void climb(const float* __restrict__ tris, uint32_t n, uint32_t i,
                                       const uint32_t* __restrict__ sortedKeys, const uint32_t* __restrict__ sortedIdx,
                                       mlbvh_internal_node* __restrict__ nodes, uint32_t* __restrict__ handoff,
@@ -40,7 +71,7 @@ __device__ __forceinline__ void climb(const float* __restrict__ tris, uint32_t n
     if (deltas && i < nInternals) deltas[i] = (uint8_t)delta_at(sortedKeys, i);
 
     f3 v0, v1, v2;
-    load_triangle(tris, tri, v0, v1, v2);
+    load_triangle_v(tris + 9ull * tri, tris + 9ull * n, v0, v1, v2);
     f3 lo = mk(kFltMax, kFltMax, kFltMax), hi = mk(-kFltMax, -kFltMax, -kFltMax);
     lo = smin3(lo, v0);
     hi = smax3(hi, v0);
@@ -50,33 +81,48 @@ __device__ __forceinline__ void climb(const float* __restrict__ tris, uint32_t n
     hi = smax3(hi, v2);
 
     uint32_t leafLower = i, leafUpper = i;
+    uint32_t deltaL = 0 < leafLower ? delta_at(sortedKeys, leafLower - 1) : 0xFFFFFFFFu;
+    uint32_t deltaR = leafUpper < nInternals ? delta_at(sortedKeys, leafUpper) : 0xFFFFFFFFu;
     uint32_t node = tri | kLeafBit;
     while (leafUpper - leafLower < nInternals) {
-        const uint32_t deltaL = 0 < leafLower ? delta_at(sortedKeys, leafLower - 1) : 0xFFFFFFFFu;
-        const uint32_t deltaR = leafUpper < nInternals ? delta_at(sortedKeys, leafUpper) : 0xFFFFFFFFu;
         const int goLeft = deltaL < deltaR ? 1 : 0;
         const uint32_t parent = goLeft ? leafLower - 1 : leafUpper;
 
         mlbvh_internal_node* p = nodes + parent;
+        float* pw = reinterpret_cast<float*>(p);
         p->children[goLeft] = node;
-        float* box = p->aabbs[goLeft].lower;
-        box[0] = lo.x;
-        box[1] = lo.y;
-        box[2] = lo.z;
-        box[3] = hi.x;
-        box[4] = hi.y;
-        box[5] = hi.z;
+        if (goLeft) {  // aabbs[1]: bytes 32-55
+            *reinterpret_cast<float4*>(pw + 8) = make_float4(lo.x, lo.y, lo.z, hi.x);
+            *reinterpret_cast<float2*>(pw + 12) = make_float2(hi.y, hi.z);
+        } else {  // aabbs[0]: bytes 8-31
+            *reinterpret_cast<float2*>(pw + 2) = make_float2(lo.x, lo.y);
+            *reinterpret_cast<float4*>(pw + 4) = make_float4(lo.z, hi.x, hi.y, hi.z);
+        }
         if (!(node & kLeafBit)) nodes[node].parent = parent;
 
-        uint32_t other = exch_acq_rel(handoff + parent, goLeft ? leafUpper : leafLower);
+        const uint32_t other = exch_acq_rel(handoff + parent, goLeft ? leafUpper : leafLower);
         if (other == 0xFFFFFFFFu) return;  // first arrival: the sibling finishes this node
 
-        leafLower = min(leafLower, other);
-        leafUpper = max(leafUpper, other);
+        if (other < leafLower) {
+            leafLower = other;
+            deltaL = 0 < leafLower ? delta_at(sortedKeys, leafLower - 1) : 0xFFFFFFFFu;
+        } else {
+            leafUpper = other;
+            deltaR = leafUpper < nInternals ? delta_at(sortedKeys, leafUpper) : 0xFFFFFFFFu;
+        }
         p->context = leafUpper < nInternals ? leafUpper : 0xFFFFFFFFu;
-        const float* ob = p->aabbs[goLeft ^ 1].lower;
-        const f3 olo = mk(__ldcg(ob + 0), __ldcg(ob + 1), __ldcg(ob + 2));
-        const f3 ohi = mk(__ldcg(ob + 3), __ldcg(ob + 4), __ldcg(ob + 5));
+        f3 olo, ohi;
+        if (goLeft) {  // the sibling is child 0
+            const float2 a = __ldcg(reinterpret_cast<const float2*>(pw + 2));
+            const float4 b = __ldcg(reinterpret_cast<const float4*>(pw + 4));
+            olo = mk(a.x, a.y, b.x);
+            ohi = mk(b.y, b.z, b.w);
+        } else {
+            const float4 a = __ldcg(reinterpret_cast<const float4*>(pw + 8));
+            const float2 b = __ldcg(reinterpret_cast<const float2*>(pw + 12));
+            olo = mk(a.x, a.y, a.z);
+            ohi = mk(a.w, b.x, b.y);
+        }
         if (goLeft) {  // this walker is child 1
             lo = smin3(lo, olo);
             hi = smax3(hi, ohi);
