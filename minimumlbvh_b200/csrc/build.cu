@@ -224,9 +224,15 @@ __global__ void __launch_bounds__(kBuildThreads)
             const uint32_t* __restrict__ sortedIdx, mlbvh_internal_node* __restrict__ nodes,
             uint32_t* __restrict__ handoff, mlbvh_node_index* __restrict__ root, uint8_t* __restrict__ deltas)
 {
+    __shared__ float s_box[kBuildThreads * 6];
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    climb(tris, n, i, sortedKeys, sortedIdx, nodes, handoff, root, deltas);
+    // tri >= n only after a sort whose bounded wait gave up (error word set)
+    const uint32_t tri = i < n ? sortedIdx[i] : 0xFFFFFFFFu;
+    f3 lo = mk(0.0f, 0.0f, 0.0f), hi = lo;
+    if (tri < n) leaf_box(tris, n, tri, lo, hi);
+    stage_leaf_box(s_box, threadIdx.x, tri < n, lo, hi);
+    if (tri >= n) return;
+    climb(n, i, tri, lo, hi, sortedKeys, nodes, handoff, root, deltas, s_box, threadIdx.x, blockDim.x - 1);
 }
 
 }  // namespace
