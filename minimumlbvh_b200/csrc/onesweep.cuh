@@ -136,9 +136,12 @@ __device__ __forceinline__ uint32_t block_scan(uint32_t v, uint32_t* s_warp /*kW
 // One pass over digit (key >> shift) & (2^kBits - 1). Launch with at least
 // as many CTAs as tiles (extra CTAs exit), kThreads threads and
 // Shape<kBits>::kSmemBytes of dynamic shared memory. kFirst: the values are
-// the keys' positions within their segment (valsIn unused).
+// the keys' positions within their segment (valsIn unused). The 8-bit passes
+// are held to three resident CTAs per SM (at most 85 registers): the pass is
+// latency-bound and more tiles in flight shorten it (measured 3 % on a 4M
+// build); the 11-bit passes are limited by shared memory to two anyway.
 template <int kBits, bool kFirst, class Segments>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, kBits == 8 ? 3 : 1)
     k_onesweep(const uint32_t* __restrict__ keysIn, uint32_t* __restrict__ keysOut,
                const uint32_t* __restrict__ valsIn, uint32_t* __restrict__ valsOut, int shift, Segments segs,
                uint32_t* __restrict__ lookback, uint32_t* __restrict__ tileCounter, uint32_t* __restrict__ errorWord,
