@@ -100,7 +100,8 @@ __device__ __forceinline__ void stage_leaf_box(float* sBox, int t, bool valid, f
 // leaf i + 1 takes leaf i's box from the CTA's staged boxes (sBox, written
 // before a barrier) and goes on from node i. Both threads decide this from the
 // same key deltas; a pair split across two CTAs uses the hand-off word.
-// Nothing else changes: the node words written are the same.
+// Nothing else changes: the node words written are the same. A caller that
+// passes t = 0 and tLast = -1 (and no sBox) turns leaf pairs off.
 __device__ __forceinline__ void climb(uint32_t n, uint32_t i, uint32_t tri, f3 lo, f3 hi,
                                       const uint32_t* __restrict__ sortedKeys,
                                       mlbvh_internal_node* __restrict__ nodes, uint32_t* __restrict__ handoff,

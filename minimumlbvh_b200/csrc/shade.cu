@@ -167,6 +167,7 @@ struct PlainTreeT {
     }
     static constexpr int kStack = kWalk > 0 ? kReplayDepth : 0;
     static constexpr int kPrimaryStack = kStack;  // closest-hit replay stack of primary rays
+    static constexpr int kMinBlocks = kWalk == 0 ? 10 : MLBVH_AO_MIN_BLOCKS;
     // Replay forms: the node where AO rays from the ball's centre start. From
     // the root, while exactly one child's box meets the ball, go down into it;
     // stop where both do (or at a leaf). Every leaf an AO ray of the pixel can
@@ -458,9 +459,21 @@ template <class Tree>
 struct StepsOf<Tree, decltype((void)Tree::kSteps)> {
     static constexpr int value = Tree::kSteps;
 };
+// Resident CTAs per SM the kernel is compiled for: a tree's kMinBlocks, else
+// MLBVH_AO_MIN_BLOCKS (8: at most 64 registers, 32 warps per SM). The
+// stack-free walk fits 10 (48 registers) without spills and gains from the
+// extra warps; the stack and wide walks spill below 64 registers.
+template <class Tree, class = void>
+struct MinBlocksOf {
+    static constexpr int value = MLBVH_AO_MIN_BLOCKS;
+};
+template <class Tree>
+struct MinBlocksOf<Tree, decltype((void)Tree::kMinBlocks)> {
+    static constexpr int value = Tree::kMinBlocks;
+};
 
 template <class Tree, bool kCount>
-__global__ void __launch_bounds__(kAoThreads, MLBVH_AO_MIN_BLOCKS)  // 8: at most 64 registers, 32 warps per SM
+__global__ void __launch_bounds__(kAoThreads, MinBlocksOf<Tree>::value)
     k_ao_rays(const AoRecord* __restrict__ records, const uint32_t* __restrict__ queueCount,
               unsigned long long* __restrict__ workCounter, int w, int nSamples, float radius, uint32_t seed,
               int useSobol, Tree tree, uint32_t* __restrict__ counts, unsigned long long* __restrict__ stats)
