@@ -16,7 +16,8 @@ build, AO frame, download of the packed image.
     python bench.py [--gpus N --steps K --warmup W] [--impl reference] [--workload NAME]
 
 Under torchrun (N > 1) every rank renders its own replica of the frame
-(the path does not shard: see DESIGN.md); times are the max over ranks.
+(the path does not shard: the build is a global sort and a bottom-up climb,
+and one frame's rays fit one GPU); times are the max over ranks.
 """
 from __future__ import annotations
 
@@ -38,7 +39,10 @@ WORKLOADS = {
     "heightfield_ao16": dict(scene="heightfield", n=212_992, w=512, h=512, ns=16, radius=0.25),
 }
 METRIC = "AO Mrays/s (primary + AO rays, stack-free LBVH traversal)"
-BUILD_BYTES_PER_TRI = 291  # algorithmic bytes per triangle of the build chain
+# algorithmic bytes per triangle of the build chain: 36 (bounds) + 36 (keys) + 8 (key write) + 8 (count)
+# + 4 x 16 (four sort passes) + 9 (deltas) + 6 (index and delta reads) + 36 (leaf triangle) + 64 (node)
+# + 24 (sibling box)
+BUILD_BYTES_PER_TRI = 291
 
 
 def make_scene(wl):
