@@ -40,6 +40,11 @@ constexpr int kAoThreads = 128;
 #endif
 // the stack-free walk's own (swept: 4 steps and a batch of 16 lanes beat 3 and
 // 8 by 1.7 %; a batch of 24 loses 7 %)
+// the wide trees' refill batch (swept 4-16: 8 is best for the quantised slots,
+// within 1 % of the best for the FP32 ones)
+#ifndef MLBVH_AO_WIDE_START_BATCH
+#define MLBVH_AO_WIDE_START_BATCH 8
+#endif
 #ifndef MLBVH_AO_PLAIN_STEPS_PER_ROUND
 #define MLBVH_AO_PLAIN_STEPS_PER_ROUND 4
 #endif
@@ -315,6 +320,7 @@ struct WideTreeT {
     static constexpr int kStack = kWideDepth;
     static constexpr int kPrimaryStack = PlainReplayLeafTree::kStack;
     static constexpr int kSteps = kQuant ? MLBVH_AO_QWIDE_STEPS_PER_ROUND : MLBVH_AO_WIDE_STEPS_PER_ROUND;
+    static constexpr int kStartBatch = MLBVH_AO_WIDE_START_BATCH;
     __device__ __forceinline__ Ctx context() const
     {
         const uint32_t r = __ldg(binary.rootPtr);
