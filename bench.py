@@ -335,6 +335,48 @@ def bench_precision(args, builder, qtree, d_tris, tris, cam, w, h, dev, stream, 
     }
 
 
+def bench_pt(args, dev, stream, max_over_ranks):
+    """Path tracing (pt, main_gpu.cu:179-272) on the 212,992-triangle
+    heightfield + icospheres scene with 1 % emissive triangles, 512 x 512,
+    Owen-Sobol samples, the reference's 1024-bounce limit with Russian
+    roulette: progressive passes (one sample per pixel each) with the
+    stack-free walk and with the replay walk over leaf-ordered triangles,
+    which must leave bit-identical accumulators."""
+    import torch
+    import minimumlbvh_b200 as mb
+    from minimumlbvh_b200 import scenes
+    tris = scenes.heightfield_icospheres()
+    n = len(tris)
+    t = torch.from_numpy(tris).to(dev)
+    at = torch.from_numpy(scenes.pt_attributes(n, light_fraction=0.01)).to(dev)
+    b = mb.BVHGPUBuilder().build(t, n, 0, mb.OnesweepSort(dev.index))
+    b.status()
+    lt = mb.leaf_triangles(b, t)
+    eye, c, up, fovy = scenes.camera_heightfield()
+    w = h = 512
+    cam = mb.RayGenerator().lookat(eye, c, up, fovy, w, h)
+    out = {}
+    accs = {}
+    for name, kw in (("plain", {}), ("replay", {"traversal": mb.TRAVERSAL_REPLAY, "leaf_triangles": lt})):
+        acc = torch.zeros((w * h, 4), dtype=torch.float32, device=dev)
+        for _ in range(args.warmup):
+            mb.render_pt(acc, (w, h), cam, b.m_rootNode, b.m_internals, t, at, 1, **kw)
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+        torch.cuda.synchronize()
+        ev[0].record(stream)
+        for _ in range(args.steps):
+            mb.render_pt(acc, (w, h), cam, b.m_rootNode, b.m_internals, t, at, 1, **kw)
+        ev[1].record(stream)
+        torch.cuda.synchronize()
+        sec = max_over_ranks(ev[0].elapsed_time(ev[1]) / 1e3)
+        out[name] = {"ms_per_pass": sec * 1e3 / args.steps, "msamples_s": w * h * args.steps / sec / 1e6}
+        accs[name] = acc
+    out["replay"]["vs_plain"] = out["plain"]["ms_per_pass"] / out["replay"]["ms_per_pass"]
+    out["replay"]["accumulators_equal"] = bool(torch.equal(accs["plain"], accs["replay"]))
+    out["workload"] = "heightfield + icospheres (212,992 triangles), 512x512, 1 % emissive, up to 1024 bounces"
+    return out
+
+
 REF_GPU_LIB = os.path.join(ROOT, "oracle", "_ref", "libmlbvh_ref_gpu.so")
 
 
@@ -728,6 +770,7 @@ def main():
         del wides
         builder.build(d_tris, n, 0, sorter)
         precision = bench_precision(args, builder, qtree, d_tris, tris, cam, w, h, dev, stream, max_over_ranks)
+        pt = bench_pt(args, dev, stream, max_over_ranks)
         reference_gpu = None
         if not args.no_reference_gpu and rank == 0 and world == 1:
             reference_gpu = bench_reference_gpu(args, builder, sorter, d_tris, n, cam, w, h, dev, stream,
@@ -831,6 +874,8 @@ def main():
     line["chosen"]["plain_node_bytes_per_ray"] = 64 * visits / max(rays_per_frame, 1)
     line["forms"] = form_lines
     line["precision"] = precision
+    line["pt"] = pt
+    line["gpu_launches"] += 2 * (args.warmup + args.steps) + 8  # pt passes, its build and leaf copy
     if reference_gpu is not None:
         line["reference_gpu_baseline"] = reference_gpu
         if "ao" in reference_gpu:  # our kernels launched in that leg: plain (3) and wide (3) frames, 2 builds

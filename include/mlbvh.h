@@ -438,6 +438,17 @@ MLBVH_API mlbvh_status mlbvh_render_pt(float* dAccumulators, int width, int heig
                              const mlbvh_node_index* dRootNode, const mlbvh_internal_node* dInternals,
                              const mlbvh_triangle* dTriangles, const mlbvh_triangle_attrib* dAttribs,
                              int useSobol, int maxSPP, int maxDepth, void* stream);
+/* mlbvh_render_pt with the walk of its closest-hit rays chosen:
+ * MLBVH_TRAVERSAL_STACKFREE (what mlbvh_render_pt runs) or
+ * MLBVH_TRAVERSAL_REPLAY (the same Hit records, so the same accumulators,
+ * from fewer node loads; dLeafTriangles from mlbvh_leaf_triangles may be
+ * NULL). No reference counterpart. */
+MLBVH_API mlbvh_status mlbvh_render_pt_ex(float* dAccumulators, int width, int height,
+                                          const mlbvh_ray_generator* camera, const mlbvh_node_index* dRootNode,
+                                          const mlbvh_internal_node* dInternals, const mlbvh_triangle* dTriangles,
+                                          const mlbvh_triangle_attrib* dAttribs, int useSobol, int maxSPP,
+                                          int maxDepth, int traversal, const mlbvh_qtri* dLeafTriangles,
+                                          void* stream);
 
 /* ------------------------------------------------ differentiable path trace ---
  * No reference counterpart (the reference's pt, main_gpu.cu:179-272, is not

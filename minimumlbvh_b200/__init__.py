@@ -77,6 +77,7 @@ def lib() -> ctypes.CDLL:
             "mlbvh_render_ao": (i32, [_vp, _vp, i32, i32, _vp, _vp, _vp, _vp, i32, i32, f32, u32, _vp, _vp, sz,
                                       _vp]),
             "mlbvh_render_pt": (i32, [_vp, i32, i32, _vp, _vp, _vp, _vp, _vp, i32, i32, i32, _vp]),
+            "mlbvh_render_pt_ex": (i32, [_vp, i32, i32, _vp, _vp, _vp, _vp, _vp, i32, i32, i32, i32, _vp, _vp]),
             "mlbvh_render_ao_ex": (i32, [_vp, _vp, i32, i32, _vp, _vp, _vp, _vp, i32, i32, f32, u32, i32, _vp, _vp,
                                          _vp, sz, _vp]),
             "mlbvh_leaf_triangles": (i32, [_vp, _vp, _vp, u32, _vp, _vp]),
@@ -451,13 +452,22 @@ def render_ao_wide(pixels, imageSize, rayGenerator: RayGenerator, w: WideBVH, us
 
 
 def render_pt(accumulators, imageSize, rayGenerator: RayGenerator, rootNode, internals, triangles,
-              triangleAttribs, useSobol: int = 1, maxSPP: int = 1 << 30, maxDepth: int = 1024, stream=None):
-    """One progressive pass of pt (main_gpu.cu:179-272)."""
+              triangleAttribs, useSobol: int = 1, maxSPP: int = 1 << 30, maxDepth: int = 1024, stream=None,
+              traversal: int = TRAVERSAL_STACKFREE, leaf_triangles=None):
+    """One progressive pass of pt (main_gpu.cu:179-272). ``traversal``
+    TRAVERSAL_REPLAY gives the same accumulators from the replay walk,
+    reading ``leaf_triangles`` (from ``leaf_triangles()``) when given."""
     w, h = imageSize
     cam = rayGenerator._cstruct()
-    _check(lib().mlbvh_render_pt(_ptr(accumulators), int(w), int(h), ctypes.addressof(cam), _ptr(rootNode),
-                                 _ptr(internals), _ptr(triangles), _ptr(triangleAttribs), int(useSobol), int(maxSPP),
-                                 int(maxDepth), _stream(stream)))
+    if traversal == TRAVERSAL_STACKFREE and leaf_triangles is None:
+        _check(lib().mlbvh_render_pt(_ptr(accumulators), int(w), int(h), ctypes.addressof(cam), _ptr(rootNode),
+                                     _ptr(internals), _ptr(triangles), _ptr(triangleAttribs), int(useSobol),
+                                     int(maxSPP), int(maxDepth), _stream(stream)))
+    else:
+        _check(lib().mlbvh_render_pt_ex(_ptr(accumulators), int(w), int(h), ctypes.addressof(cam), _ptr(rootNode),
+                                        _ptr(internals), _ptr(triangles), _ptr(triangleAttribs), int(useSobol),
+                                        int(maxSPP), int(maxDepth), int(traversal), _ptr(leaf_triangles),
+                                        _stream(stream)))
     return accumulators
 
 

@@ -210,6 +210,18 @@ mlbvh_status mlbvh_render_pt(float* dAccumulators, int width, int height, const 
                      maxSPP, maxDepth, as_stream(stream));
 }
 
+mlbvh_status mlbvh_render_pt_ex(float* dAccumulators, int width, int height, const mlbvh_ray_generator* camera,
+                                const mlbvh_node_index* dRootNode, const mlbvh_internal_node* dInternals,
+                                const mlbvh_triangle* dTriangles, const mlbvh_triangle_attrib* dAttribs,
+                                int useSobol, int maxSPP, int maxDepth, int traversal,
+                                const mlbvh_qtri* dLeafTriangles, void* stream)
+{
+    clear_error();
+    if (!camera) return fail(MLBVH_ERR_INVALID_ARG, "null camera");
+    return render_pt(dAccumulators, width, height, *camera, dRootNode, dInternals, dTriangles, dAttribs, useSobol,
+                     maxSPP, maxDepth, as_stream(stream), traversal, dLeafTriangles);
+}
+
 mlbvh_status mlbvh_quantise(const mlbvh_internal_node* dInternals, const mlbvh_node_index* dRootNode,
                             const mlbvh_triangle* dTriangles, uint32_t nTriangles, mlbvh_qnode* dQNodes,
                             uint32_t* dQParents, mlbvh_qtri* dQTris, mlbvh_qheader* dQHeader, void* stream)

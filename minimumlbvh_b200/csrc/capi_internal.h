@@ -91,7 +91,8 @@ mlbvh_status trace_quantised(const mlbvh_qnode* dQNodes, const uint32_t* dQParen
 mlbvh_status render_pt(float* dAccum, int w, int h, const mlbvh_ray_generator& cam, const mlbvh_node_index* dRoot,
                        const mlbvh_internal_node* dNodes, const mlbvh_triangle* dTris,
                        const mlbvh_triangle_attrib* dAttribs, int useSobol, int maxSPP, int maxDepth,
-                       cudaStream_t stream);
+                       cudaStream_t stream, int traversal = MLBVH_TRAVERSAL_STACKFREE,
+                       const mlbvh_qtri* dLeafTris = nullptr);
 mlbvh_status pack(uint32_t* dPixels, const float* dAccum, int n, cudaStream_t stream);
 mlbvh_status pt_diff_render(float* dImage, int w, int h, int spp, int bounces, const mlbvh_ray_generator& cam,
                             const mlbvh_node_index* dRoot, const mlbvh_internal_node* dNodes,

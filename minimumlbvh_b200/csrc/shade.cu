@@ -667,12 +667,18 @@ struct PtRandom {
     }
 };
 
-// pt (main_gpu.cu:179-272): one progressive sample per pixel.
+// pt (main_gpu.cu:179-272): one progressive sample per pixel. Tree: the
+// walk of every closest-hit ray (PlainTree: intersect_stackfree as the
+// reference; the replay trees: the same Hit records from a per-thread stack
+// of pending far children in shared memory), so the accumulators are the same.
+template <class Tree>
 __global__ void __launch_bounds__(kTileW* kTileH)
-    k_pt(float4* __restrict__ accum, mlbvh_ray_generator gen, int w, int h,
-         const mlbvh_node_index* __restrict__ rootPtr, const mlbvh_internal_node* __restrict__ nodes,
-         const float* __restrict__ tris, const float* __restrict__ attribs, int useSobol, int maxSPP, int maxDepth)
+    k_pt(float4* __restrict__ accum, mlbvh_ray_generator gen, int w, int h, Tree tree,
+         const float* __restrict__ attribs, int useSobol, int maxSPP, int maxDepth)
 {
+    __shared__ uint2 s_pstack[Tree::kPrimaryStack > 0 ? Tree::kPrimaryStack : 1][kTileW * kTileH];
+    uint2* const pstack = &s_pstack[0][threadIdx.x];
+    Counts cnt;
     int xi, yi;
     if (!tile_pixel(w, h, xi, yi)) return;
     const Camera cam = to_camera(gen);
@@ -681,7 +687,7 @@ __global__ void __launch_bounds__(kTileW* kTileH)
     const int iteration = (int)acc.w;
     PtRandom rr{useSobol, (uint32_t)iteration, (uint32_t)xi, (uint32_t)yi, 0u,
                 Pcg(hash_pcg(hash_pcg((uint32_t)pixel) + (uint32_t)iteration), 0)};
-    const uint32_t root = __ldg(rootPtr);
+    const typename Tree::Ctx ctx = tree.context();
     float2 rnd = rr.next();
     f3 ro, rd;
     shoot(cam, ((float)xi + rnd.x) / (float)w, ((float)yi + rnd.y) / (float)h, ro, rd);
@@ -690,7 +696,7 @@ __global__ void __launch_bounds__(kTileW* kTileH)
     HitRecord hit;
     hit.t = kFltMax;
     hit.tri = 0xFFFFFFFFu;
-    trace_stackfree<false, false, true>(hit, nodes, tris, root, ro, rd, inv_rd(rd), 0.0f);
+    tree.template trace<false, false>(ctx, hit, ro, rd, cnt, pstack, kTileW * kTileH);
     if (hit.t != kFltMax)
         for (int depth = 0; depth < maxDepth; depth++) {
             const float2 r2 = rr.next();
@@ -716,7 +722,7 @@ __global__ void __launch_bounds__(kTileW* kTileH)
             hit.u = hit.v = 0.0f;
             hit.ng = mk(0.0f, 0.0f, 0.0f);
             hit.tri = 0xFFFFFFFFu;
-            trace_stackfree<false, false, true>(hit, nodes, tris, root, next_ro, next_rd, inv_rd(next_rd), 0.0f);
+            tree.template trace<false, false>(ctx, hit, next_ro, next_rd, cnt, pstack, kTileW * kTileH);
             if (hit.t == kFltMax) break;
             ro = next_ro;
             rd = next_rd;
@@ -920,17 +926,29 @@ mlbvh_status render_ao_quantised(uint32_t* dPixels, uint32_t* dOccluded, int w, 
 mlbvh_status render_pt(float* dAccum, int w, int h, const mlbvh_ray_generator& cam, const mlbvh_node_index* dRoot,
                        const mlbvh_internal_node* dNodes, const mlbvh_triangle* dTris,
                        const mlbvh_triangle_attrib* dAttribs, int useSobol, int maxSPP, int maxDepth,
-                       cudaStream_t stream)
+                       cudaStream_t stream, int traversal, const mlbvh_qtri* dLeafTris)
 {
     if (mlbvh_status s = check_image(w, h)) return s;
     if (!dAccum || !dRoot || !dTris || !dAttribs) return fail(MLBVH_ERR_INVALID_ARG, "null pointer");
-    if (!aligned16(dAccum) || !aligned16(dRoot) || !aligned32(dNodes) || !aligned16(dTris) || !aligned16(dAttribs))
+    if (!aligned16(dAccum) || !aligned16(dRoot) || !aligned32(dNodes) || !aligned16(dTris) || !aligned16(dAttribs) ||
+        !aligned16(dLeafTris))
         return fail(MLBVH_ERR_INVALID_ARG, "device pointers must be 16-byte aligned");
     if (maxDepth < 0) return fail(MLBVH_ERR_INVALID_ARG, "maxDepth must be >= 0");
-    k_pt<<<tile_grid(w, h), kTileW * kTileH, 0, stream>>>(reinterpret_cast<float4*>(dAccum), cam, w, h, dRoot, dNodes,
-                                                          reinterpret_cast<const float*>(dTris),
-                                                          reinterpret_cast<const float*>(dAttribs), useSobol, maxSPP,
-                                                          maxDepth);
+    if (traversal != MLBVH_TRAVERSAL_STACKFREE && traversal != MLBVH_TRAVERSAL_REPLAY)
+        return fail(MLBVH_ERR_INVALID_ARG, "PT traversal must be MLBVH_TRAVERSAL_STACKFREE or MLBVH_TRAVERSAL_REPLAY");
+    float4* acc = reinterpret_cast<float4*>(dAccum);
+    const float* tris = reinterpret_cast<const float*>(dTris);
+    const float* at = reinterpret_cast<const float*>(dAttribs);
+    const dim3 grid = tile_grid(w, h);
+    if (traversal == MLBVH_TRAVERSAL_REPLAY && dLeafTris)
+        k_pt<<<grid, kTileW * kTileH, 0, stream>>>(acc, cam, w, h, PlainReplayLeafTree{dNodes, tris, dRoot, dLeafTris},
+                                                   at, useSobol, maxSPP, maxDepth);
+    else if (traversal == MLBVH_TRAVERSAL_REPLAY)
+        k_pt<<<grid, kTileW * kTileH, 0, stream>>>(acc, cam, w, h, PlainReplayTree{dNodes, tris, dRoot, nullptr}, at,
+                                                   useSobol, maxSPP, maxDepth);
+    else
+        k_pt<<<grid, kTileW * kTileH, 0, stream>>>(acc, cam, w, h, PlainTree{dNodes, tris, dRoot, nullptr}, at,
+                                                   useSobol, maxSPP, maxDepth);
     MLBVH_CHECK_LAUNCH("k_pt");
     return MLBVH_OK;
 }

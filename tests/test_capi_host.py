@@ -78,6 +78,9 @@ def test_trace_and_render_reject_bad_arguments():
                              None) == 1
     assert L.mlbvh_render_ao(p, None, 8, 8, None, p, p, p, 1, 16, 1.0, 1, None, p, 1 << 30, None) == 1
     assert L.mlbvh_render_pt(p, 8, 8, ctypes.addressof(cam), p, p, p, p, 1, 4, -1, None) == 1
+    assert L.mlbvh_render_pt_ex(p, 8, 8, ctypes.addressof(cam), p, p, p, p, 1, 4, 8, 7, None, None) == 1  # traversal
+    assert b"traversal" in L.mlbvh_last_error_string()
+    assert L.mlbvh_render_pt_ex(p, 8, 8, None, p, p, p, p, 1, 4, 8, 3, None, None) == 1  # null camera
 
 
 def test_camera_lookat_matches_reference():

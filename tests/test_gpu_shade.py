@@ -170,6 +170,34 @@ def test_pt_heightfield(cuda):
     assert ref[:, 0].sum() > 0
 
 
+def test_pt_replay_walk_equals_stackfree(cuda):
+    """mlbvh_render_pt_ex with the replay walk (with and without the
+    leaf-ordered triangle copy) gives the stack-free walk's accumulators bit
+    for bit over several progressive passes: the same Hit records per ray."""
+    import torch
+    tris = scenes.heightfield_icospheres()
+    b, t, out = G.build(tris)
+    attribs = scenes.pt_attributes(len(tris), light_fraction=0.01)
+    eye, c, up, fovy = scenes.camera_heightfield()
+    w, h = 128, 96
+    cam = mb.RayGenerator.from_array(O.lookat(eye, c, up, fovy, w, h))
+    at = G.dev(attribs)
+    lt = mb.leaf_triangles(b, t)
+    accs = [torch.zeros((w * h, 4), dtype=torch.float32, device="cuda") for _ in range(3)]
+    for sobol in (1, 0):
+        for a in accs:
+            a.zero_()
+        for _ in range(3):
+            mb.render_pt(accs[0], (w, h), cam, b.m_rootNode, b.m_internals, t, at, sobol)
+            mb.render_pt(accs[1], (w, h), cam, b.m_rootNode, b.m_internals, t, at, sobol,
+                         traversal=mb.TRAVERSAL_REPLAY)
+            mb.render_pt(accs[2], (w, h), cam, b.m_rootNode, b.m_internals, t, at, sobol,
+                         traversal=mb.TRAVERSAL_REPLAY, leaf_triangles=lt)
+        torch.cuda.synchronize()
+        assert torch.equal(accs[1], accs[0]) and torch.equal(accs[2], accs[0])
+        assert float(accs[0][:, 0].sum()) > 0
+
+
 def test_pt_obj_scene(cuda, tmp_path):
     """A scene read from OBJ / MTL (mlbvh_obj_load): the Cornell-style test
     box with a lamp, path traced on the GPU, equals the oracle's pt
