@@ -335,13 +335,17 @@ def bench_precision(args, builder, qtree, d_tris, tris, cam, w, h, dev, stream, 
     }
 
 
-def bench_pt(args, dev, stream, max_over_ranks):
+def bench_pt(args, dev, stream, max_over_ranks, reference_gpu=False):
     """Path tracing (pt, main_gpu.cu:179-272) on the 212,992-triangle
     heightfield + icospheres scene with 1 % emissive triangles, 512 x 512,
     Owen-Sobol samples, the reference's 1024-bounce limit with Russian
     roulette: progressive passes (one sample per pixel each) with the
     stack-free walk and with the replay walk over leaf-ordered triangles,
-    which must leave bit-identical accumulators."""
+    which must leave bit-identical accumulators. With ``reference_gpu`` (one
+    process only) the reference's own pt kernel, compiled unmodified for
+    sm_100a (oracle/_ref/libmlbvh_ref_gpu.so), runs the same passes over the
+    same tree for comparison."""
+    import ctypes
     import torch
     import minimumlbvh_b200 as mb
     from minimumlbvh_b200 import scenes
@@ -374,6 +378,47 @@ def bench_pt(args, dev, stream, max_over_ranks):
     out["replay"]["vs_plain"] = out["plain"]["ms_per_pass"] / out["replay"]["ms_per_pass"]
     out["replay"]["accumulators_equal"] = bool(torch.equal(accs["plain"], accs["replay"]))
     out["workload"] = "heightfield + icospheres (212,992 triangles), 512x512, 1 % emissive, up to 1024 bounces"
+    if reference_gpu and os.path.exists(REF_GPU_LIB):
+        # 512 is a multiple of the reference's 16 x 16 blocks: its grid covers the image exactly
+        L = ctypes.CDLL(REF_GPU_LIB)
+        vp, i32, i64 = ctypes.c_void_p, ctypes.c_int, ctypes.c_longlong
+        L.refgpu_pt.argtypes = [vp, i64, i32, i32, vp, vp, vp, vp, vp, i32, i32, vp]
+        L.refgpu_pt.restype = i32
+        cam_arr = np.ascontiguousarray(cam.as_array(), np.float32)
+        acc = torch.zeros((w * h, 4), dtype=torch.float32, device=dev)
+
+        def ref_pass():
+            rc = L.refgpu_pt(mb._ptr(acc), w * h, w, h, cam_arr.ctypes.data, mb._ptr(b.m_rootNode),
+                             mb._ptr(b.m_internals), mb._ptr(t), mb._ptr(at), 1, 1 << 30, stream.cuda_stream)
+            if rc != 0:
+                raise RuntimeError(f"reference GPU pt: status {rc}")
+        for _ in range(args.warmup):
+            ref_pass()
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+        torch.cuda.synchronize()
+        ev[0].record(stream)
+        for _ in range(args.steps):
+            ref_pass()
+        ev[1].record(stream)
+        torch.cuda.synchronize()
+        sec = ev[0].elapsed_time(ev[1]) / 1e3
+
+        def mean_radiance(a):
+            a = a.double()
+            return float(a[:, :3].sum() / a[:, 3].sum())
+        ref_mean, our_mean = mean_radiance(acc), mean_radiance(accs["plain"])
+        out["reference_gpu"] = {
+            "what": "the reference's own pt kernel (main_gpu.cu) compiled unmodified for sm_100a, 16x16 blocks, "
+                    "over the same tree and inputs",
+            "ms_per_pass": sec * 1e3 / args.steps, "msamples_s": w * h * args.steps / sec / 1e6,
+            "plain_vs_reference": sec / args.steps / (out["plain"]["ms_per_pass"] / 1e3),
+            "replay_vs_reference": sec / args.steps / (out["replay"]["ms_per_pass"] / 1e3),
+            "mean_radiance_reference": ref_mean, "mean_radiance_ours": our_mean,
+            "accumulators_equal": bool(torch.equal(acc, accs["plain"])),
+            "note": "the reference is compiled with nvcc's default FMA contraction and CUDA's cosf/sinf; ours "
+                    "rounds like the reference's host code, so individual paths may diverge while the image "
+                    "means agree",
+        }
     return out
 
 
@@ -770,7 +815,8 @@ def main():
         del wides
         builder.build(d_tris, n, 0, sorter)
         precision = bench_precision(args, builder, qtree, d_tris, tris, cam, w, h, dev, stream, max_over_ranks)
-        pt = bench_pt(args, dev, stream, max_over_ranks)
+        pt = bench_pt(args, dev, stream, max_over_ranks,
+                      reference_gpu=not args.no_reference_gpu and rank == 0 and world == 1)
         reference_gpu = None
         if not args.no_reference_gpu and rank == 0 and world == 1:
             reference_gpu = bench_reference_gpu(args, builder, sorter, d_tris, n, cam, w, h, dev, stream,

@@ -1,6 +1,6 @@
 // Baseline infrastructure only: a launcher for the reference's OWN GPU kernels
 // (minimum_lbvh.cu: getSceneAABB, buildMortons, computeDeltas, build;
-// main_gpu.cu: ao), compiled unmodified for sm_100a from the reference
+// main_gpu.cu: ao, pt), compiled unmodified for sm_100a from the reference
 // checkout by oracle/Makefile (nothing is copied) into
 // oracle/_ref/libmlbvh_ref_gpu.so. The reference launches them through Orochi
 // (minimum_lbvh.h:783-871, main_gpu.cpp:337-350), which is not available; this
@@ -18,9 +18,10 @@
 //   * build: the grid covers ceil((n-1)/256) blocks of 256 threads for n leaves
 //     (minimum_lbvh.h:859-862), which skips the last leaf when (n-1) % 256 == 0
 //     and leaves an incomplete tree; such n are refused.
-//   * ao: the bounds test is `w <= x && h <= y` (main_gpu.cu:116), so threads
-//     past one edge write past the image; the pixel buffer must cover the whole
-//     padded grid (ceil(w/16) * 16 by ceil(h/16) * 16 pixels), checked here.
+//   * ao, pt: the bounds test is `w <= x && h <= y` (main_gpu.cu:116, 184), so
+//     threads past one edge write past the image; the pixel (accumulator)
+//     buffer must cover the whole padded grid (ceil(w/16) * 16 by
+//     ceil(h/16) * 16 pixels), checked here.
 // The reference's headers first: under nvcc, helper_math.h declares the
 // fixed-width integer types itself (helper_math.h:46-53), which a prior
 // <cstdint> would contradict.
@@ -31,6 +32,9 @@
 
 using namespace minimum_lbvh;
 
+// main_gpu.cu:10-15 (global scope); the launcher only passes the pointer on.
+struct TriangleAttrib;
+
 extern "C" __global__ void getSceneAABB(AABB* sceneAABB, const Triangle* triangles, int nTriangles);
 extern "C" __global__ void buildMortons(IndexedMorton* indexedMortons, const Triangle* triangles, int nTriangles,
                                         const AABB* sceneAABB, uint32_t buildOption);
@@ -39,6 +43,9 @@ extern "C" __global__ void build(NodeIndex* rootNode, InternalNode* internals, c
                                  int nTriangles, uint8_t* deltas, const IndexedMorton* indexedMortons);
 extern "C" __global__ void ao(uint32_t* pixels, int2 imageSize, RayGenerator rayGenerator, const NodeIndex* rootNode,
                               const InternalNode* internals, const Triangle* triangles, int useSobol);
+extern "C" __global__ void pt(uint32_t* pixels, float4* accumulators, int2 imageSize, RayGenerator rayGenerator,
+                              const NodeIndex* rootNode, const InternalNode* internals, const Triangle* triangles,
+                              const TriangleAttrib* triangleAttribs, int useSobol, int maxSPP);
 
 namespace {
 
@@ -113,6 +120,27 @@ int refgpu_ao(void* dPixels, long long bufferPixels, int w, int h, const float* 
     ao<<<grid, block, 0, static_cast<cudaStream_t>(stream)>>>(
         static_cast<uint32_t*>(dPixels), make_int2(w, h), gen, static_cast<const NodeIndex*>(dRoot),
         static_cast<const InternalNode*>(dNodes), static_cast<const Triangle*>(dTris), useSobol);
+    return status_of(cudaGetLastError());
+}
+
+// pt with 16 x 16 blocks (main_gpu.cpp:355-368): one progressive pass over
+// the float4 accumulators (w = samples so far). attribs: TriangleAttrib
+// (main_gpu.cu:10-15). bufferPixels as for refgpu_ao.
+int refgpu_pt(void* dAccum, long long bufferPixels, int w, int h, const float* camera, const void* dRoot,
+              const void* dNodes, const void* dTris, const void* dAttribs, int useSobol, int maxSPP, void* stream)
+{
+    if (w < 1 || h < 1) return -1;
+    const long long padded = (long long)blocks_of(w, 16) * 16 * (long long)blocks_of(h, 16) * 16;
+    if (bufferPixels < padded) return -2;
+    RayGenerator gen;
+    gen.m_origin = make_float3(camera[0], camera[1], camera[2]);
+    gen.m_right = make_float3(camera[3], camera[4], camera[5]);
+    gen.m_up = make_float3(camera[6], camera[7], camera[8]);
+    const dim3 grid(blocks_of(w, 16), blocks_of(h, 16), 1), block(16, 16, 1);
+    pt<<<grid, block, 0, static_cast<cudaStream_t>(stream)>>>(
+        nullptr, static_cast<float4*>(dAccum), make_int2(w, h), gen, static_cast<const NodeIndex*>(dRoot),
+        static_cast<const InternalNode*>(dNodes), static_cast<const Triangle*>(dTris),
+        static_cast<const TriangleAttrib*>(dAttribs), useSobol, maxSPP);
     return status_of(cudaGetLastError());
 }
 
