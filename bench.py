@@ -422,6 +422,107 @@ def bench_pt(args, dev, stream, max_over_ranks, reference_gpu=False):
     return out
 
 
+def sah_cost_device(nodes, root_t):
+    """Surface-area cost of a tree on the device: half areas of every internal
+    node's box and of every leaf's box over the root box's (unit costs)."""
+    import torch
+    nd = nodes
+    box = nd[:, 2:14].view(torch.float32).double().reshape(-1, 2, 6)
+    lo = torch.minimum(box[:, 0, :3], box[:, 1, :3])
+    hi = torch.maximum(box[:, 0, 3:], box[:, 1, 3:])
+
+    def half(l, h):
+        d = h - l
+        return d[..., 0] * d[..., 1] + d[..., 1] * d[..., 2] + d[..., 2] * d[..., 0]
+    leaf = nd[:, :2] < 0  # leaf bit (bit 31)
+    total = half(lo, hi).sum() + (half(box[..., :3], box[..., 3:]) * leaf).sum()
+    r = int(root_t[0].item())
+    return float(total / half(lo[r], hi[r]))
+
+
+def bench_ploc(args, wl, d_tris, n, cam, w, h, dev, stream, barrier, max_over_ranks, flush, lbvh, lbvh_forms,
+               occ_plain):
+    """The higher-quality build (mlbvh_build_ploc, radius 8; the reference's
+    counterpart is Embree's SAH build behind buildByEmbree, which cannot run
+    here) on the same scene: build time against the LBVH's, surface-area
+    cost of both trees, and AO frames over the PLOC tree (plain stack-free,
+    replay and 4-wide forms) against the same forms over the LBVH, with the
+    occlusion counts of every pixel compared with the LBVH's plain frame."""
+    import torch
+    import minimumlbvh_b200 as mb
+    launches = 0
+    pb = mb.BVHGPUBuilder()
+    ps = mb.OnesweepSort(dev.index)
+    kev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    bev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    for _ in range(args.warmup):
+        pb.buildByPLOC(d_tris, n, 0, ps, 8)
+    pb.status()
+    barrier()
+    torch.cuda.synchronize()
+    for i in range(args.steps):
+        if flush is not None:
+            flush.zero_()
+        bev[i][0].record(stream)
+        mb.profile_events(*kev[i])
+        pb.buildByPLOC(d_tris, n, 0, ps, 8)
+        bev[i][1].record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    pb.status()
+    launches += 8 * (args.warmup + args.steps)  # bounds, keys, 4 sort passes, init, the cooperative k_ploc
+    build_s = max_over_ranks(sum(a.elapsed_time(b) for a, b in bev) / 1e3) / args.steps
+    kernel_ms = float(np.mean([a.elapsed_time(b) for a, b in kev]))
+    sah_ploc = sah_cost_device(pb.m_internals[: n - 1], pb.m_rootNode)
+    sah_lbvh = sah_cost_device(lbvh.m_internals[: n - 1], lbvh.m_rootNode)
+
+    lt = mb.leaf_triangles(pb, d_tris)
+    wide = mb.WideBVH.from_builder(pb, d_tris)
+    launches += 3
+    px = torch.zeros(w * h, dtype=torch.int32, device=dev)
+
+    def plain(occluded=None):
+        mb.render_ao(px, (w, h), cam, pb.m_rootNode, pb.m_internals, d_tris, 1, wl["ns"], wl["radius"], 12345,
+                     occluded=occluded)
+
+    def replay(occluded=None):
+        mb.render_ao(px, (w, h), cam, pb.m_rootNode, pb.m_internals, d_tris, 1, wl["ns"], wl["radius"], 12345,
+                     occluded=occluded, traversal=mb.TRAVERSAL_REPLAY, leaf_triangles=lt)
+
+    def wide_form(occluded=None):
+        mb.render_ao_wide(px, (w, h), cam, wide, 1, wl["ns"], wl["radius"], 12345, occluded=occluded)
+
+    out = {"radius": 8, "build_ms": build_s * 1e3, "build_mtri_s": n / build_s / 1e6,
+           "k_ploc_ms": kernel_ms, "lbvh_build_ms": lbvh_forms["build_ms"],
+           "sah_cost": sah_ploc, "lbvh_sah_cost": sah_lbvh, "sah_vs_lbvh": sah_ploc / sah_lbvh, "forms": {}}
+    for name, frame in (("plain", plain), ("replay", replay), ("wide", wide_form)):
+        occ = torch.empty_like(occ_plain)
+        frame(occluded=occ)
+        for _ in range(args.warmup):
+            frame()
+        fev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+        barrier()
+        torch.cuda.synchronize()
+        for i in range(args.steps):
+            if flush is not None:
+                flush.zero_()
+            fev[i][0].record(stream)
+            frame()
+            fev[i][1].record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        launches += 3 * (1 + args.warmup + args.steps)
+        t = max_over_ranks(sum(a.elapsed_time(b) for a, b in fev) / 1e3) / args.steps
+        lb_ms = lbvh_forms[name]
+        out["forms"][name] = {"ms_per_frame": t * 1e3, "mrays_s": lbvh_forms["rays_per_frame"] / t / 1e6,
+                              "lbvh_ms_per_frame": lb_ms, "vs_lbvh_same_form": lb_ms / (t * 1e3),
+                              "occlusion_agreement_with_lbvh": float((occ == occ_plain).float().mean().item())}
+    out["launches"] = launches
+    out["note"] = ("PLOC: parallel locally-ordered clustering over the LBVH's Morton order, in-order node numbering "
+                   "(the LBVH's conventions), one cooperative kernel after the shared key and sort passes")
+    return out
+
+
 REF_GPU_LIB = os.path.join(ROOT, "oracle", "_ref", "libmlbvh_ref_gpu.so")
 
 
@@ -585,6 +686,7 @@ def main():
     ap.add_argument("--no-batched", action="store_true", help="skip the batched (1,024-mesh) workload")
     ap.add_argument("--batched-meshes", type=int, default=1024, help="meshes of the batched workload (small cases)")
     ap.add_argument("--no-autotune", action="store_true", help="batched workload with default launch parameters")
+    ap.add_argument("--no-ploc", action="store_true", help="skip the higher-quality (PLOC) build section")
     ap.add_argument("--no-reference-gpu", action="store_true",
                     help="skip the baseline leg running the reference's own GPU kernels")
     args = ap.parse_args()
@@ -752,6 +854,13 @@ def main():
         build_ms = [a.elapsed_time(b) for a, b in bev]
         build_total_s = max_over_ranks(sum(build_ms) / 1e3)
         builder.status()
+
+        # ---- the higher-quality (PLOC) build and the forms over its tree
+        lbvh_forms = {"build_ms": build_total_s * 1e3 / args.steps, "rays_per_frame": rays_per_frame,
+                      "plain": ao_total_s * 1e3 / args.steps, "replay": forms["replay"][0] * 1e3 / args.steps,
+                      "wide": forms["wide"][0] * 1e3 / args.steps}
+        ploc = None if args.no_ploc else bench_ploc(args, wl, d_tris, n, cam, w, h, dev, stream, barrier,
+                                                    max_over_ranks, flush, builder, lbvh_forms, occ_plain)
 
         # ---- end to end through the C ABI from host buffers: every step uploads
         # its triangles from pinned host memory, builds, renders and reads the
@@ -921,6 +1030,9 @@ def main():
     line["forms"] = form_lines
     line["precision"] = precision
     line["pt"] = pt
+    if ploc is not None:
+        line["ploc"] = ploc
+        line["gpu_launches"] += ploc["launches"]
     line["gpu_launches"] += 2 * (args.warmup + args.steps) + 8  # pt passes, its build and leaf copy
     if reference_gpu is not None:
         line["reference_gpu_baseline"] = reference_gpu

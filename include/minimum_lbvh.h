@@ -242,14 +242,7 @@ public:
     void build(const Triangle* triangles, int nTriangles, uint32_t buildOption, tinyhiponesweep::OnesweepSort& sorter,
                cudaStream_t stream)
     {
-        m_nTriangles = nTriangles;
-        const size_t nodes = nTriangles > 1 ? (size_t)nTriangles - 1 : 1;
-        if (nodes > m_capacity) {
-            if (m_internals) detail::check(cudaFreeAsync(m_internals, stream), "cudaFreeAsync");
-            detail::check(cudaMallocAsync((void**)&m_internals, sizeof(InternalNode) * nodes, stream),
-                          "cudaMallocAsync");
-            m_capacity = nodes;
-        }
+        reserve_nodes(nTriangles, stream);
         const size_t bytes = mlbvh_build_scratch_bytes((uint32_t)nTriangles);
         void* scratch = sorter.reserve(bytes, stream);
         detail::check(mlbvh_build(reinterpret_cast<const mlbvh_triangle*>(triangles), (uint32_t)nTriangles,
@@ -257,6 +250,21 @@ public:
                                   reinterpret_cast<mlbvh_node_index*>(m_rootNode),
                                   reinterpret_cast<mlbvh_aabb*>(m_sceneAABB), scratch, bytes, stream),
                       "mlbvh_build");
+    }
+    // The higher-quality build, counterpart of BVHCPUBuilder::buildByEmbree
+    // (minimum_lbvh.h:594-656) on the GPU: PLOC with neighbourhood radius
+    // `radius`, the same members and node conventions as build().
+    void buildByPLOC(const Triangle* triangles, int nTriangles, uint32_t buildOption,
+                     tinyhiponesweep::OnesweepSort& sorter, cudaStream_t stream, int radius = 8)
+    {
+        reserve_nodes(nTriangles, stream);
+        const size_t bytes = mlbvh_build_ploc_scratch_bytes((uint32_t)nTriangles);
+        void* scratch = sorter.reserve(bytes, stream);
+        detail::check(mlbvh_build_ploc(reinterpret_cast<const mlbvh_triangle*>(triangles), (uint32_t)nTriangles,
+                                       buildOption, radius, reinterpret_cast<mlbvh_internal_node*>(m_internals),
+                                       reinterpret_cast<mlbvh_node_index*>(m_rootNode),
+                                       reinterpret_cast<mlbvh_aabb*>(m_sceneAABB), scratch, bytes, stream),
+                      "mlbvh_build_ploc");
     }
     bool empty() const { return m_nTriangles == 0; }
 
@@ -266,6 +274,17 @@ public:
     int m_nTriangles = 0;
 
 private:
+    void reserve_nodes(int nTriangles, cudaStream_t stream)
+    {
+        m_nTriangles = nTriangles;
+        const size_t nodes = nTriangles > 1 ? (size_t)nTriangles - 1 : 1;
+        if (nodes > m_capacity) {
+            if (m_internals) detail::check(cudaFreeAsync(m_internals, stream), "cudaFreeAsync");
+            detail::check(cudaMallocAsync((void**)&m_internals, sizeof(InternalNode) * nodes, stream),
+                          "cudaMallocAsync");
+            m_capacity = nodes;
+        }
+    }
     size_t m_capacity = 0;
 };
 

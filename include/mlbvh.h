@@ -201,6 +201,26 @@ MLBVH_API mlbvh_status mlbvh_build_noalloc(const mlbvh_triangle* dTriangles, uin
                                            uint32_t buildOption, mlbvh_internal_node* dInternals,
                                            mlbvh_node_index* dRootNode, mlbvh_aabb* dSceneAABB, void* stream);
 
+/* The higher-quality build: the counterpart of BVHCPUBuilder::buildByEmbree
+ * (minimum_lbvh.h:594-656, Embree's SAH builder with one triangle per leaf
+ * written into the same InternalNode array). Parallel locally-ordered
+ * clustering over the Morton order of mlbvh_build (same keys, buildOption
+ * included): each cluster merges with its nearest neighbour, by the area of
+ * the union box, among the `radius` clusters on either side (1-32; 8 is a
+ * good default) when that choice is mutual, until one cluster remains. The
+ * output has mlbvh_build's form exactly: n - 1 nodes numbered in in-order (a
+ * left leaf child of node j is leaf j of the in-order, a right one leaf
+ * j + 1), parent links, the root's parent invalid, context the escape index
+ * of intersect_escape_link, so every walk and every other entry point takes
+ * it. Its boxes cost less to traverse (a smaller surface-area sum) at a
+ * longer build. One cooperative launch after the sort; needs
+ * mlbvh_build_ploc_scratch_bytes(n) bytes of scratch; timeouts are reported
+ * by mlbvh_scratch_status like mlbvh_build's. */
+MLBVH_API size_t mlbvh_build_ploc_scratch_bytes(uint32_t nTriangles);
+MLBVH_API mlbvh_status mlbvh_build_ploc(const mlbvh_triangle* dTriangles, uint32_t nTriangles, uint32_t buildOption,
+                                        int radius, mlbvh_internal_node* dInternals, mlbvh_node_index* dRootNode,
+                                        mlbvh_aabb* dSceneAABB, void* dScratch, size_t scratchBytes, void* stream);
+
 /* Synchronises `stream`, then reports MLBVH_ERR_TIMEOUT if a bounded wait of
  * the last build that used dScratch gave up (its output is then unusable),
  * else MLBVH_OK. */

@@ -70,6 +70,8 @@ def lib() -> ctypes.CDLL:
             "mlbvh_build_scratch_bytes": (sz, [u32]),
             "mlbvh_build": (i32, [_vp, u32, u32, _vp, _vp, _vp, _vp, sz, _vp]),
             "mlbvh_build_ex": (i32, [_vp, u32, u32, _vp, _vp, _vp, _vp, _vp, _vp, _vp, sz, _vp]),
+            "mlbvh_build_ploc_scratch_bytes": (sz, [u32]),
+            "mlbvh_build_ploc": (i32, [_vp, u32, u32, i32, _vp, _vp, _vp, _vp, sz, _vp]),
             "mlbvh_scratch_status": (i32, [_vp, _vp]),
             "mlbvh_trace": (i32, [_vp, _vp, _vp, _vp, _vp, u32, i32, i32, _vp]),
             "mlbvh_render_scratch_bytes": (sz, [i32, i32]),
@@ -248,6 +250,33 @@ class BVHGPUBuilder:
             _check(lib().mlbvh_build(_ptr(triangles), n, int(buildOption), _ptr(self.m_internals),
                                      _ptr(self.m_rootNode), _ptr(self.m_sceneAABB), _ptr(scratch), scratch.numel(),
                                      _stream(stream)))
+        self.m_nTriangles = n
+        self._sorter = sorter
+        return self
+
+    def buildByPLOC(self, triangles, nTriangles: int | None = None, buildOption: int = 0,
+                    sorter: OnesweepSort | None = None, radius: int = 8, stream=None):
+        """The higher-quality build (mlbvh_build_ploc), the GPU counterpart of
+        BVHCPUBuilder::buildByEmbree (minimum_lbvh.h:594-656): the same
+        members, the same node layout and numbering conventions as ``build``,
+        a tree of smaller surface-area cost."""
+        import torch
+        _require_cuda(triangles, "triangles")
+        n = int(nTriangles if nTriangles is not None else triangles.numel() // 9)
+        if n <= 0 or triangles.numel() < 9 * n:
+            raise MlbvhError(1, "nTriangles must be positive and fit the triangle tensor")
+        dev = triangles.device
+        if sorter is None:
+            sorter = OnesweepSort(dev.index)
+        scratch = sorter.reserve(lib().mlbvh_build_ploc_scratch_bytes(n))
+        if self.m_internals is None or self.m_internals.shape[0] != max(n - 1, 1) or self.m_internals.device != dev:
+            self.m_internals = torch.empty((max(n - 1, 1), 16), dtype=torch.int32, device=dev)
+        if self.m_rootNode is None or self.m_rootNode.device != dev:
+            self.m_rootNode = torch.empty(4, dtype=torch.int32, device=dev)
+            self.m_sceneAABB = torch.empty(8, dtype=torch.float32, device=dev)
+        _check(lib().mlbvh_build_ploc(_ptr(triangles), n, int(buildOption), int(radius), _ptr(self.m_internals),
+                                      _ptr(self.m_rootNode), _ptr(self.m_sceneAABB), _ptr(scratch), scratch.numel(),
+                                      _stream(stream)))
         self.m_nTriangles = n
         self._sorter = sorter
         return self

@@ -239,20 +239,12 @@ __global__ void __launch_bounds__(kBuildThreads)
 
 size_t build_scratch_bytes(uint32_t n) { return build_layout(n).total; }
 
-mlbvh_status build(const mlbvh_triangle* dTris, uint32_t n, uint32_t option, mlbvh_internal_node* dNodes,
-                   mlbvh_node_index* dRoot, mlbvh_aabb* dScene, uint32_t* dKeysOut, uint32_t* dIdxOut,
-                   uint8_t* dDeltasOut, void* dScratch, size_t scratchBytes, cudaStream_t stream, uint32_t spinLimit)
+mlbvh_status sort_leaves(const mlbvh_triangle* dTris, uint32_t n, uint32_t option, mlbvh_aabb* dScene,
+                         uint32_t* dKeysOut, uint32_t* dIdxOut, uint8_t* dDeltasOut, void* dScratch,
+                         cudaStream_t stream, uint32_t spinLimit, SortedLeaves* out)
 {
-    if (n == 0 || n >= (1u << 30)) return fail(MLBVH_ERR_INVALID_ARG, "nTriangles must be in [1, 2^30)");
-    if (!dTris || !dRoot || !dScratch) return fail(MLBVH_ERR_INVALID_ARG, "null triangles, root or scratch pointer");
-    if (n > 1 && !dNodes) return fail(MLBVH_ERR_INVALID_ARG, "null internal-node pointer");
-    if (!aligned16(dTris) || !aligned16(dNodes) || !aligned16(dScratch) || !aligned16(dRoot) || !aligned16(dScene) ||
-        !aligned16(dKeysOut) || !aligned16(dIdxOut) || !aligned16(dDeltasOut))
-        return fail(MLBVH_ERR_INVALID_ARG, "device pointers must be 16-byte aligned");
     const BuildLayout L = build_layout(n);
-    if (scratchBytes < L.total) return fail(MLBVH_ERR_INVALID_ARG, "scratch smaller than mlbvh_build_scratch_bytes(n)");
     if (spinLimit == 0) spinLimit = kDefaultSpinLimit;
-
     char* s = static_cast<char*>(dScratch);
     uint32_t* header = reinterpret_cast<uint32_t*>(s + L.header);
     float* partials = reinterpret_cast<float*>(s + L.partials);
@@ -263,7 +255,6 @@ mlbvh_status build(const mlbvh_triangle* dTris, uint32_t n, uint32_t option, mlb
     uint32_t* valsA = reinterpret_cast<uint32_t*>(s + L.valsA);
     uint32_t* valsB = reinterpret_cast<uint32_t*>(s + L.valsB);
     uint32_t* handoff = reinterpret_cast<uint32_t*>(s + L.handoff);
-    uint8_t* deltas = dDeltasOut ? dDeltasOut : reinterpret_cast<uint8_t*>(s + L.deltas);
     uint32_t* keysFinal = dKeysOut ? dKeysOut : keysA;
     uint32_t* valsFinal = dIdxOut ? dIdxOut : valsA;
     const float* tris = reinterpret_cast<const float*>(dTris);
@@ -300,10 +291,35 @@ mlbvh_status build(const mlbvh_triangle* dTris, uint32_t n, uint32_t option, mlb
         kin = kout;
         vin = vout;
     }
+    out->keys = keysFinal;
+    out->indices = valsFinal;
+    out->error = header;
+    out->handoff = handoff;
+    out->deltas = dDeltasOut ? dDeltasOut : reinterpret_cast<uint8_t*>(s + L.deltas);
+    out->spinLimit = spinLimit;
+    return MLBVH_OK;
+}
+
+mlbvh_status build(const mlbvh_triangle* dTris, uint32_t n, uint32_t option, mlbvh_internal_node* dNodes,
+                   mlbvh_node_index* dRoot, mlbvh_aabb* dScene, uint32_t* dKeysOut, uint32_t* dIdxOut,
+                   uint8_t* dDeltasOut, void* dScratch, size_t scratchBytes, cudaStream_t stream, uint32_t spinLimit)
+{
+    if (n == 0 || n >= (1u << 30)) return fail(MLBVH_ERR_INVALID_ARG, "nTriangles must be in [1, 2^30)");
+    if (!dTris || !dRoot || !dScratch) return fail(MLBVH_ERR_INVALID_ARG, "null triangles, root or scratch pointer");
+    if (n > 1 && !dNodes) return fail(MLBVH_ERR_INVALID_ARG, "null internal-node pointer");
+    if (!aligned16(dTris) || !aligned16(dNodes) || !aligned16(dScratch) || !aligned16(dRoot) || !aligned16(dScene) ||
+        !aligned16(dKeysOut) || !aligned16(dIdxOut) || !aligned16(dDeltasOut))
+        return fail(MLBVH_ERR_INVALID_ARG, "device pointers must be 16-byte aligned");
+    if (scratchBytes < build_layout(n).total)
+        return fail(MLBVH_ERR_INVALID_ARG, "scratch smaller than mlbvh_build_scratch_bytes(n)");
+    SortedLeaves sl;
+    mlbvh_status st = sort_leaves(dTris, n, option, dScene, dKeysOut, dIdxOut, dDeltasOut, dScratch, stream,
+                                  spinLimit, &sl);
+    if (st != MLBVH_OK) return st;
     ProfileEvents ev = take_profile_events();
     if (ev.start) cudaEventRecord(ev.start, stream);
-    k_build<<<(n + kBuildThreads - 1) / kBuildThreads, kBuildThreads, 0, stream>>>(tris, n, keysFinal, valsFinal, dNodes,
-                                                                                   handoff, dRoot, deltas);
+    k_build<<<(n + kBuildThreads - 1) / kBuildThreads, kBuildThreads, 0, stream>>>(
+        reinterpret_cast<const float*>(dTris), n, sl.keys, sl.indices, dNodes, sl.handoff, dRoot, sl.deltas);
     MLBVH_CHECK_LAUNCH("k_build");
     if (ev.stop) cudaEventRecord(ev.stop, stream);
     return MLBVH_OK;

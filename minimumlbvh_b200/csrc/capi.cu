@@ -57,6 +57,17 @@ const char* mlbvh_last_error_string(void) { return g_lastError.c_str(); }
 
 size_t mlbvh_build_scratch_bytes(uint32_t nTriangles) { return build_scratch_bytes(nTriangles); }
 
+size_t mlbvh_build_ploc_scratch_bytes(uint32_t nTriangles) { return build_ploc_scratch_bytes(nTriangles); }
+
+mlbvh_status mlbvh_build_ploc(const mlbvh_triangle* dTriangles, uint32_t nTriangles, uint32_t buildOption, int radius,
+                              mlbvh_internal_node* dInternals, mlbvh_node_index* dRootNode, mlbvh_aabb* dSceneAABB,
+                              void* dScratch, size_t scratchBytes, void* stream)
+{
+    clear_error();
+    return build_ploc(dTriangles, nTriangles, buildOption, radius, dInternals, dRootNode, dSceneAABB, dScratch,
+                      scratchBytes, as_stream(stream), 0);
+}
+
 mlbvh_status mlbvh_build(const mlbvh_triangle* dTriangles, uint32_t nTriangles, uint32_t buildOption,
                          mlbvh_internal_node* dInternals, mlbvh_node_index* dRootNode, mlbvh_aabb* dSceneAABB,
                          void* dScratch, size_t scratchBytes, void* stream)

@@ -38,6 +38,26 @@ mlbvh_status build(const mlbvh_triangle* dTris, uint32_t n, uint32_t option, mlb
                    uint8_t* dDeltasOut, void* dScratch, size_t scratchBytes, cudaStream_t stream, uint32_t spinLimit);
 mlbvh_status scratch_status(const void* dScratch, cudaStream_t stream);
 
+// The build chain up to the sorted leaves (scene bounds, keys, four stable
+// sort passes), shared by build() and build_ploc(); the caller has checked
+// the arguments. Pointers into the caller's scratch (or its outputs).
+struct SortedLeaves {
+    const uint32_t* keys;     // n sorted Morton keys
+    const uint32_t* indices;  // n triangle indices in that order
+    uint32_t* error;          // the build's error word (scratch offset 0)
+    uint32_t* handoff;        // n words, zeroed for build_lbvh's hand-off
+    uint8_t* deltas;          // n bytes
+    uint32_t spinLimit;       // polls per bounded wait
+};
+mlbvh_status sort_leaves(const mlbvh_triangle* dTris, uint32_t n, uint32_t option, mlbvh_aabb* dScene,
+                         uint32_t* dKeysOut, uint32_t* dIdxOut, uint8_t* dDeltasOut, void* dScratch,
+                         cudaStream_t stream, uint32_t spinLimit, SortedLeaves* out);
+
+size_t build_ploc_scratch_bytes(uint32_t n);
+mlbvh_status build_ploc(const mlbvh_triangle* dTris, uint32_t n, uint32_t option, int radius,
+                        mlbvh_internal_node* dNodes, mlbvh_node_index* dRoot, mlbvh_aabb* dScene, void* dScratch,
+                        size_t scratchBytes, cudaStream_t stream, uint32_t spinLimit);
+
 mlbvh_status trace(const mlbvh_internal_node* dNodes, const mlbvh_node_index* dRoot, const mlbvh_triangle* dTris,
                    const mlbvh_ray* dRays, mlbvh_hit* dHits, uint32_t nRays, int rayQuery, int traversal,
                    cudaStream_t stream);

@@ -1,0 +1,575 @@
+// Higher-quality build on B200: parallel locally-ordered clustering (PLOC;
+// Meister and Bittner, "Parallel Locally-Ordered Clustering for Bounding
+// Volume Hierarchy Construction", 2018) over the Morton order of the LBVH
+// build, written into the same InternalNode array as build.cu.
+//
+// The reference's higher-quality build is Embree's SAH builder behind
+// BVHCPUBuilder::buildByEmbree (minimum_lbvh.h:594-656): binary nodes, one
+// triangle per leaf, boxes of both children in each node, root parent
+// invalid. Here the nodes are numbered in in-order (node j lies between the
+// j-th and (j+1)-th leaf of a left-to-right walk), as build_lbvh's are, so
+// a left leaf child of node j is leaf j, a right one leaf j + 1, and context
+// (the escape index intersect_escape_link reads) is the in-order index of
+// the subtree's last leaf when below n - 1, else ~0, exactly build_lbvh's
+// convention: every walk, the leaf-ordered triangles, the 4-wide regrouping
+// and the quantisers take this tree unchanged.
+//
+// Clustering rule (the oracle states the same): a cluster's nearest
+// neighbour among the r clusters on either side minimises the half area of
+// the union box (dx*dy + dy*dz + dz*dx, union taken lower position first, NaN
+// above everything), ties to the smaller position: a strict order on pairs,
+// so the closest pair overall is mutual and every iteration merges. Mutual
+// nearest neighbours merge into the lower position; survivors keep order.
+//
+// Launch chain on one stream (no host synchronisation):
+//   k_scene_bounds, k_keys, k_onesweep x4   build.cu's chain (sorted leaves)
+//   k_ploc_init   cluster i = sorted leaf i (box, id, one leaf); zeroes the
+//                 look-back words and the control block
+//   k_ploc        one cooperative launch (every CTA resident), three phases:
+//     grid phase, while more than kTailClusters clusters remain: tiles of
+//       kTile clusters; a tile stages its clusters and 2r on each side in
+//       shared memory, finds the nearest neighbours of its clusters and of r
+//       on each side, keeps or merges, and finds where its survivors and new
+//       nodes go by decoupled look-back over the earlier tiles of the
+//       iteration; a grid barrier ends the iteration;
+//     tail: CTA 0 finishes the last clusters in shared memory;
+//     placement, top-down from the root: each node's in-order index is its
+//       first leaf's in-order index (handed down by its parent) plus its left
+//       child's leaf count minus one; one grid barrier per grid-phase
+//       iteration, nodes of later iterations first.
+//
+// Every wait is bounded: a look-back or barrier wait that gives up sets the
+// build's error word (reported by mlbvh_scratch_status), skips its writes,
+// and the kernel returns at the next barrier. Data written by another CTA in
+// the same launch is read through L2 (ld.global.cg / .relaxed.gpu), never L1.
+#include <algorithm>
+
+#include "capi_internal.h"
+#include "../../include/mlbvh_device.cuh"
+#include "climb.cuh"
+#include "onesweep.cuh"
+
+namespace mlbvh {
+
+namespace {
+
+constexpr int kPlocThreads = sort::kThreads;  // 256 (block_scan's width)
+constexpr int kPer = 4;                       // clusters per thread in a tile
+constexpr uint32_t kTile = kPlocThreads * kPer;
+constexpr uint32_t kTailClusters = kTile;
+constexpr int kMaxRadius = 32;
+constexpr uint32_t kSpan = kTile + 4 * kMaxRadius;  // staged clusters per tile
+constexpr int kInitThreads = 256;
+constexpr int kMaxCtasPerSm = 4;
+
+constexpr unsigned long long kFlagAggregate = 1ull << 62;
+constexpr unsigned long long kFlagInclusive = 2ull << 62;
+constexpr unsigned long long kValueMask = (1ull << 62) - 1;
+constexpr int kMergeShift = 31;  // packed counts: survivors bits 0-30, merges bits 31-61
+constexpr unsigned long long kCountMask = (1ull << 31) - 1;
+
+// clusters / merged after grid-phase iteration k sit in slot (k + 1) & 1: the
+// last tile of iteration k writes them while a CTA without tiles may still be
+// reading slot k & 1, and cannot read slot (k + 1) & 1 before the barrier.
+struct PlocControl {
+    uint32_t barrierCount, barrierGen;
+    uint32_t clusters[2], merged[2];
+};
+
+struct PlocArgs {
+    float4* clusters[2];  // per cluster {lo.xyz, id} {hi.xyz, leaf count}
+    float4* tmp;          // per new node, creation order: {lo0, id0} {hi0, id1} {lo1, cnt0} {hi1, cnt1}
+    uint2* info;          // per new node: {in-order index of its first leaf, parent's in-order index}
+    uint32_t* bounds;     // first creation index of each iteration (and the end)
+    unsigned long long* flags;  // 2 x maxTiles look-back words
+    PlocControl* ctl;
+    uint32_t* error;
+    mlbvh_internal_node* out;
+    mlbvh_node_index* root;
+    uint32_t n, maxTiles, radius, spinLimit;
+};
+
+// Scratch after build.cu's layout.
+struct PlocLayout {
+    size_t control, flags, clustersA, clustersB, tmp, info, bounds, total;
+    uint32_t maxTiles;
+};
+
+size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+
+PlocLayout ploc_layout(uint32_t n)
+{
+    PlocLayout L;
+    L.maxTiles = (n + kTile - 1) / kTile;
+    size_t o = align256(build_scratch_bytes(n));
+    L.control = o;
+    o += 256;
+    L.flags = o;
+    o = align256(o + sizeof(unsigned long long) * 2 * (size_t)L.maxTiles);
+    L.clustersA = o;
+    o = align256(o + 32 * (size_t)n);
+    L.clustersB = o;
+    o = align256(o + 32 * (size_t)n);
+    L.tmp = o;
+    o = align256(o + 64 * (size_t)n);
+    L.info = o;
+    o = align256(o + 8 * (size_t)n);
+    L.bounds = o;
+    o = align256(o + 4 * ((size_t)n + 1));
+    L.total = o;
+    return L;
+}
+
+__device__ __forceinline__ uint32_t ld_acquire(const uint32_t* p)
+{
+    uint32_t v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release(uint32_t* p, uint32_t v)
+{
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ unsigned long long ld_relaxed64(const unsigned long long* p)
+{
+    unsigned long long v;
+    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_relaxed64(unsigned long long* p, unsigned long long v)
+{
+    asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+__device__ __forceinline__ f3 xyz(float4 v) { return mk(v.x, v.y, v.z); }
+
+// Half area of the box (lo, hi) as an order key: the float's bits (never
+// negative), NaN above everything.
+__device__ __forceinline__ uint32_t area_key(f3 lo, f3 hi)
+{
+    const float dx = __fsub_rn(hi.x, lo.x), dy = __fsub_rn(hi.y, lo.y), dz = __fsub_rn(hi.z, lo.z);
+    const float a = __fadd_rn(__fadd_rn(__fmul_rn(dx, dy), __fmul_rn(dy, dz)), __fmul_rn(dz, dx));
+    return a != a ? 0xFFFFFFFFu : __float_as_uint(a);
+}
+
+// Nearest neighbours of the kPer consecutive positions p0 .. p0 + kPer - 1
+// (those in [first, end) are written to sNN); clusters [base, staged) are in
+// sLo/sHi, and staged covers r past end or reaches the last cluster. Each
+// staged box of the window is read from shared memory once for all kPer
+// positions; positions and window are clamped to the staged clusters (the
+// positions cut off that way are not written).
+__device__ __forceinline__ void nearest_group(uint32_t p0, uint32_t first, uint32_t end, uint32_t base,
+                                              uint32_t staged, int r, const float4* sLo, const float4* sHi,
+                                              uint32_t* sNN)
+{
+    f3 plo[kPer], phi[kPer];
+    uint32_t bestA[kPer], bestJ[kPer];
+#pragma unroll
+    for (int q = 0; q < kPer; ++q) {
+        const uint32_t p = min(p0 + q, staged - 1);
+        plo[q] = xyz(sLo[p - base]);
+        phi[q] = xyz(sHi[p - base]);
+        bestA[q] = 0xFFFFFFFFu;
+        bestJ[q] = 0xFFFFFFFFu;
+    }
+    const int64_t jFirst = (int64_t)p0 > r ? (int64_t)p0 - r : 0;
+    const int64_t jEnd = (int64_t)p0 + kPer + r < (int64_t)staged ? (int64_t)p0 + kPer + r : (int64_t)staged;
+    for (int64_t jj = jFirst; jj < jEnd; ++jj) {
+        const uint32_t j = (uint32_t)jj;
+        const f3 jlo = xyz(sLo[j - base]), jhi = xyz(sHi[j - base]);
+#pragma unroll
+        for (int q = 0; q < kPer; ++q) {
+            const int64_t d = jj - (int64_t)(p0 + q);
+            if (d == 0 || d < -r || d > r) continue;
+            const uint32_t a = d < 0 ? area_key(smin3(jlo, plo[q]), smax3(jhi, phi[q]))
+                                     : area_key(smin3(plo[q], jlo), smax3(phi[q], jhi));
+            // ascending j: a strict improvement keeps the smaller position on ties
+            if (a < bestA[q] || bestJ[q] == 0xFFFFFFFFu) {
+                bestA[q] = a;
+                bestJ[q] = j;
+            }
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < kPer; ++q) {
+        const uint32_t p = p0 + q;
+        if (p >= first && p < end) sNN[p - base] = bestJ[q];
+    }
+}
+
+// Keep / merge decisions of the kPer positions p0 .. (those below end).
+struct Decision {
+    uint32_t keepMask, mergeMask;
+};
+__device__ __forceinline__ Decision decide(uint32_t p0, uint32_t end, uint32_t base, const uint32_t* sNN)
+{
+    Decision dc{0u, 0u};
+#pragma unroll
+    for (int q = 0; q < kPer; ++q) {
+        const uint32_t p = p0 + q;
+        if (p >= end) continue;
+        const uint32_t j = sNN[p - base];
+        const bool mutual = sNN[j - base] == p;
+        if (!mutual || p < j) dc.keepMask |= 1u << q;
+        if (mutual && p < j) dc.mergeMask |= 1u << q;
+    }
+    return dc;
+}
+
+// Writes the new node m (creation order) that merges clusters p (lower) and
+// j and returns the merged cluster in (lo, hi).
+__device__ __forceinline__ void merge_pair(float4* __restrict__ tmp, uint32_t m, float4 plo, float4 phi, float4 jlo,
+                                           float4 jhi, float4& lo, float4& hi)
+{
+    float4* t = tmp + 4ull * m;
+    t[0] = make_float4(plo.x, plo.y, plo.z, plo.w);                    // lo0, id0
+    t[1] = make_float4(phi.x, phi.y, phi.z, jlo.w);                    // hi0, id1
+    t[2] = make_float4(jlo.x, jlo.y, jlo.z, phi.w);                    // lo1, cnt0
+    t[3] = make_float4(jhi.x, jhi.y, jhi.z, jhi.w);                    // hi1, cnt1
+    const f3 l = smin3(xyz(plo), xyz(jlo)), h = smax3(xyz(phi), xyz(jhi));
+    lo = make_float4(l.x, l.y, l.z, __uint_as_float(m));
+    hi = make_float4(h.x, h.y, h.z, __uint_as_float(__float_as_uint(phi.w) + __float_as_uint(jhi.w)));
+}
+
+// Exclusive prefix of tile t's packed counts over tiles 0 .. t-1 of this
+// iteration (warp 0; the result is valid in every lane). ok = false when a
+// wait gave up.
+__device__ unsigned long long lookback(unsigned long long* flags, uint32_t t, unsigned long long agg, uint32_t* error,
+                                       uint32_t spinLimit, bool& ok)
+{
+    const int lane = threadIdx.x & 31;
+    if (t == 0) {
+        if (lane == 0) st_relaxed64(&flags[0], kFlagInclusive | agg);
+        return 0;
+    }
+    if (lane == 0) st_relaxed64(&flags[t], kFlagAggregate | agg);
+    unsigned long long excl = 0;
+    int64_t top = (int64_t)t - 1;
+    for (;;) {
+        const int64_t k = top - lane;
+        unsigned long long v = k >= 0 ? ld_relaxed64(&flags[k]) : kFlagInclusive;
+        uint32_t spins = 0;
+        while (__any_sync(0xffffffffu, (v >> 62) == 0)) {
+            if (++spins > spinLimit) {
+                if (lane == 0) atomicOr(error, 1u);
+                ok = false;
+                if ((v >> 62) == 0) v = kFlagInclusive;
+                break;
+            }
+            __nanosleep(32);
+            if ((v >> 62) == 0) v = ld_relaxed64(&flags[k]);
+        }
+        const uint32_t incl = __ballot_sync(0xffffffffu, (v >> 62) == 2);
+        const int stop = incl ? __ffs(incl) - 1 : 31;
+        unsigned long long mine = lane <= stop ? (v & kValueMask) : 0ull;
+#pragma unroll
+        for (int o = 16; o; o >>= 1) mine += __shfl_xor_sync(0xffffffffu, mine, o);
+        excl += mine;
+        if (incl) break;
+        top -= 32;
+    }
+    if (lane == 0) st_relaxed64(&flags[t], kFlagInclusive | (excl + agg));
+    return excl;
+}
+
+// Grid-wide barrier over the cooperative launch. Returns false (in every
+// thread of the CTA) when its wait gave up or the error word is set.
+__device__ bool grid_barrier(PlocControl* ctl, uint32_t* error, uint32_t spinLimit, int* sFlag)
+{
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const uint32_t gen = ld_acquire(&ctl->barrierGen);
+        __threadfence();
+        bool ok = true;
+        if (atomicAdd(&ctl->barrierCount, 1u) == gridDim.x - 1) {
+            atomicExch(&ctl->barrierCount, 0u);
+            __threadfence();
+            st_release(&ctl->barrierGen, gen + 1);
+        } else {
+            uint32_t spins = 0;
+            while (ld_acquire(&ctl->barrierGen) == gen) {
+                if (++spins > spinLimit) {
+                    atomicOr(error, 1u);
+                    ok = false;
+                    break;
+                }
+                __nanosleep(64);
+            }
+        }
+        *sFlag = ok && ld_acquire(error) == 0;
+    }
+    __syncthreads();
+    return *sFlag != 0;
+}
+
+// Places new node m (creation order): its in-order index from the first
+// leaf handed down in info[m], the 64-byte InternalNode at that index, and
+// the hand-down for its internal children.
+__device__ __forceinline__ void place_node(const PlocArgs& a, uint32_t m)
+{
+    const float4* t = a.tmp + 4ull * m;
+    const float4 t0 = __ldcg(t), t1 = __ldcg(t + 1), t2 = __ldcg(t + 2), t3 = __ldcg(t + 3);
+    const uint2 in = __ldcg(a.info + m);
+    const uint32_t id0 = __float_as_uint(t0.w), id1 = __float_as_uint(t1.w);
+    const uint32_t cnt0 = __float_as_uint(t2.w), cnt1 = __float_as_uint(t3.w);
+    const uint32_t nInternal = a.n - 1;
+    const uint32_t rank = in.x + cnt0 - 1;
+    const uint32_t last = in.x + cnt0 + cnt1 - 1;
+    if (rank >= nInternal) return;  // only after a wait gave up (error word set)
+    uint32_t c0 = id0, c1 = id1;
+    if (!(id0 & kLeafBit) && id0 < nInternal) {
+        c0 = in.x + __float_as_uint(__ldcg(&a.tmp[4ull * id0 + 2].w)) - 1;
+        a.info[id0] = make_uint2(in.x, rank);
+    }
+    if (!(id1 & kLeafBit) && id1 < nInternal) {
+        const uint32_t off1 = in.x + cnt0;
+        c1 = off1 + __float_as_uint(__ldcg(&a.tmp[4ull * id1 + 2].w)) - 1;
+        a.info[id1] = make_uint2(off1, rank);
+    }
+    float4* o = reinterpret_cast<float4*>(a.out + rank);
+    o[0] = make_float4(__uint_as_float(c0), __uint_as_float(c1), t0.x, t0.y);
+    o[1] = make_float4(t0.z, t1.x, t1.y, t1.z);
+    o[2] = make_float4(t2.x, t2.y, t2.z, t3.x);
+    o[3] = make_float4(t3.y, t3.z, __uint_as_float(in.y), __uint_as_float(last < nInternal ? last : 0xFFFFFFFFu));
+    if (in.y == kInvalid) *a.root = rank;
+}
+
+__global__ void __launch_bounds__(kInitThreads)
+    k_ploc_init(const float* __restrict__ tris, const uint32_t* __restrict__ sortedIdx, uint32_t n,
+                float4* __restrict__ clusters, unsigned long long* __restrict__ flags, uint32_t nFlags,
+                PlocControl* __restrict__ ctl, uint32_t* __restrict__ bounds)
+{
+    const uint32_t stride = gridDim.x * blockDim.x;
+    const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+    for (uint32_t i = g; i < nFlags; i += stride) flags[i] = 0ull;
+    if (g == 0) {
+        ctl->barrierCount = 0;
+        ctl->barrierGen = 0;
+        ctl->clusters[0] = ctl->clusters[1] = n;
+        ctl->merged[0] = ctl->merged[1] = 0;
+        bounds[0] = 0;
+    }
+    for (uint32_t i = g; i < n; i += stride) {
+        uint32_t tri = sortedIdx[i];
+        if (tri >= n) tri = 0;  // only after a sort whose bounded wait gave up (error word set)
+        f3 lo, hi;
+        leaf_box(tris, n, tri, lo, hi);
+        clusters[2ull * i] = make_float4(lo.x, lo.y, lo.z, __uint_as_float(kLeafBit | tri));
+        clusters[2ull * i + 1] = make_float4(hi.x, hi.y, hi.z, __uint_as_float(1u));
+    }
+}
+
+__global__ void __launch_bounds__(kPlocThreads) k_ploc(PlocArgs a)
+{
+    __shared__ float4 sLo[kSpan], sHi[kSpan];
+    __shared__ uint32_t sNN[kSpan];
+    __shared__ uint32_t sWarp[sort::kWarps];
+    __shared__ unsigned long long sPrefix;
+    __shared__ int sOk, sFlag;
+    const int tid = threadIdx.x;
+    const int r = (int)a.radius;
+
+    uint32_t C = a.n, merged = 0, iter = 0;
+    int cur = 0;
+    // ------------------------------------------------------------ grid phase
+    while (C > kTailClusters) {
+        const uint32_t tiles = (C + kTile - 1) / kTile;
+        unsigned long long* flags = a.flags + (size_t)(iter & 1) * a.maxTiles;
+        unsigned long long* nextFlags = a.flags + (size_t)((iter + 1) & 1) * a.maxTiles;
+        const float4* src = cur ? a.clusters[1] : a.clusters[0];
+        float4* dst = cur ? a.clusters[0] : a.clusters[1];
+        for (uint32_t t = blockIdx.x; t < tiles; t += gridDim.x) {
+            const uint32_t s = t * kTile, e = min(s + kTile, C);
+            const uint32_t base = s > 2u * r ? s - 2u * r : 0u;
+            const uint32_t stagedEnd = min(C, e + 2u * r);
+            __syncthreads();  // the previous tile's shared-memory reads are done
+            for (uint32_t k = tid; k < stagedEnd - base; k += kPlocThreads) {
+                sLo[k] = __ldcg(src + 2ull * (base + k));
+                sHi[k] = __ldcg(src + 2ull * (base + k) + 1);
+            }
+            __syncthreads();
+            const uint32_t nnFirst = s > (uint32_t)r ? s - r : 0u, nnEnd = min(C, e + r);
+            for (uint32_t p0 = nnFirst + kPer * tid; p0 < nnEnd; p0 += kPer * kPlocThreads)
+                nearest_group(p0, nnFirst, nnEnd, base, stagedEnd, r, sLo, sHi, sNN);
+            __syncthreads();
+            const uint32_t p0 = s + kPer * tid;
+            const Decision dc = decide(p0, e, base, sNN);
+            uint32_t total;
+            const uint32_t before = sort::block_scan(__popc(dc.keepMask) | __popc(dc.mergeMask) << 16, sWarp, &total);
+            if (tid < 32) {
+                const unsigned long long agg =
+                    (unsigned long long)(total & 0xFFFFu) | (unsigned long long)(total >> 16) << kMergeShift;
+                bool ok = true;
+                const unsigned long long pre = lookback(flags, t, agg, a.error, a.spinLimit, ok);
+                if (tid == 0) {
+                    sPrefix = pre;
+                    sOk = ok;
+                    nextFlags[t] = 0ull;
+                    if (t == tiles - 1) {
+                        const uint32_t survivors = (uint32_t)(pre & kCountMask) + (total & 0xFFFFu);
+                        const uint32_t mergedAfter = merged + (uint32_t)((pre >> kMergeShift) & kCountMask) + (total >> 16);
+                        a.ctl->clusters[(iter + 1) & 1] = survivors;
+                        a.ctl->merged[(iter + 1) & 1] = mergedAfter;
+                        a.bounds[iter + 1] = mergedAfter;
+                    }
+                }
+            }
+            __syncthreads();
+            if (!sOk) continue;
+            uint32_t outPos = (uint32_t)(sPrefix & kCountMask) + (before & 0xFFFFu);
+            uint32_t node = merged + (uint32_t)((sPrefix >> kMergeShift) & kCountMask) + (before >> 16);
+#pragma unroll
+            for (int q = 0; q < kPer; ++q) {
+                if (!((dc.keepMask >> q) & 1u)) continue;
+                const uint32_t p = p0 + q;
+                float4 lo = sLo[p - base], hi = sHi[p - base];
+                if ((dc.mergeMask >> q) & 1u) {
+                    const uint32_t j = sNN[p - base];
+                    if (node < a.n - 1) merge_pair(a.tmp, node, lo, hi, sLo[j - base], sHi[j - base], lo, hi);
+                    ++node;
+                }
+                if (outPos < C) {
+                    dst[2ull * outPos] = lo;
+                    dst[2ull * outPos + 1] = hi;
+                }
+                ++outPos;
+            }
+        }
+        if (!grid_barrier(a.ctl, a.error, a.spinLimit, &sFlag)) return;
+        cur ^= 1;
+        ++iter;
+        C = ld_acquire(&a.ctl->clusters[iter & 1]);
+        merged = ld_acquire(&a.ctl->merged[iter & 1]);
+    }
+    const uint32_t gridIters = iter;
+
+    // ------------------------------------------------------------------ tail
+    if (blockIdx.x == 0) {
+        const float4* src = cur ? a.clusters[1] : a.clusters[0];
+        for (uint32_t k = tid; k < C; k += kPlocThreads) {
+            sLo[k] = __ldcg(src + 2ull * k);
+            sHi[k] = __ldcg(src + 2ull * k + 1);
+        }
+        __syncthreads();
+        while (C > 1) {
+            for (uint32_t p0 = kPer * tid; p0 < C; p0 += kPer * kPlocThreads)
+                nearest_group(p0, 0, C, 0, C, r, sLo, sHi, sNN);
+            __syncthreads();
+            const uint32_t p0 = kPer * tid;
+            const Decision dc = decide(p0, C, 0, sNN);
+            uint32_t total;
+            const uint32_t before = sort::block_scan(__popc(dc.keepMask) | __popc(dc.mergeMask) << 16, sWarp, &total);
+            float4 keepLo[kPer], keepHi[kPer];
+            uint32_t node = merged + (before >> 16);
+#pragma unroll
+            for (int q = 0; q < kPer; ++q) {
+                keepLo[q] = keepHi[q] = make_float4(0.f, 0.f, 0.f, 0.f);
+                if (!((dc.keepMask >> q) & 1u)) continue;
+                const uint32_t p = p0 + q;
+                keepLo[q] = sLo[p];
+                keepHi[q] = sHi[p];
+                if ((dc.mergeMask >> q) & 1u) {
+                    const uint32_t j = sNN[p];
+                    if (node < a.n - 1) merge_pair(a.tmp, node, keepLo[q], keepHi[q], sLo[j], sHi[j], keepLo[q], keepHi[q]);
+                    ++node;
+                }
+            }
+            __syncthreads();  // every read of this iteration's clusters is done
+            uint32_t outPos = before & 0xFFFFu;
+#pragma unroll
+            for (int q = 0; q < kPer; ++q) {
+                if (!((dc.keepMask >> q) & 1u)) continue;
+                sLo[outPos] = keepLo[q];
+                sHi[outPos] = keepHi[q];
+                ++outPos;
+            }
+            merged += total >> 16;
+            C = total & 0xFFFFu;
+            ++iter;
+            if (tid == 0) a.bounds[iter] = merged;
+            __syncthreads();
+        }
+        // placement of the tail's nodes, the root first
+        if (tid == 0 && merged > 0) a.info[merged - 1] = make_uint2(0u, kInvalid);
+        __syncthreads();
+        for (uint32_t k = iter; k-- > gridIters;) {
+            const uint32_t b0 = __ldcg(a.bounds + k), b1 = __ldcg(a.bounds + k + 1);
+            for (uint32_t m = b0 + tid; m < b1; m += kPlocThreads) place_node(a, m);
+            __syncthreads();
+        }
+    }
+    if (!grid_barrier(a.ctl, a.error, a.spinLimit, &sFlag)) return;
+
+    // ------------------------------------------- placement of the grid phase
+    const uint32_t stride = gridDim.x * kPlocThreads;
+    for (uint32_t k = gridIters; k-- > 0;) {
+        const uint32_t b0 = __ldcg(a.bounds + k), b1 = __ldcg(a.bounds + k + 1);
+        for (uint32_t m = b0 + blockIdx.x * kPlocThreads + tid; m < b1; m += stride) place_node(a, m);
+        if (k > 0 && !grid_barrier(a.ctl, a.error, a.spinLimit, &sFlag)) return;
+    }
+}
+
+}  // namespace
+
+size_t build_ploc_scratch_bytes(uint32_t n) { return ploc_layout(n).total; }
+
+mlbvh_status build_ploc(const mlbvh_triangle* dTris, uint32_t n, uint32_t option, int radius,
+                        mlbvh_internal_node* dNodes, mlbvh_node_index* dRoot, mlbvh_aabb* dScene, void* dScratch,
+                        size_t scratchBytes, cudaStream_t stream, uint32_t spinLimit)
+{
+    if (n == 0 || n >= (1u << 30)) return fail(MLBVH_ERR_INVALID_ARG, "nTriangles must be in [1, 2^30)");
+    if (radius < 1 || radius > kMaxRadius) return fail(MLBVH_ERR_INVALID_ARG, "radius must be in [1, 32]");
+    if (!dTris || !dRoot || !dScratch) return fail(MLBVH_ERR_INVALID_ARG, "null triangles, root or scratch pointer");
+    if (n > 1 && !dNodes) return fail(MLBVH_ERR_INVALID_ARG, "null internal-node pointer");
+    if (!aligned16(dTris) || !aligned16(dNodes) || !aligned16(dScratch) || !aligned16(dRoot) || !aligned16(dScene))
+        return fail(MLBVH_ERR_INVALID_ARG, "device pointers must be 16-byte aligned");
+    const PlocLayout L = ploc_layout(n);
+    if (scratchBytes < L.total)
+        return fail(MLBVH_ERR_INVALID_ARG, "scratch smaller than mlbvh_build_ploc_scratch_bytes(n)");
+    if (n == 1)  // one leaf: every builder's tree
+        return build(dTris, n, option, dNodes, dRoot, dScene, nullptr, nullptr, nullptr, dScratch, scratchBytes,
+                     stream, spinLimit);
+
+    SortedLeaves sl;
+    mlbvh_status st = sort_leaves(dTris, n, option, dScene, nullptr, nullptr, nullptr, dScratch, stream, spinLimit, &sl);
+    if (st != MLBVH_OK) return st;
+
+    char* s = static_cast<char*>(dScratch);
+    PlocArgs a;
+    a.clusters[0] = reinterpret_cast<float4*>(s + L.clustersA);
+    a.clusters[1] = reinterpret_cast<float4*>(s + L.clustersB);
+    a.tmp = reinterpret_cast<float4*>(s + L.tmp);
+    a.info = reinterpret_cast<uint2*>(s + L.info);
+    a.bounds = reinterpret_cast<uint32_t*>(s + L.bounds);
+    a.flags = reinterpret_cast<unsigned long long*>(s + L.flags);
+    a.ctl = reinterpret_cast<PlocControl*>(s + L.control);
+    a.error = sl.error;
+    a.out = dNodes;
+    a.root = dRoot;
+    a.n = n;
+    a.maxTiles = L.maxTiles;
+    a.radius = (uint32_t)radius;
+    a.spinLimit = sl.spinLimit;
+
+    const int sms = device_sm_count();
+    const int initBlocks = std::max(1, std::min<int>((n + kInitThreads - 1) / kInitThreads, 8 * sms));
+    k_ploc_init<<<initBlocks, kInitThreads, 0, stream>>>(reinterpret_cast<const float*>(dTris), sl.indices, n,
+                                                         a.clusters[0], a.flags, 2 * L.maxTiles, a.ctl, a.bounds);
+    MLBVH_CHECK_LAUNCH("k_ploc_init");
+
+    int perSm = 0;
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_ploc, kPlocThreads, 0);
+    if (e != cudaSuccess) return fail(MLBVH_ERR_LAUNCH, cudaGetErrorString(e));
+    if (perSm < 1) return fail(MLBVH_ERR_LAUNCH, "k_ploc does not fit on a multiprocessor");
+    const int grid = (int)std::max<uint32_t>(1u, std::min<uint32_t>(L.maxTiles, (uint32_t)(std::min(perSm, kMaxCtasPerSm) * sms)));
+    ProfileEvents ev = take_profile_events();
+    if (ev.start) cudaEventRecord(ev.start, stream);
+    void* args[] = {&a};
+    e = cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(k_ploc), dim3(grid), dim3(kPlocThreads), args, 0,
+                                    stream);
+    if (e != cudaSuccess) return fail(MLBVH_ERR_LAUNCH, cudaGetErrorString(e));
+    if (ev.stop) cudaEventRecord(ev.stop, stream);
+    return MLBVH_OK;
+}
+
+}  // namespace mlbvh

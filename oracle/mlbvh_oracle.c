@@ -361,6 +361,196 @@ int orc_build(const orc_triangle* tris, uint32_t n, uint32_t option,
     return rc;
 }
 
+/* ------------------------------------------------------------ PLOC build
+ * The higher-quality builder. The reference's is Embree's SAH build
+ * (BVHCPUBuilder::buildByEmbree, minimum_lbvh.h:594-656: one triangle per
+ * leaf, binary nodes written into the same InternalNode array, root parent
+ * invalid); Embree is a binary-only dependency. This is the published
+ * parallel locally-ordered clustering (Meister and Bittner, "Parallel
+ * Locally-Ordered Clustering for Bounding Volume Hierarchy Construction",
+ * 2018) restated over the stable Morton order of orc_build:
+ *   - clusters start as the leaves in sorted order;
+ *   - each cluster's nearest neighbour is sought among the `radius` clusters
+ *     on either side by the half surface area of the union box, the union
+ *     taken lower position first (dx*dy + dy*dz + dz*dx, NaN above
+ *     everything); ties go to the smaller position. That is a strict order
+ *     on pairs, so the closest pair overall is always mutual and every
+ *     iteration merges at least once;
+ *   - mutual nearest neighbours merge into the lower position, all other
+ *     clusters stay, and the survivors keep their order.
+ * Nodes are then numbered in in-order (node j between the j-th and the
+ * (j+1)-th leaf of a left-to-right walk), as build_lbvh's are, so the
+ * leaf-order conventions of the other walks hold; context is the in-order
+ * index of the subtree's last leaf when below n - 1, else ~0 (the escape
+ * index intersect_escape_link reads, minimum_lbvh.h:1090-1122). */
+static uint32_t ploc_area_key(orc_f3 lo, orc_f3 hi)
+{
+    float dx = hi.x - lo.x, dy = hi.y - lo.y, dz = hi.z - lo.z;
+    float a = dx * dy + dy * dz + dz * dx;
+    if (a != a) return 0xFFFFFFFFu;
+    uint32_t k;
+    memcpy(&k, &a, 4);
+    return k;
+}
+
+typedef struct {
+    uint32_t id[2];
+    orc_aabb box[2];
+    uint32_t cnt[2];
+} ploc_node;
+
+int orc_build_ploc(const orc_triangle* tris, uint32_t n, uint32_t option, int radius, orc_node* nodes,
+                   uint32_t* root)
+{
+    if (n == 0 || radius < 1) return -1;
+    orc_aabb scene;
+    orc_scene_aabb(tris, n, &scene);
+    uint32_t* keys = (uint32_t*)malloc(sizeof(uint32_t) * n);
+    uint32_t* idx = (uint32_t*)malloc(sizeof(uint32_t) * n);
+    orc_morton_keys(tris, n, option, &scene, keys);
+    for (uint32_t i = 0; i < n; ++i) idx[i] = i;
+    orc_sort_pairs(keys, idx, n);
+    free(keys);
+    if (n == 1)
+    {
+        *root = ORC_LEAF_BIT | idx[0];
+        free(idx);
+        return 0;
+    }
+    orc_aabb* box[2] = {(orc_aabb*)malloc(sizeof(orc_aabb) * n), (orc_aabb*)malloc(sizeof(orc_aabb) * n)};
+    uint32_t* id[2] = {(uint32_t*)malloc(4ull * n), (uint32_t*)malloc(4ull * n)};
+    uint32_t* cnt[2] = {(uint32_t*)malloc(4ull * n), (uint32_t*)malloc(4ull * n)};
+    uint32_t* nn = (uint32_t*)malloc(4ull * n);
+    ploc_node* tmp = (ploc_node*)malloc(sizeof(ploc_node) * (n - 1));
+    for (uint32_t i = 0; i < n; ++i)
+    {
+        aabb_set_empty(&box[0][i]);
+        for (int j = 0; j < 3; ++j) aabb_extend_p(&box[0][i], tris[idx[i]].v[j]);
+        id[0][i] = ORC_LEAF_BIT | idx[i];
+        cnt[0][i] = 1;
+    }
+    free(idx);
+    uint32_t C = n, created = 0;
+    int cur = 0, iterations = 0;
+    const uint32_t r = (uint32_t)radius;
+    while (C > 1)
+    {
+        const orc_aabb* b = box[cur];
+        for (uint32_t p = 0; p < C; ++p)
+        {
+            uint64_t best = ~0ull;
+            uint32_t lo = p > r ? p - r : 0, hi = p + r < C - 1 ? p + r : C - 1;
+            for (uint32_t j = lo; j <= hi; ++j)
+            {
+                if (j == p) continue;
+                const orc_aabb* a0 = &b[j < p ? j : p];
+                const orc_aabb* a1 = &b[j < p ? p : j];
+                uint64_t key = (uint64_t)ploc_area_key(min3(a0->lower, a1->lower), max3(a0->upper, a1->upper)) << 32 | j;
+                if (key < best) best = key;
+            }
+            nn[p] = (uint32_t)best;
+        }
+        uint32_t w = 0;
+        for (uint32_t p = 0; p < C; ++p)
+        {
+            uint32_t j = nn[p];
+            int mutual = nn[j] == p;
+            if (mutual && j < p) continue;
+            if (mutual)
+            {
+                ploc_node* t = &tmp[created];
+                t->id[0] = id[cur][p];
+                t->id[1] = id[cur][j];
+                t->box[0] = b[p];
+                t->box[1] = b[j];
+                t->cnt[0] = cnt[cur][p];
+                t->cnt[1] = cnt[cur][j];
+                box[cur ^ 1][w].lower = min3(b[p].lower, b[j].lower);
+                box[cur ^ 1][w].upper = max3(b[p].upper, b[j].upper);
+                id[cur ^ 1][w] = created++;
+                cnt[cur ^ 1][w] = cnt[cur][p] + cnt[cur][j];
+            }
+            else
+            {
+                box[cur ^ 1][w] = b[p];
+                id[cur ^ 1][w] = id[cur][p];
+                cnt[cur ^ 1][w] = cnt[cur][p];
+            }
+            ++w;
+        }
+        C = w;
+        cur ^= 1;
+        ++iterations;
+    }
+    /* in-order numbering, parents before children (creation order reversed) */
+    uint32_t* off = (uint32_t*)malloc(4ull * (n - 1));
+    uint32_t* par = (uint32_t*)malloc(4ull * (n - 1));
+    off[created - 1] = 0;
+    par[created - 1] = ORC_INVALID;
+    for (uint32_t m = created; m-- > 0;)
+    {
+        const ploc_node* t = &tmp[m];
+        uint32_t rank = off[m] + t->cnt[0] - 1;
+        uint32_t last = off[m] + t->cnt[0] + t->cnt[1] - 1;
+        orc_node* o = &nodes[rank];
+        for (int c = 0; c < 2; ++c)
+        {
+            uint32_t ch = t->id[c];
+            uint32_t co = c == 0 ? off[m] : off[m] + t->cnt[0];
+            if (ch & ORC_LEAF_BIT)
+                o->children[c] = ch;
+            else
+            {
+                o->children[c] = co + tmp[ch].cnt[0] - 1;
+                off[ch] = co;
+                par[ch] = rank;
+            }
+            o->aabbs[c] = t->box[c];
+        }
+        o->parent = par[m];
+        o->context = last < n - 1 ? last : 0xFFFFFFFFu;
+        if (par[m] == ORC_INVALID) *root = rank;
+    }
+    free(off);
+    free(par);
+    for (int k = 0; k < 2; ++k)
+    {
+        free(box[k]);
+        free(id[k]);
+        free(cnt[k]);
+    }
+    free(nn);
+    free(tmp);
+    return iterations;
+}
+
+static double half_area(const orc_aabb* b)
+{
+    double dx = (double)b->upper.x - b->lower.x, dy = (double)b->upper.y - b->lower.y,
+           dz = (double)b->upper.z - b->lower.z;
+    return dx * dy + dy * dz + dz * dx;
+}
+
+double orc_sah_cost(const orc_node* nodes, uint32_t n, uint32_t root)
+{
+    if (n < 2) return 1.0;
+    orc_aabb rb;
+    rb.lower = min3(nodes[root].aabbs[0].lower, nodes[root].aabbs[1].lower);
+    rb.upper = max3(nodes[root].aabbs[0].upper, nodes[root].aabbs[1].upper);
+    double sum = 0.0;
+    for (uint32_t i = 0; i + 1 < n; ++i)
+    {
+        const orc_aabb* b = nodes[i].aabbs;
+        orc_aabb u;
+        u.lower = min3(b[0].lower, b[1].lower);
+        u.upper = max3(b[0].upper, b[1].upper);
+        sum += half_area(&u);
+        for (int c = 0; c < 2; ++c)
+            if (nodes[i].children[c] & ORC_LEAF_BIT) sum += half_area(&b[c]);
+    }
+    return sum / half_area(&rb);
+}
+
 /* validate_lbvh (minimum_lbvh.h:415-426), iterative; returns 1 when every
  * child's split delta is <= its parent's. */
 int orc_validate(const orc_node* nodes, const uint8_t* deltas, uint32_t n, uint32_t root, int maxDelta)

@@ -80,6 +80,17 @@ int orc_build_from_keys(const uint32_t* sorted_keys, const uint32_t* sorted_indi
                         const orc_triangle* tris, uint32_t n,
                         orc_node* nodes, uint8_t* deltas, uint32_t* root);
 int orc_validate(const orc_node* nodes, const uint8_t* deltas, uint32_t n, uint32_t root, int maxDelta);
+/* The higher-quality builder (csrc/ploc.cu; the reference's is Embree's SAH
+ * build behind the same InternalNode array, minimum_lbvh.h:594-656):
+ * parallel locally-ordered clustering over orc_build's sorted order with
+ * neighbourhood radius `radius`, nodes numbered in in-order. Returns the
+ * number of clustering iterations (0 for n == 1), negative on bad input. */
+int orc_build_ploc(const orc_triangle* tris, uint32_t n, uint32_t option, int radius, orc_node* nodes,
+                   uint32_t* root);
+/* Surface-area cost of a tree: sum over internal nodes of their box's
+ * half area plus, over leaves, that of their box, each over the root box's
+ * half area (unit costs for a node visit and a triangle test). */
+double orc_sah_cost(const orc_node* nodes, uint32_t n, uint32_t root);
 int orc_check_tree(const orc_node* nodes, const orc_triangle* tris, uint32_t n, uint32_t root);
 
 /* Queries (minimum_lbvh.h:898-1137); mode 0 stack-free, 1 escape-link,

@@ -60,6 +60,8 @@ def oracle() -> ctypes.CDLL:
             "orc_build_from_keys": (_i32, [_vp, _vp, _vp, _u32, _vp, _vp, _vp]),
             "orc_validate": (_i32, [_vp, _vp, _u32, _u32, _i32]),
             "orc_check_tree": (_i32, [_vp, _vp, _u32, _u32]),
+            "orc_build_ploc": (_i32, [_vp, _u32, _u32, _i32, _vp, _vp]),
+            "orc_sah_cost": (ctypes.c_double, [_vp, _u32, _u32]),
             "orc_trace": (None, [_vp, _vp, _u32, _vp, _u32, _i32, _i32, _vp, _vp, _vp]),
             "orc_trace_replay": (None, [_vp, _vp, _u32, _vp, _u32, _i32, _i32, _vp, _vp, _vp]),
             "orc_build_wide": (None, [_vp, _u32, _vp]),
@@ -140,6 +142,29 @@ def build(tris: np.ndarray, option: int = 0):
     rc = oracle().orc_build(P(tris), n, option, P(nodes), P(deltas), P(root), P(keys), P(idx), P(scene))
     assert rc == 0
     return dict(nodes=nodes[: n - 1], deltas=deltas[: n - 1], root=int(root[0]), keys=keys, indices=idx, scene=scene)
+
+
+def build_ploc(tris: np.ndarray, option: int = 0, radius: int = 8):
+    """Oracle PLOC build: dict of nodes (n-1, 16) u32 (in-order numbering),
+    root and the number of clustering iterations."""
+    tris = np.ascontiguousarray(tris, np.float32).reshape(-1, 9)
+    n = tris.shape[0]
+    nodes = np.zeros((max(n - 1, 1), 16), np.uint32)
+    root = np.zeros(1, np.uint32)
+    it = oracle().orc_build_ploc(P(tris), n, option, radius, P(nodes), P(root))
+    assert it >= 0
+    return dict(nodes=nodes[: n - 1], root=int(root[0]), iterations=it)
+
+
+def sah_cost(nodes, root: int) -> float:
+    nodes = np.ascontiguousarray(nodes, np.uint32).reshape(-1, 16)
+    return float(oracle().orc_sah_cost(P(nodes), nodes.shape[0] + 1, root))
+
+
+def check_tree(nodes, tris, root: int) -> bool:
+    nodes = np.ascontiguousarray(nodes, np.uint32).reshape(-1, 16)
+    tris = np.ascontiguousarray(tris, np.float32).reshape(-1, 9)
+    return bool(oracle().orc_check_tree(P(nodes), P(tris), tris.shape[0], root))
 
 
 def ref_build(tris: np.ndarray, option: int = 0, parallel: int = 0):

@@ -7,6 +7,7 @@
 // out.bin: root (4 B), nodes ((n-1) x 64 B), stack-free hits (m x 32 B),
 // escape-link any-hit hits (m x 32 B).
 #include <cstdio>
+#include <cstdlib>
 #include <vector>
 
 #include "minimum_lbvh.h"
@@ -45,7 +46,8 @@ static std::vector<char> load(const char* path)
 
 int main(int argc, char** argv)
 {
-    if (argc != 4) return 2;
+    // argv[4] (optional): a PLOC radius; the tree then comes from buildByPLOC
+    if (argc != 4 && argc != 5) return 2;
     std::vector<char> tris = load(argv[1]), rays = load(argv[2]);
     const int n = (int)(tris.size() / sizeof(Triangle)), m = (int)(rays.size() / 32);
     if (n < 2 || m < 1) return 3;
@@ -63,7 +65,10 @@ int main(int argc, char** argv)
     cudaStreamCreate(&stream);
     tinyhiponesweep::OnesweepSort onesweep(0);
     BVHGPUBuilder builder("unused/minimum_lbvh.cu", "unused/");
-    builder.build(dTris, n, 0, onesweep, stream);
+    if (argc == 5)
+        builder.buildByPLOC(dTris, n, 0, onesweep, stream, std::atoi(argv[4]));
+    else
+        builder.build(dTris, n, 0, onesweep, stream);
     user_trace<<<(m + 127) / 128, 128, 0, stream>>>(dHits, dAny, dRays, m, builder.m_rootNode, builder.m_internals, dTris);
     if (cudaStreamSynchronize(stream) != cudaSuccess) return 4;
 

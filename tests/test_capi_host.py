@@ -65,6 +65,23 @@ def test_build_rejects_null_and_misaligned():
     assert b"scratch" in L.mlbvh_last_error_string()
 
 
+def test_ploc_build_rejects_bad_arguments():
+    L = mb.lib()
+    v = ctypes.c_void_p
+    for n in (1, 2, 1025, 1 << 20):
+        assert L.mlbvh_build_ploc_scratch_bytes(n) >= L.mlbvh_build_scratch_bytes(n) + 128 * n
+    for n, radius, word in ((0, 8, b"nTriangles"), (1 << 30, 8, b"nTriangles"), (10, 0, b"radius"),
+                            (10, 33, b"radius")):
+        assert L.mlbvh_build_ploc(v(256), n, 0, radius, v(256), v(256), None, v(256), 1 << 40, None) == 1
+        assert word in L.mlbvh_last_error_string()
+    assert L.mlbvh_build_ploc(None, 10, 0, 8, v(256), v(256), None, v(256), 1 << 40, None) == 1
+    assert L.mlbvh_build_ploc(v(264), 10, 0, 8, v(256), v(256), None, v(256), 1 << 40, None) == 1
+    assert b"aligned" in L.mlbvh_last_error_string()
+    need = L.mlbvh_build_ploc_scratch_bytes(10)
+    assert L.mlbvh_build_ploc(v(256), 10, 0, 8, v(256), v(256), None, v(256), need - 1, None) == 1
+    assert b"scratch" in L.mlbvh_last_error_string()
+
+
 def test_trace_and_render_reject_bad_arguments():
     L = mb.lib()
     p = ctypes.c_void_p(256)

@@ -55,3 +55,25 @@ def test_drop_in_program(cuda, tmp_path):
     np.testing.assert_array_equal(hits[:, cols], exp[:, cols])
     exp_any = O.trace(ref["nodes"], tris, ref["root"], rays, 1, 1)
     np.testing.assert_array_equal(anyh[:, cols], exp_any[:, cols])
+
+
+@pytest.mark.gpu
+def test_drop_in_program_ploc(cuda, tmp_path):
+    """The same program with the tree from BVHGPUBuilder::buildByPLOC
+    (radius 8): the oracle's PLOC tree and the oracle's Hit records over it
+    from the caller's own kernel."""
+    exe = compile_drop_in()
+    tris = scenes.heightfield_icospheres(seed=3, quads=64, spheres=16, level=2)
+    rays = scenes.random_rays(20000, tris.reshape(-1, 3).min(0), tris.reshape(-1, 3).max(0), seed=5)
+    (tmp_path / "t.bin").write_bytes(tris.tobytes())
+    (tmp_path / "r.bin").write_bytes(rays.tobytes())
+    subprocess.run([exe, str(tmp_path / "t.bin"), str(tmp_path / "r.bin"), str(tmp_path / "o.bin"), "8"], check=True)
+    out = np.frombuffer((tmp_path / "o.bin").read_bytes(), dtype=np.uint32)
+    n, m = len(tris), len(rays)
+    ref = O.build_ploc(tris, 0, 8)
+    assert int(out[0]) == ref["root"]
+    np.testing.assert_array_equal(out[1:1 + 16 * (n - 1)].reshape(n - 1, 16), ref["nodes"])
+    hits = out[1 + 16 * (n - 1):1 + 16 * (n - 1) + 8 * m].reshape(m, 8)
+    exp = O.trace(ref["nodes"], tris, ref["root"], rays, 0, 0)
+    cols = [0, 2, 3, 4, 5, 6, 7]
+    np.testing.assert_array_equal(hits[:, cols], exp[:, cols])
