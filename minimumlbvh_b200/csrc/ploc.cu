@@ -27,11 +27,13 @@
 //                 look-back words and the control block
 //   k_ploc        one cooperative launch (every CTA resident), three phases:
 //     grid phase, while more than kTailClusters clusters remain: tiles of
-//       kTile clusters; a tile stages its clusters and 2r on each side in
-//       shared memory, finds the nearest neighbours of its clusters and of r
-//       on each side, keeps or merges, and finds where its survivors and new
-//       nodes go by decoupled look-back over the earlier tiles of the
-//       iteration; a grid barrier ends the iteration;
+//       kTile - 2r clusters; a tile stages its clusters and 2r on each side
+//       in shared memory, finds the nearest neighbours of its clusters and of
+//       r on each side (kTile positions, four consecutive per thread, radius
+//       unrolled at compile time for 4, 8, 16 and 32), keeps or merges, and
+//       finds where its survivors and new nodes go by decoupled look-back
+//       (the whole CTA reading 256 earlier tiles per step) over the earlier
+//       tiles of the iteration; a grid barrier ends the iteration;
 //     tail: CTA 0 finishes the last clusters in shared memory;
 //     placement, top-down from the root: each node's in-order index is its
 //       first leaf's in-order index (handed down by its parent) plus its left
@@ -58,7 +60,13 @@ constexpr int kPer = 4;                       // clusters per thread in a tile
 constexpr uint32_t kTile = kPlocThreads * kPer;
 constexpr uint32_t kTailClusters = kTile;
 constexpr int kMaxRadius = 32;
-constexpr uint32_t kSpan = kTile + 4 * kMaxRadius;  // staged clusters per tile
+constexpr uint32_t kSpan = kTile + 2 * kMaxRadius;  // staged clusters per tile (kTile - 2r + 4r)
+// Shared-memory slot of staged cluster k: one pad slot after every four, so
+// that lanes reading clusters four apart (each thread owns four consecutive
+// positions) hit distinct banks.
+__host__ __device__ constexpr uint32_t pad(uint32_t k) { return k + (k >> 2); }
+constexpr uint32_t kSpanP = pad(kSpan);
+constexpr size_t kPlocSmem = (size_t)kSpanP * (2 * sizeof(float4) + sizeof(uint32_t));
 constexpr int kInitThreads = 256;
 constexpr int kMaxCtasPerSm = 4;
 
@@ -100,7 +108,7 @@ size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 PlocLayout ploc_layout(uint32_t n)
 {
     PlocLayout L;
-    L.maxTiles = (n + kTile - 1) / kTile;
+    L.maxTiles = (n + (kTile - 2 * kMaxRadius) - 1) / (kTile - 2 * kMaxRadius);
     size_t o = align256(build_scratch_bytes(n));
     L.control = o;
     o += 256;
@@ -143,13 +151,17 @@ __device__ __forceinline__ void st_relaxed64(unsigned long long* p, unsigned lon
 
 __device__ __forceinline__ f3 xyz(float4 v) { return mk(v.x, v.y, v.z); }
 
-// Half area of the box (lo, hi) as an order key: the float's bits (never
-// negative), NaN above everything.
-__device__ __forceinline__ uint32_t area_key(f3 lo, f3 hi)
+// Half area of the union of boxes a and b as an order key: union by
+// fminf / fmaxf (a NaN operand is ignored), area dx*dy + dy*dz + dz*dx, key
+// the bits of min(|area|, +inf): a zero area of either sign is 0, a NaN
+// area counts as +inf, and the key is symmetric in a and b.
+__device__ __forceinline__ uint32_t area_key(f3 alo, f3 ahi, f3 blo, f3 bhi)
 {
-    const float dx = __fsub_rn(hi.x, lo.x), dy = __fsub_rn(hi.y, lo.y), dz = __fsub_rn(hi.z, lo.z);
+    const float dx = __fsub_rn(fmaxf(ahi.x, bhi.x), fminf(alo.x, blo.x));
+    const float dy = __fsub_rn(fmaxf(ahi.y, bhi.y), fminf(alo.y, blo.y));
+    const float dz = __fsub_rn(fmaxf(ahi.z, bhi.z), fminf(alo.z, blo.z));
     const float a = __fadd_rn(__fadd_rn(__fmul_rn(dx, dy), __fmul_rn(dy, dz)), __fmul_rn(dz, dx));
-    return a != a ? 0xFFFFFFFFu : __float_as_uint(a);
+    return __float_as_uint(fminf(fabsf(a), __int_as_float(0x7f800000)));
 }
 
 // Nearest neighbours of the kPer consecutive positions p0 .. p0 + kPer - 1
@@ -157,7 +169,9 @@ __device__ __forceinline__ uint32_t area_key(f3 lo, f3 hi)
 // sLo/sHi, and staged covers r past end or reaches the last cluster. Each
 // staged box of the window is read from shared memory once for all kPer
 // positions; positions and window are clamped to the staged clusters (the
-// positions cut off that way are not written).
+// positions cut off that way are not written). Keys are at most +inf's bits,
+// so the first candidate always beats the initial 0xFFFFFFFF and ascending j
+// keeps the smaller position on ties.
 __device__ __forceinline__ void nearest_group(uint32_t p0, uint32_t first, uint32_t end, uint32_t base,
                                               uint32_t staged, int r, const float4* sLo, const float4* sHi,
                                               uint32_t* sNN)
@@ -167,34 +181,79 @@ __device__ __forceinline__ void nearest_group(uint32_t p0, uint32_t first, uint3
 #pragma unroll
     for (int q = 0; q < kPer; ++q) {
         const uint32_t p = min(p0 + q, staged - 1);
-        plo[q] = xyz(sLo[p - base]);
-        phi[q] = xyz(sHi[p - base]);
+        plo[q] = xyz(sLo[pad(p - base)]);
+        phi[q] = xyz(sHi[pad(p - base)]);
         bestA[q] = 0xFFFFFFFFu;
         bestJ[q] = 0xFFFFFFFFu;
     }
-    const int64_t jFirst = (int64_t)p0 > r ? (int64_t)p0 - r : 0;
-    const int64_t jEnd = (int64_t)p0 + kPer + r < (int64_t)staged ? (int64_t)p0 + kPer + r : (int64_t)staged;
-    for (int64_t jj = jFirst; jj < jEnd; ++jj) {
-        const uint32_t j = (uint32_t)jj;
-        const f3 jlo = xyz(sLo[j - base]), jhi = xyz(sHi[j - base]);
+    const int jFirst = (int)p0 > r ? (int)p0 - r : 0;
+    const int jEnd = (int)p0 + kPer + r < (int)staged ? (int)p0 + kPer + r : (int)staged;
+    for (int j = jFirst; j < jEnd; ++j) {
+        const f3 jlo = xyz(sLo[pad(j - base)]), jhi = xyz(sHi[pad(j - base)]);
 #pragma unroll
         for (int q = 0; q < kPer; ++q) {
-            const int64_t d = jj - (int64_t)(p0 + q);
+            const int d = j - (int)(p0 + q);
             if (d == 0 || d < -r || d > r) continue;
-            const uint32_t a = d < 0 ? area_key(smin3(jlo, plo[q]), smax3(jhi, phi[q]))
-                                     : area_key(smin3(plo[q], jlo), smax3(phi[q], jhi));
-            // ascending j: a strict improvement keeps the smaller position on ties
-            if (a < bestA[q] || bestJ[q] == 0xFFFFFFFFu) {
+            const uint32_t a = area_key(plo[q], phi[q], jlo, jhi);
+            if (a < bestA[q]) {
                 bestA[q] = a;
-                bestJ[q] = j;
+                bestJ[q] = (uint32_t)j;
             }
         }
     }
 #pragma unroll
     for (int q = 0; q < kPer; ++q) {
         const uint32_t p = p0 + q;
-        if (p >= first && p < end) sNN[p - base] = bestJ[q];
+        if (p >= first && p < end) sNN[pad(p - base)] = bestJ[q];
     }
+}
+
+// nearest_group with the radius fixed at compile time, for groups whose whole
+// window [p0 - R, p0 + kPer - 1 + R] is staged: the loops unroll and every
+// window test resolves at compile time.
+template <int R>
+__device__ __forceinline__ void nearest_fixed(uint32_t p0, uint32_t first, uint32_t end, uint32_t base,
+                                              const float4* sLo, const float4* sHi, uint32_t* sNN)
+{
+    f3 plo[kPer], phi[kPer];
+    uint32_t bestA[kPer], bestJ[kPer];
+#pragma unroll
+    for (int q = 0; q < kPer; ++q) {
+        plo[q] = xyz(sLo[pad(p0 + q - base)]);
+        phi[q] = xyz(sHi[pad(p0 + q - base)]);
+        bestA[q] = 0xFFFFFFFFu;
+        bestJ[q] = 0u;
+    }
+    const uint32_t j0 = p0 - R;
+#pragma unroll
+    for (int k = 0; k < 2 * R + kPer; ++k) {
+        const f3 jlo = xyz(sLo[pad(j0 + k - base)]), jhi = xyz(sHi[pad(j0 + k - base)]);
+#pragma unroll
+        for (int q = 0; q < kPer; ++q) {
+            const int d = k - R - q;
+            if (d == 0 || d < -R || d > R) continue;
+            const uint32_t a = area_key(plo[q], phi[q], jlo, jhi);
+            if (a < bestA[q]) {
+                bestA[q] = a;
+                bestJ[q] = j0 + k;
+            }
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < kPer; ++q) {
+        const uint32_t p = p0 + q;
+        if (p >= first && p < end) sNN[pad(p - base)] = bestJ[q];
+    }
+}
+
+template <int R>
+__device__ __forceinline__ void nearest(uint32_t p0, uint32_t first, uint32_t end, uint32_t base, uint32_t staged,
+                                        int r, const float4* sLo, const float4* sHi, uint32_t* sNN)
+{
+    if (R > 0 && p0 >= base + R && p0 + kPer - 1 + R < staged)
+        nearest_fixed<R>(p0, first, end, base, sLo, sHi, sNN);
+    else
+        nearest_group(p0, first, end, base, staged, r, sLo, sHi, sNN);
 }
 
 // Keep / merge decisions of the kPer positions p0 .. (those below end).
@@ -208,8 +267,8 @@ __device__ __forceinline__ Decision decide(uint32_t p0, uint32_t end, uint32_t b
     for (int q = 0; q < kPer; ++q) {
         const uint32_t p = p0 + q;
         if (p >= end) continue;
-        const uint32_t j = sNN[p - base];
-        const bool mutual = sNN[j - base] == p;
+        const uint32_t j = sNN[pad(p - base)];
+        const bool mutual = sNN[pad(j - base)] == p;
         if (!mutual || p < j) dc.keepMask |= 1u << q;
         if (mutual && p < j) dc.mergeMask |= 1u << q;
     }
@@ -232,26 +291,32 @@ __device__ __forceinline__ void merge_pair(float4* __restrict__ tmp, uint32_t m,
 }
 
 // Exclusive prefix of tile t's packed counts over tiles 0 .. t-1 of this
-// iteration (warp 0; the result is valid in every lane). ok = false when a
-// wait gave up.
+// iteration, by the whole CTA (every thread gets it): each step reads the
+// 256 tiles below `top` at once and stops at the nearest one that holds an
+// inclusive prefix, so a tile that is k tiles into its round of the grid
+// takes k / 256 + 1 steps. ok = false when a wait gave up.
+struct LookbackShared {
+    unsigned long long sum[sort::kWarps];
+    int stop[sort::kWarps];
+};
 __device__ unsigned long long lookback(unsigned long long* flags, uint32_t t, unsigned long long agg, uint32_t* error,
-                                       uint32_t spinLimit, bool& ok)
+                                       uint32_t spinLimit, bool& ok, LookbackShared& sh)
 {
-    const int lane = threadIdx.x & 31;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     if (t == 0) {
-        if (lane == 0) st_relaxed64(&flags[0], kFlagInclusive | agg);
+        if (tid == 0) st_relaxed64(&flags[0], kFlagInclusive | agg);
         return 0;
     }
-    if (lane == 0) st_relaxed64(&flags[t], kFlagAggregate | agg);
+    if (tid == 0) st_relaxed64(&flags[t], kFlagAggregate | agg);
     unsigned long long excl = 0;
     int64_t top = (int64_t)t - 1;
     for (;;) {
-        const int64_t k = top - lane;
+        const int64_t k = top - tid;
         unsigned long long v = k >= 0 ? ld_relaxed64(&flags[k]) : kFlagInclusive;
         uint32_t spins = 0;
-        while (__any_sync(0xffffffffu, (v >> 62) == 0)) {
+        while (__syncthreads_or((v >> 62) == 0)) {
             if (++spins > spinLimit) {
-                if (lane == 0) atomicOr(error, 1u);
+                if (tid == 0) atomicOr(error, 1u);
                 ok = false;
                 if ((v >> 62) == 0) v = kFlagInclusive;
                 break;
@@ -259,16 +324,25 @@ __device__ unsigned long long lookback(unsigned long long* flags, uint32_t t, un
             __nanosleep(32);
             if ((v >> 62) == 0) v = ld_relaxed64(&flags[k]);
         }
+        // the nearest inclusive tile is the lowest thread holding one
         const uint32_t incl = __ballot_sync(0xffffffffu, (v >> 62) == 2);
-        const int stop = incl ? __ffs(incl) - 1 : 31;
-        unsigned long long mine = lane <= stop ? (v & kValueMask) : 0ull;
+        if (lane == 0) sh.stop[warp] = incl ? warp * 32 + __ffs(incl) - 1 : kPlocThreads;
+        __syncthreads();
+        int stop = kPlocThreads;
+#pragma unroll
+        for (int w = 0; w < sort::kWarps; ++w) stop = min(stop, sh.stop[w]);
+        unsigned long long mine = tid <= stop ? (v & kValueMask) : 0ull;
 #pragma unroll
         for (int o = 16; o; o >>= 1) mine += __shfl_xor_sync(0xffffffffu, mine, o);
-        excl += mine;
-        if (incl) break;
-        top -= 32;
+        if (lane == 0) sh.sum[warp] = mine;
+        __syncthreads();
+#pragma unroll
+        for (int w = 0; w < sort::kWarps; ++w) excl += sh.sum[w];
+        __syncthreads();  // sh is reused by the next step
+        if (stop < kPlocThreads) break;
+        top -= kPlocThreads;
     }
-    if (lane == 0) st_relaxed64(&flags[t], kFlagInclusive | (excl + agg));
+    if (tid == 0) st_relaxed64(&flags[t], kFlagInclusive | (excl + agg));
     return excl;
 }
 
@@ -359,73 +433,77 @@ __global__ void __launch_bounds__(kInitThreads)
     }
 }
 
+// R: the radius when it is one of the compiled-in values (its groups take the
+// unrolled search), 0 for any radius (the generic search everywhere).
+template <int R>
 __global__ void __launch_bounds__(kPlocThreads) k_ploc(PlocArgs a)
 {
-    __shared__ float4 sLo[kSpan], sHi[kSpan];
-    __shared__ uint32_t sNN[kSpan];
+    extern __shared__ float4 smem[];
+    float4* sLo = smem;
+    float4* sHi = smem + kSpanP;
+    uint32_t* sNN = reinterpret_cast<uint32_t*>(smem + 2 * kSpanP);
     __shared__ uint32_t sWarp[sort::kWarps];
-    __shared__ unsigned long long sPrefix;
-    __shared__ int sOk, sFlag;
+    __shared__ LookbackShared sLook;
+    __shared__ int sFlag;
     const int tid = threadIdx.x;
-    const int r = (int)a.radius;
+    const int r = R > 0 ? R : (int)a.radius;
+    const uint32_t tileClusters = kTile - 2u * r;  // the search range of a tile is kTile positions
 
     uint32_t C = a.n, merged = 0, iter = 0;
     int cur = 0;
     // ------------------------------------------------------------ grid phase
     while (C > kTailClusters) {
-        const uint32_t tiles = (C + kTile - 1) / kTile;
+        const uint32_t tiles = (C + tileClusters - 1) / tileClusters;
         unsigned long long* flags = a.flags + (size_t)(iter & 1) * a.maxTiles;
         unsigned long long* nextFlags = a.flags + (size_t)((iter + 1) & 1) * a.maxTiles;
         const float4* src = cur ? a.clusters[1] : a.clusters[0];
         float4* dst = cur ? a.clusters[0] : a.clusters[1];
         for (uint32_t t = blockIdx.x; t < tiles; t += gridDim.x) {
-            const uint32_t s = t * kTile, e = min(s + kTile, C);
+            const uint32_t s = t * tileClusters, e = min(s + tileClusters, C);
             const uint32_t base = s > 2u * r ? s - 2u * r : 0u;
             const uint32_t stagedEnd = min(C, e + 2u * r);
             __syncthreads();  // the previous tile's shared-memory reads are done
             for (uint32_t k = tid; k < stagedEnd - base; k += kPlocThreads) {
-                sLo[k] = __ldcg(src + 2ull * (base + k));
-                sHi[k] = __ldcg(src + 2ull * (base + k) + 1);
+                sLo[pad(k)] = __ldcg(src + 2ull * (base + k));
+                sHi[pad(k)] = __ldcg(src + 2ull * (base + k) + 1);
             }
             __syncthreads();
             const uint32_t nnFirst = s > (uint32_t)r ? s - r : 0u, nnEnd = min(C, e + r);
-            for (uint32_t p0 = nnFirst + kPer * tid; p0 < nnEnd; p0 += kPer * kPlocThreads)
-                nearest_group(p0, nnFirst, nnEnd, base, stagedEnd, r, sLo, sHi, sNN);
+            {
+                const uint32_t g0 = nnFirst + kPer * tid;  // nnEnd - nnFirst <= kTile: one group per thread
+                if (g0 < nnEnd) nearest<R>(g0, nnFirst, nnEnd, base, stagedEnd, r, sLo, sHi, sNN);
+            }
             __syncthreads();
             const uint32_t p0 = s + kPer * tid;
             const Decision dc = decide(p0, e, base, sNN);
             uint32_t total;
             const uint32_t before = sort::block_scan(__popc(dc.keepMask) | __popc(dc.mergeMask) << 16, sWarp, &total);
-            if (tid < 32) {
-                const unsigned long long agg =
-                    (unsigned long long)(total & 0xFFFFu) | (unsigned long long)(total >> 16) << kMergeShift;
-                bool ok = true;
-                const unsigned long long pre = lookback(flags, t, agg, a.error, a.spinLimit, ok);
-                if (tid == 0) {
-                    sPrefix = pre;
-                    sOk = ok;
-                    nextFlags[t] = 0ull;
-                    if (t == tiles - 1) {
-                        const uint32_t survivors = (uint32_t)(pre & kCountMask) + (total & 0xFFFFu);
-                        const uint32_t mergedAfter = merged + (uint32_t)((pre >> kMergeShift) & kCountMask) + (total >> 16);
-                        a.ctl->clusters[(iter + 1) & 1] = survivors;
-                        a.ctl->merged[(iter + 1) & 1] = mergedAfter;
-                        a.bounds[iter + 1] = mergedAfter;
-                    }
+            const unsigned long long agg =
+                (unsigned long long)(total & 0xFFFFu) | (unsigned long long)(total >> 16) << kMergeShift;
+            bool ok = true;
+            const unsigned long long pre = lookback(flags, t, agg, a.error, a.spinLimit, ok, sLook);
+            if (tid == 0) {
+                nextFlags[t] = 0ull;
+                if (t == tiles - 1) {
+                    const uint32_t survivors = (uint32_t)(pre & kCountMask) + (total & 0xFFFFu);
+                    const uint32_t mergedAfter = merged + (uint32_t)((pre >> kMergeShift) & kCountMask) + (total >> 16);
+                    a.ctl->clusters[(iter + 1) & 1] = survivors;
+                    a.ctl->merged[(iter + 1) & 1] = mergedAfter;
+                    a.bounds[iter + 1] = mergedAfter;
                 }
             }
-            __syncthreads();
-            if (!sOk) continue;
-            uint32_t outPos = (uint32_t)(sPrefix & kCountMask) + (before & 0xFFFFu);
-            uint32_t node = merged + (uint32_t)((sPrefix >> kMergeShift) & kCountMask) + (before >> 16);
+            if (!ok) continue;  // uniform: every thread took the same waits
+            uint32_t outPos = (uint32_t)(pre & kCountMask) + (before & 0xFFFFu);
+            uint32_t node = merged + (uint32_t)((pre >> kMergeShift) & kCountMask) + (before >> 16);
 #pragma unroll
             for (int q = 0; q < kPer; ++q) {
                 if (!((dc.keepMask >> q) & 1u)) continue;
                 const uint32_t p = p0 + q;
-                float4 lo = sLo[p - base], hi = sHi[p - base];
+                float4 lo = sLo[pad(p - base)], hi = sHi[pad(p - base)];
                 if ((dc.mergeMask >> q) & 1u) {
-                    const uint32_t j = sNN[p - base];
-                    if (node < a.n - 1) merge_pair(a.tmp, node, lo, hi, sLo[j - base], sHi[j - base], lo, hi);
+                    const uint32_t j = sNN[pad(p - base)];
+                    if (node < a.n - 1)
+                        merge_pair(a.tmp, node, lo, hi, sLo[pad(j - base)], sHi[pad(j - base)], lo, hi);
                     ++node;
                 }
                 if (outPos < C) {
@@ -447,13 +525,15 @@ __global__ void __launch_bounds__(kPlocThreads) k_ploc(PlocArgs a)
     if (blockIdx.x == 0) {
         const float4* src = cur ? a.clusters[1] : a.clusters[0];
         for (uint32_t k = tid; k < C; k += kPlocThreads) {
-            sLo[k] = __ldcg(src + 2ull * k);
-            sHi[k] = __ldcg(src + 2ull * k + 1);
+            sLo[pad(k)] = __ldcg(src + 2ull * k);
+            sHi[pad(k)] = __ldcg(src + 2ull * k + 1);
         }
         __syncthreads();
         while (C > 1) {
-            for (uint32_t p0 = kPer * tid; p0 < C; p0 += kPer * kPlocThreads)
-                nearest_group(p0, 0, C, 0, C, r, sLo, sHi, sNN);
+            {
+                const uint32_t g0 = kPer * tid;  // C <= kTile: one group per thread
+                if (g0 < C) nearest<R>(g0, 0, C, 0, C, r, sLo, sHi, sNN);
+            }
             __syncthreads();
             const uint32_t p0 = kPer * tid;
             const Decision dc = decide(p0, C, 0, sNN);
@@ -466,11 +546,12 @@ __global__ void __launch_bounds__(kPlocThreads) k_ploc(PlocArgs a)
                 keepLo[q] = keepHi[q] = make_float4(0.f, 0.f, 0.f, 0.f);
                 if (!((dc.keepMask >> q) & 1u)) continue;
                 const uint32_t p = p0 + q;
-                keepLo[q] = sLo[p];
-                keepHi[q] = sHi[p];
+                keepLo[q] = sLo[pad(p)];
+                keepHi[q] = sHi[pad(p)];
                 if ((dc.mergeMask >> q) & 1u) {
-                    const uint32_t j = sNN[p];
-                    if (node < a.n - 1) merge_pair(a.tmp, node, keepLo[q], keepHi[q], sLo[j], sHi[j], keepLo[q], keepHi[q]);
+                    const uint32_t j = sNN[pad(p)];
+                    if (node < a.n - 1)
+                        merge_pair(a.tmp, node, keepLo[q], keepHi[q], sLo[pad(j)], sHi[pad(j)], keepLo[q], keepHi[q]);
                     ++node;
                 }
             }
@@ -479,8 +560,8 @@ __global__ void __launch_bounds__(kPlocThreads) k_ploc(PlocArgs a)
 #pragma unroll
             for (int q = 0; q < kPer; ++q) {
                 if (!((dc.keepMask >> q) & 1u)) continue;
-                sLo[outPos] = keepLo[q];
-                sHi[outPos] = keepHi[q];
+                sLo[pad(outPos)] = keepLo[q];
+                sHi[pad(outPos)] = keepHi[q];
                 ++outPos;
             }
             merged += total >> 16;
@@ -507,6 +588,27 @@ __global__ void __launch_bounds__(kPlocThreads) k_ploc(PlocArgs a)
         for (uint32_t m = b0 + blockIdx.x * kPlocThreads + tid; m < b1; m += stride) place_node(a, m);
         if (k > 0 && !grid_barrier(a.ctl, a.error, a.spinLimit, &sFlag)) return;
     }
+}
+
+// The cooperative launch of k_ploc<R> with as many CTAs as can be resident
+// (at most kMaxCtasPerSm per multiprocessor, at most one per first-iteration
+// tile).
+template <int R>
+mlbvh_status launch_ploc(PlocArgs& a, uint32_t firstTiles, cudaStream_t stream)
+{
+    cudaError_t e = cudaFuncSetAttribute(k_ploc<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPlocSmem);
+    int perSm = 0;
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_ploc<R>, kPlocThreads, kPlocSmem);
+    if (e != cudaSuccess) return fail(MLBVH_ERR_LAUNCH, cudaGetErrorString(e));
+    if (perSm < 1) return fail(MLBVH_ERR_LAUNCH, "k_ploc does not fit on a multiprocessor");
+    const uint32_t sms = (uint32_t)device_sm_count();
+    const int grid = (int)std::max<uint32_t>(
+        1u, std::min<uint32_t>(firstTiles, (uint32_t)std::min(perSm, kMaxCtasPerSm) * sms));
+    void* args[] = {&a};
+    e = cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(k_ploc<R>), dim3(grid), dim3(kPlocThreads), args,
+                                    kPlocSmem, stream);
+    if (e != cudaSuccess) return fail(MLBVH_ERR_LAUNCH, cudaGetErrorString(e));
+    return MLBVH_OK;
 }
 
 }  // namespace
@@ -557,17 +659,17 @@ mlbvh_status build_ploc(const mlbvh_triangle* dTris, uint32_t n, uint32_t option
                                                          a.clusters[0], a.flags, 2 * L.maxTiles, a.ctl, a.bounds);
     MLBVH_CHECK_LAUNCH("k_ploc_init");
 
-    int perSm = 0;
-    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_ploc, kPlocThreads, 0);
-    if (e != cudaSuccess) return fail(MLBVH_ERR_LAUNCH, cudaGetErrorString(e));
-    if (perSm < 1) return fail(MLBVH_ERR_LAUNCH, "k_ploc does not fit on a multiprocessor");
-    const int grid = (int)std::max<uint32_t>(1u, std::min<uint32_t>(L.maxTiles, (uint32_t)(std::min(perSm, kMaxCtasPerSm) * sms)));
     ProfileEvents ev = take_profile_events();
     if (ev.start) cudaEventRecord(ev.start, stream);
-    void* args[] = {&a};
-    e = cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(k_ploc), dim3(grid), dim3(kPlocThreads), args, 0,
-                                    stream);
-    if (e != cudaSuccess) return fail(MLBVH_ERR_LAUNCH, cudaGetErrorString(e));
+    const uint32_t firstTiles = (n + (kTile - 2u * radius) - 1) / (kTile - 2u * radius);
+    switch (radius) {
+        case 4: st = launch_ploc<4>(a, firstTiles, stream); break;
+        case 8: st = launch_ploc<8>(a, firstTiles, stream); break;
+        case 16: st = launch_ploc<16>(a, firstTiles, stream); break;
+        case 32: st = launch_ploc<32>(a, firstTiles, stream); break;
+        default: st = launch_ploc<0>(a, firstTiles, stream); break;
+    }
+    if (st != MLBVH_OK) return st;
     if (ev.stop) cudaEventRecord(ev.stop, stream);
     return MLBVH_OK;
 }

@@ -371,11 +371,12 @@ int orc_build(const orc_triangle* tris, uint32_t n, uint32_t option,
  * 2018) restated over the stable Morton order of orc_build:
  *   - clusters start as the leaves in sorted order;
  *   - each cluster's nearest neighbour is sought among the `radius` clusters
- *     on either side by the half surface area of the union box, the union
- *     taken lower position first (dx*dy + dy*dz + dz*dx, NaN above
- *     everything); ties go to the smaller position. That is a strict order
- *     on pairs, so the closest pair overall is always mutual and every
- *     iteration merges at least once;
+ *     on either side by the half surface area of the union box (the union by
+ *     fminf / fmaxf, which ignore a NaN operand; area dx*dy + dy*dz + dz*dx;
+ *     the order key is the bit pattern of min(|area|, +inf), so a zero area
+ *     of either sign is 0 and a NaN area counts as +inf); ties go to the
+ *     smaller position. That is a strict order on pairs, so the closest pair
+ *     overall is always mutual and every iteration merges at least once;
  *   - mutual nearest neighbours merge into the lower position, all other
  *     clusters stay, and the survivors keep their order.
  * Nodes are then numbered in in-order (node j between the j-th and the
@@ -383,11 +384,14 @@ int orc_build(const orc_triangle* tris, uint32_t n, uint32_t option,
  * leaf-order conventions of the other walks hold; context is the in-order
  * index of the subtree's last leaf when below n - 1, else ~0 (the escape
  * index intersect_escape_link reads, minimum_lbvh.h:1090-1122). */
-static uint32_t ploc_area_key(orc_f3 lo, orc_f3 hi)
+static uint32_t ploc_area_key(const orc_aabb* a0, const orc_aabb* a1)
 {
-    float dx = hi.x - lo.x, dy = hi.y - lo.y, dz = hi.z - lo.z;
-    float a = dx * dy + dy * dz + dz * dx;
-    if (a != a) return 0xFFFFFFFFu;
+    float lx = fminf(a0->lower.x, a1->lower.x), ly = fminf(a0->lower.y, a1->lower.y);
+    float lz = fminf(a0->lower.z, a1->lower.z);
+    float hx = fmaxf(a0->upper.x, a1->upper.x), hy = fmaxf(a0->upper.y, a1->upper.y);
+    float hz = fmaxf(a0->upper.z, a1->upper.z);
+    float dx = hx - lx, dy = hy - ly, dz = hz - lz;
+    float a = fminf(fabsf(dx * dy + dy * dz + dz * dx), INFINITY);
     uint32_t k;
     memcpy(&k, &a, 4);
     return k;
@@ -443,9 +447,7 @@ int orc_build_ploc(const orc_triangle* tris, uint32_t n, uint32_t option, int ra
             for (uint32_t j = lo; j <= hi; ++j)
             {
                 if (j == p) continue;
-                const orc_aabb* a0 = &b[j < p ? j : p];
-                const orc_aabb* a1 = &b[j < p ? p : j];
-                uint64_t key = (uint64_t)ploc_area_key(min3(a0->lower, a1->lower), max3(a0->upper, a1->upper)) << 32 | j;
+                uint64_t key = (uint64_t)ploc_area_key(&b[p], &b[j]) << 32 | j;
                 if (key < best) best = key;
             }
             nn[p] = (uint32_t)best;
