@@ -35,10 +35,11 @@
 //       (the whole CTA reading 256 earlier tiles per step) over the earlier
 //       tiles of the iteration; a grid barrier ends the iteration;
 //     tail: CTA 0 finishes the last clusters in shared memory;
-//     placement, top-down from the root: each node's in-order index is its
-//       first leaf's in-order index (handed down by its parent) plus its left
-//       child's leaf count minus one; one grid barrier per grid-phase
-//       iteration, nodes of later iterations first.
+//     placement, top-down from the root without barriers: each node's
+//       in-order index is its first leaf's in-order index (handed down by its
+//       parent) plus its left child's leaf count minus one; warps take the
+//       nodes in descending creation order (parents before children) and a
+//       lane places its node once its parent has handed the first leaf down.
 //
 // Every wait is bounded: a look-back or barrier wait that gives up sets the
 // build's error word (reported by mlbvh_scratch_status), skips its writes,
@@ -68,6 +69,8 @@ __host__ __device__ constexpr uint32_t pad(uint32_t k) { return k + (k >> 2); }
 constexpr uint32_t kSpanP = pad(kSpan);
 constexpr size_t kPlocSmem = (size_t)kSpanP * (2 * sizeof(float4) + sizeof(uint32_t));
 constexpr int kInitThreads = 256;
+constexpr uint32_t kPlaceChunk = 128;  // placement positions a warp takes at a time
+constexpr uint32_t kUnset = 0xFFFFFFFFu;
 constexpr int kMaxCtasPerSm = 4;
 
 constexpr unsigned long long kFlagAggregate = 1ull << 62;
@@ -82,13 +85,14 @@ constexpr unsigned long long kCountMask = (1ull << 31) - 1;
 struct PlocControl {
     uint32_t barrierCount, barrierGen;
     uint32_t clusters[2], merged[2];
+    uint32_t placeNext;  // next position of the placement order to hand out
 };
 
 struct PlocArgs {
     float4* clusters[2];  // per cluster {lo.xyz, id} {hi.xyz, leaf count}
     float4* tmp;          // per new node, creation order: {lo0, id0} {hi0, id1} {lo1, cnt0} {hi1, cnt1}
-    uint2* info;          // per new node: {in-order index of its first leaf, parent's in-order index}
-    uint32_t* bounds;     // first creation index of each iteration (and the end)
+    unsigned long long* info;  // per new node: in-order index of its first leaf | parent's in-order index << 32
+                               // (first leaf ~0: not handed down yet)
     unsigned long long* flags;  // 2 x maxTiles look-back words
     PlocControl* ctl;
     uint32_t* error;
@@ -99,7 +103,7 @@ struct PlocArgs {
 
 // Scratch after build.cu's layout.
 struct PlocLayout {
-    size_t control, flags, clustersA, clustersB, tmp, info, bounds, total;
+    size_t control, flags, clustersA, clustersB, tmp, info, total;
     uint32_t maxTiles;
 };
 
@@ -122,8 +126,6 @@ PlocLayout ploc_layout(uint32_t n)
     o = align256(o + 64 * (size_t)n);
     L.info = o;
     o = align256(o + 8 * (size_t)n);
-    L.bounds = o;
-    o = align256(o + 4 * ((size_t)n + 1));
     L.total = o;
     return L;
 }
@@ -376,52 +378,117 @@ __device__ bool grid_barrier(PlocControl* ctl, uint32_t* error, uint32_t spinLim
     return *sFlag != 0;
 }
 
-// Places new node m (creation order): its in-order index from the first
-// leaf handed down in info[m], the 64-byte InternalNode at that index, and
-// the hand-down for its internal children.
-__device__ __forceinline__ void place_node(const PlocArgs& a, uint32_t m)
+// What a node's placement reads that does not depend on its parent: its
+// creation record and the left-leaf counts of its internal children. Loaded
+// before the lane waits for the parent's hand-down.
+struct NodeRecord {
+    float4 t0, t1, t2, t3;  // {lo0, id0} {hi0, id1} {lo1, cnt0} {hi1, cnt1}
+    uint32_t left0, left1;  // left-leaf counts of internal children 0 / 1
+};
+__device__ __forceinline__ NodeRecord load_record(const PlocArgs& a, uint32_t m)
 {
+    NodeRecord r;
     const float4* t = a.tmp + 4ull * m;
-    const float4 t0 = __ldcg(t), t1 = __ldcg(t + 1), t2 = __ldcg(t + 2), t3 = __ldcg(t + 3);
-    const uint2 in = __ldcg(a.info + m);
-    const uint32_t id0 = __float_as_uint(t0.w), id1 = __float_as_uint(t1.w);
-    const uint32_t cnt0 = __float_as_uint(t2.w), cnt1 = __float_as_uint(t3.w);
+    r.t0 = __ldcg(t);
+    r.t1 = __ldcg(t + 1);
+    r.t2 = __ldcg(t + 2);
+    r.t3 = __ldcg(t + 3);
+    const uint32_t id0 = __float_as_uint(r.t0.w), id1 = __float_as_uint(r.t1.w), nInternal = a.n - 1;
+    r.left0 = (!(id0 & kLeafBit) && id0 < nInternal) ? __float_as_uint(__ldcg(&a.tmp[4ull * id0 + 2].w)) : 0u;
+    r.left1 = (!(id1 & kLeafBit) && id1 < nInternal) ? __float_as_uint(__ldcg(&a.tmp[4ull * id1 + 2].w)) : 0u;
+    return r;
+}
+
+// Places node `rec` given its hand-down word `in` (first leaf's in-order
+// index | parent's in-order index << 32): the 64-byte InternalNode at its
+// in-order index, and the hand-down words of its internal children (one
+// 8-byte store each, read whole by the child's lane).
+__device__ __forceinline__ void place_node(const PlocArgs& a, const NodeRecord& rec, unsigned long long in)
+{
+    const uint32_t first = (uint32_t)in, parent = (uint32_t)(in >> 32);
+    const uint32_t id0 = __float_as_uint(rec.t0.w), id1 = __float_as_uint(rec.t1.w);
+    const uint32_t cnt0 = __float_as_uint(rec.t2.w), cnt1 = __float_as_uint(rec.t3.w);
     const uint32_t nInternal = a.n - 1;
-    const uint32_t rank = in.x + cnt0 - 1;
-    const uint32_t last = in.x + cnt0 + cnt1 - 1;
+    const uint32_t rank = first + cnt0 - 1;
+    const uint32_t last = first + cnt0 + cnt1 - 1;
     if (rank >= nInternal) return;  // only after a wait gave up (error word set)
     uint32_t c0 = id0, c1 = id1;
     if (!(id0 & kLeafBit) && id0 < nInternal) {
-        c0 = in.x + __float_as_uint(__ldcg(&a.tmp[4ull * id0 + 2].w)) - 1;
-        a.info[id0] = make_uint2(in.x, rank);
+        c0 = first + rec.left0 - 1;
+        st_relaxed64(a.info + id0, (unsigned long long)first | (unsigned long long)rank << 32);
     }
     if (!(id1 & kLeafBit) && id1 < nInternal) {
-        const uint32_t off1 = in.x + cnt0;
-        c1 = off1 + __float_as_uint(__ldcg(&a.tmp[4ull * id1 + 2].w)) - 1;
-        a.info[id1] = make_uint2(off1, rank);
+        const uint32_t off1 = first + cnt0;
+        c1 = off1 + rec.left1 - 1;
+        st_relaxed64(a.info + id1, (unsigned long long)off1 | (unsigned long long)rank << 32);
     }
     float4* o = reinterpret_cast<float4*>(a.out + rank);
-    o[0] = make_float4(__uint_as_float(c0), __uint_as_float(c1), t0.x, t0.y);
-    o[1] = make_float4(t0.z, t1.x, t1.y, t1.z);
-    o[2] = make_float4(t2.x, t2.y, t2.z, t3.x);
-    o[3] = make_float4(t3.y, t3.z, __uint_as_float(in.y), __uint_as_float(last < nInternal ? last : 0xFFFFFFFFu));
-    if (in.y == kInvalid) *a.root = rank;
+    o[0] = make_float4(__uint_as_float(c0), __uint_as_float(c1), rec.t0.x, rec.t0.y);
+    o[1] = make_float4(rec.t0.z, rec.t1.x, rec.t1.y, rec.t1.z);
+    o[2] = make_float4(rec.t2.x, rec.t2.y, rec.t2.z, rec.t3.x);
+    o[3] = make_float4(rec.t3.y, rec.t3.z, __uint_as_float(parent), __uint_as_float(last < nInternal ? last : 0xFFFFFFFFu));
+    if (parent == kInvalid) *a.root = rank;
+}
+
+// Placement of all n - 1 nodes, in descending creation order (a parent is
+// always created after its children): a warp takes kPlaceChunk positions at a
+// time, 32 per step; each lane loads its node's record, then places the node
+// once the node's hand-down word is set, and lanes of one step that wait on
+// each other resolve over the step's rounds. The lowest unplaced position
+// always has its parent placed and every CTA is resident, so each wait ends;
+// it is still bounded.
+__device__ void place_all(const PlocArgs& a)
+{
+    const int lane = threadIdx.x & 31;
+    const uint32_t total = a.n - 1;
+    for (;;) {
+        uint32_t c0 = 0;
+        if (lane == 0) c0 = atomicAdd(&a.ctl->placeNext, kPlaceChunk);
+        c0 = __shfl_sync(0xffffffffu, c0, 0);
+        if (c0 >= total) return;
+        for (uint32_t step = 0; step < kPlaceChunk; step += 32) {
+            const uint32_t pos = c0 + step + lane;
+            bool done = pos >= total;
+            const uint32_t m = done ? 0u : total - 1 - pos;
+            NodeRecord rec;
+            if (!done) rec = load_record(a, m);
+            uint32_t spins = 0;
+            while (!__all_sync(0xffffffffu, done)) {
+                if (!done) {
+                    const unsigned long long in = ld_relaxed64(a.info + m);
+                    if ((uint32_t)in != kUnset) {
+                        place_node(a, rec, in);
+                        done = true;
+                    }
+                }
+                __syncwarp();
+                if (!__all_sync(0xffffffffu, done)) {
+                    if (++spins > a.spinLimit) {
+                        if (lane == 0) atomicOr(a.error, 1u);
+                        return;
+                    }
+                    __nanosleep(32);
+                }
+            }
+        }
+    }
 }
 
 __global__ void __launch_bounds__(kInitThreads)
     k_ploc_init(const float* __restrict__ tris, const uint32_t* __restrict__ sortedIdx, uint32_t n,
                 float4* __restrict__ clusters, unsigned long long* __restrict__ flags, uint32_t nFlags,
-                PlocControl* __restrict__ ctl, uint32_t* __restrict__ bounds)
+                PlocControl* __restrict__ ctl, unsigned long long* __restrict__ info)
 {
     const uint32_t stride = gridDim.x * blockDim.x;
     const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
     for (uint32_t i = g; i < nFlags; i += stride) flags[i] = 0ull;
+    for (uint32_t i = g; i + 1 < n; i += stride) info[i] = ~0ull;
     if (g == 0) {
         ctl->barrierCount = 0;
         ctl->barrierGen = 0;
         ctl->clusters[0] = ctl->clusters[1] = n;
         ctl->merged[0] = ctl->merged[1] = 0;
-        bounds[0] = 0;
+        ctl->placeNext = 0;
     }
     for (uint32_t i = g; i < n; i += stride) {
         uint32_t tri = sortedIdx[i];
@@ -489,7 +556,6 @@ __global__ void __launch_bounds__(kPlocThreads) k_ploc(PlocArgs a)
                     const uint32_t mergedAfter = merged + (uint32_t)((pre >> kMergeShift) & kCountMask) + (total >> 16);
                     a.ctl->clusters[(iter + 1) & 1] = survivors;
                     a.ctl->merged[(iter + 1) & 1] = mergedAfter;
-                    a.bounds[iter + 1] = mergedAfter;
                 }
             }
             if (!ok) continue;  // uniform: every thread took the same waits
@@ -519,7 +585,6 @@ __global__ void __launch_bounds__(kPlocThreads) k_ploc(PlocArgs a)
         C = ld_acquire(&a.ctl->clusters[iter & 1]);
         merged = ld_acquire(&a.ctl->merged[iter & 1]);
     }
-    const uint32_t gridIters = iter;
 
     // ------------------------------------------------------------------ tail
     if (blockIdx.x == 0) {
@@ -566,28 +631,16 @@ __global__ void __launch_bounds__(kPlocThreads) k_ploc(PlocArgs a)
             }
             merged += total >> 16;
             C = total & 0xFFFFu;
-            ++iter;
-            if (tid == 0) a.bounds[iter] = merged;
             __syncthreads();
         }
-        // placement of the tail's nodes, the root first
-        if (tid == 0 && merged > 0) a.info[merged - 1] = make_uint2(0u, kInvalid);
-        __syncthreads();
-        for (uint32_t k = iter; k-- > gridIters;) {
-            const uint32_t b0 = __ldcg(a.bounds + k), b1 = __ldcg(a.bounds + k + 1);
-            for (uint32_t m = b0 + tid; m < b1; m += kPlocThreads) place_node(a, m);
-            __syncthreads();
-        }
+        // the root (the last node made) has the first leaf and no parent
+        if (tid == 0 && merged > 0)
+            st_relaxed64(a.info + merged - 1, (unsigned long long)kInvalid << 32);
     }
     if (!grid_barrier(a.ctl, a.error, a.spinLimit, &sFlag)) return;
 
-    // ------------------------------------------- placement of the grid phase
-    const uint32_t stride = gridDim.x * kPlocThreads;
-    for (uint32_t k = gridIters; k-- > 0;) {
-        const uint32_t b0 = __ldcg(a.bounds + k), b1 = __ldcg(a.bounds + k + 1);
-        for (uint32_t m = b0 + blockIdx.x * kPlocThreads + tid; m < b1; m += stride) place_node(a, m);
-        if (k > 0 && !grid_barrier(a.ctl, a.error, a.spinLimit, &sFlag)) return;
-    }
+    // ------------------------------------------------------------- placement
+    place_all(a);
 }
 
 // The cooperative launch of k_ploc<R> with as many CTAs as can be resident
@@ -641,8 +694,7 @@ mlbvh_status build_ploc(const mlbvh_triangle* dTris, uint32_t n, uint32_t option
     a.clusters[0] = reinterpret_cast<float4*>(s + L.clustersA);
     a.clusters[1] = reinterpret_cast<float4*>(s + L.clustersB);
     a.tmp = reinterpret_cast<float4*>(s + L.tmp);
-    a.info = reinterpret_cast<uint2*>(s + L.info);
-    a.bounds = reinterpret_cast<uint32_t*>(s + L.bounds);
+    a.info = reinterpret_cast<unsigned long long*>(s + L.info);
     a.flags = reinterpret_cast<unsigned long long*>(s + L.flags);
     a.ctl = reinterpret_cast<PlocControl*>(s + L.control);
     a.error = sl.error;
@@ -656,7 +708,7 @@ mlbvh_status build_ploc(const mlbvh_triangle* dTris, uint32_t n, uint32_t option
     const int sms = device_sm_count();
     const int initBlocks = std::max(1, std::min<int>((n + kInitThreads - 1) / kInitThreads, 8 * sms));
     k_ploc_init<<<initBlocks, kInitThreads, 0, stream>>>(reinterpret_cast<const float*>(dTris), sl.indices, n,
-                                                         a.clusters[0], a.flags, 2 * L.maxTiles, a.ctl, a.bounds);
+                                                         a.clusters[0], a.flags, 2 * L.maxTiles, a.ctl, a.info);
     MLBVH_CHECK_LAUNCH("k_ploc_init");
 
     ProfileEvents ev = take_profile_events();
