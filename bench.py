@@ -377,6 +377,35 @@ def bench_pt(args, dev, stream, max_over_ranks, reference_gpu=False):
         accs[name] = acc
     out["replay"]["vs_plain"] = out["plain"]["ms_per_pass"] / out["replay"]["ms_per_pass"]
     out["replay"]["accumulators_equal"] = bool(torch.equal(accs["plain"], accs["replay"]))
+    if not args.no_ploc:
+        # the replay walk over the higher-quality (PLOC, radius 8) tree of the same
+        # triangles: the same closest distances; a path may take another branch
+        # only where two triangles meet a ray at the same distance
+        pb = mb.BVHGPUBuilder().buildByPLOC(t, n, 0, mb.OnesweepSort(dev.index), 8)
+        pb.status()
+        plt = mb.leaf_triangles(pb, t)
+        acc = torch.zeros((w * h, 4), dtype=torch.float32, device=dev)
+        for _ in range(args.warmup):
+            mb.render_pt(acc, (w, h), cam, pb.m_rootNode, pb.m_internals, t, at, 1, traversal=mb.TRAVERSAL_REPLAY,
+                         leaf_triangles=plt)
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+        torch.cuda.synchronize()
+        ev[0].record(stream)
+        for _ in range(args.steps):
+            mb.render_pt(acc, (w, h), cam, pb.m_rootNode, pb.m_internals, t, at, 1, traversal=mb.TRAVERSAL_REPLAY,
+                         leaf_triangles=plt)
+        ev[1].record(stream)
+        torch.cuda.synchronize()
+        sec = max_over_ranks(ev[0].elapsed_time(ev[1]) / 1e3)
+
+        def mean_rad(a):
+            a = a.double()
+            return float(a[:, :3].sum() / a[:, 3].sum())
+        out["ploc_replay"] = {"ms_per_pass": sec * 1e3 / args.steps, "msamples_s": w * h * args.steps / sec / 1e6,
+                              "vs_lbvh_replay": out["replay"]["ms_per_pass"] / (sec * 1e3 / args.steps),
+                              "vs_plain": out["plain"]["ms_per_pass"] / (sec * 1e3 / args.steps),
+                              "mean_radiance": mean_rad(acc), "lbvh_mean_radiance": mean_rad(accs["replay"]),
+                              "pixels_equal_to_lbvh": float((acc == accs["replay"]).all(1).float().mean().item())}
     out["workload"] = "heightfield + icospheres (212,992 triangles), 512x512, 1 % emissive, up to 1024 bounces"
     if reference_gpu and os.path.exists(REF_GPU_LIB):
         # 512 is a multiple of the reference's 16 x 16 blocks: its grid covers the image exactly
@@ -517,6 +546,33 @@ def bench_ploc(args, wl, d_tris, n, cam, w, h, dev, stream, barrier, max_over_ra
         out["forms"][name] = {"ms_per_frame": t * 1e3, "mrays_s": lbvh_forms["rays_per_frame"] / t / 1e6,
                               "lbvh_ms_per_frame": lb_ms, "vs_lbvh_same_form": lb_ms / (t * 1e3),
                               "occlusion_agreement_with_lbvh": float((occ == occ_plain).float().mean().item())}
+    # closest hits of camera rays (every other pixel of the frame): the replay
+    # walk over both trees; the same distances (the triangle may differ only
+    # where two meet a ray at the same distance)
+    from minimumlbvh_b200 import scenes
+    rays = torch.from_numpy(scenes.camera_rays(cam.m_origin, cam.m_right, cam.m_up, w, h, 2)).to(dev)
+    nr = rays.shape[0]
+    hits = {}
+    cam_out = {"rays": nr}
+    for name, bld in (("lbvh", lbvh), ("ploc", pb)):
+        hb = torch.empty((nr, 8), dtype=torch.int32, device=dev)
+        for _ in range(args.warmup):
+            mb.intersect(bld, d_tris, rays, traversal=mb.TRAVERSAL_REPLAY, hits=hb)
+        cev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+        torch.cuda.synchronize()
+        cev[0].record(stream)
+        for _ in range(args.steps):
+            mb.intersect(bld, d_tris, rays, traversal=mb.TRAVERSAL_REPLAY, hits=hb)
+        cev[1].record(stream)
+        torch.cuda.synchronize()
+        t = max_over_ranks(cev[0].elapsed_time(cev[1]) / 1e3) / args.steps
+        launches += args.warmup + args.steps
+        cam_out[name + "_mrays_s"] = nr / t / 1e6
+        hits[name] = hb
+    cam_out["vs_lbvh"] = cam_out["ploc_mrays_s"] / cam_out["lbvh_mrays_s"]
+    cam_out["t_equal"] = float((hits["lbvh"][:, 0] == hits["ploc"][:, 0]).float().mean().item())
+    cam_out["triangle_equal"] = float((hits["lbvh"][:, 7] == hits["ploc"][:, 7]).float().mean().item())
+    out["camera_rays_closest"] = cam_out
     out["launches"] = launches
     out["note"] = ("PLOC: parallel locally-ordered clustering over the LBVH's Morton order, in-order node numbering "
                    "(the LBVH's conventions), one cooperative kernel after the shared key and sort passes")
@@ -1034,6 +1090,8 @@ def main():
         line["ploc"] = ploc
         line["gpu_launches"] += ploc["launches"]
     line["gpu_launches"] += 2 * (args.warmup + args.steps) + 8  # pt passes, its build and leaf copy
+    if "ploc_replay" in pt:
+        line["gpu_launches"] += (args.warmup + args.steps) + 9  # PLOC pt passes, its build and leaf copy
     if reference_gpu is not None:
         line["reference_gpu_baseline"] = reference_gpu
         if "ao" in reference_gpu:  # our kernels launched in that leg: plain (3) and wide (3) frames, 2 builds
