@@ -221,6 +221,14 @@ MLBVH_API mlbvh_status mlbvh_build_ploc(const mlbvh_triangle* dTriangles, uint32
                                         int radius, mlbvh_internal_node* dInternals, mlbvh_node_index* dRootNode,
                                         mlbvh_aabb* dSceneAABB, void* dScratch, size_t scratchBytes, void* stream);
 
+/* Test hook: the number of polls after which a bounded device wait of the
+ * builds that this host thread starts afterwards (mlbvh_build, _ex, _ploc)
+ * gives up; 0 restores each build's default (a second or so). A wait that
+ * gives up sets the build's error word and the build ends without hanging
+ * (its output is then unusable); mlbvh_scratch_status reports it. Lets tests
+ * make a wait run out without a device fault. */
+MLBVH_API void mlbvh_set_spin_limit(uint32_t polls);
+
 /* Synchronises `stream`, then reports MLBVH_ERR_TIMEOUT if a bounded wait of
  * the last build that used dScratch gave up (its output is then unusable),
  * else MLBVH_OK. */

@@ -72,6 +72,7 @@ def lib() -> ctypes.CDLL:
             "mlbvh_build_ex": (i32, [_vp, u32, u32, _vp, _vp, _vp, _vp, _vp, _vp, _vp, sz, _vp]),
             "mlbvh_build_ploc_scratch_bytes": (sz, [u32]),
             "mlbvh_build_ploc": (i32, [_vp, u32, u32, i32, _vp, _vp, _vp, _vp, sz, _vp]),
+            "mlbvh_set_spin_limit": (None, [u32]),
             "mlbvh_scratch_status": (i32, [_vp, _vp]),
             "mlbvh_trace": (i32, [_vp, _vp, _vp, _vp, _vp, u32, i32, i32, _vp]),
             "mlbvh_render_scratch_bytes": (sz, [i32, i32]),

@@ -23,6 +23,7 @@ void clear_error() { g_lastError.clear(); }
 
 namespace {
 thread_local ProfileEvents g_profile;
+thread_local uint32_t g_spinLimit = 0;  // 0: each build's default
 }
 void set_profile_events(cudaEvent_t start, cudaEvent_t stop)
 {
@@ -59,13 +60,15 @@ size_t mlbvh_build_scratch_bytes(uint32_t nTriangles) { return build_scratch_byt
 
 size_t mlbvh_build_ploc_scratch_bytes(uint32_t nTriangles) { return build_ploc_scratch_bytes(nTriangles); }
 
+void mlbvh_set_spin_limit(uint32_t polls) { g_spinLimit = polls; }
+
 mlbvh_status mlbvh_build_ploc(const mlbvh_triangle* dTriangles, uint32_t nTriangles, uint32_t buildOption, int radius,
                               mlbvh_internal_node* dInternals, mlbvh_node_index* dRootNode, mlbvh_aabb* dSceneAABB,
                               void* dScratch, size_t scratchBytes, void* stream)
 {
     clear_error();
     return build_ploc(dTriangles, nTriangles, buildOption, radius, dInternals, dRootNode, dSceneAABB, dScratch,
-                      scratchBytes, as_stream(stream), 0);
+                      scratchBytes, as_stream(stream), g_spinLimit);
 }
 
 mlbvh_status mlbvh_build(const mlbvh_triangle* dTriangles, uint32_t nTriangles, uint32_t buildOption,
@@ -74,7 +77,7 @@ mlbvh_status mlbvh_build(const mlbvh_triangle* dTriangles, uint32_t nTriangles, 
 {
     clear_error();
     return build(dTriangles, nTriangles, buildOption, dInternals, dRootNode, dSceneAABB, nullptr, nullptr, nullptr,
-                 dScratch, scratchBytes, as_stream(stream), 0);
+                 dScratch, scratchBytes, as_stream(stream), g_spinLimit);
 }
 
 mlbvh_status mlbvh_build_ex(const mlbvh_triangle* dTriangles, uint32_t nTriangles, uint32_t buildOption,
@@ -84,7 +87,7 @@ mlbvh_status mlbvh_build_ex(const mlbvh_triangle* dTriangles, uint32_t nTriangle
 {
     clear_error();
     return build(dTriangles, nTriangles, buildOption, dInternals, dRootNode, dSceneAABB, dSortedKeys, dSortedIndices,
-                 dDeltas, dScratch, scratchBytes, as_stream(stream), 0);
+                 dDeltas, dScratch, scratchBytes, as_stream(stream), g_spinLimit);
 }
 
 mlbvh_status mlbvh_scratch_status(const void* dScratch, void* stream)
