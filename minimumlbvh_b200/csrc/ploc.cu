@@ -582,8 +582,10 @@ __global__ void __launch_bounds__(kPlocThreads) k_ploc(PlocArgs a)
         if (!grid_barrier(a.ctl, a.error, a.spinLimit, &sFlag)) return;
         cur ^= 1;
         ++iter;
-        C = ld_acquire(&a.ctl->clusters[iter & 1]);
-        merged = ld_acquire(&a.ctl->merged[iter & 1]);
+        // counts only shrink (every iteration merges); the clamps keep a wrong
+        // count from reaching past the buffers
+        C = min(C, ld_acquire(&a.ctl->clusters[iter & 1]));
+        merged = min(a.n - 1, ld_acquire(&a.ctl->merged[iter & 1]));
     }
 
     // ------------------------------------------------------------------ tail
