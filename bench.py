@@ -451,6 +451,78 @@ def bench_pt(args, dev, stream, max_over_ranks, reference_gpu=False):
     return out
 
 
+def bench_diff(args, dev, stream, max_over_ranks):
+    """Differentiable path tracing and its path-replay adjoint on the
+    heightfield + icospheres scene with a 0.5 x 0.5 quad light of radiance 10
+    (212,994 triangles), per-triangle grey albedo uniform in [0.1, 0.9], 512 x
+    512 at 64 samples per pixel, 3 bounces: the forward render, the L2 loss
+    against a target rendered with a second albedo seed, and the adjoint
+    giving dLoss/dAlbedo for every triangle (paths recomputed from their
+    seeds). Timed with CUDA events. A directional finite difference of the
+    loss (GPU renders at albedo +- eps along a random direction over the
+    triangles with the largest gradients) against the gradient's projection
+    checks the adjoint without the host oracle."""
+    import torch
+    import minimumlbvh_b200 as mb
+    from minimumlbvh_b200 import scenes
+    tris, alb, em = scenes.diff_scene()
+    n = len(tris)
+    t = torch.from_numpy(tris).to(dev)
+    b = mb.BVHGPUBuilder().build(t, n, 0, mb.OnesweepSort(dev.index))
+    b.status()
+    w = h = 512
+    spp, bounces = 64, 3
+    eye, c, up, fovy = scenes.camera_heightfield()
+    cam = mb.RayGenerator().lookat(eye, c, up, fovy, w, h)
+    a = torch.from_numpy(alb).to(dev)
+    e = torch.from_numpy(em).to(dev)
+    target = torch.empty(w * h, dtype=torch.float32, device=dev)
+    mb.pt_diff_render(target, (w, h), cam, b, t, torch.from_numpy(scenes.albedo(n, 2)).to(dev), e, spp, bounces)
+    img = torch.empty_like(target)
+    grad = torch.zeros(n, dtype=torch.float32, device=dev)
+
+    def timed(fn):
+        for _ in range(args.warmup):
+            fn()
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+        torch.cuda.synchronize()
+        ev[0].record(stream)
+        for _ in range(args.steps):
+            fn()
+        ev[1].record(stream)
+        torch.cuda.synchronize()
+        return max_over_ranks(ev[0].elapsed_time(ev[1]) / 1e3) / args.steps
+
+    t_fwd = timed(lambda: mb.pt_diff_render(img, (w, h), cam, b, t, a, e, spp, bounces))
+    gimg = 2.0 * (img - target)
+
+    def adjoint():
+        grad.zero_()
+        mb.pt_diff_adjoint(grad, gimg, (w, h), cam, b, t, a, e, spp, bounces)
+    t_adj = timed(adjoint)
+
+    def loss(albedo):
+        mb.pt_diff_render(img, (w, h), cam, b, t, albedo, e, spp, bounces)
+        return float(((img.double() - target.double()) ** 2).sum().item())
+    g = grad.double()
+    top = torch.topk(g.abs(), 1000).indices
+    rng = torch.Generator(device="cpu").manual_seed(11)
+    v = torch.zeros(n, dtype=torch.float64, device=dev)
+    v[top] = (torch.rand(1000, generator=rng, dtype=torch.float64) * 2 - 1).to(dev)
+    eps = 1e-2
+    fd = (loss((a.double() + eps * v).float()) - loss((a.double() - eps * v).float())) / (2 * eps)
+    proj = float((g * v).sum().item())
+    paths = w * h * spp
+    return {"workload": "heightfield + icospheres + quad light (212,994 triangles), 512x512, 64 spp, 3 bounces",
+            "forward_ms": t_fwd * 1e3, "forward_mpaths_s": paths / t_fwd / 1e6,
+            "adjoint_ms": t_adj * 1e3, "adjoint_mpaths_s": paths / t_adj / 1e6,
+            "adjoint_vs_forward": t_adj / t_fwd,
+            "directional_check": {"finite_difference": fd, "gradient_projection": proj,
+                                  "rel_err": abs(fd - proj) / max(abs(proj), 1e-30), "eps": eps,
+                                  "direction": "random in [-1, 1] on the 1,000 triangles with the largest gradients"},
+            "launches": 2 * (args.warmup + args.steps) + 10}  # + target and two FD renders, 7 build launches
+
+
 def sah_cost_device(nodes, root_t):
     """Surface-area cost of a tree on the device: half areas of every internal
     node's box and of every leaf's box over the root box's (unit costs)."""
@@ -743,6 +815,7 @@ def main():
     ap.add_argument("--batched-meshes", type=int, default=1024, help="meshes of the batched workload (small cases)")
     ap.add_argument("--no-autotune", action="store_true", help="batched workload with default launch parameters")
     ap.add_argument("--no-ploc", action="store_true", help="skip the higher-quality (PLOC) build section")
+    ap.add_argument("--no-diff", action="store_true", help="skip the differentiable path-tracing section")
     ap.add_argument("--no-reference-gpu", action="store_true",
                     help="skip the baseline leg running the reference's own GPU kernels")
     args = ap.parse_args()
@@ -982,6 +1055,7 @@ def main():
         precision = bench_precision(args, builder, qtree, d_tris, tris, cam, w, h, dev, stream, max_over_ranks)
         pt = bench_pt(args, dev, stream, max_over_ranks,
                       reference_gpu=not args.no_reference_gpu and rank == 0 and world == 1)
+        diff = None if args.no_diff else bench_diff(args, dev, stream, max_over_ranks)
         reference_gpu = None
         if not args.no_reference_gpu and rank == 0 and world == 1:
             reference_gpu = bench_reference_gpu(args, builder, sorter, d_tris, n, cam, w, h, dev, stream,
@@ -1089,6 +1163,9 @@ def main():
     if ploc is not None:
         line["ploc"] = ploc
         line["gpu_launches"] += ploc["launches"]
+    if diff is not None:
+        line["differentiation"] = diff
+        line["gpu_launches"] += diff["launches"]
     line["gpu_launches"] += 2 * (args.warmup + args.steps) + 8  # pt passes, its build and leaf copy
     if "ploc_replay" in pt:
         line["gpu_launches"] += (args.warmup + args.steps) + 9  # PLOC pt passes, its build and leaf copy

@@ -24,6 +24,24 @@ namespace {
 
 constexpr int kDiffThreads = 128;
 constexpr int kMaxBounces = 8;
+constexpr int kDiffStack = 16;  // replay-walk stack entries per thread (shared memory)
+
+// intersect_stackfree's closest hit (minimum_lbvh.h:981-1061) through the
+// replay walk (stackfree_replay_step): the same Hit record, ties included,
+// with every internal node loaded once. `stack` is this thread's column of a
+// kDiffStack x kDiffThreads shared-memory array.
+__device__ __forceinline__ void trace_closest(HitRecord& hit, const mlbvh_internal_node* __restrict__ nodes,
+                                              const float* __restrict__ tris, uint32_t root, f3 ro, f3 rd,
+                                              uint2* stack)
+{
+    const f3 inv = inv_rd(rd);
+    uint32_t curr = root, prev = kInvalid, nv = 0, nt = 0;
+    int depth = 0;
+    for (uint32_t steps = 1; steps < kMaxTraversalSteps; ++steps)
+        if (stackfree_replay_step<false, false, kDiffStack>(curr, prev, depth, stack, kDiffThreads, hit, nodes, tris,
+                                                             ro, rd, inv, 0.0f, nv, nt))
+            break;
+}
 
 struct PathVertex {
     uint32_t tri;
@@ -35,7 +53,7 @@ struct PathVertex {
 __device__ __forceinline__ int trace_path(PathVertex* v, int bounces, uint32_t s, int xi, int yi, int w, int h,
                                           const Camera& cam, uint32_t root, const mlbvh_internal_node* __restrict__ nodes,
                                           const float* __restrict__ tris, const float* __restrict__ albedo,
-                                          const float* __restrict__ emission)
+                                          const float* __restrict__ emission, uint2* stack)
 {
     const float2 jitter = sobol2d(s, (uint32_t)xi, (uint32_t)yi, 0u);
     f3 ro, rd;
@@ -43,7 +61,7 @@ __device__ __forceinline__ int trace_path(PathVertex* v, int bounces, uint32_t s
     HitRecord hit;
     hit.t = kFltMax;
     hit.tri = 0xFFFFFFFFu;
-    trace_stackfree<false, false, true>(hit, nodes, tris, root, ro, rd, inv_rd(rd), 0.0f);
+    trace_closest(hit, nodes, tris, root, ro, rd, stack);
     if (hit.t == kFltMax) return 0;
     float throughput = 1.0f;
     int count = 0;
@@ -65,7 +83,7 @@ __device__ __forceinline__ int trace_path(PathVertex* v, int bounces, uint32_t s
         throughput = throughput * __ldg(albedo + t);
         hit.t = kFltMax;
         hit.tri = 0xFFFFFFFFu;
-        trace_stackfree<false, false, true>(hit, nodes, tris, root, ro, rd, inv_rd(rd), 0.0f);
+        trace_closest(hit, nodes, tris, root, ro, rd, stack);
         if (hit.t == kFltMax) break;
     }
     return count;
@@ -86,6 +104,7 @@ __global__ void __launch_bounds__(kDiffThreads)
                      const float* __restrict__ tris, const float* __restrict__ albedo,
                      const float* __restrict__ emission)
 {
+    __shared__ uint2 s_stack[kDiffStack][kDiffThreads];
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= w * h) return;
     const int xi = p % w, yi = p / w;
@@ -94,7 +113,8 @@ __global__ void __launch_bounds__(kDiffThreads)
     PathVertex v[kMaxBounces + 1];
     float sum = 0.0f;
     for (int s = 0; s < spp; ++s) {
-        const int n = trace_path(v, bounces, (uint32_t)s, xi, yi, w, h, cam, root, nodes, tris, albedo, emission);
+        const int n = trace_path(v, bounces, (uint32_t)s, xi, yi, w, h, cam, root, nodes, tris, albedo, emission,
+                                 &s_stack[0][threadIdx.x]);
         float L = 0.0f;
         for (int d = 0; d < n; ++d) L += v[d].collected;
         sum += L;
@@ -108,6 +128,7 @@ __global__ void __launch_bounds__(kDiffThreads)
                       const mlbvh_internal_node* __restrict__ nodes, const float* __restrict__ tris,
                       const float* __restrict__ albedo, const float* __restrict__ emission)
 {
+    __shared__ uint2 s_stack[kDiffStack][kDiffThreads];
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= w * h) return;
     const float g = __ldg(gradImage + p) / (float)spp;
@@ -117,7 +138,8 @@ __global__ void __launch_bounds__(kDiffThreads)
     const uint32_t root = __ldg(rootPtr);
     PathVertex v[kMaxBounces + 1];
     for (int s = 0; s < spp; ++s) {
-        const int n = trace_path(v, bounces, (uint32_t)s, xi, yi, w, h, cam, root, nodes, tris, albedo, emission);
+        const int n = trace_path(v, bounces, (uint32_t)s, xi, yi, w, h, cam, root, nodes, tris, albedo, emission,
+                                 &s_stack[0][threadIdx.x]);
         // suffix sums of the collected radiance: the part of L that depends on
         // the albedo of vertex j is everything collected after it
         float after = 0.0f;
