@@ -213,9 +213,9 @@ MLBVH_API mlbvh_status mlbvh_build_noalloc(const mlbvh_triangle* dTriangles, uin
  * j + 1), parent links, the root's parent invalid, context the escape index
  * of intersect_escape_link, so every walk and every other entry point takes
  * it. Its boxes cost less to traverse (a smaller surface-area sum) at a
- * longer build. One cooperative launch after the sort; needs
- * mlbvh_build_ploc_scratch_bytes(n) bytes of scratch; timeouts are reported
- * by mlbvh_scratch_status like mlbvh_build's. */
+ * longer build. One cooperative launch after the sort (it can be captured in
+ * a CUDA graph); needs mlbvh_build_ploc_scratch_bytes(n) bytes of scratch;
+ * timeouts are reported by mlbvh_scratch_status like mlbvh_build's. */
 MLBVH_API size_t mlbvh_build_ploc_scratch_bytes(uint32_t nTriangles);
 MLBVH_API mlbvh_status mlbvh_build_ploc(const mlbvh_triangle* dTriangles, uint32_t nTriangles, uint32_t buildOption,
                                         int radius, mlbvh_internal_node* dInternals, mlbvh_node_index* dRootNode,

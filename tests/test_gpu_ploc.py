@@ -186,3 +186,29 @@ def test_quantised_tree_over_ploc_tree(ploc_case):
     got = G.host(mb.intersect_quantised(q, G.dev(rays)), np.uint32)
     ref = O.trace_quantised(O.quantise(out, tris), rays)
     np.testing.assert_array_equal(got[:, HIT_COLS], ref[:, HIT_COLS])
+
+
+def test_ploc_build_captures_in_a_graph(cuda):
+    """The whole PLOC build (key and sort passes, k_ploc_init, the cooperative
+    k_ploc) captured in a CUDA graph on a side stream: the replay writes the
+    oracle's tree."""
+    import torch
+    tris = scenes.gaussian_soup(200000, clusters=8, seed=3)
+    n = len(tris)
+    t = G.dev(tris)
+    b = mb.BVHGPUBuilder()
+    s = mb.OnesweepSort(0)
+    st = torch.cuda.Stream()
+    with torch.cuda.stream(st):
+        b.buildByPLOC(t, n, 0, s, 8, stream=st)  # allocations outside the capture
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g, stream=st):
+        b.buildByPLOC(t, n, 0, s, 8, stream=st)
+    b.m_internals.zero_()
+    torch.cuda.synchronize()
+    g.replay()
+    torch.cuda.synchronize()
+    b.status()
+    got = dict(nodes=G.host(b.m_internals, np.uint32)[: n - 1], root=int(G.host(b.m_rootNode, np.uint32)[0]))
+    assert_same_tree(got, O.build_ploc(tris, 0, 8), n)
