@@ -18,8 +18,13 @@
 // neighbour among the r clusters on either side minimises the half area of
 // the union box (dx*dy + dy*dz + dz*dx, union taken lower position first, NaN
 // above everything), ties to the smaller position: a strict order on pairs,
-// so the closest pair overall is mutual and every iteration merges. Mutual
-// nearest neighbours merge into the lower position; survivors keep order.
+// so the closest pair overall is mutual and every iteration merges. Once an
+// iteration has removed fewer than 1/64 of the clusters, later iterations
+// break exact ties first by the smaller pair_hash of the two positions (still
+// a strict order), so runs of equal union areas (duplicated or collinear
+// triangles) pair up about a quarter at a time instead of one pair per run.
+// Mutual nearest neighbours merge into the lower position; survivors keep
+// order.
 //
 // Launch chain on one stream (no host synchronisation):
 //   k_scene_bounds, k_keys, k_onesweep x4   build.cu's chain (sorted leaves)
@@ -166,6 +171,39 @@ __device__ __forceinline__ uint32_t area_key(f3 alo, f3 ahi, f3 blo, f3 bhi)
     return __float_as_uint(fminf(fabsf(a), __int_as_float(0x7f800000)));
 }
 
+// A symmetric mix of a pair's two positions (integer hashing in the style of
+// MurmurHash3's finaliser), the tie-break once ties stall the clustering.
+__device__ __forceinline__ uint32_t pair_hash(uint32_t a, uint32_t b)
+{
+    const uint32_t lo = min(a, b), hi = max(a, b);
+    uint32_t h = lo * 0x9E3779B1u ^ hi * 0x85EBCA77u;
+    h ^= h >> 15;
+    h *= 0x2C1B3C6Du;
+    h ^= h >> 12;
+    return h;
+}
+
+// Once ties stall the clustering: among the candidates of position p (window
+// [jFirst, jEnd), staged from `base`) whose key equals the minimum bestA, the
+// one with the smallest pair_hash, the smaller position on equal hashes. A
+// second, plain scan, so that the unrolled search above keeps its registers.
+__device__ __noinline__ uint32_t resolve_tie(uint32_t p, uint32_t bestA, uint32_t bestJ, int jFirst, int jEnd,
+                                             uint32_t base, const float4* sLo, const float4* sHi)
+{
+    const f3 plo = xyz(sLo[pad(p - base)]), phi = xyz(sHi[pad(p - base)]);
+    uint32_t bestH = pair_hash(p, bestJ);
+    for (int j = jFirst; j < jEnd; ++j) {
+        if ((uint32_t)j == p || (uint32_t)j == bestJ) continue;
+        if (area_key(plo, phi, xyz(sLo[pad(j - base)]), xyz(sHi[pad(j - base)])) != bestA) continue;
+        const uint32_t h = pair_hash(p, (uint32_t)j);
+        if (h < bestH || (h == bestH && (uint32_t)j < bestJ)) {
+            bestH = h;
+            bestJ = (uint32_t)j;
+        }
+    }
+    return bestJ;
+}
+
 // Nearest neighbours of the kPer consecutive positions p0 .. p0 + kPer - 1
 // (those in [first, end) are written to sNN); clusters [base, staged) are in
 // sLo/sHi, and staged covers r past end or reaches the last cluster. Each
@@ -256,6 +294,26 @@ __device__ __forceinline__ void nearest(uint32_t p0, uint32_t first, uint32_t en
         nearest_fixed<R>(p0, first, end, base, sLo, sHi, sNN);
     else
         nearest_group(p0, first, end, base, staged, r, sLo, sHi, sNN);
+}
+
+// The tie pass of the kPer positions p0 .. (those in [first, end)) once ties
+// stall the clustering: each keeps, among its window's candidates with the
+// key of the neighbour found, the one with the smallest pair_hash (the window
+// as nearest_group clamps it). Run after the search, so the unrolled search
+// keeps its registers; it reads boxes and writes only its own entries.
+__device__ __forceinline__ void resolve_ties(uint32_t p0, uint32_t first, uint32_t end, uint32_t base,
+                                             uint32_t staged, int r, const float4* sLo, const float4* sHi,
+                                             uint32_t* sNN)
+{
+    for (int q = 0; q < kPer; ++q) {
+        const uint32_t p = p0 + q;
+        if (p < first || p >= end) continue;
+        const uint32_t j = sNN[pad(p - base)];
+        const uint32_t key = area_key(xyz(sLo[pad(p - base)]), xyz(sHi[pad(p - base)]), xyz(sLo[pad(j - base)]),
+                                      xyz(sHi[pad(j - base)]));
+        sNN[pad(p - base)] = resolve_tie(p, key, j, (int)p > r ? (int)p - r : 0,
+                                         (int)p + r + 1 < (int)staged ? (int)p + r + 1 : (int)staged, base, sLo, sHi);
+    }
 }
 
 // Keep / merge decisions of the kPer positions p0 .. (those below end).
@@ -503,7 +561,7 @@ __global__ void __launch_bounds__(kInitThreads)
 // R: the radius when it is one of the compiled-in values (its groups take the
 // unrolled search), 0 for any radius (the generic search everywhere).
 template <int R>
-__global__ void __launch_bounds__(kPlocThreads) k_ploc(PlocArgs a)
+__global__ void __launch_bounds__(kPlocThreads, 3) k_ploc(PlocArgs a)
 {
     extern __shared__ float4 smem[];
     float4* sLo = smem;
@@ -518,6 +576,7 @@ __global__ void __launch_bounds__(kPlocThreads) k_ploc(PlocArgs a)
 
     uint32_t C = a.n, merged = 0, iter = 0;
     int cur = 0;
+    bool hashTies = false;  // the same in every CTA: it follows the cluster counts
     // ------------------------------------------------------------ grid phase
     while (C > kTailClusters) {
         const uint32_t tiles = (C + tileClusters - 1) / tileClusters;
@@ -541,6 +600,11 @@ __global__ void __launch_bounds__(kPlocThreads) k_ploc(PlocArgs a)
                 if (g0 < nnEnd) nearest<R>(g0, nnFirst, nnEnd, base, stagedEnd, r, sLo, sHi, sNN);
             }
             __syncthreads();
+            if (hashTies) {  // uniform over the grid
+                const uint32_t g0 = nnFirst + kPer * tid;
+                if (g0 < nnEnd) resolve_ties(g0, nnFirst, nnEnd, base, stagedEnd, r, sLo, sHi, sNN);
+                __syncthreads();
+            }
             const uint32_t p0 = s + kPer * tid;
             const Decision dc = decide(p0, e, base, sNN);
             uint32_t total;
@@ -584,7 +648,9 @@ __global__ void __launch_bounds__(kPlocThreads) k_ploc(PlocArgs a)
         ++iter;
         // counts only shrink (every iteration merges); the clamps keep a wrong
         // count from reaching past the buffers
-        C = min(C, ld_acquire(&a.ctl->clusters[iter & 1]));
+        const uint32_t next = min(C, ld_acquire(&a.ctl->clusters[iter & 1]));
+        if ((unsigned long long)(C - next) * 64ull < C) hashTies = true;
+        C = next;
         merged = min(a.n - 1, ld_acquire(&a.ctl->merged[iter & 1]));
     }
 
@@ -602,6 +668,11 @@ __global__ void __launch_bounds__(kPlocThreads) k_ploc(PlocArgs a)
                 if (g0 < C) nearest<R>(g0, 0, C, 0, C, r, sLo, sHi, sNN);
             }
             __syncthreads();
+            if (hashTies) {
+                const uint32_t g0 = kPer * tid;
+                if (g0 < C) resolve_ties(g0, 0, C, 0, C, r, sLo, sHi, sNN);
+                __syncthreads();
+            }
             const uint32_t p0 = kPer * tid;
             const Decision dc = decide(p0, C, 0, sNN);
             uint32_t total;
@@ -632,7 +703,9 @@ __global__ void __launch_bounds__(kPlocThreads) k_ploc(PlocArgs a)
                 ++outPos;
             }
             merged += total >> 16;
-            C = total & 0xFFFFu;
+            const uint32_t next = total & 0xFFFFu;
+            if ((unsigned long long)(C - next) * 64ull < C) hashTies = true;
+            C = next;
             __syncthreads();
         }
         // the root (the last node made) has the first leaf and no parent

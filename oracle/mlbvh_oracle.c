@@ -376,7 +376,13 @@ int orc_build(const orc_triangle* tris, uint32_t n, uint32_t option,
  *     the order key is the bit pattern of min(|area|, +inf), so a zero area
  *     of either sign is 0 and a NaN area counts as +inf); ties go to the
  *     smaller position. That is a strict order on pairs, so the closest pair
- *     overall is always mutual and every iteration merges at least once;
+ *     overall is always mutual and every iteration merges at least once. Once
+ *     an iteration has removed fewer than 1/64 of the clusters, every later
+ *     iteration breaks exact ties first by the smaller ploc_pair_hash of the
+ *     pair's two positions (still a strict order): where all union areas are
+ *     equal (duplicated or collinear triangles) ties to the smaller position
+ *     merge only the first pair of a run per iteration, the hash about a
+ *     quarter of the clusters;
  *   - mutual nearest neighbours merge into the lower position, all other
  *     clusters stay, and the survivors keep their order.
  * Nodes are then numbered in in-order (node j between the j-th and the
@@ -395,6 +401,18 @@ static uint32_t ploc_area_key(const orc_aabb* a0, const orc_aabb* a1)
     uint32_t k;
     memcpy(&k, &a, 4);
     return k;
+}
+
+/* A symmetric mix of the two positions of a pair (integer hashing in the
+ * style of MurmurHash3's finaliser). */
+static uint32_t ploc_pair_hash(uint32_t a, uint32_t b)
+{
+    uint32_t lo = a < b ? a : b, hi = a < b ? b : a;
+    uint32_t h = lo * 0x9E3779B1u ^ hi * 0x85EBCA77u;
+    h ^= h >> 15;
+    h *= 0x2C1B3C6Du;
+    h ^= h >> 12;
+    return h;
 }
 
 typedef struct {
@@ -435,22 +453,26 @@ int orc_build_ploc(const orc_triangle* tris, uint32_t n, uint32_t option, int ra
     }
     free(idx);
     uint32_t C = n, created = 0;
-    int cur = 0, iterations = 0;
+    int cur = 0, iterations = 0, hashTies = 0;
     const uint32_t r = (uint32_t)radius;
     while (C > 1)
     {
         const orc_aabb* b = box[cur];
         for (uint32_t p = 0; p < C; ++p)
         {
-            uint64_t best = ~0ull;
+            uint32_t bestA = 0xFFFFFFFFu, bestJ = 0;
             uint32_t lo = p > r ? p - r : 0, hi = p + r < C - 1 ? p + r : C - 1;
             for (uint32_t j = lo; j <= hi; ++j)
             {
                 if (j == p) continue;
-                uint64_t key = (uint64_t)ploc_area_key(&b[p], &b[j]) << 32 | j;
-                if (key < best) best = key;
+                uint32_t a = ploc_area_key(&b[p], &b[j]);
+                if (a < bestA || (a == bestA && hashTies && ploc_pair_hash(p, j) < ploc_pair_hash(p, bestJ)))
+                {
+                    bestA = a;
+                    bestJ = j;
+                }
             }
-            nn[p] = (uint32_t)best;
+            nn[p] = bestJ;
         }
         uint32_t w = 0;
         for (uint32_t p = 0; p < C; ++p)
@@ -480,6 +502,7 @@ int orc_build_ploc(const orc_triangle* tris, uint32_t n, uint32_t option, int ra
             }
             ++w;
         }
+        if ((uint64_t)(C - w) * 64 < C) hashTies = 1;
         C = w;
         cur ^= 1;
         ++iterations;

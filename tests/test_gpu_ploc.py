@@ -212,3 +212,41 @@ def test_ploc_build_captures_in_a_graph(cuda):
     b.status()
     got = dict(nodes=G.host(b.m_internals, np.uint32)[: n - 1], root=int(G.host(b.m_rootNode, np.uint32)[0]))
     assert_same_tree(got, O.build_ploc(tris, 0, 8), n)
+
+
+@pytest.mark.parametrize("radius,n", [(8, 1008), (8, 1009), (8, 2016), (8, 2017), (32, 960), (32, 961), (32, 1921),
+                                      (1, 1022), (1, 1023), (16, 992), (16, 993), (4, 1016), (4, 1025)])
+def test_ploc_tile_boundaries(cuda, radius, n):
+    """Cluster counts at the edges of a tile (kTile - 2r clusters) and of the
+    single-CTA tail (1,024 clusters)."""
+    tris = scenes.gaussian_soup(n, clusters=3, seed=n + radius)
+    _, _, got = gpu_ploc(tris, 0, radius)
+    assert_same_tree(got, O.build_ploc(tris, 0, radius), n)
+
+
+@pytest.mark.parametrize("kind", ["identical", "points", "collinear"])
+def test_ploc_degenerate_inputs(cuda, kind):
+    """Every area key equal (one triangle repeated), zero-area triangles at a
+    few points, and triangles along a line: ties resolve to the smaller
+    position on both sides, and the tree is the oracle's."""
+    rng = np.random.default_rng(17)
+    n = 5000
+    if kind == "identical":
+        tris = np.tile(scenes.gaussian_soup(1, seed=4), (n, 1))
+    elif kind == "points":
+        pts = rng.random((7, 3)).astype(np.float32)
+        tris = np.repeat(pts[rng.integers(0, 7, n)], 3, axis=0).reshape(n, 9)
+    else:
+        x = np.sort(rng.random(n)).astype(np.float32)
+        tris = np.zeros((n, 9), np.float32)
+        tris[:, 0] = x
+        tris[:, 3] = x + 0.001
+        tris[:, 6] = x + 0.002
+    tris = np.ascontiguousarray(tris, np.float32)
+    t = G.dev(tris)
+    b = mb.BVHGPUBuilder().buildByPLOC(t, n, 0, None, 8)
+    b.status()
+    got = dict(nodes=G.host(b.m_internals, np.uint32)[: n - 1], root=int(G.host(b.m_rootNode, np.uint32)[0]))
+    ref = O.build_ploc(tris, 0, 8)
+    assert_same_tree(got, ref, n)
+    assert O.check_tree(ref["nodes"], tris, ref["root"])
