@@ -22,9 +22,12 @@
 // iteration has removed fewer than 1/64 of the clusters, later iterations
 // break exact ties first by the smaller pair_hash of the two positions (still
 // a strict order), so runs of equal union areas (duplicated or collinear
-// triangles) pair up about a quarter at a time instead of one pair per run.
-// Mutual nearest neighbours merge into the lower position; survivors keep
-// order.
+// triangles) pair up about a quarter at a time instead of one pair per run;
+// and if such an iteration still removes fewer than 1/64 (a chain of growing
+// gaps, each cluster nearest to the one before it), the next iteration pairs
+// positions 2k and 2k + 1 outright, so every build ends in O(log n)
+// iterations. Mutual nearest neighbours merge into the lower position;
+// survivors keep order.
 //
 // Launch chain on one stream (no host synchronisation):
 //   k_scene_bounds, k_keys, k_onesweep x4   build.cu's chain (sorted leaves)
@@ -294,6 +297,20 @@ __device__ __forceinline__ void nearest(uint32_t p0, uint32_t first, uint32_t en
         nearest_fixed<R>(p0, first, end, base, sLo, sHi, sNN);
     else
         nearest_group(p0, first, end, base, staged, r, sLo, sHi, sNN);
+}
+
+// A pairing iteration: position 2k's neighbour is 2k + 1 and the other way
+// round; an odd last cluster points back and stays (tiles start at even
+// positions, so no pair straddles two tiles).
+__device__ __forceinline__ void pair_partners(uint32_t p0, uint32_t first, uint32_t end, uint32_t base, uint32_t C,
+                                              uint32_t* sNN)
+{
+#pragma unroll
+    for (int q = 0; q < kPer; ++q) {
+        const uint32_t p = p0 + q;
+        if (p < first || p >= end) continue;
+        sNN[pad(p - base)] = (p ^ 1u) < C ? p ^ 1u : (p > 0 ? p - 1 : p);
+    }
 }
 
 // The tie pass of the kPer positions p0 .. (those in [first, end)) once ties
@@ -576,9 +593,10 @@ __global__ void __launch_bounds__(kPlocThreads, 3) k_ploc(PlocArgs a)
 
     uint32_t C = a.n, merged = 0, iter = 0;
     int cur = 0;
-    bool hashTies = false;  // the same in every CTA: it follows the cluster counts
+    bool hashTies = false, pairNext = false;  // the same in every CTA: they follow the cluster counts
     // ------------------------------------------------------------ grid phase
     while (C > kTailClusters) {
+        const bool pairs = pairNext;
         const uint32_t tiles = (C + tileClusters - 1) / tileClusters;
         unsigned long long* flags = a.flags + (size_t)(iter & 1) * a.maxTiles;
         unsigned long long* nextFlags = a.flags + (size_t)((iter + 1) & 1) * a.maxTiles;
@@ -597,10 +615,15 @@ __global__ void __launch_bounds__(kPlocThreads, 3) k_ploc(PlocArgs a)
             const uint32_t nnFirst = s > (uint32_t)r ? s - r : 0u, nnEnd = min(C, e + r);
             {
                 const uint32_t g0 = nnFirst + kPer * tid;  // nnEnd - nnFirst <= kTile: one group per thread
-                if (g0 < nnEnd) nearest<R>(g0, nnFirst, nnEnd, base, stagedEnd, r, sLo, sHi, sNN);
+                if (g0 < nnEnd) {
+                    if (pairs)
+                        pair_partners(g0, nnFirst, nnEnd, base, C, sNN);
+                    else
+                        nearest<R>(g0, nnFirst, nnEnd, base, stagedEnd, r, sLo, sHi, sNN);
+                }
             }
             __syncthreads();
-            if (hashTies) {  // uniform over the grid
+            if (hashTies && !pairs) {  // uniform over the grid
                 const uint32_t g0 = nnFirst + kPer * tid;
                 if (g0 < nnEnd) resolve_ties(g0, nnFirst, nnEnd, base, stagedEnd, r, sLo, sHi, sNN);
                 __syncthreads();
@@ -649,7 +672,12 @@ __global__ void __launch_bounds__(kPlocThreads, 3) k_ploc(PlocArgs a)
         // counts only shrink (every iteration merges); the clamps keep a wrong
         // count from reaching past the buffers
         const uint32_t next = min(C, ld_acquire(&a.ctl->clusters[iter & 1]));
-        if ((unsigned long long)(C - next) * 64ull < C) hashTies = true;
+        if ((unsigned long long)(C - next) * 64ull < C) {
+            pairNext = hashTies;
+            hashTies = true;
+        } else {
+            pairNext = false;
+        }
         C = next;
         merged = min(a.n - 1, ld_acquire(&a.ctl->merged[iter & 1]));
     }
@@ -663,12 +691,18 @@ __global__ void __launch_bounds__(kPlocThreads, 3) k_ploc(PlocArgs a)
         }
         __syncthreads();
         while (C > 1) {
+            const bool pairs = pairNext;
             {
                 const uint32_t g0 = kPer * tid;  // C <= kTile: one group per thread
-                if (g0 < C) nearest<R>(g0, 0, C, 0, C, r, sLo, sHi, sNN);
+                if (g0 < C) {
+                    if (pairs)
+                        pair_partners(g0, 0, C, 0, C, sNN);
+                    else
+                        nearest<R>(g0, 0, C, 0, C, r, sLo, sHi, sNN);
+                }
             }
             __syncthreads();
-            if (hashTies) {
+            if (hashTies && !pairs) {
                 const uint32_t g0 = kPer * tid;
                 if (g0 < C) resolve_ties(g0, 0, C, 0, C, r, sLo, sHi, sNN);
                 __syncthreads();
@@ -704,7 +738,12 @@ __global__ void __launch_bounds__(kPlocThreads, 3) k_ploc(PlocArgs a)
             }
             merged += total >> 16;
             const uint32_t next = total & 0xFFFFu;
-            if ((unsigned long long)(C - next) * 64ull < C) hashTies = true;
+            if ((unsigned long long)(C - next) * 64ull < C) {
+                pairNext = hashTies;
+                hashTies = true;
+            } else {
+                pairNext = false;
+            }
             C = next;
             __syncthreads();
         }

@@ -382,7 +382,12 @@ int orc_build(const orc_triangle* tris, uint32_t n, uint32_t option,
  *     pair's two positions (still a strict order): where all union areas are
  *     equal (duplicated or collinear triangles) ties to the smaller position
  *     merge only the first pair of a run per iteration, the hash about a
- *     quarter of the clusters;
+ *     quarter of the clusters. If an iteration that already breaks ties by
+ *     the hash still removes fewer than 1/64 of the clusters (a chain of
+ *     strictly growing gaps, where every cluster's nearest neighbour is the
+ *     one before it), the next iteration pairs positions 2k and 2k + 1
+ *     outright, halving the count; so every build ends in O(log n)
+ *     iterations;
  *   - mutual nearest neighbours merge into the lower position, all other
  *     clusters stay, and the survivors keep their order.
  * Nodes are then numbered in in-order (node j between the j-th and the
@@ -453,12 +458,15 @@ int orc_build_ploc(const orc_triangle* tris, uint32_t n, uint32_t option, int ra
     }
     free(idx);
     uint32_t C = n, created = 0;
-    int cur = 0, iterations = 0, hashTies = 0;
+    int cur = 0, iterations = 0, hashTies = 0, pairNext = 0;
     const uint32_t r = (uint32_t)radius;
     while (C > 1)
     {
         const orc_aabb* b = box[cur];
-        for (uint32_t p = 0; p < C; ++p)
+        const int pairs = pairNext;
+        for (uint32_t p = 0; p < C && pairs; ++p)  /* position 2k with 2k + 1; an odd last one stays */
+            nn[p] = (p ^ 1u) < C ? p ^ 1u : (p > 0 ? p - 1 : p);
+        for (uint32_t p = 0; p < C && !pairs; ++p)
         {
             uint32_t bestA = 0xFFFFFFFFu, bestJ = 0;
             uint32_t lo = p > r ? p - r : 0, hi = p + r < C - 1 ? p + r : C - 1;
@@ -502,7 +510,13 @@ int orc_build_ploc(const orc_triangle* tris, uint32_t n, uint32_t option, int ra
             }
             ++w;
         }
-        if ((uint64_t)(C - w) * 64 < C) hashTies = 1;
+        if ((uint64_t)(C - w) * 64 < C)
+        {
+            if (hashTies) pairNext = 1;
+            hashTies = 1;
+        }
+        else
+            pairNext = 0;
         C = w;
         cur ^= 1;
         ++iterations;

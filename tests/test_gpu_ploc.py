@@ -224,14 +224,32 @@ def test_ploc_tile_boundaries(cuda, radius, n):
     assert_same_tree(got, O.build_ploc(tris, 0, radius), n)
 
 
-@pytest.mark.parametrize("kind", ["identical", "points", "collinear"])
+def chain_triangles(n):
+    """Thin triangles along x with strictly growing gaps: each cluster's
+    nearest neighbour is the one before it, PLOC's worst case without ties."""
+    x = np.cumsum(1.0 + np.arange(n) * 1e-3)
+    x = (x / x[-1]).astype(np.float32)
+    tris = np.zeros((n, 9), np.float32)
+    tris[:, 0] = x
+    tris[:, 3] = x + 1e-6
+    tris[:, 4] = 0.001
+    tris[:, 6] = x
+    tris[:, 7] = 0.001
+    tris[:, 8] = 0.0005
+    return tris
+
+
+@pytest.mark.parametrize("kind", ["identical", "points", "collinear", "chain"])
 def test_ploc_degenerate_inputs(cuda, kind):
     """Every area key equal (one triangle repeated), zero-area triangles at a
-    few points, and triangles along a line: ties resolve to the smaller
-    position on both sides, and the tree is the oracle's."""
+    few points, triangles along a line, and a chain of growing gaps: the
+    stall rules (hashed ties, then a pairing iteration) take the same turns
+    on both sides, and the tree is the oracle's."""
     rng = np.random.default_rng(17)
-    n = 5000
-    if kind == "identical":
+    n = 20000 if kind == "chain" else 5000
+    if kind == "chain":
+        tris = chain_triangles(n)
+    elif kind == "identical":
         tris = np.tile(scenes.gaussian_soup(1, seed=4), (n, 1))
     elif kind == "points":
         pts = rng.random((7, 3)).astype(np.float32)

@@ -167,3 +167,27 @@ def test_bad_arguments():
     root = np.zeros(1, np.uint32)
     assert O.oracle().orc_build_ploc(O.P(tris), 10, 0, 0, O.P(nodes), O.P(root)) < 0
     assert O.oracle().orc_build_ploc(O.P(tris), 0, 0, 8, O.P(nodes), O.P(root)) < 0
+
+
+@pytest.mark.parametrize("kind", ["identical", "collinear", "chain"])
+def test_stalls_end_in_few_iterations(kind):
+    """Inputs where ties (identical boxes, zero union areas) or a chain of
+    growing gaps let only one pair merge per run and iteration: the stall
+    rules keep the iteration count logarithmic (it would be about n without
+    them)."""
+    n = 20000
+    if kind == "identical":
+        tris = np.tile(scenes.gaussian_soup(1, seed=4), (n, 1))
+    elif kind == "collinear":
+        x = np.sort(np.random.default_rng(3).random(n)).astype(np.float32)
+        tris = np.zeros((n, 9), np.float32)
+        tris[:, 0], tris[:, 3], tris[:, 6] = x, x + 0.001, x + 0.002
+    else:
+        x = np.cumsum(1.0 + np.arange(n) * 1e-3)
+        x = (x / x[-1]).astype(np.float32)
+        tris = np.zeros((n, 9), np.float32)
+        tris[:, 0], tris[:, 3], tris[:, 4] = x, x + 1e-6, 0.001
+        tris[:, 6], tris[:, 7], tris[:, 8] = x, 0.001, 0.0005
+    pl = O.build_ploc(np.ascontiguousarray(tris, np.float32), 0, 8)
+    assert O.check_tree(pl["nodes"], tris, pl["root"])
+    assert pl["iterations"] < 150
