@@ -16,8 +16,8 @@
 //
 // Clustering rule (the oracle states the same): a cluster's nearest
 // neighbour among the r clusters on either side minimises the half area of
-// the union box (dx*dy + dy*dz + dz*dx, union taken lower position first, NaN
-// above everything), ties to the smaller position: a strict order on pairs,
+// the union box (area_key: union by fminf / fmaxf, dx*dy + dy*dz + dz*dx, a
+// NaN area counted as +inf), ties to the smaller position: a strict order on pairs,
 // so the closest pair overall is mutual and every iteration merges. Once an
 // iteration has removed fewer than 1/64 of the clusters, later iterations
 // break exact ties first by the smaller pair_hash of the two positions (still
