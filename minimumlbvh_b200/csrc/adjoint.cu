@@ -48,9 +48,12 @@ struct PathVertex {
     float collected;  // throughput * emission at this vertex
 };
 
-// Traces the path of sample s of pixel (xi, yi); returns its vertex count
-// and fills v (at most bounces + 1 vertices).
-__device__ __forceinline__ int trace_path(PathVertex* v, int bounces, uint32_t s, int xi, int yi, int w, int h,
+// Traces the path of sample s of pixel (xi, yi). kStore: fills v (at most
+// bounces + 1 vertices) and returns the vertex count; otherwise adds the
+// collected radiance, vertex by vertex in path order, to *L (the same sum the
+// forward render forms from v) and keeps no vertices.
+template <bool kStore>
+__device__ __forceinline__ int trace_path(PathVertex* v, float* L, int bounces, uint32_t s, int xi, int yi, int w, int h,
                                           const Camera& cam, uint32_t root, const mlbvh_internal_node* __restrict__ nodes,
                                           const float* __restrict__ tris, const float* __restrict__ albedo,
                                           const float* __restrict__ emission, uint2* stack)
@@ -67,8 +70,13 @@ __device__ __forceinline__ int trace_path(PathVertex* v, int bounces, uint32_t s
     int count = 0;
     for (int d = 0; d <= bounces; ++d) {
         const uint32_t t = hit.tri;
-        v[count].tri = t;
-        v[count].collected = throughput * __ldg(emission + t);
+        const float collected = throughput * __ldg(emission + t);
+        if (kStore) {
+            v[count].tri = t;
+            v[count].collected = collected;
+        } else {
+            *L += collected;
+        }
         ++count;
         if (d == bounces) break;
         const f3 p = ro + rd * hit.t;
@@ -110,13 +118,11 @@ __global__ void __launch_bounds__(kDiffThreads)
     const int xi = p % w, yi = p / w;
     const Camera cam = camera_of(gen);
     const uint32_t root = __ldg(rootPtr);
-    PathVertex v[kMaxBounces + 1];
     float sum = 0.0f;
     for (int s = 0; s < spp; ++s) {
-        const int n = trace_path(v, bounces, (uint32_t)s, xi, yi, w, h, cam, root, nodes, tris, albedo, emission,
-                                 &s_stack[0][threadIdx.x]);
         float L = 0.0f;
-        for (int d = 0; d < n; ++d) L += v[d].collected;
+        trace_path<false>(nullptr, &L, bounces, (uint32_t)s, xi, yi, w, h, cam, root, nodes, tris, albedo, emission,
+                          &s_stack[0][threadIdx.x]);
         sum += L;
     }
     image[p] = sum / (float)spp;
@@ -138,8 +144,8 @@ __global__ void __launch_bounds__(kDiffThreads)
     const uint32_t root = __ldg(rootPtr);
     PathVertex v[kMaxBounces + 1];
     for (int s = 0; s < spp; ++s) {
-        const int n = trace_path(v, bounces, (uint32_t)s, xi, yi, w, h, cam, root, nodes, tris, albedo, emission,
-                                 &s_stack[0][threadIdx.x]);
+        const int n = trace_path<true>(v, nullptr, bounces, (uint32_t)s, xi, yi, w, h, cam, root, nodes, tris, albedo,
+                                       emission, &s_stack[0][threadIdx.x]);
         // suffix sums of the collected radiance: the part of L that depends on
         // the albedo of vertex j is everything collected after it
         float after = 0.0f;
