@@ -135,10 +135,13 @@ def committed_traffic(workload):
         return json.load(f).get(workload)
 
 
-def cpu_sample_ao(wl, tris, cam_arr, out, seconds: float):
+def cpu_sample_ao(wl, tris, cam_arr, out, seconds: float, rows=None):
     """Reference CPU AO (oracle/_ref: the reference's intersect_stackfree and
-    sampling code, all host threads) on a band of rows around the middle of
-    the frame, grown until about `seconds` of wall time."""
+    sampling code, all host threads). With `rows` = (first, end) it times
+    exactly those rows of the frame; else a band around the middle of the
+    frame, grown until about `seconds` of wall time. Returns the baseline
+    record, the elapsed seconds and the per-pixel occlusion counts (rows
+    outside the band are 0)."""
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     import _oracle as O
     w, h = wl["w"], wl["h"]
@@ -161,19 +164,31 @@ def cpu_sample_ao(wl, tris, cam_arr, out, seconds: float):
             _, _, cnt = O.render_ao(cam_arr, out["root"], nodes, tris, w, h, wl["ns"], wl["radius"], 12345, 1,
                                     trig=0, rows=(r0, r1), counters=True)
             return int(cnt[2])
-    rows, rays, elapsed = 2, 0, 0.0
-    mid = h // 2
-    while True:
-        r0 = max(0, mid - rows // 2)
-        r1 = min(h, r0 + rows)
+    if rows is not None:
+        r0, r1 = rows
         t0 = time.perf_counter()
         rays = run(r0, r1)
         elapsed = time.perf_counter() - t0
-        if elapsed >= seconds or r1 - r0 >= h:
-            break
-        rows = min(h, max(rows * 2, int(rows * seconds / max(elapsed, 1e-3))))
+    else:
+        band, rays, elapsed = 2, 0, 0.0
+        mid = h // 2
+        while True:
+            r0 = max(0, mid - band // 2)
+            r1 = min(h, r0 + band)
+            t0 = time.perf_counter()
+            rays = run(r0, r1)
+            elapsed = time.perf_counter() - t0
+            if elapsed >= seconds or r1 - r0 >= h:
+                break
+            band = min(h, max(band * 2, int(band * seconds / max(elapsed, 1e-3))))
     return {"value": rays / elapsed / 1e6, "unit": "Mrays/s", "cores": threads, "kind": kind,
-            "sample": f"AO rows {r0}-{r1 - 1} of the {w}x{h} frame ({rays} rays, {elapsed:.1f} s)"}, elapsed
+            "sample": f"AO rows {r0}-{r1 - 1} of the {w}x{h} frame ({rays} rays, {elapsed:.1f} s)"}, elapsed, occ
+
+
+def cpu_rows(wl):
+    """The rows both CPU legs (cpu_baseline and --impl reference) time: the
+    whole frame, so that both run the same rays."""
+    return (0, wl["h"])
 
 
 def cpu_build_baseline(tris):
@@ -193,6 +208,28 @@ def cpu_build_baseline(tris):
     O.build(tris)
     dt = time.perf_counter() - t0
     return {"mtri_s": n / dt / 1e6, "ms": dt * 1e3, "kind": "port", "what": "oracle build (serial)"}
+
+
+def oracle_agreement(wl, tris, cam_arr, out, occ_plain, form_occ, occ_ref, ref_kind):
+    """Per-pixel occlusion counts of the timed frame (plain form and every
+    other form) against the oracle's restatement over the whole frame, with
+    this project's FP32 sincos for the sample directions as the kernels use
+    it (all host threads; outside the timed regions), and the plain form
+    against the reference's own CPU code (its libm sincos: a few AO rays
+    differ by an ulp of direction)."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import _oracle as O
+    w, h = wl["w"], wl["h"]
+    t0 = time.perf_counter()
+    _, occ_oracle = O.render_ao(cam_arr, out["root"], out["nodes"], tris, w, h, wl["ns"], wl["radius"], 12345, 1,
+                                trig=1)
+    res = {"pixels": int(w * h), "oracle_s": time.perf_counter() - t0,
+           "plain": float((occ_plain == occ_oracle).mean())}
+    for name, occ in form_occ.items():
+        res[name] = float((occ == occ_oracle).mean())
+    res["plain_vs_reference_cpu"] = float((occ_plain == occ_ref).mean())
+    res["reference_cpu_kind"] = ref_kind
+    return res
 
 
 def bench_batched(args, dev, stream, barrier, max_over_ranks, world, n_meshes=1024, autotune=True):
@@ -780,7 +817,8 @@ def run_reference(args, wl, rank):
     values = []
     sample = None
     for i in range(args.warmup + args.steps):
-        s, _ = cpu_sample_ao(wl, tris, cam_arr, out, seconds=args.ref_seconds)
+        # the whole frame, the same rays as the cpu_baseline leg of this bench's own arm
+        s, _, _ = cpu_sample_ao(wl, tris, cam_arr, out, seconds=args.ref_seconds, rows=cpu_rows(wl))
         if i >= args.warmup:
             values.append(s["value"])
             sample = s
@@ -942,6 +980,8 @@ def main():
                               stats=stats, quantised=True)
 
         forms = {}
+        form_occ_host = {}
+        occ_plain_host = occ_plain.cpu().numpy().view(np.uint32)
         for name, frame in (("replay", replay_frame), ("quantised", quantised_frame), ("wide", wide_frame),
                             ("wide_quantised", wide_quantised_frame)):
             occ = torch.empty_like(occ_plain)
@@ -967,6 +1007,7 @@ def main():
             forms[name] = (max_over_ranks(sum(a.elapsed_time(b) for a, b in fev) / 1e3),
                            float((occ_plain == occ).float().mean().item()), fst.cpu().numpy(),
                            float(np.mean([a.elapsed_time(b) for a, b in fkev])) / 1e3)
+            form_occ_host[name] = occ.cpu().numpy().view(np.uint32)
 
         # ---- builds
         bev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
@@ -1181,9 +1222,11 @@ def main():
         out = {"nodes": builder.m_internals.cpu().numpy().view(np.uint32)[: n - 1],
                "root": int(builder.m_rootNode.cpu().numpy().view(np.uint32)[0])}
         cam_arr = cam.as_array()
-        cb, _ = cpu_sample_ao(wl, tris, cam_arr, out, args.cpu_seconds)
+        cb, _, occ_ref = cpu_sample_ao(wl, tris, cam_arr, out, args.cpu_seconds, rows=cpu_rows(wl))
         cb["build"] = cpu_build_baseline(tris)
         line["cpu_baseline"] = cb
+        line["occlusion_agreement_vs_oracle"] = oracle_agreement(wl, tris, cam_arr, out, occ_plain_host,
+                                                                 form_occ_host, occ_ref, cb["kind"])
     reps.close()
     if reps.is_root:
         print(json.dumps(line), flush=True)

@@ -17,17 +17,29 @@
 //   m_internals, m_rootNode, m_sceneAABB,             same members (device
 //     m_nTriangles (:876-884)                           pointers), same meaning
 //   tinyhiponesweep::OnesweepSort(device) (:575)      owns the build scratch
+//   BVHCPUBuilder::build(tris, n, opt) (:512)         same call and members
+//     m_internals, m_deltas, m_rootNode (:666-668),     (host std::vectors, a
+//     empty(), validate() (:657-664)                    host NodeIndex); the
+//                                                       build runs on the GPU
 //
-// Differences, by design: build() neither prints its time nor synchronises
-// (the reference's DeviceStopwatch does both, :785-870); errors abort with the
-// library's message, as the reference's host asserts abort (:23); the query
-// functions take rays with t in [0, hit->t] exactly as the reference's.
+// Differences, by design: BVHGPUBuilder::build() neither prints its time nor
+// synchronises (the reference's DeviceStopwatch does both, :785-870), so a
+// bounded device wait that gave up is reported by status(stream), which
+// synchronises; errors abort with the library's message, as the reference's
+// host asserts abort (:23); the query functions take rays with t in
+// [0, hit->t] exactly as the reference's. BVHCPUBuilder keeps the reference's
+// host-side results, but there is no CPU build: it uploads the triangles,
+// builds on the GPU and copies the tree back, synchronously. The reference's
+// intersect_* are host+device functions (:5-24); here they are device-only,
+// since nothing of this library runs the path on the CPU.
 #pragma once
 
 #include <cstddef>
 #include <cstdint>
 #include <cstdio>
 #include <cstdlib>
+#include <utility>
+#include <vector>
 #include <cuda_runtime.h>
 
 #include "mlbvh.h"
@@ -250,6 +262,7 @@ public:
                                   reinterpret_cast<mlbvh_node_index*>(m_rootNode),
                                   reinterpret_cast<mlbvh_aabb*>(m_sceneAABB), scratch, bytes, stream),
                       "mlbvh_build");
+        m_scratch = scratch;
     }
     // The higher-quality build, counterpart of BVHCPUBuilder::buildByEmbree
     // (minimum_lbvh.h:594-656) on the GPU: PLOC with neighbourhood radius
@@ -265,6 +278,19 @@ public:
                                        reinterpret_cast<mlbvh_node_index*>(m_rootNode),
                                        reinterpret_cast<mlbvh_aabb*>(m_sceneAABB), scratch, bytes, stream),
                       "mlbvh_build_ploc");
+        m_scratch = scratch;
+    }
+    // Synchronises `stream` and reports on the last build (build or
+    // buildByPLOC): MLBVH_ERR_TIMEOUT if one of its bounded device waits gave
+    // up (the tree is then unusable; build again), else MLBVH_OK. The
+    // reference's build synchronised on return and had no such waits; this
+    // one returns after the launches, so call status() where the reference's
+    // caller relied on a finished build. The scratch is the sorter's, so
+    // the sorter must not have run another build since.
+    mlbvh_status status(cudaStream_t stream) const
+    {
+        if (!m_scratch) return MLBVH_ERR_INVALID_ARG;
+        return mlbvh_scratch_status(m_scratch, stream);
     }
     bool empty() const { return m_nTriangles == 0; }
 
@@ -274,6 +300,7 @@ public:
     int m_nTriangles = 0;
 
 private:
+    const void* m_scratch = nullptr;  // the scratch of the last build, for status()
     void reserve_nodes(int nTriangles, cudaStream_t stream)
     {
         m_nTriangles = nTriangles;
@@ -286,6 +313,122 @@ private:
         }
     }
     size_t m_capacity = 0;
+};
+
+// BVHCPUBuilder (minimum_lbvh.h:509-669): the reference's host-side build
+// API, with the tree in host memory (m_internals, m_deltas, m_rootNode) for
+// callers that read it on the host, as main.cpp:246-249 does. The build runs
+// on the GPU (device `device`, its own stream): build() uploads the host
+// triangles, runs mlbvh_build_ex and copies nodes, deltas and root back, and
+// returns when they are there. Its tree is the GPU build's, i.e. the
+// reference's with equal Morton keys in triangle-index order (the reference's
+// CPU build sorts with std::sort, whose order of equal keys is unspecified;
+// its GPU build sorts stably, as here). BUILD_OPTION_CPU_PARALLEL is accepted
+// and has no effect. Device buffers are kept for the next build and freed
+// with the object. Errors (and a bounded device wait that gave up) abort
+// with the library's message, as the reference's host asserts abort.
+class BVHCPUBuilder {
+public:
+    explicit BVHCPUBuilder(int device = 0) : m_device(device) {}
+    ~BVHCPUBuilder()
+    {
+        if (!m_stream) return;
+        int prev = 0;
+        cudaGetDevice(&prev);
+        cudaSetDevice(m_device);
+        cudaFree(m_dTriangles);
+        cudaFree(m_dInternals);
+        cudaFree(m_dRoot);
+        cudaFree(m_dDeltas);
+        cudaFree(m_dScratch);
+        cudaStreamDestroy(m_stream);
+        cudaSetDevice(prev);
+    }
+    BVHCPUBuilder(const BVHCPUBuilder&) = delete;
+    void operator=(const BVHCPUBuilder&) = delete;
+
+    void build(const Triangle* triangles, int nTriangles, uint32_t buildOption)
+    {
+        m_internals.clear();
+        m_deltas.clear();
+        m_rootNode = NodeIndex();
+        if (nTriangles <= 0) return;  // the reference requires nTriangles >= 1 (:515)
+        const uint32_t n = (uint32_t)nTriangles;
+        int prev = 0;
+        detail::check(cudaGetDevice(&prev), "cudaGetDevice");
+        detail::check(cudaSetDevice(m_device), "cudaSetDevice");
+        if (!m_stream) detail::check(cudaStreamCreateWithFlags(&m_stream, cudaStreamNonBlocking), "cudaStreamCreate");
+        grow(&m_dTriangles, &m_trianglesBytes, sizeof(Triangle) * n);
+        grow(&m_dInternals, &m_internalsBytes, sizeof(InternalNode) * (n > 1 ? n - 1 : 1));
+        grow(&m_dRoot, &m_rootBytes, 16);
+        grow(&m_dDeltas, &m_deltasBytes, n);
+        grow(&m_dScratch, &m_scratchBytes, mlbvh_build_scratch_bytes(n));
+        detail::check(cudaMemcpyAsync(m_dTriangles, triangles, sizeof(Triangle) * n, cudaMemcpyHostToDevice, m_stream),
+                      "cudaMemcpyAsync");
+        detail::check(mlbvh_build_ex(static_cast<const mlbvh_triangle*>(m_dTriangles), n, buildOption,
+                                     n > 1 ? static_cast<mlbvh_internal_node*>(m_dInternals) : nullptr,
+                                     static_cast<mlbvh_node_index*>(m_dRoot), nullptr, nullptr, nullptr,
+                                     static_cast<uint8_t*>(m_dDeltas), m_dScratch, m_scratchBytes, m_stream),
+                      "mlbvh_build_ex");
+        detail::check(mlbvh_scratch_status(m_dScratch, m_stream), "BVHCPUBuilder::build");
+        m_internals.resize(n - 1);
+        m_deltas.resize(n - 1);
+        if (n > 1) {
+            detail::check(cudaMemcpyAsync(m_internals.data(), m_dInternals, sizeof(InternalNode) * (n - 1),
+                                          cudaMemcpyDeviceToHost, m_stream),
+                          "cudaMemcpyAsync");
+            detail::check(cudaMemcpyAsync(m_deltas.data(), m_dDeltas, n - 1, cudaMemcpyDeviceToHost, m_stream),
+                          "cudaMemcpyAsync");
+        }
+        detail::check(cudaMemcpyAsync(&m_rootNode, m_dRoot, sizeof(NodeIndex), cudaMemcpyDeviceToHost, m_stream),
+                      "cudaMemcpyAsync");
+        detail::check(cudaStreamSynchronize(m_stream), "cudaStreamSynchronize");
+        detail::check(cudaSetDevice(prev), "cudaSetDevice");
+    }
+    bool empty() const { return m_internals.empty(); }
+    // validate_lbvh (minimum_lbvh.h:415-426) from the root with maxDelta 255:
+    // every internal node's split delta is at most its parent's. Walked with
+    // an explicit stack (a chain of equal keys makes the tree as deep as the
+    // chain is long); aborts on a violation, as the reference's assert does.
+    void validate() const
+    {
+        if (m_rootNode.m_isLeaf || m_internals.empty()) return;
+        std::vector<std::pair<NodeIndex, int>> todo{{m_rootNode, 255}};
+        while (!todo.empty()) {
+            const std::pair<NodeIndex, int> top = todo.back();
+            todo.pop_back();
+            if (top.first.m_isLeaf) continue;
+            const uint32_t i = top.first.m_index;
+            if (i >= m_internals.size() || (int)m_deltas[i] > top.second) {
+                std::fprintf(stderr, "minimum_lbvh: BVHCPUBuilder::validate failed at node %u\n", i);
+                std::abort();
+            }
+            todo.push_back({m_internals[i].children[0], (int)m_deltas[i]});
+            todo.push_back({m_internals[i].children[1], (int)m_deltas[i]});
+        }
+    }
+
+    NodeIndex m_rootNode;
+    std::vector<InternalNode> m_internals;
+    std::vector<uint8_t> m_deltas;
+
+private:
+    void grow(void** p, size_t* have, size_t need)
+    {
+        if (need <= *have) return;
+        if (*p) detail::check(cudaFree(*p), "cudaFree");
+        *p = nullptr;
+        detail::check(cudaMalloc(p, need), "cudaMalloc");
+        *have = need;
+    }
+    int m_device;
+    cudaStream_t m_stream = nullptr;
+    void* m_dTriangles = nullptr;
+    void* m_dInternals = nullptr;
+    void* m_dRoot = nullptr;
+    void* m_dDeltas = nullptr;
+    void* m_dScratch = nullptr;
+    size_t m_trianglesBytes = 0, m_internalsBytes = 0, m_rootBytes = 0, m_deltasBytes = 0, m_scratchBytes = 0;
 };
 
 }  // namespace minimum_lbvh

@@ -192,11 +192,16 @@ MLBVH_API mlbvh_status mlbvh_build_ex(const mlbvh_triangle* dTriangles, uint32_t
  * every GPU that loads the library until the process exits; it limits the
  * build to nTriangles <= 65536 (larger sizes return MLBVH_ERR_INVALID_ARG).
  * The caller still passes the triangles and the output buffers. The first
- * call on a device looks up the array's device address (cudaGetSymbolAddress,
- * with that device current); make that first call before any stream capture.
- * Every call shares the one array, which keeps the last call's contents:
- * calls that overlap on the GPU (e.g. on two streams) race and must be
- * serialised by the caller. Nothing is allocated or freed. */
+ * call in each CUDA context of a device (the first call on the device, and
+ * again after cudaDeviceReset) looks up the array's device address
+ * (cudaGetSymbolAddress, with that device current); make that first call
+ * before any stream capture. Every call shares the one array, which keeps
+ * the last call's contents: calls that overlap on the GPU (e.g. on two
+ * streams) race and must be serialised by the caller. Nothing is allocated
+ * or freed. Like mlbvh_build it does not synchronise; whether a bounded wait
+ * of the last call on this device gave up (its tree is then unusable) is
+ * reported by mlbvh_scratch_status(NULL, stream), and mlbvh_set_spin_limit
+ * applies to it as to mlbvh_build. */
 MLBVH_API mlbvh_status mlbvh_build_noalloc(const mlbvh_triangle* dTriangles, uint32_t nTriangles,
                                            uint32_t buildOption, mlbvh_internal_node* dInternals,
                                            mlbvh_node_index* dRootNode, mlbvh_aabb* dSceneAABB, void* stream);
@@ -222,8 +227,8 @@ MLBVH_API mlbvh_status mlbvh_build_ploc(const mlbvh_triangle* dTriangles, uint32
                                         mlbvh_aabb* dSceneAABB, void* dScratch, size_t scratchBytes, void* stream);
 
 /* Test hook: the number of polls after which a bounded device wait of the
- * builds that this host thread starts afterwards (mlbvh_build, _ex, _ploc)
- * gives up; 0 restores each build's default (a second or so). A wait that
+ * builds that this host thread starts afterwards (mlbvh_build, _ex, _ploc,
+ * _noalloc) gives up; 0 restores each build's default (a second or so). A wait that
  * gives up sets the build's error word and the build ends without hanging
  * (its output is then unusable); mlbvh_scratch_status reports it. Lets tests
  * make a wait run out without a device fault. */
@@ -231,7 +236,9 @@ MLBVH_API void mlbvh_set_spin_limit(uint32_t polls);
 
 /* Synchronises `stream`, then reports MLBVH_ERR_TIMEOUT if a bounded wait of
  * the last build that used dScratch gave up (its output is then unusable),
- * else MLBVH_OK. */
+ * else MLBVH_OK. dScratch = NULL asks the same of the last
+ * mlbvh_build_noalloc on the current device (its built-in scratch);
+ * MLBVH_ERR_INVALID_ARG when there was none in the current context. */
 MLBVH_API mlbvh_status mlbvh_scratch_status(const void* dScratch, void* stream);
 
 /* ---------------------------------------------------------------- query ---

@@ -30,6 +30,7 @@ void set_profile_events(cudaEvent_t start, cudaEvent_t stop)
     g_profile.start = start;
     g_profile.stop = stop;
 }
+uint32_t spin_limit() { return g_spinLimit; }
 ProfileEvents take_profile_events()
 {
     ProfileEvents e = g_profile;
@@ -93,6 +94,7 @@ mlbvh_status mlbvh_build_ex(const mlbvh_triangle* dTriangles, uint32_t nTriangle
 mlbvh_status mlbvh_scratch_status(const void* dScratch, void* stream)
 {
     clear_error();
+    if (!dScratch) return noalloc_scratch_status(as_stream(stream));
     return scratch_status(dScratch, as_stream(stream));
 }
 

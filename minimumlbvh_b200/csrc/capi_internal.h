@@ -37,6 +37,12 @@ mlbvh_status build(const mlbvh_triangle* dTris, uint32_t n, uint32_t option, mlb
                    mlbvh_node_index* dRoot, mlbvh_aabb* dScene, uint32_t* dKeysOut, uint32_t* dIdxOut,
                    uint8_t* dDeltasOut, void* dScratch, size_t scratchBytes, cudaStream_t stream, uint32_t spinLimit);
 mlbvh_status scratch_status(const void* dScratch, cudaStream_t stream);
+// The bounded-wait poll count set by mlbvh_set_spin_limit on this host thread
+// (0: each build's default).
+uint32_t spin_limit();
+// scratch_status of mlbvh_build_noalloc's built-in array in the current
+// context (noalloc.cu).
+mlbvh_status noalloc_scratch_status(cudaStream_t stream);
 
 // The build chain up to the sorted leaves (scene bounds, keys, four stable
 // sort passes), shared by build() and build_ploc(); the caller has checked

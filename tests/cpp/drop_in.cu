@@ -2,12 +2,13 @@
 // intersect_stackfree / intersect_escape_link inside the caller's own kernel),
 // compiled against include/minimum_lbvh.h and linked with libmlbvh_b200.so.
 // Used by tests/test_gpu_dropin.py:
-//   drop_in <triangles.bin> <rays.bin> <out.bin>
+//   drop_in <triangles.bin> <rays.bin> <out.bin> [ploc radius, 0 = LBVH] [timeout]
 // triangles.bin: n x 36 B; rays.bin: m x 32 B (ro, tmin, rd, tmax);
 // out.bin: root (4 B), nodes ((n-1) x 64 B), stack-free hits (m x 32 B),
 // escape-link any-hit hits (m x 32 B).
 #include <cstdio>
 #include <cstdlib>
+#include <string>
 #include <vector>
 
 #include "minimum_lbvh.h"
@@ -44,10 +45,38 @@ static std::vector<char> load(const char* path)
     return v;
 }
 
+// With the bounded device waits cut to one poll (mlbvh_set_spin_limit, a
+// test hook), builds whose waits give up must say so through
+// BVHGPUBuilder::status. Returns the number of MLBVH_ERR_TIMEOUT reports in
+// `tries` builds, or -1 on any status other than that and MLBVH_OK. The spin
+// limit is restored before returning; the caller then builds once more with
+// the default limit, and that tree is the one checked.
+static int count_timeouts(BVHGPUBuilder& builder, tinyhiponesweep::OnesweepSort& onesweep, const Triangle* dTris,
+                          int n, cudaStream_t stream, int ploc, int tries)
+{
+    int timeouts = 0;
+    mlbvh_set_spin_limit(1);
+    for (int i = 0; i < tries; ++i) {
+        if (ploc)
+            builder.buildByPLOC(dTris, n, 0, onesweep, stream, ploc);
+        else
+            builder.build(dTris, n, 0, onesweep, stream);
+        const mlbvh_status s = builder.status(stream);
+        if (s == MLBVH_ERR_TIMEOUT)
+            ++timeouts;
+        else if (s != MLBVH_OK)
+            timeouts = -1000;
+    }
+    mlbvh_set_spin_limit(0);
+    return timeouts < 0 ? -1 : timeouts;
+}
+
 int main(int argc, char** argv)
 {
-    // argv[4] (optional): a PLOC radius; the tree then comes from buildByPLOC
-    if (argc != 4 && argc != 5) return 2;
+    // argv[4] (optional): a PLOC radius; the tree then comes from buildByPLOC.
+    // argv[5] (optional): "timeout" first runs builds with one-poll waits
+    // (count_timeouts) and prints how many reported MLBVH_ERR_TIMEOUT.
+    if (argc < 4 || argc > 6) return 2;
     std::vector<char> tris = load(argv[1]), rays = load(argv[2]);
     const int n = (int)(tris.size() / sizeof(Triangle)), m = (int)(rays.size() / 32);
     if (n < 2 || m < 1) return 3;
@@ -65,10 +94,17 @@ int main(int argc, char** argv)
     cudaStreamCreate(&stream);
     tinyhiponesweep::OnesweepSort onesweep(0);
     BVHGPUBuilder builder("unused/minimum_lbvh.cu", "unused/");
-    if (argc == 5)
-        builder.buildByPLOC(dTris, n, 0, onesweep, stream, std::atoi(argv[4]));
+    const int ploc = argc >= 5 ? std::atoi(argv[4]) : 0;
+    if (argc == 6 && std::string(argv[5]) == "timeout") {
+        const int timeouts = count_timeouts(builder, onesweep, dTris, n, stream, ploc, 3);
+        if (timeouts < 0) return 6;
+        std::printf("drop_in: %d of 3 builds with one-poll waits reported MLBVH_ERR_TIMEOUT\n", timeouts);
+    }
+    if (ploc)
+        builder.buildByPLOC(dTris, n, 0, onesweep, stream, ploc);
     else
         builder.build(dTris, n, 0, onesweep, stream);
+    if (builder.status(stream) != MLBVH_OK) return 7;
     user_trace<<<(m + 127) / 128, 128, 0, stream>>>(dHits, dAny, dRays, m, builder.m_rootNode, builder.m_internals, dTris);
     if (cudaStreamSynchronize(stream) != cudaSuccess) return 4;
 

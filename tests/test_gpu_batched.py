@@ -4,7 +4,8 @@ that mesh alone (pinned to the reference's BVHCPUBuilder) bit for bit, and
 every ray's Hit record the oracle's stack-free traversal of its mesh. At the
 full batched configuration (1,024 meshes, 30.8M triangles, 169M rays) the
 batch is checked against the single-mesh entry points mesh by mesh, which
-are themselves oracle-pinned."""
+are themselves oracle-pinned, and a seeded sample of 64 meshes (the smallest
+and the largest among them) straight against the oracle."""
 import numpy as np
 import pytest
 
@@ -231,3 +232,24 @@ def test_batched_full_config_matches_single_mesh_path(cuda):
         h = mb.intersect(nodes.clone(), meshes[m], rays[r0:r1], root=root)
         bad_hits += int((h != hits[r0:r1]).any(1).sum())
     assert bad_hits == 0, bad_hits
+
+    # and straight against the oracle: a seeded sample of 64 meshes, the
+    # smallest and the largest among them, every node and every Hit record
+    counts = np.diff(offsets)
+    rng = np.random.default_rng(2026)
+    ends = [int(np.argmin(counts)), int(np.argmax(counts))]
+    sample = ends + [int(m) for m in rng.permutation(1024) if m not in ends][:62]
+    host_nodes = G.host(bb.internals, np.uint32)
+    host_roots = G.host(bb.roots, np.uint32)
+    host_hits = G.host(hits, np.uint32)
+    for m in sample:
+        a, e = int(offsets[m]), int(offsets[m + 1])
+        r0, r1 = int(roff[m]), int(roff[m + 1])
+        mesh = G.host(tris[a:e])
+        ref = O.build(mesh)
+        assert int(host_roots[m]) == ref["root"], f"mesh {m} root"
+        if e - a > 1:
+            assert (host_nodes[a - m: e - m - 1] == ref["nodes"]).all(), f"mesh {m} ({e - a} triangles) nodes"
+        exp = O.trace(ref["nodes"], mesh, ref["root"], G.host(rays[r0:r1]))
+        bad = int((host_hits[r0:r1] != exp).any(1).sum())
+        assert bad == 0, f"mesh {m} ({e - a} triangles): {bad} of {r1 - r0} hits differ from the oracle"

@@ -124,20 +124,6 @@ def test_ao_wide_equals_plain_heightfield(cuda, sobol):
     assert st1[6] == 0               # no restarts on this scene
 
 
-def test_ao_wide_equals_plain_soup(cuda):
-    """4M-triangle soup, 1920 x 1080, 64 AO rays of radius 0.1 per hit."""
-    tris = scenes.gaussian_soup()
-    b, t, out = G.build(tris)
-    eye, c, up, fovy = scenes.camera_soup()
-    cam = mb.RayGenerator.from_array(O.lookat(eye, c, up, fovy, 1920, 1080))
-    _, occ0, st0 = _ao(lambda *a, **k: mb.render_ao(a[0], a[1], a[2], b.m_rootNode, b.m_internals, t, *a[3:], **k),
-                       1920, 1080, 64, 0.1, 1, cam)
-    w = mb.WideBVH.from_builder(b, t)
-    _, occ1, st1 = _ao(mb.render_ao_wide, 1920, 1080, 64, 0.1, 1, cam, w)
-    np.testing.assert_array_equal(occ1, occ0)
-    assert (occ0 != MISS).mean() > 0.05
-
-
 def test_quantised_wide_slots_match_oracle(wcase):
     import torch
     _, tris, _, _, out, w, _ = wcase
@@ -200,15 +186,3 @@ def test_ao_quantised_wide_equals_plain_heightfield(cuda, sobol):
     np.testing.assert_array_equal(occ1, occ0)
     np.testing.assert_array_equal(px1, px0)
     assert st1[0] == st0[0] and st1[3] < 0.5 * st0[3]
-
-
-def test_ao_quantised_wide_equals_plain_soup(cuda):
-    tris = scenes.gaussian_soup()
-    b, t, out = G.build(tris)
-    eye, c, up, fovy = scenes.camera_soup()
-    cam = mb.RayGenerator.from_array(O.lookat(eye, c, up, fovy, 1920, 1080))
-    _, occ0, _ = _ao(lambda *a, **k: mb.render_ao(a[0], a[1], a[2], b.m_rootNode, b.m_internals, t, *a[3:], **k),
-                     1920, 1080, 64, 0.1, 1, cam)
-    w = mb.WideBVH.from_builder(b, t).quantise()
-    _, occ1, _ = _ao(lambda *a, **k: mb.render_ao_wide(*a, quantised=True, **k), 1920, 1080, 64, 0.1, 1, cam, w)
-    np.testing.assert_array_equal(occ1, occ0)
