@@ -125,6 +125,39 @@ def peaks():
     return 6650.0, "fallback"
 
 
+def onchip_peaks(dev, stream, reps: int = 10):
+    """Bandwidths this project measures itself with its own probe kernel
+    (mlbvh_read_probe: the traversal's 32-byte node load), CUDA events, best
+    of `reps` launches after a warm-up: 32-byte sectors streamed and gathered
+    at random from a 64 MiB buffer (resident in the 126 MB L2, beyond the
+    L1s) and from a 4 GiB one (HBM). GB/s."""
+    import torch
+    import minimumlbvh_b200 as mb
+    sink = torch.zeros(1024, dtype=torch.int32, device=dev)
+    out = {}
+    for where, nbytes in (("l2", 64 << 20), ("hbm", 4 << 30)):
+        buf = torch.empty(nbytes, dtype=torch.uint8, device=dev)
+        buf.random_(0, 256)
+        for pattern, name, loads in ((0, "stream", 64 if where == "l2" else 2), (1, "gather", 256)):
+            best = 0.0
+            for i in range(reps + 2):
+                a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                a.record(stream)
+                nread = mb.read_probe(buf, pattern, loads, sink, stream)
+                b.record(stream)
+                b.synchronize()
+                if i >= 2:
+                    best = max(best, nread / (a.elapsed_time(b) / 1e3) / 1e9)
+            out[f"{where}_{name}_gbs"] = best
+        del buf
+    torch.cuda.synchronize()
+    out["what"] = ("mlbvh_read_probe (ld.global.nc.v8, 32 B per load): 'stream' = consecutive sectors per warp, "
+                   "'gather' = one random 32-byte sector per load; l2 = 64 MiB buffer, hbm = 4 GiB buffer; "
+                   "best of 10 event-timed launches")
+    out["launches"] = 4 * (reps + 2)
+    return out
+
+
 def committed_traffic(workload):
     """DRAM bytes per launch of the dominant kernel from the committed ncu
     summary (profiles/traffic.json), or None."""
@@ -327,22 +360,23 @@ def bench_batched(args, dev, stream, barrier, max_over_ranks, world, n_meshes=10
     }
 
 
-def bench_precision(args, builder, qtree, d_tris, tris, cam, w, h, dev, stream, max_over_ranks):
+def bench_precision(args, builder, qtree, wide, d_tris, tris, cam, w, h, dev, stream, max_over_ranks):
     """The precision configuration: closest hits of 1M camera rays of the
-    frame (every other pixel) over the FP32 and the quantised tree: hit-ID
-    agreement, t equality, the largest t error against the FP64 evaluation of
-    the ray-plane formula (with its stated bound, fp64check), node bytes per
-    ray, and Mrays/s of both traversals (rays resident, CUDA events)."""
+    frame (every other pixel) over the FP32 and the quantised trees, each at
+    the same walk: the binary tree's replay walk (64-byte nodes against the
+    quantised 32-byte nodes) and the 4-wide tree's closest-hit walk (128-byte
+    slots against 64-byte quantised slots), beside the plain form (the
+    reference's stack-free walk). Hit-ID agreement and t equality with the
+    plain form, the largest t error against the FP64 evaluation of the
+    ray-plane formula (with its stated bound, fp64check), node bytes per ray,
+    and Mrays/s (rays resident, CUDA events)."""
     import torch
     import minimumlbvh_b200 as mb
     from minimumlbvh_b200 import fp64check, scenes
     rays_h = scenes.camera_rays(cam.m_origin, cam.m_right, cam.m_up, w, h, 2)
     n = len(rays_h)
     rays = torch.from_numpy(rays_h).to(dev)
-    hp = torch.empty((n, 8), dtype=torch.int32, device=dev)
-    hq = torch.empty_like(hp)
-    counts = torch.zeros(3 * n, dtype=torch.int32, device=dev)
-    mb.intersect_quantised(qtree, rays, 0, hits=hq, stack_depth=16, counts=counts)
+    closest = mb.RAY_QUERY_CLOSEST
 
     def run(fn):
         for _ in range(args.warmup):
@@ -356,19 +390,56 @@ def bench_precision(args, builder, qtree, d_tris, tris, cam, w, h, dev, stream, 
         torch.cuda.synchronize()
         return max_over_ranks(ev[0].elapsed_time(ev[1]) / 1e3 / args.steps)
 
-    tp = run(lambda: mb.intersect(builder, d_tris, rays, hits=hp))
-    tq = run(lambda: mb.intersect_quantised(qtree, rays, 0, hits=hq))
-    a = hp.cpu().numpy().view(np.uint32)
-    b = hq.cpu().numpy().view(np.uint32)
-    c = counts.cpu().numpy().astype(np.int64)
-    chk = fp64check.check_hits(tris, rays_h, b)
+    hits = {k: torch.empty((n, 8), dtype=torch.int32, device=dev) for k in
+            ("plain", "replay", "quantised_replay", "wide", "wide_quantised")}
+    calls = {
+        "plain": lambda: mb.intersect(builder, d_tris, rays, hits=hits["plain"]),
+        "replay": lambda: mb.intersect(builder, d_tris, rays, traversal=mb.TRAVERSAL_REPLAY, hits=hits["replay"]),
+        "quantised_replay": lambda: mb.intersect_quantised(qtree, rays, closest, hits=hits["quantised_replay"]),
+        "wide": lambda: mb.intersect_wide(wide, rays, hits=hits["wide"], rayQuery=closest),
+        "wide_quantised": lambda: mb.intersect_wide(wide, rays, hits=hits["wide_quantised"], quantised=True,
+                                                    rayQuery=closest),
+    }
+    # node bytes per ray from the counting variants
+    cq = torch.zeros(3 * n, dtype=torch.int32, device=dev)
+    mb.intersect_quantised(qtree, rays, closest, stack_depth=16, counts=cq)
+    cw = torch.zeros(3 * n, dtype=torch.int32, device=dev)
+    mb.intersect_wide(wide, rays, counts=cw, rayQuery=closest)
+    cwq = torch.zeros(3 * n, dtype=torch.int32, device=dev)
+    mb.intersect_wide(wide, rays, counts=cwq, quantised=True, rayQuery=closest)
+    times = {k: run(f) for k, f in calls.items()}
+    host = {k: v.cpu().numpy().view(np.uint32) for k, v in hits.items()}
+    c = cq.cpu().numpy().astype(np.int64)
+    cwh = cw.cpu().numpy().astype(np.int64)
+    cwqh = cwq.cpu().numpy().astype(np.int64)
+    a = host["plain"]
+    forms = {}
+    node_bytes = {"quantised_replay": (32 * c[:n].sum() + 4 * c[2 * n:].sum()) / n,
+                  "wide": 128 * cwh[:n].sum() / n, "wide_quantised": 64 * cwqh[:n].sum() / n}
+    for k in calls:
+        b = host[k]
+        forms[k] = {"mrays_s": n / times[k] / 1e6, "vs_plain": times["plain"] / times[k],
+                    "hit_id_agreement": float((a[:, 7] == b[:, 7]).mean()),
+                    "t_equal": float((a[:, 0] == b[:, 0]).mean())}
+        if k in node_bytes:
+            forms[k]["node_bytes_per_ray"] = node_bytes[k]
+    chk = fp64check.check_hits(tris, rays_h, host["quantised_replay"])
+    chkw = fp64check.check_hits(tris, rays_h, host["wide_quantised"])
     return {
         "rays": n, "rays_desc": f"camera rays of every other pixel of the {w}x{h} frame, closest hit",
-        "hit_id_agreement": float((a[:, 7] == b[:, 7]).mean()), "t_equal": float((a[:, 0] == b[:, 0]).mean()),
+        "hit_id_agreement": forms["quantised_replay"]["hit_id_agreement"],
+        "t_equal": forms["quantised_replay"]["t_equal"],
         "hits": chk["hits"], "max_abs_t_err_vs_fp64": chk["max_abs_err"], "max_rel_t_err_vs_fp64": chk["max_rel_err"],
         "max_t_err_over_bound": chk["max_bound_ratio"],
-        "node_bytes_per_ray": (32 * c[:n].sum() + 4 * c[2 * n:].sum()) / n,
-        "quantised_mrays_s": n / tq / 1e6, "plain_mrays_s": n / tp / 1e6, "vs_plain": tp / tq,
+        "wide_quantised_max_t_err_over_bound": chkw["max_bound_ratio"],
+        "node_bytes_per_ray": node_bytes["quantised_replay"],
+        "quantised_mrays_s": forms["quantised_replay"]["mrays_s"], "plain_mrays_s": forms["plain"]["mrays_s"],
+        "vs_plain": forms["quantised_replay"]["vs_plain"],
+        "equal_walk": {"quantised_vs_fp32_binary_replay": times["replay"] / times["quantised_replay"],
+                       "quantised_vs_fp32_wide": times["wide"] / times["wide_quantised"]},
+        "best": max(forms, key=lambda k: forms[k]["mrays_s"] if forms[k]["hit_id_agreement"] == 1.0 else 0),
+        "forms": forms,
+        "launches": 3 + (len(calls)) * (args.warmup + args.steps),
     }
 
 
@@ -1093,7 +1164,7 @@ def main():
         e2e_chosen_s = max_over_ranks(cev[0].elapsed_time(cev[1]) / 1e3)
         del wides
         builder.build(d_tris, n, 0, sorter)
-        precision = bench_precision(args, builder, qtree, d_tris, tris, cam, w, h, dev, stream, max_over_ranks)
+        precision = bench_precision(args, builder, qtree, wide, d_tris, tris, cam, w, h, dev, stream, max_over_ranks)
         pt = bench_pt(args, dev, stream, max_over_ranks,
                       reference_gpu=not args.no_reference_gpu and rank == 0 and world == 1)
         diff = None if args.no_diff else bench_diff(args, dev, stream, max_over_ranks)
@@ -1103,6 +1174,7 @@ def main():
                                                 lambda x: x)
         batched = None if args.no_batched else bench_batched(args, dev, stream, barrier, max_over_ranks,
                                                                    world, args.batched_meshes, not args.no_autotune)
+        onchip = onchip_peaks(dev, stream)
     clocks = sampler.summary()
 
     ms_per_step = ao_total_s * 1e3 / args.steps
@@ -1129,11 +1201,25 @@ def main():
     kernel_bytes = 64 * ao_visits + 36 * ao_tests
     achieved = kernel_bytes / kernel_avg_s / 1e9
     traffic = committed_traffic(args.workload)
-    line["roofline"] = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                        "traffic": traffic, "kernel": "k_ao_rays", "kernel_ms": kernel_avg_s * 1e3,
-                        "peak_source": f"{peak_kind} hbm_gbs",
+    # The kernel's bytes are served on chip (L1 and L2 hits; its DRAM traffic
+    # is a fraction of a percent of them), so its roofline is the on-chip
+    # bandwidth of its own load pattern: 32-byte sectors gathered at random
+    # from an L2-resident buffer, measured by this project's probe kernel.
+    # The HBM copy bandwidth is kept as the denominator of its DRAM traffic.
+    onchip_peak = onchip["l2_gather_gbs"]
+    line["roofline"] = {"bound": "l2", "achieved": achieved, "peak": onchip_peak, "unit": "GB/s",
+                        "frac": achieved / onchip_peak, "traffic": traffic, "kernel": "k_ao_rays",
+                        "kernel_ms": kernel_avg_s * 1e3,
+                        "peak_source": "builder-measured: mlbvh_read_probe gathering random 32-byte sectors from a "
+                                       "64 MiB L2-resident buffer (the traversal's load), CUDA events",
+                        "frac_of_l2_stream": achieved / onchip["l2_stream_gbs"],
+                        "hbm": {"peak": peak, "peak_source": f"{peak_kind} hbm_gbs",
+                                "traffic_gbs": (traffic / kernel_avg_s / 1e9) if traffic else None,
+                                "frac": (traffic / kernel_avg_s / 1e9 / peak) if traffic else None},
+                        "onchip_peaks": onchip,
                         "bytes_model": "64 B per internal-node visit + 36 B per triangle test",
-                        "node_visits_per_ray": visits / rays_per_frame, "tri_tests_per_ray": tests / rays_per_frame, "kernel_bytes": kernel_bytes}
+                        "node_visits_per_ray": visits / rays_per_frame, "tri_tests_per_ray": tests / rays_per_frame,
+                        "kernel_bytes": kernel_bytes}
     build_s = build_total_s / args.steps
     line["build"] = {"ms": build_s * 1e3, "mtri_s": n * world / build_s / 1e6,
                      "achieved_gbs": n * BUILD_BYTES_PER_TRI / build_s / 1e9,
@@ -1176,8 +1262,8 @@ def main():
             ao_node_bytes = (128 if name == "wide" else 64) * int(fst[3])
         f_kernel_bytes = ao_node_bytes + 48 * int(fst[4])
         f_achieved = f_kernel_bytes / f_kernel_s / 1e9
-        form_lines_roof = {"kernel_ms": f_kernel_s * 1e3, "achieved": f_achieved, "peak": peak, "unit": "GB/s",
-                           "frac": f_achieved / peak, "kernel_bytes": f_kernel_bytes}
+        form_lines_roof = {"kernel_ms": f_kernel_s * 1e3, "achieved": f_achieved, "peak": onchip_peak,
+                           "unit": "GB/s", "frac": f_achieved / onchip_peak, "kernel_bytes": f_kernel_bytes}
         form_lines[name] = {
             "form": form_desc[name],
             "value": f_rays * args.steps * world / total_s / 1e6, "unit": "Mrays/s",
@@ -1200,6 +1286,7 @@ def main():
     line["chosen"]["plain_node_bytes_per_ray"] = 64 * visits / max(rays_per_frame, 1)
     line["forms"] = form_lines
     line["precision"] = precision
+    line["gpu_launches"] += precision["launches"]
     line["pt"] = pt
     if ploc is not None:
         line["ploc"] = ploc
@@ -1215,6 +1302,7 @@ def main():
         if "ao" in reference_gpu:  # our kernels launched in that leg: plain (3) and wide (3) frames, 2 builds
             line["gpu_launches"] += (args.warmup + args.steps) * (3 + 3 + 7) + 2
     line["gpu_launches"] += 2 * (args.warmup + args.steps) + 1
+    line["gpu_launches"] += onchip["launches"]
     if batched is not None:
         line["batched"] = batched
         line["gpu_launches"] += batched["launches"]

@@ -531,6 +531,19 @@ MLBVH_API void mlbvh_obj_free(mlbvh_obj_mesh* mesh);
  * build kernel). NULL, NULL cancels. */
 MLBVH_API void mlbvh_profile_events(void* startEvent, void* stopEvent);
 
+/* Measurement hook (no reference counterpart): one launch that reads dBuffer
+ * with the traversal kernels' node load (32 bytes per instruction through L1
+ * and L2), so that CUDA events around it give the bandwidth such loads reach
+ * from where the buffer lives (tens of MB: L2; GBs: HBM). pattern 0 streams:
+ * consecutive threads read consecutive 32-byte sectors, `loads` sweeps over
+ * the buffer; pattern 1 gathers: each thread makes `loads` (a multiple of 8)
+ * loads of pseudo-random sectors (bytes must then be 32 * 2^k). *bytesRead
+ * (host) receives the bytes the launch reads. dSink: 1024 device words that
+ * keep the loads from being optimised away (practically never written).
+ * bytes: a multiple of 32, at least 32 KiB; dBuffer 32-byte aligned. */
+MLBVH_API mlbvh_status mlbvh_read_probe(const void* dBuffer, size_t bytes, int pattern, uint32_t loads,
+                                        uint32_t* dSink, size_t* bytesRead, void* stream);
+
 /* RayGenerator::lookat (camera.h:10-22), on the host. */
 MLBVH_API mlbvh_status mlbvh_camera_lookat(mlbvh_ray_generator* out, const float eye[3], const float center[3],
                                  const float up[3], float fovy, int width, int height);

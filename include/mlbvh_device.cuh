@@ -1053,11 +1053,13 @@ __device__ __forceinline__ uint32_t wpick(const uint4& v, int k)
 }
 
 // One visit: which non-empty children pass (bit mask), the nearest of them
-// (entry distance, ties to the lower slot; -1 if none) and the child words.
+// (entry distance, ties to the lower slot; -1 if none), the child words and
+// every child's entry distance (the closest-hit walk orders by them).
 struct WideVisit {
     uint32_t pass;
     int best;
     uint4 ch;
+    float entry[4];
 };
 // FP32 slot: three 32-byte plane loads and the 16-byte child words.
 __device__ __forceinline__ WideVisit wide_visit(const mlbvh_wnode* __restrict__ wnodes, uint32_t i, f3 ro, f3 inv,
@@ -1068,12 +1070,13 @@ __device__ __forceinline__ WideVisit wide_visit(const mlbvh_wnode* __restrict__ 
     ldg32(p, lx, hx);
     ldg32(p + 2, ly, hy);
     ldg32(p + 4, lz, hz);
-    WideVisit w{0u, -1, __ldg(reinterpret_cast<const uint4*>(p + 6))};
+    WideVisit w{0u, -1, __ldg(reinterpret_cast<const uint4*>(p + 6)), {}};
     float bestT = 0.0f;
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
         const float2 r = slab(ro, inv, mk(wpick(lx, k), wpick(ly, k), wpick(lz, k)),
                               mk(wpick(hx, k), wpick(hy, k), wpick(hz, k)), tmin, hitT);
+        w.entry[k] = r.x;
         if (wpick(w.ch, k) != kWideEmpty && r.x <= r.y) {
             w.pass |= 1u << k;
             if (w.best < 0 || r.x < bestT) {
@@ -1086,16 +1089,32 @@ __device__ __forceinline__ WideVisit wide_visit(const mlbvh_wnode* __restrict__ 
 }
 
 // Quantised slot (two 32-byte loads). Plane code q of axis a stands for
-// base[a] + scale[a] * (1 + q / 2^15): one byte permute writes q into
-// mantissa byte 1 of the power of two scale[a]. Relative to the ray origin,
-// lower planes are base - ro rounded down plus that value rounded down, upper
-// planes the same rounded up, so they lie at or outside the exact planes (the
-// codes were rounded outward too) and the slab test on them passes wherever
-// it passes on the exact box.
+// base[a] + V, V = scale[a] (1 + q / 2^15): one byte permute writes q into
+// mantissa byte 1 of the power of two scale[a], which gives V exactly.
 __device__ __forceinline__ float qw_value(uint32_t codes, uint32_t scaleBits, int k)
 {
     return __uint_as_float(__byte_perm(codes, scaleBits, 0x7604u | ((uint32_t)k << 4)));
 }
+// Relative margins of the quantised slab test: 2^-22 below the entry and
+// 2^-21 above the exit (see qwide_visit).
+constexpr float kQEntryMargin = 2.384185791015625e-07f;
+constexpr float kQExitMargin = 4.76837158203125e-07f;
+
+// The distance of a plane along the ray, (base + V - ro) inv, is one FMA per
+// plane: V inv + C, where C = base inv - ro inv bounds (base - ro) inv from
+// below for near planes (ro inv rounded up, the FMA rounded down) and from
+// above for far planes (ro inv rounded down, the FMA rounded up); the plane's
+// FMA is rounded the same way. On an axis whose inv is positive the near
+// plane is the lower one, on one whose inv is negative the upper one (inv is
+// never 0). A child's entry is the largest of its near distances, its exit
+// the smallest far one, each moved outward by a relative margin (entry -
+// 2^-22 |entry| rounded down, exit + 2^-21 |exit| rounded up) that covers
+// the reference slab's own rounding on the exact box (two roundings per
+// distance, then the 1.00000024 factor on the exit and its rounding). The
+// codes were rounded outward too, so entry <= the reference's entry and exit
+// >= its exit: the test passes wherever the reference's passes on the exact
+// box. Every rounding is directed, so a distance that overflows stays on its
+// conservative side (an FMA rounded down gives FLT_MAX or -inf).
 __device__ __forceinline__ WideVisit qwide_visit(const mlbvh_qwnode* __restrict__ qw, uint32_t i, f3 ro, f3 inv,
                                                  float tmin, float hitT)
 {
@@ -1103,26 +1122,39 @@ __device__ __forceinline__ WideVisit qwide_visit(const mlbvh_qwnode* __restrict_
     float4 a, b, c, d;
     ldg32(p, a, b);
     ldg32(p + 2, c, d);
-    const f3 dlo = mk(__fsub_rd(a.x, ro.x), __fsub_rd(a.y, ro.y), __fsub_rd(a.z, ro.z));
-    const f3 dhi = mk(__fsub_ru(a.x, ro.x), __fsub_ru(a.y, ro.y), __fsub_ru(a.z, ro.z));
     const uint32_t sx = __float_as_uint(a.w), sy = __float_as_uint(b.x), sz = __float_as_uint(b.y);
+    const bool fx = inv.x < 0.0f, fy = inv.y < 0.0f, fz = inv.z < 0.0f;
     const uint32_t qxl = __float_as_uint(b.z), qxh = __float_as_uint(b.w), qyl = __float_as_uint(c.x),
                    qyh = __float_as_uint(c.y), qzl = __float_as_uint(c.z), qzh = __float_as_uint(c.w);
+    const uint32_t nqx = fx ? qxh : qxl, fqx = fx ? qxl : qxh;
+    const uint32_t nqy = fy ? qyh : qyl, fqy = fy ? qyl : qyh;
+    const uint32_t nqz = fz ? qzh : qzl, fqz = fz ? qzl : qzh;
+    const float cnx = __fmaf_rd(a.x, inv.x, -__fmul_ru(ro.x, inv.x));
+    const float cny = __fmaf_rd(a.y, inv.y, -__fmul_ru(ro.y, inv.y));
+    const float cnz = __fmaf_rd(a.z, inv.z, -__fmul_ru(ro.z, inv.z));
+    const float cfx = __fmaf_ru(a.x, inv.x, -__fmul_rd(ro.x, inv.x));
+    const float cfy = __fmaf_ru(a.y, inv.y, -__fmul_rd(ro.y, inv.y));
+    const float cfz = __fmaf_ru(a.z, inv.z, -__fmul_rd(ro.z, inv.z));
+    const float lo = fmaxf(0.0f, tmin);
     WideVisit w{0u, -1, make_uint4(__float_as_uint(d.x), __float_as_uint(d.y), __float_as_uint(d.z),
-                                   __float_as_uint(d.w))};
+                                   __float_as_uint(d.w)), {}};
     float bestT = 0.0f;
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
-        const f3 lo = mk(__fadd_rd(dlo.x, qw_value(qxl, sx, k)), __fadd_rd(dlo.y, qw_value(qyl, sy, k)),
-                         __fadd_rd(dlo.z, qw_value(qzl, sz, k)));
-        const f3 hi = mk(__fadd_ru(dhi.x, qw_value(qxh, sx, k)), __fadd_ru(dhi.y, qw_value(qyh, sy, k)),
-                         __fadd_ru(dhi.z, qw_value(qzh, sz, k)));
-        const float2 r = slab_offsets(lo, hi, inv, tmin, hitT);
-        if (wpick(w.ch, k) != kWideEmpty && r.x <= r.y) {
+        const float en = fmaxf(fmaxf(__fmaf_rd(qw_value(nqx, sx, k), inv.x, cnx),
+                                     __fmaf_rd(qw_value(nqy, sy, k), inv.y, cny)),
+                               __fmaf_rd(qw_value(nqz, sz, k), inv.z, cnz));
+        const float ex = fminf(fminf(__fmaf_ru(qw_value(fqx, sx, k), inv.x, cfx),
+                                     __fmaf_ru(qw_value(fqy, sy, k), inv.y, cfy)),
+                               __fmaf_ru(qw_value(fqz, sz, k), inv.z, cfz));
+        const float entry = fmaxf(__fmaf_rd(fabsf(en), -kQEntryMargin, en), lo);
+        const float exit = fminf(__fmaf_ru(fabsf(ex), kQExitMargin, ex), hitT);
+        w.entry[k] = entry;
+        if (wpick(w.ch, k) != kWideEmpty && entry <= exit) {
             w.pass |= 1u << k;
-            if (w.best < 0 || r.x < bestT) {
+            if (w.best < 0 || entry < bestT) {
                 w.best = k;
-                bestT = r.x;
+                bestT = entry;
             }
         }
     }
@@ -1188,6 +1220,95 @@ __device__ __forceinline__ bool wide_any_step(uint32_t& curr, uint32_t& prev, in
     if (depth == 0) return true;
     curr = stack[--depth * stride];
     return false;
+}
+
+// The closest-hit walk over the wide tree (FP32 slots, or quantised slots
+// with kQuant). At a slot, the children whose box passes are entered in the
+// order of their sort keys, nearest first: the key of child k is the bits of
+// its entry distance (>= 0) with the two lowest bits replaced by k, so entries
+// within four ulps go in slot order. The others are pushed farthest first,
+// each with its key's distance (at most its entry), and a popped child is
+// entered only if that distance is still <= hit.t (a box whose entry lies
+// beyond hit.t fails the slab test). A triangle hit at t <= hit.t (the
+// reference's inclusive test) replaces the hit; on the quantised slots only
+// if the leaf's exact box passes the slab test too. A visit whose pushes would
+// overflow the stack (kWideDepth entries of {child, distance}, `stride` apart)
+// continues with the closest-hit stack-free walk over the binary tree from
+// `binaryRoot`, keeping the hit found so far (depth < 0 from then on; ++nr).
+// The hit found is intersect_stackfree's wherever the nearest hit triangle's
+// own box passes the slab test at that triangle's distance (a box holds its
+// triangle, and the boxes above it pass whenever it does, so the walk enters
+// it whatever the order); the order decides only between hits at
+// bit-identical t, and where the rounded slabs exclude the hit point from its
+// triangle's box. Returns true when the walk is over.
+__device__ __forceinline__ uint32_t wide_sort_key(const WideVisit& w, int k)
+{
+    return (w.pass & (1u << k)) ? ((__float_as_uint(w.entry[k]) & 0x7FFFFFFCu) | (uint32_t)k) : 0xFFFFFFFFu;
+}
+template <bool kCount, bool kQuant, class Slot>
+__device__ __forceinline__ bool wide_closest_step(uint32_t& curr, uint32_t& prev, int& depth, uint2* stack,
+                                                  int stride, HitRecord& hit, const Slot* __restrict__ slots,
+                                                  const mlbvh_internal_node* __restrict__ nodes,
+                                                  const float* __restrict__ tris,
+                                                  const mlbvh_qtri* __restrict__ leafTris, uint32_t binaryRoot, f3 ro,
+                                                  f3 rd, f3 inv, float tmin, uint32_t& nv, uint32_t& nt,
+                                                  uint32_t& nr)
+{
+    if (depth < 0) return stackfree_step<false, kCount, true>(curr, prev, hit, nodes, tris, ro, rd, inv, tmin, nv, nt);
+    if (curr & kLeafBit) {
+        if (kCount) ++nt;
+        const float4* t = reinterpret_cast<const float4*>(leafTris + (curr & ~kLeafBit));
+        const float4 a = __ldg(t), b = __ldg(t + 1), c = __ldg(t + 2);
+        const f3 v0 = mk(a.x, a.y, a.z), v1 = mk(a.w, b.x, b.y), v2 = mk(b.z, b.w, c.x);
+        float tt, u, v;
+        f3 ng;
+        if (intersect_triangle(tt, u, v, ng, tmin, hit.t, ro, rd, v0, v1, v2) &&
+            (!kQuant || leaf_box_passes(ro, inv, v0, v1, v2, tmin, hit.t))) {
+            hit.t = tt;
+            hit.u = u;
+            hit.v = v;
+            hit.ng = ng;
+            hit.tri = __float_as_uint(c.y);
+        }
+    } else {
+        if (kCount) ++nv;
+        WideVisit w;
+        if constexpr (kQuant)
+            w = qwide_visit(slots, curr, ro, inv, tmin, hit.t);
+        else
+            w = wide_visit(slots, curr, ro, inv, tmin, hit.t);
+        if (w.pass) {
+            const int np = __popc(w.pass);
+            if (depth + np - 1 > kWideDepth) {
+                if (kCount) ++nr;
+                depth = -1;
+                curr = binaryRoot;
+                prev = kInvalid;
+                return false;
+            }
+            // sort the four keys (a five-exchange network); non-passing children sort last
+            uint32_t k0 = wide_sort_key(w, 0), k1 = wide_sort_key(w, 1), k2 = wide_sort_key(w, 2),
+                     k3 = wide_sort_key(w, 3), x;
+            x = min(k0, k1); k1 = max(k0, k1); k0 = x;
+            x = min(k2, k3); k3 = max(k2, k3); k2 = x;
+            x = min(k0, k2); k2 = max(k0, k2); k0 = x;
+            x = min(k1, k3); k3 = max(k1, k3); k1 = x;
+            x = min(k1, k2); k2 = max(k1, k2); k1 = x;
+            if (np == 4) stack[depth++ * stride] = make_uint2(wpick(w.ch, (int)(k3 & 3u)), k3 & 0x7FFFFFFCu);
+            if (np >= 3) stack[depth++ * stride] = make_uint2(wpick(w.ch, (int)(k2 & 3u)), k2 & 0x7FFFFFFCu);
+            if (np >= 2) stack[depth++ * stride] = make_uint2(wpick(w.ch, (int)(k1 & 3u)), k1 & 0x7FFFFFFCu);
+            curr = wpick(w.ch, (int)(k0 & 3u));
+            return false;
+        }
+    }
+    while (depth > 0) {
+        const uint2 e = stack[--depth * stride];
+        if (__uint_as_float(e.y) <= hit.t) {
+            curr = e.x;
+            return false;
+        }
+    }
+    return true;
 }
 
 }  // namespace mlbvh

@@ -23,7 +23,7 @@ __all__ = [
     "WideBVH", "intersect_wide", "render_ao_wide",
     "render_normal", "render_ao", "render_pt", "pack", "profile_events", "FLT_MAX", "INVALID_NODE",
     "QuantisedBVH", "intersect_quantised", "render_ao_quantised", "pt_diff_render", "pt_diff_adjoint",
-    "BatchParams", "BatchedBVH", "leaf_triangles", "load_obj",
+    "BatchParams", "BatchedBVH", "leaf_triangles", "load_obj", "read_probe",
 ]
 
 BUILD_OPTION_USE_NORMAL = 1   # minimum_lbvh.h:44
@@ -115,6 +115,7 @@ def lib() -> ctypes.CDLL:
             "mlbvh_batch_graph_create": (i32, [_vp, _vp, i32, _vp]),
             "mlbvh_batch_graph_launch": (i32, [_vp, _vp]),
             "mlbvh_batch_graph_destroy": (None, [_vp]),
+            "mlbvh_read_probe": (i32, [_vp, sz, i32, u32, _vp, _vp, _vp]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -327,6 +328,19 @@ def render_normal(pixels, imageSize, rayGenerator: RayGenerator, rootNode, inter
 _render_scratch = {}
 
 
+def read_probe(buffer, pattern: int, loads: int, sink, stream=None) -> int:
+    """mlbvh_read_probe: one launch reading ``buffer`` (a 32-byte aligned
+    device tensor) with the traversal's 32-byte node load, streaming
+    (pattern 0, ``loads`` sweeps) or gathering random sectors (pattern 1,
+    ``loads`` per thread); ``sink`` is a device tensor of at least 1024 int32.
+    Returns the bytes the launch reads; time it with CUDA events."""
+    _require_cuda(buffer, "buffer")
+    out = ctypes.c_size_t(0)
+    _check(lib().mlbvh_read_probe(_ptr(buffer), buffer.numel() * buffer.element_size(), int(pattern), int(loads),
+                                  _ptr(sink), ctypes.byref(out), _stream(stream)))
+    return int(out.value)
+
+
 def profile_events(start=None, stop=None):
     """Make the next render_ao / BVHGPUBuilder.build on this thread record
     the torch.cuda.Event pair around its dominant kernel."""
@@ -433,11 +447,13 @@ class WideBVH:
         return self
 
 
-def intersect_wide(w: WideBVH, rays, hits=None, counts=None, stream=None, quantised: bool = False):
-    """Any-hit rays over the 4-wide tree (mlbvh_trace_wide, or with
-    ``quantised`` mlbvh_trace_wide_quantised over ``w.quantise()``'s slots).
-    ``counts`` (int32 CUDA tensor of 3 * nRays) receives per-ray node visits,
-    triangle tests and restarts."""
+def intersect_wide(w: WideBVH, rays, hits=None, counts=None, stream=None, quantised: bool = False,
+                   rayQuery: int = RAY_QUERY_ANY):
+    """Rays over the 4-wide tree (mlbvh_trace_wide, or with ``quantised``
+    mlbvh_trace_wide_quantised over ``w.quantise()``'s slots), any-hit
+    (default) or closest-hit (``rayQuery=RAY_QUERY_CLOSEST``: the stack-free
+    walk's Hit records). ``counts`` (int32 CUDA tensor of 3 * nRays) receives
+    per-ray node visits, triangle tests and restarts."""
     import torch
     _require_cuda(rays, "rays")
     n = rays.numel() // 8
@@ -447,12 +463,12 @@ def intersect_wide(w: WideBVH, rays, hits=None, counts=None, stream=None, quanti
     if quantised:
         _check(lib().mlbvh_trace_wide_quantised(_ptr(w.qwide), _ptr(w.status), _ptr(b.m_internals),
                                                 _ptr(b.m_rootNode), _ptr(w.triangles), _ptr(w.leaf_triangles),
-                                                _ptr(rays), _ptr(hits), n, RAY_QUERY_ANY, _ptr(counts),
+                                                _ptr(rays), _ptr(hits), n, int(rayQuery), _ptr(counts),
                                                 _stream(stream)))
     else:
         _check(lib().mlbvh_trace_wide(_ptr(w.wide), _ptr(b.m_internals), _ptr(b.m_rootNode), _ptr(w.triangles),
-                                      _ptr(w.leaf_triangles), _ptr(rays), _ptr(hits), n, RAY_QUERY_ANY, _ptr(counts),
-                                      _stream(stream)))
+                                      _ptr(w.leaf_triangles), _ptr(rays), _ptr(hits), n, int(rayQuery),
+                                      _ptr(counts), _stream(stream)))
     return hits
 
 

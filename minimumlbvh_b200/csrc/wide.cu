@@ -1,7 +1,7 @@
-// The 4-wide tree for any-hit rays (no reference counterpart): a regrouping
-// of the binary tree that intersect_stackfree walks (minimum_lbvh.h:981-1061)
-// with the same leaves and the same boxes, so that an any-hit ray loads half
-// as many nodes in a chain. Slot i of the wide array is the expansion of
+// The 4-wide tree (no reference counterpart): a regrouping of the binary tree
+// that intersect_stackfree walks (minimum_lbvh.h:981-1061) with the same
+// leaves and the same boxes, so that a ray loads half as many nodes in a
+// chain (any-hit and closest-hit walks). Slot i of the wide array is the expansion of
 // binary internal node i, written by one thread with no order between slots:
 // the walk starts at the root's slot and only ever follows child indices,
 // which name the slots of their own expansions.
@@ -171,11 +171,12 @@ __global__ void __launch_bounds__(kWideThreads)
     reinterpret_cast<uint4*>(dst)[3] = ch;
 }
 
-// One thread per ray, any-hit, over FP32 slots or (kQuant) quantised slots.
-// counts (may be null): per ray, node visits, triangle tests and restarts at
+// One thread per ray, any-hit (wide_any_step) or closest-hit
+// (wide_closest_step), over FP32 slots or (kQuant) quantised slots. counts
+// (may be null): per ray, node visits, triangle tests and restarts at
 // counts[i], counts[n + i], counts[2n + i]. status (quantised slots): nonzero
 // sends every ray to the stack-free walk over the binary tree.
-template <bool kCount, bool kQuant, class Slot>
+template <bool kAny, bool kCount, bool kQuant, class Slot>
 __global__ void __launch_bounds__(kWideTraceThreads)
     k_trace_wide(const Slot* __restrict__ slots, const uint32_t* __restrict__ status,
                  const mlbvh_internal_node* __restrict__ nodes, const mlbvh_node_index* __restrict__ rootPtr,
@@ -183,7 +184,8 @@ __global__ void __launch_bounds__(kWideTraceThreads)
                  const float4* __restrict__ rays, float4* __restrict__ hits, uint32_t n,
                  uint32_t* __restrict__ counts)
 {
-    __shared__ uint32_t s_stack[kWideDepth][kWideTraceThreads];
+    using Entry = typename ReplayStack<kAny>::Entry;
+    __shared__ Entry s_stack[kWideDepth][kWideTraceThreads];
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const float4 a = __ldg(rays + 2 * (size_t)i), b = __ldg(rays + 2 * (size_t)i + 1);
@@ -203,10 +205,17 @@ __global__ void __launch_bounds__(kWideTraceThreads)
         curr = root;
         depth = -1;
     }
-    for (uint32_t steps = 1; steps < kMaxTraversalSteps; ++steps)
-        if (wide_any_step<kCount, kQuant>(curr, prev, depth, &s_stack[0][threadIdx.x], kWideTraceThreads, hit, slots,
-                                          nodes, tris, leafTris, root, ro, rd, inv, a.w, nv, nt, nr))
-            break;
+    for (uint32_t steps = 1; steps < kMaxTraversalSteps; ++steps) {
+        bool done;
+        if constexpr (kAny)
+            done = wide_any_step<kCount, kQuant>(curr, prev, depth, &s_stack[0][threadIdx.x], kWideTraceThreads, hit,
+                                                 slots, nodes, tris, leafTris, root, ro, rd, inv, a.w, nv, nt, nr);
+        else
+            done = wide_closest_step<kCount, kQuant>(curr, prev, depth, &s_stack[0][threadIdx.x], kWideTraceThreads,
+                                                     hit, slots, nodes, tris, leafTris, root, ro, rd, inv, a.w, nv,
+                                                     nt, nr);
+        if (done) break;
+    }
     hits[2 * (size_t)i] = make_float4(hit.t, 0.0f, hit.u, hit.v);
     hits[2 * (size_t)i + 1] = make_float4(hit.ng.x, hit.ng.y, hit.ng.z, __uint_as_float(hit.tri));
     if (kCount) {
@@ -243,7 +252,8 @@ mlbvh_status launch_trace_wide(const Slot* dSlots, const uint32_t* dStatus, cons
                                int rayQuery, uint32_t* dCounts, cudaStream_t stream)
 {
     if (nRays == 0) return MLBVH_OK;
-    if (rayQuery != MLBVH_RAY_QUERY_ANY) return fail(MLBVH_ERR_INVALID_ARG, "the wide tree takes any-hit rays only");
+    if (rayQuery != MLBVH_RAY_QUERY_ANY && rayQuery != MLBVH_RAY_QUERY_CLOSEST)
+        return fail(MLBVH_ERR_INVALID_ARG, "rayQuery must be MLBVH_RAY_QUERY_CLOSEST or MLBVH_RAY_QUERY_ANY");
     if (!dRoot || !dTris || !dLeafTris || !dRays || !dHits || (kQuant && !dStatus))
         return fail(MLBVH_ERR_INVALID_ARG, "null pointer");
     if (!(kQuant ? aligned32(dSlots) : aligned128(dSlots)) || !aligned32(dNodes) || !aligned16(dRoot) ||
@@ -256,12 +266,19 @@ mlbvh_status launch_trace_wide(const Slot* dSlots, const uint32_t* dStatus, cons
     const float4* rays = reinterpret_cast<const float4*>(dRays);
     float4* hits = reinterpret_cast<float4*>(dHits);
     const float* tris = reinterpret_cast<const float*>(dTris);
-    if (dCounts)
-        k_trace_wide<true, kQuant><<<blocks, kWideTraceThreads, 0, stream>>>(dSlots, dStatus, dNodes, dRoot, tris,
-                                                                             dLeafTris, rays, hits, nRays, dCounts);
+    const bool any = rayQuery == MLBVH_RAY_QUERY_ANY;
+    if (any && dCounts)
+        k_trace_wide<true, true, kQuant><<<blocks, kWideTraceThreads, 0, stream>>>(
+            dSlots, dStatus, dNodes, dRoot, tris, dLeafTris, rays, hits, nRays, dCounts);
+    else if (any)
+        k_trace_wide<true, false, kQuant><<<blocks, kWideTraceThreads, 0, stream>>>(
+            dSlots, dStatus, dNodes, dRoot, tris, dLeafTris, rays, hits, nRays, nullptr);
+    else if (dCounts)
+        k_trace_wide<false, true, kQuant><<<blocks, kWideTraceThreads, 0, stream>>>(
+            dSlots, dStatus, dNodes, dRoot, tris, dLeafTris, rays, hits, nRays, dCounts);
     else
-        k_trace_wide<false, kQuant><<<blocks, kWideTraceThreads, 0, stream>>>(dSlots, dStatus, dNodes, dRoot, tris,
-                                                                              dLeafTris, rays, hits, nRays, nullptr);
+        k_trace_wide<false, false, kQuant><<<blocks, kWideTraceThreads, 0, stream>>>(
+            dSlots, dStatus, dNodes, dRoot, tris, dLeafTris, rays, hits, nRays, nullptr);
     MLBVH_CHECK_LAUNCH("k_trace_wide");
     return MLBVH_OK;
 }

@@ -1129,6 +1129,29 @@ static float mul_dir(float a, float b, int up)
     if (up) return (double)f < p ? nextafterf(f, INFINITY) : f;
     return (double)f > p ? nextafterf(f, -INFINITY) : f;
 }
+/* a * b + c with one rounding, down (up != 0: up), as __fmaf_rd / __fmaf_ru
+ * (fma.rm / fma.rp): the double product of two floats is exact, TwoSum gives
+ * the exact sum as s + e, and the float nearest s is stepped once toward the
+ * rounding side if it lies beyond s + e. An exact zero sum of opposite signs
+ * is -0 when rounding down, +0 when rounding up (IEEE 754). */
+static float fma_dir(float a, float b, float c, int up)
+{
+    if (isinf(c)) return c;
+    const double p = (double)a * (double)b;
+    const double s = p + (double)c;
+    const double bb = s - p;
+    const double e = (p - (s - bb)) + ((double)c - bb);
+    if (s == 0.0 && e == 0.0)
+    {
+        if (signbit(p) && signbit(c)) return -0.0f;
+        if (!signbit(p) && !signbit(c)) return 0.0f;
+        return up ? 0.0f : -0.0f;
+    }
+    const float f = (float)s;
+    const double diff = (double)f - s; /* exact: f and s are within one float ulp (or f is infinite) */
+    if (up) return diff < e ? nextafterf(f, INFINITY) : f;
+    return diff > e ? nextafterf(f, -INFINITY) : f;
+}
 /* a / b rounded up (b = 255 here: the product q * 255 is exact in double) */
 static float div_up(float a, float b)
 {
@@ -1237,6 +1260,77 @@ static inline void slabs_offsets(orc_f3 dlo, orc_f3 dhi, orc_f3 inv, float known
     *rmax = smin(region_max, knownHitT);
 }
 
+/* The slab test of child k of a quantised slot w (csrc/wide.cu layout:
+ * base[3], scale[3], then per axis the lower and upper plane codes, then the
+ * child words), as qwide_visit (include/mlbvh_device.cuh) forms it: per axis
+ * the near plane (lower where inv > 0, upper where inv < 0) and the far plane
+ * at V inv + C, C = base inv - ro inv, near planes rounded down with ro inv
+ * rounded up, far planes rounded up with ro inv rounded down; entry = the
+ * largest near distance moved down by 2^-22 of itself, exit = the smallest far
+ * one moved up by 2^-21 of itself, then clipped to [max(0, tmin), hitT]. */
+#define ORC_Q_ENTRY_MARGIN 2.384185791015625e-07f
+#define ORC_Q_EXIT_MARGIN 4.76837158203125e-07f
+static void qwide_child(const uint32_t* w, int k, orc_f3 ro, orc_f3 inv, float tmin, float hitT, float* entry,
+                        float* exitOut)
+{
+    float base[3];
+    memcpy(base, w, 12);
+    const float r[3] = {ro.x, ro.y, ro.z}, iv[3] = {inv.x, inv.y, inv.z};
+    float en = 0.0f, ex = 0.0f;
+    for (int a = 0; a < 3; ++a)
+    {
+        const int neg = iv[a] < 0.0f;
+        const uint32_t qn = w[6 + 2 * a + neg], qf = w[6 + 2 * a + (1 - neg)];
+        const float cn = fma_dir(base[a], iv[a], -mul_dir(r[a], iv[a], 1), 0);
+        const float cf = fma_dir(base[a], iv[a], -mul_dir(r[a], iv[a], 0), 1);
+        const float tn = fma_dir(qw_value(qn, w[3 + a], k), iv[a], cn, 0);
+        const float tf = fma_dir(qw_value(qf, w[3 + a], k), iv[a], cf, 1);
+        en = a ? smax(en, tn) : tn;
+        ex = a ? smin(ex, tf) : tf;
+    }
+    *entry = smax(fma_dir(fabsf(en), -ORC_Q_ENTRY_MARGIN, en, 0), smax(0.0f, tmin));
+    *exitOut = smin(fma_dir(fabsf(ex), ORC_Q_EXIT_MARGIN, ex, 1), hitT);
+}
+
+/* Which children of wide slot `curr` pass the slab test (FP32 slots: the
+ * reference's slabs on the exact boxes; quantised slots: qwide_child), with
+ * each child's entry distance. Returns the number that pass. */
+static int wide_children(const uint32_t* wide, const uint32_t* qwide, uint32_t curr, orc_f3 ro, orc_f3 inv,
+                         float tmin, float hitT, int pass[4], float entry[4], const uint32_t** chOut)
+{
+    const uint32_t* w = qwide ? qwide + 16 * (size_t)curr : wide + 32 * (size_t)curr;
+    const uint32_t* ch = qwide ? w + 12 : w + 24;
+    int npass = 0;
+    for (int k = 0; k < 4; ++k)
+    {
+        pass[k] = 0;
+        entry[k] = 0.0f;
+        float rmin, rmax;
+        if (qwide)
+            qwide_child(w, k, ro, inv, tmin, hitT, &rmin, &rmax);
+        else
+        {
+            orc_aabb b;
+            memcpy(&b.lower.x, &w[k], 4);
+            memcpy(&b.upper.x, &w[4 + k], 4);
+            memcpy(&b.lower.y, &w[8 + k], 4);
+            memcpy(&b.upper.y, &w[12 + k], 4);
+            memcpy(&b.lower.z, &w[16 + k], 4);
+            memcpy(&b.upper.z, &w[20 + k], 4);
+            slabs(ro, inv, &b, hitT, &rmin, &rmax);
+            rmin = smax(rmin, tmin);
+        }
+        entry[k] = rmin;
+        if (ch[k] != ORC_WIDE_EMPTY && rmin <= rmax)
+        {
+            pass[k] = 1;
+            ++npass;
+        }
+    }
+    *chOut = ch;
+    return npass;
+}
+
 /* The any-hit walk over the wide tree from `start` (a wide slot or leaf
  * position; ORC_INVALID: nothing to test). leafIndex maps leaf positions to
  * triangle indices. Children whose box passes: the nearest entry first (ties
@@ -1269,46 +1363,12 @@ static void trace_wide_any(orc_hit* hit, const uint32_t* wide, const uint32_t* q
         else
         {
             (*visits)++;
-            const uint32_t* w = qwide ? qwide + 16 * (size_t)curr : wide + 32 * (size_t)curr;
-            const uint32_t* ch = qwide ? w + 12 : w + 24;
-            int best = -1, npass = 0, pass[4] = {0, 0, 0, 0};
-            float bestT = 0.0f;
+            const uint32_t* ch;
+            int pass[4], best = -1;
+            float entry[4], bestT = 0.0f;
+            const int npass = wide_children(wide, qwide, curr, ro, inv, tmin, hit->t, pass, entry, &ch);
             for (int k = 0; k < 4; ++k)
-            {
-                if (ch[k] == ORC_WIDE_EMPTY) continue;
-                float rmin, rmax;
-                if (qwide)
-                {
-                    float base[3];
-                    memcpy(base, w, 12);
-                    const float r[3] = {ro.x, ro.y, ro.z};
-                    float dl[3], dh[3];
-                    for (int a = 0; a < 3; ++a)
-                    {
-                        dl[a] = add_dir(add_dir(base[a], -r[a], 0), qw_value(w[6 + 2 * a], w[3 + a], k), 0);
-                        dh[a] = add_dir(add_dir(base[a], -r[a], 1), qw_value(w[7 + 2 * a], w[3 + a], k), 1);
-                    }
-                    slabs_offsets(f3(dl[0], dl[1], dl[2]), f3(dh[0], dh[1], dh[2]), inv, hit->t, &rmin, &rmax);
-                }
-                else
-                {
-                    orc_aabb b;
-                    memcpy(&b.lower.x, &w[k], 4);
-                    memcpy(&b.upper.x, &w[4 + k], 4);
-                    memcpy(&b.lower.y, &w[8 + k], 4);
-                    memcpy(&b.upper.y, &w[12 + k], 4);
-                    memcpy(&b.lower.z, &w[16 + k], 4);
-                    memcpy(&b.upper.z, &w[20 + k], 4);
-                    slabs(ro, inv, &b, hit->t, &rmin, &rmax);
-                }
-                rmin = smax(rmin, tmin);
-                if (rmin <= rmax)
-                {
-                    pass[k] = 1;
-                    ++npass;
-                    if (best < 0 || rmin < bestT) { best = k; bestT = rmin; }
-                }
-            }
+                if (pass[k] && (best < 0 || entry[k] < bestT)) { best = k; bestT = entry[k]; }
             if (best >= 0)
             {
                 if (top + npass - 1 > ORC_WIDE_DEPTH)
@@ -1325,6 +1385,90 @@ static void trace_wide_any(orc_hit* hit, const uint32_t* wide, const uint32_t* q
         }
         if (top == 0) return;
         curr = stack[--top];
+    }
+}
+
+/* The closest-hit walk over the wide tree (wide_closest_step,
+ * include/mlbvh_device.cuh): at a slot the passing children in the order of
+ * their sort keys (entry bits with the two lowest replaced by the slot), the
+ * nearest entered, the others pushed farthest first with their key's
+ * distance; a popped child is entered only if that distance is <= hit.t;
+ * every triangle hit at t <= hit.t replaces the hit (quantised slots: only if
+ * the leaf's exact box passes too); a visit whose pushes would overflow
+ * ORC_WIDE_DEPTH entries continues with the closest-hit stack-free walk from
+ * binaryRoot, keeping the hit. */
+static uint32_t wide_sort_key(int pass, float entry, int k)
+{
+    uint32_t u;
+    memcpy(&u, &entry, 4);
+    return pass ? ((u & 0x7FFFFFFCu) | (uint32_t)k) : 0xFFFFFFFFu;
+}
+static void trace_wide_closest(orc_hit* hit, const uint32_t* wide, const uint32_t* qwide, const orc_node* nodes,
+                               const orc_triangle* tris, const uint32_t* leafIndex, uint32_t start,
+                               uint32_t binaryRoot, orc_f3 ro, orc_f3 rd, orc_f3 inv, float tmin, uint32_t* visits,
+                               uint32_t* tests, uint32_t* restarts)
+{
+    uint32_t stackNode[ORC_WIDE_DEPTH], stackKey[ORC_WIDE_DEPTH];
+    int top = 0;
+    uint32_t curr = start;
+    if (start == ORC_INVALID) return;
+    for (;;)
+    {
+        int descend = 0;
+        if (is_leaf(curr))
+        {
+            const orc_triangle* tri = &tris[leafIndex[idx_of(curr)]];
+            orc_hit probe = *hit;
+            int h;
+            leaf_test(&probe, tris, ORC_LEAF_BIT | leafIndex[idx_of(curr)], ro, rd, tmin, &h, tests);
+            if (h && (!qwide || leaf_box_passes(ro, inv, tri->v, tmin, hit->t))) *hit = probe;
+        }
+        else
+        {
+            (*visits)++;
+            const uint32_t* ch;
+            int pass[4];
+            float entry[4];
+            const int npass = wide_children(wide, qwide, curr, ro, inv, tmin, hit->t, pass, entry, &ch);
+            if (npass > 0)
+            {
+                if (top + npass - 1 > ORC_WIDE_DEPTH)
+                {
+                    (*restarts)++;
+                    stackfree_walk(hit, nodes, tris, binaryRoot, ORC_INVALID, ro, rd, inv, tmin, 0, visits, tests);
+                    return;
+                }
+                uint32_t key[4];
+                for (int k = 0; k < 4; ++k) key[k] = wide_sort_key(pass[k], entry[k], k);
+                for (int i = 1; i < 4; ++i) /* insertion sort, ascending */
+                    for (int j = i; j > 0 && key[j] < key[j - 1]; --j)
+                    {
+                        uint32_t x = key[j];
+                        key[j] = key[j - 1];
+                        key[j - 1] = x;
+                    }
+                for (int r = npass - 1; r >= 1; --r)
+                {
+                    stackNode[top] = ch[key[r] & 3u];
+                    stackKey[top++] = key[r] & 0x7FFFFFFCu;
+                }
+                curr = ch[key[0] & 3u];
+                descend = 1;
+            }
+        }
+        if (descend) continue;
+        for (;;)
+        {
+            if (top == 0) return;
+            --top;
+            float d;
+            memcpy(&d, &stackKey[top], 4);
+            if (d <= hit->t)
+            {
+                curr = stackNode[top];
+                break;
+            }
+        }
     }
 }
 
@@ -1350,6 +1494,7 @@ typedef struct {
     const orc_ray* rays;
     orc_hit* hits;
     uint32_t *visits, *tests, *restarts;
+    int any; /* any-hit (1) or closest-hit (0) rays */
 } wide_ctx;
 
 static void wide_range(void* p, uint32_t b, uint32_t e)
@@ -1365,10 +1510,14 @@ static void wide_range(void* p, uint32_t b, uint32_t e)
         uint32_t nv = 0, nt = 0, nr = 0;
         uint32_t start = is_leaf(c->root) ? ORC_LEAF_BIT : c->root;
         if (c->fallback)
-            stackfree_walk(&hit, c->nodes, c->tris, c->root, ORC_INVALID, ro, rd, inv_rd(rd), r->tmin, 1, &nv, &nt);
-        else
+            stackfree_walk(&hit, c->nodes, c->tris, c->root, ORC_INVALID, ro, rd, inv_rd(rd), r->tmin, c->any, &nv,
+                           &nt);
+        else if (c->any)
             trace_wide_any(&hit, c->wide, c->qwide, c->nodes, c->tris, c->leafIndex, start, c->root, ro, rd,
                            inv_rd(rd), r->tmin, &nv, &nt, &nr);
+        else
+            trace_wide_closest(&hit, c->wide, c->qwide, c->nodes, c->tris, c->leafIndex, start, c->root, ro, rd,
+                               inv_rd(rd), r->tmin, &nv, &nt, &nr);
         c->hits[i] = hit;
         if (c->visits) c->visits[i] = nv;
         if (c->tests) c->tests[i] = nt;
@@ -1378,22 +1527,23 @@ static void wide_range(void* p, uint32_t b, uint32_t e)
 
 void orc_trace_wide(const uint32_t* wide, const orc_node* nodes, const orc_triangle* tris, uint32_t n, uint32_t root,
                     const orc_ray* rays, uint32_t nRays, orc_hit* hits, uint32_t* visits, uint32_t* tests,
-                    uint32_t* restarts)
+                    uint32_t* restarts, int query)
 {
     uint32_t* leafIndex = (uint32_t*)malloc(sizeof(uint32_t) * (n ? n : 1));
     leaf_positions(nodes, n, root, leafIndex);
-    wide_ctx c = {wide, NULL, 0, nodes, tris, leafIndex, root, rays, hits, visits, tests, restarts};
+    wide_ctx c = {wide, NULL, 0, nodes, tris, leafIndex, root, rays, hits, visits, tests, restarts, query != 0};
     orc_parallel_for(nRays, 1024, wide_range, &c);
     free(leafIndex);
 }
 
 void orc_trace_wide_quantised(const uint32_t* qwide, int fallback, const orc_node* nodes, const orc_triangle* tris,
                               uint32_t n, uint32_t root, const orc_ray* rays, uint32_t nRays, orc_hit* hits,
-                              uint32_t* visits, uint32_t* tests, uint32_t* restarts)
+                              uint32_t* visits, uint32_t* tests, uint32_t* restarts, int query)
 {
     uint32_t* leafIndex = (uint32_t*)malloc(sizeof(uint32_t) * (n ? n : 1));
     leaf_positions(nodes, n, root, leafIndex);
-    wide_ctx c = {NULL, qwide, fallback, nodes, tris, leafIndex, root, rays, hits, visits, tests, restarts};
+    wide_ctx c = {NULL, qwide, fallback, nodes, tris, leafIndex, root, rays, hits, visits, tests, restarts,
+                  query != 0};
     orc_parallel_for(nRays, 1024, wide_range, &c);
     free(leafIndex);
 }

@@ -105,13 +105,14 @@ void orc_trace_replay(const orc_node* nodes, const orc_triangle* tris, uint32_t 
                       uint32_t nRays, int query, int depth, orc_hit* hits, uint32_t* nodeVisits, uint32_t* triTests);
 
 /* The 4-wide tree (no reference counterpart; csrc/wide.cu): 32 words per
- * slot, n - 1 slots. orc_trace_wide: any-hit rays over it (restarting with
- * the stack-free walk where its 24-entry stack would overflow); per ray the
- * wide-node (then binary-node) visits, triangle tests and restarts. */
+ * slot, n - 1 slots. orc_trace_wide: any-hit (query 1) or closest-hit
+ * (query 0) rays over it (restarting with the stack-free walk where its
+ * 24-entry stack would overflow); per ray the wide-node (then binary-node)
+ * visits, triangle tests and restarts. */
 void orc_build_wide(const orc_node* nodes, uint32_t n, uint32_t* out);
 void orc_trace_wide(const uint32_t* wide, const orc_node* nodes, const orc_triangle* tris, uint32_t n, uint32_t root,
                     const orc_ray* rays, uint32_t nRays, orc_hit* hits, uint32_t* visits, uint32_t* tests,
-                    uint32_t* restarts);
+                    uint32_t* restarts, int query);
 /* Quantised slots (16 words each; csrc/wide.cu): returns 1 when every slot
  * was quantised. orc_trace_wide_quantised walks them (a hit counts only where
  * the triangle's exact box passes too); fallback != 0: the stack-free walk
@@ -119,7 +120,7 @@ void orc_trace_wide(const uint32_t* wide, const orc_node* nodes, const orc_trian
 int orc_quantise_wide(const uint32_t* wide, uint32_t n, uint32_t* out);
 void orc_trace_wide_quantised(const uint32_t* qwide, int fallback, const orc_node* nodes, const orc_triangle* tris,
                               uint32_t n, uint32_t root, const orc_ray* rays, uint32_t nRays, orc_hit* hits,
-                              uint32_t* visits, uint32_t* tests, uint32_t* restarts);
+                              uint32_t* visits, uint32_t* tests, uint32_t* restarts, int query);
 
 /* Camera (camera.h:10-31) */
 void orc_lookat(orc_f3 eye, orc_f3 center, orc_f3 up, float fovy, int w, int h, orc_camera* cam);

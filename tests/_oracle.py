@@ -65,9 +65,10 @@ def oracle() -> ctypes.CDLL:
             "orc_trace": (None, [_vp, _vp, _u32, _vp, _u32, _i32, _i32, _vp, _vp, _vp]),
             "orc_trace_replay": (None, [_vp, _vp, _u32, _vp, _u32, _i32, _i32, _vp, _vp, _vp]),
             "orc_build_wide": (None, [_vp, _u32, _vp]),
-            "orc_trace_wide": (None, [_vp, _vp, _vp, _u32, _u32, _vp, _u32, _vp, _vp, _vp, _vp]),
+            "orc_trace_wide": (None, [_vp, _vp, _vp, _u32, _u32, _vp, _u32, _vp, _vp, _vp, _vp, _i32]),
             "orc_quantise_wide": (_i32, [_vp, _u32, _vp]),
-            "orc_trace_wide_quantised": (None, [_vp, _i32, _vp, _vp, _u32, _u32, _vp, _u32, _vp, _vp, _vp, _vp]),
+            "orc_trace_wide_quantised": (None, [_vp, _i32, _vp, _vp, _u32, _u32, _vp, _u32, _vp, _vp, _vp, _vp,
+                                                _i32]),
             "orc_lookat": (None, [F3, F3, F3, _f32, _i32, _i32, _vp]),
             "orc_sobol": (None, [_u32, _u32, _u32, _u32, _vp, _vp]),
             "orc_hash_pcg": (_u32, [_u32]),
@@ -218,9 +219,9 @@ def build_wide(nodes, n):
     return out
 
 
-def trace_wide(wide, nodes, tris, root, rays):
-    """Any-hit rays over the 4-wide tree: hits and per-ray (visits, tests,
-    restarts)."""
+def trace_wide(wide, nodes, tris, root, rays, query=1):
+    """Rays over the 4-wide tree (query 1 any-hit, 0 closest-hit): hits and
+    per-ray (visits, tests, restarts)."""
     rays = np.ascontiguousarray(rays, np.float32).reshape(-1, 8)
     tris = np.ascontiguousarray(tris, np.float32).reshape(-1, 9)
     n, m = len(tris), rays.shape[0]
@@ -228,7 +229,8 @@ def trace_wide(wide, nodes, tris, root, rays):
     nv, nt, nr = (np.zeros(m, np.uint32) for _ in range(3))
     wide_c = np.ascontiguousarray(wide, np.uint32) if len(wide) else np.zeros((1, 32), np.uint32)
     nodes_c = np.ascontiguousarray(nodes, np.uint32) if len(nodes) else np.zeros((1, 16), np.uint32)
-    oracle().orc_trace_wide(P(wide_c), P(nodes_c), P(tris), n, root, P(rays), m, P(hits), P(nv), P(nt), P(nr))
+    oracle().orc_trace_wide(P(wide_c), P(nodes_c), P(tris), n, root, P(rays), m, P(hits), P(nv), P(nt), P(nr),
+                            query)
     return hits, nv, nt, nr
 
 
@@ -241,8 +243,9 @@ def quantise_wide(wide, n):
     return out, bool(ok)
 
 
-def trace_wide_quantised(qwide, nodes, tris, root, rays, fallback=False):
-    """Any-hit rays over quantised wide slots: hits, visits, tests, restarts."""
+def trace_wide_quantised(qwide, nodes, tris, root, rays, fallback=False, query=1):
+    """Rays over quantised wide slots (query 1 any-hit, 0 closest-hit): hits,
+    visits, tests, restarts."""
     rays = np.ascontiguousarray(rays, np.float32).reshape(-1, 8)
     tris = np.ascontiguousarray(tris, np.float32).reshape(-1, 9)
     n, m = len(tris), rays.shape[0]
@@ -251,7 +254,7 @@ def trace_wide_quantised(qwide, nodes, tris, root, rays, fallback=False):
     q_c = np.ascontiguousarray(qwide, np.uint32) if len(qwide) else np.zeros((1, 16), np.uint32)
     nodes_c = np.ascontiguousarray(nodes, np.uint32) if len(nodes) else np.zeros((1, 16), np.uint32)
     oracle().orc_trace_wide_quantised(P(q_c), int(fallback), P(nodes_c), P(tris), n, root, P(rays), m, P(hits),
-                                      P(nv), P(nt), P(nr))
+                                      P(nv), P(nt), P(nr), query)
     return hits, nv, nt, nr
 
 

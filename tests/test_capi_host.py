@@ -171,8 +171,8 @@ def test_wide_entry_points_reject_bad_arguments():
     assert L.mlbvh_build_wide(p, p, 1, None, None) == 0  # one triangle: no slots, nothing to do
     assert L.mlbvh_build_wide(p, p, 10, odd, None) == 1  # wide nodes must be 128-byte aligned
     assert b"aligned" in L.mlbvh_last_error_string()
-    assert L.mlbvh_trace_wide(p, p, p, p, p, p, p, 4, 0, None, None) == 1  # closest hit: not on this tree
-    assert b"any-hit" in L.mlbvh_last_error_string()
+    assert L.mlbvh_trace_wide(p, p, p, p, p, p, p, 4, 2, None, None) == 1  # no such query
+    assert b"rayQuery" in L.mlbvh_last_error_string()
     assert L.mlbvh_trace_wide(odd, p, p, p, p, p, p, 4, 1, None, None) == 1
     assert L.mlbvh_trace_wide(p, p, p, p, p, p, p, 0, 1, None, None) == 0  # nothing to do
     cam = (ctypes.c_float * 9)()
@@ -183,7 +183,7 @@ def test_wide_entry_points_reject_bad_arguments():
     # quantised wide slots
     assert L.mlbvh_quantise_wide(p, 10, p, None, None) == 1  # no status word
     assert L.mlbvh_quantise_wide(p, 0, p, p, None) == 1      # no triangles
-    assert L.mlbvh_trace_wide_quantised(p, p, p, p, p, p, p, p, 4, 0, None, None) == 1  # closest hit
+    assert L.mlbvh_trace_wide_quantised(p, p, p, p, p, p, p, p, 4, 2, None, None) == 1  # no such query
     assert L.mlbvh_trace_wide_quantised(p, None, p, p, p, p, p, p, 4, 1, None, None) == 1  # no status word
     assert L.mlbvh_trace_wide_quantised(ctypes.c_void_p(256 + 16), p, p, p, p, p, p, p, 4, 1, None, None) == 1
     assert L.mlbvh_render_ao_wide_quantised(p, None, 8, 8, ctypes.addressof(cam), p, p, p, p, None, p, 1, 16, 1.0, 1,

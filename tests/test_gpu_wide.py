@@ -1,8 +1,9 @@
 """GPU parity of the 4-wide tree (mlbvh_build_wide, mlbvh_trace_wide,
 mlbvh_render_ao_wide; no reference counterpart). Every slot must equal the
-oracle's regrouping bit for bit; any-hit rays must return the oracle's wide
-walk Hit records and counts exactly, and hit exactly when the stack-free
-walk (pinned to the reference's intersect_stackfree) does; AO over the wide
+oracle's regrouping bit for bit; any-hit and closest-hit rays must return the
+oracle's wide walk Hit records and counts exactly; any-hit rays hit exactly
+when the stack-free walk (pinned to the reference's intersect_stackfree)
+does, and closest-hit rays report its Hit records; AO over the wide
 tree must give every pixel's occlusion count of mlbvh_render_ao."""
 import numpy as np
 import pytest
@@ -92,6 +93,65 @@ def test_trace_wide_restarts_on_stack_overflow(cuda):
     np.testing.assert_array_equal(hits, ref)
     np.testing.assert_array_equal(c[2], nr)
     assert nr.sum() > 0
+
+
+@pytest.mark.parametrize("quantised", [False, True])
+def test_trace_wide_closest_matches_oracle(wcase, quantised):
+    """Closest-hit rays over the FP32 and the quantised slots: the oracle's
+    wide walk Hit records and counts exactly, and the stack-free walk's Hit
+    records (on duplicated triangles, where copies give bit-identical t, the
+    walk order picks which copy reports)."""
+    import torch
+    name, tris, b, t, out, w, rays = wcase
+    if quantised:
+        w.quantise()
+    counts = torch.zeros(3 * len(rays), dtype=torch.int32, device="cuda")
+    hits = G.host(mb.intersect_wide(w, G.dev(rays), counts=counts, quantised=quantised,
+                                    rayQuery=mb.RAY_QUERY_CLOSEST), np.uint32)
+    c = G.host(counts, np.uint32).reshape(3, -1)
+    wide = O.build_wide(out["nodes"], len(tris))
+    if quantised:
+        q, _ = O.quantise_wide(wide, len(tris))
+        ref, nv, nt, nr = O.trace_wide_quantised(q, out["nodes"], tris, out["root"], rays, query=0)
+    else:
+        ref, nv, nt, nr = O.trace_wide(wide, out["nodes"], tris, out["root"], rays, query=0)
+    np.testing.assert_array_equal(hits, ref)
+    np.testing.assert_array_equal(c[0], nv)
+    np.testing.assert_array_equal(c[1], nt)
+    np.testing.assert_array_equal(c[2], nr)
+    plain = G.trace(b, t, rays, mb.RAY_QUERY_CLOSEST)
+    if name == "duplicates":
+        np.testing.assert_array_equal(hits[:, [0, 2, 3, 4, 5, 6]], plain[:, [0, 2, 3, 4, 5, 6]])
+    else:
+        np.testing.assert_array_equal(hits, plain)
+
+
+def test_trace_wide_closest_restarts_on_stack_overflow(cuda):
+    """400 nested copies of a triangle and rays parallel to their plane from
+    outside the smallest ones: the closest-hit walk's stack overflows and the
+    ray restarts with the stack-free walk (the oracle's hits and counts, the
+    stack-free walk's hits), on FP32 and quantised slots."""
+    import torch
+    from test_oracle_walks import nested_triangles
+    tris, rays = nested_triangles()
+    b, t, out = G.build(tris)
+    w = mb.WideBVH.from_builder(b, t).quantise()
+    wide = O.build_wide(out["nodes"], len(tris))
+    plain = G.trace(b, t, rays, mb.RAY_QUERY_CLOSEST)
+    for quantised in (False, True):
+        counts = torch.zeros(3 * len(rays), dtype=torch.int32, device="cuda")
+        hits = G.host(mb.intersect_wide(w, G.dev(rays), counts=counts, quantised=quantised,
+                                        rayQuery=mb.RAY_QUERY_CLOSEST), np.uint32)
+        c = G.host(counts, np.uint32).reshape(3, -1)
+        if quantised:
+            ref, nv, nt, nr = O.trace_wide_quantised(O.quantise_wide(wide, len(tris))[0], out["nodes"], tris,
+                                                     out["root"], rays, query=0)
+        else:
+            ref, nv, nt, nr = O.trace_wide(wide, out["nodes"], tris, out["root"], rays, query=0)
+        np.testing.assert_array_equal(hits, ref)
+        np.testing.assert_array_equal(c, np.stack([nv, nt, nr]))
+        np.testing.assert_array_equal(hits, plain)
+        assert nr.sum() > 0
 
 
 def _ao(fn, w, h, ns, radius, sobol, *args):

@@ -234,6 +234,86 @@ def test_quantised_wide_any_hit_equals_stackfree(case):
         assert nv.sum() >= nv32.sum() and nv.sum() < 1.3 * nv32.sum()
 
 
+def _closest_equal(got, ref, tris, name):
+    """Closest hits: every Hit word equal, except that where duplicated
+    triangles give bit-identical t the walk order picks which one reports
+    (then t, uv and the normal are equal and the triangle is a copy)."""
+    if name != "duplicates":
+        np.testing.assert_array_equal(got, ref)
+        return
+    np.testing.assert_array_equal(got[:, [0, 2, 3, 4, 5, 6]], ref[:, [0, 2, 3, 4, 5, 6]])
+    hit = got[:, 7] != MISS
+    np.testing.assert_array_equal(tris[got[hit, 7]], tris[ref[hit, 7]])
+
+
+def test_wide_closest_hit_equals_stackfree(case):
+    """Closest-hit rays over the wide tree report intersect_stackfree's Hit
+    records, with fewer node visits."""
+    name, tris, b, _, rays = case
+    wide = O.build_wide(b["nodes"], len(tris))
+    got, nv, nt, nr = O.trace_wide(wide, b["nodes"], tris, b["root"], rays, query=0)
+    ref, nv0, _ = O.trace(b["nodes"], tris, b["root"], rays, 0, 0, counters=True)
+    _closest_equal(got, ref, tris, name)
+    if name != "duplicates":
+        assert nv.sum() < 0.7 * nv0.sum()
+
+
+def test_quantised_wide_closest_hit_equals_stackfree(case):
+    """The same over the quantised slots (a hit counts only where the
+    triangle's exact box passes too): the FP32 walk's Hit records, at most a
+    few more visits."""
+    name, tris, b, _, rays = case
+    n = len(tris)
+    wide = O.build_wide(b["nodes"], n)
+    q, _ = O.quantise_wide(wide, n)
+    got, nv, nt, nr = O.trace_wide_quantised(q, b["nodes"], tris, b["root"], rays, query=0)
+    ref = O.trace(b["nodes"], tris, b["root"], rays, 0, 0)
+    _closest_equal(got, ref, tris, name)
+    _, nv32, _, _ = O.trace_wide(wide, b["nodes"], tris, b["root"], rays, query=0)
+    if name != "duplicates":
+        assert nv.sum() >= nv32.sum() and nv.sum() < 1.3 * nv32.sum()
+
+
+def nested_triangles():
+    """400 scaled copies of one triangle about its centroid, growing with the
+    index (one Morton key: a chain), and 64 rays parallel to their plane just
+    above it from outside the smallest copies: every box passes, the nearest
+    child of each slot is the internal one (the union of the larger copies),
+    and no triangle is hit."""
+    base = scenes.gaussian_soup(3, seed=6)
+    v = base[0].reshape(3, 3).astype(np.float64)
+    c = v.mean(0)
+    nrm = np.cross(v[1] - v[0], v[2] - v[1])
+    nrm /= np.linalg.norm(nrm)
+    tris = np.array([(c + s * (v - c)).reshape(9) for s in np.linspace(0.2, 2.0, 400)], np.float32)
+    rng = np.random.default_rng(3)
+    rays = np.zeros((64, 8), np.float32)
+    for i in range(64):
+        d = np.cross(nrm, rng.standard_normal(3))
+        d /= np.linalg.norm(d)
+        rays[i, 0:3] = c + nrm * 1e-5 - d * 0.1
+        rays[i, 4:7] = d
+        rays[i, 7] = 0.3
+    return tris, rays
+
+
+def test_wide_closest_stack_overflow_restarts_with_stackfree_walk():
+    """The closest-hit walk enters the nearest child and pushes the others:
+    on nested_triangles() that overflows the wide stack, the walk restarts
+    with the stack-free walk and still reports the stack-free walk's hits."""
+    tris, rays = nested_triangles()
+    b = O.build(tris)
+    wide = O.build_wide(b["nodes"], len(tris))
+    for q in (None, O.quantise_wide(wide, len(tris))[0]):
+        if q is None:
+            got, nv, nt, nr = O.trace_wide(wide, b["nodes"], tris, b["root"], rays, query=0)
+        else:
+            got, nv, nt, nr = O.trace_wide_quantised(q, b["nodes"], tris, b["root"], rays, query=0)
+        ref = O.trace(b["nodes"], tris, b["root"], rays, 0, 0)
+        np.testing.assert_array_equal(got, ref)
+        assert nr.sum() > 0
+
+
 def test_quantised_wide_fallback_for_huge_extents():
     """Coordinates spread over about 1e37 cannot be quantised (codes beyond
     8 bits at every scale up to 2^127): the slots are flagged and every ray
