@@ -752,6 +752,32 @@ def bench_ploc(args, wl, d_tris, n, cam, w, h, dev, stream, barrier, max_over_ra
     cam_out["vs_lbvh"] = cam_out["ploc_mrays_s"] / cam_out["lbvh_mrays_s"]
     cam_out["t_equal"] = float((hits["lbvh"][:, 0] == hits["ploc"][:, 0]).float().mean().item())
     cam_out["triangle_equal"] = float((hits["lbvh"][:, 7] == hits["ploc"][:, 7]).float().mean().item())
+    # the same rays on the closest-hit walk over each tree's 4-wide regrouping
+    # (leaf-ordered triangles: neighbouring leaves share cache lines), with
+    # the walk's per-ray wide-node visits and triangle tests
+    lbvh_wide = mb.WideBVH.from_builder(lbvh, d_tris)
+    launches += 2
+    for name, wt in (("lbvh", lbvh_wide), ("ploc", wide)):
+        hw = torch.empty((nr, 8), dtype=torch.int32, device=dev)
+        cnt = torch.zeros(3 * nr, dtype=torch.int32, device=dev)
+        mb.intersect_wide(wt, rays, hits=hw, counts=cnt, rayQuery=mb.RAY_QUERY_CLOSEST)
+        for _ in range(args.warmup):
+            mb.intersect_wide(wt, rays, hits=hw, rayQuery=mb.RAY_QUERY_CLOSEST)
+        cev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+        torch.cuda.synchronize()
+        cev[0].record(stream)
+        for _ in range(args.steps):
+            mb.intersect_wide(wt, rays, hits=hw, rayQuery=mb.RAY_QUERY_CLOSEST)
+        cev[1].record(stream)
+        torch.cuda.synchronize()
+        t = max_over_ranks(cev[0].elapsed_time(cev[1]) / 1e3) / args.steps
+        launches += 1 + args.warmup + args.steps
+        c = cnt.cpu().numpy().astype(np.int64)
+        cam_out[name + "_wide_mrays_s"] = nr / t / 1e6
+        cam_out[name + "_wide_node_visits_per_ray"] = c[:nr].sum() / nr
+        cam_out[name + "_wide_tri_tests_per_ray"] = c[nr:2 * nr].sum() / nr
+        cam_out[name + "_wide_t_equal_replay"] = float((hw[:, 0] == hits[name][:, 0]).float().mean().item())
+    cam_out["wide_vs_lbvh"] = cam_out["ploc_wide_mrays_s"] / cam_out["lbvh_wide_mrays_s"]
     out["camera_rays_closest"] = cam_out
     out["launches"] = launches
     out["note"] = ("PLOC: parallel locally-ordered clustering over the LBVH's Morton order, in-order node numbering "
@@ -909,6 +935,109 @@ def run_reference(args, wl, rank):
     print(json.dumps(line), flush=True)
 
 
+PROFILE_CASES = ("build", "ao_rays", "ao_rays_wide", "ao_rays_wide_quantised", "trace_wide_closest",
+                 "camera_replay_lbvh", "camera_replay_ploc", "batch_trace", "pt", "adjoint")
+
+
+def profile_case(name, dev):
+    """One small case of one kernel for an ncu capture: the set-up, then the
+    kernel's launch chain twice (capture the second launch: ncu -s 1 -c 1 -k
+    <kernel>), with the inputs larger than L2 and a few GB on the device at
+    most. No timing; prints what ran.
+      build                   4M-triangle soup: the build chain (k_scene_bounds,
+                              k_keys, 4 x sort::k_onesweep, k_build)
+      ao_rays                 4M soup, one 1920x1080 AO frame (64 rays of
+                              radius 0.1): k_ao_primary, k_ao_rays, k_ao_finish
+      ao_rays_wide(_quantised) the same frame over the 4-wide tree (its
+                              8-bit slots)
+      trace_wide_closest      4M soup, 1M camera rays closest-hit over the
+                              quantised 4-wide slots (k_trace_wide)
+      camera_replay_lbvh/_ploc 4M soup, the same camera rays closest-hit on the
+                              replay walk (k_trace) over the LBVH / the PLOC tree
+      batch_trace             48 meshes of the batched workload (64..262,144
+                              triangles, 4,096..1M rays each): k_batch_trace
+      pt                      heightfield + icospheres, one 512x512 path-tracing
+                              pass (k_pt, stack-free walk)
+      adjoint                 the differentiation workload (512x512, 64 spp, 3
+                              bounces): k_pt_diff_render, k_pt_diff_adjoint"""
+    import torch
+    import minimumlbvh_b200 as mb
+    from minimumlbvh_b200 import scenes
+    if name in ("build", "ao_rays", "ao_rays_wide", "ao_rays_wide_quantised", "trace_wide_closest",
+                "camera_replay_lbvh", "camera_replay_ploc"):
+        wl = WORKLOADS["soup4m_ao64"]
+        tris, (eye, c, up, fovy) = make_scene(wl)
+        n, w, h = len(tris), wl["w"], wl["h"]
+        d_tris = torch.from_numpy(tris).to(dev)
+        b = mb.BVHGPUBuilder()
+        sorter = mb.OnesweepSort(dev.index)
+        cam = mb.RayGenerator().lookat(eye, c, up, fovy, w, h)
+        if name == "camera_replay_ploc":
+            b.buildByPLOC(d_tris, n, 0, sorter, 8)
+        else:
+            b.build(d_tris, n, 0, sorter)
+        b.status()
+        px = torch.zeros(w * h, dtype=torch.int32, device=dev)
+        wide = None
+        if name.startswith("ao_rays_wide") or name == "trace_wide_closest":
+            wide = mb.WideBVH.from_builder(b, d_tris).quantise()
+        rays = None
+        if name == "trace_wide_closest" or name.startswith("camera_replay"):
+            rays = torch.from_numpy(scenes.camera_rays(cam.m_origin, cam.m_right, cam.m_up, w, h, 2)).to(dev)
+        for _ in range(2):
+            if name == "build":
+                b.build(d_tris, n, 0, sorter)
+            elif name == "ao_rays":
+                mb.render_ao(px, (w, h), cam, b.m_rootNode, b.m_internals, d_tris, 1, wl["ns"], wl["radius"], 12345)
+            elif name == "trace_wide_closest":
+                mb.intersect_wide(wide, rays, quantised=True, rayQuery=mb.RAY_QUERY_CLOSEST)
+            elif name.startswith("camera_replay"):
+                mb.intersect(b, d_tris, rays, traversal=mb.TRAVERSAL_REPLAY)
+            else:
+                mb.render_ao_wide(px, (w, h), cam, wide, 1, wl["ns"], wl["radius"], 12345,
+                                  quantised=name.endswith("quantised"))
+        b.status()
+    elif name == "batch_trace":
+        tris, offsets = scenes.batched_soup(48, 64, 262_144, seed=7, device=dev)
+        rays, roff = scenes.batched_rays(tris, offsets, 4096, 1_048_576, seed=8)
+        bb = mb.BatchedBVH(tris, torch.as_tensor(offsets.astype(np.int32), device=dev), len(offsets) - 1)
+        bb.set_rays(rays, torch.as_tensor(roff.astype(np.int32), device=dev))
+        bb.build()
+        for _ in range(2):
+            bb.trace()
+        bb.status()
+        n = int(offsets[-1])
+    elif name == "pt":
+        tris = scenes.heightfield_icospheres()
+        n = len(tris)
+        t = torch.from_numpy(tris).to(dev)
+        at = torch.from_numpy(scenes.pt_attributes(n)).to(dev)
+        b = mb.BVHGPUBuilder().build(t, n, 0, mb.OnesweepSort(dev.index))
+        eye, c, up, fovy = scenes.camera_heightfield()
+        cam = mb.RayGenerator().lookat(eye, c, up, fovy, 512, 512)
+        acc = torch.zeros(512 * 512 * 4, dtype=torch.float32, device=dev)
+        for _ in range(2):
+            mb.render_pt(acc, (512, 512), cam, b.m_rootNode, b.m_internals, t, at)
+        b.status()
+    elif name == "adjoint":
+        tris, alb, em = scenes.diff_scene()
+        n = len(tris)
+        t = torch.from_numpy(tris).to(dev)
+        b = mb.BVHGPUBuilder().build(t, n, 0, mb.OnesweepSort(dev.index))
+        eye, c, up, fovy = scenes.camera_heightfield()
+        cam = mb.RayGenerator().lookat(eye, c, up, fovy, 512, 512)
+        a = torch.from_numpy(alb).to(dev)
+        e = torch.from_numpy(em).to(dev)
+        img = torch.empty(512 * 512, dtype=torch.float32, device=dev)
+        grad = torch.zeros(n, dtype=torch.float32, device=dev)
+        for _ in range(2):
+            mb.pt_diff_render(img, (512, 512), cam, b, t, a, e, 64, 3)
+            mb.pt_diff_adjoint(grad, img, (512, 512), cam, b, t, a, e, 64, 3)
+        b.status()
+    torch.cuda.synchronize()
+    print(json.dumps({"profile_case": name, "triangles": n, "device_bytes": torch.cuda.max_memory_allocated(dev)}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -927,7 +1056,14 @@ def main():
     ap.add_argument("--no-diff", action="store_true", help="skip the differentiable path-tracing section")
     ap.add_argument("--no-reference-gpu", action="store_true",
                     help="skip the baseline leg running the reference's own GPU kernels")
+    ap.add_argument("--profile-case", choices=PROFILE_CASES, default=None,
+                    help="run one small case of one kernel for an ncu capture (no timing) and exit")
     args = ap.parse_args()
+    if args.profile_case:
+        import torch
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+        profile_case(args.profile_case, torch.device("cuda", torch.cuda.current_device()))
+        return
     wl = dict(WORKLOADS[args.workload])
     if args.image:
         wl["w"], wl["h"] = (int(v) for v in args.image.lower().split("x"))
