@@ -1220,14 +1220,18 @@ def main():
         bev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
         barrier()
         torch.cuda.synchronize()
+        cbev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+                for _ in range(args.steps)]
         for i in range(args.steps):
             if flush is not None:
                 flush.zero_()
             bev[i][0].record(stream)
+            mb.profile_events(*cbev[i])  # around the agglomerative climb (k_build)
             builder.build(d_tris, n, 0, sorter)
             bev[i][1].record(stream)
         torch.cuda.synchronize()
         barrier()
+        climb_ms = float(np.mean([a.elapsed_time(b) for a, b in cbev]))
         build_ms = [a.elapsed_time(b) for a, b in bev]
         build_total_s = max_over_ranks(sum(build_ms) / 1e3)
         builder.status()
@@ -1357,7 +1361,7 @@ def main():
                         "node_visits_per_ray": visits / rays_per_frame, "tri_tests_per_ray": tests / rays_per_frame,
                         "kernel_bytes": kernel_bytes}
     build_s = build_total_s / args.steps
-    line["build"] = {"ms": build_s * 1e3, "mtri_s": n * world / build_s / 1e6,
+    line["build"] = {"ms": build_s * 1e3, "climb_ms": climb_ms, "mtri_s": n * world / build_s / 1e6,
                      "achieved_gbs": n * BUILD_BYTES_PER_TRI / build_s / 1e9,
                      "frac": n * BUILD_BYTES_PER_TRI / build_s / 1e9 / peak, "bytes_per_tri": BUILD_BYTES_PER_TRI}
     line["e2e"] = {"value": rays_per_frame * args.steps * world / e2e_s / 1e6, "unit": "Mrays/s",
