@@ -1152,6 +1152,9 @@ static float fma_dir(float a, float b, float c, int up)
     if (up) return diff < e ? nextafterf(f, INFINITY) : f;
     return diff > e ? nextafterf(f, -INFINITY) : f;
 }
+/* Test hook: fma_dir exported (tests/test_oracle_walks.py checks it against
+ * exact rational arithmetic). */
+float orc_fma_dir(float a, float b, float c, int up) { return fma_dir(a, b, c, up); }
 /* a / b rounded up (b = 255 here: the product q * 255 is exact in double) */
 static float div_up(float a, float b)
 {

@@ -118,6 +118,9 @@ void orc_trace_wide(const uint32_t* wide, const orc_node* nodes, const orc_trian
  * the triangle's exact box passes too); fallback != 0: the stack-free walk
  * for every ray, as the kernels do when a slot could not be quantised. */
 int orc_quantise_wide(const uint32_t* wide, uint32_t n, uint32_t* out);
+/* a * b + c rounded once, down (up = 0) or up (up = 1): the emulation of
+ * __fmaf_rd / __fmaf_ru the quantised walks use (exported for its test). */
+float orc_fma_dir(float a, float b, float c, int up);
 void orc_trace_wide_quantised(const uint32_t* qwide, int fallback, const orc_node* nodes, const orc_triangle* tris,
                               uint32_t n, uint32_t root, const orc_ray* rays, uint32_t nRays, orc_hit* hits,
                               uint32_t* visits, uint32_t* tests, uint32_t* restarts, int query);

@@ -67,6 +67,7 @@ def oracle() -> ctypes.CDLL:
             "orc_build_wide": (None, [_vp, _u32, _vp]),
             "orc_trace_wide": (None, [_vp, _vp, _vp, _u32, _u32, _vp, _u32, _vp, _vp, _vp, _vp, _i32]),
             "orc_quantise_wide": (_i32, [_vp, _u32, _vp]),
+            "orc_fma_dir": (_f32, [_f32, _f32, _f32, _i32]),
             "orc_trace_wide_quantised": (None, [_vp, _i32, _vp, _vp, _u32, _u32, _vp, _u32, _vp, _vp, _vp, _vp,
                                                 _i32]),
             "orc_lookat": (None, [F3, F3, F3, _f32, _i32, _i32, _vp]),

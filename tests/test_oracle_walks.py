@@ -330,3 +330,48 @@ def test_quantised_wide_fallback_for_huge_extents():
                                           rays, fallback=True)
     ref = O.trace(b["nodes"], tris, b["root"], rays, 1, 0)
     np.testing.assert_array_equal(got, ref)
+
+
+def _round_dir(x, up):
+    """The float32 next to the exact rational x in the direction `up`
+    (float32 overflow: +-inf or +-FLT_MAX, as directed rounding gives)."""
+    from fractions import Fraction
+    f = np.float32(float(x))  # nearest or adjacent
+    if not np.isfinite(f):
+        big = np.float32(3.4028234663852886e38)
+        if x > 0:
+            return np.float32(np.inf) if up else big
+        return -big if up else np.float32(-np.inf)
+    if Fraction(float(f)) < x and up:
+        f = np.nextafter(f, np.float32(np.inf))
+    elif Fraction(float(f)) > x and not up:
+        f = np.nextafter(f, np.float32(-np.inf))
+    while up and Fraction(float(np.nextafter(f, np.float32(-np.inf)))) >= x:
+        f = np.nextafter(f, np.float32(-np.inf))
+    while not up and Fraction(float(np.nextafter(f, np.float32(np.inf)))) <= x:
+        f = np.nextafter(f, np.float32(np.inf))
+    return np.float32(f)
+
+
+def test_directed_fma_emulation_is_exact():
+    """The oracle's a * b + c rounded down / up (the emulation of __fmaf_rd /
+    __fmaf_ru in the quantised walks) equals the exact rational result
+    rounded in that direction: random operands over many binades, products
+    that cancel the addend, subnormal results and overflow."""
+    from fractions import Fraction
+    rng = np.random.default_rng(5)
+    cases = []
+    for _ in range(3000):
+        a, b, c = (np.float32(rng.standard_normal() * 2.0 ** rng.integers(-60, 60)) for _ in range(3))
+        cases.append((a, b, c))
+        cases.append((a, b, np.float32(-np.float64(a) * np.float64(b))))  # cancellation
+    cases += [(np.float32(1e-30), np.float32(1e-15), np.float32(0)), (np.float32(3e38), np.float32(10), np.float32(1)),
+              (np.float32(-3e38), np.float32(10), np.float32(-1)), (np.float32(1.5), np.float32(2), np.float32(-3)),
+              (np.float32(1e-40), np.float32(0.5), np.float32(1e-45))]
+    for a, b, c in cases:
+        exact = Fraction(float(a)) * Fraction(float(b)) + Fraction(float(c))
+        for up in (0, 1):
+            got = np.float32(O.oracle().orc_fma_dir(float(a), float(b), float(c), up))
+            want = _round_dir(exact, up)
+            assert got == want or (np.isinf(got) and np.isinf(want) and got == want), (a, b, c, up, got, want)
+
