@@ -1139,6 +1139,36 @@ __device__ __forceinline__ WideVisit qwide_visit(const mlbvh_qwnode* __restrict_
     WideVisit w{0u, -1, make_uint4(__float_as_uint(d.x), __float_as_uint(d.y), __float_as_uint(d.z),
                                    __float_as_uint(d.w)), {}};
     float bestT = 0.0f;
+    // C reaches the end of the float range (+-FLT_MAX or +-inf) where |inv| is
+    // huge, i.e. for a ray with a zero direction component (inv clamped to
+    // +-FLT_MAX): the base
+    // lies 2^E, about 128 node extents, below the planes, so (base - ro) inv
+    // leaves the float range although the planes' own distances do not. Such
+    // a slot takes the planes relative to the ray origin instead: base - ro
+    // plus V with directed adds, then the reference's slab (rounding to
+    // nearest is monotone, so it passes wherever it passes on the exact box).
+    if (!(fmaxf(fmaxf(fmaxf(fabsf(cnx), fabsf(cfx)), fmaxf(fabsf(cny), fabsf(cfy))),
+                fmaxf(fabsf(cnz), fabsf(cfz))) < kFltMax)) {
+        const f3 dlo = mk(__fsub_rd(a.x, ro.x), __fsub_rd(a.y, ro.y), __fsub_rd(a.z, ro.z));
+        const f3 dhi = mk(__fsub_ru(a.x, ro.x), __fsub_ru(a.y, ro.y), __fsub_ru(a.z, ro.z));
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const f3 plo = mk(__fadd_rd(dlo.x, qw_value(qxl, sx, k)), __fadd_rd(dlo.y, qw_value(qyl, sy, k)),
+                              __fadd_rd(dlo.z, qw_value(qzl, sz, k)));
+            const f3 phi = mk(__fadd_ru(dhi.x, qw_value(qxh, sx, k)), __fadd_ru(dhi.y, qw_value(qyh, sy, k)),
+                              __fadd_ru(dhi.z, qw_value(qzh, sz, k)));
+            const float2 r = slab_offsets(plo, phi, inv, tmin, hitT);
+            w.entry[k] = r.x;
+            if (wpick(w.ch, k) != kWideEmpty && r.x <= r.y) {
+                w.pass |= 1u << k;
+                if (w.best < 0 || r.x < bestT) {
+                    w.best = k;
+                    bestT = r.x;
+                }
+            }
+        }
+        return w;
+    }
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
         const float en = fmaxf(fmaxf(__fmaf_rd(qw_value(nqx, sx, k), inv.x, cnx),

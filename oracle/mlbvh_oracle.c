@@ -1279,6 +1279,27 @@ static void qwide_child(const uint32_t* w, int k, orc_f3 ro, orc_f3 inv, float t
     float base[3];
     memcpy(base, w, 12);
     const float r[3] = {ro.x, ro.y, ro.z}, iv[3] = {inv.x, inv.y, inv.z};
+    /* where a C reaches the end of the float range (a zero direction
+     * component: inv clamped to +-FLT_MAX), the slot takes its planes relative to the ray origin
+     * (base - ro plus V, directed adds) and the reference's slab */
+    int overflow = 0;
+    for (int a = 0; a < 3; ++a)
+        if (fabsf(fma_dir(base[a], iv[a], -mul_dir(r[a], iv[a], 1), 0)) >= ORC_FLT_MAX ||
+            fabsf(fma_dir(base[a], iv[a], -mul_dir(r[a], iv[a], 0), 1)) >= ORC_FLT_MAX)
+            overflow = 1;
+    if (overflow)
+    {
+        float dl[3], dh[3], rmin, rmax;
+        for (int a = 0; a < 3; ++a)
+        {
+            dl[a] = add_dir(add_dir(base[a], -r[a], 0), qw_value(w[6 + 2 * a], w[3 + a], k), 0);
+            dh[a] = add_dir(add_dir(base[a], -r[a], 1), qw_value(w[7 + 2 * a], w[3 + a], k), 1);
+        }
+        slabs_offsets(f3(dl[0], dl[1], dl[2]), f3(dh[0], dh[1], dh[2]), inv, hitT, &rmin, &rmax);
+        *entry = smax(rmin, tmin);
+        *exitOut = rmax;
+        return;
+    }
     float en = 0.0f, ex = 0.0f;
     for (int a = 0; a < 3; ++a)
     {
