@@ -1100,6 +1100,42 @@ __device__ __forceinline__ float qw_value(uint32_t codes, uint32_t scaleBits, in
 constexpr float kQEntryMargin = 2.384185791015625e-07f;
 constexpr float kQExitMargin = 4.76837158203125e-07f;
 
+// The slab test of a quantised slot with the planes relative to the ray
+// origin: base - ro plus V with directed adds (lower planes down, upper ones
+// up), then the reference's slab (rounding to nearest is monotone, so it
+// passes wherever it passes on the exact box). qwide_visit takes it only for
+// slots whose FMA form would leave the float range; it is not inlined, so
+// that the common path keeps its registers. a, b, c: the slot's first 48
+// bytes (base, scales, plane codes).
+static __device__ __noinline__ WideVisit qwide_visit_positions(float4 a, float4 b, float4 c, uint4 ch, f3 ro,
+                                                               f3 inv, float tmin, float hitT)
+{
+    const uint32_t sx = __float_as_uint(a.w), sy = __float_as_uint(b.x), sz = __float_as_uint(b.y);
+    const uint32_t qxl = __float_as_uint(b.z), qxh = __float_as_uint(b.w), qyl = __float_as_uint(c.x),
+                   qyh = __float_as_uint(c.y), qzl = __float_as_uint(c.z), qzh = __float_as_uint(c.w);
+    const f3 dlo = mk(__fsub_rd(a.x, ro.x), __fsub_rd(a.y, ro.y), __fsub_rd(a.z, ro.z));
+    const f3 dhi = mk(__fsub_ru(a.x, ro.x), __fsub_ru(a.y, ro.y), __fsub_ru(a.z, ro.z));
+    WideVisit w{0u, -1, ch, {}};
+    float bestT = 0.0f;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const f3 plo = mk(__fadd_rd(dlo.x, qw_value(qxl, sx, k)), __fadd_rd(dlo.y, qw_value(qyl, sy, k)),
+                          __fadd_rd(dlo.z, qw_value(qzl, sz, k)));
+        const f3 phi = mk(__fadd_ru(dhi.x, qw_value(qxh, sx, k)), __fadd_ru(dhi.y, qw_value(qyh, sy, k)),
+                          __fadd_ru(dhi.z, qw_value(qzh, sz, k)));
+        const float2 r = slab_offsets(plo, phi, inv, tmin, hitT);
+        w.entry[k] = r.x;
+        if (wpick(w.ch, k) != kWideEmpty && r.x <= r.y) {
+            w.pass |= 1u << k;
+            if (w.best < 0 || r.x < bestT) {
+                w.best = k;
+                bestT = r.x;
+            }
+        }
+    }
+    return w;
+}
+
 // The distance of a plane along the ray, (base + V - ro) inv, is one FMA per
 // plane: V inv + C, where C = base inv - ro inv bounds (base - ro) inv from
 // below for near planes (ro inv rounded up, the FMA rounded down) and from
@@ -1141,34 +1177,12 @@ __device__ __forceinline__ WideVisit qwide_visit(const mlbvh_qwnode* __restrict_
     float bestT = 0.0f;
     // C reaches the end of the float range (+-FLT_MAX or +-inf) where |inv| is
     // huge, i.e. for a ray with a zero direction component (inv clamped to
-    // +-FLT_MAX): the base
-    // lies 2^E, about 128 node extents, below the planes, so (base - ro) inv
-    // leaves the float range although the planes' own distances do not. Such
-    // a slot takes the planes relative to the ray origin instead: base - ro
-    // plus V with directed adds, then the reference's slab (rounding to
-    // nearest is monotone, so it passes wherever it passes on the exact box).
+    // +-FLT_MAX): the base lies 2^E, about 128 node extents, below the planes,
+    // so (base - ro) inv leaves the float range although the planes' own
+    // distances do not. Such a slot takes qwide_visit_positions instead.
     if (!(fmaxf(fmaxf(fmaxf(fabsf(cnx), fabsf(cfx)), fmaxf(fabsf(cny), fabsf(cfy))),
-                fmaxf(fabsf(cnz), fabsf(cfz))) < kFltMax)) {
-        const f3 dlo = mk(__fsub_rd(a.x, ro.x), __fsub_rd(a.y, ro.y), __fsub_rd(a.z, ro.z));
-        const f3 dhi = mk(__fsub_ru(a.x, ro.x), __fsub_ru(a.y, ro.y), __fsub_ru(a.z, ro.z));
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            const f3 plo = mk(__fadd_rd(dlo.x, qw_value(qxl, sx, k)), __fadd_rd(dlo.y, qw_value(qyl, sy, k)),
-                              __fadd_rd(dlo.z, qw_value(qzl, sz, k)));
-            const f3 phi = mk(__fadd_ru(dhi.x, qw_value(qxh, sx, k)), __fadd_ru(dhi.y, qw_value(qyh, sy, k)),
-                              __fadd_ru(dhi.z, qw_value(qzh, sz, k)));
-            const float2 r = slab_offsets(plo, phi, inv, tmin, hitT);
-            w.entry[k] = r.x;
-            if (wpick(w.ch, k) != kWideEmpty && r.x <= r.y) {
-                w.pass |= 1u << k;
-                if (w.best < 0 || r.x < bestT) {
-                    w.best = k;
-                    bestT = r.x;
-                }
-            }
-        }
-        return w;
-    }
+                fmaxf(fabsf(cnz), fabsf(cfz))) < kFltMax))
+        return qwide_visit_positions(a, b, c, w.ch, ro, inv, tmin, hitT);
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
         const float en = fmaxf(fmaxf(__fmaf_rd(qw_value(nqx, sx, k), inv.x, cnx),
