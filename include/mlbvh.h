@@ -430,7 +430,7 @@ MLBVH_API mlbvh_status mlbvh_trace_wide(const mlbvh_wnode* dWideNodes, const mlb
 /* The quantised slots of a 4-wide tree: nTriangles - 1 mlbvh_qwnode (none for
  * one triangle), 32-byte aligned, from the FP32 slots of mlbvh_build_wide.
  * *dStatus (one device word) becomes 0 when every slot was quantised, 1 when
- * one could not be (non-finite planes, or extents beyond about 1e36); the
+ * one could not be (non-finite planes, or coordinates beyond about 1e18); the
  * quantised walks then take the stack-free walk over the binary tree for
  * every ray (the same answers, slower). No reference counterpart. */
 MLBVH_API mlbvh_status mlbvh_quantise_wide(const mlbvh_wnode* dWideNodes, uint32_t nTriangles,

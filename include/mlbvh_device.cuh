@@ -1095,6 +1095,19 @@ __device__ __forceinline__ float qw_value(uint32_t codes, uint32_t scaleBits, in
 {
     return __uint_as_float(__byte_perm(codes, scaleBits, 0x7604u | ((uint32_t)k << 4)));
 }
+// The quantiser keeps every slot's base below 2^60 and its scale at most
+// 2^59 (else its status word sends the rays elsewhere), so every plane lies
+// below 2^61. A ray whose |inv| and |ro| components are below 2^62 then keeps
+// every term of qwide_visit's FMA form below 2^125, in the float range:
+// qwide_ray_fits, tested once per ray. Other rays (a zero direction component:
+// the reference clamps its inverse to +-FLT_MAX) take qwide_visit_positions.
+constexpr float kQBaseLimit = 1.152921504606846976e18f;  // 2^60
+constexpr float kQRayLimit = 4.611686018427387904e18f;   // 2^62
+__device__ __forceinline__ bool qwide_ray_fits(f3 ro, f3 inv)
+{
+    return fmaxf(fmaxf(fabsf(inv.x), fabsf(inv.y)), fmaxf(fabsf(inv.z), fmaxf(fmaxf(fabsf(ro.x), fabsf(ro.y)),
+                                                                               fabsf(ro.z)))) < kQRayLimit;
+}
 // Relative margins of the quantised slab test: 2^-22 below the entry and
 // 2^-21 above the exit (see qwide_visit).
 constexpr float kQEntryMargin = 2.384185791015625e-07f;
@@ -1104,8 +1117,8 @@ constexpr float kQExitMargin = 4.76837158203125e-07f;
 // origin: base - ro plus V with directed adds (lower planes down, upper ones
 // up), then the reference's slab (rounding to nearest is monotone, so it
 // passes wherever it passes on the exact box). qwide_visit takes it only for
-// slots whose FMA form would leave the float range; it is not inlined, so
-// that the common path keeps its registers. a, b, c: the slot's first 48
+// rays that qwide_ray_fits rejects; it is not inlined, so that the common
+// path keeps its registers. a, b, c: the slot's first 48
 // bytes (base, scales, plane codes).
 static __device__ __noinline__ WideVisit qwide_visit_positions(float4 a, float4 b, float4 c, uint4 ch, f3 ro,
                                                                f3 inv, float tmin, float hitT)
@@ -1152,7 +1165,7 @@ static __device__ __noinline__ WideVisit qwide_visit_positions(float4 a, float4 
 // box. Every rounding is directed, so a distance that overflows stays on its
 // conservative side (an FMA rounded down gives FLT_MAX or -inf).
 __device__ __forceinline__ WideVisit qwide_visit(const mlbvh_qwnode* __restrict__ qw, uint32_t i, f3 ro, f3 inv,
-                                                 float tmin, float hitT)
+                                                 float tmin, float hitT, bool fits)
 {
     const float4* p = reinterpret_cast<const float4*>(qw + i);
     float4 a, b, c, d;
@@ -1175,14 +1188,7 @@ __device__ __forceinline__ WideVisit qwide_visit(const mlbvh_qwnode* __restrict_
     WideVisit w{0u, -1, make_uint4(__float_as_uint(d.x), __float_as_uint(d.y), __float_as_uint(d.z),
                                    __float_as_uint(d.w)), {}};
     float bestT = 0.0f;
-    // C reaches the end of the float range (+-FLT_MAX or +-inf) where |inv| is
-    // huge, i.e. for a ray with a zero direction component (inv clamped to
-    // +-FLT_MAX): the base lies 2^E, about 128 node extents, below the planes,
-    // so (base - ro) inv leaves the float range although the planes' own
-    // distances do not. Such a slot takes qwide_visit_positions instead.
-    if (!(fmaxf(fmaxf(fmaxf(fabsf(cnx), fabsf(cfx)), fmaxf(fabsf(cny), fabsf(cfy))),
-                fmaxf(fabsf(cnz), fabsf(cfz))) < kFltMax))
-        return qwide_visit_positions(a, b, c, w.ch, ro, inv, tmin, hitT);
+    if (!fits) return qwide_visit_positions(a, b, c, w.ch, ro, inv, tmin, hitT);
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
         const float en = fmaxf(fmaxf(__fmaf_rd(qw_value(nqx, sx, k), inv.x, cnx),
@@ -1219,7 +1225,7 @@ __device__ __forceinline__ bool wide_any_step(uint32_t& curr, uint32_t& prev, in
                                               const mlbvh_internal_node* __restrict__ nodes,
                                               const float* __restrict__ tris, const mlbvh_qtri* __restrict__ leafTris,
                                               uint32_t binaryRoot, f3 ro, f3 rd, f3 inv, float tmin, uint32_t& nv,
-                                              uint32_t& nt, uint32_t& nr)
+                                              uint32_t& nt, uint32_t& nr, bool fits = true)
 {
     if (depth < 0) return stackfree_step<true, kCount, true>(curr, prev, hit, nodes, tris, ro, rd, inv, tmin, nv, nt);
     if (curr & kLeafBit) {
@@ -1242,7 +1248,7 @@ __device__ __forceinline__ bool wide_any_step(uint32_t& curr, uint32_t& prev, in
         if (kCount) ++nv;
         WideVisit w;
         if constexpr (kQuant)
-            w = qwide_visit(slots, curr, ro, inv, tmin, hit.t);
+            w = qwide_visit(slots, curr, ro, inv, tmin, hit.t, fits);
         else
             w = wide_visit(slots, curr, ro, inv, tmin, hit.t);
         if (w.pass) {
@@ -1296,7 +1302,7 @@ __device__ __forceinline__ bool wide_closest_step(uint32_t& curr, uint32_t& prev
                                                   const float* __restrict__ tris,
                                                   const mlbvh_qtri* __restrict__ leafTris, uint32_t binaryRoot, f3 ro,
                                                   f3 rd, f3 inv, float tmin, uint32_t& nv, uint32_t& nt,
-                                                  uint32_t& nr)
+                                                  uint32_t& nr, bool fits = true)
 {
     if (depth < 0) return stackfree_step<false, kCount, true>(curr, prev, hit, nodes, tris, ro, rd, inv, tmin, nv, nt);
     if (curr & kLeafBit) {
@@ -1318,7 +1324,7 @@ __device__ __forceinline__ bool wide_closest_step(uint32_t& curr, uint32_t& prev
         if (kCount) ++nv;
         WideVisit w;
         if constexpr (kQuant)
-            w = qwide_visit(slots, curr, ro, inv, tmin, hit.t);
+            w = qwide_visit(slots, curr, ro, inv, tmin, hit.t, fits);
         else
             w = wide_visit(slots, curr, ro, inv, tmin, hit.t);
         if (w.pass) {

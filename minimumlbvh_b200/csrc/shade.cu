@@ -237,7 +237,7 @@ struct PlainTreeT {
     }
     template <bool kAny, bool kCount>
     __device__ __forceinline__ bool step(const Ctx&, uint32_t& curr, uint32_t& prev, int& depth, uint32_t* stack,
-                                         HitRecord& hit, f3 ro, f3 rd, f3 inv, Counts& n) const
+                                         HitRecord& hit, f3 ro, f3 rd, f3 inv, Counts& n, bool fits) const
     {
         static_assert(kWalk == 0 || kAny, "AO rays are any-hit");
         return walk<kAny, kCount>(curr, prev, depth, stack, kAoThreads, hit, ro, rd, inv, n);
@@ -292,7 +292,7 @@ struct QuantTree {
     }
     template <bool kAny, bool kCount>
     __device__ __forceinline__ bool step(const Ctx& c, uint32_t& curr, uint32_t& prev, int& depth, uint32_t* stack,
-                                         HitRecord& hit, f3 ro, f3 rd, f3 inv, Counts& n) const
+                                         HitRecord& hit, f3 ro, f3 rd, f3 inv, Counts& n, bool fits) const
     {
         return quantised_replay_step<kAny, kCount, kStack>(curr, prev, depth, stack, kAoThreads, hit, qnodes, parents,
                                                            qtris, c.eBase, ro, rd, inv, 0.0f, n.visits, n.tests,
@@ -386,7 +386,7 @@ struct WideTreeT {
     }
     template <bool kAny, bool kCount>
     __device__ __forceinline__ bool step(const Ctx& c, uint32_t& curr, uint32_t& prev, int& depth, uint32_t* stack,
-                                         HitRecord& hit, f3 ro, f3 rd, f3 inv, Counts& n) const
+                                         HitRecord& hit, f3 ro, f3 rd, f3 inv, Counts& n, bool fits) const
     {
         static_assert(kAny, "AO rays are any-hit");
         if (kQuant && c.fallback && depth >= 0) {  // unusable slots: the stack-free walk from the binary root
@@ -396,7 +396,7 @@ struct WideTreeT {
         }
         return wide_any_step<kCount, kQuant>(curr, prev, depth, stack, kAoThreads, hit, slots, binary.nodes,
                                              binary.tris, binary.leafTris, c.binaryRoot, ro, rd, inv, 0.0f, n.visits,
-                                             n.tests, n.ups);
+                                             n.tests, n.ups, fits);
     }
 };
 using WideTree = WideTreeT<false>;
@@ -519,6 +519,7 @@ __global__ void __launch_bounds__(kAoThreads, MinBlocksOf<Tree>::value)
     uint32_t pixel = 0, curr = 0, prev = 0, steps = 0;
     int depth = 0;
     f3 origin = mk(0, 0, 0), dir = origin, inv = origin;
+    bool fits = true;  // qwide_ray_fits of this lane's ray (only the quantised wide slots use it)
     HitRecord hit;
     hit.t = radius;
     for (;;) {
@@ -562,6 +563,7 @@ __global__ void __launch_bounds__(kAoThreads, MinBlocksOf<Tree>::value)
                     const f3 dl = sample_hemisphere(rnd.x, rnd.y);
                     dir = xaxis * dl.x + zaxis * dl.z + n * dl.y;
                     inv = inv_rd(dir);
+                    fits = qwide_ray_fits(origin, inv);
                     hit.t = radius;
                     hit.tri = 0xFFFFFFFFu;
                     curr = start;
@@ -583,7 +585,8 @@ __global__ void __launch_bounds__(kAoThreads, MinBlocksOf<Tree>::value)
 #pragma unroll
         for (int rep = 0; rep < StepsOf<Tree>::value; ++rep)
             if (live) {
-                if (tree.template step<true, kCount>(ctx, curr, prev, depth, stack, hit, origin, dir, inv, cnt) ||
+                if (tree.template step<true, kCount>(ctx, curr, prev, depth, stack, hit, origin, dir, inv, cnt,
+                                                     fits) ||
                     ++steps >= kMaxTraversalSteps) {
                     live = false;
                     occluded = hit.t != radius;

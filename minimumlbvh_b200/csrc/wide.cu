@@ -5,8 +5,6 @@
 // binary internal node i, written by one thread with no order between slots:
 // the walk starts at the root's slot and only ever follows child indices,
 // which name the slots of their own expansions.
-#include <algorithm>
-
 #include "capi_internal.h"
 #include "../../include/mlbvh_device.cuh"
 
@@ -101,6 +99,8 @@ __global__ void __launch_bounds__(kWideThreads)
 // base + 2^E (1 + q / 2^15) <= lo and an upper code >= hi, in exact
 // arithmetic: every step rounds toward that side. E is the smallest exponent
 // (>= -111, so that 2^(E-15) stays a normal number) whose codes fit 8 bits.
+// An axis whose base would reach 2^60 or whose scale would exceed 2^59
+// (coordinates beyond about 1e18) counts as not quantised.
 __device__ __forceinline__ bool quantise_axis(const float lo[4], const float hi[4], uint32_t valid, float& base,
                                               float& scale, uint32_t& qlo, uint32_t& qhi)
 {
@@ -137,7 +137,8 @@ __device__ __forceinline__ bool quantise_axis(const float lo[4], const float hi[
                 qlo |= (uint32_t)fminf(fmaxf(ql, 0.0f), 255.0f) << (8 * k);
                 qhi |= (uint32_t)fminf(fmaxf(qh, 0.0f), 255.0f) << (8 * k);
             }
-        if (fits) return true;
+        // the walks' FMA form relies on bases below 2^60 and scales of at most 2^59 (qwide_ray_fits)
+        if (fits) return fabsf(base) < kQBaseLimit && e <= 59;
     }
     return false;
 }
@@ -173,23 +174,13 @@ __global__ void __launch_bounds__(kWideThreads)
     reinterpret_cast<uint4*>(dst)[3] = ch;
 }
 
-// Rays over FP32 slots or (kQuant) quantised slots, any-hit (wide_any_step)
-// or closest-hit (wide_closest_step), on a persistent grid with lane refill:
-// warp w takes the chunks of kWideChunk consecutive rays w, w + W, w + 2W, ...
-// (W warps in the grid; a fixed round-robin, so no queue counter is needed)
-// and hands their rays to its idle lanes; each lane walks its own ray,
-// kWideStepsPerRound steps between refills, and takes the next ray of the
-// chunk as soon as it finishes (a new chunk once kWideRefillLanes lanes are
-// idle), so a warp is not held by its longest ray. Every ray's walk is the
-// one-ray-per-thread walk, so the Hit records and counts do not depend on
-// the schedule. counts (may be null): per ray, node visits, triangle tests
-// and restarts at counts[i], counts[n + i], counts[2n + i]. status (quantised
-// slots): nonzero sends every ray to the stack-free walk over the binary tree.
-constexpr uint32_t kWideChunk = 64;
-constexpr int kWideRefillLanes = 8;
-constexpr int kWideStepsPerRound = 2;
+// One thread per ray, any-hit (wide_any_step) or closest-hit
+// (wide_closest_step), over FP32 slots or (kQuant) quantised slots. counts
+// (may be null): per ray, node visits, triangle tests and restarts at
+// counts[i], counts[n + i], counts[2n + i]. status (quantised slots): nonzero
+// sends every ray to the stack-free walk over the binary tree.
 template <bool kAny, bool kCount, bool kQuant, class Slot>
-__global__ void __launch_bounds__(kWideTraceThreads, 8)
+__global__ void __launch_bounds__(kWideTraceThreads)
     k_trace_wide(const Slot* __restrict__ slots, const uint32_t* __restrict__ status,
                  const mlbvh_internal_node* __restrict__ nodes, const mlbvh_node_index* __restrict__ rootPtr,
                  const float* __restrict__ tris, const mlbvh_qtri* __restrict__ leafTris,
@@ -198,90 +189,44 @@ __global__ void __launch_bounds__(kWideTraceThreads, 8)
 {
     using Entry = typename ReplayStack<kAny>::Entry;
     __shared__ Entry s_stack[kWideDepth][kWideTraceThreads];
-    const uint32_t root = __ldg(rootPtr);
-    const bool fallback = kQuant && __ldg(status) != 0u;
-    const int lane = threadIdx.x & 31;
-    const uint32_t lanesBelow = (1u << lane) - 1u;
-    const uint32_t nWarps = (gridDim.x * blockDim.x) >> 5;
-    uint32_t nextChunk = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;  // warp-uniform
-    uint32_t poolNext = 0, poolEnd = 0;                                  // warp-uniform
-    bool exhausted = false;                                              // warp-uniform
-    bool live = false;
-    uint32_t ray = 0, curr = 0, prev = 0, steps = 0, nv = 0, nt = 0, nr = 0;
-    int depth = 0;
-    f3 ro = mk(0.0f, 0.0f, 0.0f), rd = ro, inv = ro;
-    float tmin = 0.0f;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float4 a = __ldg(rays + 2 * (size_t)i), b = __ldg(rays + 2 * (size_t)i + 1);
+    const f3 ro = mk(a.x, a.y, a.z), rd = mk(b.x, b.y, b.z);
     HitRecord hit;
-    hit.t = 0.0f;
-    for (;;) {
-        const uint32_t idle = __ballot_sync(0xffffffffu, !live);
-        if (idle) {
-            if (poolNext >= poolEnd && !exhausted &&
-                (__popc(idle) >= kWideRefillLanes || idle == 0xffffffffu)) {
-                const uint64_t base = (uint64_t)nextChunk * kWideChunk;
-                nextChunk += nWarps;
-                if (base >= n) {
-                    exhausted = true;
-                } else {
-                    poolNext = (uint32_t)base;
-                    poolEnd = (uint32_t)min(base + kWideChunk, (uint64_t)n);
-                }
-            }
-            if (poolNext < poolEnd) {
-                const uint32_t avail = poolEnd - poolNext;
-                const uint32_t rank = __popc(idle & lanesBelow);
-                if (!live && rank < avail) {
-                    ray = poolNext + rank;
-                    const float4 a = __ldg(rays + 2 * (size_t)ray), b = __ldg(rays + 2 * (size_t)ray + 1);
-                    ro = mk(a.x, a.y, a.z);
-                    rd = mk(b.x, b.y, b.z);
-                    tmin = a.w;
-                    inv = inv_rd(rd);
-                    hit.t = b.w;
-                    hit.u = 0.0f;
-                    hit.v = 0.0f;
-                    hit.ng = mk(0.0f, 0.0f, 0.0f);
-                    hit.tri = 0xFFFFFFFFu;
-                    curr = (root & kLeafBit) ? kLeafBit : root;
-                    prev = kInvalid;
-                    depth = 0;
-                    if (fallback) {
-                        curr = root;
-                        depth = -1;
-                    }
-                    steps = nv = nt = nr = 0;
-                    live = true;
-                }
-                poolNext += min((uint32_t)__popc(idle), avail);
-            }
-        }
-        if (!__any_sync(0xffffffffu, live)) {
-            if (exhausted) break;
-            continue;
-        }
-#pragma unroll
-        for (int r = 0; r < kWideStepsPerRound; ++r) {
-            if (!live) continue;
-            bool done;
-            if constexpr (kAny)
-                done = wide_any_step<kCount, kQuant>(curr, prev, depth, &s_stack[0][threadIdx.x], kWideTraceThreads,
-                                                     hit, slots, nodes, tris, leafTris, root, ro, rd, inv, tmin, nv,
-                                                     nt, nr);
-            else
-                done = wide_closest_step<kCount, kQuant>(curr, prev, depth, &s_stack[0][threadIdx.x],
-                                                         kWideTraceThreads, hit, slots, nodes, tris, leafTris, root,
-                                                         ro, rd, inv, tmin, nv, nt, nr);
-            if (done || ++steps >= kMaxTraversalSteps) {
-                hits[2 * (size_t)ray] = make_float4(hit.t, 0.0f, hit.u, hit.v);
-                hits[2 * (size_t)ray + 1] = make_float4(hit.ng.x, hit.ng.y, hit.ng.z, __uint_as_float(hit.tri));
-                if (kCount) {
-                    counts[ray] = nv;
-                    counts[n + ray] = nt;
-                    counts[2 * (size_t)n + ray] = nr;
-                }
-                live = false;
-            }
-        }
+    hit.t = b.w;
+    hit.u = 0.0f;
+    hit.v = 0.0f;
+    hit.ng = mk(0.0f, 0.0f, 0.0f);
+    hit.tri = 0xFFFFFFFFu;
+    const uint32_t root = __ldg(rootPtr);
+    const f3 inv = inv_rd(rd);
+    const bool fits = !kQuant || qwide_ray_fits(ro, inv);
+    uint32_t nv = 0, nt = 0, nr = 0;
+    uint32_t curr = (root & kLeafBit) ? kLeafBit : root, prev = kInvalid;
+    int depth = 0;
+    if (kQuant && __ldg(status) != 0u) {
+        curr = root;
+        depth = -1;
+    }
+    for (uint32_t steps = 1; steps < kMaxTraversalSteps; ++steps) {
+        bool done;
+        if constexpr (kAny)
+            done = wide_any_step<kCount, kQuant>(curr, prev, depth, &s_stack[0][threadIdx.x], kWideTraceThreads, hit,
+                                                 slots, nodes, tris, leafTris, root, ro, rd, inv, a.w, nv, nt, nr,
+                                                 fits);
+        else
+            done = wide_closest_step<kCount, kQuant>(curr, prev, depth, &s_stack[0][threadIdx.x], kWideTraceThreads,
+                                                     hit, slots, nodes, tris, leafTris, root, ro, rd, inv, a.w, nv,
+                                                     nt, nr, fits);
+        if (done) break;
+    }
+    hits[2 * (size_t)i] = make_float4(hit.t, 0.0f, hit.u, hit.v);
+    hits[2 * (size_t)i + 1] = make_float4(hit.ng.x, hit.ng.y, hit.ng.z, __uint_as_float(hit.tri));
+    if (kCount) {
+        counts[i] = nv;
+        counts[n + i] = nt;
+        counts[2 * (size_t)n + i] = nr;
     }
 }
 
@@ -322,14 +267,7 @@ mlbvh_status launch_trace_wide(const Slot* dSlots, const uint32_t* dStatus, cons
         return fail(MLBVH_ERR_INVALID_ARG,
                     "device pointers misaligned (wide slots 128 B, quantised slots and nodes 32 B, others 16 B)");
     if (nRays >= (1u << 30) && dCounts) return fail(MLBVH_ERR_INVALID_ARG, "nRays must be below 2^30 with counts");
-    // a persistent grid: every resident CTA, no more than the rays need
-    int perSM = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, k_trace_wide<true, false, kQuant, Slot>,
-                                                  kWideTraceThreads, 0);
-    const uint64_t needed = ((uint64_t)nRays + kWideChunk - 1) / kWideChunk;  // warps with a chunk
-    const unsigned blocks = (unsigned)std::max<uint64_t>(
-        1, std::min<uint64_t>((uint64_t)device_sm_count() * std::max(perSM, 1),
-                              (needed + kWideTraceThreads / 32 - 1) / (kWideTraceThreads / 32)));
+    const unsigned blocks = (nRays + kWideTraceThreads - 1) / kWideTraceThreads;
     const float4* rays = reinterpret_cast<const float4*>(dRays);
     float4* hits = reinterpret_cast<float4*>(dHits);
     const float* tris = reinterpret_cast<const float*>(dTris);

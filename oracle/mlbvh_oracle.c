@@ -1220,7 +1220,7 @@ static int quantise_axis(const float lo[4], const float hi[4], uint32_t valid, f
         *scale = sc;
         *qlo = ql_all;
         *qhi = qh_all;
-        if (fits) return 1;
+        if (fits) return fabsf(b) < 1.152921504606846976e18f && e <= 59; /* base < 2^60, scale <= 2^59 */
     }
     return 0;
 }
@@ -1279,15 +1279,13 @@ static void qwide_child(const uint32_t* w, int k, orc_f3 ro, orc_f3 inv, float t
     float base[3];
     memcpy(base, w, 12);
     const float r[3] = {ro.x, ro.y, ro.z}, iv[3] = {inv.x, inv.y, inv.z};
-    /* where a C reaches the end of the float range (a zero direction
-     * component: inv clamped to +-FLT_MAX), the slot takes its planes relative to the ray origin
-     * (base - ro plus V, directed adds) and the reference's slab */
-    int overflow = 0;
-    for (int a = 0; a < 3; ++a)
-        if (fabsf(fma_dir(base[a], iv[a], -mul_dir(r[a], iv[a], 1), 0)) >= ORC_FLT_MAX ||
-            fabsf(fma_dir(base[a], iv[a], -mul_dir(r[a], iv[a], 0), 1)) >= ORC_FLT_MAX)
-            overflow = 1;
-    if (overflow)
+    /* a ray with some |inv| or |ro| of 2^62 or more (a zero direction
+     * component: inv clamped to +-FLT_MAX) takes the planes relative to the
+     * ray origin (base - ro plus V, directed adds) and the reference's slab */
+    const float lim = 4.611686018427387904e18f; /* 2^62 */
+    const int fits = fabsf(iv[0]) < lim && fabsf(iv[1]) < lim && fabsf(iv[2]) < lim && fabsf(r[0]) < lim &&
+                     fabsf(r[1]) < lim && fabsf(r[2]) < lim;
+    if (!fits)
     {
         float dl[3], dh[3], rmin, rmax;
         for (int a = 0; a < 3; ++a)

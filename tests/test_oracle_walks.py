@@ -341,6 +341,19 @@ def test_quantised_wide_rays_with_zero_direction_components_keep_culling():
         assert nv.sum() < 1.3 * nv32.sum() and nv.max() < 2 * nv32.max() + 64 and nr.sum() == 0
 
 
+def test_quantised_wide_slots_refuse_coordinates_beyond_2_60():
+    """Slots whose base would reach 2^60 (coordinates about 1e19) are not
+    quantised: the walks' FMA form needs every plane below 2^61."""
+    rng = np.random.default_rng(10)
+    tris = (rng.random((300, 9)).astype(np.float32) + np.float32(8.0)) * np.float32(2e18)
+    b = O.build(tris)
+    wide = O.build_wide(b["nodes"], len(tris))
+    _, ok = O.quantise_wide(wide, len(tris))
+    assert not ok
+    _, ok = O.quantise_wide(O.build_wide(O.build(tris / np.float32(1e3))["nodes"], len(tris)), len(tris))
+    assert ok
+
+
 def test_quantised_wide_fallback_for_huge_extents():
     """Coordinates spread over about 1e37 cannot be quantised (codes beyond
     8 bits at every scale up to 2^127): the slots are flagged and every ray
