@@ -1096,11 +1096,13 @@ __device__ __forceinline__ float qw_value(uint32_t codes, uint32_t scaleBits, in
     return __uint_as_float(__byte_perm(codes, scaleBits, 0x7604u | ((uint32_t)k << 4)));
 }
 // The quantiser keeps every slot's base below 2^60 and its scale at most
-// 2^59 (else its status word sends the rays elsewhere), so every plane lies
-// below 2^61. A ray whose |inv| and |ro| components are below 2^62 then keeps
-// every term of qwide_visit's FMA form below 2^125, in the float range:
-// qwide_ray_fits, tested once per ray. Other rays (a zero direction component:
-// the reference clamps its inverse to +-FLT_MAX) take qwide_visit_positions.
+// 2^59 (else its status word sends every ray to the binary tree), so every
+// plane lies below 2^61. A ray whose |inv| and |ro| components are below 2^62
+// then keeps every term of qwide_visit's FMA form below 2^125, in the float
+// range (qwide_ray_fits, tested once per ray). The walks send other rays (in
+// practice those with a zero direction component, whose inverse the
+// reference clamps to +-FLT_MAX) to the stack-free walk over the binary tree,
+// which gives the reference's own answers.
 constexpr float kQBaseLimit = 1.152921504606846976e18f;  // 2^60
 constexpr float kQRayLimit = 4.611686018427387904e18f;   // 2^62
 __device__ __forceinline__ bool qwide_ray_fits(f3 ro, f3 inv)
@@ -1112,42 +1114,6 @@ __device__ __forceinline__ bool qwide_ray_fits(f3 ro, f3 inv)
 // 2^-21 above the exit (see qwide_visit).
 constexpr float kQEntryMargin = 2.384185791015625e-07f;
 constexpr float kQExitMargin = 4.76837158203125e-07f;
-
-// The slab test of a quantised slot with the planes relative to the ray
-// origin: base - ro plus V with directed adds (lower planes down, upper ones
-// up), then the reference's slab (rounding to nearest is monotone, so it
-// passes wherever it passes on the exact box). qwide_visit takes it only for
-// rays that qwide_ray_fits rejects; it is not inlined, so that the common
-// path keeps its registers. a, b, c: the slot's first 48
-// bytes (base, scales, plane codes).
-static __device__ __noinline__ WideVisit qwide_visit_positions(float4 a, float4 b, float4 c, uint4 ch, f3 ro,
-                                                               f3 inv, float tmin, float hitT)
-{
-    const uint32_t sx = __float_as_uint(a.w), sy = __float_as_uint(b.x), sz = __float_as_uint(b.y);
-    const uint32_t qxl = __float_as_uint(b.z), qxh = __float_as_uint(b.w), qyl = __float_as_uint(c.x),
-                   qyh = __float_as_uint(c.y), qzl = __float_as_uint(c.z), qzh = __float_as_uint(c.w);
-    const f3 dlo = mk(__fsub_rd(a.x, ro.x), __fsub_rd(a.y, ro.y), __fsub_rd(a.z, ro.z));
-    const f3 dhi = mk(__fsub_ru(a.x, ro.x), __fsub_ru(a.y, ro.y), __fsub_ru(a.z, ro.z));
-    WideVisit w{0u, -1, ch, {}};
-    float bestT = 0.0f;
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-        const f3 plo = mk(__fadd_rd(dlo.x, qw_value(qxl, sx, k)), __fadd_rd(dlo.y, qw_value(qyl, sy, k)),
-                          __fadd_rd(dlo.z, qw_value(qzl, sz, k)));
-        const f3 phi = mk(__fadd_ru(dhi.x, qw_value(qxh, sx, k)), __fadd_ru(dhi.y, qw_value(qyh, sy, k)),
-                          __fadd_ru(dhi.z, qw_value(qzh, sz, k)));
-        const float2 r = slab_offsets(plo, phi, inv, tmin, hitT);
-        w.entry[k] = r.x;
-        if (wpick(w.ch, k) != kWideEmpty && r.x <= r.y) {
-            w.pass |= 1u << k;
-            if (w.best < 0 || r.x < bestT) {
-                w.best = k;
-                bestT = r.x;
-            }
-        }
-    }
-    return w;
-}
 
 // The distance of a plane along the ray, (base + V - ro) inv, is one FMA per
 // plane: V inv + C, where C = base inv - ro inv bounds (base - ro) inv from
@@ -1165,7 +1131,7 @@ static __device__ __noinline__ WideVisit qwide_visit_positions(float4 a, float4 
 // box. Every rounding is directed, so a distance that overflows stays on its
 // conservative side (an FMA rounded down gives FLT_MAX or -inf).
 __device__ __forceinline__ WideVisit qwide_visit(const mlbvh_qwnode* __restrict__ qw, uint32_t i, f3 ro, f3 inv,
-                                                 float tmin, float hitT, bool fits)
+                                                 float tmin, float hitT)
 {
     const float4* p = reinterpret_cast<const float4*>(qw + i);
     float4 a, b, c, d;
@@ -1188,7 +1154,6 @@ __device__ __forceinline__ WideVisit qwide_visit(const mlbvh_qwnode* __restrict_
     WideVisit w{0u, -1, make_uint4(__float_as_uint(d.x), __float_as_uint(d.y), __float_as_uint(d.z),
                                    __float_as_uint(d.w)), {}};
     float bestT = 0.0f;
-    if (!fits) return qwide_visit_positions(a, b, c, w.ch, ro, inv, tmin, hitT);
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
         const float en = fmaxf(fmaxf(__fmaf_rd(qw_value(nqx, sx, k), inv.x, cnx),
@@ -1225,7 +1190,7 @@ __device__ __forceinline__ bool wide_any_step(uint32_t& curr, uint32_t& prev, in
                                               const mlbvh_internal_node* __restrict__ nodes,
                                               const float* __restrict__ tris, const mlbvh_qtri* __restrict__ leafTris,
                                               uint32_t binaryRoot, f3 ro, f3 rd, f3 inv, float tmin, uint32_t& nv,
-                                              uint32_t& nt, uint32_t& nr, bool fits = true)
+                                              uint32_t& nt, uint32_t& nr)
 {
     if (depth < 0) return stackfree_step<true, kCount, true>(curr, prev, hit, nodes, tris, ro, rd, inv, tmin, nv, nt);
     if (curr & kLeafBit) {
@@ -1248,7 +1213,7 @@ __device__ __forceinline__ bool wide_any_step(uint32_t& curr, uint32_t& prev, in
         if (kCount) ++nv;
         WideVisit w;
         if constexpr (kQuant)
-            w = qwide_visit(slots, curr, ro, inv, tmin, hit.t, fits);
+            w = qwide_visit(slots, curr, ro, inv, tmin, hit.t);
         else
             w = wide_visit(slots, curr, ro, inv, tmin, hit.t);
         if (w.pass) {
@@ -1302,7 +1267,7 @@ __device__ __forceinline__ bool wide_closest_step(uint32_t& curr, uint32_t& prev
                                                   const float* __restrict__ tris,
                                                   const mlbvh_qtri* __restrict__ leafTris, uint32_t binaryRoot, f3 ro,
                                                   f3 rd, f3 inv, float tmin, uint32_t& nv, uint32_t& nt,
-                                                  uint32_t& nr, bool fits = true)
+                                                  uint32_t& nr)
 {
     if (depth < 0) return stackfree_step<false, kCount, true>(curr, prev, hit, nodes, tris, ro, rd, inv, tmin, nv, nt);
     if (curr & kLeafBit) {
@@ -1324,7 +1289,7 @@ __device__ __forceinline__ bool wide_closest_step(uint32_t& curr, uint32_t& prev
         if (kCount) ++nv;
         WideVisit w;
         if constexpr (kQuant)
-            w = qwide_visit(slots, curr, ro, inv, tmin, hit.t, fits);
+            w = qwide_visit(slots, curr, ro, inv, tmin, hit.t);
         else
             w = wide_visit(slots, curr, ro, inv, tmin, hit.t);
         if (w.pass) {

@@ -389,14 +389,15 @@ struct WideTreeT {
                                          HitRecord& hit, f3 ro, f3 rd, f3 inv, Counts& n, bool fits) const
     {
         static_assert(kAny, "AO rays are any-hit");
-        if (kQuant && c.fallback && depth >= 0) {  // unusable slots: the stack-free walk from the binary root
+        // unusable slots, or a ray outside qwide_ray_fits: the stack-free walk from the binary root
+        if (kQuant && (c.fallback || !fits) && depth >= 0) {
             depth = -1;
             curr = c.binaryRoot;
             prev = kInvalid;
         }
         return wide_any_step<kCount, kQuant>(curr, prev, depth, stack, kAoThreads, hit, slots, binary.nodes,
                                              binary.tris, binary.leafTris, c.binaryRoot, ro, rd, inv, 0.0f, n.visits,
-                                             n.tests, n.ups, fits);
+                                             n.tests, n.ups);
     }
 };
 using WideTree = WideTreeT<false>;

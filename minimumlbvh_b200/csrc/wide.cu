@@ -178,7 +178,8 @@ __global__ void __launch_bounds__(kWideThreads)
 // (wide_closest_step), over FP32 slots or (kQuant) quantised slots. counts
 // (may be null): per ray, node visits, triangle tests and restarts at
 // counts[i], counts[n + i], counts[2n + i]. status (quantised slots): nonzero
-// sends every ray to the stack-free walk over the binary tree.
+// sends every ray to the stack-free walk over the binary tree; so does a ray
+// that qwide_ray_fits rejects.
 template <bool kAny, bool kCount, bool kQuant, class Slot>
 __global__ void __launch_bounds__(kWideTraceThreads)
     k_trace_wide(const Slot* __restrict__ slots, const uint32_t* __restrict__ status,
@@ -201,11 +202,10 @@ __global__ void __launch_bounds__(kWideTraceThreads)
     hit.tri = 0xFFFFFFFFu;
     const uint32_t root = __ldg(rootPtr);
     const f3 inv = inv_rd(rd);
-    const bool fits = !kQuant || qwide_ray_fits(ro, inv);
     uint32_t nv = 0, nt = 0, nr = 0;
     uint32_t curr = (root & kLeafBit) ? kLeafBit : root, prev = kInvalid;
     int depth = 0;
-    if (kQuant && __ldg(status) != 0u) {
+    if (kQuant && (__ldg(status) != 0u || !qwide_ray_fits(ro, inv))) {
         curr = root;
         depth = -1;
     }
@@ -213,12 +213,11 @@ __global__ void __launch_bounds__(kWideTraceThreads)
         bool done;
         if constexpr (kAny)
             done = wide_any_step<kCount, kQuant>(curr, prev, depth, &s_stack[0][threadIdx.x], kWideTraceThreads, hit,
-                                                 slots, nodes, tris, leafTris, root, ro, rd, inv, a.w, nv, nt, nr,
-                                                 fits);
+                                                 slots, nodes, tris, leafTris, root, ro, rd, inv, a.w, nv, nt, nr);
         else
             done = wide_closest_step<kCount, kQuant>(curr, prev, depth, &s_stack[0][threadIdx.x], kWideTraceThreads,
                                                      hit, slots, nodes, tris, leafTris, root, ro, rd, inv, a.w, nv,
-                                                     nt, nr, fits);
+                                                     nt, nr);
         if (done) break;
     }
     hits[2 * (size_t)i] = make_float4(hit.t, 0.0f, hit.u, hit.v);

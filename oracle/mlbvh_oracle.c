@@ -1271,6 +1271,16 @@ static inline void slabs_offsets(orc_f3 dlo, orc_f3 dhi, orc_f3 inv, float known
  * rounded up, far planes rounded up with ro inv rounded down; entry = the
  * largest near distance moved down by 2^-22 of itself, exit = the smallest far
  * one moved up by 2^-21 of itself, then clipped to [max(0, tmin), hitT]. */
+/* qwide_ray_fits: every |inv| and |ro| component below 2^62, which keeps the
+ * FMA form in the float range given the quantiser's bound (bases below 2^60,
+ * scales at most 2^59); other rays take the stack-free walk over the binary
+ * tree instead of the quantised slots */
+static int qwide_ray_fits(orc_f3 ro, orc_f3 inv)
+{
+    const float lim = 4.611686018427387904e18f; /* 2^62 */
+    return fabsf(inv.x) < lim && fabsf(inv.y) < lim && fabsf(inv.z) < lim && fabsf(ro.x) < lim &&
+           fabsf(ro.y) < lim && fabsf(ro.z) < lim;
+}
 #define ORC_Q_ENTRY_MARGIN 2.384185791015625e-07f
 #define ORC_Q_EXIT_MARGIN 4.76837158203125e-07f
 static void qwide_child(const uint32_t* w, int k, orc_f3 ro, orc_f3 inv, float tmin, float hitT, float* entry,
@@ -1279,25 +1289,6 @@ static void qwide_child(const uint32_t* w, int k, orc_f3 ro, orc_f3 inv, float t
     float base[3];
     memcpy(base, w, 12);
     const float r[3] = {ro.x, ro.y, ro.z}, iv[3] = {inv.x, inv.y, inv.z};
-    /* a ray with some |inv| or |ro| of 2^62 or more (a zero direction
-     * component: inv clamped to +-FLT_MAX) takes the planes relative to the
-     * ray origin (base - ro plus V, directed adds) and the reference's slab */
-    const float lim = 4.611686018427387904e18f; /* 2^62 */
-    const int fits = fabsf(iv[0]) < lim && fabsf(iv[1]) < lim && fabsf(iv[2]) < lim && fabsf(r[0]) < lim &&
-                     fabsf(r[1]) < lim && fabsf(r[2]) < lim;
-    if (!fits)
-    {
-        float dl[3], dh[3], rmin, rmax;
-        for (int a = 0; a < 3; ++a)
-        {
-            dl[a] = add_dir(add_dir(base[a], -r[a], 0), qw_value(w[6 + 2 * a], w[3 + a], k), 0);
-            dh[a] = add_dir(add_dir(base[a], -r[a], 1), qw_value(w[7 + 2 * a], w[3 + a], k), 1);
-        }
-        slabs_offsets(f3(dl[0], dl[1], dl[2]), f3(dh[0], dh[1], dh[2]), inv, hitT, &rmin, &rmax);
-        *entry = smax(rmin, tmin);
-        *exitOut = rmax;
-        return;
-    }
     float en = 0.0f, ex = 0.0f;
     for (int a = 0; a < 3; ++a)
     {
@@ -1531,7 +1522,7 @@ static void wide_range(void* p, uint32_t b, uint32_t e)
         hit_init(&hit, r->tmax);
         uint32_t nv = 0, nt = 0, nr = 0;
         uint32_t start = is_leaf(c->root) ? ORC_LEAF_BIT : c->root;
-        if (c->fallback)
+        if (c->fallback || (c->qwide && !qwide_ray_fits(ro, inv_rd(rd))))
             stackfree_walk(&hit, c->nodes, c->tris, c->root, ORC_INVALID, ro, rd, inv_rd(rd), r->tmin, c->any, &nv,
                            &nt);
         else if (c->any)

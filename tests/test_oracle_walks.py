@@ -314,11 +314,13 @@ def test_wide_closest_stack_overflow_restarts_with_stackfree_walk():
         assert nr.sum() > 0
 
 
-def test_quantised_wide_rays_with_zero_direction_components_keep_culling():
-    """Rays with a zero direction component (inv clamped to +-FLT_MAX, where the
-    slot's FMA form would overflow) take the position-space form on such slots
-    and still cull: the quantised walks visit about as many slots as the FP32
-    ones, with the same hits."""
+def test_quantised_wide_rays_with_zero_direction_components_take_the_stackfree_walk():
+    """A ray with a zero direction component (the reference clamps its
+    inverse to +-FLT_MAX) could overflow the quantised slots' FMA form, which
+    would lose its culling (an earlier form visited up to 22,040 slots per
+    such ray). Such rays take the stack-free walk over the binary tree: the
+    reference's Hit records and visit counts exactly. Rays that fit keep the
+    quantised walk, with the FP32 walk's hits."""
     tris = scenes.gaussian_soup(50000, clusters=8, seed=5)
     b = O.build(tris)
     wide = O.build_wide(b["nodes"], len(tris))
@@ -327,18 +329,23 @@ def test_quantised_wide_rays_with_zero_direction_components_keep_culling():
     rays = np.zeros((3000, 8), np.float32)
     rays[:, 0:3] = rng.uniform(-0.2, 1.2, (3000, 3))
     d = rng.standard_normal((3000, 3))
-    d[np.arange(3000), rng.integers(0, 3, 3000)] = 0.0  # one zero component per ray
-    d[:1000:7, :] *= [0.0, 1.0, 0.0]                    # some rays along an axis
+    d[:2000][np.arange(2000), rng.integers(0, 3, 2000)] = 0.0  # one zero component
+    d[:700:7, :] *= [0.0, 1.0, 0.0]                          # some rays along an axis
     rays[:, 4:7] = d / np.linalg.norm(d, axis=1, keepdims=True)
     rays[:, 7] = np.float32(3.402823466e38)
+    zero = (rays[:, 4:7] == 0).any(1)
     for query in (1, 0):
-        got, nv, _, nr = O.trace_wide_quantised(q, b["nodes"], tris, b["root"], rays, query=query)
+        got, nv, nt, nr = O.trace_wide_quantised(q, b["nodes"], tris, b["root"], rays, query=query)
+        sf, nv0, nt0 = O.trace(b["nodes"], tris, b["root"], rays, query, 0, counters=True)
+        np.testing.assert_array_equal(got[zero], sf[zero])
+        np.testing.assert_array_equal(nv[zero], nv0[zero])
+        np.testing.assert_array_equal(nt[zero], nt0[zero])
         ref, nv32, _, _ = O.trace_wide(wide, b["nodes"], tris, b["root"], rays, query=query)
         if query:
             np.testing.assert_array_equal(got[:, 7] == MISS, ref[:, 7] == MISS)
         else:
             np.testing.assert_array_equal(got, ref)
-        assert nv.sum() < 1.3 * nv32.sum() and nv.max() < 2 * nv32.max() + 64 and nr.sum() == 0
+        assert nv[~zero].sum() < 1.3 * nv32[~zero].sum() and nr.sum() == 0
 
 
 def test_quantised_wide_slots_refuse_coordinates_beyond_2_60():
