@@ -32,7 +32,7 @@ constexpr int kBoundsThreads = 256;
 constexpr int kBoundsMaxBlocks = 1024;
 constexpr int kKeysThreads = 256;
 constexpr int kSortTile = sort::kTile;  // 4096 keys per tile
-constexpr int kBuildThreads = 256;
+constexpr int kBuildThreads = (int)kTileLeaves;
 constexpr uint32_t kDefaultSpinLimit = 1u << 22;
 
 // Scratch layout of one build (offsets from the caller's dScratch). The
@@ -218,21 +218,24 @@ __global__ void __launch_bounds__(kKeysThreads)
 }
 
 
-// One thread per sorted leaf of the single-mesh build.
+// One thread per sorted leaf of the single-mesh build, one CTA per tile of
+// 256 leaves (climb_tile: the tile's own nodes meet in shared memory).
+static_assert(kBuildThreads == (int)kTileLeaves, "one thread per leaf of a tile");
 __global__ void __launch_bounds__(kBuildThreads)
     k_build(const float* __restrict__ tris, uint32_t n, const uint32_t* __restrict__ sortedKeys,
             const uint32_t* __restrict__ sortedIdx, mlbvh_internal_node* __restrict__ nodes,
             uint32_t* __restrict__ handoff, mlbvh_node_index* __restrict__ root, uint8_t* __restrict__ deltas)
 {
-    __shared__ float s_box[kBuildThreads * 6];
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    __shared__ TileClimbShared sh;
+    const uint32_t t0 = blockIdx.x * kTileLeaves;
+    const uint32_t i = t0 + threadIdx.x;
     // tri >= n only after a sort whose bounded wait gave up (error word set)
     const uint32_t tri = i < n ? sortedIdx[i] : 0xFFFFFFFFu;
     f3 lo = mk(0.0f, 0.0f, 0.0f), hi = lo;
     if (tri < n) leaf_box(tris, n, tri, lo, hi);
-    stage_leaf_box(s_box, threadIdx.x, tri < n, lo, hi);
+    tile_climb_prepare(sh, sortedKeys, n, t0);
     if (tri >= n) return;
-    climb(n, i, tri, lo, hi, sortedKeys, nodes, handoff, root, deltas, s_box, threadIdx.x, blockDim.x - 1);
+    climb_tile(sh, t0, n, i, tri, lo, hi, sortedKeys, nodes, handoff, root, deltas);
 }
 
 }  // namespace

@@ -197,4 +197,166 @@ __device__ __forceinline__ void climb(uint32_t n, uint32_t i, uint32_t tri, f3 l
     if (!(node & kLeafBit)) nodes[node].parent = kInvalid;
 }
 
+// ------------------------------------------------------------ tile climb
+// build_lbvh (minimum_lbvh.h:284-361) with the hand-offs of a CTA's own nodes
+// in shared memory. A CTA holds the leaves [t0, t1] of one tile. The range
+// [L, U] of internal node p (split between leaves p and p + 1) follows from
+// the split deltas alone: L = 1 + the nearest j < p with delta(j) >= delta(p),
+// U = the nearest k > p with delta(k) > delta(p) (deltas outside [0, n - 2]
+// count as infinite), which is the range the climb gives p (its parent rule
+// goes left exactly when delta(lo - 1) < delta(hi)). A node whose range lies
+// in the tile is "interior": both walkers that reach it climb from leaves of
+// this CTA, so they meet through a shared-memory hand-off word and a
+// shared-memory copy of each child's box, ordered at block scope. Every other
+// node (its range crosses a tile boundary; a few per cent of them) takes the
+// GPU-scope acquire-release hand-off of climb(). Both walkers of a node
+// decide alike, since each decides from the same deltas. The node words
+// written are climb()'s.
+// leaves per tile = threads per CTA of the tile climb (build-time override for sweeps: -DMLBVH_BUILD_TILE=...)
+#ifndef MLBVH_BUILD_TILE
+#define MLBVH_BUILD_TILE 64
+#endif
+constexpr uint32_t kTileLeaves = MLBVH_BUILD_TILE;
+struct TileClimbShared {
+    uint32_t delta[kTileLeaves + 1];  // delta(t0 - 1 + j), j = 0 .. kTileLeaves
+    uint32_t hand[kTileLeaves];       // hand-off word of node t0 + j
+    uint32_t interior[kTileLeaves / 32];
+    float box[kTileLeaves][2][6];     // child boxes of node t0 + j (index: the child's side)
+};
+
+// Stages the tile's deltas, resets its hand-off words and marks its interior
+// nodes; every thread of the CTA calls it (it ends with a barrier). keys: the
+// sorted Morton keys of all n leaves. Node p is interior exactly when some
+// delta(j), t0 - 1 <= j < p, is >= delta(p) (then L(p) >= t0) and some
+// delta(k), p < k <= t1, is > delta(p) (then U(p) <= t1): delta(p) against the
+// exclusive prefix and suffix maxima of the tile's deltas, two max-scans of
+// the CTA (warp shuffles, then the warps' totals). Needs blockDim.x ==
+// kTileLeaves.
+__device__ __forceinline__ void tile_climb_prepare(TileClimbShared& sh, const uint32_t* __restrict__ keys, uint32_t n,
+                                                   uint32_t t0)
+{
+    __shared__ uint32_t s_warpMax[2][kTileLeaves / 32];
+    const uint32_t t1 = min(t0 + kTileLeaves - 1, n - 1);
+    const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    for (uint32_t j = tid; j <= kTileLeaves; j += blockDim.x) {
+        const long long g = (long long)t0 - 1 + j;  // delta index
+        sh.delta[j] = (g >= 0 && g + 1 < (long long)n && g <= (long long)t1) ? delta_at(keys, (uint32_t)g) : 0xFFFFFFFFu;
+    }
+    sh.hand[tid] = 0xFFFFFFFFu;
+    __syncthreads();
+    // prefix: max of delta(t0 - 1 .. t0 - 1 + tid), i.e. of the deltas left of node t0 + tid
+    uint32_t pre = sh.delta[tid];
+    // suffix: max of delta(t0 + tid .. t1)
+    uint32_t suf = t0 + tid <= t1 ? sh.delta[tid + 1] : 0u;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t a = __shfl_up_sync(0xffffffffu, pre, o);
+        const uint32_t b = __shfl_down_sync(0xffffffffu, suf, o);
+        if (lane >= (uint32_t)o) pre = max(pre, a);
+        if (lane + o < 32) suf = max(suf, b);
+    }
+    if (lane == 31) s_warpMax[0][warp] = pre;
+    if (lane == 0) s_warpMax[1][warp] = suf;
+    __syncthreads();
+    uint32_t carry = 0u;  // max of the later warps' deltas
+    for (uint32_t w = 0; w < warp; ++w) pre = max(pre, s_warpMax[0][w]);
+    for (uint32_t w = warp + 1; w < kTileLeaves / 32; ++w) carry = max(carry, s_warpMax[1][w]);
+    suf = max(suf, carry);
+    // node p = t0 + tid needs the suffix from delta(p + 1): the next thread's (the later warps' for lane 31)
+    uint32_t sufNext = __shfl_down_sync(0xffffffffu, suf, 1);
+    if (lane == 31) sufNext = carry;
+    const uint32_t p = t0 + tid, dp = sh.delta[tid + 1];
+    const bool interior = p < t1 && dp <= pre && dp < sufNext;
+    const uint32_t mask = __ballot_sync(0xffffffffu, interior);
+    if (lane == 0) sh.interior[warp] = mask;
+    __syncthreads();
+}
+
+// The climb of sorted leaf i (triangle `tri`, box lo/hi) of a tile prepared
+// by tile_climb_prepare. Node words, parent links, root: as climb().
+__device__ __forceinline__ void climb_tile(TileClimbShared& sh, uint32_t t0, uint32_t n, uint32_t i, uint32_t tri,
+                                           f3 lo, f3 hi, const uint32_t* __restrict__ sortedKeys,
+                                           mlbvh_internal_node* __restrict__ nodes, uint32_t* __restrict__ handoff,
+                                           mlbvh_node_index* __restrict__ root, uint8_t* __restrict__ deltas)
+{
+    const uint32_t nInternals = n - 1;
+    const uint32_t t1 = min(t0 + kTileLeaves - 1, n - 1);
+    // delta(g) from the tile's copy where it holds it, else from the keys
+    auto delta_of = [&](uint32_t g) -> uint32_t {
+        if (g + 1 >= t0 && g <= t1) return sh.delta[g + 1 - t0];
+        return delta_at(sortedKeys, g);
+    };
+    if (deltas && i < nInternals) deltas[i] = (uint8_t)sh.delta[i + 1 - t0];
+
+    uint32_t leafLower = i, leafUpper = i;
+    uint32_t deltaL = 0 < leafLower ? delta_of(leafLower - 1) : 0xFFFFFFFFu;
+    uint32_t deltaR = leafUpper < nInternals ? delta_of(leafUpper) : 0xFFFFFFFFu;
+    uint32_t node = tri | kLeafBit;
+    while (leafUpper - leafLower < nInternals) {
+        const int goLeft = deltaL < deltaR ? 1 : 0;
+        const uint32_t parent = goLeft ? leafLower - 1 : leafUpper;
+
+        mlbvh_internal_node* p = nodes + parent;
+        float* pw = reinterpret_cast<float*>(p);
+        p->children[goLeft] = node;
+        if (goLeft) {  // aabbs[1]: bytes 32-55
+            *reinterpret_cast<float4*>(pw + 8) = make_float4(lo.x, lo.y, lo.z, hi.x);
+            *reinterpret_cast<float2*>(pw + 12) = make_float2(hi.y, hi.z);
+        } else {  // aabbs[0]: bytes 8-31
+            *reinterpret_cast<float2*>(pw + 2) = make_float2(lo.x, lo.y);
+            *reinterpret_cast<float4*>(pw + 4) = make_float4(lo.z, hi.x, hi.y, hi.z);
+        }
+        if (!(node & kLeafBit)) nodes[node].parent = parent;
+
+        const uint32_t j = parent - t0;  // wraps (large) below the tile
+        const bool interior = j < kTileLeaves && ((sh.interior[j >> 5] >> (j & 31)) & 1u);
+        const uint32_t mine = goLeft ? leafUpper : leafLower;
+        uint32_t other;
+        f3 olo, ohi;
+        if (interior) {
+            float* b = sh.box[j][goLeft];
+            b[0] = lo.x; b[1] = lo.y; b[2] = lo.z; b[3] = hi.x; b[4] = hi.y; b[5] = hi.z;
+            __threadfence_block();
+            other = atomicExch(sh.hand + j, mine);
+            if (other == 0xFFFFFFFFu) return;  // first arrival: the sibling finishes this node
+            __threadfence_block();
+            const float* ob = sh.box[j][1 - goLeft];
+            olo = mk(ob[0], ob[1], ob[2]);
+            ohi = mk(ob[3], ob[4], ob[5]);
+        } else {
+            other = exch_acq_rel(handoff + parent, mine);
+            if (other == 0xFFFFFFFFu) return;
+            if (goLeft) {  // the sibling is child 0
+                const float2 a = __ldcg(reinterpret_cast<const float2*>(pw + 2));
+                const float4 c = __ldcg(reinterpret_cast<const float4*>(pw + 4));
+                olo = mk(a.x, a.y, c.x);
+                ohi = mk(c.y, c.z, c.w);
+            } else {
+                const float4 a = __ldcg(reinterpret_cast<const float4*>(pw + 8));
+                const float2 c = __ldcg(reinterpret_cast<const float2*>(pw + 12));
+                olo = mk(a.x, a.y, a.z);
+                ohi = mk(a.w, c.x, c.y);
+            }
+        }
+        if (other < leafLower) {
+            leafLower = other;
+            deltaL = 0 < leafLower ? delta_of(leafLower - 1) : 0xFFFFFFFFu;
+        } else {
+            leafUpper = other;
+            deltaR = leafUpper < nInternals ? delta_of(leafUpper) : 0xFFFFFFFFu;
+        }
+        p->context = leafUpper < nInternals ? leafUpper : 0xFFFFFFFFu;
+        if (goLeft) {  // this walker is child 1
+            lo = smin3(lo, olo);
+            hi = smax3(hi, ohi);
+        } else {
+            lo = smin3(olo, lo);
+            hi = smax3(ohi, hi);
+        }
+        node = parent;
+    }
+    *root = node;
+    if (!(node & kLeafBit)) nodes[node].parent = kInvalid;
+}
+
 }  // namespace mlbvh
