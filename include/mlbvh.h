@@ -414,12 +414,16 @@ MLBVH_API mlbvh_status mlbvh_leaf_triangles(const mlbvh_internal_node* dInternal
  * for one triangle), 128-byte aligned. No reference counterpart. */
 MLBVH_API mlbvh_status mlbvh_build_wide(const mlbvh_internal_node* dInternals, const mlbvh_node_index* dRootNode,
                                         uint32_t nTriangles, mlbvh_wnode* dWideNodes, void* stream);
-/* Any-hit rays over the 4-wide tree (rayQuery must be MLBVH_RAY_QUERY_ANY):
- * a ray has a hit exactly when mlbvh_trace's any-hit walk finds one; the Hit
- * record is that of the first triangle this walk finds (the reference's walk
- * may stop at another one). dLeafTriangles from mlbvh_leaf_triangles. A
- * ray whose stack (24 entries) would overflow restarts with the stack-free
- * walk over dInternals / dTriangles. dCounts (may be NULL; 3 * nRays words,
+/* Rays over the 4-wide tree, one thread per ray. MLBVH_RAY_QUERY_ANY: a ray
+ * has a hit exactly when mlbvh_trace's any-hit walk finds one; the Hit record
+ * is that of the first triangle this walk finds (the reference's walk may
+ * stop at another one). MLBVH_RAY_QUERY_CLOSEST: children are entered nearest
+ * first and pending ones skipped once beyond hit.t; the Hit record is
+ * intersect_stackfree's, except that where two triangles meet the ray at
+ * bit-identical t either may report. dLeafTriangles from
+ * mlbvh_leaf_triangles. A ray whose stack (24 entries) would overflow
+ * continues with the stack-free walk over dInternals / dTriangles, keeping
+ * its hit. dCounts (may be NULL; 3 * nRays words,
  * nRays < 2^30) receives per ray the node visits (wide nodes, then binary
  * nodes after a restart), triangle tests and restarts at [i], [nRays + i],
  * [2 nRays + i]. */
@@ -435,8 +439,12 @@ MLBVH_API mlbvh_status mlbvh_trace_wide(const mlbvh_wnode* dWideNodes, const mlb
  * every ray (the same answers, slower). No reference counterpart. */
 MLBVH_API mlbvh_status mlbvh_quantise_wide(const mlbvh_wnode* dWideNodes, uint32_t nTriangles,
                                            mlbvh_qwnode* dQWideNodes, uint32_t* dStatus, void* stream);
-/* mlbvh_trace_wide over the quantised slots (any-hit only; a hit counts only
- * where the triangle's exact box passes the slab test as well). */
+/* mlbvh_trace_wide over the quantised slots (either query; a hit counts only
+ * where the triangle's exact box passes the slab test as well, so the answers
+ * are mlbvh_trace_wide's). A ray with a direction component of magnitude
+ * below 2^-62 (the reference clamps its inverse to +-FLT_MAX) or an origin
+ * coordinate of 2^62 or more takes the stack-free walk over dInternals
+ * instead, as every ray does when *dStatus is set. */
 MLBVH_API mlbvh_status mlbvh_trace_wide_quantised(const mlbvh_qwnode* dQWideNodes, const uint32_t* dStatus,
                                                   const mlbvh_internal_node* dInternals,
                                                   const mlbvh_node_index* dRootNode, const mlbvh_triangle* dTriangles,
