@@ -12,7 +12,11 @@ namespace mlbvh {
 namespace {
 
 constexpr int kWideThreads = 256;
-constexpr int kWideTraceThreads = 128;
+// threads per CTA of the wide trace kernel (build-time override for sweeps: -DMLBVH_WIDE_TRACE_THREADS=...)
+#ifndef MLBVH_WIDE_TRACE_THREADS
+#define MLBVH_WIDE_TRACE_THREADS 128
+#endif
+constexpr int kWideTraceThreads = MLBVH_WIDE_TRACE_THREADS;
 
 struct WideKid {
     uint32_t name;  // internal index, kLeafBit | leaf position, or kWideEmpty
