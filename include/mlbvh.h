@@ -533,10 +533,10 @@ MLBVH_API const mlbvh_triangle_attrib* mlbvh_obj_attribs(const mlbvh_obj_mesh* m
 MLBVH_API void mlbvh_obj_free(mlbvh_obj_mesh* mesh);
 
 /* Profiling hook (no reference counterpart; the reference times whole calls
- * with its DeviceStopwatch, minimum_lbvh.h:693-724): the next mlbvh_render_ao
- * or mlbvh_build on this host thread records the two cudaEvent_t handles
- * around its dominant kernel (the AO-ray kernel, resp. the agglomerative
- * build kernel). NULL, NULL cancels. */
+ * with its DeviceStopwatch, minimum_lbvh.h:693-724): the next mlbvh_render_ao,
+ * mlbvh_build or mlbvh_build_batched on this host thread records the two
+ * cudaEvent_t handles around its dominant kernel (the AO-ray kernel, resp. the
+ * agglomerative build kernel). NULL, NULL cancels. */
 MLBVH_API void mlbvh_profile_events(void* startEvent, void* stopEvent);
 
 /* Measurement hook (no reference counterpart): one launch that reads dBuffer

@@ -20,7 +20,7 @@
 //                     histograms per mesh, reset of the hand-off words
 //   k_onesweep x P    segmented Onesweep passes (onesweep.cuh), one segment
 //                     per mesh; P = 4 (8-bit digits) or 3 (11-bit digits)
-//   k_batch_build     one thread per sorted leaf: the climb of mlbvh_build
+//   k_batch_build     one thread per sorted leaf: the tile climb of mlbvh_build
 //
 // Traversal: k_batch_trace is persistent (one grid of resident CTAs). A warp
 // takes `queueChunk` consecutive rays per atomic on the queue counter and
@@ -45,7 +45,7 @@ namespace {
 constexpr int kPlanThreads = 1024;
 constexpr int kTileThreads = 256;  // bounds / keys kernels: one CTA per sort tile
 constexpr int kStageTris = 256;    // triangles staged in shared memory per step
-constexpr int kBuildThreads = 256;
+constexpr int kBuildThreads = (int)kTileLeaves;  // build: one CTA per tile of the climb
 constexpr uint32_t kDefaultSpinLimit = 1u << 22;
 constexpr uint32_t kMaxMeshes = 1u << 20;
 constexpr uint32_t kErrTimeout = 1u, kErrOffsets = 2u;
@@ -358,28 +358,37 @@ __global__ void __launch_bounds__(kTileThreads)
 }
 
 
-// build_lbvh (minimum_lbvh.h:284-361), one thread per sorted leaf: the climb
-// of the single-mesh build over the arrays of the leaf's mesh.
+// build_lbvh (minimum_lbvh.h:284-361), one thread per sorted leaf: the tile
+// climb of the single-mesh build, over tiles of kTileLeaves consecutive leaves
+// of the whole batch. A tile may hold the end of one mesh and the start of the
+// next: the delta across a mesh boundary is staged as infinite (the value each
+// mesh's climb gives the deltas outside its range), so each node's range, and
+// with it its interior test, stays inside its mesh.
+static_assert(kBuildThreads == (int)kTileLeaves, "one thread per leaf of a tile");
 __global__ void __launch_bounds__(kBuildThreads)
     k_batch_build(const float* __restrict__ tris, uint32_t n, const uint32_t* __restrict__ off, uint32_t nMeshes,
                   const uint32_t* __restrict__ sortedKeys, const uint32_t* __restrict__ sortedIdx,
                   mlbvh_internal_node* __restrict__ allNodes, uint32_t* __restrict__ allHandoff,
                   mlbvh_node_index* __restrict__ roots, const uint32_t* __restrict__ header)
 {
-    const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
-    if (g >= n || (__ldcg(header + kHdrError) & kErrOffsets)) return;
-    const uint32_t m = find_segment(off, nMeshes, g);
-    const uint32_t start = __ldg(off + m);
-    const uint32_t len = __ldg(off + m + 1) - start;
-    const uint32_t tri = sortedIdx[g];
-    if (tri >= len) return;  // only after a sort whose bounded wait gave up (error word set)
-    f3 lo, hi;
-    leaf_box(tris + 9 * (size_t)start, len, tri, lo, hi);
-    // no leaf pairs here (t = 0, tLast = -1): a CTA's threads span several
-    // meshes, and the barrier of the staging step would hold every thread
-    // for the CTA's slowest mesh lookup (measured slower on 1,024 meshes)
-    climb(len, g - start, tri, lo, hi, sortedKeys + start, allNodes + (start - m), allHandoff + (start - m),
-          roots + m, nullptr, nullptr, 0, -1);
+    __shared__ TileClimbShared sh;
+    if (__ldcg(header + kHdrError) & kErrOffsets) return;  // the whole CTA: the plan's word is set before
+    const uint32_t t0 = blockIdx.x * kTileLeaves;
+    const uint32_t g = t0 + threadIdx.x;
+    uint32_t m = 0, start = n, end = n, tri = 0xFFFFFFFFu;
+    f3 lo = mk(0.0f, 0.0f, 0.0f), hi = lo;
+    if (g < n) {
+        m = find_segment(off, nMeshes, g);
+        start = __ldg(off + m);
+        end = __ldg(off + m + 1);
+        tri = sortedIdx[g];
+        // tri >= the mesh's size only after a sort whose bounded wait gave up (error word set)
+        if (tri < end - start) leaf_box(tris + 9 * (size_t)start, end - start, tri, lo, hi);
+    }
+    tile_climb_prepare(sh, sortedKeys, n, t0, start, end);
+    if (g >= n || tri >= end - start) return;
+    climb_tile(sh, t0 - start, end - start, g - start, tri, lo, hi, sortedKeys + start, allNodes + (start - m),
+               allHandoff + (start - m), roots + m, nullptr);
 }
 
 // The persistent traversal (see the file comment). Hits are written as
@@ -562,9 +571,12 @@ mlbvh_status launch_build(const mlbvh_batch& B, const BatchLayout& L, cudaStream
         kin = kout;
         vin = vout;
     }
+    const ProfileEvents ev = take_profile_events();
+    if (ev.start) cudaEventRecord(ev.start, stream);
     k_batch_build<<<(n + kBuildThreads - 1) / kBuildThreads, kBuildThreads, 0, stream>>>(
         tris, n, off, nm, kin, vin, B.dInternals, handoff, B.dRootNodes, header);
     MLBVH_CHECK_LAUNCH("k_batch_build");
+    if (ev.stop) cudaEventRecord(ev.stop, stream);
     return MLBVH_OK;
 }
 

@@ -219,7 +219,7 @@ __global__ void __launch_bounds__(kKeysThreads)
 
 
 // One thread per sorted leaf of the single-mesh build, one CTA per tile of
-// 256 leaves (climb_tile: the tile's own nodes meet in shared memory).
+// kTileLeaves leaves (climb_tile: the tile's own nodes meet in shared memory).
 static_assert(kBuildThreads == (int)kTileLeaves, "one thread per leaf of a tile");
 __global__ void __launch_bounds__(kBuildThreads)
     k_build(const float* __restrict__ tris, uint32_t n, const uint32_t* __restrict__ sortedKeys,
@@ -233,7 +233,7 @@ __global__ void __launch_bounds__(kBuildThreads)
     const uint32_t tri = i < n ? sortedIdx[i] : 0xFFFFFFFFu;
     f3 lo = mk(0.0f, 0.0f, 0.0f), hi = lo;
     if (tri < n) leaf_box(tris, n, tri, lo, hi);
-    tile_climb_prepare(sh, sortedKeys, n, t0);
+    tile_climb_prepare(sh, sortedKeys, n, t0, 0u, n);
     if (tri >= n) return;
     climb_tile(sh, t0, n, i, tri, lo, hi, sortedKeys, nodes, handoff, root, deltas);
 }

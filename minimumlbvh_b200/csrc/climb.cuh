@@ -226,22 +226,29 @@ struct TileClimbShared {
 
 // Stages the tile's deltas, resets its hand-off words and marks its interior
 // nodes; every thread of the CTA calls it (it ends with a barrier). keys: the
-// sorted Morton keys of all n leaves. Node p is interior exactly when some
+// sorted Morton keys of all n leaves. Leaves may belong to several trees laid
+// end to end (the batched build): [segStart, segEnd) is the range of the tree
+// of this thread's leaf t0 + threadIdx.x ([0, n) for a single tree; a thread
+// past the last leaf passes segEnd <= its leaf + 1). The delta between the
+// last leaf of one tree and the first of the next is staged as infinite, the
+// value the climb of each tree gives the deltas outside its own range, so no
+// node range crosses a tree boundary. Node p is interior exactly when some
 // delta(j), t0 - 1 <= j < p, is >= delta(p) (then L(p) >= t0) and some
 // delta(k), p < k <= t1, is > delta(p) (then U(p) <= t1): delta(p) against the
 // exclusive prefix and suffix maxima of the tile's deltas, two max-scans of
 // the CTA (warp shuffles, then the warps' totals). Needs blockDim.x ==
 // kTileLeaves.
 __device__ __forceinline__ void tile_climb_prepare(TileClimbShared& sh, const uint32_t* __restrict__ keys, uint32_t n,
-                                                   uint32_t t0)
+                                                   uint32_t t0, uint32_t segStart, uint32_t segEnd)
 {
     __shared__ uint32_t s_warpMax[2][kTileLeaves / 32];
     const uint32_t t1 = min(t0 + kTileLeaves - 1, n - 1);
     const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    for (uint32_t j = tid; j <= kTileLeaves; j += blockDim.x) {
-        const long long g = (long long)t0 - 1 + j;  // delta index
-        sh.delta[j] = (g >= 0 && g + 1 < (long long)n && g <= (long long)t1) ? delta_at(keys, (uint32_t)g) : 0xFFFFFFFFu;
-    }
+    // slot j holds delta(t0 - 1 + j): slot tid + 1 the delta right of this
+    // thread's leaf, slot 0 the one left of the tile
+    const uint32_t g = t0 + tid;
+    sh.delta[tid + 1] = g + 1 < segEnd ? delta_at(keys, g) : 0xFFFFFFFFu;
+    if (tid == 0) sh.delta[0] = t0 > segStart ? delta_at(keys, t0 - 1) : 0xFFFFFFFFu;
     sh.hand[tid] = 0xFFFFFFFFu;
     __syncthreads();
     // prefix: max of delta(t0 - 1 .. t0 - 1 + tid), i.e. of the deltas left of node t0 + tid
@@ -272,21 +279,25 @@ __device__ __forceinline__ void tile_climb_prepare(TileClimbShared& sh, const ui
     __syncthreads();
 }
 
-// The climb of sorted leaf i (triangle `tri`, box lo/hi) of a tile prepared
-// by tile_climb_prepare. Node words, parent links, root: as climb().
-__device__ __forceinline__ void climb_tile(TileClimbShared& sh, uint32_t t0, uint32_t n, uint32_t i, uint32_t tri,
-                                           f3 lo, f3 hi, const uint32_t* __restrict__ sortedKeys,
+// The climb of sorted leaf i (triangle `tri`, box lo/hi) of a tree of n
+// leaves, in a tile prepared by tile_climb_prepare. tileBase: the tree's own
+// index of the tile's first leaf, modulo 2^32 (t0 for a single tree; below 0,
+// wrapped, for a tree that starts inside the tile). sortedKeys, nodes,
+// handoff, root: the tree's own arrays. Node words, parent links, root: as
+// climb().
+__device__ __forceinline__ void climb_tile(TileClimbShared& sh, uint32_t tileBase, uint32_t n, uint32_t i,
+                                           uint32_t tri, f3 lo, f3 hi, const uint32_t* __restrict__ sortedKeys,
                                            mlbvh_internal_node* __restrict__ nodes, uint32_t* __restrict__ handoff,
                                            mlbvh_node_index* __restrict__ root, uint8_t* __restrict__ deltas)
 {
     const uint32_t nInternals = n - 1;
-    const uint32_t t1 = min(t0 + kTileLeaves - 1, n - 1);
-    // delta(g) from the tile's copy where it holds it, else from the keys
+    // delta(g), 0 <= g < n - 1, from the tile's copy where it holds it (slot
+    // g + 1 - tileBase, wrapping large left of the tile), else from the keys
     auto delta_of = [&](uint32_t g) -> uint32_t {
-        if (g + 1 >= t0 && g <= t1) return sh.delta[g + 1 - t0];
-        return delta_at(sortedKeys, g);
+        const uint32_t s = g + 1 - tileBase;
+        return s <= kTileLeaves ? sh.delta[s] : delta_at(sortedKeys, g);
     };
-    if (deltas && i < nInternals) deltas[i] = (uint8_t)sh.delta[i + 1 - t0];
+    if (deltas && i < nInternals) deltas[i] = (uint8_t)sh.delta[i + 1 - tileBase];
 
     uint32_t leafLower = i, leafUpper = i;
     uint32_t deltaL = 0 < leafLower ? delta_of(leafLower - 1) : 0xFFFFFFFFu;
@@ -308,7 +319,7 @@ __device__ __forceinline__ void climb_tile(TileClimbShared& sh, uint32_t t0, uin
         }
         if (!(node & kLeafBit)) nodes[node].parent = parent;
 
-        const uint32_t j = parent - t0;  // wraps (large) below the tile
+        const uint32_t j = parent - tileBase;  // wraps (large) below the tile
         const bool interior = j < kTileLeaves && ((sh.interior[j >> 5] >> (j & 31)) & 1u);
         const uint32_t mine = goLeft ? leafUpper : leafLower;
         uint32_t other;

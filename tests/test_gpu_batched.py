@@ -82,6 +82,21 @@ def test_batched_build_matches_oracle(cuda, bits):
     _check_meshes(bb, tris, offsets)
 
 
+def test_batched_build_many_meshes_per_tile(cuda):
+    """The climb's tiles of 64 consecutive sorted leaves hold the ends and
+    starts of many meshes here: 300 meshes of 1 to 7 triangles, then meshes
+    of 63, 64, 65 and 127 triangles (boundaries on and beside tile edges)."""
+    rng = np.random.default_rng(17)
+    sizes = [int(s) for s in rng.integers(1, 8, 300)] + [63, 64, 65, 127, 1, 64]
+    parts = [scenes.gaussian_soup(s, clusters=2, seed=100 + i) for i, s in enumerate(sizes)]
+    offsets = np.concatenate([[0], np.cumsum(sizes)]).astype(np.int64)
+    tris = np.ascontiguousarray(np.concatenate(parts), np.float32)
+    bb = _batch(tris, offsets)
+    bb.build()
+    bb.status()
+    _check_meshes(bb, tris, offsets)
+
+
 def test_batched_build_use_normal_option(cuda):
     tris, offsets = _small_batch(seed=11)
     bb = _batch(tris, offsets, option=mb.BUILD_OPTION_USE_NORMAL)
