@@ -447,6 +447,29 @@ def bench_precision(args, builder, qtree, wide, d_tris, tris, cam, w, h, dev, st
     }
 
 
+def bench_precision_heightfield(args, dev, stream, max_over_ranks):
+    """The precision configuration on the other scene: the heightfield +
+    icospheres (212,992 triangles), camera rays of every other pixel of a
+    1448x1448 frame (1,048,352 rays, the same count as the soup's), the same
+    forms and checks as bench_precision."""
+    import torch
+    import minimumlbvh_b200 as mb
+    from minimumlbvh_b200 import scenes
+    tris = scenes.heightfield_icospheres()
+    n = len(tris)
+    d_tris = torch.from_numpy(tris).to(dev)
+    builder = mb.BVHGPUBuilder().build(d_tris, n, 0, mb.OnesweepSort(dev.index))
+    builder.status()
+    qtree = mb.QuantisedBVH.from_builder(builder, d_tris)
+    wide = mb.WideBVH.from_builder(builder, d_tris).quantise()
+    w = h = 1448
+    eye, c, up, fovy = scenes.camera_heightfield()
+    cam = mb.RayGenerator().lookat(eye, c, up, fovy, w, h)
+    out = bench_precision(args, builder, qtree, wide, d_tris, tris, cam, w, h, dev, stream, max_over_ranks)
+    out["workload"] = f"heightfield + icospheres ({n:,} triangles)"
+    return out
+
+
 def bench_pt(args, dev, stream, max_over_ranks, reference_gpu=False):
     """Path tracing (pt, main_gpu.cu:179-272) on the 212,992-triangle
     heightfield + icospheres scene with 1 % emissive triangles, 512 x 512,
@@ -1309,6 +1332,7 @@ def main():
         del wides
         builder.build(d_tris, n, 0, sorter)
         precision = bench_precision(args, builder, qtree, wide, d_tris, tris, cam, w, h, dev, stream, max_over_ranks)
+        precision["heightfield"] = bench_precision_heightfield(args, dev, stream, max_over_ranks)
         pt = bench_pt(args, dev, stream, max_over_ranks,
                       reference_gpu=not args.no_reference_gpu and rank == 0 and world == 1)
         diff = None if args.no_diff else bench_diff(args, dev, stream, max_over_ranks)
@@ -1430,7 +1454,7 @@ def main():
     line["chosen"]["plain_node_bytes_per_ray"] = 64 * visits / max(rays_per_frame, 1)
     line["forms"] = form_lines
     line["precision"] = precision
-    line["gpu_launches"] += precision["launches"]
+    line["gpu_launches"] += precision["launches"] + precision["heightfield"]["launches"]
     line["pt"] = pt
     if ploc is not None:
         line["ploc"] = ploc
