@@ -91,18 +91,20 @@ typedef struct mlbvh_triangle_attrib {
 
 /* The quantised tree (no reference counterpart; a replacement node format for
  * the same topology, 32 bytes instead of 64):
- *   origin     the node's box lower corner (FP32), the min of both child boxes
- *   q[c*6+0..2], q[c*6+3..5]  child c's lower / upper corner in steps of
- *              2^(eBase - k_axis) above origin, rounded down / up, so the
- *              decoded box always contains the exact one
+ *   base       per axis a the base b_a (FP32); axis a has the scale 2^E_a
+ *   q[4*a+0..3] the 8-bit codes of axis a: child 0 lower, child 0 upper,
+ *              child 1 lower, child 1 upper. Code q stands for the plane
+ *              b_a + 2^E_a (1 + q / 2^15); lower planes lie at or below the
+ *              exact child box, upper ones at or above it (exact arithmetic)
  *   child[c]   bit 31 leaf flag; bits 0-22 internal-node index or leaf
- *              position; bits 23-30 carry the three 5-bit axis codes k_axis
- *              (child[0]: k_x | k_y bits 0-2; child[1]: k_y bits 3-4 | k_z)
+ *              position; bits 23-30 carry the three 5-bit axis codes
+ *              k_a = eBase - E_a (child[0]: k_x | k_y bits 0-2; child[1]:
+ *              k_y bits 3-4 | k_z)
  * Parents live in a separate array (read only when the walk moves up).
  * Leaves are stored in sorted (leaf) order as mlbvh_qtri: the triangle's three
  * FP32 corners, unchanged, and its original index. */
 typedef struct mlbvh_qnode {
-    float origin[3];
+    float base[3];
     uint8_t q[12];
     uint32_t child[2];
 } mlbvh_qnode;
@@ -112,10 +114,12 @@ typedef struct mlbvh_qtri {
     uint32_t _pad[2];
 } mlbvh_qtri;
 typedef struct mlbvh_qheader {
-    uint32_t root; /* bit 31 leaf flag, bits 0-22 index */
-    int32_t eBase; /* step exponent of code k = 0 */
+    uint32_t root;   /* bit 31 leaf flag, bits 0-22 index */
+    int32_t eBase;   /* the scale exponent of axis code k = 0: E = eBase - k */
     uint32_t nTriangles;
-    uint32_t _pad;
+    uint32_t status; /* bit 0: a base of 2^60 or more or a scale above 2^59 (the walks then
+                        test the decoded boxes with the reference's slabs); bit 1: a
+                        non-finite coordinate (every box then passes) */
 } mlbvh_qheader;
 
 /* The 4-wide tree for any-hit rays (no reference counterpart): a 4-wide

@@ -769,69 +769,144 @@ constexpr uint32_t kQMaxLeaves = 1u << 23;
 
 __device__ __forceinline__ float pow2f(int e) { return __int_as_float((127 + e) << 23); }  // e in [-126, 127]
 
-// The step exponent e of one axis: the smallest e with 255 * 2^e >= d
-// (d >= 0, already rounded up), at least -126.
-__device__ __forceinline__ int step_exponent(float d)
+// Plane code q under scale 2^E stands for V = 2^E (1 + q / 2^15): one byte
+// permute writes q (byte k of `codes`) into mantissa byte 1 of the bits of
+// 2^E, which gives V exactly. A plane is base + V. Used by the quantised
+// binary nodes and the quantised 4-wide slots alike.
+__device__ __forceinline__ float qw_value(uint32_t codes, uint32_t scaleBits, int k)
 {
-    if (!(d >= 1.17549435e-38f)) return -126;  // zero, subnormal (or NaN)
-    int x = (int)((__float_as_uint(d) >> 23) & 0xFFu) - 126;  // d = m * 2^x, m in [0.5, 1)
-    int e = x - 8;
-    if (e < -126) e = -126;
-    if (255.0f * pow2f(e) < d) e += 1;
-    return e;
+    return __uint_as_float(__byte_perm(codes, scaleBits, 0x7604u | ((uint32_t)k << 4)));
 }
+// The quantisers keep every base below 2^60 and every scale at most 2^59
+// (else the tree's status word sends its rays to a walk without the FMA
+// form), so every plane lies below 2^61. A ray whose |inv| and |ro|
+// components are below 2^62 then keeps every term of the FMA form (V inv + C,
+// C = base inv - ro inv) below 2^125, in the float range (qwide_ray_fits,
+// tested once per ray). Other rays (in practice those with a zero direction
+// component, whose inverse the reference clamps to +-FLT_MAX) take a walk
+// without it.
+constexpr float kQBaseLimit = 1.152921504606846976e18f;  // 2^60
+constexpr float kQRayLimit = 4.611686018427387904e18f;   // 2^62
+__device__ __forceinline__ bool qwide_ray_fits(f3 ro, f3 inv)
+{
+    return fmaxf(fmaxf(fabsf(inv.x), fabsf(inv.y)), fmaxf(fabsf(inv.z), fmaxf(fmaxf(fabsf(ro.x), fabsf(ro.y)),
+                                                                               fabsf(ro.z)))) < kQRayLimit;
+}
+// Relative margins of the quantised slab test: 2^-22 below the entry and
+// 2^-21 above the exit (see qnode_test and qwide_visit).
+constexpr float kQEntryMargin = 2.384185791015625e-07f;
+constexpr float kQExitMargin = 4.76837158203125e-07f;
 
-struct QBox {
-    f3 lo0, hi0, lo1, hi1;
+// The per-walk parameters of the quantised binary tree: its scale exponent
+// EB (mlbvh_qheader::eBase), its status word, and whether this ray takes the
+// FMA form (status 0 and qwide_ray_fits).
+struct QParams {
+    int eb;
+    uint32_t status;
+    bool fma;
 };
-
-__device__ __forceinline__ void decode_steps(uint32_t c0, uint32_t c1, int eBase, float& sx, float& sy, float& sz)
+__device__ __forceinline__ QParams qparams(const mlbvh_qheader* __restrict__ header, f3 ro, f3 inv)
 {
-    const uint32_t code = ((c0 >> 23) & 0xFFu) | (((c1 >> 23) & 0xFFu) << 8);
-    int ex = eBase - (int)(code & 31u), ey = eBase - (int)((code >> 5) & 31u), ez = eBase - (int)((code >> 10) & 31u);
-    sx = pow2f(max(ex, -126));
-    sy = pow2f(max(ey, -126));
-    sz = pow2f(max(ez, -126));
+    const int eb = __ldg(&header->eBase);
+    const uint32_t status = __ldg(&header->status);
+    return QParams{eb, status, status == 0u && qwide_ray_fits(ro, inv)};
 }
 
-__device__ __forceinline__ float qlo(float o, float q, float s) { return __fadd_rd(o, q * s); }
-__device__ __forceinline__ float qhi(float o, float q, float s) { return __fadd_ru(o, q * s); }
-// Byte k of w as a float, exactly: the byte permute builds 0x4B0000qq, which
-// is 2^23 + q as a float, and the subtraction of 2^23 is exact.
-__device__ __forceinline__ float qbyte(uint32_t w, int k)
-{
-    return __uint_as_float(__byte_perm(w, 0x4B000000u, 0x7540u + (uint32_t)k)) - 8388608.0f;
-}
-
-struct QNodeView {
-    uint32_t c0, c1;  // leaf flag | 23-bit index
-    QBox box;
+// A quantised node's words: base (3 floats), the codes of axis x, y, z (bytes
+// child 0 lower, child 0 upper, child 1 lower, child 1 upper), the child
+// words (bits 23-30 the axis exponents as k = EB - E, 5 bits each: child 0
+// k_x | k_y bits 0-2, child 1 k_y bits 3-4 | k_z). One 32-byte load.
+struct QNodeWords {
+    f3 base;
+    uint32_t q[3];
+    uint32_t c0, c1;       // leaf flag | 23-bit index
+    uint32_t scale[3];     // bits of 2^E per axis
 };
-template <bool kWide = false>
-__device__ __forceinline__ QNodeView load_qnode(const mlbvh_qnode* __restrict__ qnodes, uint32_t i, int eBase)
+__device__ __forceinline__ QNodeWords load_qnode(const mlbvh_qnode* __restrict__ qnodes, uint32_t i, int eb)
 {
-    const float4* p = reinterpret_cast<const float4*>(qnodes + i);
     float4 a, b;
-    if (kWide) {
-        ldg32(p, a, b);
-    } else {
-        a = __ldg(p);
-        b = __ldg(p + 1);
-    }
-    const uint32_t w0 = __float_as_uint(a.w), w1 = __float_as_uint(b.x), w2 = __float_as_uint(b.y);
-    const uint32_t c0 = __float_as_uint(b.z), c1 = __float_as_uint(b.w);
-    float sx, sy, sz;
-    decode_steps(c0, c1, eBase, sx, sy, sz);
-    const f3 o = mk(a.x, a.y, a.z);
-    QNodeView n;
-    n.c0 = c0 & (kLeafBit | kQIndexMask);
-    n.c1 = c1 & (kLeafBit | kQIndexMask);
-    // q bytes: w0 = q0..q3, w1 = q4..q7, w2 = q8..q11
-    n.box.lo0 = mk(qlo(o.x, qbyte(w0, 0), sx), qlo(o.y, qbyte(w0, 1), sy), qlo(o.z, qbyte(w0, 2), sz));
-    n.box.hi0 = mk(qhi(o.x, qbyte(w0, 3), sx), qhi(o.y, qbyte(w1, 0), sy), qhi(o.z, qbyte(w1, 1), sz));
-    n.box.lo1 = mk(qlo(o.x, qbyte(w1, 2), sx), qlo(o.y, qbyte(w1, 3), sy), qlo(o.z, qbyte(w2, 0), sz));
-    n.box.hi1 = mk(qhi(o.x, qbyte(w2, 1), sx), qhi(o.y, qbyte(w2, 2), sy), qhi(o.z, qbyte(w2, 3), sz));
+    ldg32(reinterpret_cast<const float4*>(qnodes + i), a, b);
+    QNodeWords n;
+    n.base = mk(a.x, a.y, a.z);
+    n.q[0] = __float_as_uint(a.w);
+    n.q[1] = __float_as_uint(b.x);
+    n.q[2] = __float_as_uint(b.y);
+    const uint32_t w6 = __float_as_uint(b.z), w7 = __float_as_uint(b.w);
+    const uint32_t code = ((w6 >> 23) & 0xFFu) | (((w7 >> 23) & 0x7Fu) << 8);
+    const int e127 = eb + 127;
+#pragma unroll
+    for (int a2 = 0; a2 < 3; ++a2) n.scale[a2] = (uint32_t)(e127 - (int)((code >> (5 * a2)) & 31u)) << 23;
+    n.c0 = w6 & (kLeafBit | kQIndexMask);
+    n.c1 = w7 & (kLeafBit | kQIndexMask);
     return n;
+}
+// Child c's decoded box: base + V with V exact, the sum rounded down for the
+// lower planes and up for the upper ones, so it contains the exact box.
+__device__ __forceinline__ void qnode_box(const QNodeWords& n, int c, f3& lo, f3& hi)
+{
+    lo = mk(__fadd_rd(n.base.x, qw_value(n.q[0], n.scale[0], 2 * c)),
+            __fadd_rd(n.base.y, qw_value(n.q[1], n.scale[1], 2 * c)),
+            __fadd_rd(n.base.z, qw_value(n.q[2], n.scale[2], 2 * c)));
+    hi = mk(__fadd_ru(n.base.x, qw_value(n.q[0], n.scale[0], 2 * c + 1)),
+            __fadd_ru(n.base.y, qw_value(n.q[1], n.scale[1], 2 * c + 1)),
+            __fadd_ru(n.base.z, qw_value(n.q[2], n.scale[2], 2 * c + 1)));
+}
+
+// The slab test of both children of a quantised node: (entry, exit) per
+// child, clipped to [max(0, tmin), hitT]; a child passes when entry <= exit.
+// FMA form (qp.fma): a plane's distance along the ray, (base + V - ro) inv,
+// is one FMA, V inv + C, with C = base inv - ro inv bounding (base - ro) inv
+// from below for near planes (ro inv rounded up, the FMA rounded down) and
+// from above for far planes (ro inv rounded down, the FMA rounded up); the
+// plane's FMA is rounded the same way. On an axis whose inv is positive the
+// near plane is the lower one, on one whose inv is negative the upper one.
+// The entry (the largest near distance) is moved down by 2^-22 of itself and
+// the exit (the smallest far one) up by 2^-21 of itself, which covers the
+// reference slab's own rounding on the exact box (two roundings per distance,
+// then its 1.00000024 factor on the exit and that product's rounding); the
+// codes were rounded outward too, so the test passes wherever the reference's
+// passes on the exact box. Otherwise the reference's slabs on the decoded
+// boxes (qnode_box), conservative at any magnitude. A tree with a
+// non-finite coordinate (status bit 1) lets every box pass.
+__device__ __forceinline__ float4 qnode_test(const QNodeWords& n, const QParams& qp, f3 ro, f3 inv, float tmin,
+                                             float hitT)
+{
+    if (qp.status & 2u) {
+        const float lo = fmaxf(0.0f, tmin);
+        return make_float4(lo, hitT, lo, hitT);
+    }
+    if (qp.fma) {
+        const float cnx = __fmaf_rd(n.base.x, inv.x, -__fmul_ru(ro.x, inv.x));
+        const float cny = __fmaf_rd(n.base.y, inv.y, -__fmul_ru(ro.y, inv.y));
+        const float cnz = __fmaf_rd(n.base.z, inv.z, -__fmul_ru(ro.z, inv.z));
+        const float cfx = __fmaf_ru(n.base.x, inv.x, -__fmul_rd(ro.x, inv.x));
+        const float cfy = __fmaf_ru(n.base.y, inv.y, -__fmul_rd(ro.y, inv.y));
+        const float cfz = __fmaf_ru(n.base.z, inv.z, -__fmul_rd(ro.z, inv.z));
+        // per axis the codes ordered (near, far) for each child: where inv is
+        // negative the upper plane is the near one, so its byte pairs swap
+        const uint32_t qx = __byte_perm(n.q[0], 0u, inv.x < 0.0f ? 0x2301u : 0x3210u);
+        const uint32_t qy = __byte_perm(n.q[1], 0u, inv.y < 0.0f ? 0x2301u : 0x3210u);
+        const uint32_t qz = __byte_perm(n.q[2], 0u, inv.z < 0.0f ? 0x2301u : 0x3210u);
+        const float lo = fmaxf(0.0f, tmin);
+        float r[4];
+#pragma unroll
+        for (int c = 0; c < 2; ++c) {
+            const float en = fmaxf(fmaxf(__fmaf_rd(qw_value(qx, n.scale[0], 2 * c), inv.x, cnx),
+                                         __fmaf_rd(qw_value(qy, n.scale[1], 2 * c), inv.y, cny)),
+                                   __fmaf_rd(qw_value(qz, n.scale[2], 2 * c), inv.z, cnz));
+            const float ex = fminf(fminf(__fmaf_ru(qw_value(qx, n.scale[0], 2 * c + 1), inv.x, cfx),
+                                         __fmaf_ru(qw_value(qy, n.scale[1], 2 * c + 1), inv.y, cfy)),
+                                   __fmaf_ru(qw_value(qz, n.scale[2], 2 * c + 1), inv.z, cfz));
+            r[2 * c] = fmaxf(__fmaf_rd(fabsf(en), -kQEntryMargin, en), lo);
+            r[2 * c + 1] = fminf(__fmaf_ru(fabsf(ex), kQExitMargin, ex), hitT);
+        }
+        return make_float4(r[0], r[1], r[2], r[3]);
+    }
+    f3 lo0, hi0, lo1, hi1;
+    qnode_box(n, 0, lo0, hi0);
+    qnode_box(n, 1, lo1, hi1);
+    const float2 a = slab(ro, inv, lo0, hi0, tmin, hitT), b = slab(ro, inv, lo1, hi1, tmin, hitT);
+    return make_float4(a.x, a.y, b.x, b.y);
 }
 
 // The reference's own test of a leaf: its slabs (minimum_lbvh.h:82-96) on the
@@ -854,13 +929,13 @@ __device__ __forceinline__ bool leaf_box_passes(f3 ro, f3 inv, f3 v0, f3 v1, f3 
 // recognised as "came from neither child" so that the parent word is read
 // only when the walk moves up. quantised_step advances it by one leaf test or
 // internal-node visit and returns true when the walk is over; nu counts
-// parent-word loads. kWide: one 32-byte node load (32-byte aligned array).
-template <bool kAny, bool kCount, bool kWide = false>
+// parent-word loads. The node test is qnode_test (qp from qparams).
+template <bool kAny, bool kCount>
 __device__ __forceinline__ bool quantised_step(uint32_t& curr, uint32_t& prev, HitRecord& hit,
                                                const mlbvh_qnode* __restrict__ qnodes,
                                                const uint32_t* __restrict__ parents,
-                                               const mlbvh_qtri* __restrict__ qtris, int eBase, f3 ro, f3 rd, f3 inv,
-                                               float tmin, uint32_t& nv, uint32_t& nt, uint32_t& nu)
+                                               const mlbvh_qtri* __restrict__ qtris, const QParams& qp, f3 ro, f3 rd,
+                                               f3 inv, float tmin, uint32_t& nv, uint32_t& nt, uint32_t& nu)
 {
     if (curr & kLeafBit) {
         if (kCount) ++nt;
@@ -884,9 +959,9 @@ __device__ __forceinline__ bool quantised_step(uint32_t& curr, uint32_t& prev, H
         return curr == kInvalid;
     }
     if (kCount) ++nv;
-    const QNodeView nd = load_qnode<kWide>(qnodes, curr, eBase);
-    const float2 rl = slab(ro, inv, nd.box.lo0, nd.box.hi0, tmin, hit.t);
-    const float2 rr = slab(ro, inv, nd.box.lo1, nd.box.hi1, tmin, hit.t);
+    const QNodeWords nd = load_qnode(qnodes, curr, qp.eb);
+    const float4 r = qnode_test(nd, qp, ro, inv, tmin, hit.t);
+    const float2 rl = make_float2(r.x, r.y), rr = make_float2(r.z, r.w);
     const bool hitL = rl.x <= rl.y, hitR = rr.x <= rr.y;
     uint32_t nearN = nd.c0, farN = nd.c1;
     int nHits = 0;
@@ -943,12 +1018,12 @@ __device__ __forceinline__ bool quantised_replay_step(uint32_t& curr, uint32_t& 
                                                       int stride, HitRecord& hit,
                                                       const mlbvh_qnode* __restrict__ qnodes,
                                                       const uint32_t* __restrict__ parents,
-                                                      const mlbvh_qtri* __restrict__ qtris, int eBase, f3 ro, f3 rd,
-                                                      f3 inv, float tmin, uint32_t& nv, uint32_t& nt, uint32_t& nu)
+                                                      const mlbvh_qtri* __restrict__ qtris, const QParams& qp, f3 ro,
+                                                      f3 rd, f3 inv, float tmin, uint32_t& nv, uint32_t& nt,
+                                                      uint32_t& nu)
 {
     if (depth < 0)
-        return quantised_step<kAny, kCount, true>(curr, prev, hit, qnodes, parents, qtris, eBase, ro, rd, inv, tmin, nv,
-                                                  nt, nu);
+        return quantised_step<kAny, kCount>(curr, prev, hit, qnodes, parents, qtris, qp, ro, rd, inv, tmin, nv, nt, nu);
     if (curr & kLeafBit) {
         if (kCount) ++nt;
         const float4* t = reinterpret_cast<const float4*>(qtris + (curr & kQIndexMask));
@@ -967,9 +1042,9 @@ __device__ __forceinline__ bool quantised_replay_step(uint32_t& curr, uint32_t& 
         }
     } else {
         if (kCount) ++nv;
-        const QNodeView nd = load_qnode<true>(qnodes, curr, eBase);
-        const float2 rl = slab(ro, inv, nd.box.lo0, nd.box.hi0, tmin, hit.t);
-        const float2 rr = slab(ro, inv, nd.box.lo1, nd.box.hi1, tmin, hit.t);
+        const QNodeWords nd = load_qnode(qnodes, curr, qp.eb);
+        const float4 r = qnode_test(nd, qp, ro, inv, tmin, hit.t);
+        const float2 rl = make_float2(r.x, r.y), rr = make_float2(r.z, r.w);
         const bool hitL = rl.x <= rl.y, hitR = rr.x <= rr.y;
         if (hitL && hitR) {
             const bool swap = rr.x < rl.x;
@@ -1009,17 +1084,17 @@ __device__ __forceinline__ bool quantised_replay_step(uint32_t& curr, uint32_t& 
     }
 }
 
-template <bool kAny, bool kCount = false, bool kWide = false>
+template <bool kAny, bool kCount = false>
 __device__ __forceinline__ void trace_quantised(HitRecord& hit, const mlbvh_qnode* __restrict__ qnodes,
                                                 const uint32_t* __restrict__ parents,
-                                                const mlbvh_qtri* __restrict__ qtris, uint32_t root, int eBase, f3 ro,
-                                                f3 rd, f3 inv, float tmin, uint32_t* visits = nullptr,
-                                                uint32_t* tests = nullptr, uint32_t* ups = nullptr)
+                                                const mlbvh_qtri* __restrict__ qtris, uint32_t root,
+                                                const QParams& qp, f3 ro, f3 rd, f3 inv, float tmin,
+                                                uint32_t* visits = nullptr, uint32_t* tests = nullptr,
+                                                uint32_t* ups = nullptr)
 {
     uint32_t curr = root, prev = kInvalid, nv = 0, nt = 0, nu = 0;
     for (uint32_t steps = 1; steps < kMaxTraversalSteps; ++steps)
-        if (quantised_step<kAny, kCount, kWide>(curr, prev, hit, qnodes, parents, qtris, eBase, ro, rd, inv, tmin, nv,
-                                                nt, nu))
+        if (quantised_step<kAny, kCount>(curr, prev, hit, qnodes, parents, qtris, qp, ro, rd, inv, tmin, nv, nt, nu))
             break;
     if (kCount) {
         *visits += nv;
@@ -1088,35 +1163,9 @@ __device__ __forceinline__ WideVisit wide_visit(const mlbvh_wnode* __restrict__ 
     return w;
 }
 
-// Quantised slot (two 32-byte loads). Plane code q of axis a stands for
-// base[a] + V, V = scale[a] (1 + q / 2^15): one byte permute writes q into
-// mantissa byte 1 of the power of two scale[a], which gives V exactly.
-__device__ __forceinline__ float qw_value(uint32_t codes, uint32_t scaleBits, int k)
-{
-    return __uint_as_float(__byte_perm(codes, scaleBits, 0x7604u | ((uint32_t)k << 4)));
-}
-// The quantiser keeps every slot's base below 2^60 and its scale at most
-// 2^59 (else its status word sends every ray to the binary tree), so every
-// plane lies below 2^61. A ray whose |inv| and |ro| components are below 2^62
-// then keeps every term of qwide_visit's FMA form below 2^125, in the float
-// range (qwide_ray_fits, tested once per ray). The walks send other rays (in
-// practice those with a zero direction component, whose inverse the
-// reference clamps to +-FLT_MAX) to the stack-free walk over the binary tree,
-// which gives the reference's own answers.
-constexpr float kQBaseLimit = 1.152921504606846976e18f;  // 2^60
-constexpr float kQRayLimit = 4.611686018427387904e18f;   // 2^62
-__device__ __forceinline__ bool qwide_ray_fits(f3 ro, f3 inv)
-{
-    return fmaxf(fmaxf(fabsf(inv.x), fabsf(inv.y)), fmaxf(fabsf(inv.z), fmaxf(fmaxf(fabsf(ro.x), fabsf(ro.y)),
-                                                                               fabsf(ro.z)))) < kQRayLimit;
-}
-// Relative margins of the quantised slab test: 2^-22 below the entry and
-// 2^-21 above the exit (see qwide_visit).
-constexpr float kQEntryMargin = 2.384185791015625e-07f;
-constexpr float kQExitMargin = 4.76837158203125e-07f;
-
-// The distance of a plane along the ray, (base + V - ro) inv, is one FMA per
-// plane: V inv + C, where C = base inv - ro inv bounds (base - ro) inv from
+// Quantised slot (two 32-byte loads): per axis a base and a scale 2^E, the
+// planes at base + V (qw_value). The distance of a plane along the ray,
+// (base + V - ro) inv, is one FMA per plane: V inv + C, where C = base inv - ro inv bounds (base - ro) inv from
 // below for near planes (ro inv rounded up, the FMA rounded down) and from
 // above for far planes (ro inv rounded down, the FMA rounded up); the plane's
 // FMA is rounded the same way. On an axis whose inv is positive the near

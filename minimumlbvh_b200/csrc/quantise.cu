@@ -1,14 +1,15 @@
 // The quantised tree: 32-byte nodes with 8-bit child boxes (no reference
 // counterpart), made from a tree built by build.cu, and its ray query.
 //
-// k_quantise: one thread per internal node. The node's origin is the min of
-// its two child boxes; per axis the step is the smallest power of two 2^e with
-// 255 * 2^e >= the node's extent (rounded up), coded as k = eBase - e in 5 bits
-// where eBase is the step of the root's extent. Child corners are quantised
-// down (lower) and up (upper) and checked against the same directed-rounding
-// decode the traversal uses, so every decoded box contains its FP32 box.
-// Leaves move to sorted (leaf) order: a left leaf child of node j is leaf j,
-// a right leaf child is leaf j+1 (node j splits leaves j and j+1).
+// k_quantise: one thread per internal node. Per axis the node stores a base b
+// and a scale 2^E; code q stands for the plane b + 2^E (1 + q / 2^15) (the
+// form of the quantised 4-wide slots, decoded with one byte permute), lower
+// planes rounded down and upper ones up in exact arithmetic. E is the
+// smallest exponent in [EB - 31, EB] whose codes fit 8 bits, stored as the
+// 5-bit code k = EB - E, where EB (tree_scale_exponent) is chosen from the
+// root box so that every node's codes fit at E = EB. Leaves move to sorted
+// (leaf) order: a left leaf child of node j is leaf j, a right leaf child is
+// leaf j+1 (node j splits leaves j and j+1).
 #include "capi_internal.h"
 #include "../../include/mlbvh_device.cuh"
 
@@ -27,9 +28,23 @@ __device__ __forceinline__ void leaf_box(const float* __restrict__ tris, uint32_
     hi = smax3(smax3(smax3(mk(-kFltMax, -kFltMax, -kFltMax), v0), v1), v2);
 }
 
-// Step exponent of the whole tree: that of the largest root-box extent.
-__device__ __forceinline__ int tree_ebase(const mlbvh_internal_node* __restrict__ nodes,
-                                          const float* __restrict__ tris, uint32_t root)
+// ceil(log2(x)) for finite x > 0; -150 for 0
+__device__ __forceinline__ int ceil_log2f(float x)
+{
+    if (!(x > 0.0f)) return -150;
+    int k;
+    const float f = frexpf(x, &k);  // x = f 2^k, f in [0.5, 1)
+    return f == 0.5f ? k - 1 : k;
+}
+
+// The tree's scale exponent EB from the root box's largest extent D and
+// largest coordinate magnitude R: EB = max(ceil(log2 D) + 9, ceil(log2 R) -
+// 13, -111). At E = EB a code's extent term stays below 64 steps of
+// 2^(E - 15) and the rounding of the base (b = nlo - 2^E rounded down, at
+// most R + 2^E in size) below 33 steps, so every node's codes fit 8 bits.
+// finite = false for a non-finite root box or an EB above 127.
+__device__ __forceinline__ int tree_scale_exponent(const mlbvh_internal_node* __restrict__ nodes,
+                                                   const float* __restrict__ tris, uint32_t root, bool& finite)
 {
     f3 lo, hi;
     if (root & kLeafBit) {
@@ -39,23 +54,65 @@ __device__ __forceinline__ int tree_ebase(const mlbvh_internal_node* __restrict_
         lo = smin3(nd.lo0, nd.lo1);
         hi = smax3(nd.hi0, nd.hi1);
     }
-    const float d = fmaxf(fmaxf(__fsub_ru(hi.x, lo.x), __fsub_ru(hi.y, lo.y)), __fsub_ru(hi.z, lo.z));
-    return step_exponent(d);
+    const float l[3] = {lo.x, lo.y, lo.z}, h[3] = {hi.x, hi.y, hi.z};
+    float d = 0.0f, r = 0.0f;
+    finite = true;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        if (!(isfinite(l[a]) && isfinite(h[a]))) finite = false;
+        d = fmaxf(d, __fsub_ru(h[a], l[a]));
+        r = fmaxf(r, fmaxf(fabsf(l[a]), fabsf(h[a])));
+    }
+    if (!finite || !isfinite(d)) {
+        finite = false;
+        return 0;
+    }
+    const int e = max(max(ceil_log2f(d) + 9, ceil_log2f(r) - 13), -111);
+    finite = e <= 127;  // a scale 2^E must be a float
+    return finite ? e : 0;
 }
 
-__device__ __forceinline__ uint32_t quantise_lo(float v, float o, float s)
+// One axis of a node: base, exponent E in [eLo, eHi] and the four codes
+// (byte 0 child 0 lower, 1 child 0 upper, 2 child 1 lower, 3 child 1 upper)
+// with base + 2^E (1 + q / 2^15) <= the lower and >= the upper plane in exact
+// arithmetic (every step rounds toward that side), E the smallest in range
+// whose codes fit. false when no E in range fits or a plane is not finite
+// (base 0, E = eHi and codes 0xFF00FF00 then).
+__device__ __forceinline__ bool quantise_axis2(const float lo[2], const float hi[2], int eLo, int eHi, float& base,
+                                               int& E, uint32_t& codes)
 {
-    float q = floorf(__fsub_rd(v, o) / s);
-    uint32_t qi = q <= 0.0f ? 0u : (q >= 255.0f ? 255u : (uint32_t)q);
-    while (qi > 0u && qlo(o, qi, s) > v) --qi;
-    return qi;
-}
-__device__ __forceinline__ uint32_t quantise_hi(float v, float o, float s)
-{
-    float q = ceilf(__fsub_ru(v, o) / s);
-    uint32_t qi = q <= 0.0f ? 0u : (q >= 255.0f ? 255u : (uint32_t)q);
-    while (qi < 255u && qhi(o, qi, s) < v) ++qi;
-    return qi;
+    base = 0.0f;
+    E = eHi;
+    codes = 0xFF00FF00u;
+    const float nlo = fminf(lo[0], lo[1]), nhi = fmaxf(hi[0], hi[1]);
+    if (!(isfinite(lo[0]) && isfinite(lo[1]) && isfinite(hi[0]) && isfinite(hi[1]) && nlo <= nhi)) return false;
+    const float m = __fdiv_ru(__fsub_ru(nhi, nlo), 255.0f);  // >= extent / 255
+    int e = -111;
+    if (m > 0.0f) e = max(e, ceil_log2f(m) + 15);
+    e = max(e, eLo);
+    for (; e <= eHi; ++e) {
+        const float sc = pow2f(e);
+        const float b = __fsub_rd(nlo, sc);
+        if (!isfinite(b)) return false;
+        const float toCode = pow2f(15 - e);
+        bool fits = true;
+        uint32_t q = 0;
+#pragma unroll
+        for (int c = 0; c < 2; ++c) {
+            const float ql = floorf(__fmul_rd(__fsub_rd(__fsub_rd(lo[c], b), sc), toCode));
+            const float qh = ceilf(__fmul_ru(__fsub_ru(__fsub_ru(hi[c], b), sc), toCode));
+            if (!(qh <= 255.0f)) fits = false;
+            q |= (uint32_t)fminf(fmaxf(ql, 0.0f), 255.0f) << (16 * c);
+            q |= (uint32_t)fminf(fmaxf(qh, 0.0f), 255.0f) << (16 * c + 8);
+        }
+        if (fits) {
+            base = b;
+            E = e;
+            codes = q;
+            return true;
+        }
+    }
+    return false;
 }
 
 __device__ __forceinline__ void write_qtri(mlbvh_qtri* __restrict__ qtris, uint32_t pos, const float* __restrict__ tris,
@@ -68,6 +125,9 @@ __device__ __forceinline__ void write_qtri(mlbvh_qtri* __restrict__ qtris, uint3
     dst[2] = make_float4(__ldg(src + 8), __uint_as_float(t), 0.0f, 0.0f);
 }
 
+// header->status must be 0 before the launch (the threads OR bits into it):
+// bit 0 a base of 2^60 or more or a scale above 2^59, bit 1 a non-finite
+// coordinate (or a scale exponent above 127).
 __global__ void __launch_bounds__(kQuantiseThreads)
     k_quantise(const mlbvh_internal_node* __restrict__ nodes, const mlbvh_node_index* __restrict__ rootPtr,
                const float* __restrict__ tris, uint32_t n, mlbvh_qnode* __restrict__ qnodes,
@@ -75,40 +135,35 @@ __global__ void __launch_bounds__(kQuantiseThreads)
 {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t root = __ldg(rootPtr);
-    const int eBase = tree_ebase(nodes, tris, root);
+    bool finite;
+    const int eb = tree_scale_exponent(nodes, tris, root, finite);
     if (i == 0) {
         header->root = (root & kLeafBit) ? kLeafBit : root;
-        header->eBase = eBase;
+        header->eBase = eb;
         header->nTriangles = n;
-        header->_pad = 0;
+        if (!finite) atomicOr(&header->status, 2u);
         if (root & kLeafBit) write_qtri(qtris, 0, tris, root & ~kLeafBit);
     }
     if (i + 1 >= n) return;
     const NodeView nd = load_node(nodes, i);
-    const f3 o = smin3(nd.lo0, nd.lo1);
-    const f3 top = smax3(nd.hi0, nd.hi1);
-    const float ext[3] = {__fsub_ru(top.x, o.x), __fsub_ru(top.y, o.y), __fsub_ru(top.z, o.z)};
-    uint32_t code = 0;
-    float step[3];
-#pragma unroll
-    for (int a = 0; a < 3; ++a) {
-        int e = max(step_exponent(ext[a]), eBase - 31);
-        int k = eBase - e;
-        if (k < 0) k = 0;  // cannot happen: every node lies inside the root box
-        code |= (uint32_t)k << (5 * a);
-        step[a] = pow2f(max(eBase - k, -126));
-    }
     const float lo0[3] = {nd.lo0.x, nd.lo0.y, nd.lo0.z}, hi0[3] = {nd.hi0.x, nd.hi0.y, nd.hi0.z};
     const float lo1[3] = {nd.lo1.x, nd.lo1.y, nd.lo1.z}, hi1[3] = {nd.hi1.x, nd.hi1.y, nd.hi1.z};
-    const float oo[3] = {o.x, o.y, o.z};
-    uint32_t q[12];
+    const int eLo = max(-111, eb - 31);
+    uint32_t code = 0, status = 0, q[3];
+    float base[3];
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
-        q[a] = quantise_lo(lo0[a], oo[a], step[a]);
-        q[3 + a] = quantise_hi(hi0[a], oo[a], step[a]);
-        q[6 + a] = quantise_lo(lo1[a], oo[a], step[a]);
-        q[9 + a] = quantise_hi(hi1[a], oo[a], step[a]);
+        const float l2[2] = {lo0[a], lo1[a]}, h2[2] = {hi0[a], hi1[a]};
+        int e = eb;
+        base[a] = 0.0f;
+        q[a] = 0xFF00FF00u;
+        if (!finite || !quantise_axis2(l2, h2, eLo, eb, base[a], e, q[a]))
+            status |= 2u;
+        else if (!(fabsf(base[a]) < kQBaseLimit && e <= 59))
+            status |= 1u;
+        code |= (uint32_t)(eb - e) << (5 * a);
     }
+    if (status) atomicOr(&header->status, status);
     uint32_t c0 = nd.c0, c1 = nd.c1;
     if (c0 & kLeafBit) {
         write_qtri(qtris, i, tris, c0 & ~kLeafBit);
@@ -119,12 +174,10 @@ __global__ void __launch_bounds__(kQuantiseThreads)
         c1 = kLeafBit | (i + 1);
     }
     c0 |= (code & 0xFFu) << 23;
-    c1 |= ((code >> 8) & 0xFFu) << 23;
+    c1 |= ((code >> 8) & 0x7Fu) << 23;
     float4* dst = reinterpret_cast<float4*>(qnodes + i);
-    dst[0] = make_float4(o.x, o.y, o.z, __uint_as_float(q[0] | q[1] << 8 | q[2] << 16 | q[3] << 24));
-    dst[1] = make_float4(__uint_as_float(q[4] | q[5] << 8 | q[6] << 16 | q[7] << 24),
-                         __uint_as_float(q[8] | q[9] << 8 | q[10] << 16 | q[11] << 24), __uint_as_float(c0),
-                         __uint_as_float(c1));
+    dst[0] = make_float4(base[0], base[1], base[2], __uint_as_float(q[0]));
+    dst[1] = make_float4(__uint_as_float(q[1]), __uint_as_float(q[2]), __uint_as_float(c0), __uint_as_float(c1));
     parents[i] = nd.parent;
 }
 
@@ -169,17 +222,17 @@ __global__ void __launch_bounds__(kTraceThreads)
     hit.ng = mk(0.0f, 0.0f, 0.0f);
     hit.tri = 0xFFFFFFFFu;
     const uint32_t root = __ldg(&header->root);
-    const int eBase = __ldg(&header->eBase);
     const f3 inv = inv_rd(rd);
+    const QParams qp = qparams(header, ro, inv);
     uint32_t nv = 0, nt = 0, nu = 0;
     if (kDepth == 0) {
-        trace_quantised<kAny, kCount, true>(hit, qnodes, parents, qtris, root, eBase, ro, rd, inv, a.w, &nv, &nt, &nu);
+        trace_quantised<kAny, kCount>(hit, qnodes, parents, qtris, root, qp, ro, rd, inv, a.w, &nv, &nt, &nu);
     } else {
         uint32_t curr = root, prev = kInvalid;
         int depth = 0;
         for (uint32_t steps = 1; steps < kMaxTraversalSteps; ++steps)
             if (quantised_replay_step<kAny, kCount, kDepth>(curr, prev, depth, &s_stack[0][threadIdx.x],
-                                                            kTraceThreads, hit, qnodes, parents, qtris, eBase, ro, rd,
+                                                            kTraceThreads, hit, qnodes, parents, qtris, qp, ro, rd,
                                                             inv, a.w, nv, nt, nu))
                 break;
     }
@@ -230,6 +283,8 @@ mlbvh_status quantise(const mlbvh_internal_node* dNodes, const mlbvh_node_index*
         !aligned16(dQTris) || !aligned16(dQHeader))
         return fail(MLBVH_ERR_INVALID_ARG, "device pointers must be 16-byte aligned (node arrays 32-byte)");
     const uint32_t threads = n > 1 ? n - 1 : 1;
+    const cudaError_t e = cudaMemsetAsync(&dQHeader->status, 0, sizeof(uint32_t), stream);
+    if (e != cudaSuccess) return fail(MLBVH_ERR_CUDA, cudaGetErrorString(e));
     k_quantise<<<(threads + kQuantiseThreads - 1) / kQuantiseThreads, kQuantiseThreads, 0, stream>>>(
         dNodes, dRoot, reinterpret_cast<const float*>(dTris), n, dQNodes, dQParents, dQTris, dQHeader);
     MLBVH_CHECK_LAUNCH("k_quantise");

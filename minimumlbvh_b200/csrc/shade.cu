@@ -38,6 +38,9 @@ constexpr int kAoThreads = 128;
 #ifndef MLBVH_AO_MIN_BLOCKS
 #define MLBVH_AO_MIN_BLOCKS 8
 #endif
+#ifndef MLBVH_AO_QUANT_MIN_BLOCKS
+#define MLBVH_AO_QUANT_MIN_BLOCKS 9
+#endif
 // the stack-free walk's own (swept: 4 steps and a batch of 16 lanes beat 3 and
 // 8 by 1.7 %; a batch of 24 loses 7 %)
 // the wide trees' refill batch (swept 4-16: 8 is best for the quantised slots,
@@ -253,11 +256,12 @@ struct QuantTree {
     const mlbvh_qheader* header;
     struct Ctx {
         uint32_t root;
-        int eBase;
+        int eb;
+        uint32_t status;
     };
     __device__ __forceinline__ Ctx context() const
     {
-        return Ctx{__ldg(&header->root), __ldg(&header->eBase)};
+        return Ctx{__ldg(&header->root), __ldg(&header->eBase), __ldg(&header->status)};
     }
     template <bool kAny, bool kCount>
     __device__ __forceinline__ void trace(const Ctx& c, HitRecord& hit, f3 ro, f3 rd, Counts& n, uint2* pstack,
@@ -265,12 +269,12 @@ struct QuantTree {
     {
         static_assert(!kAny, "primary rays are closest-hit");
         const f3 inv = inv_rd(rd);
+        const QParams qp{c.eb, c.status, c.status == 0u && qwide_ray_fits(ro, inv)};
         uint32_t curr = c.root, prev = kInvalid;
         int depth = 0;
         for (uint32_t steps = 1; steps < kMaxTraversalSteps; ++steps)
             if (quantised_replay_step<false, kCount, kStack>(curr, prev, depth, pstack, stride, hit, qnodes, parents,
-                                                            qtris, c.eBase, ro, rd, inv, 0.0f, n.visits, n.tests,
-                                                            n.ups))
+                                                            qtris, qp, ro, rd, inv, 0.0f, n.visits, n.tests, n.ups))
                 break;
     }
     // the replay walk: the stack-free walk's leaf order with a stack of
@@ -278,12 +282,17 @@ struct QuantTree {
     // only any-hit steps are taken (AO rays)
     static constexpr int kStack = 16;
     static constexpr int kPrimaryStack = kStack;
+    static constexpr int kMinBlocks = MLBVH_AO_QUANT_MIN_BLOCKS;
     __device__ __forceinline__ uint32_t ball_start(const Ctx& c, const AoBall& b) const
     {
+        if (c.status & 2u) return c.root;  // every box passes: no box bounds the ball
         uint32_t curr = c.root;
         for (uint32_t steps = 0; !(curr & kLeafBit) && steps < kMaxTraversalSteps; ++steps) {
-            const QNodeView nd = load_qnode<true>(qnodes, curr, c.eBase);
-            const bool m0 = box_meets(nd.box.lo0, nd.box.hi0, b), m1 = box_meets(nd.box.lo1, nd.box.hi1, b);
+            const QNodeWords nd = load_qnode(qnodes, curr, c.eb);
+            f3 lo0, hi0, lo1, hi1;
+            qnode_box(nd, 0, lo0, hi0);
+            qnode_box(nd, 1, lo1, hi1);
+            const bool m0 = box_meets(lo0, hi0, b), m1 = box_meets(lo1, hi1, b);
             if (m0 && m1) return curr;
             if (!m0 && !m1) return kInvalid;
             curr = m0 ? nd.c0 : nd.c1;
@@ -294,9 +303,9 @@ struct QuantTree {
     __device__ __forceinline__ bool step(const Ctx& c, uint32_t& curr, uint32_t& prev, int& depth, uint32_t* stack,
                                          HitRecord& hit, f3 ro, f3 rd, f3 inv, Counts& n, bool fits) const
     {
+        const QParams qp{c.eb, c.status, c.status == 0u && fits};
         return quantised_replay_step<kAny, kCount, kStack>(curr, prev, depth, stack, kAoThreads, hit, qnodes, parents,
-                                                           qtris, c.eBase, ro, rd, inv, 0.0f, n.visits, n.tests,
-                                                           n.ups);
+                                                           qtris, qp, ro, rd, inv, 0.0f, n.visits, n.tests, n.ups);
     }
 };
 
@@ -520,7 +529,7 @@ __global__ void __launch_bounds__(kAoThreads, MinBlocksOf<Tree>::value)
     uint32_t pixel = 0, curr = 0, prev = 0, steps = 0;
     int depth = 0;
     f3 origin = mk(0, 0, 0), dir = origin, inv = origin;
-    bool fits = true;  // qwide_ray_fits of this lane's ray (only the quantised wide slots use it)
+    bool fits = true;  // qwide_ray_fits of this lane's ray (the quantised trees use it)
     HitRecord hit;
     hit.t = radius;
     for (;;) {

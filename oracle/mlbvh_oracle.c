@@ -2008,71 +2008,110 @@ void orc_pack(uint32_t* pixels, const float* accum4, int n)
 }
 
 /* ------------------------------------------------------------ quantised tree
- * Restates csrc/quantise.cu and trace_quantised of the device header (this
+ * Restates csrc/quantise.cu and the quantised walks of the device header (this
  * node format has no reference counterpart; its checker is this code plus
- * the FP32 traversal above, whose closest hits it must reproduce).
- * Directed-rounding sums are formed exactly with the TwoSum error term
- * (Knuth), so they equal CUDA's __fadd_rd / __fadd_ru except possibly in the
- * sign of a zero result, which no comparison here can see. */
+ * the FP32 traversal above, whose closest hits it must reproduce). The
+ * directed roundings are those of the quantised slots above (add_dir,
+ * mul_dir, fma_dir). */
 #define ORC_QMASK 0x7FFFFFu
 
-static inline float two_sum_err(float a, float b, float s)
-{
-    float bp = s - a;
-    float ap = s - bp;
-    return (a - ap) + (b - bp);
-}
-static inline float add_rd(float a, float b)
-{
-    float s = a + b;
-    return two_sum_err(a, b, s) < 0.0f ? nextafterf(s, -INFINITY) : s;
-}
-static inline float add_ru(float a, float b)
-{
-    float s = a + b;
-    return two_sum_err(a, b, s) > 0.0f ? nextafterf(s, INFINITY) : s;
-}
-static inline float pow2f_(int e)
-{
-    uint32_t b = (uint32_t)(127 + e) << 23;
-    float f;
-    memcpy(&f, &b, 4);
-    return f;
-}
-static inline int step_exponent(float d)
-{
-    if (!(d >= 1.17549435e-38f)) return -126;
-    uint32_t bits;
-    memcpy(&bits, &d, 4);
-    int e = (int)((bits >> 23) & 0xFFu) - 126 - 8;
-    if (e < -126) e = -126;
-    if (255.0f * pow2f_(e) < d) e += 1;
-    return e;
-}
-static inline float qdec_lo(float o, uint32_t q, float s) { return add_rd(o, (float)q * s); }
-static inline float qdec_hi(float o, uint32_t q, float s) { return add_ru(o, (float)q * s); }
-static inline uint32_t quant_lo(float v, float o, float s)
-{
-    float q = floorf(add_rd(v, -o) / s);
-    uint32_t qi = q <= 0.0f ? 0u : (q >= 255.0f ? 255u : (uint32_t)q);
-    while (qi > 0u && qdec_lo(o, qi, s) > v) --qi;
-    return qi;
-}
-static inline uint32_t quant_hi(float v, float o, float s)
-{
-    float q = ceilf(add_ru(v, -o) / s);
-    uint32_t qi = q <= 0.0f ? 0u : (q >= 255.0f ? 255u : (uint32_t)q);
-    while (qi < 255u && qdec_hi(o, qi, s) < v) ++qi;
-    return qi;
-}
 static void tri_box(const orc_triangle* t, orc_aabb* b)
 {
     aabb_set_empty(b);
     for (int j = 0; j < 3; ++j) aabb_extend_p(b, t->v[j]);
 }
 
-/* k_quantise (csrc/quantise.cu). qnodes: 8 words per node; qtris: 12 words
- * per leaf; header: 4 words. Returns 0. */
+/* ceil(log2(x)) for finite x > 0; -150 for 0 */
+static int ceil_log2(float x)
+{
+    if (!(x > 0.0f)) return -150;
+    int k;
+    const float f = frexpf(x, &k); /* x = f 2^k, f in [0.5, 1) */
+    return f == 0.5f ? k - 1 : k;
+}
+
+/* The tree's scale exponent EB (quantise.cu: tree_scale_exponent): every
+ * node's axis scale is 2^E with E in [max(-111, EB - 31), EB]. From the root
+ * box's largest extent D and largest coordinate magnitude R, EB = max(ceil(log2
+ * D) + 9, ceil(log2 R) - 13, -111): at E = EB the extent term of a code stays
+ * below 64 steps and the rounding of the base below 33, so every node's codes
+ * fit 8 bits. Returns 0 (and *ok = 0) for a non-finite root box or an EB
+ * above 127. */
+static int tree_scale_exponent(const orc_aabb* rb, int* ok)
+{
+    const float lo[3] = {rb->lower.x, rb->lower.y, rb->lower.z}, hi[3] = {rb->upper.x, rb->upper.y, rb->upper.z};
+    float d = 0.0f, r = 0.0f;
+    for (int a = 0; a < 3; ++a)
+    {
+        if (!(isfinite(lo[a]) && isfinite(hi[a]))) { *ok = 0; return 0; }
+        d = fmaxf(d, add_dir(hi[a], -lo[a], 1));
+        r = fmaxf(r, fmaxf(fabsf(lo[a]), fabsf(hi[a])));
+    }
+    if (!isfinite(d)) { *ok = 0; return 0; }
+    int e = ceil_log2(d) + 9;
+    const int e2 = ceil_log2(r) - 13;
+    if (e2 > e) e = e2;
+    if (e < -111) e = -111;
+    *ok = e <= 127; /* a scale 2^E must be a float */
+    return *ok ? e : 0;
+}
+
+/* One axis of a node (quantise.cu: quantise_axis2): base, exponent E in
+ * [eLo, eHi] and the four codes (byte 0 child 0 lower, 1 child 0 upper,
+ * 2 child 1 lower, 3 child 1 upper) with base + 2^E (1 + q / 2^15) <= the
+ * lower and >= the upper plane in exact arithmetic (every step rounds toward
+ * that side), E the smallest in range whose codes fit 8 bits. Returns 0 when
+ * no E in range fits or a plane is not finite (then *codes, clamped, must not
+ * be used). */
+static int quantise_axis2(const float lo[2], const float hi[2], int eLo, int eHi, float* base, int* E,
+                          uint32_t* codes)
+{
+    *base = 0.0f;
+    *E = eHi;
+    *codes = 0xFF00FF00u;
+    const float nlo = fminf(lo[0], lo[1]), nhi = fmaxf(hi[0], hi[1]);
+    if (!(isfinite(lo[0]) && isfinite(lo[1]) && isfinite(hi[0]) && isfinite(hi[1]) && nlo <= nhi)) return 0;
+    const float m = div_up(add_dir(nhi, -nlo, 1), 255.0f);
+    int e = -111;
+    if (m > 0.0f)
+    {
+        const int c = ceil_log2(m) + 15;
+        if (c > e) e = c;
+    }
+    if (e < eLo) e = eLo;
+    for (; e <= eHi; ++e)
+    {
+        const float sc = pow2_of(e);
+        const float b = add_dir(nlo, -sc, 0);
+        if (!isfinite(b)) return 0;
+        const float toCode = pow2_of(15 - e);
+        int fits = 1;
+        uint32_t q = 0;
+        for (int c = 0; c < 2; ++c)
+        {
+            const float ql = floorf(mul_dir(add_dir(add_dir(lo[c], -b, 0), -sc, 0), toCode, 0));
+            const float qh = ceilf(mul_dir(add_dir(add_dir(hi[c], -b, 1), -sc, 1), toCode, 1));
+            if (!(qh <= 255.0f)) fits = 0;
+            q |= (uint32_t)fminf(fmaxf(ql, 0.0f), 255.0f) << (16 * c);
+            q |= (uint32_t)fminf(fmaxf(qh, 0.0f), 255.0f) << (16 * c + 8);
+        }
+        if (fits)
+        {
+            *base = b;
+            *E = e;
+            *codes = q;
+            return 1;
+        }
+    }
+    return 0;
+}
+
+/* k_quantise (csrc/quantise.cu). qnodes: 8 words per node (base x y z; the
+ * codes of axis x, y, z, one word each; the child words, bits 23-30 holding
+ * the axis exponents as k = EB - E, 5 bits each: child 0 k_x | k_y bits 0-2,
+ * child 1 k_y bits 3-4 | k_z); qtris: 12 words per leaf; header: root, EB,
+ * n, status (bit 0: some node's base or scale lies beyond the walks' FMA form,
+ * bit 1: a non-finite coordinate). Returns 0. */
 int orc_quantise(const orc_node* nodes, uint32_t root, const orc_triangle* tris, uint32_t n,
                  uint32_t* qnodes, uint32_t* parents, uint32_t* qtris, uint32_t* header)
 {
@@ -2083,13 +2122,12 @@ int orc_quantise(const orc_node* nodes, uint32_t root, const orc_triangle* tris,
         rb.lower = min3(nodes[root].aabbs[0].lower, nodes[root].aabbs[1].lower);
         rb.upper = max3(nodes[root].aabbs[0].upper, nodes[root].aabbs[1].upper);
     }
-    float d = fmaxf(fmaxf(add_ru(rb.upper.x, -rb.lower.x), add_ru(rb.upper.y, -rb.lower.y)),
-                    add_ru(rb.upper.z, -rb.lower.z));
-    int eBase = step_exponent(d);
+    int finite = 1;
+    const int eb = tree_scale_exponent(&rb, &finite);
+    uint32_t status = finite ? 0u : 2u;
     header[0] = (root & ORC_LEAF_BIT) ? ORC_LEAF_BIT : root;
-    memcpy(&header[1], &eBase, 4);
+    memcpy(&header[1], &eb, 4);
     header[2] = n;
-    header[3] = 0;
 #define PUT_QTRI(pos, t)                                                  \
     do {                                                                  \
         memcpy(qtris + 12 * (size_t)(pos), &tris[t], 36);                 \
@@ -2098,79 +2136,98 @@ int orc_quantise(const orc_node* nodes, uint32_t root, const orc_triangle* tris,
         qtris[12 * (size_t)(pos) + 11] = 0;                               \
     } while (0)
     if (root & ORC_LEAF_BIT) PUT_QTRI(0, root & ~ORC_LEAF_BIT);
+    const int eLo = eb - 31 < -111 ? -111 : eb - 31;
     for (uint32_t i = 0; i + 1 < n; ++i)
     {
         const orc_node* nd = &nodes[i];
-        orc_f3 o = min3(nd->aabbs[0].lower, nd->aabbs[1].lower);
-        orc_f3 top = max3(nd->aabbs[0].upper, nd->aabbs[1].upper);
-        float oo[3] = {o.x, o.y, o.z}, tt[3] = {top.x, top.y, top.z};
-        float lo[2][3] = {{nd->aabbs[0].lower.x, nd->aabbs[0].lower.y, nd->aabbs[0].lower.z},
-                          {nd->aabbs[1].lower.x, nd->aabbs[1].lower.y, nd->aabbs[1].lower.z}};
-        float hi[2][3] = {{nd->aabbs[0].upper.x, nd->aabbs[0].upper.y, nd->aabbs[0].upper.z},
-                          {nd->aabbs[1].upper.x, nd->aabbs[1].upper.y, nd->aabbs[1].upper.z}};
-        uint32_t code = 0, q[12];
+        const float lo[2][3] = {{nd->aabbs[0].lower.x, nd->aabbs[0].lower.y, nd->aabbs[0].lower.z},
+                                {nd->aabbs[1].lower.x, nd->aabbs[1].lower.y, nd->aabbs[1].lower.z}};
+        const float hi[2][3] = {{nd->aabbs[0].upper.x, nd->aabbs[0].upper.y, nd->aabbs[0].upper.z},
+                                {nd->aabbs[1].upper.x, nd->aabbs[1].upper.y, nd->aabbs[1].upper.z}};
+        uint32_t code = 0, q[3];
+        float base[3];
         for (int a = 0; a < 3; ++a)
         {
-            int e = step_exponent(add_ru(tt[a], -oo[a]));
-            if (e < eBase - 31) e = eBase - 31;
-            int k = eBase - e;
-            if (k < 0) k = 0;
-            code |= (uint32_t)k << (5 * a);
-            int es = eBase - k;
-            float s = pow2f_(es < -126 ? -126 : es);
-            q[a] = quant_lo(lo[0][a], oo[a], s);
-            q[3 + a] = quant_hi(hi[0][a], oo[a], s);
-            q[6 + a] = quant_lo(lo[1][a], oo[a], s);
-            q[9 + a] = quant_hi(hi[1][a], oo[a], s);
+            const float l2[2] = {lo[0][a], lo[1][a]}, h2[2] = {hi[0][a], hi[1][a]};
+            int e = eb;
+            base[a] = 0.0f;
+            q[a] = 0xFF00FF00u;
+            if (!finite || !quantise_axis2(l2, h2, eLo, eb, &base[a], &e, &q[a])) status |= 2u;
+            else if (!(fabsf(base[a]) < 1.152921504606846976e18f && e <= 59)) status |= 1u; /* 2^60, 2^59 */
+            code |= (uint32_t)(eb - e) << (5 * a);
         }
         uint32_t c0 = nd->children[0], c1 = nd->children[1];
         if (c0 & ORC_LEAF_BIT) { PUT_QTRI(i, c0 & ~ORC_LEAF_BIT); c0 = ORC_LEAF_BIT | i; }
         if (c1 & ORC_LEAF_BIT) { PUT_QTRI(i + 1, c1 & ~ORC_LEAF_BIT); c1 = ORC_LEAF_BIT | (i + 1); }
         c0 |= (code & 0xFFu) << 23;
-        c1 |= ((code >> 8) & 0xFFu) << 23;
+        c1 |= ((code >> 8) & 0x7Fu) << 23;
         uint32_t* w = qnodes + 8 * (size_t)i;
-        memcpy(&w[0], &o, 12);
-        w[3] = q[0] | q[1] << 8 | q[2] << 16 | q[3] << 24;
-        w[4] = q[4] | q[5] << 8 | q[6] << 16 | q[7] << 24;
-        w[5] = q[8] | q[9] << 8 | q[10] << 16 | q[11] << 24;
+        memcpy(&w[0], base, 12);
+        w[3] = q[0];
+        w[4] = q[1];
+        w[5] = q[2];
         w[6] = c0;
         w[7] = c1;
         parents[i] = nd->parent;
     }
+    header[3] = status;
 #undef PUT_QTRI
     return 0;
 }
 
-static inline void qnode_boxes(const uint32_t* w, int eBase, orc_aabb* b0, orc_aabb* b1)
+/* The scale bits 2^E of each axis of node w (E = EB - k). */
+static inline void qnode_scales(const uint32_t* w, int eb, uint32_t s[3])
 {
-    uint32_t code = ((w[6] >> 23) & 0xFFu) | (((w[7] >> 23) & 0xFFu) << 8);
-    int ex = eBase - (int)(code & 31u), ey = eBase - (int)((code >> 5) & 31u), ez = eBase - (int)((code >> 10) & 31u);
-    float sx = pow2f_(ex < -126 ? -126 : ex), sy = pow2f_(ey < -126 ? -126 : ey), sz = pow2f_(ez < -126 ? -126 : ez);
-    float o[3];
-    memcpy(o, w, 12);
-    uint32_t w0 = w[3], w1 = w[4], w2 = w[5];
-    b0->lower = f3(qdec_lo(o[0], w0 & 255u, sx), qdec_lo(o[1], (w0 >> 8) & 255u, sy), qdec_lo(o[2], (w0 >> 16) & 255u, sz));
-    b0->upper = f3(qdec_hi(o[0], w0 >> 24, sx), qdec_hi(o[1], w1 & 255u, sy), qdec_hi(o[2], (w1 >> 8) & 255u, sz));
-    b1->lower = f3(qdec_lo(o[0], (w1 >> 16) & 255u, sx), qdec_lo(o[1], w1 >> 24, sy), qdec_lo(o[2], w2 & 255u, sz));
-    b1->upper = f3(qdec_hi(o[0], (w2 >> 8) & 255u, sx), qdec_hi(o[1], (w2 >> 16) & 255u, sy), qdec_hi(o[2], w2 >> 24, sz));
+    const uint32_t code = ((w[6] >> 23) & 0xFFu) | (((w[7] >> 23) & 0x7Fu) << 8);
+    for (int a = 0; a < 3; ++a) s[a] = (uint32_t)(eb - (int)((code >> (5 * a)) & 31u) + 127) << 23;
 }
 
-/* Checks that every decoded child box of the quantised tree contains the
- * FP32 child box of the same node. Returns 1 when all do. */
+/* The decoded child boxes (load_qnode): base + V, V = 2^E (1 + q / 2^15)
+ * exact, the sum rounded down for lower planes and up for upper ones. */
+static inline void qnode_boxes(const uint32_t* w, int eb, orc_aabb* b0, orc_aabb* b1)
+{
+    uint32_t s[3];
+    qnode_scales(w, eb, s);
+    float base[3], l[2][3], h[2][3];
+    memcpy(base, w, 12);
+    for (int a = 0; a < 3; ++a)
+        for (int c = 0; c < 2; ++c)
+        {
+            l[c][a] = add_dir(base[a], qw_value(w[3 + a], s[a], 2 * c), 0);
+            h[c][a] = add_dir(base[a], qw_value(w[3 + a], s[a], 2 * c + 1), 1);
+        }
+    b0->lower = f3(l[0][0], l[0][1], l[0][2]);
+    b0->upper = f3(h[0][0], h[0][1], h[0][2]);
+    b1->lower = f3(l[1][0], l[1][1], l[1][2]);
+    b1->upper = f3(h[1][0], h[1][1], h[1][2]);
+}
+
+/* Checks that every child box of the quantised tree, in exact arithmetic
+ * (base + V: rounded up it is <= a lower plane iff the exact sum is, rounded
+ * down >= an upper one iff the exact sum is), contains the FP32 child box of
+ * the same node. Returns 1 when all do (and the tree is usable: status bit 1
+ * clear). */
 int orc_check_quantised(const orc_node* nodes, uint32_t n, const uint32_t* qnodes, const uint32_t* header)
 {
-    int eBase;
-    memcpy(&eBase, &header[1], 4);
+    int eb;
+    memcpy(&eb, &header[1], 4);
+    if (header[3] & 2u) return 0;
     for (uint32_t i = 0; i + 1 < n; ++i)
     {
-        orc_aabb b[2];
-        qnode_boxes(qnodes + 8 * (size_t)i, eBase, &b[0], &b[1]);
+        const uint32_t* w = qnodes + 8 * (size_t)i;
+        uint32_t s[3];
+        qnode_scales(w, eb, s);
+        float base[3];
+        memcpy(base, w, 12);
         for (int c = 0; c < 2; ++c)
         {
             const orc_aabb* e = &nodes[i].aabbs[c];
-            if (b[c].lower.x > e->lower.x || b[c].lower.y > e->lower.y || b[c].lower.z > e->lower.z ||
-                b[c].upper.x < e->upper.x || b[c].upper.y < e->upper.y || b[c].upper.z < e->upper.z)
-                return 0;
+            const float el[3] = {e->lower.x, e->lower.y, e->lower.z}, eh[3] = {e->upper.x, e->upper.y, e->upper.z};
+            for (int a = 0; a < 3; ++a)
+            {
+                if (add_dir(base[a], qw_value(w[3 + a], s[a], 2 * c), 1) > el[a]) return 0;
+                if (add_dir(base[a], qw_value(w[3 + a], s[a], 2 * c + 1), 0) < eh[a]) return 0;
+            }
         }
     }
     return 1;
@@ -2179,7 +2236,8 @@ int orc_check_quantised(const orc_node* nodes, uint32_t n, const uint32_t* qnode
 typedef struct {
     const uint32_t *qnodes, *parents, *qtris;
     uint32_t root;
-    int eBase;
+    int eb;          /* the tree's scale exponent EB */
+    uint32_t status; /* header[3] */
     const orc_ray* rays;
     int query;
     orc_hit* hits;
@@ -2200,12 +2258,70 @@ static int leaf_box_passes(orc_f3 ro, orc_f3 inv, const orc_f3* v, float tmin, f
     return e <= x;
 }
 
+/* qnode_test (include/mlbvh_device.cuh): the slab test of both children of
+ * quantised node w, as entry / exit pairs clipped to [max(0, tmin), hitT].
+ * fma (a ray for which qwide_ray_fits holds, in a tree whose status is 0):
+ * per axis the near plane (lower where inv > 0, upper where inv < 0) and the
+ * far plane at V inv + C, C = base inv - ro inv, near planes rounded down
+ * with ro inv rounded up, far planes up with ro inv rounded down; the entry
+ * (largest near distance) moved down by 2^-22 of itself, the exit (smallest
+ * far distance) up by 2^-21 of itself, as the quantised slots do. Otherwise
+ * the reference's slabs on the decoded boxes (qnode_boxes). Status bit 1 (a
+ * non-finite coordinate): every box passes. */
+static void qnode_test(const qtrace_ctx* c, const uint32_t* w, orc_f3 ro, orc_f3 inv, float tmin, float hitT, int fma,
+                       float* lmin, float* lmax, float* rmin, float* rmax)
+{
+    if (c->status & 2u)
+    {
+        *lmin = *rmin = smax(0.0f, tmin);
+        *lmax = *rmax = hitT;
+        return;
+    }
+    if (fma)
+    {
+        uint32_t sb[3];
+        qnode_scales(w, c->eb, sb);
+        float base[3];
+        memcpy(base, w, 12);
+        const float r[3] = {ro.x, ro.y, ro.z}, iv[3] = {inv.x, inv.y, inv.z};
+        float e[2], x[2];
+        for (int k = 0; k < 2; ++k)
+        {
+            float en = 0.0f, ex = 0.0f;
+            for (int a = 0; a < 3; ++a)
+            {
+                const int neg = iv[a] < 0.0f;
+                const float cn = fma_dir(base[a], iv[a], -mul_dir(r[a], iv[a], 1), 0);
+                const float cf = fma_dir(base[a], iv[a], -mul_dir(r[a], iv[a], 0), 1);
+                const float tn = fma_dir(qw_value(w[3 + a], sb[a], 2 * k + neg), iv[a], cn, 0);
+                const float tf = fma_dir(qw_value(w[3 + a], sb[a], 2 * k + 1 - neg), iv[a], cf, 1);
+                en = a ? smax(en, tn) : tn;
+                ex = a ? smin(ex, tf) : tf;
+            }
+            e[k] = smax(fma_dir(fabsf(en), -ORC_Q_ENTRY_MARGIN, en, 0), smax(0.0f, tmin));
+            x[k] = smin(fma_dir(fabsf(ex), ORC_Q_EXIT_MARGIN, ex, 1), hitT);
+        }
+        *lmin = e[0];
+        *lmax = x[0];
+        *rmin = e[1];
+        *rmax = x[1];
+        return;
+    }
+    orc_aabb b0, b1;
+    qnode_boxes(w, c->eb, &b0, &b1);
+    slabs(ro, inv, &b0, hitT, lmin, lmax);
+    slabs(ro, inv, &b1, hitT, rmin, rmax);
+    *lmin = smax(*lmin, tmin);
+    *rmin = smax(*rmin, tmin);
+}
+
 /* trace_quantised (include/mlbvh_device.cuh): the stack-free state machine
  * over quantised nodes; "came from the parent" is "came from neither child",
  * and the parent word is read only when moving up. */
 static void qtrace_walk(const qtrace_ctx* c, orc_hit* hit, orc_f3 ro, orc_f3 rd, orc_f3 inv, float tmin, uint32_t curr,
                         uint32_t prev, uint32_t* nv, uint32_t* nt, uint32_t* nu)
 {
+    const int fma = c->status == 0u && qwide_ray_fits(ro, inv);
     while (curr != ORC_INVALID)
     {
         if (curr & ORC_LEAF_BIT)
@@ -2233,14 +2349,9 @@ static void qtrace_walk(const qtrace_ctx* c, orc_hit* hit, orc_f3 ro, orc_f3 rd,
         }
         (*nv)++;
         const uint32_t* w = c->qnodes + 8 * (size_t)curr;
-        orc_aabb b0, b1;
-        qnode_boxes(w, c->eBase, &b0, &b1);
         uint32_t c0 = w[6] & (ORC_LEAF_BIT | ORC_QMASK), c1 = w[7] & (ORC_LEAF_BIT | ORC_QMASK);
         float lmin, lmax, rmin, rmax;
-        slabs(ro, inv, &b0, hit->t, &lmin, &lmax);
-        slabs(ro, inv, &b1, hit->t, &rmin, &rmax);
-        lmin = smax(lmin, tmin);
-        rmin = smax(rmin, tmin);
+        qnode_test(c, w, ro, inv, tmin, hit->t, fma, &lmin, &lmax, &rmin, &rmax);
         int hitL = lmin <= lmax, hitR = rmin <= rmax;
         uint32_t nearN = c0, farN = c1;
         int nHits = 0;
@@ -2285,6 +2396,7 @@ static void qreplay_one(const qtrace_ctx* c, int depth, orc_hit* hit, orc_f3 ro,
                         uint32_t* nt, uint32_t* nu)
 {
     orc_f3 inv = inv_rd(rd);
+    const int fma = c->status == 0u && qwide_ray_fits(ro, inv);
     uint32_t stackNode[64];
     float stackEntry[64];
     int top = 0;
@@ -2316,14 +2428,9 @@ static void qreplay_one(const qtrace_ctx* c, int depth, orc_hit* hit, orc_f3 ro,
         {
             (*nv)++;
             const uint32_t* w = c->qnodes + 8 * (size_t)curr;
-            orc_aabb b0, b1;
-            qnode_boxes(w, c->eBase, &b0, &b1);
             uint32_t c0 = w[6] & (ORC_LEAF_BIT | ORC_QMASK), c1 = w[7] & (ORC_LEAF_BIT | ORC_QMASK);
             float lmin, lmax, rmin, rmax;
-            slabs(ro, inv, &b0, hit->t, &lmin, &lmax);
-            slabs(ro, inv, &b1, hit->t, &rmin, &rmax);
-            lmin = smax(lmin, tmin);
-            rmin = smax(rmin, tmin);
+            qnode_test(c, w, ro, inv, tmin, hit->t, fma, &lmin, &lmax, &rmin, &rmax);
             int hitL = lmin <= lmax, hitR = rmin <= rmax;
             if (hitL && hitR)
             {
@@ -2388,7 +2495,8 @@ void orc_trace_quantised(const uint32_t* qnodes, const uint32_t* parents, const 
     c.parents = parents;
     c.qtris = qtris;
     c.root = header[0];
-    memcpy(&c.eBase, &header[1], 4);
+    memcpy(&c.eb, &header[1], 4);
+    c.status = header[3];
     c.rays = rays;
     c.query = query;
     c.hits = hits;
@@ -2408,7 +2516,8 @@ void orc_trace_quantised_replay(const uint32_t* qnodes, const uint32_t* parents,
     c.parents = parents;
     c.qtris = qtris;
     c.root = header[0];
-    memcpy(&c.eBase, &header[1], 4);
+    memcpy(&c.eb, &header[1], 4);
+    c.status = header[3];
     c.rays = rays;
     c.query = query;
     c.hits = hits;

@@ -148,3 +148,32 @@ def test_quantised_precision_config(cuda):
     np.testing.assert_array_equal(quant[:, 0], plain[:, 0])
     r = F.check_hits(tris, rays, quant)
     assert r["hits"] > 100000 and r["max_bound_ratio"] <= 1.0, r
+
+
+@pytest.mark.parametrize("scale,status", [(1.0, 0), (1e20, 1), (1e37, 2)])
+def test_quantised_status_paths_match_oracle(cuda, scale, status):
+    """The three node tests of the quantised binary tree (the FMA form; the
+    reference's slabs on the decoded boxes, for status bit 0 and for rays with
+    a zero direction component; every box passing, for status bit 1) give the
+    oracle's nodes, header, Hit records and per-ray counts on both walks, and
+    the FP32 tree's closest hits."""
+    import torch
+    rng = np.random.default_rng(31)
+    tris = ((rng.random((3000, 9)) - 0.5) * scale).astype(np.float32)
+    b, t, out, qb, gq, ref = quantise_both(tris)
+    for k in ("qnodes", "parents", "qtris", "header"):
+        np.testing.assert_array_equal(gq[k], ref[k], err_msg=k)
+    assert int(gq["header"][3]) == status
+    rays = scenes.random_rays(3000, [-0.5 * scale] * 3, [0.5 * scale] * 3, seed=32)
+    rays[0::3, 4 + (np.arange(0, 3000, 3) % 3)] = 0.0  # zero components: outside the FMA form's range
+    n = len(rays)
+    for depth in (0, 4):
+        counts = torch.zeros(3 * n, dtype=torch.int32, device="cuda")
+        got = G.host(mb.intersect_quantised(qb, G.dev(rays), 0, stack_depth=depth, counts=counts), np.uint32)
+        hits, nv, nt, nu = O.trace_quantised(ref, rays, 0, counters=True, stack_depth=depth)
+        np.testing.assert_array_equal(got, hits)
+        c = G.host(counts, np.uint32)
+        np.testing.assert_array_equal(c[:n], nv, err_msg="node visits")
+        np.testing.assert_array_equal(c[n:2 * n], nt, err_msg="triangle tests")
+    plain = O.trace(out["nodes"], tris, out["root"], rays, 0, 0)
+    np.testing.assert_array_equal(got[:, 7], plain[:, 7])

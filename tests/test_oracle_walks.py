@@ -422,3 +422,35 @@ def test_directed_fma_emulation_is_exact():
             want = _round_dir(exact, up)
             assert got == want or (np.isinf(got) and np.isinf(want) and got == want), (a, b, c, up, got, want)
 
+
+
+def _axis_rays(n, lo, hi, seed):
+    """Random rays, a third of them with one direction component exactly 0
+    (the reference clamps its inverse to +-FLT_MAX, outside the FMA form's
+    range): those take the decoded-box slab test."""
+    rays = scenes.random_rays(n, lo, hi, seed=seed)
+    rays[0::3, 4 + (np.arange(0, n, 3) % 3)] = 0.0
+    return rays
+
+
+@pytest.mark.parametrize("scale,status", [(1.0, 0), (1e20, 1), (1e37, 2)])
+def test_quantised_status_paths_find_fp32_hits(scale, status):
+    """The quantised binary tree's three node tests: the FMA form (status 0,
+    rays within its range), the reference's slabs on the decoded boxes
+    (status bit 0: coordinates near 1e20 give bases beyond 2^60; also every
+    ray outside the FMA form's range) and every box passing (status bit 1: a
+    scale exponent above 127 at about 1e37). Each returns the FP32 tree's
+    closest hits; the replay walk returns the stack-free walk's Hit records."""
+    rng = np.random.default_rng(31)
+    tris = ((rng.random((3000, 9)) - 0.5) * scale).astype(np.float32)
+    b = O.build(tris)
+    q = O.quantise(b, tris)
+    assert int(q["header"][3]) == status
+    if status != 2:
+        assert O.oracle().orc_check_quantised(O.P(b["nodes"]), len(tris), O.P(q["qnodes"]), O.P(q["header"])) == 1
+    rays = _axis_rays(3000, [-0.5 * scale] * 3, [0.5 * scale] * 3, seed=32)
+    got = O.trace_quantised(q, rays, 0)
+    plain = O.trace(b["nodes"], tris, b["root"], rays, 0, 0)
+    np.testing.assert_array_equal(got[:, 7], plain[:, 7])
+    np.testing.assert_array_equal(got[:, 0], plain[:, 0])
+    np.testing.assert_array_equal(O.trace_quantised(q, rays, 0, stack_depth=4), got)
