@@ -24,6 +24,19 @@ namespace {
 
 constexpr int kDiffThreads = 128;
 constexpr int kMaxBounces = 8;
+// Lanes per pixel: one warp per pixel, lane l tracing samples l, l + 32, ...
+// in order; the render adds the lanes' partial sums as a pairwise tree in lane
+// order ((p0 + p1) + (p2 + p3)) + ... . Measured on the differentiation
+// workload (forward / adjoint ms): one thread per pixel 35.3 / 32.3 (2.3 waves
+// of long CTAs, the last on a third of the SMs), 2 lanes 30.1 / 27.1, 4 lanes
+// 26.5 / 23.3, 8 lanes 24.4 / 21.0, 16 lanes 23.2 / 19.6, 32 lanes 22.7 / 18.3:
+// a pixel's samples start from nearby rays, so its warp walks the same nodes.
+// (Build-time override for sweeps: -DMLBVH_DIFF_LANES=2, 4, 8 or 16.)
+#ifndef MLBVH_DIFF_LANES
+#define MLBVH_DIFF_LANES 32
+#endif
+constexpr int kLanesPerPixel = MLBVH_DIFF_LANES;
+static_assert(kDiffThreads % kLanesPerPixel == 0, "a pixel's lanes share a warp");
 constexpr int kDiffStack = 16;  // replay-walk stack entries per thread (shared memory)
 
 // intersect_stackfree's closest hit (minimum_lbvh.h:981-1061) through the
@@ -106,26 +119,33 @@ __device__ __forceinline__ Camera camera_of(const mlbvh_ray_generator& g)
     return c;
 }
 
-__global__ void __launch_bounds__(kDiffThreads)
+__global__ void __launch_bounds__(kDiffThreads, 6)
     k_pt_diff_render(float* __restrict__ image, int w, int h, int spp, int bounces, mlbvh_ray_generator gen,
                      const mlbvh_node_index* __restrict__ rootPtr, const mlbvh_internal_node* __restrict__ nodes,
                      const float* __restrict__ tris, const float* __restrict__ albedo,
                      const float* __restrict__ emission)
 {
     __shared__ uint2 s_stack[kDiffStack][kDiffThreads];
-    const int p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= w * h) return;
-    const int xi = p % w, yi = p / w;
-    const Camera cam = camera_of(gen);
-    const uint32_t root = __ldg(rootPtr);
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int p = t / kLanesPerPixel, lane = t % kLanesPerPixel;
+    const bool valid = p < w * h;  // every lane takes part in the shuffles below
     float sum = 0.0f;
-    for (int s = 0; s < spp; ++s) {
-        float L = 0.0f;
-        trace_path<false>(nullptr, &L, bounces, (uint32_t)s, xi, yi, w, h, cam, root, nodes, tris, albedo, emission,
-                          &s_stack[0][threadIdx.x]);
-        sum += L;
+    if (valid) {
+        const int xi = p % w, yi = p / w;
+        const Camera cam = camera_of(gen);
+        const uint32_t root = __ldg(rootPtr);
+        for (int s = lane; s < spp; s += kLanesPerPixel) {
+            float L = 0.0f;
+            trace_path<false>(nullptr, &L, bounces, (uint32_t)s, xi, yi, w, h, cam, root, nodes, tris, albedo,
+                              emission, &s_stack[0][threadIdx.x]);
+            sum += L;
+        }
     }
-    image[p] = sum / (float)spp;
+    // the pairwise tree in lane order: after step o every lane holds the sum of
+    // its aligned group of 2o lanes, the same bits on each (a + b == b + a)
+#pragma unroll
+    for (int o = 1; o < kLanesPerPixel; o <<= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+    if (valid && lane == 0) image[p] = sum / (float)spp;
 }
 
 __global__ void __launch_bounds__(kDiffThreads)
@@ -135,7 +155,8 @@ __global__ void __launch_bounds__(kDiffThreads)
                       const float* __restrict__ albedo, const float* __restrict__ emission)
 {
     __shared__ uint2 s_stack[kDiffStack][kDiffThreads];
-    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int p = t / kLanesPerPixel, lane = t % kLanesPerPixel;
     if (p >= w * h) return;
     const float g = __ldg(gradImage + p) / (float)spp;
     if (g == 0.0f) return;
@@ -143,7 +164,7 @@ __global__ void __launch_bounds__(kDiffThreads)
     const Camera cam = camera_of(gen);
     const uint32_t root = __ldg(rootPtr);
     PathVertex v[kMaxBounces + 1];
-    for (int s = 0; s < spp; ++s) {
+    for (int s = lane; s < spp; s += kLanesPerPixel) {
         const int n = trace_path<true>(v, nullptr, bounces, (uint32_t)s, xi, yi, w, h, cam, root, nodes, tris, albedo,
                                        emission, &s_stack[0][threadIdx.x]);
         // suffix sums of the collected radiance: the part of L that depends on
@@ -151,8 +172,8 @@ __global__ void __launch_bounds__(kDiffThreads)
         float after = 0.0f;
         for (int j = n - 1; j >= 0; --j) {
             if (j < bounces && after != 0.0f) {
-                const uint32_t t = v[j].tri;
-                atomicAdd(grad + t, g * after / __ldg(albedo + t));
+                const uint32_t tj = v[j].tri;
+                atomicAdd(grad + tj, g * after / __ldg(albedo + tj));
             }
             after += v[j].collected;
         }
@@ -180,8 +201,9 @@ mlbvh_status pt_diff_render(float* dImage, int w, int h, int spp, int bounces, c
 {
     if (mlbvh_status s = check_diff_args(w, h, spp, bounces, dImage, dRoot, dTris, dAlbedo, dEmission)) return s;
     if (!aligned32(dNodes)) return fail(MLBVH_ERR_INVALID_ARG, "device pointers must be 16-byte aligned");
-    const int px = w * h;
-    k_pt_diff_render<<<(px + kDiffThreads - 1) / kDiffThreads, kDiffThreads, 0, stream>>>(
+    const long long threads = (long long)w * h * kLanesPerPixel;
+    if (threads >= (1ll << 31)) return fail(MLBVH_ERR_INVALID_ARG, "bad image size");
+    k_pt_diff_render<<<(unsigned)((threads + kDiffThreads - 1) / kDiffThreads), kDiffThreads, 0, stream>>>(
         dImage, w, h, spp, bounces, cam, dRoot, dNodes, reinterpret_cast<const float*>(dTris), dAlbedo, dEmission);
     MLBVH_CHECK_LAUNCH("k_pt_diff_render");
     return MLBVH_OK;
@@ -195,8 +217,9 @@ mlbvh_status pt_diff_adjoint(float* dGrad, const float* dGradImage, int w, int h
     if (mlbvh_status s = check_diff_args(w, h, spp, bounces, dGrad, dRoot, dTris, dAlbedo, dEmission)) return s;
     if (!dGradImage || !aligned16(dGradImage) || !aligned32(dNodes))
         return fail(MLBVH_ERR_INVALID_ARG, "null or misaligned pointer");
-    const int px = w * h;
-    k_pt_diff_adjoint<<<(px + kDiffThreads - 1) / kDiffThreads, kDiffThreads, 0, stream>>>(
+    const long long threads = (long long)w * h * kLanesPerPixel;
+    if (threads >= (1ll << 31)) return fail(MLBVH_ERR_INVALID_ARG, "bad image size");
+    k_pt_diff_adjoint<<<(unsigned)((threads + kDiffThreads - 1) / kDiffThreads), kDiffThreads, 0, stream>>>(
         dGrad, dGradImage, w, h, spp, bounces, cam, dRoot, dNodes, reinterpret_cast<const float*>(dTris), dAlbedo,
         dEmission);
     MLBVH_CHECK_LAUNCH("k_pt_diff_adjoint");

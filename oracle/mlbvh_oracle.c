@@ -2598,6 +2598,10 @@ static void atomic_add_double(double* p, double v)
     } while (!__atomic_compare_exchange_n((uint64_t*)p, &old, upd, 1, __ATOMIC_RELAXED, __ATOMIC_RELAXED));
 }
 
+/* k_pt_diff_render gives each pixel a warp: lane l sums the radiance of
+ * samples l, l + 32, ... in order, and the pixel's sum is the pairwise tree of
+ * the lanes' sums in lane order, ((p0 + p1) + (p2 + p3)) + ... */
+#define ORC_DIFF_LANES 32
 static void diff_rows(void* p, uint32_t b, uint32_t e)
 {
     diff_ctx* c = (diff_ctx*)p;
@@ -2606,7 +2610,7 @@ static void diff_rows(void* p, uint32_t b, uint32_t e)
         for (int x = 0; x < c->w; ++x)
         {
             int px = x + (int)y * c->w;
-            float sum32 = 0.0f;
+            float part32[ORC_DIFF_LANES] = {0.0f};
             double sum64 = 0.0;
             double g = c->gradImage ? c->gradImage[px] / (double)c->spp : 0.0;
             for (int s = 0; s < c->spp; ++s)
@@ -2622,7 +2626,7 @@ static void diff_rows(void* p, uint32_t b, uint32_t e)
                         if (d < c->bounces) thr = thr * c->albedo32[tri[d]];
                     }
                     for (int d = 0; d < n; ++d) L += coll[d];
-                    sum32 += L;
+                    part32[s % ORC_DIFF_LANES] += L; /* the pixel's lane s % 32, its samples in order */
                 }
                 if (c->image64 || c->grad)
                 {
@@ -2646,7 +2650,12 @@ static void diff_rows(void* p, uint32_t b, uint32_t e)
                     }
                 }
             }
-            if (c->image32) c->image32[px] = sum32 / (float)c->spp;
+            if (c->image32)
+            {
+                for (int width = ORC_DIFF_LANES; width > 1; width /= 2)
+                    for (int i = 0; i < width / 2; ++i) part32[i] = part32[2 * i] + part32[2 * i + 1];
+                c->image32[px] = part32[0] / (float)c->spp;
+            }
             if (c->image64) c->image64[px] = sum64 / (double)c->spp;
         }
 }

@@ -37,10 +37,14 @@ def pick(grad, k=32, seed=5):
     return np.sort(rng.choice(big, size=min(k, len(big)), replace=False))
 
 
-def test_diff_render_matches_oracle(scene):
+@pytest.mark.parametrize("w,h,spp", [(96, 64, 8), (48, 40, 37), (40, 32, 64)])
+def test_diff_render_matches_oracle(scene, w, h, spp):
+    """Bit for bit: a pixel's samples are spread over the 32 lanes of a warp
+    (lane l: samples l, l + 32, ...) and added as a pairwise tree in lane order;
+    fewer samples than lanes, a count that is not a multiple of 32, and two
+    samples per lane."""
     import torch
     tris, alb, em, b, t, out = scene
-    w, h, spp = 96, 64, 8
     cam = camera(w, h)
     img = torch.empty(w * h, dtype=torch.float32, device="cuda")
     mb.pt_diff_render(img, (w, h), cam, b, t, G.dev(alb), G.dev(em), spp, 3)
