@@ -22,7 +22,14 @@ namespace mlbvh {
 
 namespace {
 
-constexpr int kDiffThreads = 128;
+// Threads per CTA: one pixel's warp (measured forward / adjoint ms: 22.6 / 18.0
+// against 22.6 / 18.3 for 64 and 22.7 / 19.1 for 128, where a CTA holds its
+// slot until its slowest pixel is done); compiled for 768 threads per SM (80
+// registers). Build-time override for sweeps: -DMLBVH_DIFF_THREADS.
+#ifndef MLBVH_DIFF_THREADS
+#define MLBVH_DIFF_THREADS 32
+#endif
+constexpr int kDiffThreads = MLBVH_DIFF_THREADS;
 constexpr int kMaxBounces = 8;
 // Lanes per pixel: one warp per pixel, lane l tracing samples l, l + 32, ...
 // in order; the render adds the lanes' partial sums as a pairwise tree in lane
@@ -119,7 +126,7 @@ __device__ __forceinline__ Camera camera_of(const mlbvh_ray_generator& g)
     return c;
 }
 
-__global__ void __launch_bounds__(kDiffThreads, 6)
+__global__ void __launch_bounds__(kDiffThreads, 768 / kDiffThreads)
     k_pt_diff_render(float* __restrict__ image, int w, int h, int spp, int bounces, mlbvh_ray_generator gen,
                      const mlbvh_node_index* __restrict__ rootPtr, const mlbvh_internal_node* __restrict__ nodes,
                      const float* __restrict__ tris, const float* __restrict__ albedo,
@@ -148,7 +155,7 @@ __global__ void __launch_bounds__(kDiffThreads, 6)
     if (valid && lane == 0) image[p] = sum / (float)spp;
 }
 
-__global__ void __launch_bounds__(kDiffThreads)
+__global__ void __launch_bounds__(kDiffThreads, 768 / kDiffThreads)
     k_pt_diff_adjoint(float* __restrict__ grad, const float* __restrict__ gradImage, int w, int h, int spp,
                       int bounces, mlbvh_ray_generator gen, const mlbvh_node_index* __restrict__ rootPtr,
                       const mlbvh_internal_node* __restrict__ nodes, const float* __restrict__ tris,
