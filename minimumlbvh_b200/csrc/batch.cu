@@ -48,7 +48,8 @@ constexpr int kStageTris = 256;    // triangles staged in shared memory per step
 constexpr int kBuildThreads = (int)kTileLeaves;  // build: one CTA per tile of the climb
 constexpr uint32_t kDefaultSpinLimit = 1u << 22;
 constexpr uint32_t kMaxMeshes = 1u << 20;
-constexpr uint32_t kErrTimeout = 1u, kErrOffsets = 2u;
+// error word bits: 1 a bounded wait gave up (set by sort::k_onesweep), 2 bad offsets
+constexpr uint32_t kErrOffsets = 2u;
 
 // header words
 constexpr int kHdrError = 0;

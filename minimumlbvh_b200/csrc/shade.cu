@@ -98,6 +98,26 @@ __device__ __forceinline__ bool tile_pixel(int w, int h, int& xi, int& yi)
     return xi < w && yi < h;
 }
 
+// The path tracer's own tiles: kPtWarps warps of 8 x 4 pixels (1: 8 x 4,
+// 2: 16 x 4, 4: 16 x 8, the other kernels' tile). A CTA holds its slot until
+// its longest path is done, and Russian roulette makes path lengths differ
+// widely; measured on the bench's PT pass (replay walk): 0.615 / 0.621 / 0.626
+// ms (build-time override for sweeps: -DMLBVH_PT_WARPS).
+#ifndef MLBVH_PT_WARPS
+#define MLBVH_PT_WARPS 1
+#endif
+constexpr int kPtWarps = MLBVH_PT_WARPS;
+static_assert(kPtWarps == 1 || kPtWarps == 2 || kPtWarps == 4, "1, 2 or 4 warps per path-tracing tile");
+constexpr int kPtThreads = 32 * kPtWarps;
+constexpr int kPtTileW = kPtWarps >= 2 ? 16 : 8, kPtTileH = kPtWarps == 4 ? 8 : 4;
+__device__ __forceinline__ bool pt_pixel(int w, int h, int& xi, int& yi)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    xi = blockIdx.x * kPtTileW + (lane & 7) + 8 * (warp & 1);
+    yi = blockIdx.y * kPtTileH + (lane >> 3) + 4 * (warp >> 1);
+    return xi < w && yi < h;
+}
+
 // PCG32 jump-ahead by `delta` steps (Brown, "Random Number Generation with
 // Arbitrary Strides", 1994), so that AO sample i can start at draw 2i.
 __device__ __forceinline__ void pcg_advance(Pcg& r, uint64_t delta)
@@ -685,15 +705,15 @@ struct PtRandom {
 // reference; the replay trees: the same Hit records from a per-thread stack
 // of pending far children in shared memory), so the accumulators are the same.
 template <class Tree>
-__global__ void __launch_bounds__(kTileW* kTileH)
+__global__ void __launch_bounds__(kPtThreads)
     k_pt(float4* __restrict__ accum, mlbvh_ray_generator gen, int w, int h, Tree tree,
          const float* __restrict__ attribs, int useSobol, int maxSPP, int maxDepth)
 {
-    __shared__ uint2 s_pstack[Tree::kPrimaryStack > 0 ? Tree::kPrimaryStack : 1][kTileW * kTileH];
+    __shared__ uint2 s_pstack[Tree::kPrimaryStack > 0 ? Tree::kPrimaryStack : 1][kPtThreads];
     uint2* const pstack = &s_pstack[0][threadIdx.x];
     Counts cnt;
     int xi, yi;
-    if (!tile_pixel(w, h, xi, yi)) return;
+    if (!pt_pixel(w, h, xi, yi)) return;
     const Camera cam = to_camera(gen);
     const int pixel = xi + yi * w;
     float4 acc = accum[pixel];
@@ -709,7 +729,7 @@ __global__ void __launch_bounds__(kTileW* kTileH)
     HitRecord hit;
     hit.t = kFltMax;
     hit.tri = 0xFFFFFFFFu;
-    tree.template trace<false, false>(ctx, hit, ro, rd, cnt, pstack, kTileW * kTileH);
+    tree.template trace<false, false>(ctx, hit, ro, rd, cnt, pstack, kPtThreads);
     if (hit.t != kFltMax)
         for (int depth = 0; depth < maxDepth; depth++) {
             const float2 r2 = rr.next();
@@ -735,7 +755,7 @@ __global__ void __launch_bounds__(kTileW* kTileH)
             hit.u = hit.v = 0.0f;
             hit.ng = mk(0.0f, 0.0f, 0.0f);
             hit.tri = 0xFFFFFFFFu;
-            tree.template trace<false, false>(ctx, hit, next_ro, next_rd, cnt, pstack, kTileW * kTileH);
+            tree.template trace<false, false>(ctx, hit, next_ro, next_rd, cnt, pstack, kPtThreads);
             if (hit.t == kFltMax) break;
             ro = next_ro;
             rd = next_rd;
@@ -952,15 +972,15 @@ mlbvh_status render_pt(float* dAccum, int w, int h, const mlbvh_ray_generator& c
     float4* acc = reinterpret_cast<float4*>(dAccum);
     const float* tris = reinterpret_cast<const float*>(dTris);
     const float* at = reinterpret_cast<const float*>(dAttribs);
-    const dim3 grid = tile_grid(w, h);
+    const dim3 grid((unsigned)((w + kPtTileW - 1) / kPtTileW), (unsigned)((h + kPtTileH - 1) / kPtTileH));
     if (traversal == MLBVH_TRAVERSAL_REPLAY && dLeafTris)
-        k_pt<<<grid, kTileW * kTileH, 0, stream>>>(acc, cam, w, h, PlainReplayLeafTree{dNodes, tris, dRoot, dLeafTris},
+        k_pt<<<grid, kPtThreads, 0, stream>>>(acc, cam, w, h, PlainReplayLeafTree{dNodes, tris, dRoot, dLeafTris},
                                                    at, useSobol, maxSPP, maxDepth);
     else if (traversal == MLBVH_TRAVERSAL_REPLAY)
-        k_pt<<<grid, kTileW * kTileH, 0, stream>>>(acc, cam, w, h, PlainReplayTree{dNodes, tris, dRoot, nullptr}, at,
+        k_pt<<<grid, kPtThreads, 0, stream>>>(acc, cam, w, h, PlainReplayTree{dNodes, tris, dRoot, nullptr}, at,
                                                    useSobol, maxSPP, maxDepth);
     else
-        k_pt<<<grid, kTileW * kTileH, 0, stream>>>(acc, cam, w, h, PlainTree{dNodes, tris, dRoot, nullptr}, at,
+        k_pt<<<grid, kPtThreads, 0, stream>>>(acc, cam, w, h, PlainTree{dNodes, tris, dRoot, nullptr}, at,
                                                    useSobol, maxSPP, maxDepth);
     MLBVH_CHECK_LAUNCH("k_pt");
     return MLBVH_OK;
