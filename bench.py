@@ -348,7 +348,7 @@ def bench_batched(args, dev, stream, barrier, max_over_ranks, world, n_meshes=10
     barrier()
     pb_s = max_over_ranks(pev[0].elapsed_time(pev[1]) / 1e3)
     pt_s = max_over_ranks(pev[1].elapsed_time(pev[2]) / 1e3)
-    agree = float((plain_hits == hits).all(1).float().mean().item())
+    agree = float((plain_hits == hits).all(1).double().mean().item())
     return {
         "workload": f"batched{nm}", "meshes": nm, "triangles": n, "rays": nr,
         "value": nr * world / trace_s / 1e6, "unit": "Mrays/s (persistent queue traversal)",
@@ -540,7 +540,7 @@ def bench_pt(args, dev, stream, max_over_ranks, reference_gpu=False):
                               "vs_lbvh_replay": out["replay"]["ms_per_pass"] / (sec * 1e3 / args.steps),
                               "vs_plain": out["plain"]["ms_per_pass"] / (sec * 1e3 / args.steps),
                               "mean_radiance": mean_rad(acc), "lbvh_mean_radiance": mean_rad(accs["replay"]),
-                              "pixels_equal_to_lbvh": float((acc == accs["replay"]).all(1).float().mean().item())}
+                              "pixels_equal_to_lbvh": float((acc == accs["replay"]).all(1).double().mean().item())}
     out["workload"] = "heightfield + icospheres (212,992 triangles), 512x512, 1 % emissive, up to 1024 bounces"
     if reference_gpu and os.path.exists(REF_GPU_LIB):
         # 512 is a multiple of the reference's 16 x 16 blocks: its grid covers the image exactly
@@ -752,7 +752,7 @@ def bench_ploc(args, wl, d_tris, n, cam, w, h, dev, stream, barrier, max_over_ra
         lb_ms = lbvh_forms[name]
         out["forms"][name] = {"ms_per_frame": t * 1e3, "mrays_s": lbvh_forms["rays_per_frame"] / t / 1e6,
                               "lbvh_ms_per_frame": lb_ms, "vs_lbvh_same_form": lb_ms / (t * 1e3),
-                              "occlusion_agreement_with_lbvh": float((occ == occ_plain).float().mean().item())}
+                              "occlusion_agreement_with_lbvh": float((occ == occ_plain).double().mean().item())}
     # closest hits of camera rays (every other pixel of the frame): the replay
     # walk over both trees; the same distances (the triangle may differ only
     # where two meet a ray at the same distance)
@@ -777,8 +777,8 @@ def bench_ploc(args, wl, d_tris, n, cam, w, h, dev, stream, barrier, max_over_ra
         cam_out[name + "_mrays_s"] = nr / t / 1e6
         hits[name] = hb
     cam_out["vs_lbvh"] = cam_out["ploc_mrays_s"] / cam_out["lbvh_mrays_s"]
-    cam_out["t_equal"] = float((hits["lbvh"][:, 0] == hits["ploc"][:, 0]).float().mean().item())
-    cam_out["triangle_equal"] = float((hits["lbvh"][:, 7] == hits["ploc"][:, 7]).float().mean().item())
+    cam_out["t_equal"] = float((hits["lbvh"][:, 0] == hits["ploc"][:, 0]).double().mean().item())
+    cam_out["triangle_equal"] = float((hits["lbvh"][:, 7] == hits["ploc"][:, 7]).double().mean().item())
     # the same rays on the closest-hit walk over each tree's 4-wide regrouping
     # (leaf-ordered triangles: neighbouring leaves share cache lines), with
     # the walk's per-ray wide-node visits and triangle tests
@@ -803,7 +803,7 @@ def bench_ploc(args, wl, d_tris, n, cam, w, h, dev, stream, barrier, max_over_ra
         cam_out[name + "_wide_mrays_s"] = nr / t / 1e6
         cam_out[name + "_wide_node_visits_per_ray"] = c[:nr].sum() / nr
         cam_out[name + "_wide_tri_tests_per_ray"] = c[nr:2 * nr].sum() / nr
-        cam_out[name + "_wide_t_equal_replay"] = float((hw[:, 0] == hits[name][:, 0]).float().mean().item())
+        cam_out[name + "_wide_t_equal_replay"] = float((hw[:, 0] == hits[name][:, 0]).double().mean().item())
     cam_out["wide_vs_lbvh"] = cam_out["ploc_wide_mrays_s"] / cam_out["lbvh_wide_mrays_s"]
     out["camera_rays_closest"] = cam_out
     out["launches"] = launches
@@ -1239,7 +1239,7 @@ def main():
             torch.cuda.synchronize()
             barrier()
             forms[name] = (max_over_ranks(sum(a.elapsed_time(b) for a, b in fev) / 1e3),
-                           float((occ_plain == occ).float().mean().item()), fst.cpu().numpy(),
+                           float((occ_plain == occ).double().mean().item()), fst.cpu().numpy(),
                            float(np.mean([a.elapsed_time(b) for a, b in fkev])) / 1e3)
             form_occ_host[name] = occ.cpu().numpy().view(np.uint32)
 
