@@ -119,7 +119,8 @@ typedef struct mlbvh_qheader {
     uint32_t nTriangles;
     uint32_t status; /* bit 0: a base of 2^60 or more or a scale above 2^59 (the walks then
                         test the decoded boxes with the reference's slabs); bit 1: a
-                        non-finite coordinate (every box then passes) */
+                        non-finite coordinate, or a root box so large that its scale
+                        exponent would exceed 127 (about 1e36; every box then passes) */
 } mlbvh_qheader;
 
 /* The 4-wide tree for any-hit rays (no reference counterpart): a 4-wide
