@@ -1123,8 +1123,8 @@ def main():
     stats = torch.zeros(8, dtype=torch.int64, device=dev)
     stream = torch.cuda.current_stream()
 
-    def ao_frame(with_stats=False, tris_buf=None):
-        mb.render_ao(pixels, (w, h), cam, builder.m_rootNode, builder.m_internals,
+    def ao_frame(with_stats=False, tris_buf=None, out=None):
+        mb.render_ao(pixels if out is None else out, (w, h), cam, builder.m_rootNode, builder.m_internals,
                      d_tris if tris_buf is None else tris_buf, 1, wl["ns"], wl["radius"], 12345,
                      stats=stats if with_stats else None)
 
@@ -1274,12 +1274,26 @@ def main():
         # its triangles from pinned host memory, builds, renders and reads the
         # image back. Two device triangle buffers: step i + 1's upload (copy
         # stream) overlaps step i's build and frame; a buffer is refilled only
-        # after the step that read it is done.
+        # after the step that read it is done. Two image buffers: step i's
+        # read-back (a second copy stream) overlaps step i + 1; an image buffer
+        # is rendered into again only after its read-back is done. The timed
+        # region ends after the last read-back.
         eev = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
         copy_stream = torch.cuda.Stream(device=dev)
+        d2h_stream = torch.cuda.Stream(device=dev)
         bufs = (d_tris, torch.empty_like(d_tris))
+        pix = (pixels, torch.zeros_like(pixels))
+        hpix = (host_pixels, torch.empty_like(host_pixels).pin_memory())
+
+        def read_back(i, done):
+            d2h_stream.wait_event(done[i])
+            with torch.cuda.stream(d2h_stream):
+                hpix[i % 2].copy_(pix[i % 2], non_blocking=True)
+            read[i].record(d2h_stream)
+
         ready = [torch.cuda.Event() for _ in range(args.steps)]
         done = [torch.cuda.Event() for _ in range(args.steps)]
+        read = [torch.cuda.Event() for _ in range(args.steps)]
         barrier()
         torch.cuda.synchronize()
         eev[0].record(stream)
@@ -1292,10 +1306,13 @@ def main():
                 buf.copy_(host_tris, non_blocking=True)
             ready[i].record(copy_stream)
             stream.wait_event(ready[i])
+            if i >= 2:
+                stream.wait_event(read[i - 2])
             builder.build(buf, n, 0, sorter)
-            ao_frame(tris_buf=buf)
-            host_pixels.copy_(pixels, non_blocking=True)
+            ao_frame(tris_buf=buf, out=pix[i % 2])
             done[i].record(stream)
+            read_back(i, done)
+        stream.wait_event(read[args.steps - 1])
         eev[1].record(stream)
         torch.cuda.synchronize()
         barrier()
@@ -1308,6 +1325,7 @@ def main():
         cev = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
         ready = [torch.cuda.Event() for _ in range(args.steps)]
         done = [torch.cuda.Event() for _ in range(args.steps)]
+        read = [torch.cuda.Event() for _ in range(args.steps)]
         barrier()
         torch.cuda.synchronize()
         cev[0].record(stream)
@@ -1320,11 +1338,14 @@ def main():
                 buf.copy_(host_tris, non_blocking=True)
             ready[i].record(copy_stream)
             stream.wait_event(ready[i])
+            if i >= 2:
+                stream.wait_event(read[i - 2])
             builder.build(buf, n, 0, sorter)
             wides[i % 2].update(stream)
-            mb.render_ao_wide(pixels, (w, h), cam, wides[i % 2], 1, wl["ns"], wl["radius"], 12345)
-            host_pixels.copy_(pixels, non_blocking=True)
+            mb.render_ao_wide(pix[i % 2], (w, h), cam, wides[i % 2], 1, wl["ns"], wl["radius"], 12345)
             done[i].record(stream)
+            read_back(i, done)
+        stream.wait_event(read[args.steps - 1])
         cev[1].record(stream)
         torch.cuda.synchronize()
         barrier()
@@ -1395,7 +1416,7 @@ def main():
     line["e2e"] = {"value": rays_per_frame * args.steps * world / e2e_s / 1e6, "unit": "Mrays/s",
                    "h2d_bytes_per_step": int(host_tris.numel() * 4), "d2h_bytes_per_step": int(w * h * 4),
                    "ms_per_step": e2e_s * 1e3 / args.steps,
-                   "pipeline": "upload of step i+1 overlaps build + frame of step i (two device triangle buffers)"}
+                   "pipeline": "upload of step i+1 overlaps build + frame of step i (two device triangle buffers); read-back of step i overlaps step i+1 (two image buffers)"}
     line["e2e_chosen"] = {"value": rays_per_frame * args.steps * world / e2e_chosen_s / 1e6, "unit": "Mrays/s",
                           "h2d_bytes_per_step": int(host_tris.numel() * 4), "d2h_bytes_per_step": int(w * h * 4),
                           "ms_per_step": e2e_chosen_s * 1e3 / args.steps,
