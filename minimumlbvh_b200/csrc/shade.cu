@@ -41,6 +41,11 @@ constexpr int kAoThreads = 128;
 #ifndef MLBVH_AO_QUANT_MIN_BLOCKS
 #define MLBVH_AO_QUANT_MIN_BLOCKS 9
 #endif
+// resident CTAs per SM of the AO kernel over quantised 4-wide slots (swept: 9
+// and 10, at 56 and 48 registers, ran 3 and 4 % slower than 8 at 63)
+#ifndef MLBVH_AO_QWIDE_MIN_BLOCKS
+#define MLBVH_AO_QWIDE_MIN_BLOCKS 8
+#endif
 // the stack-free walk's own (swept: 4 steps and a batch of 16 lanes beat 3 and
 // 8 by 1.7 %; a batch of 24 loses 7 %)
 // the wide trees' refill batch (swept 4-16: 8 is best for the quantised slots,
@@ -350,6 +355,7 @@ struct WideTreeT {
     static constexpr int kPrimaryStack = PlainReplayLeafTree::kStack;
     static constexpr int kSteps = kQuant ? MLBVH_AO_QWIDE_STEPS_PER_ROUND : MLBVH_AO_WIDE_STEPS_PER_ROUND;
     static constexpr int kStartBatch = MLBVH_AO_WIDE_START_BATCH;
+    static constexpr int kMinBlocks = kQuant ? MLBVH_AO_QWIDE_MIN_BLOCKS : MLBVH_AO_MIN_BLOCKS;
     __device__ __forceinline__ Ctx context() const
     {
         const uint32_t r = __ldg(binary.rootPtr);
