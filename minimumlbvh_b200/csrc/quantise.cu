@@ -18,7 +18,14 @@ namespace mlbvh {
 namespace {
 
 constexpr int kQuantiseThreads = 256;
-constexpr int kTraceThreads = 128;
+// Threads per CTA of k_trace_quantised: a CTA holds its slot until its longest
+// ray is done (1M camera / random rays of the 4M soup, replay walk: 128 threads
+// 0.599 / 1.59 ms, 64 0.578 / 1.52, 32 0.604 / 1.57). Build-time override for
+// sweeps: -DMLBVH_QTRACE_THREADS.
+#ifndef MLBVH_QTRACE_THREADS
+#define MLBVH_QTRACE_THREADS 64
+#endif
+constexpr int kTraceThreads = MLBVH_QTRACE_THREADS;
 
 __device__ __forceinline__ void leaf_box(const float* __restrict__ tris, uint32_t t, f3& lo, f3& hi)
 {
