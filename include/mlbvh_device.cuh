@@ -19,6 +19,7 @@
 
 #include "mlbvh.h"
 
+
 namespace mlbvh {
 
 constexpr float kFltMax = 3.402823466e+38F;  // minimum_lbvh.h:37
@@ -868,6 +869,10 @@ __device__ __forceinline__ void qnode_box(const QNodeWords& n, int c, f3& lo, f3
 // passes on the exact box. Otherwise the reference's slabs on the decoded
 // boxes (qnode_box), conservative at any magnitude. A tree with a
 // non-finite coordinate (status bit 1) lets every box pass.
+// kPacked takes both children's planes as packed FP32 pairs (the same
+// values); the any-hit walks use it (AO rays 1.7 % faster), the closest-hit
+// walks do not (camera rays 3.8 % slower with it).
+template <bool kPacked>
 __device__ __forceinline__ float4 qnode_test(const QNodeWords& n, const QParams& qp, f3 ro, f3 inv, float tmin,
                                              float hitT)
 {
@@ -888,19 +893,44 @@ __device__ __forceinline__ float4 qnode_test(const QNodeWords& n, const QParams&
         const uint32_t qy = __byte_perm(n.q[1], 0u, inv.y < 0.0f ? 0x2301u : 0x3210u);
         const uint32_t qz = __byte_perm(n.q[2], 0u, inv.z < 0.0f ? 0x2301u : 0x3210u);
         const float lo = fmaxf(0.0f, tmin);
-        float r[4];
+        if constexpr (kPacked) {
+            // both children side by side: per axis and side one packed FMA
+            // (sm_100) over their planes (codes 0 and 2 near, 1 and 3 far)
+            const float2 nx = __ffma2_rd(make_float2(qw_value(qx, n.scale[0], 0), qw_value(qx, n.scale[0], 2)),
+                                         make_float2(inv.x, inv.x), make_float2(cnx, cnx));
+            const float2 ny = __ffma2_rd(make_float2(qw_value(qy, n.scale[1], 0), qw_value(qy, n.scale[1], 2)),
+                                         make_float2(inv.y, inv.y), make_float2(cny, cny));
+            const float2 nz = __ffma2_rd(make_float2(qw_value(qz, n.scale[2], 0), qw_value(qz, n.scale[2], 2)),
+                                         make_float2(inv.z, inv.z), make_float2(cnz, cnz));
+            const float2 fx2 = __ffma2_ru(make_float2(qw_value(qx, n.scale[0], 1), qw_value(qx, n.scale[0], 3)),
+                                          make_float2(inv.x, inv.x), make_float2(cfx, cfx));
+            const float2 fy2 = __ffma2_ru(make_float2(qw_value(qy, n.scale[1], 1), qw_value(qy, n.scale[1], 3)),
+                                          make_float2(inv.y, inv.y), make_float2(cfy, cfy));
+            const float2 fz2 = __ffma2_ru(make_float2(qw_value(qz, n.scale[2], 1), qw_value(qz, n.scale[2], 3)),
+                                          make_float2(inv.z, inv.z), make_float2(cfz, cfz));
+            const float2 en = make_float2(fmaxf(fmaxf(nx.x, ny.x), nz.x), fmaxf(fmaxf(nx.y, ny.y), nz.y));
+            // entry - 2^-22 entry rounded down: the same as with |entry|
+            // wherever entry >= 0, and both are negative (clipped to lo >= 0)
+            // elsewhere
+            const float2 em = __ffma2_rd(en, make_float2(-kQEntryMargin, -kQEntryMargin), en);
+            const float exa = fminf(fminf(fx2.x, fy2.x), fz2.x), exb = fminf(fminf(fx2.y, fy2.y), fz2.y);
+            return make_float4(fmaxf(em.x, lo), fminf(__fmaf_ru(fabsf(exa), kQExitMargin, exa), hitT),
+                               fmaxf(em.y, lo), fminf(__fmaf_ru(fabsf(exb), kQExitMargin, exb), hitT));
+        } else {
+            float r[4];
 #pragma unroll
-        for (int c = 0; c < 2; ++c) {
-            const float en = fmaxf(fmaxf(__fmaf_rd(qw_value(qx, n.scale[0], 2 * c), inv.x, cnx),
-                                         __fmaf_rd(qw_value(qy, n.scale[1], 2 * c), inv.y, cny)),
-                                   __fmaf_rd(qw_value(qz, n.scale[2], 2 * c), inv.z, cnz));
-            const float ex = fminf(fminf(__fmaf_ru(qw_value(qx, n.scale[0], 2 * c + 1), inv.x, cfx),
-                                         __fmaf_ru(qw_value(qy, n.scale[1], 2 * c + 1), inv.y, cfy)),
-                                   __fmaf_ru(qw_value(qz, n.scale[2], 2 * c + 1), inv.z, cfz));
-            r[2 * c] = fmaxf(__fmaf_rd(fabsf(en), -kQEntryMargin, en), lo);
-            r[2 * c + 1] = fminf(__fmaf_ru(fabsf(ex), kQExitMargin, ex), hitT);
+            for (int c = 0; c < 2; ++c) {
+                const float en = fmaxf(fmaxf(__fmaf_rd(qw_value(qx, n.scale[0], 2 * c), inv.x, cnx),
+                                             __fmaf_rd(qw_value(qy, n.scale[1], 2 * c), inv.y, cny)),
+                                       __fmaf_rd(qw_value(qz, n.scale[2], 2 * c), inv.z, cnz));
+                const float ex = fminf(fminf(__fmaf_ru(qw_value(qx, n.scale[0], 2 * c + 1), inv.x, cfx),
+                                             __fmaf_ru(qw_value(qy, n.scale[1], 2 * c + 1), inv.y, cfy)),
+                                       __fmaf_ru(qw_value(qz, n.scale[2], 2 * c + 1), inv.z, cfz));
+                r[2 * c] = fmaxf(__fmaf_rd(fabsf(en), -kQEntryMargin, en), lo);
+                r[2 * c + 1] = fminf(__fmaf_ru(fabsf(ex), kQExitMargin, ex), hitT);
+            }
+            return make_float4(r[0], r[1], r[2], r[3]);
         }
-        return make_float4(r[0], r[1], r[2], r[3]);
     }
     f3 lo0, hi0, lo1, hi1;
     qnode_box(n, 0, lo0, hi0);
@@ -960,7 +990,7 @@ __device__ __forceinline__ bool quantised_step(uint32_t& curr, uint32_t& prev, H
     }
     if (kCount) ++nv;
     const QNodeWords nd = load_qnode(qnodes, curr, qp.eb);
-    const float4 r = qnode_test(nd, qp, ro, inv, tmin, hit.t);
+    const float4 r = qnode_test<kAny>(nd, qp, ro, inv, tmin, hit.t);
     const float2 rl = make_float2(r.x, r.y), rr = make_float2(r.z, r.w);
     const bool hitL = rl.x <= rl.y, hitR = rr.x <= rr.y;
     uint32_t nearN = nd.c0, farN = nd.c1;
@@ -1043,7 +1073,7 @@ __device__ __forceinline__ bool quantised_replay_step(uint32_t& curr, uint32_t& 
     } else {
         if (kCount) ++nv;
         const QNodeWords nd = load_qnode(qnodes, curr, qp.eb);
-        const float4 r = qnode_test(nd, qp, ro, inv, tmin, hit.t);
+        const float4 r = qnode_test<kAny>(nd, qp, ro, inv, tmin, hit.t);
         const float2 rl = make_float2(r.x, r.y), rr = make_float2(r.z, r.w);
         const bool hitL = rl.x <= rl.y, hitR = rr.x <= rr.y;
         if (hitL && hitR) {
@@ -1137,6 +1167,11 @@ struct WideVisit {
     float entry[4];
 };
 // FP32 slot: three 32-byte plane loads and the 16-byte child words.
+// kPacked computes the slabs as packed FP32 pairs (the same values); the
+// closest-hit walk uses it (camera rays 4 % faster), the any-hit walk does not
+// (AO rays 5 % slower with it). The same holds for qwide_visit (2 % faster,
+// 3.5 % slower).
+template <bool kPacked>
 __device__ __forceinline__ WideVisit wide_visit(const mlbvh_wnode* __restrict__ wnodes, uint32_t i, f3 ro, f3 inv,
                                                 float tmin, float hitT)
 {
@@ -1147,10 +1182,41 @@ __device__ __forceinline__ WideVisit wide_visit(const mlbvh_wnode* __restrict__ 
     ldg32(p + 4, lz, hz);
     WideVisit w{0u, -1, __ldg(reinterpret_cast<const uint4*>(p + 6)), {}};
     float bestT = 0.0f;
+    // kPacked: slab() on two children at a time, each plane's difference and
+    // product as packed FP32 pairs (sm_100), rounded to nearest per
+    // component, so every distance is the scalar slab's bit for bit
+    float en4[4], ex4[4];
+    if constexpr (kPacked) {
+        const float2 nrx = make_float2(-ro.x, -ro.x), nry = make_float2(-ro.y, -ro.y), nrz = make_float2(-ro.z, -ro.z);
+        const float2 ix = make_float2(inv.x, inv.x), iy = make_float2(inv.y, inv.y), iz = make_float2(inv.z, inv.z);
+#pragma unroll
+        for (int p = 0; p < 4; p += 2) {
+            const float2 t0x = __fmul2_rn(__fadd2_rn(make_float2(wpick(lx, p), wpick(lx, p + 1)), nrx), ix);
+            const float2 t1x = __fmul2_rn(__fadd2_rn(make_float2(wpick(hx, p), wpick(hx, p + 1)), nrx), ix);
+            const float2 t0y = __fmul2_rn(__fadd2_rn(make_float2(wpick(ly, p), wpick(ly, p + 1)), nry), iy);
+            const float2 t1y = __fmul2_rn(__fadd2_rn(make_float2(wpick(hy, p), wpick(hy, p + 1)), nry), iy);
+            const float2 t0z = __fmul2_rn(__fadd2_rn(make_float2(wpick(lz, p), wpick(lz, p + 1)), nrz), iz);
+            const float2 t1z = __fmul2_rn(__fadd2_rn(make_float2(wpick(hz, p), wpick(hz, p + 1)), nrz), iz);
+            const float2 rmax = __fmul2_rn(
+                make_float2(fminf(fminf(fmaxf(t0x.x, t1x.x), fmaxf(t0y.x, t1y.x)), fmaxf(t0z.x, t1z.x)),
+                            fminf(fminf(fmaxf(t0x.y, t1x.y), fmaxf(t0y.y, t1y.y)), fmaxf(t0z.y, t1z.y))),
+                make_float2(1.00000024f, 1.00000024f));
+            en4[p] = fmaxf(fmaxf(fmaxf(fmaxf(fminf(t0x.x, t1x.x), fminf(t0y.x, t1y.x)), fminf(t0z.x, t1z.x)), 0.0f),
+                           tmin);
+            en4[p + 1] = fmaxf(
+                fmaxf(fmaxf(fmaxf(fminf(t0x.y, t1x.y), fminf(t0y.y, t1y.y)), fminf(t0z.y, t1z.y)), 0.0f), tmin);
+            ex4[p] = fminf(rmax.x, hitT);
+            ex4[p + 1] = fminf(rmax.y, hitT);
+        }
+    }
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
-        const float2 r = slab(ro, inv, mk(wpick(lx, k), wpick(ly, k), wpick(lz, k)),
-                              mk(wpick(hx, k), wpick(hy, k), wpick(hz, k)), tmin, hitT);
+        float2 r;
+        if constexpr (kPacked)
+            r = make_float2(en4[k], ex4[k]);
+        else
+            r = slab(ro, inv, mk(wpick(lx, k), wpick(ly, k), wpick(lz, k)), mk(wpick(hx, k), wpick(hy, k), wpick(hz, k)),
+                     tmin, hitT);
         w.entry[k] = r.x;
         if (wpick(w.ch, k) != kWideEmpty && r.x <= r.y) {
             w.pass |= 1u << k;
@@ -1179,6 +1245,7 @@ __device__ __forceinline__ WideVisit wide_visit(const mlbvh_wnode* __restrict__ 
 // >= its exit: the test passes wherever the reference's passes on the exact
 // box. Every rounding is directed, so a distance that overflows stays on its
 // conservative side (an FMA rounded down gives FLT_MAX or -inf).
+template <bool kPacked>
 __device__ __forceinline__ WideVisit qwide_visit(const mlbvh_qwnode* __restrict__ qw, uint32_t i, f3 ro, f3 inv,
                                                  float tmin, float hitT)
 {
@@ -1203,16 +1270,52 @@ __device__ __forceinline__ WideVisit qwide_visit(const mlbvh_qwnode* __restrict_
     WideVisit w{0u, -1, make_uint4(__float_as_uint(d.x), __float_as_uint(d.y), __float_as_uint(d.z),
                                    __float_as_uint(d.w)), {}};
     float bestT = 0.0f;
+    // kPacked: two children at a time, per axis and side one packed FMA
+    // (sm_100) over the pair's planes and one for the pair's entry margins
+    float en4[4], ex4[4];
+    if constexpr (kPacked) {
+        const float2 ix = make_float2(inv.x, inv.x), iy = make_float2(inv.y, inv.y), iz = make_float2(inv.z, inv.z);
+#pragma unroll
+        for (int p = 0; p < 4; p += 2) {
+            const float2 nx = __ffma2_rd(make_float2(qw_value(nqx, sx, p), qw_value(nqx, sx, p + 1)), ix,
+                                         make_float2(cnx, cnx));
+            const float2 ny = __ffma2_rd(make_float2(qw_value(nqy, sy, p), qw_value(nqy, sy, p + 1)), iy,
+                                         make_float2(cny, cny));
+            const float2 nz = __ffma2_rd(make_float2(qw_value(nqz, sz, p), qw_value(nqz, sz, p + 1)), iz,
+                                         make_float2(cnz, cnz));
+            const float2 fx2 = __ffma2_ru(make_float2(qw_value(fqx, sx, p), qw_value(fqx, sx, p + 1)), ix,
+                                          make_float2(cfx, cfx));
+            const float2 fy2 = __ffma2_ru(make_float2(qw_value(fqy, sy, p), qw_value(fqy, sy, p + 1)), iy,
+                                          make_float2(cfy, cfy));
+            const float2 fz2 = __ffma2_ru(make_float2(qw_value(fqz, sz, p), qw_value(fqz, sz, p + 1)), iz,
+                                          make_float2(cfz, cfz));
+            const float2 en = make_float2(fmaxf(fmaxf(nx.x, ny.x), nz.x), fmaxf(fmaxf(nx.y, ny.y), nz.y));
+            // entry - 2^-22 entry rounded down: the same as with |entry|
+            // wherever entry >= 0, and both are negative (clipped to lo >= 0)
+            // elsewhere
+            const float2 em = __ffma2_rd(en, make_float2(-kQEntryMargin, -kQEntryMargin), en);
+            const float exa = fminf(fminf(fx2.x, fy2.x), fz2.x), exb = fminf(fminf(fx2.y, fy2.y), fz2.y);
+            en4[p] = fmaxf(em.x, lo);
+            en4[p + 1] = fmaxf(em.y, lo);
+            ex4[p] = fminf(__fmaf_ru(fabsf(exa), kQExitMargin, exa), hitT);
+            ex4[p + 1] = fminf(__fmaf_ru(fabsf(exb), kQExitMargin, exb), hitT);
+        }
+    } else {
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const float en = fmaxf(fmaxf(__fmaf_rd(qw_value(nqx, sx, k), inv.x, cnx),
+                                         __fmaf_rd(qw_value(nqy, sy, k), inv.y, cny)),
+                                   __fmaf_rd(qw_value(nqz, sz, k), inv.z, cnz));
+            const float ex = fminf(fminf(__fmaf_ru(qw_value(fqx, sx, k), inv.x, cfx),
+                                         __fmaf_ru(qw_value(fqy, sy, k), inv.y, cfy)),
+                                   __fmaf_ru(qw_value(fqz, sz, k), inv.z, cfz));
+            en4[k] = fmaxf(__fmaf_rd(fabsf(en), -kQEntryMargin, en), lo);
+            ex4[k] = fminf(__fmaf_ru(fabsf(ex), kQExitMargin, ex), hitT);
+        }
+    }
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
-        const float en = fmaxf(fmaxf(__fmaf_rd(qw_value(nqx, sx, k), inv.x, cnx),
-                                     __fmaf_rd(qw_value(nqy, sy, k), inv.y, cny)),
-                               __fmaf_rd(qw_value(nqz, sz, k), inv.z, cnz));
-        const float ex = fminf(fminf(__fmaf_ru(qw_value(fqx, sx, k), inv.x, cfx),
-                                     __fmaf_ru(qw_value(fqy, sy, k), inv.y, cfy)),
-                               __fmaf_ru(qw_value(fqz, sz, k), inv.z, cfz));
-        const float entry = fmaxf(__fmaf_rd(fabsf(en), -kQEntryMargin, en), lo);
-        const float exit = fminf(__fmaf_ru(fabsf(ex), kQExitMargin, ex), hitT);
+        const float entry = en4[k], exit = ex4[k];
         w.entry[k] = entry;
         if (wpick(w.ch, k) != kWideEmpty && entry <= exit) {
             w.pass |= 1u << k;
@@ -1262,9 +1365,9 @@ __device__ __forceinline__ bool wide_any_step(uint32_t& curr, uint32_t& prev, in
         if (kCount) ++nv;
         WideVisit w;
         if constexpr (kQuant)
-            w = qwide_visit(slots, curr, ro, inv, tmin, hit.t);
+            w = qwide_visit<false>(slots, curr, ro, inv, tmin, hit.t);
         else
-            w = wide_visit(slots, curr, ro, inv, tmin, hit.t);
+            w = wide_visit<false>(slots, curr, ro, inv, tmin, hit.t);
         if (w.pass) {
             const uint32_t others = w.pass & ~(1u << w.best);
             if (depth + __popc(others) > kWideDepth) {
@@ -1338,9 +1441,9 @@ __device__ __forceinline__ bool wide_closest_step(uint32_t& curr, uint32_t& prev
         if (kCount) ++nv;
         WideVisit w;
         if constexpr (kQuant)
-            w = qwide_visit(slots, curr, ro, inv, tmin, hit.t);
+            w = qwide_visit<true>(slots, curr, ro, inv, tmin, hit.t);
         else
-            w = wide_visit(slots, curr, ro, inv, tmin, hit.t);
+            w = wide_visit<true>(slots, curr, ro, inv, tmin, hit.t);
         if (w.pass) {
             const int np = __popc(w.pass);
             if (depth + np - 1 > kWideDepth) {
