@@ -423,6 +423,28 @@ def test_directed_fma_emulation_is_exact():
             assert got == want or (np.isinf(got) and np.isinf(want) and got == want), (a, b, c, up, got, want)
 
 
+def test_entry_margin_without_abs_after_clip():
+    """The packed slab tests move an entry down by 2^-22 of itself rather
+    than of its magnitude (entry - 2^-22 entry rounded down, no |.| in a
+    packed FMA). After the clip to lo = max(0, tmin) that is the scalar form
+    max(entry - 2^-22 |entry| rounded down, lo) on every finite entry: equal
+    where entry >= 0, both negative (so lo) where entry < 0, including
+    subnormal entries, signed zeros and -FLT_MAX (whose scalar margin
+    overflows to -inf)."""
+    m = np.float32(2.384185791015625e-07)  # 2^-22
+    rng = np.random.default_rng(11)
+    ens = [np.float32(s * rng.random() * 2.0 ** rng.integers(-149, 127)) for s in (1, -1) for _ in range(2000)]
+    ens += [np.float32(v) for v in (0.0, -0.0, 1e-45, -1e-45, 3e-45, -3e-45, 1.17549435e-38, -1.17549435e-38,
+                                    3.4028235e38, -3.4028235e38, 1.0, -1.0)]
+    los = [np.float32(0.0), np.float32(1e-45), np.float32(1e-3), np.float32(2.5)]
+    fma = O.oracle().orc_fma_dir
+    for en in ens:
+        scalar = np.float32(fma(float(abs(en)), float(-m), float(en), 0))
+        packed = np.float32(fma(float(en), float(-m), float(en), 0))
+        for lo in los:
+            assert max(scalar, lo) == max(packed, lo), (en, lo, scalar, packed)
+
+
 
 def _axis_rays(n, lo, hi, seed):
     """Random rays, a third of them with one direction component exactly 0
