@@ -990,7 +990,7 @@ __device__ __forceinline__ bool quantised_step(uint32_t& curr, uint32_t& prev, H
     }
     if (kCount) ++nv;
     const QNodeWords nd = load_qnode(qnodes, curr, qp.eb);
-    const float4 r = qnode_test<kAny>(nd, qp, ro, inv, tmin, hit.t);
+    const float4 r = qnode_test<kAny>(nd, qp, ro, inv, tmin, hit.t);  // packed pairs on any-hit walks
     const float2 rl = make_float2(r.x, r.y), rr = make_float2(r.z, r.w);
     const bool hitL = rl.x <= rl.y, hitR = rr.x <= rr.y;
     uint32_t nearN = nd.c0, farN = nd.c1;
@@ -1073,7 +1073,7 @@ __device__ __forceinline__ bool quantised_replay_step(uint32_t& curr, uint32_t& 
     } else {
         if (kCount) ++nv;
         const QNodeWords nd = load_qnode(qnodes, curr, qp.eb);
-        const float4 r = qnode_test<kAny>(nd, qp, ro, inv, tmin, hit.t);
+        const float4 r = qnode_test<kAny>(nd, qp, ro, inv, tmin, hit.t);  // packed pairs on any-hit walks
         const float2 rl = make_float2(r.x, r.y), rr = make_float2(r.z, r.w);
         const bool hitL = rl.x <= rl.y, hitR = rr.x <= rr.y;
         if (hitL && hitR) {
@@ -1215,8 +1215,8 @@ __device__ __forceinline__ WideVisit wide_visit(const mlbvh_wnode* __restrict__ 
         if constexpr (kPacked)
             r = make_float2(en4[k], ex4[k]);
         else
-            r = slab(ro, inv, mk(wpick(lx, k), wpick(ly, k), wpick(lz, k)), mk(wpick(hx, k), wpick(hy, k), wpick(hz, k)),
-                     tmin, hitT);
+            r = slab(ro, inv, mk(wpick(lx, k), wpick(ly, k), wpick(lz, k)),
+                     mk(wpick(hx, k), wpick(hy, k), wpick(hz, k)), tmin, hitT);
         w.entry[k] = r.x;
         if (wpick(w.ch, k) != kWideEmpty && r.x <= r.y) {
             w.pass |= 1u << k;
